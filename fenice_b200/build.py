@@ -1,0 +1,57 @@
+"""Builds the CUDA library of the package in-tree: fenice_b200/libfenice_gpu.so (sm_100a only).
+
+    python -m fenice_b200.build            # or: python fenice_b200/build.py
+
+The library is plain nvcc output with a C ABI (include/fenice_gpu.h); it does not link PyTorch. The floating-point
+flags are part of the numerics: --fmad=false keeps every multiply and add separately rounded (the reference is built
+with -ffp-contract=off), and double division and square root are IEEE-rounded, so the FP64 kernels give the
+reference's bits.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+SRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libfenice_gpu.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+SOURCES = ["runtime.cu"]
+HEADERS = ["physics.cuh", "grid.cuh", "stage.cuh", "viscous.cuh", "hancock.cuh"]
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17",
+    "--fmad=false", "-prec-div=true", "-prec-sqrt=true",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+    "-I" + os.path.join(ROOT, "include"),
+    "--cudart", "static",
+]
+
+
+def _stale():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(SRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "fenice_gpu.h"), __file__]
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(force=False, verbose=False, extra=()):
+    if not force and not _stale():
+        return LIB
+    cmd = [NVCC] + NVCC_FLAGS + list(extra) + ["-shared", "-o", LIB] + [os.path.join(SRC, f) for f in SOURCES]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("nvcc failed building " + LIB)
+    if verbose and (r.stdout or r.stderr):
+        print(r.stdout + r.stderr)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True, extra=[a for a in sys.argv[1:] if a != "--force"])

@@ -1,0 +1,192 @@
+// The mesh, its boundary conditions and the device-side control block of a run.
+//
+// HBM layout: the conservative state is stored as NV planes (structure of arrays), NV = 4 on a 2-D mesh
+// ([rho, rho u, rho v, rho E]; the reference's rho w is identically +0 there) and 5 on a 3-D mesh; plane q of
+// cell (i, j, k) is at q * plane + (k * ny + j) * nx + i, the reference's row-major cell order
+// (cpp/include/fv/Core.hpp:114). `plane` is the cell count rounded up to 32 so every plane starts on a 256-byte
+// boundary.
+#pragma once
+
+#include "physics.cuh"
+
+namespace fvg {
+
+// boundary types, in the order of the reference's BCType (cpp/include/fv/Boundaries.hpp:15)
+constexpr int kBcWall = 0, kBcNoSlip = 1, kBcMovingWall = 2, kBcVelInlet = 3, kBcMassflowInlet = 4, kBcOutlet = 5,
+              kBcTransmissive = 6, kBcPeriodic = 7, kBcNonReflecting = 8;
+// what lies beyond a side for the reconstruction stencil (cpp/src/Simulation.cpp:868-905): nothing (edge
+// replication, first-order boundary faces), the periodic wrap, or the ghost slab of the boundary condition
+constexpr int kHaloNone = 0, kHaloWrap = 1, kHaloSlab = 2;
+
+// Device control block of a run: the clock, the step and the wave speeds, all on the device so a step needs no
+// host round trip (and can be captured in a CUDA graph).
+struct Ctl {
+    double t, t_end, dt, dt_max, cfl, L;
+    double s_lag;       // MUSCL-Hancock: wave speed of the previous step (0: none yet)
+    double s_step;      // largest wave speed of the current step
+    double s_stage[3];  // wave speed of each stage of the step
+    double half_dt;     // MUSCL-Hancock: half the step the predictor advances the face states by
+    int active;         // this step runs (t < t_end, steps < max_steps, no error)
+    int seed;           // MUSCL-Hancock: this step first takes one plain residual for the wave speed
+    int always;         // 1: the gate of calls outside the time loop
+    int steps, max_steps;
+    int status;         // 0 ok; 1 the solution diverged (non-finite speed or dt, or t no longer advances)
+};
+
+struct Mesh {
+    int nx, ny, nz;
+    long long ncells, plane;
+    double dx, dy, dz;
+    double area[3];   // face areas used by the balance: 2-D (dy, dx); 3-D (dy dz, dx dz, dx dy)
+    double inv_cell;  // 1 / cell area (2-D) or 1 / cell volume (3-D)
+};
+
+struct Bc {
+    int type[6];   // left, right, bottom, top, front, back
+    int halo[6];   // kHalo* of each side for the reconstruction stencil
+    double u_in, v_in, p_out;
+};
+
+// BoundaryManager::ghost_state (cpp/src/Boundaries.cpp:106-153) for the sides a device run supports (every type but
+// the mass-flow inlet and the non-reflecting outlet, which need more than one cell).
+template <typename T, int NV>
+__device__ __forceinline__ St<T, NV> ghost_state(const Eos<T>& e, const Bc& bc, int side, const St<T, NV>& Ui) {
+    const int type = bc.type[side];
+    if (type == kBcTransmissive) return Ui;
+    const int axis = side >> 1;
+    const T nxn = axis == 0 ? T(1) : T(0), nyn = axis == 1 ? T(1) : T(0), nzn = axis == 2 ? T(1) : T(0);
+    const St<T, NV> Wi = c2p(e, Ui);
+    St<T, NV> Wg = Wi;
+    const T wi = NV == 5 ? Wi[NV - 1] : T(0);   // the z velocity (+0 on a planar mesh, as in the reference)
+    switch (type) {
+    case kBcWall: {
+        const T Vn = Wi[1] * nxn + Wi[2] * nyn + wi * nzn;
+        Wg[1] = Wi[1] - T(2) * Vn * nxn;
+        Wg[2] = Wi[2] - T(2) * Vn * nyn;
+        if constexpr (NV == 5) Wg[4] = Wi[4] - T(2) * Vn * nzn;
+        break;
+    }
+    case kBcNoSlip:
+        Wg[1] = -Wi[1];
+        Wg[2] = -Wi[2];
+        if constexpr (NV == 5) Wg[4] = -Wi[4];
+        break;
+    case kBcMovingWall:
+    case kBcVelInlet:
+        Wg[1] = T(2) * T(bc.u_in) - Wi[1];
+        Wg[2] = T(2) * T(bc.v_in) - Wi[2];
+        if constexpr (NV == 5) Wg[4] = -Wi[4];
+        break;
+    case kBcOutlet: {
+        const T Vn = Wi[1] * nxn + Wi[2] * nyn + wi * nzn;
+        const bool outflow = Vn >= T(0);
+        Wg[1] = outflow ? Wi[1] : T(0);
+        Wg[2] = outflow ? Wi[2] : T(0);
+        if constexpr (NV == 5) Wg[4] = outflow ? Wi[4] : T(0);
+        Wg[3] = vmax(T(bc.p_out), T(1e-5));
+        break;
+    }
+    default: break;
+    }
+    return p2c(e, Wg);
+}
+
+template <int NV> __device__ __forceinline__ St<double, NV> read_cell(const double* __restrict__ U, long long plane, long long c) {
+    St<double, NV> s;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) s[q] = U[q * plane + c];
+    return s;
+}
+
+// The conservative state at cell position (i, j, k) of the reconstruction stencil, which may lie outside the mesh along
+// one axis: the periodic wrap, the ghost-slab state of the mirrored cell (fill_ghost_slab, cpp/src/Boundaries.cpp:202-228:
+// layer l beyond the side is ghost_state of the interior cell l cells from it), or edge replication (pad_primitives,
+// cpp/src/Schemes.cpp:915-969). Positions outside along two axes (never on a stencil of a face of the mesh) and those of a
+// tile that overhangs the mesh are clamped, so every read is inside the state arrays.
+template <int DIM, int NV>
+__device__ __forceinline__ St<double, NV> stencil_cons(const Mesh& m, const Bc& bc, const Eos<double>& e, const double* __restrict__ U, int i, int j,
+                                                       int k) {
+    int idx[3] = {i, j, k};
+    const int n3[3] = {m.nx, m.ny, m.nz};
+    int out_axis = -1, nout = 0;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+        const bool lo = idx[a] < 0, hi = idx[a] >= n3[a];
+        if (!lo && !hi) continue;
+        if (bc.halo[2 * a + (hi ? 1 : 0)] == kHaloWrap) {
+            idx[a] = ((idx[a] % n3[a]) + n3[a]) % n3[a];
+            continue;
+        }
+        out_axis = a;
+        ++nout;
+    }
+    if (nout == 1) {
+        const int a = out_axis;
+        const bool hi = idx[a] >= n3[a];
+        const int side = 2 * a + (hi ? 1 : 0);
+        if (bc.halo[side] == kHaloSlab) {
+            int l = hi ? idx[a] - n3[a] : -1 - idx[a];
+            l = l < n3[a] ? l : n3[a] - 1;
+            idx[a] = hi ? n3[a] - 1 - l : l;
+            const long long c = ((long long)idx[2] * m.ny + idx[1]) * m.nx + idx[0];
+            return ghost_state(e, bc, side, read_cell<NV>(U, m.plane, c));
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) idx[a] = idx[a] < 0 ? 0 : (idx[a] >= n3[a] ? n3[a] - 1 : idx[a]);
+    const long long c = ((long long)idx[2] * m.ny + idx[1]) * m.nx + idx[0];
+    return read_cell<NV>(U, m.plane, c);
+}
+
+// The first-order states of a boundary face whose side has no halo (BoundaryManager::apply_side,
+// cpp/src/Boundaries.cpp:277-373): the cell next to the side and its ghost (the opposite cell on a periodic side).
+template <int NV>
+__device__ __forceinline__ void side_states(const Mesh& m, const Bc& bc, const Eos<double>& e, const double* __restrict__ U, int side, int i, int j, int k,
+                                            St<double, NV>& UL, St<double, NV>& UR) {
+    const long long c = ((long long)k * m.ny + j) * m.nx + i;
+    const St<double, NV> Ui = read_cell<NV>(U, m.plane, c);
+    St<double, NV> Ug;
+    if (bc.type[side] == kBcPeriodic) {
+        int idx[3] = {i, j, k};
+        const int a = side >> 1, n = a == 0 ? m.nx : (a == 1 ? m.ny : m.nz);
+        idx[a] = (side & 1) ? idx[a] - (n - 1) : idx[a] + (n - 1);
+        Ug = read_cell<NV>(U, m.plane, ((long long)idx[2] * m.ny + idx[1]) * m.nx + idx[0]);
+    } else {
+        Ug = ghost_state(e, bc, side, Ui);
+    }
+    if (side & 1) {
+        UL = Ui;
+        UR = Ug;
+    } else {
+        UL = Ug;
+        UR = Ui;
+    }
+}
+
+// Warp and block maximum of a wave speed with the reference's rule `if (s > local) local = s` (a NaN never wins).
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double w = __shfl_xor_sync(0xffffffffu, v, o);
+        if (w > v) v = w;
+    }
+    return v;
+}
+
+template <int NT> __device__ __forceinline__ double block_max(double v, double* red) {
+    v = warp_max(v);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int NW = (NT + 31) / 32;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0) {
+        r = red[0];
+        for (int w = 1; w < NW; ++w)
+            if (red[w] > r) r = red[w];
+    }
+    return r;
+}
+
+}   // namespace fvg

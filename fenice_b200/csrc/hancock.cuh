@@ -1,0 +1,224 @@
+// The MUSCL-Hancock residual of a 2-D mesh, fused with its update: the limited face states of every cell, advanced by
+// half a step with the cell's own flux difference (predictor), then the Riemann solves and the flux balance
+// (MusclReconstruction::hancock_residual_2d, cpp/src/Schemes.cpp:2135-2477 and 2782-2830).
+//
+// A CTA owns a TX x TY tile:
+//   1. the primitive state of the tile and two cells around it (boundary conditions by index mapping);
+//   2. the four limited states (low / high side along x and y) of the tile's cells and of the ring of cells around it,
+//      predicted for every cell of the mesh (the ring's wrapped cells of a periodic axis included); a ring position
+//      beyond another side keeps the unpredicted state, which is what the reference puts on a face of a side with a
+//      ghost slab (stencil_face_state); at a side without a halo the cell's own state there is the round trip of the
+//      cell (hancock_row); a state the predictor would make inadmissible stays as it was (hancock_cell);
+//   3. the x faces, then the y faces: left state = high-side state of the cell before the face, right state = low-side
+//      state of the cell after it; on a wall side the ghost is the wall state of the predicted cell state, on a side
+//      without a halo the round trip of the first-order ghost (hancock_xfaces / hancock_yfaces);
+//   4. the balance ((0 - (Fr dy - Fl dy)) - (Ft dx - Fb dx)) / area and the update U + dt R (or R alone).
+#pragma once
+
+#include "grid.cuh"
+
+namespace fvg {
+
+struct HancockArgs {
+    Mesh m;
+    Bc bc;
+    Eos<double> eos;
+    double shock_blend;
+    int limiter;
+    int mode;          // kStoreR or kAxpy
+    const double* U;
+    double* out;
+    double* blockmax;
+    const Ctl* ctl;    // dt and half_dt
+    const int* gate;
+    int tiles[3];
+};
+
+template <int TX, int TY> struct HancockShape {
+    static constexpr int PX = TX + 4, PY = TY + 4;   // primitive box
+    static constexpr int BX = TX + 2, BY = TY + 2;   // predicted-state box
+    static constexpr int NF = (TX + 1) * TY > TX * (TY + 1) ? (TX + 1) * TY : TX * (TY + 1);
+    // P [4][PX*PY], S [4 states][4][BX*BY], F [4][NF], acc [4][TX*TY], red [32]
+    static constexpr int SMEM_DOUBLES = 4 * PX * PY + 16 * BX * BY + 4 * NF + 4 * TX * TY + 32;
+    static constexpr size_t SMEM_BYTES = sizeof(double) * SMEM_DOUBLES;
+};
+
+// euler_flux_axis (Schemes.cpp:2137-2141) of a planar state
+__device__ __forceinline__ St<double, 4> euler_flux2(const Eos<double>& e, const St<double, 4>& U, int a) {
+    const St<double, 4> W = c2p(e, U);
+    const double un = a == 0 ? W[1] : W[2], p = W[3];
+    St<double, 4> F;
+    F[0] = U[0] * un;
+    F[1] = U[1] * un + (a == 0 ? p : 0.0);
+    F[2] = U[2] * un + (a == 1 ? p : 0.0);
+    F[3] = (U[3] + p) * un;
+    return F;
+}
+
+// admissible_state (Schemes.cpp:2145-2148): rho > floor and p + p_inf > 0, NaN inadmissible
+__device__ __forceinline__ bool admissible(const Eos<double>& e, const St<double, 4>& U) {
+    if (!(U[0] > Num<double>::eos_eps)) return false;
+    return 0.5 * (U[1] * U[1] + U[2] * U[2] + 0.0 * 0.0) < U[0] * (U[3] - e.p_inf);
+}
+
+template <int RIEMANN, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) hancock_kernel(const HancockArgs a) {
+    using S = HancockShape<TX, TY>;
+    constexpr int PX = S::PX, PY = S::PY, BX = S::BX, BY = S::BY, NB = BX * BY, NP = PX * PY, NC = TX * TY;
+    extern __shared__ double smem[];
+    double* P = smem;                  // [4][NP]
+    double* Sx = P + 4 * NP;           // [state 0..3: xl, xr, yb, yt][4][NB]
+    double* Fl = Sx + 16 * NB;         // [4][NF]
+    double* acc = Fl + 4 * S::NF;      // [4][NC]
+    double* red = acc + 4 * NC;
+    if (!*a.gate) return;
+    const Mesh& m = a.m;
+    const Eos<double>& e = a.eos;
+    const int tid = threadIdx.x, b = blockIdx.x;
+    const int ox = (b % a.tiles[0]) * TX, oy = (b / a.tiles[0]) * TY;
+    const int nx = m.nx, ny = m.ny;
+    const double half_dt = a.ctl->half_dt;
+    const double hx = half_dt / m.dx, hy = half_dt / m.dy;
+
+    // ---- 1. primitive box: cells ox-2 .. ox+TX+1, oy-2 .. oy+TY+1
+    for (int p = tid; p < NP; p += NT) {
+        const int i = ox + p % PX - 2, j = oy + p / PX - 2;
+        const St<double, 4> w = c2p(e, stencil_cons<2, 4>(m, a.bc, e, a.U, i, j, 0));
+#pragma unroll
+        for (int q = 0; q < 4; ++q) P[q * NP + p] = w[q];
+    }
+    __syncthreads();
+    // ---- 2. the four states of the cells ox-1 .. ox+TX, oy-1 .. oy+TY (not the four corners)
+    const bool wrap_x = a.bc.halo[0] == kHaloWrap, wrap_y = a.bc.halo[2] == kHaloWrap;
+    for (int p = tid; p < NB; p += NT) {
+        const int bi = p % BX, bj = p / BX;
+        if ((bi == 0 || bi == BX - 1) && (bj == 0 || bj == BY - 1)) continue;
+        const int gi = ox + bi - 1, gj = oy + bj - 1;
+        const int pc = (bj + 1) * PX + (bi + 1);   // the cell in the primitive box
+        St<double, 4> st[4];
+        // muscl_cell_states_line (Schemes.cpp:2204-2229): hi = c + 1/2 phi(c - cm, cp - c), lo = c - 1/2 phi(cp - c, c - cm)
+#pragma unroll
+        for (int ax = 0; ax < 2; ++ax) {
+            const int s = ax == 0 ? 1 : PX;
+            St<double, 4> wl, wr;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const double cm = P[q * NP + pc - s], c = P[q * NP + pc], cp = P[q * NP + pc + s];
+                wl[q] = c + 0.5 * limiter(a.limiter, c - cm, cp - c);
+                wr[q] = c - 0.5 * limiter(a.limiter, cp - c, c - cm);
+            }
+            st[2 * ax + 1] = p2c(e, wl);
+            st[2 * ax] = p2c(e, wr);
+        }
+        const bool in_x = gi >= 0 && gi < nx, in_y = gj >= 0 && gj < ny;
+        const bool real = (in_x || wrap_x) && (in_y || wrap_y) && gi < nx + 1 && gj < ny + 1 && gi >= -1 && gj >= -1;
+        if (real) {
+            // the mesh cell (wrapped): sides without a halo give it the round trip of its own state there
+            const int ci = (gi + nx) % nx, cj = (gj + ny) % ny;
+            const bool b0 = ci == 0 && a.bc.halo[0] == kHaloNone, b1 = ci == nx - 1 && a.bc.halo[1] == kHaloNone;
+            const bool b2 = cj == 0 && a.bc.halo[2] == kHaloNone, b3 = cj == ny - 1 && a.bc.halo[3] == kHaloNone;
+            if (b0 || b1 || b2 || b3) {
+                const St<double, 4> rt = round_trip(e, read_cell<4>(a.U, m.plane, (long long)cj * nx + ci));
+                if (b0) st[0] = rt;
+                if (b1) st[1] = rt;
+                if (b2) st[2] = rt;
+                if (b3) st[3] = rt;
+            }
+            // hancock_cell (Schemes.cpp:2153-2172)
+            const St<double, 4> fxl = euler_flux2(e, st[0], 0), fxr = euler_flux2(e, st[1], 0);
+            const St<double, 4> fyb = euler_flux2(e, st[2], 1), fyt = euler_flux2(e, st[3], 1);
+            St<double, 4> d;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) d[q] = hx * (fxr[q] - fxl[q]) + hy * (fyt[q] - fyb[q]);
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                St<double, 4> n;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) n[q] = st[s][q] - d[q];
+                if (admissible(e, n)) st[s] = n;
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) Sx[(s * 4 + q) * NB + p] = st[s][q];
+    }
+    __syncthreads();
+    double smax = 0.0;
+    // ---- 3. faces: axis 0 (x), then axis 1 (y)
+#pragma unroll 1
+    for (int axis = 0; axis < 2; ++axis) {
+        const int FX = TX + (axis == 0), FY = TY + (axis == 1);
+        const int nF = FX * FY;
+        const int lo_side = 2 * axis, hi_side = lo_side + 1;
+        const bool wall_lo = a.bc.type[lo_side] == kBcWall || a.bc.type[lo_side] == kBcNoSlip || a.bc.type[lo_side] == kBcMovingWall;
+        const bool wall_hi = a.bc.type[hi_side] == kBcWall || a.bc.type[hi_side] == kBcNoSlip || a.bc.type[hi_side] == kBcMovingWall;
+        for (int f = tid; f < nF; f += NT) {
+            const int fi = f % FX, fj = f / FX;
+            const int gi = ox + fi, gj = oy + fj;
+            const int n_a = axis == 0 ? nx : ny, t = axis == 0 ? gi : gj;
+            const bool inside = axis == 0 ? (gi <= nx && gj < ny) : (gi < nx && gj <= ny);
+            St<double, 4> F;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) F[q] = 0.0;
+            if (inside) {
+                // the cells before and after the face in the state box
+                const int pR = (fj + 1) * BX + (fi + 1);
+                const int pL = axis == 0 ? pR - 1 : pR - BX;
+                const int sL = axis == 0 ? 1 : 3, sR = axis == 0 ? 0 : 2;   // high-side state of L, low-side state of R
+                St<double, 4> UL, UR;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    UL[q] = Sx[(sL * 4 + q) * NB + pL];
+                    UR[q] = Sx[(sR * 4 + q) * NB + pR];
+                }
+                if (t == 0) {
+                    if (wall_lo)
+                        UL = ghost_state(e, a.bc, lo_side, UR);
+                    else if (a.bc.halo[lo_side] == kHaloNone)
+                        UL = round_trip(e, ghost_state(e, a.bc, lo_side, read_cell<4>(a.U, m.plane, (long long)gj * nx + gi)));
+                }
+                if (t == n_a) {
+                    const int ci = axis == 0 ? nx - 1 : gi, cj = axis == 0 ? gj : ny - 1;
+                    if (wall_hi)
+                        UR = ghost_state(e, a.bc, hi_side, UL);
+                    else if (a.bc.halo[hi_side] == kHaloNone)
+                        UR = round_trip(e, ghost_state(e, a.bc, hi_side, read_cell<4>(a.U, m.plane, (long long)cj * nx + ci)));
+                }
+                const double s = face_flux<RIEMANN>(e, a.shock_blend, UL, UR, axis, F);
+                if (s > smax) smax = s;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) Fl[q * S::NF + f] = F[q];
+        }
+        __syncthreads();
+        const double A = m.area[axis];
+        for (int c = tid; c < NC; c += NT) {
+            const int ci = c % TX, cj = c / TX;
+            const int fl = cj * FX + ci, fr = fl + (axis == 0 ? 1 : FX);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const double dd = Fl[q * S::NF + fr] * A - Fl[q * S::NF + fl] * A;
+                acc[q * NC + c] = axis == 0 ? 0.0 - dd : acc[q * NC + c] - dd;
+            }
+        }
+        __syncthreads();
+    }
+    // ---- 4. the residual and the update
+    const double dt = a.ctl->dt;
+    for (int c = tid; c < NC; c += NT) {
+        const int gi = ox + c % TX, gj = oy + c / TX;
+        if (gi >= nx || gj >= ny) continue;
+        const long long cell = (long long)gj * nx + gi;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const double r = acc[q * NC + c] * m.inv_cell;
+            const long long x = q * m.plane + cell;
+            a.out[x] = a.mode == 0 ? r : a.U[x] + dt * r;
+        }
+    }
+    const double bm = block_max<NT>(smax, red);
+    if (tid == 0) a.blockmax[b] = bm;
+}
+
+}   // namespace fvg

@@ -1,0 +1,797 @@
+// Host runtime of the B200 finite-volume path and its C ABI (include/fenice_gpu.h).
+//
+// A run owns its device arrays (the state, a stage state, a residual / stage buffer, the viscous residual, per-CTA
+// wave-speed maxima) and a control block on the device (grid.cuh: Ctl) that holds the clock, dt and the wave speeds, so
+// the time loop never waits for the host: every step is a fixed sequence of kernel launches, captured once into a CUDA
+// graph and replayed.
+//
+// Step sequences (the reference's TimeScheme::step, cpp/src/TimeScheme.cpp:110-319):
+//   Euler:    [viscous] stage(U -> R) ; dt ; U = U + dt R ; end
+//   SSP-RK2:  [viscous] stage(U -> R) ; dt ; Ut = U + dt R ; [viscous] stage(Ut, U0 = U -> U: 1/2 U0 + 1/2 (Ut + dt R)) ; end
+//   SSP-RK3:  [viscous] stage(U -> R) ; dt ; Ut = U + dt R ; [viscous] stage(Ut, U0 = U -> R: 3/4 U0 + 1/4 (Ut + dt R)) ;
+//             [viscous] stage(R, U0 = U -> U: 1/3 U0 + 2/3 (R + dt R3)) ; end
+//   MUSCL-Hancock: seed (first step only: one plain residual for the wave speed) ; dt from the lagged speed ;
+//             hancock(U -> Ut = U + dt R) ; end (the speed of this step is the next step's) ; the state then lives in Ut
+//             (ping-pong, tracked by the host).
+// "dt" reduces the CTA maxima of stage 1 into s1 and sets dt = cfl L / (s1 + 1e-10), clamped to t_end - t and dt_max;
+// "end" reduces the later stages, applies check_progress, advances t and the step count and decides whether the next
+// step runs (t < t_end, step limit, no error).
+#include "../../include/fenice_gpu.h"
+#include "hancock.cuh"
+#include "stage.cuh"
+#include "viscous.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace fvg;
+
+namespace {
+
+constexpr double kDtEps = 1e-10;   // TimeScheme.cpp:19
+thread_local std::string g_create_error;
+
+// ------------------------------------------------------------------------------------------------ control kernels
+__device__ double block_reduce_max(const double* a, int n, const double* b, int nb) {
+    __shared__ double red[32];
+    double v = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (a[i] > v) v = a[i];
+    for (int i = threadIdx.x; i < nb; i += blockDim.x)
+        if (b[i] > v) v = b[i];
+    v = warp_max(v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w)
+            if (red[w] > r) r = red[w];
+    return r;
+}
+
+__device__ __forceinline__ void set_next_active(Ctl* c) {
+    c->active = (c->t < c->t_end) && (c->max_steps <= 0 || c->steps < c->max_steps) && c->status == 0;
+}
+
+__global__ void k_begin(Ctl* c, double t_end, int max_steps) {
+    c->t_end = t_end;
+    c->max_steps = max_steps;
+    c->steps = 0;
+    c->status = 0;
+    set_next_active(c);
+}
+
+// stage 1 of a Runge-Kutta / Euler step: its wave speed and the step dt
+__global__ void k_stage1_dt(Ctl* c, const double* bm, int nb, const double* bmv, int nbv) {
+    if (!c->active) return;
+    const double s = block_reduce_max(bm, nb, bmv, nbv);
+    if (threadIdx.x == 0) {
+        c->s_stage[0] = s;
+        double dt = c->cfl * c->L / (s + kDtEps);
+        dt = vmin(dt, c->t_end - c->t);
+        if (c->dt_max > 0.0) dt = vmin(dt, c->dt_max);
+        c->dt = dt;
+    }
+}
+
+__global__ void k_stage_max(Ctl* c, const int* gate, int stage, const double* bm, int nb, const double* bmv, int nbv) {
+    if (!*gate) return;
+    const double s = block_reduce_max(bm, nb, bmv, nbv);
+    if (threadIdx.x == 0) c->s_stage[stage] = s;
+}
+
+// check_progress (cpp/src/SimulationInternal.hpp:259-267), t += dt, and whether the next step runs
+__device__ void finish_step(Ctl* c, double s) {
+    c->s_step = s;
+    if (!(isfinite(s) && isfinite(c->dt) && c->t + c->dt > c->t)) {
+        c->status = 1;
+        c->active = 0;
+        return;
+    }
+    c->t = c->t + c->dt;
+    c->steps += 1;
+    set_next_active(c);
+}
+
+// end of a Runge-Kutta / Euler step with `nstages` stages: S = max(s1, max(s2, s3))
+__global__ void k_end_rk(Ctl* c, int nstages) {
+    if (!c->active) return;
+    double s = c->s_stage[0];
+    if (nstages == 2) s = vmax(c->s_stage[0], c->s_stage[1]);
+    if (nstages == 3) s = vmax(c->s_stage[0], vmax(c->s_stage[1], c->s_stage[2]));
+    finish_step(c, s);
+}
+
+// MUSCL-Hancock (MusclHancock::step, TimeScheme.cpp:296-319)
+__global__ void k_hancock_begin(Ctl* c) { c->seed = c->active && !(c->s_lag > 0.0); }
+__global__ void k_hancock_seed(Ctl* c, const double* bm, int nb) {
+    if (!c->seed) return;
+    const double s = block_reduce_max(bm, nb, bm, 0);
+    if (threadIdx.x == 0) c->s_lag = s;
+}
+__global__ void k_hancock_dt(Ctl* c) {
+    if (!c->active) return;
+    double dt = c->cfl * c->L / (c->s_lag + kDtEps);
+    dt = vmin(dt, c->t_end - c->t);
+    if (c->dt_max > 0.0) dt = vmin(dt, c->dt_max);
+    c->dt = dt;
+    c->half_dt = 0.5 * dt;
+}
+__global__ void k_hancock_end(Ctl* c, const double* bm, int nb) {
+    if (!c->active) return;
+    const double s = block_reduce_max(bm, nb, bm, 0);
+    if (threadIdx.x == 0) {
+        c->s_lag = s;
+        finish_step(c, s);
+    }
+}
+
+// out = a + dt b over the state planes (TimeScheme.cpp:27-59: axpy)
+__global__ void k_axpy(const Ctl* c, double* out, const double* a, const double* b, long long plane, long long n, int nvar) {
+    if (!c->active) return;
+    const double dt = c->dt;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n * nvar; e += (long long)gridDim.x * blockDim.x) {
+        const long long q = e / n, i = e % n;
+        const long long x = q * plane + i;
+        out[x] = a[x] + dt * b[x];
+    }
+}
+
+// reference layout (cells of 5 doubles) <-> state planes; a 2-D mesh carries no rho w (it must be zero)
+__global__ void k_aos_to_planes(const double* aos, double* U, long long plane, long long n, int nvar, int* bad) {
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        for (int q = 0; q < nvar; ++q) U[q * plane + c] = aos[5 * c + q];
+        if (nvar == 4 && aos[5 * c + 4] != 0.0) atomicOr(bad, 1);
+    }
+}
+__global__ void k_planes_to_aos(const double* U, double* aos, long long plane, long long n, int nvar) {
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        for (int q = 0; q < 5; ++q) aos[5 * c + q] = q < nvar ? U[q * plane + c] : 0.0;
+    }
+}
+
+template <int RIEMANN, int NV>
+__global__ void k_face_flux(Eos<double> e, double shock_blend, const double* UL, const double* UR, const int* axis, long long n, double* F, double* sm) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        St<double, NV> ul, ur, f;
+        for (int q = 0; q < NV; ++q) {
+            ul[q] = UL[5 * k + q];
+            ur[q] = UR[5 * k + q];
+        }
+        sm[k] = face_flux<RIEMANN>(e, shock_blend, ul, ur, axis[k], f);
+        for (int q = 0; q < NV; ++q) F[5 * k + q] = f[q];
+    }
+}
+
+// ------------------------------------------------------------------------------------------------ kernel dispatch
+template <int DIM> struct Tile;
+template <> struct Tile<3> { static constexpr int X = 8, Y = 8, Z = 8, NT = 192; };
+template <> struct Tile<2> { static constexpr int X = 16, Y = 15, Z = 1, NT = 256; };
+
+// Each kernel gets its shared-memory limit raised once, when a run is created (never during a graph capture).
+template <int DIM, int RECON, int RIEMANN> struct StageK {
+    using Tl = Tile<DIM>;
+    using S = StageShape<DIM, RECON, Tl::X, Tl::Y, Tl::Z>;
+    static cudaError_t prepare() {
+        return cudaFuncSetAttribute(stage_kernel<DIM, RECON, RIEMANN, Tl::X, Tl::Y, Tl::Z, Tl::NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)S::SMEM_BYTES);
+    }
+    static cudaError_t launch(const StageArgs& a, int nblocks, cudaStream_t s) {
+        stage_kernel<DIM, RECON, RIEMANN, Tl::X, Tl::Y, Tl::Z, Tl::NT><<<nblocks, Tl::NT, S::SMEM_BYTES, s>>>(a);
+        return cudaGetLastError();
+    }
+};
+
+struct StageLauncher {
+    cudaError_t (*prepare)() = nullptr;
+    cudaError_t (*launch)(const StageArgs&, int, cudaStream_t) = nullptr;
+};
+
+template <int DIM, int RECON> StageLauncher stage_launcher_r(int riemann) {
+    if (riemann == kLowMach) return {StageK<DIM, RECON, kLowMach>::prepare, StageK<DIM, RECON, kLowMach>::launch};
+    return {StageK<DIM, RECON, kHLLC>::prepare, StageK<DIM, RECON, kHLLC>::launch};
+}
+
+template <int DIM> StageLauncher stage_launcher(int recon, int riemann) {
+    switch (recon) {
+    case kFirstOrder: return stage_launcher_r<DIM, kFirstOrder>(riemann);
+    case kMuscl: return stage_launcher_r<DIM, kMuscl>(riemann);
+    case kWeno3: return stage_launcher_r<DIM, kWeno3>(riemann);
+    default: return stage_launcher_r<DIM, kWeno5>(riemann);
+    }
+}
+
+cudaError_t prepare_viscous() {
+    return cudaFuncSetAttribute(viscous_kernel<8, 8, 8, 192>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ViscShape<8, 8, 8>::SMEM_BYTES);
+}
+cudaError_t launch_viscous(const ViscArgs& a, int nblocks, cudaStream_t s) {
+    viscous_kernel<8, 8, 8, 192><<<nblocks, 192, ViscShape<8, 8, 8>::SMEM_BYTES, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int RIEMANN> cudaError_t prepare_hancock_t() {
+    return cudaFuncSetAttribute(hancock_kernel<RIEMANN, 16, 16, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HancockShape<16, 16>::SMEM_BYTES);
+}
+template <int RIEMANN> cudaError_t launch_hancock_t(const HancockArgs& a, int nblocks, cudaStream_t s) {
+    hancock_kernel<RIEMANN, 16, 16, 256><<<nblocks, 256, HancockShape<16, 16>::SMEM_BYTES, s>>>(a);
+    return cudaGetLastError();
+}
+
+}   // namespace
+
+// ------------------------------------------------------------------------------------------------ the run
+struct fvg_run {
+    fvg_config cfg{};
+    std::string err;
+    int dim = 2, nvar = 4;
+    Mesh m{};
+    Bc bc{};
+    Eos<double> eos{};
+    double L = 0.0;
+    cudaStream_t stream = nullptr;
+    double *U = nullptr, *Ut = nullptr, *R = nullptr, *Rv = nullptr, *staging = nullptr;
+    double* bm[3] = {nullptr, nullptr, nullptr};
+    double* bmv[3] = {nullptr, nullptr, nullptr};
+    double* bm_seed = nullptr;
+    Ctl* ctl = nullptr;
+    int tiles[3] = {1, 1, 1}, nb = 0, ntiles_v[3] = {1, 1, 1}, nbv = 0, ntiles_h[3] = {1, 1, 1}, nbh = 0;
+    StageLauncher stage;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};   // two steps, by the buffer the state starts in (MUSCL-Hancock ping-pong)
+    int cur = 0;   // MUSCL-Hancock ping-pong: 0 the state is in U, 1 in Ut
+    double* Ucur() { return cur ? Ut : U; }
+};
+
+namespace {
+
+int fail(fvg_run* r, int code, const std::string& msg) {
+    r->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) return fail(run, FVG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+std::string validate(const fvg_config& c) {
+    if (c.nx < 1 || c.ny < 1 || c.nz < 1) return "nx, ny, nz must be >= 1";
+    if (!(c.Lx > 0 && c.Ly > 0 && c.Lz > 0)) return "Lx, Ly, Lz must be > 0";
+    if ((long long)c.nx * c.ny * c.nz > (1LL << 31) - 1) return "more than 2^31 - 1 cells";
+    if (c.eos_type != FVG_EOS_IDEAL && c.eos_type != FVG_EOS_STIFFENED) return "unknown eos_type";
+    if (!(c.gamma > 1.0)) return "gamma must be > 1";
+    if (c.riemann != FVG_RIEMANN_HLLC && c.riemann != FVG_RIEMANN_LOWMACH) return "unknown riemann_solver";
+    if (c.reconstruction < FVG_RECON_NONE || c.reconstruction > FVG_RECON_WENO5) return "unknown reconstruction";
+    if (c.limiter < 0 || c.limiter > 3) return "unknown muscl_limiter";
+    if (c.time_scheme < 0 || c.time_scheme > 3) return "unknown time_scheme";
+    if (c.boundary_order != 1 && c.boundary_order != 2) return "boundary_order must be 1 or 2";
+    if (c.precision != FVG_PREC_FP64) return "precision: only FVG_PREC_FP64 is built into this library";
+    const int naxes = c.nz > 1 ? 3 : 2;
+    for (int s = 0; s < 2 * naxes; ++s) {
+        if (c.bc[s] < 0 || c.bc[s] > FVG_BC_NONREFLECTING) return "unknown boundary type";
+        if (c.bc[s] == FVG_BC_MASSFLOWINLET) return "the mass-flow inlet is not supported on the device";
+        if (c.bc[s] == FVG_BC_NONREFLECTING) return "the non-reflecting outlet is not supported on the device";
+    }
+    for (int a = 0; a < naxes; ++a)
+        if ((c.bc[2 * a] == FVG_BC_PERIODIC) != (c.bc[2 * a + 1] == FVG_BC_PERIODIC))
+            return "a periodic axis needs both of its sides periodic";
+    if (c.time_scheme == FVG_TS_HANCOCK) {
+        if (c.reconstruction != FVG_RECON_MUSCL) return "MUSCL-Hancock needs reconstruction = muscl";
+        if (c.nz > 1) return "MUSCL-Hancock is built for 2-D meshes only";
+        if (c.use_viscous) return "MUSCL-Hancock with viscous fluxes is not supported on the device";
+    }
+    if (c.use_viscous && c.nz == 1) return "the 2-D viscous sweep is not supported on the device (3-D only)";
+    if (!(c.cfl > 0)) return "cfl must be > 0";
+    return "";
+}
+
+// halo kinds of the sides for a reconstruction `depth` cells deep (Simulation.cpp:868-905, 1107-1176)
+void halo_kinds(const fvg_config& c, int depth, int kinds[6]) {
+    const int n3[3] = {c.nx, c.ny, c.nz};
+    for (int s = 0; s < 6; ++s) kinds[s] = kHaloNone;
+    if (c.reconstruction == FVG_RECON_NONE) return;
+    const int naxes = c.nz > 1 ? 3 : 2;
+    for (int a = 0; a < naxes; ++a) {
+        const bool per = c.bc[2 * a] == FVG_BC_PERIODIC && c.bc[2 * a + 1] == FVG_BC_PERIODIC;
+        for (int h = 0; h < 2; ++h) {
+            const int s = 2 * a + h, bt = c.bc[s];
+            if (per && n3[a] >= depth)
+                kinds[s] = kHaloWrap;
+            else if (c.boundary_order == 2 && bt != FVG_BC_PERIODIC && bt != FVG_BC_NONREFLECTING && n3[a] >= depth)
+                kinds[s] = kHaloSlab;
+        }
+    }
+}
+
+StageArgs stage_args(fvg_run* r, const double* Uin, const double* U0, double* out, int mode, double ca, double cb, const double* Rv, double* bm,
+                     const int* gate) {
+    StageArgs a{};
+    a.m = r->m;
+    a.bc = r->bc;
+    a.eos = r->eos;
+    a.shock_blend = r->cfg.shock_blend;
+    a.weno_eps = r->cfg.weno_epsilon;
+    a.limiter = r->cfg.limiter;
+    a.mode = mode;
+    a.ca = ca;
+    a.cb = cb;
+    a.U = Uin;
+    a.U0 = U0;
+    a.out = out;
+    a.Rv = Rv;
+    a.blockmax = bm;
+    a.ctl = r->ctl;
+    a.gate = gate;
+    for (int d = 0; d < 3; ++d) a.tiles[d] = r->tiles[d];
+    return a;
+}
+
+ViscArgs visc_args(fvg_run* r, const double* Uin, double* bmv, const int* gate) {
+    ViscArgs a{};
+    a.m = r->m;
+    a.bc = r->bc;
+    a.eos = r->eos;
+    const double g = r->cfg.gamma;
+    a.mu = r->cfg.mu;
+    a.k_cond = r->cfg.mu * g / (r->cfg.pr * (g - 1.0));   // TransportLaw (Core.hpp:194-197)
+    a.L = r->L;
+    a.inv_h2 = 1.0 / (r->m.dx * r->m.dx) + 1.0 / (r->m.dy * r->m.dy) + 1.0 / (r->m.dz * r->m.dz);
+    a.u_in = r->cfg.u_in;
+    a.v_in = r->cfg.v_in;
+    a.bface2 = r->cfg.boundary_order == 2;
+    for (int d = 0; d < 3; ++d) a.periodic[d] = r->cfg.bc[2 * d] == FVG_BC_PERIODIC && r->cfg.bc[2 * d + 1] == FVG_BC_PERIODIC;
+    a.U = Uin;
+    a.Rv = r->Rv;
+    a.blockmax = bmv;
+    a.gate = gate;
+    for (int d = 0; d < 3; ++d) a.tiles[d] = r->ntiles_v[d];
+    return a;
+}
+
+HancockArgs hancock_args(fvg_run* r, const double* Uin, double* out, int mode, double* bm, const int* gate) {
+    HancockArgs a{};
+    a.m = r->m;
+    a.bc = r->bc;
+    a.eos = r->eos;
+    a.shock_blend = r->cfg.shock_blend;
+    a.limiter = r->cfg.limiter;
+    a.mode = mode;
+    a.U = Uin;
+    a.out = out;
+    a.blockmax = bm;
+    a.ctl = r->ctl;
+    a.gate = gate;
+    for (int d = 0; d < 3; ++d) a.tiles[d] = r->ntiles_h[d];
+    return a;
+}
+
+cudaError_t launch_hancock(fvg_run* r, const HancockArgs& a) {
+    return r->cfg.riemann == FVG_RIEMANN_LOWMACH ? launch_hancock_t<kLowMach>(a, r->nbh, r->stream) : launch_hancock_t<kHLLC>(a, r->nbh, r->stream);
+}
+
+// One residual stage of Uin: the viscous sweep (3-D viscous runs), then the inviscid stage kernel.
+cudaError_t residual_stage(fvg_run* r, const double* Uin, const double* U0, double* out, int mode, double ca, double cb, int stage, const int* gate) {
+    cudaError_t e;
+    if (r->cfg.use_viscous) {
+        e = launch_viscous(visc_args(r, Uin, r->bmv[stage], gate), r->nbv, r->stream);
+        if (e != cudaSuccess) return e;
+    }
+    return r->stage.launch(stage_args(r, Uin, U0, out, mode, ca, cb, r->cfg.use_viscous ? r->Rv : nullptr, r->bm[stage], gate), r->nb, r->stream);
+}
+
+int axpy_blocks(const fvg_run* r) {
+    const long long n = r->m.ncells * r->nvar;
+    long long b = (n + 255) / 256;
+    return (int)(b < 148 * 16 ? b : 148 * 16);
+}
+
+// The launches of one time step on the run's stream (no host synchronisation).
+cudaError_t enqueue_step(fvg_run* r) {
+    cudaError_t e;
+    Ctl* c = r->ctl;
+    const int* act = &c->active;
+    const int nbv = r->cfg.use_viscous ? r->nbv : 0;
+    const int ts = r->cfg.time_scheme;
+    if (ts == FVG_TS_HANCOCK) {
+        double* Uin = r->Ucur();
+        double* Uout = r->cur ? r->U : r->Ut;
+        k_hancock_begin<<<1, 1, 0, r->stream>>>(c);
+        if ((e = r->stage.launch(stage_args(r, Uin, nullptr, r->R, kStoreR, 0, 0, nullptr, r->bm_seed, &c->seed), r->nb, r->stream))) return e;
+        k_hancock_seed<<<1, 1024, 0, r->stream>>>(c, r->bm_seed, r->nb);
+        k_hancock_dt<<<1, 1, 0, r->stream>>>(c);
+        if ((e = launch_hancock(r, hancock_args(r, Uin, Uout, kAxpy, r->bm[0], act)))) return e;
+        k_hancock_end<<<1, 1024, 0, r->stream>>>(c, r->bm[0], r->nbh);
+        r->cur ^= 1;
+        return cudaGetLastError();
+    }
+    if ((e = residual_stage(r, r->U, nullptr, r->R, kStoreR, 0, 0, 0, act))) return e;
+    k_stage1_dt<<<1, 1024, 0, r->stream>>>(c, r->bm[0], r->nb, r->bmv[0], nbv);
+    if (ts == FVG_TS_EULER) {
+        k_axpy<<<axpy_blocks(r), 256, 0, r->stream>>>(c, r->U, r->U, r->R, r->m.plane, r->m.ncells, r->nvar);
+        k_end_rk<<<1, 1, 0, r->stream>>>(c, 1);
+        return cudaGetLastError();
+    }
+    k_axpy<<<axpy_blocks(r), 256, 0, r->stream>>>(c, r->Ut, r->U, r->R, r->m.plane, r->m.ncells, r->nvar);
+    if (ts == FVG_TS_SSPRK2) {
+        if ((e = residual_stage(r, r->Ut, r->U, r->U, kCombine, 0.5, 0.5, 1, act))) return e;
+        k_stage_max<<<1, 1024, 0, r->stream>>>(c, act, 1, r->bm[1], r->nb, r->bmv[1], nbv);
+        k_end_rk<<<1, 1, 0, r->stream>>>(c, 2);
+        return cudaGetLastError();
+    }
+    if ((e = residual_stage(r, r->Ut, r->U, r->R, kCombine, 0.75, 0.25, 1, act))) return e;
+    k_stage_max<<<1, 1024, 0, r->stream>>>(c, act, 1, r->bm[1], r->nb, r->bmv[1], nbv);
+    if ((e = residual_stage(r, r->R, r->U, r->U, kCombine, 1.0 / 3.0, 2.0 / 3.0, 2, act))) return e;
+    k_stage_max<<<1, 1024, 0, r->stream>>>(c, act, 2, r->bm[2], r->nb, r->bmv[2], nbv);
+    k_end_rk<<<1, 1, 0, r->stream>>>(c, 3);
+    return cudaGetLastError();
+}
+
+int read_ctl(fvg_run* run, Ctl* h) {
+    CK(cudaMemcpyAsync(h, run->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, run->stream));
+    CK(cudaStreamSynchronize(run->stream));
+    return FVG_OK;
+}
+
+}   // namespace
+
+// ------------------------------------------------------------------------------------------------ C ABI
+extern "C" {
+
+int fvg_abi_version(void) { return FVG_ABI_VERSION; }
+const char* fvg_create_error(void) { return g_create_error.c_str(); }
+const char* fvg_last_error(const fvg_run* run) { return run ? run->err.c_str() : "null run"; }
+
+int fvg_create(const fvg_config* cfg, fvg_run** out) {
+    if (!cfg || !out) {
+        g_create_error = "null argument";
+        return FVG_ERR_ARGUMENT;
+    }
+    *out = nullptr;
+    const std::string v = validate(*cfg);
+    if (!v.empty()) {
+        g_create_error = v;
+        return FVG_ERR_CONFIG;
+    }
+    auto* run = new fvg_run();
+    run->cfg = *cfg;
+    const fvg_config& c = run->cfg;
+    auto bail = [&](int code) {
+        g_create_error = run->err;
+        fvg_destroy(run);
+        return code;
+    };
+    if (cudaSetDevice(c.device) != cudaSuccess) {
+        run->err = "cudaSetDevice failed (no CUDA device?)";
+        return bail(FVG_ERR_CUDA);
+    }
+    run->dim = c.nz > 1 ? 3 : 2;
+    run->nvar = run->dim == 3 ? 5 : 4;
+    Mesh& m = run->m;
+    m.nx = c.nx;
+    m.ny = c.ny;
+    m.nz = c.nz;
+    m.ncells = (long long)c.nx * c.ny * c.nz;
+    m.plane = (m.ncells + 31) / 32 * 32;
+    m.dx = c.Lx / c.nx;   // generate_cartesian_mesh_3d (Core.cpp:20-40)
+    m.dy = c.Ly / c.ny;
+    m.dz = c.Lz / c.nz;
+    if (run->dim == 3) {
+        m.area[0] = m.dy * m.dz;
+        m.area[1] = m.dx * m.dz;
+        m.area[2] = m.dx * m.dy;
+        m.inv_cell = 1.0 / (m.dx * m.dy * m.dz);
+        run->L = 2.0 / (1.0 / (c.Lx / c.nx) + 1.0 / (c.Ly / c.ny) + 1.0 / (c.Lz / c.nz));
+    } else {
+        m.area[0] = m.dy;
+        m.area[1] = m.dx;
+        m.area[2] = 0.0;
+        m.inv_cell = 1.0 / (m.dx * m.dy);
+        run->L = vmin(c.Lx / c.nx, c.Ly / c.ny);
+    }
+    run->eos.type = c.eos_type;
+    run->eos.gamma = c.gamma;
+    run->eos.p_inf = c.p_inf;
+    for (int s = 0; s < 6; ++s) run->bc.type[s] = c.bc[s];
+    halo_kinds(c, c.reconstruction == FVG_RECON_WENO5 ? 3 : 2, run->bc.halo);
+    run->bc.u_in = c.u_in;
+    run->bc.v_in = c.v_in;
+    run->bc.p_out = c.p_out;
+    const int TX = run->dim == 3 ? Tile<3>::X : Tile<2>::X, TY = run->dim == 3 ? Tile<3>::Y : Tile<2>::Y, TZ = run->dim == 3 ? Tile<3>::Z : 1;
+    run->tiles[0] = (c.nx + TX - 1) / TX;
+    run->tiles[1] = (c.ny + TY - 1) / TY;
+    run->tiles[2] = (c.nz + TZ - 1) / TZ;
+    run->nb = run->tiles[0] * run->tiles[1] * run->tiles[2];
+    run->ntiles_v[0] = (c.nx + 7) / 8;
+    run->ntiles_v[1] = (c.ny + 7) / 8;
+    run->ntiles_v[2] = (c.nz + 7) / 8;
+    run->nbv = run->ntiles_v[0] * run->ntiles_v[1] * run->ntiles_v[2];
+    run->ntiles_h[0] = (c.nx + 15) / 16;
+    run->ntiles_h[1] = (c.ny + 15) / 16;
+    run->ntiles_h[2] = 1;
+    run->nbh = run->ntiles_h[0] * run->ntiles_h[1];
+    run->stage = run->dim == 3 ? stage_launcher<3>(c.reconstruction, c.riemann) : stage_launcher<2>(c.reconstruction, c.riemann);
+    // the seed residual of MUSCL-Hancock and every residual use the stage kernel; the viscous and predictor kernels as needed
+    if (run->stage.prepare() != cudaSuccess || (c.use_viscous && prepare_viscous() != cudaSuccess) ||
+        (run->dim == 2 && c.reconstruction == FVG_RECON_MUSCL &&
+         (c.riemann == FVG_RIEMANN_LOWMACH ? prepare_hancock_t<kLowMach>() : prepare_hancock_t<kHLLC>()) != cudaSuccess)) {
+        run->err = "kernel set-up failed (shared-memory limit)";
+        return bail(FVG_ERR_CUDA);
+    }
+    const size_t sbytes = sizeof(double) * run->m.plane * run->nvar;
+    if (cudaStreamCreateWithFlags(&run->stream, cudaStreamNonBlocking) != cudaSuccess || cudaMalloc(&run->U, sbytes) != cudaSuccess ||
+        cudaMalloc(&run->Ut, sbytes) != cudaSuccess || cudaMalloc(&run->R, sbytes) != cudaSuccess ||
+        (c.use_viscous && cudaMalloc(&run->Rv, sbytes) != cudaSuccess) || cudaMalloc(&run->ctl, sizeof(Ctl)) != cudaSuccess ||
+        cudaMalloc(&run->bm_seed, sizeof(double) * run->nb) != cudaSuccess) {
+        run->err = "device allocation failed";
+        return bail(FVG_ERR_CUDA);
+    }
+    const int nbmax = run->nb > run->nbh ? run->nb : run->nbh;
+    for (int s = 0; s < 3; ++s)
+        if (cudaMalloc(&run->bm[s], sizeof(double) * nbmax) != cudaSuccess || cudaMalloc(&run->bmv[s], sizeof(double) * run->nbv) != cudaSuccess) {
+            run->err = "device allocation failed";
+            return bail(FVG_ERR_CUDA);
+        }
+    cudaMemsetAsync(run->U, 0, sbytes, run->stream);
+    cudaMemsetAsync(run->Ut, 0, sbytes, run->stream);
+    Ctl h{};
+    h.cfl = c.cfl;
+    h.L = run->L;
+    h.dt_max = c.dt_max;
+    h.always = 1;
+    h.t_end = 0.0;
+    cudaMemcpyAsync(run->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, run->stream);
+    if (cudaStreamSynchronize(run->stream) != cudaSuccess) {
+        run->err = "device initialisation failed";
+        return bail(FVG_ERR_CUDA);
+    }
+    *out = run;
+    return FVG_OK;
+}
+
+int fvg_destroy(fvg_run* run) {
+    if (!run) return FVG_OK;
+    cudaSetDevice(run->cfg.device);
+    if (run->stream) cudaStreamSynchronize(run->stream);
+    for (int g = 0; g < 2; ++g)
+        if (run->graph[g]) cudaGraphExecDestroy(run->graph[g]);
+    for (double* p : {run->U, run->Ut, run->R, run->Rv, run->staging, run->bm_seed, run->bm[0], run->bm[1], run->bm[2], run->bmv[0], run->bmv[1], run->bmv[2]})
+        if (p) cudaFree(p);
+    if (run->ctl) cudaFree(run->ctl);
+    if (run->stream) cudaStreamDestroy(run->stream);
+    delete run;
+    return FVG_OK;
+}
+
+static int ensure_staging(fvg_run* run) {
+    if (run->staging) return FVG_OK;
+    CK(cudaMalloc(&run->staging, sizeof(double) * 5 * run->m.ncells));
+    return FVG_OK;
+}
+
+int fvg_upload_state(fvg_run* run, const double* U, size_t ncells) {
+    if (!run || !U) return FVG_ERR_ARGUMENT;
+    if ((long long)ncells != run->m.ncells) return fail(run, FVG_ERR_ARGUMENT, "ncells is not the mesh's");
+    CK(cudaSetDevice(run->cfg.device));
+    int rc = ensure_staging(run);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(run->staging, U, sizeof(double) * 5 * ncells, cudaMemcpyHostToDevice, run->stream));
+    int* bad = reinterpret_cast<int*>(run->bm_seed);
+    CK(cudaMemsetAsync(bad, 0, sizeof(int), run->stream));
+    run->cur = 0;
+    k_aos_to_planes<<<axpy_blocks(run), 256, 0, run->stream>>>(run->staging, run->U, run->m.plane, run->m.ncells, run->nvar, bad);
+    CK(cudaGetLastError());
+    int hbad = 0;
+    CK(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, run->stream));
+    CK(cudaStreamSynchronize(run->stream));
+    if (hbad) return fail(run, FVG_ERR_STATE, "rho w must be zero on a 2-D mesh");
+    return FVG_OK;
+}
+
+int fvg_download_state(fvg_run* run, double* U, size_t ncells) {
+    if (!run || !U) return FVG_ERR_ARGUMENT;
+    if ((long long)ncells != run->m.ncells) return fail(run, FVG_ERR_ARGUMENT, "ncells is not the mesh's");
+    CK(cudaSetDevice(run->cfg.device));
+    int rc = ensure_staging(run);
+    if (rc) return rc;
+    k_planes_to_aos<<<axpy_blocks(run), 256, 0, run->stream>>>(run->Ucur(), run->staging, run->m.plane, run->m.ncells, run->nvar);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(U, run->staging, sizeof(double) * 5 * ncells, cudaMemcpyDeviceToHost, run->stream));
+    CK(cudaStreamSynchronize(run->stream));
+    return FVG_OK;
+}
+
+int fvg_residual(fvg_run* run, double predictor_half_dt, double* R, size_t ncells, double* smax) {
+    if (!run) return FVG_ERR_ARGUMENT;
+    if (R && (long long)ncells != run->m.ncells) return fail(run, FVG_ERR_ARGUMENT, "ncells is not the mesh's");
+    CK(cudaSetDevice(run->cfg.device));
+    Ctl* c = run->ctl;
+    const int* always = &c->always;
+    double* out = run->cur ? run->U : run->Ut;   // a buffer that is not the state
+    if (predictor_half_dt > 0.0) {
+        if (run->cfg.reconstruction != FVG_RECON_MUSCL || run->dim != 2 || run->cfg.use_viscous)
+            return fail(run, FVG_ERR_CONFIG, "the MUSCL-Hancock predictor needs a 2-D inviscid MUSCL run");
+        CK(cudaMemcpyAsync(&c->half_dt, &predictor_half_dt, sizeof(double), cudaMemcpyHostToDevice, run->stream));
+        CK(launch_hancock(run, hancock_args(run, run->Ucur(), out, kStoreR, run->bm[0], always)));
+        k_stage_max<<<1, 1024, 0, run->stream>>>(c, always, 0, run->bm[0], run->nbh, run->bmv[0], 0);
+    } else {
+        CK(residual_stage(run, run->Ucur(), nullptr, out, kStoreR, 0, 0, 0, always));
+        k_stage_max<<<1, 1024, 0, run->stream>>>(c, always, 0, run->bm[0], run->nb, run->bmv[0], run->cfg.use_viscous ? run->nbv : 0);
+    }
+    CK(cudaGetLastError());
+    Ctl h;
+    int rc = read_ctl(run, &h);
+    if (rc) return rc;
+    if (smax) *smax = h.s_stage[0];
+    if (R) {
+        if ((rc = ensure_staging(run))) return rc;
+        k_planes_to_aos<<<axpy_blocks(run), 256, 0, run->stream>>>(out, run->staging, run->m.plane, run->m.ncells, run->nvar);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(R, run->staging, sizeof(double) * 5 * ncells, cudaMemcpyDeviceToHost, run->stream));
+        CK(cudaStreamSynchronize(run->stream));
+    }
+    return FVG_OK;
+}
+
+static int run_steps(fvg_run* run, double t_end, int max_steps, int use_graph, int* steps) {
+    CK(cudaSetDevice(run->cfg.device));
+    k_begin<<<1, 1, 0, run->stream>>>(run->ctl, t_end, max_steps);
+    CK(cudaGetLastError());
+    Ctl h;
+    int rc;
+    const bool hancock = run->cfg.time_scheme == FVG_TS_HANCOCK;
+    int done = 0;
+    if (!use_graph) {
+        // one step at a time (fvg_step)
+        cudaError_t e = enqueue_step(run);
+        if (e != cudaSuccess) return fail(run, FVG_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+        if ((rc = read_ctl(run, &h))) return rc;
+        done = h.steps;
+        if (hancock && done == 0) run->cur ^= 1;   // the step did not run: the state stayed where it was
+    } else {
+        // a graph of two steps (the MUSCL-Hancock ping-pong returns to its buffer after two)
+        cudaGraphExec_t& graph = run->graph[run->cur];
+        if (!graph) {
+            const int cur0 = run->cur;
+            cudaGraph_t g;
+            CK(cudaStreamBeginCapture(run->stream, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e1 = enqueue_step(run), e2 = enqueue_step(run);
+            cudaError_t e3 = cudaStreamEndCapture(run->stream, &g);
+            run->cur = cur0;
+            if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+                return fail(run, FVG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e1 ? e1 : (e2 ? e2 : e3)));
+            CK(cudaGraphInstantiate(&graph, g, 0));
+            cudaGraphDestroy(g);
+        }
+        int chunk = 4;
+        while (true) {
+            for (int k = 0; k < chunk; ++k) CK(cudaGraphLaunch(graph, run->stream));
+            if ((rc = read_ctl(run, &h))) return rc;
+            if (!h.active) break;
+            if (chunk < 64) chunk *= 2;
+        }
+        done = h.steps;
+        if (hancock && (done & 1)) run->cur ^= 1;
+    }
+    if (steps) *steps = done;
+    if (h.status) {
+        char msg[256];
+        std::snprintf(msg, sizeof msg, "the solution diverged at step %d (t = %.6g, dt = %.3g, largest wave speed = %.3g)", done + 1, h.t, h.dt,
+                      h.s_step);
+        return fail(run, FVG_ERR_DIVERGED, msg);
+    }
+    return FVG_OK;
+}
+
+int fvg_step(fvg_run* run, double t_end, double* dt, double* smax) {
+    if (!run) return FVG_ERR_ARGUMENT;
+    int n = 0;
+    const int rc = run_steps(run, t_end, 1, 0, &n);
+    if (rc) return rc;
+    Ctl h;
+    int r2 = read_ctl(run, &h);
+    if (r2) return r2;
+    if (dt) *dt = n ? h.dt : 0.0;
+    if (smax) *smax = n ? h.s_step : 0.0;
+    return FVG_OK;
+}
+
+int fvg_run_until(fvg_run* run, double t_end, int max_steps, int* steps) {
+    if (!run) return FVG_ERR_ARGUMENT;
+    return run_steps(run, t_end, max_steps, 1, steps);
+}
+
+int fvg_get_time(const fvg_run* run, double* t) {
+    if (!run || !t) return FVG_ERR_ARGUMENT;
+    fvg_run* r = const_cast<fvg_run*>(run);
+    Ctl h;
+    int rc = read_ctl(r, &h);
+    if (rc) return rc;
+    *t = h.t;
+    return FVG_OK;
+}
+
+int fvg_set_time(fvg_run* run, double t) {
+    if (!run) return FVG_ERR_ARGUMENT;
+    CK(cudaMemcpyAsync(&run->ctl->t, &t, sizeof(double), cudaMemcpyHostToDevice, run->stream));
+    CK(cudaStreamSynchronize(run->stream));
+    return FVG_OK;
+}
+
+int fvg_get_lagged_speed(const fvg_run* run, double* s) {
+    if (!run || !s) return FVG_ERR_ARGUMENT;
+    Ctl h;
+    int rc = read_ctl(const_cast<fvg_run*>(run), &h);
+    if (rc) return rc;
+    *s = h.s_lag;
+    return FVG_OK;
+}
+
+int fvg_set_lagged_speed(fvg_run* run, double s) {
+    if (!run) return FVG_ERR_ARGUMENT;
+    CK(cudaMemcpyAsync(&run->ctl->s_lag, &s, sizeof(double), cudaMemcpyHostToDevice, run->stream));
+    CK(cudaStreamSynchronize(run->stream));
+    return FVG_OK;
+}
+
+int fvg_dt_length(const fvg_run* run, double* L) {
+    if (!run || !L) return FVG_ERR_ARGUMENT;
+    *L = run->L;
+    return FVG_OK;
+}
+
+int fvg_device_state(fvg_run* run, double** planes, long long* plane, int* nvar) {
+    if (!run) return FVG_ERR_ARGUMENT;
+    if (planes) *planes = run->Ucur();
+    if (plane) *plane = run->m.plane;
+    if (nvar) *nvar = run->nvar;
+    return FVG_OK;
+}
+
+int fvg_stream(fvg_run* run, void** stream) {
+    if (!run || !stream) return FVG_ERR_ARGUMENT;
+    *stream = run->stream;
+    return FVG_OK;
+}
+
+int fvg_synchronize(fvg_run* run) {
+    if (!run) return FVG_ERR_ARGUMENT;
+    CK(cudaStreamSynchronize(run->stream));
+    return FVG_OK;
+}
+
+int fvg_face_flux_batch(fvg_run* run, const double* UL, const double* UR, const int* axis, size_t n, double* F, double* smax) {
+    if (!run || !UL || !UR || !axis || !F || !smax) return FVG_ERR_ARGUMENT;
+    CK(cudaSetDevice(run->cfg.device));
+    double *dUL, *dUR, *dF, *dS;
+    int* dA;
+    CK(cudaMalloc(&dUL, sizeof(double) * 5 * n));
+    CK(cudaMalloc(&dUR, sizeof(double) * 5 * n));
+    CK(cudaMalloc(&dF, sizeof(double) * 5 * n));
+    CK(cudaMalloc(&dS, sizeof(double) * n));
+    CK(cudaMalloc(&dA, sizeof(int) * n));
+    CK(cudaMemcpyAsync(dUL, UL, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, run->stream));
+    CK(cudaMemcpyAsync(dUR, UR, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, run->stream));
+    CK(cudaMemcpyAsync(dA, axis, sizeof(int) * n, cudaMemcpyHostToDevice, run->stream));
+    CK(cudaMemsetAsync(dF, 0, sizeof(double) * 5 * n, run->stream));
+    const int blocks = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+    // the batch always uses the full 3-D state (rho w kept)
+    if (run->cfg.riemann == FVG_RIEMANN_LOWMACH)
+        k_face_flux<kLowMach, 5><<<blocks, 256, 0, run->stream>>>(run->eos, run->cfg.shock_blend, dUL, dUR, dA, (long long)n, dF, dS);
+    else
+        k_face_flux<kHLLC, 5><<<blocks, 256, 0, run->stream>>>(run->eos, run->cfg.shock_blend, dUL, dUR, dA, (long long)n, dF, dS);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(F, dF, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost, run->stream));
+    CK(cudaMemcpyAsync(smax, dS, sizeof(double) * n, cudaMemcpyDeviceToHost, run->stream));
+    CK(cudaStreamSynchronize(run->stream));
+    cudaFree(dUL);
+    cudaFree(dUR);
+    cudaFree(dF);
+    cudaFree(dS);
+    cudaFree(dA);
+    return FVG_OK;
+}
+
+}   // extern "C"

@@ -1,0 +1,312 @@
+// Navier-Stokes viscous and heat fluxes on a 3-D mesh (NavierStokes::viscous_residual_3d, cpp/src/Physics.cpp:484-830).
+//
+// A CTA owns a TX x TY x TZ tile and sweeps its axes in turn, like the stage kernel. Per axis d:
+//   1. cells:   for the tile extended by one cell along d, the cell quantities of the reference's sweep: velocity,
+//               T = p / rho, and the four velocity-gradient entries G[a][b] = (d(rho u_a)/dx_b - u_a d(rho)/dx_b) / rho
+//               that the faces of axis d read (central differences of the padded conservative state); a position beyond
+//               a periodic side is the wrapped cell, beyond another side the ghost entry (velocity and T only);
+//   2. faces:   compact normal derivatives, face-averaged cross derivatives, Stokes stress and Fourier heat flux;
+//   3. balance: ((0 + (Fr - Fl)) + (Ft - Fb)) + (Fk - Ff), accumulated in shared memory in that order.
+// The result, times 1 / volume, is the viscous residual Rv of every cell (added to the inviscid one by the stage
+// kernel, R + Rv being the reference's `r += ...`), and each CTA writes the largest viscous speed bound of its cells
+// (ViscousBound.hpp: max |u_a| + c + 2 L sum(1/h^2) max(4/3 mu/rho, k (gamma-1)/rho) + 1e-12).
+#pragma once
+
+#include "grid.cuh"
+
+namespace fvg {
+
+struct ViscArgs {
+    Mesh m;
+    Bc bc;
+    Eos<double> eos;
+    double mu, k_cond, L, inv_h2;
+    double u_in, v_in;
+    int bface2;        // boundary_order == 2
+    int periodic[3];   // both sides of the axis periodic
+    const double* U;
+    double* Rv;
+    double* blockmax;
+    const int* gate;   // the kernel does nothing unless *gate
+    int tiles[3];
+};
+
+// the zero-gradient copy with the momentum rules of a wall side (BoundaryManager::viscous_ghost_3d, Boundaries.cpp:258-275)
+__device__ __forceinline__ St<double, 5> viscous_ghost_3d(const ViscArgs& a, int side, const St<double, 5>& c) {
+    St<double, 5> gh = c;
+    const int d = side >> 1;
+    const int type = a.bc.type[side];
+    const int mom[3] = {1, 2, 4};
+    if (type == kBcNoSlip) {
+        gh[1] = -c[1];
+        gh[2] = -c[2];
+        gh[4] = -c[4];
+    } else if (type == kBcWall) {
+        gh[mom[d]] = -c[mom[d]];
+    } else if (type == kBcMovingWall) {
+        const double uw[3] = {a.u_in, a.v_in, 0.0};
+#pragma unroll
+        for (int t = 0; t < 3; ++t) gh[mom[t]] = (t == d) ? -c[mom[t]] : 2.0 * c[0] * uw[t] - c[mom[t]];
+        if (a.bface2)   // match_kinetic_energy (Boundaries.cpp:197-200)
+            gh[3] = c[3] + 0.5 * (gh[1] * gh[1] + gh[2] * gh[2] + gh[4] * gh[4] - c[1] * c[1] - c[2] * c[2] - c[4] * c[4]) / c[0];
+    }
+    return gh;
+}
+
+__device__ __forceinline__ St<double, 5> cell_at(const ViscArgs& a, int i, int j, int k) {
+    return read_cell<5>(a.U, a.m.plane, ((long long)k * a.m.ny + j) * a.m.nx + i);
+}
+
+// The padded entry beyond one side along axis d (padded_3d, Boundaries.cpp:621-700): the opposite layer of a periodic
+// side, the wall ghost of a wall side, else the replicated edge cell. idx[d] is -1 or n_d; the other indices are inside.
+__device__ __forceinline__ St<double, 5> face_ghost(const ViscArgs& a, int d, int idx0, int idx1, int idx2) {
+    int idx[3] = {idx0, idx1, idx2};
+    const int n3[3] = {a.m.nx, a.m.ny, a.m.nz};
+    const bool hi = idx[d] >= n3[d];
+    const int side = 2 * d + (hi ? 1 : 0);
+    const int type = a.bc.type[side];
+    if (type == kBcPeriodic) {
+        idx[d] = hi ? 0 : n3[d] - 1;
+        return cell_at(a, idx[0], idx[1], idx[2]);
+    }
+    idx[d] = hi ? n3[d] - 1 : 0;
+    const St<double, 5> c = cell_at(a, idx[0], idx[1], idx[2]);
+    if (type == kBcNoSlip || type == kBcWall || type == kBcMovingWall) return viscous_ghost_3d(a, side, c);
+    return c;
+}
+
+// Any entry of the reference's padded conservative state, cell indices -1 .. n per axis: the cell, a face ghost, an
+// edge (two axes outside: fix_padded_corners, Boundaries.cpp:509-548, with boundary_order = 2, else edge replication)
+// or a corner (replication).
+__device__ __forceinline__ St<double, 5> padded_cons(const ViscArgs& a, int i, int j, int k) {
+    const int n3[3] = {a.m.nx, a.m.ny, a.m.nz};
+    int p[3] = {i, j, k};
+    int ng = 0, ga[2] = {-1, -1};
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+        if (p[d] < 0 || p[d] >= n3[d]) {
+            if (ng < 2) ga[ng] = d;
+            ++ng;
+        }
+    if (ng == 0) return cell_at(a, i, j, k);
+    if (ng == 1) return face_ghost(a, ga[0], i, j, k);
+    if (ng == 2 && a.bface2) {
+        const int d = ga[0], e = ga[1];
+        const bool hi = p[d] >= n3[d];
+        int q[3] = {p[0], p[1], p[2]};
+        q[d] = hi ? n3[d] - 1 : 0;
+        const int side = 2 * d + (hi ? 1 : 0);
+        if (a.bc.type[side] == kBcPeriodic) {
+            q[d] = hi ? 0 : n3[d] - 1;
+            return face_ghost(a, e, q[0], q[1], q[2]);
+        }
+        return viscous_ghost_3d(a, side, face_ghost(a, e, q[0], q[1], q[2]));
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) p[d] = p[d] < 0 ? 0 : (p[d] >= n3[d] ? n3[d] - 1 : p[d]);
+    return cell_at(a, p[0], p[1], p[2]);
+}
+
+template <int TX, int TY, int TZ> struct ViscShape {
+    static constexpr int NC = TX * TY * TZ;
+    static constexpr int cmax(int x, int y) { return x > y ? x : y; }
+    static constexpr int NE = cmax(cmax((TX + 2) * TY * TZ, TX * (TY + 2) * TZ), TX * TY * (TZ + 2));
+    static constexpr int NF = cmax(cmax((TX + 1) * TY * TZ, TX * (TY + 1) * TZ), TX * TY * (TZ + 1));
+    // Q [8][NE] cell quantities (u, v, w, T, four G), F [4][NF] face fluxes (components 1..4), acc [5][NC], red [32]
+    static constexpr int SMEM_DOUBLES = 8 * NE + 4 * NF + 5 * NC + 32;
+    static constexpr size_t SMEM_BYTES = sizeof(double) * SMEM_DOUBLES;
+};
+
+template <int TX, int TY, int TZ, int NT>
+__global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
+    using S = ViscShape<TX, TY, TZ>;
+    constexpr int NC = S::NC;
+    extern __shared__ double smem[];
+    double* Q = smem;                 // [8][NE]
+    double* Fv = Q + 8 * S::NE;       // [4][NF]
+    double* acc = Fv + 4 * S::NF;     // [5][NC]
+    double* red = acc + 5 * NC;
+    if (!*a.gate) return;
+    const Mesh& m = a.m;
+    const int tid = threadIdx.x, b = blockIdx.x;
+    const int o3[3] = {(b % a.tiles[0]) * TX, ((b / a.tiles[0]) % a.tiles[1]) * TY, (b / (a.tiles[0] * a.tiles[1])) * TZ};
+    const int n3[3] = {m.nx, m.ny, m.nz};
+    const double h[3] = {m.dx, m.dy, m.dz};
+    const int mom[3] = {1, 2, 4};
+    // the (a, b) of the four gradient entries the faces of axis d read, in the reference's CrossGhosts order
+    const int GA[3][4] = {{0, 1, 2, 0}, {0, 1, 2, 1}, {0, 1, 2, 2}};
+    const int GB[3][4] = {{1, 1, 2, 2}, {0, 0, 2, 2}, {0, 1, 0, 1}};
+
+#pragma unroll 1
+    for (int d = 0; d < 3; ++d) {
+        int E[3] = {TX, TY, TZ}, Fd[3] = {TX, TY, TZ};
+        E[d] += 2;
+        Fd[d] += 1;
+        const int nE = E[0] * E[1] * E[2], nF = Fd[0] * Fd[1] * Fd[2];
+        // ---- 1. cell quantities
+        for (int e = tid; e < nE; e += NT) {
+            int g[3] = {e % E[0], (e / E[0]) % E[1], e / (E[0] * E[1])};
+            g[d] -= 1;
+#pragma unroll
+            for (int x = 0; x < 3; ++x) g[x] += o3[x];
+            bool ghost = false;
+            if (g[d] < 0 || g[d] >= n3[d]) {
+                if (a.periodic[d])
+                    g[d] = ((g[d] % n3[d]) + n3[d]) % n3[d];
+                else
+                    ghost = true;
+            }
+            // a tile that overhangs the mesh: any cell inside (its results are not used)
+#pragma unroll
+            for (int x = 0; x < 3; ++x)
+                if (x != d) g[x] = g[x] < n3[x] ? g[x] : n3[x] - 1;
+            double qv[8];
+            if (ghost) {
+                const St<double, 5> gc = face_ghost(a, d, g[0], g[1], g[2]);
+                const St<double, 5> w = c2p(a.eos, gc);
+                qv[0] = w[1];
+                qv[1] = w[2];
+                qv[2] = w[4];
+                qv[3] = w[3] / w[0];
+                qv[4] = qv[5] = qv[6] = qv[7] = 0.0;
+            } else {
+                const St<double, 5> w = c2p(a.eos, cell_at(a, g[0], g[1], g[2]));
+                const double rho = w[0];
+                qv[0] = w[1];
+                qv[1] = w[2];
+                qv[2] = w[4];
+                qv[3] = w[3] / rho;
+                // central differences along the two tangential axes of this face family
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    const int ga = GA[d][s], gb = GB[d][s];
+                    int lo[3] = {g[0], g[1], g[2]}, hi[3] = {g[0], g[1], g[2]};
+                    lo[gb] -= 1;
+                    hi[gb] += 1;
+                    const St<double, 5> ul = padded_cons(a, lo[0], lo[1], lo[2]);
+                    const St<double, 5> uh = padded_cons(a, hi[0], hi[1], hi[2]);
+                    const double gq = (uh[mom[ga]] - ul[mom[ga]]) / (2.0 * h[gb]);
+                    const double g0 = (uh[0] - ul[0]) / (2.0 * h[gb]);
+                    qv[4 + s] = (gq - w[mom[ga]] * g0) / rho;
+                }
+            }
+#pragma unroll
+            for (int x = 0; x < 8; ++x) Q[x * S::NE + e] = qv[x];
+        }
+        __syncthreads();
+        // ---- 2. faces
+        const double area = m.area[d];
+        const int estride = d == 0 ? 1 : (d == 1 ? E[0] : E[0] * E[1]);
+        for (int f = tid; f < nF; f += NT) {
+            const int f3[3] = {f % Fd[0], (f / Fd[0]) % Fd[1], f / (Fd[0] * Fd[1])};
+            const int g3[3] = {o3[0] + f3[0], o3[1] + f3[1], o3[2] + f3[2]};
+            const int t = g3[d];
+            bool inside = true;
+#pragma unroll
+            for (int x = 0; x < 3; ++x) inside = inside && (x == d ? g3[x] <= n3[x] : g3[x] < n3[x]);
+            double out[4] = {0.0, 0.0, 0.0, 0.0};
+            if (inside) {
+                const bool lo = t == 0, hi = t == n3[d];
+                const int eL = (f3[2] * E[1] + f3[1]) * E[0] + f3[0];   // extended position of cell t-1 (or the ghost)
+                const int eR = eL + estride;
+                double vL[3], vR[3];
+#pragma unroll
+                for (int x = 0; x < 3; ++x) {
+                    vL[x] = Q[x * S::NE + eL];
+                    vR[x] = Q[x * S::NE + eR];
+                }
+                const double TL = Q[3 * S::NE + eL], TR = Q[3 * S::NE + eR];
+                // cross terms: the cells on either side; at a side that is not periodic the cell next to it (both slots)
+                const int xL = (lo && !a.periodic[d]) ? eR : eL;
+                const int xR = (hi && !a.periodic[d]) ? eL : eR;
+                const bool phys = a.bface2 && !a.periodic[d] && (lo || hi);
+                double Gc[4];
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    if (phys) {
+                        const int ga = GA[d][s], gb = GB[d][s];
+                        int pg[3] = {g3[0], g3[1], g3[2]}, pc[3] = {g3[0], g3[1], g3[2]};
+                        pg[d] = lo ? -1 : n3[d];
+                        pc[d] = lo ? 0 : n3[d] - 1;
+                        double fc[2];
+#pragma unroll
+                        for (int w2 = 0; w2 < 2; ++w2) {
+                            const int off = w2 == 0 ? 1 : -1;
+                            int gg[3] = {pg[0], pg[1], pg[2]}, cc[3] = {pc[0], pc[1], pc[2]};
+                            gg[gb] += off;
+                            cc[gb] += off;
+                            const St<double, 5> wg = c2p(a.eos, padded_cons(a, gg[0], gg[1], gg[2]));
+                            const St<double, 5> wc = c2p(a.eos, padded_cons(a, cc[0], cc[1], cc[2]));
+                            fc[w2] = 0.5 * (wg[mom[ga]] + wc[mom[ga]]);
+                        }
+                        Gc[s] = (fc[0] - fc[1]) / (2.0 * h[gb]);
+                    } else {
+                        Gc[s] = 0.5 * (Q[(4 + s) * S::NE + xL] + Q[(4 + s) * S::NE + xR]);
+                    }
+                }
+                double Gn[3], vf[3];
+#pragma unroll
+                for (int x = 0; x < 3; ++x) {
+                    Gn[x] = (vR[x] - vL[x]) / h[d];
+                    vf[x] = 0.5 * (vL[x] + vR[x]);
+                }
+                const double dT = (TR - TL) / h[d];
+                // Gc slots: d=0: [du/dy, dv/dy, dw/dz, du/dz]; d=1: [du/dx, dv/dx, dw/dz, dv/dz]; d=2: [du/dx, dv/dy, dw/dx, dw/dy]
+                double tau[3];
+                if (d == 0) {
+                    tau[0] = a.mu * ((4.0 / 3.0) * Gn[0] - (2.0 / 3.0) * ((0.0 + Gc[1]) + Gc[2]));
+                    tau[1] = a.mu * (Gn[1] + Gc[0]);
+                    tau[2] = a.mu * (Gn[2] + Gc[3]);
+                } else if (d == 1) {
+                    tau[0] = a.mu * (Gn[0] + Gc[1]);
+                    tau[1] = a.mu * ((4.0 / 3.0) * Gn[1] - (2.0 / 3.0) * ((0.0 + Gc[0]) + Gc[2]));
+                    tau[2] = a.mu * (Gn[2] + Gc[3]);
+                } else {
+                    tau[0] = a.mu * (Gn[0] + Gc[2]);
+                    tau[1] = a.mu * (Gn[1] + Gc[3]);
+                    tau[2] = a.mu * ((4.0 / 3.0) * Gn[2] - (2.0 / 3.0) * ((0.0 + Gc[0]) + Gc[1]));
+                }
+                const double q_d = -a.k_cond * dT;
+                out[0] = tau[0] * area;
+                out[1] = tau[1] * area;
+                out[2] = (vf[0] * tau[0] + vf[1] * tau[1] + vf[2] * tau[2] - q_d) * area;
+                out[3] = tau[2] * area;
+            }
+#pragma unroll
+            for (int x = 0; x < 4; ++x) Fv[x * S::NF + f] = out[x];
+        }
+        __syncthreads();
+        // ---- 3. balance (component 0 of every viscous flux is +0)
+        for (int c = tid; c < NC; c += NT) {
+            const int c3[3] = {c % TX, (c / TX) % TY, c / (TX * TY)};
+            const int fl = (c3[2] * Fd[1] + c3[1]) * Fd[0] + c3[0];
+            const int fr = fl + (d == 0 ? 1 : (d == 1 ? Fd[0] : Fd[0] * Fd[1]));
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                const double dif = q == 0 ? 0.0 - 0.0 : Fv[(q - 1) * S::NF + fr] - Fv[(q - 1) * S::NF + fl];
+                acc[q * NC + c] = d == 0 ? 0.0 + dif : acc[q * NC + c] + dif;
+            }
+        }
+        __syncthreads();
+    }
+    // ---- residual and speed bound
+    double smax = 0.0;
+    for (int c = tid; c < NC; c += NT) {
+        const int c3[3] = {c % TX, (c / TX) % TY, c / (TX * TY)};
+        const int g3[3] = {o3[0] + c3[0], o3[1] + c3[1], o3[2] + c3[2]};
+        if (g3[0] >= m.nx || g3[1] >= m.ny || g3[2] >= m.nz) continue;
+        const long long cell = ((long long)g3[2] * m.ny + g3[1]) * m.nx + g3[0];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) a.Rv[q * m.plane + cell] = acc[q * NC + c] * m.inv_cell;
+        const St<double, 5> w = c2p(a.eos, cell_at(a, g3[0], g3[1], g3[2]));
+        const double rho = w[0];
+        const double nu_eff = vmax((4.0 / 3.0) * (a.mu / rho), (a.k_cond * (a.eos.gamma - 1.0)) / rho) + 1e-12;
+        const double vm = vmax(vmax(fabs(w[1]), fabs(w[2])), fabs(w[4]));
+        const double s = vm + sound_speed(a.eos, w[3], rho) + 2.0 * a.L * a.inv_h2 * nu_eff;
+        if (s > smax) smax = s;
+    }
+    const double bm = block_max<NT>(smax, red);
+    if (tid == 0) a.blockmax[b] = bm;
+}
+
+}   // namespace fvg

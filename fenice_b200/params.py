@@ -1,0 +1,119 @@
+"""The reference's run parameters and case files, turned into the C ABI's fvg_config.
+
+A run is described with the reference's own parameter keys (its case-file / ``--set`` keys, cpp/src/Params.cpp:100-160)
+and values, e.g. ``{"nx": 256, "reconstruction": "weno5", "riemann_solver": "HLLC (Low-Mach Thornber)"}``; missing keys
+take the reference's defaults. Names are parsed as the reference parses them (case-insensitive, GUI labels and aliases:
+parse_riemann / parse_limiter / parse_reconstruction, cpp/src/Schemes.cpp:77-102; parse_bc,
+cpp/src/Boundaries.cpp:15-27; parse_time_scheme, cpp/src/TimeScheme.cpp:73-80) and an unknown name raises ValueError,
+as the reference raises std::invalid_argument. ``time_scheme = "auto"`` resolves as in SimParams::from
+(cpp/src/Params.cpp:360-363).
+"""
+import ctypes
+import tomllib
+
+DEFAULTS = {
+    "Lx": 1.0, "Ly": 1.0, "Lz": 1.0, "nx": 100, "ny": 100, "nz": 1,
+    "eos_type": "Ideal Gas", "gamma": 1.4, "p_inf": 0.0,
+    "use_viscous": False, "mu": 1e-3, "pr": 0.72,
+    "bc_xmin": "wall", "bc_xmax": "wall", "bc_ymin": "wall", "bc_ymax": "wall", "bc_zmin": "periodic", "bc_zmax": "periodic",
+    "u_in": 0.0, "v_in": 0.0, "rho_in": 1.0, "p_out": 1.0,
+    "riemann_solver": "HLLC", "reconstruction": "none", "muscl_limiter": "Van Leer", "weno_epsilon": 1e-6,
+    "boundary_order": 2, "time_scheme": "auto", "cfl": 0.5, "shock_blend": 0.2, "dt_max": 0.0, "t_end": 0.005,
+    "max_steps": 0,
+}
+
+BC_NAMES = {"wall": 0, "inviscid wall (slip)": 0, "no_slip": 1, "viscous wall (no-slip)": 1, "moving_wall": 2, "moving wall": 2,
+            "vel_inlet": 3, "velocity inlet": 3, "massflow_inlet": 4, "mass flow inlet": 4, "outlet": 5, "pressure outlet": 5,
+            "transmissive": 6, "periodic": 7, "nonreflecting": 8, "non_reflecting": 8, "non-reflecting outlet": 8}
+RIEMANN_NAMES = {"hllc": 0, "hllc (low-mach thornber)": 1, "lowmach": 1, "lowmachhllc": 1, "low-mach": 1}
+RECON_NAMES = {"none": 0, "muscl": 1, "weno3": 2, "weno5": 3}
+LIMITER_NAMES = {"minmod": 0, "van leer": 1, "vanleer": 1, "mc": 2, "koren": 3}
+SCHEME_NAMES = {"explicit euler": 0, "euler": 0, "explicit_euler": 0, "ssp runge-kutta 2": 1, "ssprk2": 1, "rk2": 1,
+                "ssp runge-kutta 3": 2, "ssprk3": 2, "rk3": 2, "muscl-hancock": 3, "hancock": 3}
+STAGES = {0: 1, 1: 2, 2: 3, 3: 1}   # residual evaluations per step (MUSCL-Hancock: one, after its first step)
+
+
+class FvgConfig(ctypes.Structure):
+    """struct fvg_config of include/fenice_gpu.h"""
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("Lx", ctypes.c_double), ("Ly", ctypes.c_double), ("Lz", ctypes.c_double),
+                ("eos_type", ctypes.c_int), ("gamma", ctypes.c_double), ("p_inf", ctypes.c_double),
+                ("bc", ctypes.c_int * 6), ("u_in", ctypes.c_double), ("v_in", ctypes.c_double),
+                ("rho_in", ctypes.c_double), ("p_out", ctypes.c_double),
+                ("riemann", ctypes.c_int), ("shock_blend", ctypes.c_double),
+                ("reconstruction", ctypes.c_int), ("limiter", ctypes.c_int), ("weno_epsilon", ctypes.c_double),
+                ("boundary_order", ctypes.c_int), ("time_scheme", ctypes.c_int),
+                ("cfl", ctypes.c_double), ("dt_max", ctypes.c_double),
+                ("use_viscous", ctypes.c_int), ("mu", ctypes.c_double), ("pr", ctypes.c_double),
+                ("precision", ctypes.c_int), ("device", ctypes.c_int)]
+
+
+def _flag(v):
+    if isinstance(v, str):
+        s = v.strip().lower()
+        if s in ("1", "true", "yes", "on"):
+            return True
+        if s in ("0", "false", "no", "off", ""):
+            return False
+        raise ValueError(f"not a boolean: {v!r}")
+    return bool(v)
+
+
+def _pick(table, value, what):
+    key = str(value).strip().lower()
+    if key not in table:
+        raise ValueError(f"Unknown {what}: '{value}'")
+    return table[key]
+
+
+def resolve(params):
+    """The parameters with the reference's defaults filled in and time_scheme = auto resolved."""
+    p = dict(DEFAULTS)
+    p.update(params)
+    if str(p["time_scheme"]).strip().lower() == "auto":
+        rec = str(p["reconstruction"]).strip().lower()
+        p["time_scheme"] = "Explicit Euler" if rec != "muscl" else ("SSP Runge-Kutta 2" if _flag(p["use_viscous"]) else "MUSCL-Hancock")
+    return p
+
+
+def to_config(params, precision=0, device=0):
+    """fvg_config of a parameter dict (reference keys)."""
+    p = resolve(params)
+    c = FvgConfig()
+    c.nx, c.ny, c.nz = int(p["nx"]), int(p["ny"]), int(p["nz"])
+    c.Lx, c.Ly, c.Lz = float(p["Lx"]), float(p["Ly"]), float(p["Lz"])
+    c.eos_type = 0 if str(p["eos_type"]).strip().lower() == "ideal gas" else 1
+    c.gamma, c.p_inf = float(p["gamma"]), float(p["p_inf"])
+    for s, key in enumerate(("bc_xmin", "bc_xmax", "bc_ymin", "bc_ymax", "bc_zmin", "bc_zmax")):
+        c.bc[s] = _pick(BC_NAMES, p[key], "boundary condition type")
+    c.u_in, c.v_in, c.rho_in, c.p_out = float(p["u_in"]), float(p["v_in"]), float(p["rho_in"]), float(p["p_out"])
+    c.riemann = _pick(RIEMANN_NAMES, p["riemann_solver"], "Riemann solver")
+    c.shock_blend = float(p["shock_blend"])
+    c.reconstruction = _pick(RECON_NAMES, p["reconstruction"], "reconstruction")
+    c.limiter = _pick(LIMITER_NAMES, p["muscl_limiter"], "MUSCL limiter")
+    c.weno_epsilon = float(p["weno_epsilon"])
+    c.boundary_order = int(p["boundary_order"])
+    c.time_scheme = _pick(SCHEME_NAMES, p["time_scheme"], "time scheme")
+    c.cfl, c.dt_max = float(p["cfl"]), float(p["dt_max"])
+    c.use_viscous = 1 if _flag(p["use_viscous"]) else 0
+    c.mu, c.pr = float(p["mu"]), float(p["pr"])
+    c.precision = int(precision)
+    c.device = int(device)
+    return c
+
+
+def load_case(path, overrides=None):
+    """The parameters of a reference case file (TOML, sections [mesh] [thermo] [physics] [boundaries] [numerics] [run] ...;
+    cpp/include/fv/CaseFile.hpp:19-37), flattened to keys, with `overrides` on top. The [initial] table is returned
+    separately (the initial condition is the caller's: a state array)."""
+    with open(path, "rb") as f:
+        doc = tomllib.load(f)
+    params = {}
+    for section, table in doc.items():
+        if section in ("case", "initial") or not isinstance(table, dict):
+            continue
+        for k, v in table.items():
+            if not isinstance(v, (dict, list)):
+                params[k] = v
+    params.update(overrides or {})
+    return params, doc.get("initial", {})

@@ -1,0 +1,190 @@
+"""Python host binding of the C ABI (include/fenice_gpu.h, fenice_b200/libfenice_gpu.so).
+
+``Run`` mirrors the reference's hot-path interface: ``residual(U)`` is Simulation::residual (returns R and the wave
+speed, cpp/src/Simulation.cpp:1351-1354), ``step(t_end)`` one pass of the serial time loop (TimeScheme::step +
+check_progress + t += dt, cpp/src/SimulationRun.cpp:441-464) returning the reference's StepResult {dt, s_max}, and
+``run(t_end, max_steps)`` the loop itself. States are (ncells, 5) float64 arrays in the reference's layout. Failures
+raise: ValueError for a configuration the reference rejects or this build does not support, RuntimeError for a
+diverged run (the reference's std::runtime_error of check_progress) or a CUDA failure.
+
+There is no CPU fallback: without the CUDA library or a device every call raises.
+"""
+import ctypes
+import os
+from collections import namedtuple
+
+import numpy as np
+
+from . import params as P
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfenice_gpu.so")
+
+FVG_OK, FVG_ERR_CONFIG, FVG_ERR_ARGUMENT, FVG_ERR_CUDA, FVG_ERR_DIVERGED, FVG_ERR_STATE = range(6)
+
+StepResult = namedtuple("StepResult", ["dt", "s_max"])
+
+# every entry point of include/fenice_gpu.h
+EXPORTS = ["fvg_abi_version", "fvg_create", "fvg_destroy", "fvg_last_error", "fvg_create_error", "fvg_upload_state",
+           "fvg_download_state", "fvg_residual", "fvg_step", "fvg_run_until", "fvg_get_time", "fvg_set_time",
+           "fvg_get_lagged_speed", "fvg_set_lagged_speed", "fvg_dt_length", "fvg_device_state", "fvg_stream",
+           "fvg_synchronize", "fvg_face_flux_batch"]
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """The CUDA library, loaded once (ctypes); raises if it was not built (python -m fenice_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m fenice_b200.build` (nvcc, sm_100a)")
+    lib = ctypes.CDLL(path)
+    c_p = ctypes.c_void_p
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.fvg_abi_version.restype = ctypes.c_int
+    lib.fvg_create.argtypes = [ctypes.POINTER(P.FvgConfig), ctypes.POINTER(c_p)]
+    lib.fvg_destroy.argtypes = [c_p]
+    lib.fvg_last_error.argtypes = [c_p]
+    lib.fvg_last_error.restype = ctypes.c_char_p
+    lib.fvg_create_error.restype = ctypes.c_char_p
+    lib.fvg_upload_state.argtypes = [c_p, dp, ctypes.c_size_t]
+    lib.fvg_download_state.argtypes = [c_p, dp, ctypes.c_size_t]
+    lib.fvg_residual.argtypes = [c_p, ctypes.c_double, dp, ctypes.c_size_t, dp]
+    lib.fvg_step.argtypes = [c_p, ctypes.c_double, dp, dp]
+    lib.fvg_run_until.argtypes = [c_p, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.fvg_get_time.argtypes = [c_p, dp]
+    lib.fvg_set_time.argtypes = [c_p, ctypes.c_double]
+    lib.fvg_get_lagged_speed.argtypes = [c_p, dp]
+    lib.fvg_set_lagged_speed.argtypes = [c_p, ctypes.c_double]
+    lib.fvg_dt_length.argtypes = [c_p, dp]
+    lib.fvg_device_state.argtypes = [c_p, ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int)]
+    lib.fvg_stream.argtypes = [c_p, ctypes.POINTER(c_p)]
+    lib.fvg_synchronize.argtypes = [c_p]
+    lib.fvg_face_flux_batch.argtypes = [c_p, dp, dp, ctypes.POINTER(ctypes.c_int), ctypes.c_size_t, dp, dp]
+    _lib = lib
+    return lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Run:
+    """A run of the finite-volume path on one GPU."""
+
+    def __init__(self, params, U=None, precision=0, device=0):
+        self.lib = load_library()
+        self.params = P.resolve(params)
+        self.cfg = P.to_config(self.params, precision=precision, device=device)
+        h = ctypes.c_void_p()
+        rc = self.lib.fvg_create(ctypes.byref(self.cfg), ctypes.byref(h))
+        if rc != FVG_OK:
+            msg = self.lib.fvg_create_error().decode()
+            raise (ValueError if rc == FVG_ERR_CONFIG else RuntimeError)(f"fvg_create: {msg}")
+        self.h = h
+        self.shape = (self.cfg.nx, self.cfg.ny, self.cfg.nz)
+        self.ncells = self.cfg.nx * self.cfg.ny * self.cfg.nz
+        self.stages = P.STAGES[self.cfg.time_scheme]
+        if U is not None:
+            self.set_state(U)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.fvg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc == FVG_OK:
+            return
+        msg = self.lib.fvg_last_error(self.h).decode()
+        if rc in (FVG_ERR_CONFIG, FVG_ERR_ARGUMENT, FVG_ERR_STATE):
+            raise ValueError(f"{what}: {msg}")
+        raise RuntimeError(f"{what}: {msg}")
+
+    def set_state(self, U):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        if U.shape != (self.ncells, 5):
+            raise ValueError(f"state must be ({self.ncells}, 5), got {U.shape}")
+        self._check(self.lib.fvg_upload_state(self.h, _dp(U), self.ncells), "upload")
+
+    def state(self):
+        U = np.empty((self.ncells, 5))
+        self._check(self.lib.fvg_download_state(self.h, _dp(U), self.ncells), "download")
+        return U
+
+    def residual(self, U=None, predictor_half_dt=0.0, want_R=True):
+        """R and the wave speed of U (default: the run's state), as Simulation::residual."""
+        if U is not None:
+            self.set_state(U)
+        R = np.empty((self.ncells, 5)) if want_R else None
+        s = ctypes.c_double()
+        self._check(self.lib.fvg_residual(self.h, float(predictor_half_dt), _dp(R) if want_R else None, self.ncells if want_R else 0,
+                                          ctypes.byref(s)), "residual")
+        return R, s.value
+
+    def step(self, t_end):
+        dt, s = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.fvg_step(self.h, float(t_end), ctypes.byref(dt), ctypes.byref(s)), "step")
+        return StepResult(dt.value, s.value)
+
+    def run(self, t_end, max_steps=0):
+        """Steps until t >= t_end or max_steps steps (graph-captured); returns the number of steps."""
+        n = ctypes.c_int()
+        self._check(self.lib.fvg_run_until(self.h, float(t_end), int(max_steps), ctypes.byref(n)), "run")
+        return n.value
+
+    @property
+    def t(self):
+        v = ctypes.c_double()
+        self._check(self.lib.fvg_get_time(self.h, ctypes.byref(v)), "time")
+        return v.value
+
+    @t.setter
+    def t(self, value):
+        self._check(self.lib.fvg_set_time(self.h, float(value)), "time")
+
+    @property
+    def lagged_speed(self):
+        v = ctypes.c_double()
+        self._check(self.lib.fvg_get_lagged_speed(self.h, ctypes.byref(v)), "lagged speed")
+        return v.value
+
+    @lagged_speed.setter
+    def lagged_speed(self, value):
+        self._check(self.lib.fvg_set_lagged_speed(self.h, float(value)), "lagged speed")
+
+    def dt_length(self):
+        v = ctypes.c_double()
+        self._check(self.lib.fvg_dt_length(self.h, ctypes.byref(v)), "dt_length")
+        return v.value
+
+    def device_state(self):
+        """(device pointer, plane stride in doubles, nvar) of the state planes."""
+        ptr = ctypes.POINTER(ctypes.c_double)()
+        plane, nvar = ctypes.c_longlong(), ctypes.c_int()
+        self._check(self.lib.fvg_device_state(self.h, ctypes.byref(ptr), ctypes.byref(plane), ctypes.byref(nvar)), "device_state")
+        return ctypes.cast(ptr, ctypes.c_void_p).value, plane.value, nvar.value
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        self._check(self.lib.fvg_stream(self.h, ctypes.byref(s)), "stream")
+        return s.value
+
+    def synchronize(self):
+        self._check(self.lib.fvg_synchronize(self.h), "synchronize")
+
+    def face_flux_batch(self, UL, UR, axis):
+        UL = np.ascontiguousarray(UL, dtype=np.float64)
+        UR = np.ascontiguousarray(UR, dtype=np.float64)
+        ax = np.ascontiguousarray(axis, dtype=np.int32)
+        n = UL.shape[0]
+        F = np.empty((n, 5))
+        S = np.empty(n)
+        self._check(self.lib.fvg_face_flux_batch(self.h, _dp(UL), _dp(UR), ax.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n, _dp(F), _dp(S)),
+                    "face_flux_batch")
+        return F, S

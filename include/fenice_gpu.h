@@ -1,0 +1,122 @@
+/* fenice_gpu.h: the C ABI of the B200 finite-volume path (libfenice_gpu.so).
+ *
+ * The reference (Fenice, C++17) has no C ABI: its hot path sits behind two C++ seams, which these entry points
+ * replace one for one:
+ *   - the residual seam  `using ResidualFn = std::function<double(const Field& U, Field& R)>`
+ *     (cpp/include/fv/TimeScheme.hpp:14), evaluated by Simulation::residual (cpp/src/Simulation.cpp:1351-1354) with the
+ *     scheme's stage_time / predictor_half_dt (cpp/include/fv/TimeScheme.hpp:88-92)           -> fvg_residual
+ *   - the integrator seam `StepResult TimeScheme::step(Field& U, const ResidualFn&, double min_delta, double t,
+ *     double t_max, double dt_max)` (cpp/include/fv/TimeScheme.hpp:48), driven by the serial time loop
+ *     (cpp/src/SimulationRun.cpp:161-191, 441-464)                                             -> fvg_step, fvg_run
+ * and the objects behind them are configured by one plain struct, the hot-path subset of the reference's SimParams
+ * (cpp/include/fv/Params.hpp:57-147) that Simulation::setup turns into EOS, BoundaryManager, RiemannSolver,
+ * MusclReconstruction, NavierStokes and TimeScheme (cpp/src/Simulation.cpp:188-360)              -> fvg_config, fvg_create.
+ *
+ * Conventions: plain pointers and sizes, no C++ types; every call returns an int status (FVG_OK = 0) and never throws;
+ * fvg_last_error gives the message of the last failure of a handle. States cross the ABI in the reference's own layout:
+ * an array of cells of 5 doubles [rho, rho u, rho v, rho E, rho w], cell (k*ny + j)*nx + i (cpp/include/fv/Core.hpp:20-24,114).
+ * One host thread per handle; each handle owns a CUDA stream.
+ */
+#ifndef FENICE_GPU_H
+#define FENICE_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FVG_ABI_VERSION 1
+
+/* status codes */
+enum {
+    FVG_OK = 0,
+    FVG_ERR_CONFIG = 1,      /* invalid or unsupported configuration */
+    FVG_ERR_ARGUMENT = 2,    /* bad pointer or size */
+    FVG_ERR_CUDA = 3,        /* a CUDA call failed (no device, out of memory, launch failure) */
+    FVG_ERR_DIVERGED = 4,    /* non-finite wave speed or time step, or t no longer advances (check_progress) */
+    FVG_ERR_STATE = 5        /* the state is not valid for the mesh (e.g. rho w != 0 on a 2-D mesh) */
+};
+
+/* enumerations, in the reference's order */
+enum { FVG_EOS_IDEAL = 0, FVG_EOS_STIFFENED = 1 };                                  /* EOS::Type */
+enum { FVG_RIEMANN_HLLC = 0, FVG_RIEMANN_LOWMACH = 1 };                             /* RiemannType */
+enum { FVG_RECON_NONE = 0, FVG_RECON_MUSCL = 1, FVG_RECON_WENO3 = 2, FVG_RECON_WENO5 = 3 };
+enum { FVG_LIM_MINMOD = 0, FVG_LIM_VANLEER = 1, FVG_LIM_MC = 2, FVG_LIM_KOREN = 3 };  /* Limiter */
+enum { FVG_BC_WALL = 0, FVG_BC_NOSLIP, FVG_BC_MOVINGWALL, FVG_BC_VELINLET, FVG_BC_MASSFLOWINLET, FVG_BC_OUTLET,
+       FVG_BC_TRANSMISSIVE, FVG_BC_PERIODIC, FVG_BC_NONREFLECTING };                  /* BCType */
+enum { FVG_TS_EULER = 0, FVG_TS_SSPRK2 = 1, FVG_TS_SSPRK3 = 2, FVG_TS_HANCOCK = 3 };  /* TimeSchemeType */
+enum { FVG_PREC_FP64 = 0, FVG_PREC_MIXED = 1 };
+
+/* The run configuration: the reference's hot-path parameters (their case-file keys in brackets). */
+typedef struct fvg_config {
+    int nx, ny, nz;              /* [mesh] nx, ny, nz (nz = 1: a 2-D mesh) */
+    double Lx, Ly, Lz;           /* [mesh] Lx, Ly, Lz */
+    int eos_type;                /* [thermo] eos_type */
+    double gamma, p_inf;         /* [thermo] gamma, p_inf */
+    int bc[6];                   /* [boundaries] bc_xmin, bc_xmax, bc_ymin, bc_ymax, bc_zmin, bc_zmax */
+    double u_in, v_in, rho_in, p_out; /* [boundaries] */
+    int riemann;                 /* [numerics] riemann_solver */
+    double shock_blend;          /* [numerics] shock_blend (default 0.2) */
+    int reconstruction;          /* [numerics] reconstruction */
+    int limiter;                 /* [numerics] muscl_limiter */
+    double weno_epsilon;         /* [numerics] weno_epsilon */
+    int boundary_order;          /* [numerics] boundary_order (default 2) */
+    int time_scheme;             /* [numerics] time_scheme (resolved: no "auto") */
+    double cfl;                  /* [numerics] cfl */
+    double dt_max;               /* [run] dt_max (0: none) */
+    int use_viscous;             /* [physics] use_viscous */
+    double mu, pr;               /* [physics] mu, pr */
+    int precision;               /* FVG_PREC_FP64: the reference's arithmetic, bit for bit; FVG_PREC_MIXED: FP32 stencil */
+    int device;                  /* CUDA device ordinal */
+} fvg_config;
+
+typedef struct fvg_run fvg_run;
+
+/* A run on the device: validates the configuration, allocates the state and work arrays, and sets t = 0. */
+int fvg_create(const fvg_config* cfg, fvg_run** out);
+int fvg_destroy(fvg_run* run);
+const char* fvg_last_error(const fvg_run* run);
+/* A message for a failure of fvg_create (no handle exists then). */
+const char* fvg_create_error(void);
+int fvg_abi_version(void);
+
+/* The state of the run (host arrays of ncells x 5 doubles, reference layout). */
+int fvg_upload_state(fvg_run* run, const double* U, size_t ncells);
+int fvg_download_state(fvg_run* run, double* U, size_t ncells);
+
+/* Simulation::residual of the current state: R (host, ncells x 5, may be NULL) and the wave speed the residual returns;
+ * predictor_half_dt > 0 applies the MUSCL-Hancock predictor of half a step (MUSCL only). */
+int fvg_residual(fvg_run* run, double predictor_half_dt, double* R, size_t ncells, double* smax);
+
+/* One step of the serial time loop from the run's time t toward t_end: TimeScheme::step, check_progress, t += dt.
+ * dt and the step's wave speed are returned. */
+int fvg_step(fvg_run* run, double t_end, double* dt, double* smax);
+
+/* Steps until t >= t_end or `max_steps` steps were taken (max_steps <= 0: no limit), launched as CUDA graphs with the
+ * clock kept on the device; *steps gets the number taken. */
+int fvg_run_until(fvg_run* run, double t_end, int max_steps, int* steps);
+
+int fvg_get_time(const fvg_run* run, double* t);
+int fvg_set_time(fvg_run* run, double t);
+/* The MUSCL-Hancock lagged wave speed (the reference's checkpoint key S; 0: the next step seeds it). */
+int fvg_get_lagged_speed(const fvg_run* run, double* s);
+int fvg_set_lagged_speed(fvg_run* run, double s);
+/* The CFL length L in dt = cfl L / S (Simulation::setup, cpp/src/Simulation.cpp:225-227). */
+int fvg_dt_length(const fvg_run* run, double* L);
+
+/* Device access for callers that keep the state on the GPU (e.g. torch): the state planes (nvar planes of `plane`
+ * doubles each, nvar = 4 on a 2-D mesh, 5 on a 3-D mesh) and the run's CUDA stream. */
+int fvg_device_state(fvg_run* run, double** planes, long long* plane, int* nvar);
+int fvg_stream(fvg_run* run, void** stream);
+/* Wait for the run's stream. */
+int fvg_synchronize(fvg_run* run);
+
+/* Face fluxes of n face pairs (UL, UR: n x 5 doubles, axis: n ints) on the device with the run's EOS and Riemann
+ * solver (RiemannSolver::face_flux, cpp/src/Schemes.cpp:202-229): F (n x 5) and the wave speeds (n). */
+int fvg_face_flux_batch(fvg_run* run, const double* UL, const double* UR, const int* axis, size_t n, double* F, double* smax);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,107 @@
+"""Seeded inputs and the configurations the parity tests run (shared by the tests and tests/golden/make_golden.py).
+
+The fields are smooth random perturbations of a uniform flow (positive density and pressure, every velocity component
+non-zero), drawn from numpy's PCG64 with a stated seed, in the reference's layout: cells of 5 doubles
+[rho, rho u, rho v, rho E, rho w], cell (k*ny + j)*nx + i; rho w = 0 on a 2-D mesh.
+"""
+import numpy as np
+
+
+def prim_to_cons(W, gamma=1.4, p_inf=0.0, stiffened=False):
+    """Core.hpp:209-215, elementwise in numpy (IEEE double, the same operation order)."""
+    rho, u, v, p, w = W[:, 0], W[:, 1], W[:, 2], W[:, 3], W[:, 4]
+    U = np.empty_like(W)
+    ke = 0.5 * rho * (u * u + v * v + w * w)
+    e = (p + gamma * p_inf) / (gamma - 1.0) if stiffened else p / (gamma - 1.0)
+    U[:, 0] = rho
+    U[:, 1] = rho * u
+    U[:, 2] = rho * v
+    U[:, 3] = e + ke
+    U[:, 4] = rho * w
+    return U
+
+
+def smooth_field(nx, ny, nz=1, seed=0, amp=0.2, gamma=1.4, jump=False):
+    """A seeded field: a few random Fourier modes per variable (plus an optional density / pressure jump)."""
+    rng = np.random.default_rng(seed)
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    x = (i.ravel() + 0.5) / nx
+    y = (j.ravel() + 0.5) / ny
+    z = (k.ravel() + 0.5) / max(nz, 1)
+    W = np.zeros((nx * ny * nz, 5))
+    base = [1.0, 0.3, -0.2, 1.0, 0.1 if nz > 1 else 0.0]
+    for q in range(5):
+        if q == 4 and nz == 1:
+            continue
+        f = np.full(x.shape, base[q])
+        for _ in range(3):
+            a, b, c = rng.integers(1, 4, size=3)
+            ph = rng.random(3) * 2 * np.pi
+            f = f + amp * rng.random() * np.sin(2 * np.pi * a * x + ph[0]) * np.cos(2 * np.pi * b * y + ph[1]) * np.cos(2 * np.pi * c * z + ph[2])
+        W[:, q] = f
+    if jump:
+        left = x < 0.5
+        W[left, 0] *= 3.0
+        W[left, 3] *= 4.0
+    W[:, 0] = np.abs(W[:, 0]) + 0.2
+    W[:, 3] = np.abs(W[:, 3]) + 0.2
+    return prim_to_cons(W, gamma=gamma)
+
+
+BC4 = ("bc_xmin", "bc_xmax", "bc_ymin", "bc_ymax")
+
+
+def bcs(*names, z=("periodic", "periodic")):
+    d = dict(zip(BC4, names))
+    d["bc_zmin"], d["bc_zmax"] = z
+    return d
+
+
+# residual cases: (name, params, seed, predictor_half_dt)
+RESIDUAL_CASES = [
+    ("muscl_vl_periodic", dict(nx=24, ny=17, reconstruction="muscl", muscl_limiter="Van Leer", **bcs("periodic", "periodic", "periodic", "periodic")), 1, 0.0),
+    ("muscl_minmod_walls", dict(nx=20, ny=19, reconstruction="muscl", muscl_limiter="Minmod", **bcs("wall", "no_slip", "moving_wall", "wall"), u_in=0.3), 2, 0.0),
+    ("muscl_mc_inlet", dict(nx=33, ny=16, reconstruction="muscl", muscl_limiter="MC", **bcs("vel_inlet", "transmissive", "transmissive", "outlet"), u_in=1.2, p_out=0.9), 3, 0.0),
+    ("muscl_koren_order1", dict(nx=18, ny=31, reconstruction="muscl", muscl_limiter="Koren", boundary_order=1, **bcs("wall", "outlet", "transmissive", "vel_inlet"), v_in=-0.4), 4, 0.0),
+    ("weno5_hllc_mixed", dict(nx=35, ny=22, reconstruction="weno5", **bcs("transmissive", "transmissive", "wall", "vel_inlet"), u_in=0.3), 5, 0.0),
+    ("weno5_lowmach_periodic", dict(nx=16, ny=30, reconstruction="weno5", riemann_solver="HLLC (Low-Mach Thornber)", **bcs("periodic", "periodic", "periodic", "periodic")), 6, 0.0),
+    ("weno3_lowmach_walls", dict(nx=21, ny=18, reconstruction="weno3", riemann_solver="lowmach", **bcs("wall", "outlet", "periodic", "periodic")), 7, 0.0),
+    ("weno5_order1_noblend", dict(nx=19, ny=20, reconstruction="weno5", boundary_order=1, shock_blend=0.0, **bcs("no_slip", "transmissive", "wall", "outlet")), 8, 0.0),
+    ("first_order_hllc", dict(nx=17, ny=15, reconstruction="none", **bcs("wall", "outlet", "periodic", "periodic")), 9, 0.0),
+    ("weno5_stiffened", dict(nx=20, ny=16, reconstruction="weno5", eos_type="Stiffened Gas", gamma=4.4, p_inf=3.0, **bcs("transmissive", "wall", "periodic", "periodic")), 10, 0.0),
+    ("weno5_1d_row", dict(nx=64, ny=1, reconstruction="weno5", **bcs("transmissive", "transmissive", "transmissive", "transmissive")), 11, 0.0),
+    ("hancock_vl_periodic", dict(nx=24, ny=17, reconstruction="muscl", muscl_limiter="Van Leer", **bcs("periodic", "periodic", "periodic", "periodic")), 12, 0.004),
+    ("hancock_mc_inlet", dict(nx=33, ny=18, reconstruction="muscl", muscl_limiter="MC", **bcs("vel_inlet", "transmissive", "wall", "transmissive"), u_in=1.5), 13, 0.003),
+    ("hancock_minmod_order1", dict(nx=20, ny=19, reconstruction="muscl", muscl_limiter="Minmod", boundary_order=1, **bcs("no_slip", "outlet", "moving_wall", "wall"), u_in=0.2), 14, 0.005),
+    ("w5_3d_periodic_lowmach", dict(nx=12, ny=10, nz=9, reconstruction="weno5", riemann_solver="lowmach", **bcs("periodic", "periodic", "periodic", "periodic")), 15, 0.0),
+    ("w5_3d_walls", dict(nx=10, ny=11, nz=12, reconstruction="weno5", **bcs("wall", "transmissive", "no_slip", "vel_inlet", z=("outlet", "wall")), u_in=0.2), 16, 0.0),
+    ("muscl_3d_mc", dict(nx=9, ny=12, nz=10, reconstruction="muscl", muscl_limiter="MC", time_scheme="SSP Runge-Kutta 2", **bcs("transmissive", "outlet", "periodic", "periodic", z=("vel_inlet", "transmissive")), u_in=0.1), 17, 0.0),
+    ("visc_3d_periodic", dict(nx=12, ny=9, nz=10, reconstruction="weno5", riemann_solver="lowmach", use_viscous=True, mu=0.02, pr=0.71, **bcs("periodic", "periodic", "periodic", "periodic")), 18, 0.0),
+    ("visc_3d_walls", dict(nx=10, ny=9, nz=11, reconstruction="muscl", muscl_limiter="Koren", use_viscous=True, mu=0.01, **bcs("no_slip", "transmissive", "wall", "moving_wall", z=("wall", "wall")), u_in=0.3, v_in=0.1), 19, 0.0),
+    ("visc_3d_order1", dict(nx=9, ny=10, nz=8, reconstruction="weno3", boundary_order=1, use_viscous=True, mu=0.01, **bcs("moving_wall", "no_slip", "periodic", "periodic", z=("no_slip", "transmissive")), u_in=0.3, v_in=0.1), 20, 0.0),
+]
+
+# time-stepping cases: (name, params, seed, n_steps)
+STEP_CASES = [
+    ("rk3_weno5_2d", dict(nx=24, ny=20, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", cfl=0.4, **bcs("transmissive", "transmissive", "transmissive", "transmissive")), 21, 4),
+    ("rk2_muscl_2d", dict(nx=22, ny=18, reconstruction="muscl", muscl_limiter="MC", time_scheme="SSP Runge-Kutta 2", **bcs("periodic", "periodic", "wall", "wall")), 22, 4),
+    ("euler_first_order", dict(nx=20, ny=16, reconstruction="none", time_scheme="Explicit Euler", **bcs("wall", "outlet", "periodic", "periodic")), 23, 5),
+    ("hancock_vl_2d", dict(nx=26, ny=21, reconstruction="muscl", muscl_limiter="Van Leer", time_scheme="MUSCL-Hancock", **bcs("periodic", "periodic", "periodic", "periodic")), 24, 5),
+    ("hancock_mc_inlet", dict(nx=30, ny=20, reconstruction="muscl", muscl_limiter="MC", time_scheme="MUSCL-Hancock", **bcs("vel_inlet", "transmissive", "transmissive", "wall"), u_in=1.4), 25, 5),
+    ("rk3_tgv_like_3d", dict(nx=12, ny=11, nz=10, reconstruction="weno5", riemann_solver="lowmach", time_scheme="SSP Runge-Kutta 3", use_viscous=True, mu=0.01, pr=0.71, **bcs("periodic", "periodic", "periodic", "periodic")), 26, 3),
+]
+
+
+def case_field(params, seed):
+    nz = int(params.get("nz", 1))
+    gamma = float(params.get("gamma", 1.4))
+    U = smooth_field(int(params["nx"]), int(params["ny"]), nz, seed=seed, gamma=gamma, jump=seed % 3 == 0)
+    if str(params.get("eos_type", "")).lower().startswith("stiff"):
+        W = np.zeros_like(U)
+        W[:, 0] = U[:, 0]
+        W[:, 1] = U[:, 1] / U[:, 0]
+        W[:, 2] = U[:, 2] / U[:, 0]
+        W[:, 4] = U[:, 4] / U[:, 0]
+        W[:, 3] = 1.0 + 0.1 * np.cos(np.arange(U.shape[0]))
+        U = prim_to_cons(W, gamma=gamma, p_inf=float(params["p_inf"]), stiffened=True)
+    return U

@@ -1,0 +1,71 @@
+"""Writes the golden fixtures of the parity tests with the reference solver itself.
+
+    make -C oracle/ref REF=/path/to/fenice -j8 && python tests/golden/make_golden.py
+
+Runs the reference compiled from its own sources (oracle/_ref/libfenice_ref.so, through oracle/ref/ref_harness.cpp) on
+the seeded inputs of tests/cases.py and stores, per case, the parameters, the input state and the reference's output:
+  residuals.npz  one residual R(U) and its wave speed (Simulation::residual, with the MUSCL-Hancock predictor where the
+                 case has a half step)
+  steps.npz      the state after n steps of the serial time loop, with each step's dt and wave speed
+  riemann.json   the reference's bench_riemann fingerprints over one pass of its 65536 state pairs
+                 (oracle/_ref/bench_riemann 65536)
+The fixtures are test data: nothing of the product reads them.
+"""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.dirname(HERE))
+
+from oracle.oracle import Reference  # noqa: E402
+import cases  # noqa: E402
+
+
+def main():
+    res = {}
+    for name, params, seed, half in cases.RESIDUAL_CASES:
+        U = cases.case_field(params, seed)
+        ref = Reference(params, initial_state=(1, 0, 0, 1, 0))
+        R, s = ref.residual(U, predictor_half_dt=half)
+        res[f"{name}/params"] = np.array(json.dumps(params))
+        res[f"{name}/U"] = U
+        res[f"{name}/R"] = R
+        res[f"{name}/smax"] = np.array(s)
+        res[f"{name}/half_dt"] = np.array(half)
+        print(f"residual {name}: smax {s:.6g}")
+    np.savez_compressed(os.path.join(HERE, "residuals.npz"), **res)
+
+    st = {}
+    for name, params, seed, n in cases.STEP_CASES:
+        U = cases.case_field(params, seed)
+        ref = Reference(params, initial_state=(1, 0, 0, 1, 0))
+        ref.set_state(U)
+        dts, sms = ref.steps(n, 1e30)
+        st[f"{name}/params"] = np.array(json.dumps(params))
+        st[f"{name}/U0"] = U
+        st[f"{name}/U"] = ref.state()
+        st[f"{name}/dts"] = dts
+        st[f"{name}/smaxs"] = sms
+        st[f"{name}/t"] = np.array(ref.t)
+        print(f"steps {name}: {len(dts)} steps, t = {ref.t:.6g}")
+    np.savez_compressed(os.path.join(HERE, "steps.npz"), **st)
+
+    out = subprocess.run([os.path.join(ROOT, "oracle", "_ref", "bench_riemann"), "65536"], capture_output=True, text=True, check=True).stdout
+    hashes = {}
+    for line in out.splitlines():
+        parts = line.split()
+        eos, solver = parts[0], " ".join(parts[1:parts.index("ns/call") - 1])
+        hashes[f"{eos} {solver}"] = parts[parts.index("hash") + 1]
+    with open(os.path.join(HERE, "riemann.json"), "w") as f:
+        json.dump({"command": "oracle/_ref/bench_riemann 65536", "hashes": hashes}, f, indent=1)
+    print(hashes)
+
+
+if __name__ == "__main__":
+    main()
