@@ -1,0 +1,292 @@
+#!/usr/bin/env python
+"""Benchmark of the finite-volume right-hand side and time step on B200: cell-updates per second per RK stage.
+
+Workload (the configuration the metric is quoted on): 3-D Taylor-Green vortex, compressible Navier-Stokes, periodic
+[0, 2 pi]^3, 256^3 cells, WENO5-Z + low-Mach HLLC + SSP-RK3, mu = 6.25e-4 (Re = 1600), Pr = 0.71, gamma = 1.4, CFL 0.5,
+Ma = 0.1 initial state. A "step" is one SSP-RK3 time step (three residual stages, each the viscous sweep and the fused
+reconstruction / Riemann / balance / update kernel); the metric counts cells x 3 per step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One JSON line on rank 0. `value` is timed on the device with CUDA events on the run's stream (state resident in HBM);
+`e2e` goes through the public API per step with the state copied from pinned host memory and the result read back;
+`roofline` relates the stage kernel's algorithmic bytes to its measured duration; `cpu_baseline` times the reference
+solver (compiled from its sources, oracle/_ref) on this machine's host cores on a bounded sample of the same workload.
+Under torchrun (N > 1) every rank runs its own replica of the workload (weak scaling, no exchange between ranks).
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s per RK stage, mixed+learned vs plain FP64 on B200 at stated L1 err"
+UNIT = "cell-updates/s"
+STAGES = 3
+BYTES_PER_CELL_STAGE = (2 + 3 + 3) / 3 * 5 * 8   # SSP-RK3, 3-D: stage 1 reads U writes R; stages 2-3 read two states, write one
+
+
+def workload(n):
+    L = 2 * math.pi
+    return dict(nx=n, ny=n, nz=n, Lx=L, Ly=L, Lz=L, gamma=1.4, use_viscous=True, mu=6.25e-4, pr=0.71,
+                bc_xmin="periodic", bc_xmax="periodic", bc_ymin="periodic", bc_ymax="periodic", bc_zmin="periodic", bc_zmax="periodic",
+                riemann_solver="HLLC (Low-Mach Thornber)", reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", cfl=0.5)
+
+
+def tgv_state(n, gamma=1.4):
+    """u = sin x cos y cos z, v = -cos x sin y cos z, w = 0, rho = 1, p = 1/(gamma Ma^2) + (cos 2x + cos 2y)(cos 2z + 2)/16,
+    Ma = 0.1, at the cell centres, as conservative cells [rho, rho u, rho v, rho E, rho w] (cell (k*n + j)*n + i)."""
+    h = 2 * math.pi / n
+    c = (np.arange(n) + 0.5) * h
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    u = (np.sin(x) * np.cos(y) * np.cos(z)).ravel()
+    v = (-np.cos(x) * np.sin(y) * np.cos(z)).ravel()
+    p = (1.0 / (gamma * 0.01) + (np.cos(2 * x) + np.cos(2 * y)) * (np.cos(2 * z) + 2.0) / 16.0).ravel()
+    U = np.zeros((n ** 3, 5))
+    U[:, 0] = 1.0
+    U[:, 1] = u
+    U[:, 2] = v
+    U[:, 3] = p / (gamma - 1.0) + 0.5 * (u * u + v * v)
+    return U
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = ["clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + ",".join(self.FIELDS), "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (getattr(self, "out", "") or "").splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) != len(self.FIELDS):
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = max(smax, float(parts[1]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[3:]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(n):
+    """Per-launch DRAM bytes of the stage kernel from the committed ncu summary, scaled to n^3 cells, or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "stage_kernel_weno5_3d.json")) as f:
+            d = json.load(f)
+        return d["dram_bytes_per_launch"] * (n ** 3) / d["cells"]
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def cpu_reference_rate(n, warm, timed):
+    """The reference solver (oracle/_ref, compiled from its sources) on the host cores: RK3 steps of the same workload."""
+    from oracle.oracle import Reference
+
+    ref = Reference({k: v for k, v in workload(n).items()}, initial_profile="taylor_green_3d")
+    ref.steps(warm, 1e30)
+    t0 = time.perf_counter()
+    done = len(ref.steps(timed, 1e30)[0])
+    wall = time.perf_counter() - t0
+    return n ** 3 * STAGES * done / wall, wall, done
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def allmax(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def gpu_arm(args, world, rank, local):
+    import torch
+
+    from fenice_b200 import Run
+
+    n = args.size
+    params = workload(n)
+    U0 = tgv_state(n)
+    run = Run(params, U=U0, device=local)
+    ext = torch.cuda.ExternalStream(run.stream(), device=torch.device("cuda", local))
+    # warm-up (untimed), then K timed steps with CUDA events on the run's stream around the whole region and around
+    # every launch of the stage and viscous kernels
+    if args.warmup:
+        run.run(1e30, max_steps=args.warmup)
+    run.synchronize()
+    run.set_timing(True)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        start.record(ext)
+        steps = run.run(1e30, max_steps=args.steps)
+        end.record(ext)
+        run.synchronize()
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = start.elapsed_time(end)
+    tm = run.timing()
+    run.set_timing(False)
+    assert steps == args.steps, f"{steps} of {args.steps} steps ran"
+    ms = allmax(ms, world)
+    cells = n ** 3
+    value = world * cells * STAGES * args.steps / (ms * 1e-3)
+
+    # end to end through the public API: per step the state goes host (pinned) -> device, one step, device -> host
+    e2e = None
+    if args.e2e_steps > 0:
+        host = torch.empty((cells, 5), dtype=torch.float64, pin_memory=True).numpy()
+        host[:] = run.state()
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            run.set_state(host)
+            run.step(1e30)
+            host[:] = run.state()
+        wall = time.perf_counter() - t0
+        wall = allmax(wall, world)
+        e2e = {"value": world * cells * STAGES * args.e2e_steps / wall, "unit": UNIT, "h2d_bytes_per_step": cells * 5 * 8,
+               "d2h_bytes_per_step": cells * 5 * 8, "steps": args.e2e_steps, "timing": "host wall clock around upload + step + download"}
+
+    peak, peak_kind = measured_peak()
+    stage_avg_ms = tm["stage_ms"] / max(tm["stage_launches"], 1)
+    alg_bytes = cells * BYTES_PER_CELL_STAGE
+    achieved = alg_bytes / (stage_avg_ms * 1e-3) / 1e9
+    traffic = ncu_traffic(n)
+    roofline = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": traffic, "peak_source": f"hbm_gbs of MEASURED_PEAKS.json ({peak_kind})",
+                "kernel": "stage_kernel<3, WENO5, LowMach> (fused reconstruction + Riemann + balance + RK update)",
+                "algorithmic_bytes_per_launch": alg_bytes, "stage_launch_ms": round(stage_avg_ms, 4),
+                "viscous_launch_ms": round(tm["viscous_ms"] / max(tm["viscous_launches"], 1), 4),
+                "stage_share_of_step": round(tm["stage_ms"] / ms, 4), "viscous_share_of_step": round(tm["viscous_ms"] / ms, 4)}
+    # my kernels per RK3 step: 3 viscous + 3 stage + dt + axpy + 2 stage maxima + end; one begin per run
+    launches = args.steps * 11 + 1
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (Taylor-Green initial state computed in numpy)",
+            "config": {"workload": f"Taylor-Green vortex 3-D {n}^3, WENO5-Z + low-Mach HLLC + SSP-RK3, viscous Re 1600 Pr 0.71, CFL 0.5, "
+                                   f"plain FP64 form", "cells": cells, "stages_per_step": STAGES,
+                       "parallelism": f"replicas{world}" if world > 1 else "single GPU",
+                       "l2": f"inputs larger than L2 ({cells * 40 / 1e6:.0f} MB per state field), no flush"},
+            "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary()}
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fenice_b200", choices=["fenice_b200", "reference"])
+    ap.add_argument("--size", type=int, default=256, help="cells per axis (256: the benchmark workload)")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-baseline", type=int, default=1, help="time the reference on the host cores (rank 0, N = 1)")
+    args = ap.parse_args()
+    world, rank, local = (1, 0, 0) if args.impl == "reference" and int(os.environ.get("WORLD_SIZE", "1")) == 1 else dist_setup()
+    threads = len(os.sched_getaffinity(0))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        warm, timed = min(args.warmup, 1), max(1, min(args.steps, 3))
+        os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+        rate, wall, done = cpu_reference_rate(args.size, warm, timed)
+        sample = f"{done} SSP-RK3 step(s) of the {args.size}^3 mesh after {warm} untimed, {threads} OpenMP threads"
+        line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": done, "warmup": warm,
+                "ms_per_step": 1e3 * wall / done, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (the reference's taylor_green_3d profile)", "impl": "reference",
+                "config": {"workload": f"Taylor-Green vortex 3-D {args.size}^3, WENO5-Z + low-Mach HLLC + SSP-RK3, viscous Re 1600 Pr 0.71, "
+                                       f"CFL 0.5", "cells": args.size ** 3, "stages_per_step": STAGES},
+                "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+                "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    line = gpu_arm(args, world, rank, local)
+    if rank == 0 and world == 1 and args.cpu_baseline:
+        os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+        try:
+            rate, wall, done = cpu_reference_rate(args.size, 1, 1)
+            line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                                    "sample": f"{done} SSP-RK3 step of the {args.size}^3 mesh after 1 untimed ({wall:.1f} s)"}
+        except Exception as e:  # the reference binary is absent: say so
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": threads, "kind": "reference", "sample": f"unavailable: {e}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -241,6 +241,16 @@ struct fvg_run {
     StageLauncher stage;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};   // two steps, by the buffer the state starts in (MUSCL-Hancock ping-pong)
     int cur = 0;   // MUSCL-Hancock ping-pong: 0 the state is in U, 1 in Ut
+    // kernel timing (fvg_set_timing): CUDA events around each launch of the stage (or predictor) kernel and of the
+    // viscous kernel, on the run's stream; the steps are then launched one by one instead of as graphs
+    struct EvTimer {
+        std::vector<cudaEvent_t> ev;
+        size_t used = 0;
+        double ms = 0.0;
+        long long n = 0;
+    };
+    bool timing = false;
+    EvTimer t_stage, t_visc;
     double* Ucur() { return cur ? Ut : U; }
 };
 
@@ -372,14 +382,41 @@ cudaError_t launch_hancock(fvg_run* r, const HancockArgs& a) {
     return r->cfg.riemann == FVG_RIEMANN_LOWMACH ? launch_hancock_t<kLowMach>(a, r->nbh, r->stream) : launch_hancock_t<kHLLC>(a, r->nbh, r->stream);
 }
 
+void timer_mark(fvg_run* r, fvg_run::EvTimer& t) {
+    if (!r->timing) return;
+    if (t.used == t.ev.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        t.ev.push_back(e);
+    }
+    cudaEventRecord(t.ev[t.used++], r->stream);
+}
+
+// after a stream synchronisation: add up the recorded (start, end) pairs
+void timer_flush(fvg_run::EvTimer& t) {
+    for (size_t k = 0; k + 1 < t.used; k += 2) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, t.ev[k], t.ev[k + 1]) == cudaSuccess) {
+            t.ms += ms;
+            t.n += 1;
+        }
+    }
+    t.used = 0;
+}
+
 // One residual stage of Uin: the viscous sweep (3-D viscous runs), then the inviscid stage kernel.
 cudaError_t residual_stage(fvg_run* r, const double* Uin, const double* U0, double* out, int mode, double ca, double cb, int stage, const int* gate) {
     cudaError_t e;
     if (r->cfg.use_viscous) {
+        timer_mark(r, r->t_visc);
         e = launch_viscous(visc_args(r, Uin, r->bmv[stage], gate), r->nbv, r->stream);
+        timer_mark(r, r->t_visc);
         if (e != cudaSuccess) return e;
     }
-    return r->stage.launch(stage_args(r, Uin, U0, out, mode, ca, cb, r->cfg.use_viscous ? r->Rv : nullptr, r->bm[stage], gate), r->nb, r->stream);
+    timer_mark(r, r->t_stage);
+    e = r->stage.launch(stage_args(r, Uin, U0, out, mode, ca, cb, r->cfg.use_viscous ? r->Rv : nullptr, r->bm[stage], gate), r->nb, r->stream);
+    timer_mark(r, r->t_stage);
+    return e;
 }
 
 int axpy_blocks(const fvg_run* r) {
@@ -402,7 +439,10 @@ cudaError_t enqueue_step(fvg_run* r) {
         if ((e = r->stage.launch(stage_args(r, Uin, nullptr, r->R, kStoreR, 0, 0, nullptr, r->bm_seed, &c->seed), r->nb, r->stream))) return e;
         k_hancock_seed<<<1, 1024, 0, r->stream>>>(c, r->bm_seed, r->nb);
         k_hancock_dt<<<1, 1, 0, r->stream>>>(c);
-        if ((e = launch_hancock(r, hancock_args(r, Uin, Uout, kAxpy, r->bm[0], act)))) return e;
+        timer_mark(r, r->t_stage);
+        e = launch_hancock(r, hancock_args(r, Uin, Uout, kAxpy, r->bm[0], act));
+        timer_mark(r, r->t_stage);
+        if (e) return e;
         k_hancock_end<<<1, 1024, 0, r->stream>>>(c, r->bm[0], r->nbh);
         r->cur ^= 1;
         return cudaGetLastError();
@@ -555,6 +595,8 @@ int fvg_destroy(fvg_run* run) {
     if (!run) return FVG_OK;
     cudaSetDevice(run->cfg.device);
     if (run->stream) cudaStreamSynchronize(run->stream);
+    for (cudaEvent_t e : run->t_stage.ev) cudaEventDestroy(e);
+    for (cudaEvent_t e : run->t_visc.ev) cudaEventDestroy(e);
     for (int g = 0; g < 2; ++g)
         if (run->graph[g]) cudaGraphExecDestroy(run->graph[g]);
     for (double* p : {run->U, run->Ut, run->R, run->Rv, run->staging, run->bm_seed, run->bm[0], run->bm[1], run->bm[2], run->bmv[0], run->bmv[1], run->bmv[2]})
@@ -650,6 +692,24 @@ static int run_steps(fvg_run* run, double t_end, int max_steps, int use_graph, i
         if ((rc = read_ctl(run, &h))) return rc;
         done = h.steps;
         if (hancock && done == 0) run->cur ^= 1;   // the step did not run: the state stayed where it was
+    } else if (run->timing) {
+        // timed: the same launches, one step at a time, events around the kernels
+        const int cur0 = run->cur;
+        int chunk = 4;
+        while (true) {
+            for (int k = 0; k < chunk; ++k) {
+                cudaError_t e = enqueue_step(run);
+                if (e != cudaSuccess) return fail(run, FVG_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+            }
+            if ((rc = read_ctl(run, &h))) return rc;
+            timer_flush(run->t_stage);
+            timer_flush(run->t_visc);
+            if (!h.active) break;
+            if (chunk < 64) chunk *= 2;
+        }
+        done = h.steps;
+        // every enqueue flipped the ping-pong; only the steps that ran moved the state
+        if (hancock) run->cur = (cur0 + done) & 1;
     } else {
         // a graph of two steps (the MUSCL-Hancock ping-pong returns to its buffer after two)
         cudaGraphExec_t& graph = run->graph[run->cur];
@@ -759,6 +819,24 @@ int fvg_stream(fvg_run* run, void** stream) {
 int fvg_synchronize(fvg_run* run) {
     if (!run) return FVG_ERR_ARGUMENT;
     CK(cudaStreamSynchronize(run->stream));
+    return FVG_OK;
+}
+
+int fvg_set_timing(fvg_run* run, int on) {
+    if (!run) return FVG_ERR_ARGUMENT;
+    run->timing = on != 0;
+    run->t_stage.ms = run->t_visc.ms = 0.0;
+    run->t_stage.n = run->t_visc.n = 0;
+    run->t_stage.used = run->t_visc.used = 0;
+    return FVG_OK;
+}
+
+int fvg_get_timing(const fvg_run* run, double* stage_ms, long long* stage_launches, double* viscous_ms, long long* viscous_launches) {
+    if (!run) return FVG_ERR_ARGUMENT;
+    if (stage_ms) *stage_ms = run->t_stage.ms;
+    if (stage_launches) *stage_launches = run->t_stage.n;
+    if (viscous_ms) *viscous_ms = run->t_visc.ms;
+    if (viscous_launches) *viscous_launches = run->t_visc.n;
     return FVG_OK;
 }
 

@@ -1,11 +1,13 @@
 // Navier-Stokes viscous and heat fluxes on a 3-D mesh (NavierStokes::viscous_residual_3d, cpp/src/Physics.cpp:484-830).
 //
-// A CTA owns a TX x TY x TZ tile and sweeps its axes in turn, like the stage kernel. Per axis d:
-//   1. cells:   for the tile extended by one cell along d, the cell quantities of the reference's sweep: velocity,
-//               T = p / rho, and the four velocity-gradient entries G[a][b] = (d(rho u_a)/dx_b - u_a d(rho)/dx_b) / rho
-//               that the faces of axis d read (central differences of the padded conservative state); a position beyond
-//               a periodic side is the wrapped cell, beyond another side the ghost entry (velocity and T only);
-//   2. faces:   compact normal derivatives, face-averaged cross derivatives, Stokes stress and Fourier heat flux;
+// A CTA owns a TX x TY x TZ tile. It first stages the reference's padded conservative state of the tile and one cell
+// around it in shared memory (padded_3d + fix_padded_corners semantics, a periodic side wrapped), then sweeps its axes
+// in turn, like the stage kernel. Per axis d:
+//   1. cells:   for the tile extended by one cell along d, the four velocity-gradient entries
+//               G[a][b] = (d(rho u_a)/dx_b - u_a d(rho)/dx_b) / rho that the faces of axis d read (central differences of
+//               the padded conservative state);
+//   2. faces:   velocity and T = p / rho on both sides, compact normal derivatives, face-averaged cross derivatives,
+//               Stokes stress and Fourier heat flux;
 //   3. balance: ((0 + (Fr - Fl)) + (Ft - Fb)) + (Fk - Ff), accumulated in shared memory in that order.
 // The result, times 1 / volume, is the viscous residual Rv of every cell (added to the inviscid one by the stage
 // kernel, R + Rv being the reference's `r += ...`), and each CTA writes the largest viscous speed bound of its cells
@@ -107,23 +109,34 @@ __device__ __forceinline__ St<double, 5> padded_cons(const ViscArgs& a, int i, i
     return cell_at(a, p[0], p[1], p[2]);
 }
 
+// the momentum slots of the velocity components, and the (a, b) of the four gradient entries the faces of axis d read, in
+// the reference's CrossGhosts order (cpp/src/Physics.cpp:653-667)
+__constant__ int kViscMom[3] = {1, 2, 4};
+__constant__ int kViscGA[3][4] = {{0, 1, 2, 0}, {0, 1, 2, 1}, {0, 1, 2, 2}};
+__constant__ int kViscGB[3][4] = {{1, 1, 2, 2}, {0, 0, 2, 2}, {0, 1, 0, 1}};
+
+// velocity component a (0, 1, 2) of a primitive state, without indexing the state by a run-time value
+__device__ __forceinline__ double velc(const St<double, 5>& w, int a) { return a == 0 ? w[1] : (a == 1 ? w[2] : w[4]); }
+
 template <int TX, int TY, int TZ> struct ViscShape {
     static constexpr int NC = TX * TY * TZ;
+    static constexpr int BX = TX + 2, BY = TY + 2, BZ = TZ + 2, NB = BX * BY * BZ;   // padded box of the tile
     static constexpr int cmax(int x, int y) { return x > y ? x : y; }
     static constexpr int NE = cmax(cmax((TX + 2) * TY * TZ, TX * (TY + 2) * TZ), TX * TY * (TZ + 2));
     static constexpr int NF = cmax(cmax((TX + 1) * TY * TZ, TX * (TY + 1) * TZ), TX * TY * (TZ + 1));
-    // Q [8][NE] cell quantities (u, v, w, T, four G), F [4][NF] face fluxes (components 1..4), acc [5][NC], red [32]
-    static constexpr int SMEM_DOUBLES = 8 * NE + 4 * NF + 5 * NC + 32;
+    // B [5][NB] padded conservative box, G [4][NE] gradient entries, F [4][NF] face fluxes (components 1..4), acc [5][NC], red [32]
+    static constexpr int SMEM_DOUBLES = 5 * NB + 4 * NE + 4 * NF + 5 * NC + 32;
     static constexpr size_t SMEM_BYTES = sizeof(double) * SMEM_DOUBLES;
 };
 
 template <int TX, int TY, int TZ, int NT>
 __global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
     using S = ViscShape<TX, TY, TZ>;
-    constexpr int NC = S::NC;
+    constexpr int NC = S::NC, BX = S::BX, BY = S::BY, NB = S::NB;
     extern __shared__ double smem[];
-    double* Q = smem;                 // [8][NE]
-    double* Fv = Q + 8 * S::NE;       // [4][NF]
+    double* B = smem;                 // [5][NB]
+    double* G = B + 5 * NB;           // [4][NE]
+    double* Fv = G + 4 * S::NE;       // [4][NF]
     double* acc = Fv + 4 * S::NF;     // [5][NC]
     double* red = acc + 5 * NC;
     if (!*a.gate) return;
@@ -132,10 +145,34 @@ __global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
     const int o3[3] = {(b % a.tiles[0]) * TX, ((b / a.tiles[0]) % a.tiles[1]) * TY, (b / (a.tiles[0] * a.tiles[1])) * TZ};
     const int n3[3] = {m.nx, m.ny, m.nz};
     const double h[3] = {m.dx, m.dy, m.dz};
-    const int mom[3] = {1, 2, 4};
-    // the (a, b) of the four gradient entries the faces of axis d read, in the reference's CrossGhosts order
-    const int GA[3][4] = {{0, 1, 2, 0}, {0, 1, 2, 1}, {0, 1, 2, 2}};
-    const int GB[3][4] = {{1, 1, 2, 2}, {0, 0, 2, 2}, {0, 1, 0, 1}};
+    const int* mom = kViscMom;
+    const auto& GA = kViscGA;
+    const auto& GB = kViscGB;
+    // box position (tile-relative cell index -1 .. T per axis) -> shared-memory index
+    auto bidx = [&](int i, int j, int k) { return ((k + 1) * BY + (j + 1)) * BX + (i + 1); };
+    auto cons = [&](int p) {
+        St<double, 5> u;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) u[q] = B[q * NB + p];
+        return u;
+    };
+
+    // ---- 0. the padded conservative state of the tile and one cell around it. A position beyond a periodic side is the
+    // wrapped cell (so the box holds the neighbours the reference reads for that cell); the rest is the reference's
+    // padded array (padded_cons). The eight corners are never read.
+    for (int e = tid; e < NB; e += NT) {
+        int g[3] = {o3[0] + e % BX - 1, o3[1] + (e / BX) % BY - 1, o3[2] + e / (BX * BY) - 1};
+#pragma unroll
+        for (int x = 0; x < 3; ++x)
+            if (a.periodic[x] && (g[x] < 0 || g[x] >= n3[x])) g[x] = ((g[x] % n3[x]) + n3[x]) % n3[x];
+        // a tile that overhangs the mesh: positions past the ghost layer are clamped onto it (their results are not used)
+#pragma unroll
+        for (int x = 0; x < 3; ++x) g[x] = g[x] < -1 ? -1 : (g[x] > n3[x] ? n3[x] : g[x]);
+        const St<double, 5> u = padded_cons(a, g[0], g[1], g[2]);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) B[q * NB + e] = u[q];
+    }
+    __syncthreads();
 
 #pragma unroll 1
     for (int d = 0; d < 3; ++d) {
@@ -143,60 +180,27 @@ __global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
         E[d] += 2;
         Fd[d] += 1;
         const int nE = E[0] * E[1] * E[2], nF = Fd[0] * Fd[1] * Fd[2];
-        // ---- 1. cell quantities
+        // ---- 1. the four gradient entries of the cells of the tile extended along d (meaningless at a ghost position)
         for (int e = tid; e < nE; e += NT) {
-            int g[3] = {e % E[0], (e / E[0]) % E[1], e / (E[0] * E[1])};
-            g[d] -= 1;
+            int l[3] = {e % E[0], (e / E[0]) % E[1], e / (E[0] * E[1])};
+            l[d] -= 1;
+            const int p = bidx(l[0], l[1], l[2]);
+            const St<double, 5> w = c2p(a.eos, cons(p));
+            const double rho = w[0];
 #pragma unroll
-            for (int x = 0; x < 3; ++x) g[x] += o3[x];
-            bool ghost = false;
-            if (g[d] < 0 || g[d] >= n3[d]) {
-                if (a.periodic[d])
-                    g[d] = ((g[d] % n3[d]) + n3[d]) % n3[d];
-                else
-                    ghost = true;
+            for (int s = 0; s < 4; ++s) {
+                const int ga = GA[d][s], gb = GB[d][s];
+                const int off = gb == 0 ? 1 : (gb == 1 ? BX : BX * BY);
+                const double gq = (B[mom[ga] * NB + p + off] - B[mom[ga] * NB + p - off]) / (2.0 * h[gb]);
+                const double g0 = (B[p + off] - B[p - off]) / (2.0 * h[gb]);
+                G[s * S::NE + e] = (gq - velc(w, ga) * g0) / rho;
             }
-            // a tile that overhangs the mesh: any cell inside (its results are not used)
-#pragma unroll
-            for (int x = 0; x < 3; ++x)
-                if (x != d) g[x] = g[x] < n3[x] ? g[x] : n3[x] - 1;
-            double qv[8];
-            if (ghost) {
-                const St<double, 5> gc = face_ghost(a, d, g[0], g[1], g[2]);
-                const St<double, 5> w = c2p(a.eos, gc);
-                qv[0] = w[1];
-                qv[1] = w[2];
-                qv[2] = w[4];
-                qv[3] = w[3] / w[0];
-                qv[4] = qv[5] = qv[6] = qv[7] = 0.0;
-            } else {
-                const St<double, 5> w = c2p(a.eos, cell_at(a, g[0], g[1], g[2]));
-                const double rho = w[0];
-                qv[0] = w[1];
-                qv[1] = w[2];
-                qv[2] = w[4];
-                qv[3] = w[3] / rho;
-                // central differences along the two tangential axes of this face family
-#pragma unroll
-                for (int s = 0; s < 4; ++s) {
-                    const int ga = GA[d][s], gb = GB[d][s];
-                    int lo[3] = {g[0], g[1], g[2]}, hi[3] = {g[0], g[1], g[2]};
-                    lo[gb] -= 1;
-                    hi[gb] += 1;
-                    const St<double, 5> ul = padded_cons(a, lo[0], lo[1], lo[2]);
-                    const St<double, 5> uh = padded_cons(a, hi[0], hi[1], hi[2]);
-                    const double gq = (uh[mom[ga]] - ul[mom[ga]]) / (2.0 * h[gb]);
-                    const double g0 = (uh[0] - ul[0]) / (2.0 * h[gb]);
-                    qv[4 + s] = (gq - w[mom[ga]] * g0) / rho;
-                }
-            }
-#pragma unroll
-            for (int x = 0; x < 8; ++x) Q[x * S::NE + e] = qv[x];
         }
         __syncthreads();
         // ---- 2. faces
         const double area = m.area[d];
         const int estride = d == 0 ? 1 : (d == 1 ? E[0] : E[0] * E[1]);
+        const int bstride = d == 0 ? 1 : (d == 1 ? BX : BX * BY);
         for (int f = tid; f < nF; f += NT) {
             const int f3[3] = {f % Fd[0], (f / Fd[0]) % Fd[1], f / (Fd[0] * Fd[1])};
             const int g3[3] = {o3[0] + f3[0], o3[1] + f3[1], o3[2] + f3[2]};
@@ -207,15 +211,14 @@ __global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
             double out[4] = {0.0, 0.0, 0.0, 0.0};
             if (inside) {
                 const bool lo = t == 0, hi = t == n3[d];
-                const int eL = (f3[2] * E[1] + f3[1]) * E[0] + f3[0];   // extended position of cell t-1 (or the ghost)
+                const int eL = (f3[2] * E[1] + f3[1]) * E[0] + f3[0];   // extended position of the cell t-1 (or the ghost)
                 const int eR = eL + estride;
-                double vL[3], vR[3];
-#pragma unroll
-                for (int x = 0; x < 3; ++x) {
-                    vL[x] = Q[x * S::NE + eL];
-                    vR[x] = Q[x * S::NE + eR];
-                }
-                const double TL = Q[3 * S::NE + eL], TR = Q[3 * S::NE + eR];
+                int lc[3] = {f3[0], f3[1], f3[2]};
+                lc[d] -= 1;
+                const int pL = bidx(lc[0], lc[1], lc[2]), pR = pL + bstride;
+                const St<double, 5> wL = c2p(a.eos, cons(pL)), wR = c2p(a.eos, cons(pR));
+                const double vL[3] = {wL[1], wL[2], wL[4]}, vR[3] = {wR[1], wR[2], wR[4]};
+                const double TL = wL[3] / wL[0], TR = wR[3] / wR[0];
                 // cross terms: the cells on either side; at a side that is not periodic the cell next to it (both slots)
                 const int xL = (lo && !a.periodic[d]) ? eR : eL;
                 const int xR = (hi && !a.periodic[d]) ? eL : eR;
@@ -224,24 +227,21 @@ __global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {
                     if (phys) {
+                        // d u_a / d x_b from the tangential difference of the face values (ghost and cell averages)
                         const int ga = GA[d][s], gb = GB[d][s];
-                        int pg[3] = {g3[0], g3[1], g3[2]}, pc[3] = {g3[0], g3[1], g3[2]};
-                        pg[d] = lo ? -1 : n3[d];
-                        pc[d] = lo ? 0 : n3[d] - 1;
+                        const int pg = lo ? pL : pR, pc = lo ? pR : pL;
+                        const int off = gb == 0 ? 1 : (gb == 1 ? BX : BX * BY);
                         double fc[2];
 #pragma unroll
                         for (int w2 = 0; w2 < 2; ++w2) {
-                            const int off = w2 == 0 ? 1 : -1;
-                            int gg[3] = {pg[0], pg[1], pg[2]}, cc[3] = {pc[0], pc[1], pc[2]};
-                            gg[gb] += off;
-                            cc[gb] += off;
-                            const St<double, 5> wg = c2p(a.eos, padded_cons(a, gg[0], gg[1], gg[2]));
-                            const St<double, 5> wc = c2p(a.eos, padded_cons(a, cc[0], cc[1], cc[2]));
-                            fc[w2] = 0.5 * (wg[mom[ga]] + wc[mom[ga]]);
+                            const int o = w2 == 0 ? off : -off;
+                            const St<double, 5> wg = c2p(a.eos, cons(pg + o));
+                            const St<double, 5> wc = c2p(a.eos, cons(pc + o));
+                            fc[w2] = 0.5 * (velc(wg, ga) + velc(wc, ga));
                         }
                         Gc[s] = (fc[0] - fc[1]) / (2.0 * h[gb]);
                     } else {
-                        Gc[s] = 0.5 * (Q[(4 + s) * S::NE + xL] + Q[(4 + s) * S::NE + xR]);
+                        Gc[s] = 0.5 * (G[s * S::NE + xL] + G[s * S::NE + xR]);
                     }
                 }
                 double Gn[3], vf[3];
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
         const long long cell = ((long long)g3[2] * m.ny + g3[1]) * m.nx + g3[0];
 #pragma unroll
         for (int q = 0; q < 5; ++q) a.Rv[q * m.plane + cell] = acc[q * NC + c] * m.inv_cell;
-        const St<double, 5> w = c2p(a.eos, cell_at(a, g3[0], g3[1], g3[2]));
+        const St<double, 5> w = c2p(a.eos, cons(bidx(c3[0], c3[1], c3[2])));
         const double rho = w[0];
         const double nu_eff = vmax((4.0 / 3.0) * (a.mu / rho), (a.k_cond * (a.eos.gamma - 1.0)) / rho) + 1e-12;
         const double vm = vmax(vmax(fabs(w[1]), fabs(w[2])), fabs(w[4]));

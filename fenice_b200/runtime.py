@@ -28,7 +28,7 @@ StepResult = namedtuple("StepResult", ["dt", "s_max"])
 EXPORTS = ["fvg_abi_version", "fvg_create", "fvg_destroy", "fvg_last_error", "fvg_create_error", "fvg_upload_state",
            "fvg_download_state", "fvg_residual", "fvg_step", "fvg_run_until", "fvg_get_time", "fvg_set_time",
            "fvg_get_lagged_speed", "fvg_set_lagged_speed", "fvg_dt_length", "fvg_device_state", "fvg_stream",
-           "fvg_synchronize", "fvg_face_flux_batch"]
+           "fvg_synchronize", "fvg_face_flux_batch", "fvg_set_timing", "fvg_get_timing"]
 
 _lib = None
 
@@ -63,6 +63,9 @@ def load_library(path=LIB_PATH):
     lib.fvg_stream.argtypes = [c_p, ctypes.POINTER(c_p)]
     lib.fvg_synchronize.argtypes = [c_p]
     lib.fvg_face_flux_batch.argtypes = [c_p, dp, dp, ctypes.POINTER(ctypes.c_int), ctypes.c_size_t, dp, dp]
+    lib.fvg_set_timing.argtypes = [c_p, ctypes.c_int]
+    ll = ctypes.POINTER(ctypes.c_longlong)
+    lib.fvg_get_timing.argtypes = [c_p, dp, ll, dp, ll]
     _lib = lib
     return lib
 
@@ -177,6 +180,15 @@ class Run:
 
     def synchronize(self):
         self._check(self.lib.fvg_synchronize(self.h), "synchronize")
+
+    def set_timing(self, on=True):
+        self._check(self.lib.fvg_set_timing(self.h, 1 if on else 0), "set_timing")
+
+    def timing(self):
+        """{stage_ms, stage_launches, viscous_ms, viscous_launches} summed since set_timing(True)."""
+        a, b, c, d = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_double(), ctypes.c_longlong()
+        self._check(self.lib.fvg_get_timing(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d)), "get_timing")
+        return {"stage_ms": a.value, "stage_launches": b.value, "viscous_ms": c.value, "viscous_launches": d.value}
 
     def face_flux_batch(self, UL, UR, axis):
         UL = np.ascontiguousarray(UL, dtype=np.float64)

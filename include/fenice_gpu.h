@@ -112,6 +112,12 @@ int fvg_stream(fvg_run* run, void** stream);
 /* Wait for the run's stream. */
 int fvg_synchronize(fvg_run* run);
 
+/* Kernel timing: with `on`, fvg_run_until launches its steps one by one with CUDA events on the run's stream around
+ * every launch of the stage kernel (reconstruction + Riemann + balance + update, or the MUSCL-Hancock kernel) and of the
+ * viscous kernel; fvg_get_timing returns the summed device milliseconds and launch counts since timing was switched on. */
+int fvg_set_timing(fvg_run* run, int on);
+int fvg_get_timing(const fvg_run* run, double* stage_ms, long long* stage_launches, double* viscous_ms, long long* viscous_launches);
+
 /* Face fluxes of n face pairs (UL, UR: n x 5 doubles, axis: n ints) on the device with the run's EOS and Riemann
  * solver (RiemannSolver::face_flux, cpp/src/Schemes.cpp:202-229): F (n x 5) and the wave speeds (n). */
 int fvg_face_flux_batch(fvg_run* run, const double* UL, const double* UR, const int* axis, size_t n, double* F, double* smax);

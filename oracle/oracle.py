@@ -11,10 +11,27 @@ shock_blend, reconstruction, muscl_limiter, weno_epsilon, boundary_order, time_s
 use_viscous, mu, pr) and states as (ncells, 5) float64 arrays in the reference's layout
 [rho, rho u, rho v, rho E, rho w], cell (k*ny + j)*nx + i.
 """
+import contextlib
 import ctypes
 import os
+import sys
 
 import numpy as np
+
+
+@contextlib.contextmanager
+def quiet_stdout():
+    """The reference prints progress lines on its setup; keep them off this process's stdout (fd 1)."""
+    sys.stdout.flush()
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    try:
+        os.dup2(devnull, 1)
+        yield
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
@@ -220,7 +237,8 @@ class Reference:
             lines.append(f"initial_profile={initial_profile}")
         if initial_state is not None:
             lines.append("initial_state=" + ",".join(repr(float(v)) for v in initial_state))
-        h = lib.ref_create("\n".join(lines).encode())
+        with quiet_stdout():
+            h = lib.ref_create("\n".join(lines).encode())
         if not h:
             raise RuntimeError("reference setup failed: " + lib.ref_error().decode())
         self.h = h
