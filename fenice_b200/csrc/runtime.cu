@@ -873,3 +873,132 @@ int fvg_face_flux_batch(fvg_run* run, const double* UL, const double* UR, const 
 }
 
 }   // extern "C"
+
+// ------------------------------------------------------------------------------------------------ residual without allocation
+// fvg_residual_noalloc: the residual of a caller's device state with no device allocation at all, for callers that may
+// not call cudaMalloc (an allocator owned by a host framework, a memory pool with a fixed budget, code that runs while
+// a caller forbids allocation). Its only scratch, the per-CTA wave-speed maxima and a control block, lives in the
+// file-scope array below: a fixed 512 KB + 4 KB that every GPU which loads this library keeps until the process exits.
+namespace {
+
+constexpr int kNoAllocMaxCtas = 65536;   // per-CTA maxima the array holds: the largest grid a call may launch
+constexpr int kNoAllocMaxDevices = 64;
+
+struct NoAllocScratch {
+    Ctl ctl;                               // gate (always = 1), dt = 0, the reduced wave speed
+    double pad[(4096 - sizeof(Ctl)) / sizeof(double)];
+    double blockmax[kNoAllocMaxCtas];
+};
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+struct NoAllocDevice {
+    bool ready = false;
+    NoAllocScratch* ptr = nullptr;         // the device address of g_noalloc_scratch on this device
+};
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+
+__global__ void k_noalloc_begin(NoAllocScratch* s) {
+    s->ctl = Ctl{};
+    s->ctl.always = 1;
+    s->ctl.active = 1;
+}
+
+__global__ void k_noalloc_reduce(NoAllocScratch* s, int nb) {
+    const double v = block_reduce_max(s->blockmax, nb, s->blockmax, 0);
+    if (threadIdx.x == 0) s->ctl.s_stage[0] = v;
+}
+
+// the message of a failed call goes where fvg_create_error() reads it (this thread's last failure)
+int noalloc_fail(int code, const std::string& msg) {
+    g_create_error = msg;
+    return code;
+}
+
+}   // namespace
+
+extern "C" int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long long plane, double* R, double* smax, void* stream) {
+    if (!cfg || !U || !R) return noalloc_fail(FVG_ERR_ARGUMENT, "null argument");
+    const std::string v = validate(*cfg);
+    if (!v.empty()) return noalloc_fail(FVG_ERR_CONFIG, v);
+    if (cfg->use_viscous) return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: viscous runs need a residual-sized scratch array; use fvg_residual");
+    const fvg_config& c = *cfg;
+    const int dim = c.nz > 1 ? 3 : 2;
+    const long long ncells = (long long)c.nx * c.ny * c.nz;
+    if (plane < ncells) return noalloc_fail(FVG_ERR_ARGUMENT, "plane is smaller than the cell count");
+    const int TX = dim == 3 ? Tile<3>::X : Tile<2>::X, TY = dim == 3 ? Tile<3>::Y : Tile<2>::Y, TZ = dim == 3 ? Tile<3>::Z : 1;
+    const long long tiles = (long long)((c.nx + TX - 1) / TX) * ((c.ny + TY - 1) / TY) * ((c.nz + TZ - 1) / TZ);
+    if (tiles > kNoAllocMaxCtas) {
+        char msg[256];
+        std::snprintf(msg, sizeof msg, "fvg_residual_noalloc: the mesh needs %lld tiles, more than the %d its fixed scratch holds "
+                                       "(at most %d tiles of %dx%dx%d cells)", tiles, kNoAllocMaxCtas, kNoAllocMaxCtas, TX, TY, TZ);
+        return noalloc_fail(FVG_ERR_CONFIG, msg);
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return noalloc_fail(FVG_ERR_CUDA, "no current CUDA device");
+    NoAllocDevice& d = g_noalloc_dev[dev];
+    const StageLauncher launcher = dim == 3 ? stage_launcher<3>(c.reconstruction, c.riemann) : stage_launcher<2>(c.reconstruction, c.riemann);
+    if (!d.ready) {
+        // once per device, with that device current: the device address of the scratch array (the host-side name is not one)
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return noalloc_fail(FVG_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        d.ptr = static_cast<NoAllocScratch*>(p);
+        d.ready = true;
+    }
+    if (launcher.prepare() != cudaSuccess) return noalloc_fail(FVG_ERR_CUDA, "kernel set-up failed (shared-memory limit)");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // the mesh description (host values only)
+    Mesh m{};
+    m.nx = c.nx;
+    m.ny = c.ny;
+    m.nz = c.nz;
+    m.ncells = ncells;
+    m.plane = plane;
+    m.dx = c.Lx / c.nx;
+    m.dy = c.Ly / c.ny;
+    m.dz = c.Lz / c.nz;
+    if (dim == 3) {
+        m.area[0] = m.dy * m.dz;
+        m.area[1] = m.dx * m.dz;
+        m.area[2] = m.dx * m.dy;
+        m.inv_cell = 1.0 / (m.dx * m.dy * m.dz);
+    } else {
+        m.area[0] = m.dy;
+        m.area[1] = m.dx;
+        m.inv_cell = 1.0 / (m.dx * m.dy);
+    }
+    StageArgs a{};
+    a.m = m;
+    for (int q = 0; q < 6; ++q) a.bc.type[q] = c.bc[q];
+    halo_kinds(c, c.reconstruction == FVG_RECON_WENO5 ? 3 : 2, a.bc.halo);
+    a.bc.u_in = c.u_in;
+    a.bc.v_in = c.v_in;
+    a.bc.p_out = c.p_out;
+    a.eos.type = c.eos_type;
+    a.eos.gamma = c.gamma;
+    a.eos.p_inf = c.p_inf;
+    a.shock_blend = c.shock_blend;
+    a.weno_eps = c.weno_epsilon;
+    a.limiter = c.limiter;
+    a.mode = kStoreR;
+    a.U = U;
+    a.out = R;
+    a.blockmax = d.ptr->blockmax;
+    a.ctl = &d.ptr->ctl;
+    a.gate = &d.ptr->ctl.always;
+    a.tiles[0] = (c.nx + TX - 1) / TX;
+    a.tiles[1] = (c.ny + TY - 1) / TY;
+    a.tiles[2] = (c.nz + TZ - 1) / TZ;
+    // the control block is written afresh by every call (gate on, dt = 0); each CTA overwrites its own maximum
+    k_noalloc_begin<<<1, 1, 0, s>>>(d.ptr);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = launcher.launch(a, (int)tiles, s);
+    if (e == cudaSuccess) {
+        k_noalloc_reduce<<<1, 1024, 0, s>>>(d.ptr, (int)tiles);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && smax) e = cudaMemcpyAsync(smax, &d.ptr->ctl.s_stage[0], sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return noalloc_fail(FVG_ERR_CUDA, std::string("fvg_residual_noalloc: ") + cudaGetErrorString(e));
+    return FVG_OK;
+}

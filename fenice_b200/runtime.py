@@ -28,7 +28,8 @@ StepResult = namedtuple("StepResult", ["dt", "s_max"])
 EXPORTS = ["fvg_abi_version", "fvg_create", "fvg_destroy", "fvg_last_error", "fvg_create_error", "fvg_upload_state",
            "fvg_download_state", "fvg_residual", "fvg_step", "fvg_run_until", "fvg_get_time", "fvg_set_time",
            "fvg_get_lagged_speed", "fvg_set_lagged_speed", "fvg_dt_length", "fvg_device_state", "fvg_stream",
-           "fvg_synchronize", "fvg_face_flux_batch", "fvg_set_timing", "fvg_get_timing"]
+           "fvg_synchronize", "fvg_face_flux_batch", "fvg_set_timing", "fvg_get_timing",
+           "fvg_residual_noalloc"]
 
 _lib = None
 
@@ -63,6 +64,7 @@ def load_library(path=LIB_PATH):
     lib.fvg_stream.argtypes = [c_p, ctypes.POINTER(c_p)]
     lib.fvg_synchronize.argtypes = [c_p]
     lib.fvg_face_flux_batch.argtypes = [c_p, dp, dp, ctypes.POINTER(ctypes.c_int), ctypes.c_size_t, dp, dp]
+    lib.fvg_residual_noalloc.argtypes = [ctypes.POINTER(P.FvgConfig), c_p, ctypes.c_longlong, c_p, dp, c_p]
     lib.fvg_set_timing.argtypes = [c_p, ctypes.c_int]
     ll = ctypes.POINTER(ctypes.c_longlong)
     lib.fvg_get_timing.argtypes = [c_p, dp, ll, dp, ll]

@@ -122,6 +122,24 @@ int fvg_get_timing(const fvg_run* run, double* stage_ms, long long* stage_launch
  * solver (RiemannSolver::face_flux, cpp/src/Schemes.cpp:202-229): F (n x 5) and the wave speeds (n). */
 int fvg_face_flux_batch(fvg_run* run, const double* UL, const double* UR, const int* axis, size_t n, double* F, double* smax);
 
+/* The residual of a state the caller keeps on the device, computed without allocating any device memory.
+ *
+ * No counterpart in the reference: it exists for callers that must not call cudaMalloc, such as code running inside a
+ * host framework that owns every device allocation (its own caching allocator or a memory pool with a fixed budget),
+ * or code that runs where the caller forbids allocation. Such a caller passes its own device buffers: U and R are nvar
+ * planes of `plane` doubles each (nvar = 4 on a 2-D mesh, 5 on a 3-D mesh, the layout of fvg_device_state), R receives the
+ * residual (Simulation::residual) and *smax (host, may be NULL) its wave speed. The work runs on `stream` (NULL: the
+ * default stream) and the call returns when it is done.
+ *
+ * The only scratch is a fixed array inside the library (about 516 KB per device, kept by every GPU that loads the library
+ * until the process exits): it holds one wave-speed maximum per tile, so a mesh may have at most 65536 tiles (8x8x8 cells
+ * in 3-D, 16x15 in 2-D: e.g. 320^3 or 4096 x 3840 cells); a larger mesh, a viscous run (its viscous residual would need a
+ * mesh-sized scratch array) or the MUSCL-Hancock predictor is rejected with FVG_ERR_CONFIG. The first call on a device
+ * finds the array's device address (with that device current), so make that first call before any stream capture. All
+ * calls share the array and leave their results in it: calls that overlap on the GPU (other threads, other streams) race
+ * and must be serialised by the caller. On failure, fvg_create_error() returns this thread's message. */
+int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long long plane, double* R, double* smax, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
