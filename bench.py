@@ -114,10 +114,10 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(n):
-    """Per-launch DRAM bytes of the stage kernel from the committed ncu summary, scaled to n^3 cells, or None."""
+def ncu_traffic(n, name):
+    """Per-launch DRAM bytes of a stage kernel from its committed ncu summary (profiles/<name>), scaled to n^3 cells, or None."""
     try:
-        with open(os.path.join(ROOT, "profiles", "stage_kernel_weno5_3d.json")) as f:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
             d = json.load(f)
         return d["dram_bytes_per_launch"] * (n ** 3) / d["cells"]
     except (OSError, KeyError, ValueError):
@@ -169,18 +169,16 @@ def barrier(world):
         dist.barrier()
 
 
-def gpu_arm(args, world, rank, local):
+def timed_run(params, U0, precision, args, world, local):
+    """W untimed steps, then K steps timed with CUDA events on the run's stream (and around every stage / viscous
+    launch), the SM clock sampled meanwhile; returns the run, the device milliseconds (max over ranks), the kernel
+    timings and the clock summary."""
     import torch
 
     from fenice_b200 import Run
 
-    n = args.size
-    params = workload(n)
-    U0 = tgv_state(n)
-    run = Run(params, U=U0, device=local)
+    run = Run(params, U=U0, precision=precision, device=local)
     ext = torch.cuda.ExternalStream(run.stream(), device=torch.device("cuda", local))
-    # warm-up (untimed), then K timed steps with CUDA events on the run's stream around the whole region and around
-    # every launch of the stage and viscous kernels
     if args.warmup:
         run.run(1e30, max_steps=args.warmup)
     run.synchronize()
@@ -195,51 +193,86 @@ def gpu_arm(args, world, rank, local):
         run.synchronize()
         torch.cuda.synchronize()
     barrier(world)
-    ms = start.elapsed_time(end)
     tm = run.timing()
     run.set_timing(False)
     assert steps == args.steps, f"{steps} of {args.steps} steps ran"
-    ms = allmax(ms, world)
-    cells = n ** 3
-    value = world * cells * STAGES * args.steps / (ms * 1e-3)
+    return run, allmax(start.elapsed_time(end), world), tm, clk.summary()
 
-    # end to end through the public API: per step the state goes host (pinned) -> device, one step, device -> host
-    e2e = None
-    if args.e2e_steps > 0:
-        host = torch.empty((cells, 5), dtype=torch.float64, pin_memory=True).numpy()
-        host[:] = run.state()
-        barrier(world)
-        t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
-            run.set_state(host)
-            run.step(1e30)
-            host[:] = run.state()
-        wall = time.perf_counter() - t0
-        wall = allmax(wall, world)
-        e2e = {"value": world * cells * STAGES * args.e2e_steps / wall, "unit": UNIT, "h2d_bytes_per_step": cells * 5 * 8,
-               "d2h_bytes_per_step": cells * 5 * 8, "steps": args.e2e_steps, "timing": "host wall clock around upload + step + download"}
 
+def roofline_of(tm, ms, cells, kernel, traffic):
     peak, peak_kind = measured_peak()
     stage_avg_ms = tm["stage_ms"] / max(tm["stage_launches"], 1)
     alg_bytes = cells * BYTES_PER_CELL_STAGE
     achieved = alg_bytes / (stage_avg_ms * 1e-3) / 1e9
-    traffic = ncu_traffic(n)
-    roofline = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": traffic, "peak_source": f"hbm_gbs of MEASURED_PEAKS.json ({peak_kind})",
-                "kernel": "stage_kernel<3, WENO5, LowMach> (fused reconstruction + Riemann + balance + RK update)",
-                "algorithmic_bytes_per_launch": alg_bytes, "stage_launch_ms": round(stage_avg_ms, 4),
-                "viscous_launch_ms": round(tm["viscous_ms"] / max(tm["viscous_launches"], 1), 4),
-                "stage_share_of_step": round(tm["stage_ms"] / ms, 4), "viscous_share_of_step": round(tm["viscous_ms"] / ms, 4)}
-    # my kernels per RK3 step: 3 viscous + 3 stage + dt + axpy + 2 stage maxima + end; one begin per run
-    launches = args.steps * 11 + 1
+    return {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": traffic, "peak_source": f"hbm_gbs of MEASURED_PEAKS.json ({peak_kind})", "kernel": kernel,
+            "algorithmic_bytes_per_launch": alg_bytes, "stage_launch_ms": round(stage_avg_ms, 4),
+            "viscous_launch_ms": round(tm["viscous_ms"] / max(tm["viscous_launches"], 1), 4),
+            "stage_share_of_step": round(tm["stage_ms"] / ms, 4), "viscous_share_of_step": round(tm["viscous_ms"] / ms, 4)}
+
+
+def l1_errors(U, Uref):
+    out = {}
+    for q, name in enumerate(["rho", "rho_u", "rho_v", "rho_E", "rho_w"]):
+        scale = float(np.abs(Uref[:, q]).sum())
+        d = np.abs(U[:, q] - Uref[:, q])
+        out[name] = {"l1_rel": float(d.sum()) / scale if scale else 0.0,
+                     "linf_rel": float(d.max()) / float(np.abs(Uref[:, q]).max()) if scale else 0.0}
+    return out
+
+
+def gpu_arm(args, world, rank, local):
+    import torch
+
+    n = args.size
+    cells = n ** 3
+    params = workload(n)
+    U0 = tgv_state(n)
+    # the plain FP64 form (the reference's arithmetic, bit for bit) and the mixed form (FP32 stencil, FP64 state)
+    plain, ms_p, tm_p, clk_p = timed_run(params, U0, 0, args, world, local)
+    U_plain = plain.state()
+    plain.close()
+    mixed, ms_m, tm_m, clk_m = timed_run(params, U0, 1, args, world, local)
+    errs = l1_errors(mixed.state(), U_plain)
+    del U_plain
+    value = world * cells * STAGES * args.steps / (ms_m * 1e-3)
+    value_p = world * cells * STAGES * args.steps / (ms_p * 1e-3)
+
+    # end to end through the public API (mixed form): per step the state goes host (pinned) -> device, one step, back
+    e2e = None
+    if args.e2e_steps > 0:
+        host = torch.empty((cells, 5), dtype=torch.float64, pin_memory=True).numpy()
+        host[:] = mixed.state()
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            mixed.set_state(host)
+            mixed.step(1e30)
+            host[:] = mixed.state()
+        wall = allmax(time.perf_counter() - t0, world)
+        e2e = {"value": world * cells * STAGES * args.e2e_steps / wall, "unit": UNIT, "h2d_bytes_per_step": cells * 5 * 8,
+               "d2h_bytes_per_step": cells * 5 * 8, "steps": args.e2e_steps, "timing": "host wall clock around upload + step + download"}
+    mixed.close()
+
+    rl_m = roofline_of(tm_m, ms_m, cells, "mixed_stage_kernel<3, WENO5, LowMach> (FP32 reconstruction + Riemann + balance, FP64 RK update)",
+                       ncu_traffic(n, "mixed_stage_kernel_weno5_3d.json"))
+    rl_p = roofline_of(tm_p, ms_p, cells, "stage_kernel<3, WENO5, LowMach> (FP64, the reference's arithmetic)",
+                       ncu_traffic(n, "stage_kernel_weno5_3d.json"))
+    launches = 2 * (args.steps * 11 + 1)   # per RK3 step: 3 viscous + 3 stage + dt + axpy + 2 stage maxima + end; one begin per run
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "ms_per_step": ms_m / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 stencil / f64 state (mixed form); plain form f64",
             "data": "synthetic (Taylor-Green initial state computed in numpy)",
-            "config": {"workload": f"Taylor-Green vortex 3-D {n}^3, WENO5-Z + low-Mach HLLC + SSP-RK3, viscous Re 1600 Pr 0.71, CFL 0.5, "
-                                   f"plain FP64 form", "cells": cells, "stages_per_step": STAGES,
+            "config": {"workload": f"Taylor-Green vortex 3-D {n}^3, WENO5-Z + low-Mach HLLC + SSP-RK3, viscous Re 1600 Pr 0.71, CFL 0.5; "
+                                   "value: the mixed-precision form (no learned sensor yet); plain_fp64: the reference's arithmetic",
+                       "cells": cells, "stages_per_step": STAGES,
                        "parallelism": f"replicas{world}" if world > 1 else "single GPU",
                        "l2": f"inputs larger than L2 ({cells * 40 / 1e6:.0f} MB per state field), no flush"},
-            "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary()}
+            "accuracy": {"vs": f"plain FP64 form after {args.warmup + args.steps} steps from the same state", "fields": errs,
+                         "l1_rho_bar": 1e-4, "l1_rho_within_bar": errs["rho"]["l1_rel"] <= 1e-4},
+            "plain_fp64": {"value": value_p, "ms_per_step": ms_p / args.steps, "roofline": rl_p, "clocks": clk_p,
+                           "speedup_of_mixed": value / value_p},
+            "roofline": rl_m, "e2e": e2e, "gpu_launches": launches, "clocks": clk_m}
     return line
 
 

@@ -17,17 +17,21 @@ SRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfenice_gpu.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["runtime.cu"]
-HEADERS = ["physics.cuh", "grid.cuh", "stage.cuh", "viscous.cuh", "hancock.cuh"]
+SOURCES = ["runtime.cu", "mixed.cu"]
+HEADERS = ["physics.cuh", "grid.cuh", "stage.cuh", "viscous.cuh", "hancock.cuh", "mixed.cuh", "mixed_api.h"]
 
-NVCC_FLAGS = [
+COMMON_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
-    "--fmad=false", "-prec-div=true", "-prec-sqrt=true",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
     "-I" + os.path.join(ROOT, "include"),
-    "--cudart", "static",
 ]
+# per translation unit: the FP64 path keeps every operation IEEE-rounded and uncontracted (the reference's bits); the
+# mixed-precision kernels use fast single-precision math
+UNIT_FLAGS = {
+    "runtime.cu": ["--fmad=false", "-prec-div=true", "-prec-sqrt=true"],
+    "mixed.cu": ["--use_fast_math"],
+}
 
 
 def _stale():
@@ -38,18 +42,28 @@ def _stale():
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(force=False, verbose=False, extra=()):
-    if not force and not _stale():
-        return LIB
-    cmd = [NVCC] + NVCC_FLAGS + list(extra) + ["-shared", "-o", LIB] + [os.path.join(SRC, f) for f in SOURCES]
+def _run(cmd, verbose):
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed building " + LIB)
+        raise RuntimeError("nvcc failed: " + " ".join(cmd))
     if verbose and (r.stdout or r.stderr):
         print(r.stdout + r.stderr)
+
+
+def build(force=False, verbose=False, extra=()):
+    if not force and not _stale():
+        return LIB
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objs = []
+    for f in SOURCES:
+        o = os.path.join(objdir, f.replace(".cu", ".o"))
+        _run([NVCC] + COMMON_FLAGS + UNIT_FLAGS[f] + list(extra) + ["-c", os.path.join(SRC, f), "-o", o], verbose)
+        objs.append(o)
+    _run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "--cudart", "static", "-shared", "-o", LIB] + objs, verbose)
     return LIB
 
 

@@ -1,0 +1,399 @@
+// The mixed-precision form of the stage and viscous kernels: stencil, flux and viscous arithmetic in FP32, the
+// conserved state and its Runge-Kutta accumulation in FP64.
+//
+// What stays FP64: the state in HBM and every stage update (a U0 + b (U + dt R), with R widened to double), and the
+// pressure recovery p = (gamma - 1)(E - 1/2 rho |u|^2) of every cell (cons_to_prim in double when a cell is loaded, so a
+// low-Mach cell, where E and the kinetic energy nearly cancel, loses nothing). What runs in FP32 (compiled with fast
+// single-precision division and square root, and contraction into FMAs): the WENO-Z / MUSCL reconstruction of the
+// primitives, the Riemann solver, the flux balance, the viscous stresses and heat flux.
+//
+// One algorithmic difference from the plain form: the Riemann solver takes the reconstructed primitive states directly
+// (their density and pressure floored as cons_to_prim floors them) instead of converting them to conservative form and
+// back, which in FP32 would recover the face pressure from a difference of nearly equal numbers. In exact arithmetic the
+// two are the same; the tests state the L1 / Linf distance of this form from the FP64 oracle per field and per case.
+#pragma once
+
+#include "grid.cuh"
+#include "stage.cuh"
+#include "viscous.cuh"
+
+namespace fvg {
+
+// HLLC / low-Mach HLLC of a face from its two primitive states (the Riemann solver of the mixed form)
+template <int RIEMANN, int NV>
+__device__ __forceinline__ float face_flux_prim(const Eos<float>& e, float shock_blend, St<float, NV> WL, St<float, NV> WR, int axis, St<float, NV>& F) {
+    WL[0] = vmax(WL[0], Num<float>::eos_eps);
+    WL[3] = vmax(WL[3], Num<float>::eos_eps);
+    WR[0] = vmax(WR[0], Num<float>::eos_eps);
+    WR[3] = vmax(WR[3], Num<float>::eos_eps);
+    const float inv_L = 1.0f / WL[0], inv_R = 1.0f / WR[0];
+    const float c_L = sound_speed_inv(e, WL[3], inv_L), c_R = sound_speed_inv(e, WR[3], inv_R);
+    if constexpr (RIEMANN == kLowMach) {
+        float mL2 = WL[1] * WL[1] + WL[2] * WL[2], mR2 = WR[1] * WR[1] + WR[2] * WR[2];
+        if constexpr (NV == 5) {
+            mL2 += WL[4] * WL[4];
+            mR2 += WR[4] * WR[4];
+        }
+        const float M_L = sqrtf(mL2) / (c_L + Num<float>::mach_eps);
+        const float M_R = sqrtf(mR2) / (c_R + Num<float>::mach_eps);
+        const float z = vmin(vmax(vmax(M_L, M_R), 1e-4f), 1.0f);
+#pragma unroll
+        for (int a = 0; a < (NV == 5 ? 3 : 2); ++a) {
+            const int m = a == 0 ? 1 : (a == 1 ? 2 : 4);
+            const float avg = 0.5f * (WL[m] + WR[m]);
+            const float half = 0.5f * (WL[m] - WR[m]);
+            WL[m] = avg + z * half;
+            WR[m] = avg - z * half;
+        }
+    }
+    return hllc_core(WL, WR, p2c(e, WL), p2c(e, WR), inv_L, inv_R, c_L, c_R, axis, shock_blend, F);
+}
+
+template <int DIM, int RECON, int TX, int TY, int TZ> struct MixedShape {
+    static constexpr int NV = DIM == 3 ? 5 : 4;
+    static constexpr int H = RECON == kWeno5 ? 3 : 2;
+    static constexpr int NC = TX * TY * TZ;
+    static constexpr int T3[3] = {TX, TY, TZ};
+    static constexpr int ext(int a) { return (T3[0] + (a == 0 ? 2 * H : 0)) * (T3[1] + (a == 1 ? 2 * H : 0)) * (T3[2] + (a == 2 ? 2 * H : 0)); }
+    static constexpr int nf(int a) { return (T3[0] + (a == 0)) * (T3[1] + (a == 1)) * (T3[2] + (a == 2)); }
+    static constexpr int cmax(int a, int b) { return a > b ? a : b; }
+    static constexpr int EXT = cmax(cmax(ext(0), ext(1)), DIM == 3 ? ext(2) : 0);
+    static constexpr int NF = cmax(cmax(nf(0), nf(1)), DIM == 3 ? nf(2) : 0);
+    // floats: P [NV][EXT], WL / WR [NV][NF] (the fluxes overwrite WL), acc [NV][NC], 64 for the reduction
+    static constexpr int SMEM_FLOATS = NV * EXT + 2 * NV * NF + NV * NC + 64;
+    static constexpr size_t SMEM_BYTES = sizeof(float) * SMEM_FLOATS;
+};
+
+// One axis of the tile sweep of mixed_stage_kernel (compile-time extents).
+template <int AXIS, int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT>
+__device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>& ef, float sb, float weps, float* __restrict__ P,
+                                           float* __restrict__ WL, float* __restrict__ WR, float* __restrict__ acc, const int o3[3], float& smax) {
+    using S = MixedShape<DIM, RECON, TX, TY, TZ>;
+    constexpr int NV = S::NV, H = S::H, NC = S::NC;
+    constexpr int axis = AXIS;
+    const Mesh& m = a.m;
+    const int tid = threadIdx.x;
+    const int n3[3] = {m.nx, m.ny, m.nz};
+    {
+        constexpr int E[3] = {TX + (AXIS == 0 ? 2 * H : 0), TY + (AXIS == 1 ? 2 * H : 0), TZ + (AXIS == 2 ? 2 * H : 0)};
+        constexpr int Fd[3] = {TX + (AXIS == 0), TY + (AXIS == 1), TZ + (AXIS == 2)};
+        constexpr int nE = E[0] * E[1] * E[2], nF = Fd[0] * Fd[1] * Fd[2];
+        // ---- 1. load: the primitive state recovered in FP64, stored as FP32
+        for (int e = tid; e < nE; e += NT) {
+            int l3[3] = {e % E[0], (e / E[0]) % E[1], e / (E[0] * E[1])};
+            l3[axis] -= H;
+            const St<double, NV> w = c2p(a.eos, stencil_cons<DIM, NV>(m, a.bc, a.eos, a.U, o3[0] + l3[0], o3[1] + l3[1], o3[2] + l3[2]));
+#pragma unroll
+            for (int q = 0; q < NV; ++q) P[q * S::EXT + e] = (float)w[q];
+        }
+        __syncthreads();
+        const int sstride = axis == 0 ? 1 : (axis == 1 ? E[0] : E[0] * E[1]);
+        // ---- 2. face values
+        for (int it = tid; it < nF * NV; it += NT) {
+            const int f = it % nF, q = it / nF;
+            const int f3[3] = {f % Fd[0], (f / Fd[0]) % Fd[1], f / (Fd[0] * Fd[1])};
+            const float* c = P + q * S::EXT + (f3[2] * E[1] + f3[1]) * E[0] + f3[0];
+            float wl, wr;
+            if constexpr (RECON == kMuscl) {
+                const float c0 = c[0], c1 = c[sstride], c2 = c[2 * sstride], c3 = c[3 * sstride];
+                const float bb = c2 - c1;
+                wl = c1 + 0.5f * limiter(a.limiter, c1 - c0, bb);
+                wr = c2 - 0.5f * limiter(a.limiter, c3 - c2, bb);
+            } else if constexpr (RECON == kWeno3) {
+                wl = weno3z(c[0], c[sstride], c[2 * sstride], weps);
+                wr = weno3z(c[3 * sstride], c[2 * sstride], c[sstride], weps);
+            } else {
+                const float c0 = c[0], c1 = c[sstride], c2 = c[2 * sstride], c3 = c[3 * sstride], c4 = c[4 * sstride], c5 = c[5 * sstride];
+                wl = weno5z(c0, c1, c2, c3, c4, weps);
+                wr = weno5z(c5, c4, c3, c2, c1, weps);
+            }
+            WL[q * S::NF + f] = wl;
+            WR[q * S::NF + f] = wr;
+        }
+        __syncthreads();
+        // ---- 3. fluxes
+        const int na = n3[axis], lo_side = 2 * axis, hi_side = 2 * axis + 1;
+        for (int f = tid; f < nF; f += NT) {
+            const int f3[3] = {f % Fd[0], (f / Fd[0]) % Fd[1], f / (Fd[0] * Fd[1])};
+            const int g3[3] = {o3[0] + f3[0], o3[1] + f3[1], o3[2] + f3[2]};
+            bool inside = true;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) inside = inside && (d == axis ? g3[d] <= n3[d] : g3[d] < n3[d]);
+            St<float, NV> F;
+#pragma unroll
+            for (int q = 0; q < NV; ++q) F[q] = 0.0f;
+            if (inside) {
+                const int t = g3[axis];
+                const bool lo_face = t == 0 && a.bc.halo[lo_side] == kHaloNone;
+                const bool hi_face = t == na && a.bc.halo[hi_side] == kHaloNone;
+                St<float, NV> wl, wr;
+                if (lo_face || hi_face) {
+                    int c3[3] = {g3[0], g3[1], g3[2]};
+                    if (hi_face) c3[axis] = na - 1;
+                    St<double, NV> UL, UR;
+                    side_states<NV>(m, a.bc, a.eos, a.U, lo_face ? lo_side : hi_side, c3[0], c3[1], c3[2], UL, UR);
+                    const St<double, NV> dl = c2p(a.eos, UL), dr = c2p(a.eos, UR);
+#pragma unroll
+                    for (int q = 0; q < NV; ++q) {
+                        wl[q] = (float)dl[q];
+                        wr[q] = (float)dr[q];
+                    }
+                } else {
+#pragma unroll
+                    for (int q = 0; q < NV; ++q) {
+                        wl[q] = WL[q * S::NF + f];
+                        wr[q] = WR[q * S::NF + f];
+                    }
+                }
+                const float s = face_flux_prim<RIEMANN>(ef, sb, wl, wr, axis, F);
+                if (s > smax) smax = s;
+            }
+#pragma unroll
+            for (int q = 0; q < NV; ++q) WL[q * S::NF + f] = F[q];
+        }
+        __syncthreads();
+        // ---- 4. balance of this axis
+        const float A = (float)m.area[axis];
+        for (int c = tid; c < NC; c += NT) {
+            const int c3[3] = {c % TX, (c / TX) % TY, c / (TX * TY)};
+            const int fl = (c3[2] * Fd[1] + c3[1]) * Fd[0] + c3[0];
+            const int fr = fl + (axis == 0 ? 1 : (axis == 1 ? Fd[0] : Fd[0] * Fd[1]));
+#pragma unroll
+            for (int q = 0; q < NV; ++q) {
+                const float d = (WL[q * S::NF + fr] - WL[q * S::NF + fl]) * A;
+                acc[q * NC + c] = axis == 0 ? -d : acc[q * NC + c] - d;
+            }
+        }
+        __syncthreads();
+        }
+}
+
+// The mixed-precision stage kernel: the tile sweep of stage_kernel (same phases, same launch geometry) with FP32 stencil
+// arithmetic; see the file comment for what stays FP64.
+template <int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT>
+__global__ void __launch_bounds__(NT) mixed_stage_kernel(const StageArgs a) {
+    using S = MixedShape<DIM, RECON, TX, TY, TZ>;
+    constexpr int NV = S::NV, H = S::H, NC = S::NC;
+    extern __shared__ double smem_d[];
+    double* red = smem_d;                                      // [32]
+    float* P = reinterpret_cast<float*>(smem_d + 32);         // [NV][EXT]
+    float* WL = P + NV * S::EXT;                               // [NV][NF]
+    float* WR = WL + NV * S::NF;                               // [NV][NF]
+    float* acc = WR + NV * S::NF;                              // [NV][NC]
+    if (!*a.gate) return;
+    const Mesh& m = a.m;
+    const Eos<float> ef{a.eos.type, (float)a.eos.gamma, (float)a.eos.p_inf};
+    const float sb = (float)a.shock_blend, weps = (float)a.weno_eps;
+    const int tid = threadIdx.x, b = blockIdx.x;
+    const int o3[3] = {(b % a.tiles[0]) * TX, ((b / a.tiles[0]) % a.tiles[1]) * TY, (b / (a.tiles[0] * a.tiles[1])) * TZ};
+    const int n3[3] = {m.nx, m.ny, m.nz};
+    float smax = 0.0f;
+
+    mixed_axis<0, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, ef, sb, weps, P, WL, WR, acc, o3, smax);
+    mixed_axis<1, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, ef, sb, weps, P, WL, WR, acc, o3, smax);
+    if constexpr (DIM == 3) mixed_axis<2, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, ef, sb, weps, P, WL, WR, acc, o3, smax);
+    // ---- epilogue: the residual widened to FP64 and the FP64 stage update
+    const double dt = a.ctl->dt;
+    for (int c = tid; c < NC; c += NT) {
+        const int c3[3] = {c % TX, (c / TX) % TY, c / (TX * TY)};
+        const int g3[3] = {o3[0] + c3[0], o3[1] + c3[1], o3[2] + c3[2]};
+        if (g3[0] >= m.nx || g3[1] >= m.ny || g3[2] >= m.nz) continue;
+        const long long cell = ((long long)g3[2] * m.ny + g3[1]) * m.nx + g3[0];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            double r = (double)acc[q * NC + c] * m.inv_cell;
+            if (a.Rv) r = r + a.Rv[q * m.plane + cell];
+            const long long e = q * m.plane + cell;
+            double o;
+            if (a.mode == kStoreR)
+                o = r;
+            else if (a.mode == kAxpy)
+                o = a.U[e] + dt * r;
+            else
+                o = a.ca * a.U0[e] + a.cb * (a.U[e] + dt * r);
+            a.out[e] = o;
+        }
+    }
+    const double bm = block_max<NT>((double)smax, red);
+    if (tid == 0) a.blockmax[b] = bm;
+}
+
+template <int TX, int TY, int TZ> struct MixedViscShape {
+    static constexpr int NC = TX * TY * TZ;
+    static constexpr int BX = TX + 2, BY = TY + 2, BZ = TZ + 2, NB = BX * BY * BZ;
+    static constexpr int cmax(int x, int y) { return x > y ? x : y; }
+    static constexpr int NE = cmax(cmax((TX + 2) * TY * TZ, TX * (TY + 2) * TZ), TX * TY * (TZ + 2));
+    static constexpr int NF = cmax(cmax((TX + 1) * TY * TZ, TX * (TY + 1) * TZ), TX * TY * (TZ + 1));
+    // red [32 doubles], floats: B [5][NB] conservative box, Wb [4][NB] (u, v, w, T), G [4][NE], F [4][NF], acc [5][NC]
+    static constexpr int SMEM_FLOATS = 64 + 9 * NB + 4 * NE + 4 * NF + 5 * NC;
+    static constexpr size_t SMEM_BYTES = sizeof(float) * SMEM_FLOATS;
+};
+
+// The mixed-precision viscous kernel: viscous_kernel's phases in FP32; the padded state is read in FP64 and each box
+// position's velocity and T = p / rho come from an FP64 pressure recovery.
+template <int TX, int TY, int TZ, int NT>
+__global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
+    using S = MixedViscShape<TX, TY, TZ>;
+    constexpr int NC = S::NC, BX = S::BX, BY = S::BY, NB = S::NB;
+    extern __shared__ double smem_d[];
+    double* red = smem_d;
+    float* B = reinterpret_cast<float*>(smem_d + 32);   // [5][NB]
+    float* Wb = B + 5 * NB;                              // [4][NB]: u, v, w, T
+    float* G = Wb + 4 * NB;                              // [4][NE]
+    float* Fv = G + 4 * S::NE;                           // [4][NF]
+    float* acc = Fv + 4 * S::NF;                         // [5][NC]
+    if (!*a.gate) return;
+    const Mesh& m = a.m;
+    const int tid = threadIdx.x, b = blockIdx.x;
+    const int o3[3] = {(b % a.tiles[0]) * TX, ((b / a.tiles[0]) % a.tiles[1]) * TY, (b / (a.tiles[0] * a.tiles[1])) * TZ};
+    const int n3[3] = {m.nx, m.ny, m.nz};
+    const float h[3] = {(float)m.dx, (float)m.dy, (float)m.dz};
+    const float mu = (float)a.mu, kc = (float)a.k_cond;
+    const int* mom = kViscMom;
+    const auto& GA = kViscGA;
+    const auto& GB = kViscGB;
+    auto bidx = [&](int i, int j, int k) { return ((k + 1) * BY + (j + 1)) * BX + (i + 1); };
+
+    for (int e = tid; e < NB; e += NT) {
+        int g[3] = {o3[0] + e % BX - 1, o3[1] + (e / BX) % BY - 1, o3[2] + e / (BX * BY) - 1};
+#pragma unroll
+        for (int x = 0; x < 3; ++x)
+            if (a.periodic[x] && (g[x] < 0 || g[x] >= n3[x])) g[x] = ((g[x] % n3[x]) + n3[x]) % n3[x];
+#pragma unroll
+        for (int x = 0; x < 3; ++x) g[x] = g[x] < -1 ? -1 : (g[x] > n3[x] ? n3[x] : g[x]);
+        const St<double, 5> u = padded_cons(a, g[0], g[1], g[2]);
+        const St<double, 5> w = c2p(a.eos, u);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) B[q * NB + e] = (float)u[q];
+        Wb[0 * NB + e] = (float)w[1];
+        Wb[1 * NB + e] = (float)w[2];
+        Wb[2 * NB + e] = (float)w[4];
+        Wb[3 * NB + e] = (float)(w[3] / w[0]);
+    }
+    __syncthreads();
+
+#pragma unroll 1
+    for (int d = 0; d < 3; ++d) {
+        int E[3] = {TX, TY, TZ}, Fd[3] = {TX, TY, TZ};
+        E[d] += 2;
+        Fd[d] += 1;
+        const int nE = E[0] * E[1] * E[2], nF = Fd[0] * Fd[1] * Fd[2];
+        for (int e = tid; e < nE; e += NT) {
+            int l[3] = {e % E[0], (e / E[0]) % E[1], e / (E[0] * E[1])};
+            l[d] -= 1;
+            const int p = bidx(l[0], l[1], l[2]);
+            const float inv_rho = 1.0f / vmax(B[p], Num<float>::eos_eps);
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const int ga = GA[d][s], gb = GB[d][s];
+                const int off = gb == 0 ? 1 : (gb == 1 ? BX : BX * BY);
+                const float inv2h = 0.5f / h[gb];
+                const float gq = (B[mom[ga] * NB + p + off] - B[mom[ga] * NB + p - off]) * inv2h;
+                const float g0 = (B[p + off] - B[p - off]) * inv2h;
+                G[s * S::NE + e] = (gq - Wb[ga * NB + p] * g0) * inv_rho;
+            }
+        }
+        __syncthreads();
+        const float area = (float)m.area[d];
+        const float inv_h = 1.0f / h[d];
+        const int estride = d == 0 ? 1 : (d == 1 ? E[0] : E[0] * E[1]);
+        const int bstride = d == 0 ? 1 : (d == 1 ? BX : BX * BY);
+        for (int f = tid; f < nF; f += NT) {
+            const int f3[3] = {f % Fd[0], (f / Fd[0]) % Fd[1], f / (Fd[0] * Fd[1])};
+            const int g3[3] = {o3[0] + f3[0], o3[1] + f3[1], o3[2] + f3[2]};
+            const int t = g3[d];
+            bool inside = true;
+#pragma unroll
+            for (int x = 0; x < 3; ++x) inside = inside && (x == d ? g3[x] <= n3[x] : g3[x] < n3[x]);
+            float out[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            if (inside) {
+                const bool lo = t == 0, hi = t == n3[d];
+                const int eL = (f3[2] * E[1] + f3[1]) * E[0] + f3[0];
+                const int eR = eL + estride;
+                int lc[3] = {f3[0], f3[1], f3[2]};
+                lc[d] -= 1;
+                const int pL = bidx(lc[0], lc[1], lc[2]), pR = pL + bstride;
+                const int xL = (lo && !a.periodic[d]) ? eR : eL;
+                const int xR = (hi && !a.periodic[d]) ? eL : eR;
+                const bool phys = a.bface2 && !a.periodic[d] && (lo || hi);
+                float Gc[4];
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    if (phys) {
+                        const int ga = GA[d][s], gb = GB[d][s];
+                        const int pg = lo ? pL : pR, pc = lo ? pR : pL;
+                        const int off = gb == 0 ? 1 : (gb == 1 ? BX : BX * BY);
+                        const float fp = 0.5f * (Wb[ga * NB + pg + off] + Wb[ga * NB + pc + off]);
+                        const float fm = 0.5f * (Wb[ga * NB + pg - off] + Wb[ga * NB + pc - off]);
+                        Gc[s] = (fp - fm) * (0.5f / h[gb]);
+                    } else {
+                        Gc[s] = 0.5f * (G[s * S::NE + xL] + G[s * S::NE + xR]);
+                    }
+                }
+                float Gn[3], vf[3];
+#pragma unroll
+                for (int x = 0; x < 3; ++x) {
+                    const float vl = Wb[x * NB + pL], vr = Wb[x * NB + pR];
+                    Gn[x] = (vr - vl) * inv_h;
+                    vf[x] = 0.5f * (vl + vr);
+                }
+                const float dT = (Wb[3 * NB + pR] - Wb[3 * NB + pL]) * inv_h;
+                float tau[3];
+                if (d == 0) {
+                    tau[0] = mu * ((4.0f / 3.0f) * Gn[0] - (2.0f / 3.0f) * (Gc[1] + Gc[2]));
+                    tau[1] = mu * (Gn[1] + Gc[0]);
+                    tau[2] = mu * (Gn[2] + Gc[3]);
+                } else if (d == 1) {
+                    tau[0] = mu * (Gn[0] + Gc[1]);
+                    tau[1] = mu * ((4.0f / 3.0f) * Gn[1] - (2.0f / 3.0f) * (Gc[0] + Gc[2]));
+                    tau[2] = mu * (Gn[2] + Gc[3]);
+                } else {
+                    tau[0] = mu * (Gn[0] + Gc[2]);
+                    tau[1] = mu * (Gn[1] + Gc[3]);
+                    tau[2] = mu * ((4.0f / 3.0f) * Gn[2] - (2.0f / 3.0f) * (Gc[0] + Gc[1]));
+                }
+                out[0] = tau[0] * area;
+                out[1] = tau[1] * area;
+                out[2] = (vf[0] * tau[0] + vf[1] * tau[1] + vf[2] * tau[2] + kc * dT) * area;
+                out[3] = tau[2] * area;
+            }
+#pragma unroll
+            for (int x = 0; x < 4; ++x) Fv[x * S::NF + f] = out[x];
+        }
+        __syncthreads();
+        for (int c = tid; c < NC; c += NT) {
+            const int c3[3] = {c % TX, (c / TX) % TY, c / (TX * TY)};
+            const int fl = (c3[2] * Fd[1] + c3[1]) * Fd[0] + c3[0];
+            const int fr = fl + (d == 0 ? 1 : (d == 1 ? Fd[0] : Fd[0] * Fd[1]));
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                const float dif = q == 0 ? 0.0f : Fv[(q - 1) * S::NF + fr] - Fv[(q - 1) * S::NF + fl];
+                acc[q * NC + c] = d == 0 ? dif : acc[q * NC + c] + dif;
+            }
+        }
+        __syncthreads();
+    }
+    double smax = 0.0;
+    const float gm1 = (float)(a.eos.gamma - 1.0);
+    for (int c = tid; c < NC; c += NT) {
+        const int c3[3] = {c % TX, (c / TX) % TY, c / (TX * TY)};
+        const int g3[3] = {o3[0] + c3[0], o3[1] + c3[1], o3[2] + c3[2]};
+        if (g3[0] >= m.nx || g3[1] >= m.ny || g3[2] >= m.nz) continue;
+        const long long cell = ((long long)g3[2] * m.ny + g3[1]) * m.nx + g3[0];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) a.Rv[q * m.plane + cell] = (double)acc[q * NC + c] * m.inv_cell;
+        const int p = bidx(c3[0], c3[1], c3[2]);
+        const float rho = vmax(B[p], Num<float>::eos_eps);
+        const float T = Wb[3 * NB + p];
+        const float nu_eff = vmax((4.0f / 3.0f) * (mu / rho), (kc * gm1) / rho) + 1e-12f;
+        const float vm = vmax(vmax(fabsf(Wb[p]), fabsf(Wb[NB + p])), fabsf(Wb[2 * NB + p]));
+        // sound speed from T = p / rho: c = sqrt(gamma (p + p_inf) / rho)
+        const float cs = sqrtf((float)a.eos.gamma * (T + (float)a.eos.p_inf / rho));
+        const double s = (double)(vm + cs + 2.0f * (float)a.L * (float)a.inv_h2 * nu_eff);
+        if (s > smax) smax = s;
+    }
+    const double bm = block_max<NT>(smax, red);
+    if (tid == 0) a.blockmax[b] = bm;
+}
+
+}   // namespace fvg

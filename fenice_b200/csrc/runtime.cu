@@ -18,6 +18,7 @@
 // step runs (t < t_end, step limit, no error).
 #include "../../include/fenice_gpu.h"
 #include "hancock.cuh"
+#include "mixed_api.h"
 #include "stage.cuh"
 #include "viscous.cuh"
 
@@ -278,7 +279,9 @@ std::string validate(const fvg_config& c) {
     if (c.limiter < 0 || c.limiter > 3) return "unknown muscl_limiter";
     if (c.time_scheme < 0 || c.time_scheme > 3) return "unknown time_scheme";
     if (c.boundary_order != 1 && c.boundary_order != 2) return "boundary_order must be 1 or 2";
-    if (c.precision != FVG_PREC_FP64) return "precision: only FVG_PREC_FP64 is built into this library";
+    if (c.precision != FVG_PREC_FP64 && c.precision != FVG_PREC_MIXED) return "unknown precision";
+    if (c.precision == FVG_PREC_MIXED && c.reconstruction == FVG_RECON_NONE) return "the mixed-precision form needs a reconstruction (muscl, weno3, weno5)";
+    if (c.precision == FVG_PREC_MIXED && c.time_scheme == FVG_TS_HANCOCK) return "the mixed-precision form runs the Runge-Kutta schemes (MUSCL-Hancock is FP64 only)";
     const int naxes = c.nz > 1 ? 3 : 2;
     for (int s = 0; s < 2 * naxes; ++s) {
         if (c.bc[s] < 0 || c.bc[s] > FVG_BC_NONREFLECTING) return "unknown boundary type";
@@ -409,7 +412,8 @@ cudaError_t residual_stage(fvg_run* r, const double* Uin, const double* U0, doub
     cudaError_t e;
     if (r->cfg.use_viscous) {
         timer_mark(r, r->t_visc);
-        e = launch_viscous(visc_args(r, Uin, r->bmv[stage], gate), r->nbv, r->stream);
+        e = r->cfg.precision == FVG_PREC_MIXED ? mixed_viscous_launch(visc_args(r, Uin, r->bmv[stage], gate), r->nbv, r->stream)
+                                               : launch_viscous(visc_args(r, Uin, r->bmv[stage], gate), r->nbv, r->stream);
         timer_mark(r, r->t_visc);
         if (e != cudaSuccess) return e;
     }
@@ -553,6 +557,15 @@ int fvg_create(const fvg_config* cfg, fvg_run** out) {
     run->ntiles_h[2] = 1;
     run->nbh = run->ntiles_h[0] * run->ntiles_h[1];
     run->stage = run->dim == 3 ? stage_launcher<3>(c.reconstruction, c.riemann) : stage_launcher<2>(c.reconstruction, c.riemann);
+    if (c.precision == FVG_PREC_MIXED) {
+        const MixedStage ms = mixed_stage(run->dim, c.reconstruction, c.riemann);
+        run->stage.prepare = ms.prepare;
+        run->stage.launch = ms.launch;
+        if (c.use_viscous && mixed_viscous_prepare() != cudaSuccess) {
+            run->err = "kernel set-up failed (shared-memory limit)";
+            return bail(FVG_ERR_CUDA);
+        }
+    }
     // the seed residual of MUSCL-Hancock and every residual use the stage kernel; the viscous and predictor kernels as needed
     if (run->stage.prepare() != cudaSuccess || (c.use_viscous && prepare_viscous() != cudaSuccess) ||
         (run->dim == 2 && c.reconstruction == FVG_RECON_MUSCL &&
@@ -920,6 +933,7 @@ extern "C" int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long
     if (!cfg || !U || !R) return noalloc_fail(FVG_ERR_ARGUMENT, "null argument");
     const std::string v = validate(*cfg);
     if (!v.empty()) return noalloc_fail(FVG_ERR_CONFIG, v);
+    if (cfg->precision != FVG_PREC_FP64) return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: the FP64 form only");
     if (cfg->use_viscous) return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: viscous runs need a residual-sized scratch array; use fvg_residual");
     const fvg_config& c = *cfg;
     const int dim = c.nz > 1 ? 3 : 2;

@@ -60,33 +60,22 @@ template <int DIM, int RECON, int TX, int TY, int TZ> struct StageShape {
     static constexpr size_t SMEM_BYTES = sizeof(double) * SMEM_DOUBLES;
 };
 
-template <int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT>
-__global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
+// One axis of the tile sweep of stage_kernel (the axis a template parameter, so the extents of the extended tile and of
+// the face grid are compile-time constants).
+template <int AXIS, int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT>
+__device__ __forceinline__ void stage_axis(const StageArgs& a, double* __restrict__ P, double* __restrict__ WL, double* __restrict__ WR,
+                                           double* __restrict__ acc, const int o3[3], double& smax) {
     using S = StageShape<DIM, RECON, TX, TY, TZ>;
     constexpr int NV = S::NV, H = S::H, NC = S::NC;
-    extern __shared__ double smem[];
-    double* P = smem;                       // [NV][EXT]
-    double* WL = P + S::P_SIZE;             // [NV][NF]
-    double* WR = WL + NV * S::NF;           // [NV][NF]
-    double* acc = WR + NV * S::NF;          // [NV][NC]
-    double* red = acc + NV * NC;            // [32]
-    if (!*a.gate) return;
-
+    constexpr int axis = AXIS;
     const Mesh& m = a.m;
     const int tid = threadIdx.x;
-    const int b = blockIdx.x;
-    const int t0 = b % a.tiles[0], t1 = (b / a.tiles[0]) % a.tiles[1], t2 = b / (a.tiles[0] * a.tiles[1]);
-    const int o3[3] = {t0 * TX, t1 * TY, t2 * TZ};
     const int n3[3] = {m.nx, m.ny, m.nz};
-    double smax = 0.0;
-
-#pragma unroll 1
-    for (int axis = 0; axis < DIM; ++axis) {
+    {
         // extents of the extended tile and of the face grid of this axis (x fastest)
-        int E[3] = {TX, TY, TZ}, Fd[3] = {TX, TY, TZ};
-        E[axis] += 2 * H;
-        Fd[axis] += 1;
-        const int nE = E[0] * E[1] * E[2], nF = Fd[0] * Fd[1] * Fd[2];
+        constexpr int E[3] = {TX + (AXIS == 0 ? 2 * H : 0), TY + (AXIS == 1 ? 2 * H : 0), TZ + (AXIS == 2 ? 2 * H : 0)};
+        constexpr int Fd[3] = {TX + (AXIS == 0), TY + (AXIS == 1), TZ + (AXIS == 2)};
+        constexpr int nE = E[0] * E[1] * E[2], nF = Fd[0] * Fd[1] * Fd[2];
         // ---- 1. load (primitive; first order keeps the conservative state)
         for (int e = tid; e < nE; e += NT) {
             int l3[3] = {e % E[0], (e / E[0]) % E[1], e / (E[0] * E[1])};
@@ -195,7 +184,32 @@ __global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
             }
         }
         __syncthreads();
-    }
+        }
+}
+
+template <int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT>
+__global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
+    using S = StageShape<DIM, RECON, TX, TY, TZ>;
+    constexpr int NV = S::NV, H = S::H, NC = S::NC;
+    extern __shared__ double smem[];
+    double* P = smem;                       // [NV][EXT]
+    double* WL = P + S::P_SIZE;             // [NV][NF]
+    double* WR = WL + NV * S::NF;           // [NV][NF]
+    double* acc = WR + NV * S::NF;          // [NV][NC]
+    double* red = acc + NV * NC;            // [32]
+    if (!*a.gate) return;
+
+    const Mesh& m = a.m;
+    const int tid = threadIdx.x;
+    const int b = blockIdx.x;
+    const int t0 = b % a.tiles[0], t1 = (b / a.tiles[0]) % a.tiles[1], t2 = b / (a.tiles[0] * a.tiles[1]);
+    const int o3[3] = {t0 * TX, t1 * TY, t2 * TZ};
+    const int n3[3] = {m.nx, m.ny, m.nz};
+    double smax = 0.0;
+
+    stage_axis<0, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, P, WL, WR, acc, o3, smax);
+    stage_axis<1, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, P, WL, WR, acc, o3, smax);
+    if constexpr (DIM == 3) stage_axis<2, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, P, WL, WR, acc, o3, smax);
     // ---- epilogue: the residual and the stage update
     const double dt = a.ctl->dt;
     for (int c = tid; c < NC; c += NT) {

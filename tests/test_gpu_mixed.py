@@ -1,0 +1,71 @@
+"""The mixed-precision form (FP32 stencil, flux and viscous arithmetic; FP64 state accumulation and pressure recovery)
+against the plain FP64 form, which the other tests pin bit for bit to the reference. The bar is the north-star one: L1
+density error <= 1e-4 relative to the FP64 result; every field's relative L1 and Linf distances are printed per case."""
+import math
+
+import numpy as np
+import pytest
+
+import cases
+from fenice_b200 import Run
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_errors(U, Uref):
+    names = ["rho", "rho u", "rho v", "rho E", "rho w"]
+    out = {}
+    for q in range(5):
+        scale = np.abs(Uref[:, q]).sum()
+        if scale == 0:
+            continue
+        d = np.abs(U[:, q] - Uref[:, q])
+        out[names[q]] = (d.sum() / scale, d.max() / np.abs(Uref[:, q]).max())
+    return out
+
+
+def quadrants(n, seed):
+    rng = np.random.default_rng(seed)
+    st = [(rng.uniform(0.1, 2), rng.uniform(-1, 1), rng.uniform(-1, 1), rng.uniform(0.1, 2)) for _ in range(4)]
+    c = (np.arange(n) + 0.5) / n
+    y, x = np.meshgrid(c, c, indexing="ij")
+    x, y = x.ravel(), y.ravel()
+    q = np.where(x >= 0.5, np.where(y >= 0.5, 0, 3), np.where(y >= 0.5, 1, 2))
+    W = np.zeros((n * n, 5))
+    for k, (r, u, v, p) in enumerate(st):
+        W[q == k] = (r, u, v, p, 0.0)
+    return cases.prim_to_cons(W)
+
+
+def tgv(n):
+    import bench
+
+    return bench.tgv_state(n)
+
+
+L2PI = 2 * math.pi
+CASES = [
+    ("tgv3d_weno5_lowmach_rk3_viscous", dict(nx=48, ny=48, nz=48, Lx=L2PI, Ly=L2PI, Lz=L2PI, use_viscous=True, mu=6.25e-4, pr=0.71,
+                                              reconstruction="weno5", riemann_solver="lowmach", time_scheme="SSP Runge-Kutta 3", cfl=0.5,
+                                              **cases.bcs("periodic", "periodic", "periodic", "periodic")), lambda: tgv(48), 1e30, 20),
+    ("riemann2d_weno5_hllc_rk3", dict(nx=128, ny=128, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", cfl=0.4,
+                                      **cases.bcs("transmissive", "transmissive", "transmissive", "transmissive")), lambda: quadrants(128, 7), 0.1, 0),
+    ("vortex2d_muscl_mc_rk2", dict(nx=96, ny=96, Lx=10.0, Ly=10.0, reconstruction="muscl", muscl_limiter="MC", time_scheme="SSP Runge-Kutta 2",
+                                   **cases.bcs("periodic", "periodic", "periodic", "periodic")), lambda: cases.smooth_field(96, 96, seed=3), 1e30, 30),
+    ("walls2d_weno3_lowmach_rk3", dict(nx=80, ny=64, reconstruction="weno3", riemann_solver="lowmach", time_scheme="SSP Runge-Kutta 3",
+                                       **cases.bcs("wall", "outlet", "no_slip", "vel_inlet"), u_in=0.2), lambda: cases.smooth_field(80, 64, seed=5), 1e30, 20),
+]
+
+
+@pytest.mark.parametrize("name,params,init,t_end,steps", CASES, ids=[c[0] for c in CASES])
+def test_mixed_within_l1_bar(name, params, init, t_end, steps):
+    U0 = init()
+    plain = Run(params, U=U0, precision=0)
+    mixed = Run(params, U=U0, precision=1)
+    n_p = plain.run(t_end, max_steps=steps)
+    n_m = mixed.run(t_end, max_steps=steps)
+    assert n_p == n_m
+    errs = rel_errors(mixed.state(), plain.state())
+    print(f"\n{name}: {n_p} steps; " + "; ".join(f"{k}: L1 {v[0]:.2e} Linf {v[1]:.2e}" for k, v in errs.items()))
+    assert errs["rho"][0] <= 1e-4
+    assert all(np.isfinite(v[0]) for v in errs.values())
