@@ -45,6 +45,11 @@ struct Bc {
     int type[6];   // left, right, bottom, top, front, back
     int halo[6];   // kHalo* of each side for the reconstruction stencil
     double u_in, v_in, p_out;
+    // immersed body (null without one): the solid mask, and the forced states the residual reads in place of the cells'
+    // own (ghost cells filled from their image points, deeper solid cells at rest): slot[c] >= 0 -> forced[5 slot + q]
+    const unsigned char* solid;
+    const int* slot;
+    const double* forced;
 };
 
 // BoundaryManager::ghost_state (cpp/src/Boundaries.cpp:106-153) for the sides a device run supports (every type but
@@ -98,6 +103,21 @@ template <int NV> __device__ __forceinline__ St<double, NV> read_cell(const doub
     return s;
 }
 
+// The state a residual reads for cell c: the cell's own, or its forced state where the immersed body overrides it
+// (ImmersedBoundary::force_in_place, cpp/src/Physics.cpp:962-973: the residual sees the forced field; the update does not).
+template <int NV> __device__ __forceinline__ St<double, NV> read_state(const Bc& bc, const double* __restrict__ U, long long plane, long long c) {
+    if (bc.slot) {
+        const int s = bc.slot[c];
+        if (s >= 0) {
+            St<double, NV> f;
+#pragma unroll
+            for (int q = 0; q < NV; ++q) f[q] = bc.forced[5 * (long long)s + q];
+            return f;
+        }
+    }
+    return read_cell<NV>(U, plane, c);
+}
+
 // The conservative state at cell position (i, j, k) of the reconstruction stencil, which may lie outside the mesh along
 // one axis: the periodic wrap, the ghost-slab state of the mirrored cell (fill_ghost_slab, cpp/src/Boundaries.cpp:202-228:
 // layer l beyond the side is ghost_state of the interior cell l cells from it), or edge replication (pad_primitives,
@@ -129,13 +149,29 @@ __device__ __forceinline__ St<double, NV> stencil_cons(const Mesh& m, const Bc& 
             l = l < n3[a] ? l : n3[a] - 1;
             idx[a] = hi ? n3[a] - 1 - l : l;
             const long long c = ((long long)idx[2] * m.ny + idx[1]) * m.nx + idx[0];
-            return ghost_state(e, bc, side, read_cell<NV>(U, m.plane, c));
+            return ghost_state(e, bc, side, read_state<NV>(bc, U, m.plane, c));
         }
     }
 #pragma unroll
     for (int a = 0; a < 3; ++a) idx[a] = idx[a] < 0 ? 0 : (idx[a] >= n3[a] ? n3[a] - 1 : idx[a]);
     const long long c = ((long long)idx[2] * m.ny + idx[1]) * m.nx + idx[0];
-    return read_cell<NV>(U, m.plane, c);
+    return read_state<NV>(bc, U, m.plane, c);
+}
+
+// Solidity of a stencil position for WENO5-Z's narrow stencil beside an immersed body (make_grid, cpp/src/Schemes.cpp:
+// 1004-1019): a position outside the mesh is solid if the cell edge replication puts there, or the cell a periodic wrap
+// puts there, is solid.
+template <int DIM> __device__ __forceinline__ unsigned char stencil_solid(const Mesh& m, const Bc& bc, int i, int j, int k) {
+    const int n3[3] = {m.nx, m.ny, m.nz};
+    const int p[3] = {i, j, k};
+    int c[3], w[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        c[a] = p[a] < 0 ? 0 : (p[a] >= n3[a] ? n3[a] - 1 : p[a]);
+        w[a] = ((p[a] % n3[a]) + n3[a]) % n3[a];
+    }
+    const long long cc = ((long long)c[2] * m.ny + c[1]) * m.nx + c[0], cw = ((long long)w[2] * m.ny + w[1]) * m.nx + w[0];
+    return (bc.solid[cc] != 0 || bc.solid[cw] != 0) ? 1 : 0;
 }
 
 // The first-order states of a boundary face whose side has no halo (BoundaryManager::apply_side,
@@ -144,13 +180,13 @@ template <int NV>
 __device__ __forceinline__ void side_states(const Mesh& m, const Bc& bc, const Eos<double>& e, const double* __restrict__ U, int side, int i, int j, int k,
                                             St<double, NV>& UL, St<double, NV>& UR) {
     const long long c = ((long long)k * m.ny + j) * m.nx + i;
-    const St<double, NV> Ui = read_cell<NV>(U, m.plane, c);
+    const St<double, NV> Ui = read_state<NV>(bc, U, m.plane, c);
     St<double, NV> Ug;
     if (bc.type[side] == kBcPeriodic) {
         int idx[3] = {i, j, k};
         const int a = side >> 1, n = a == 0 ? m.nx : (a == 1 ? m.ny : m.nz);
         idx[a] = (side & 1) ? idx[a] - (n - 1) : idx[a] + (n - 1);
-        Ug = read_cell<NV>(U, m.plane, ((long long)idx[2] * m.ny + idx[1]) * m.nx + idx[0]);
+        Ug = read_state<NV>(bc, U, m.plane, ((long long)idx[2] * m.ny + idx[1]) * m.nx + idx[0]);
     } else {
         Ug = ghost_state(e, bc, side, Ui);
     }

@@ -118,24 +118,36 @@ __global__ void __launch_bounds__(NT) hancock_kernel(const HancockArgs a) {
             const bool b0 = ci == 0 && a.bc.halo[0] == kHaloNone, b1 = ci == nx - 1 && a.bc.halo[1] == kHaloNone;
             const bool b2 = cj == 0 && a.bc.halo[2] == kHaloNone, b3 = cj == ny - 1 && a.bc.halo[3] == kHaloNone;
             if (b0 || b1 || b2 || b3) {
-                const St<double, 4> rt = round_trip(e, read_cell<4>(a.U, m.plane, (long long)cj * nx + ci));
+                const St<double, 4> rt = round_trip(e, read_state<4>(a.bc, a.U, m.plane, (long long)cj * nx + ci));
                 if (b0) st[0] = rt;
                 if (b1) st[1] = rt;
                 if (b2) st[2] = rt;
                 if (b3) st[3] = rt;
             }
-            // hancock_cell (Schemes.cpp:2153-2172)
-            const St<double, 4> fxl = euler_flux2(e, st[0], 0), fxr = euler_flux2(e, st[1], 0);
-            const St<double, 4> fyb = euler_flux2(e, st[2], 1), fyt = euler_flux2(e, st[3], 1);
-            St<double, 4> d;
+            // an immersed body: its cells are not predicted, nor the sides of a cell that face one (the states of those
+            // sides keep the time level of the ghost cells; solid_side_mask, Schemes.cpp:2890-2905, no wrap-around)
+            const unsigned char* sol = a.bc.solid;
+            const bool is_solid = sol && sol[(long long)cj * nx + ci];
+            int sd = 0;
+            if (sol && !is_solid) {
+                sd = (ci > 0 && sol[(long long)cj * nx + ci - 1] ? 1 : 0) | (ci < nx - 1 && sol[(long long)cj * nx + ci + 1] ? 2 : 0) |
+                     (cj > 0 && sol[(long long)(cj - 1) * nx + ci] ? 4 : 0) | (cj < ny - 1 && sol[(long long)(cj + 1) * nx + ci] ? 8 : 0);
+            }
+            if (!is_solid) {
+                // hancock_cell (Schemes.cpp:2153-2172)
+                const St<double, 4> fxl = euler_flux2(e, st[0], 0), fxr = euler_flux2(e, st[1], 0);
+                const St<double, 4> fyb = euler_flux2(e, st[2], 1), fyt = euler_flux2(e, st[3], 1);
+                St<double, 4> d;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) d[q] = hx * (fxr[q] - fxl[q]) + hy * (fyt[q] - fyb[q]);
+                for (int q = 0; q < 4; ++q) d[q] = hx * (fxr[q] - fxl[q]) + hy * (fyt[q] - fyb[q]);
 #pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                St<double, 4> n;
+                for (int s = 0; s < 4; ++s) {
+                    if (sd & (1 << s)) continue;
+                    St<double, 4> n;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) n[q] = st[s][q] - d[q];
-                if (admissible(e, n)) st[s] = n;
+                    for (int q = 0; q < 4; ++q) n[q] = st[s][q] - d[q];
+                    if (admissible(e, n)) st[s] = n;
+                }
             }
         }
 #pragma unroll
@@ -176,14 +188,14 @@ __global__ void __launch_bounds__(NT) hancock_kernel(const HancockArgs a) {
                     if (wall_lo)
                         UL = ghost_state(e, a.bc, lo_side, UR);
                     else if (a.bc.halo[lo_side] == kHaloNone)
-                        UL = round_trip(e, ghost_state(e, a.bc, lo_side, read_cell<4>(a.U, m.plane, (long long)gj * nx + gi)));
+                        UL = round_trip(e, ghost_state(e, a.bc, lo_side, read_state<4>(a.bc, a.U, m.plane, (long long)gj * nx + gi)));
                 }
                 if (t == n_a) {
                     const int ci = axis == 0 ? nx - 1 : gi, cj = axis == 0 ? gj : ny - 1;
                     if (wall_hi)
                         UR = ghost_state(e, a.bc, hi_side, UL);
                     else if (a.bc.halo[hi_side] == kHaloNone)
-                        UR = round_trip(e, ghost_state(e, a.bc, hi_side, read_cell<4>(a.U, m.plane, (long long)cj * nx + ci)));
+                        UR = round_trip(e, ghost_state(e, a.bc, hi_side, read_state<4>(a.bc, a.U, m.plane, (long long)cj * nx + ci)));
                 }
                 const double s = face_flux<RIEMANN>(e, a.shock_blend, UL, UR, axis, F);
                 if (s > smax) smax = s;

@@ -61,13 +61,15 @@ template <int DIM, int RECON, int TX, int TY, int TZ> struct MixedShape {
     static constexpr int NF = cmax(cmax(nf(0), nf(1)), DIM == 3 ? nf(2) : 0);
     // floats: P [NV][EXT], WL / WR [NV][NF] (the fluxes overwrite WL), acc [NV][NC], 64 for the reduction
     static constexpr int SMEM_FLOATS = NV * EXT + 2 * NV * NF + NV * NC + 64;
-    static constexpr size_t SMEM_BYTES = sizeof(float) * SMEM_FLOATS;
+    static constexpr int FLAG_BYTES = (EXT + 7) / 8 * 8;   // solidity of the extended tile (WENO5-Z beside an immersed body)
+    static constexpr size_t SMEM_BYTES = sizeof(float) * SMEM_FLOATS + FLAG_BYTES;
 };
 
 // One axis of the tile sweep of mixed_stage_kernel (compile-time extents).
 template <int AXIS, int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT>
 __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>& ef, float sb, float weps, float* __restrict__ P,
-                                           float* __restrict__ WL, float* __restrict__ WR, float* __restrict__ acc, const int o3[3], float& smax) {
+                                           float* __restrict__ WL, float* __restrict__ WR, float* __restrict__ acc, unsigned char* __restrict__ Sf,
+                                           const int o3[3], float& smax) {
     using S = MixedShape<DIM, RECON, TX, TY, TZ>;
     constexpr int NV = S::NV, H = S::H, NC = S::NC;
     constexpr int axis = AXIS;
@@ -83,6 +85,8 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
             int l3[3] = {e % E[0], (e / E[0]) % E[1], e / (E[0] * E[1])};
             l3[axis] -= H;
             const St<double, NV> w = c2p(a.eos, stencil_cons<DIM, NV>(m, a.bc, a.eos, a.U, o3[0] + l3[0], o3[1] + l3[1], o3[2] + l3[2]));
+            if constexpr (RECON == kWeno5)
+                if (a.bc.solid) Sf[e] = stencil_solid<DIM>(m, a.bc, o3[0] + l3[0], o3[1] + l3[1], o3[2] + l3[2]);
 #pragma unroll
             for (int q = 0; q < NV; ++q) P[q * S::EXT + e] = (float)w[q];
         }
@@ -104,8 +108,18 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
                 wr = weno3z(c[3 * sstride], c[2 * sstride], c[sstride], weps);
             } else {
                 const float c0 = c[0], c1 = c[sstride], c2 = c[2 * sstride], c3 = c[3 * sstride], c4 = c[4 * sstride], c5 = c[5 * sstride];
-                wl = weno5z(c0, c1, c2, c3, c4, weps);
-                wr = weno5z(c5, c4, c3, c2, c1, weps);
+                const int base = (f3[2] * E[1] + f3[1]) * E[0] + f3[0];
+                bool four = false;
+                if (a.bc.solid)
+#pragma unroll
+                    for (int s6 = 0; s6 < 6; ++s6) four = four || Sf[base + s6 * sstride] != 0;
+                if (four) {
+                    wl = weno3z(c1, c2, c3, weps);
+                    wr = weno3z(c4, c3, c2, weps);
+                } else {
+                    wl = weno5z(c0, c1, c2, c3, c4, weps);
+                    wr = weno5z(c5, c4, c3, c2, c1, weps);
+                }
             }
             WL[q * S::NF + f] = wl;
             WR[q * S::NF + f] = wr;
@@ -173,25 +187,25 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
 template <int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT>
 __global__ void __launch_bounds__(NT) mixed_stage_kernel(const StageArgs a) {
     using S = MixedShape<DIM, RECON, TX, TY, TZ>;
-    constexpr int NV = S::NV, H = S::H, NC = S::NC;
+    constexpr int NV = S::NV, NC = S::NC;
     extern __shared__ double smem_d[];
     double* red = smem_d;                                      // [32]
     float* P = reinterpret_cast<float*>(smem_d + 32);         // [NV][EXT]
     float* WL = P + NV * S::EXT;                               // [NV][NF]
     float* WR = WL + NV * S::NF;                               // [NV][NF]
     float* acc = WR + NV * S::NF;                              // [NV][NC]
+    unsigned char* Sf = reinterpret_cast<unsigned char*>(acc + NV * NC);   // [EXT]
     if (!*a.gate) return;
     const Mesh& m = a.m;
     const Eos<float> ef{a.eos.type, (float)a.eos.gamma, (float)a.eos.p_inf};
     const float sb = (float)a.shock_blend, weps = (float)a.weno_eps;
     const int tid = threadIdx.x, b = blockIdx.x;
     const int o3[3] = {(b % a.tiles[0]) * TX, ((b / a.tiles[0]) % a.tiles[1]) * TY, (b / (a.tiles[0] * a.tiles[1])) * TZ};
-    const int n3[3] = {m.nx, m.ny, m.nz};
     float smax = 0.0f;
 
-    mixed_axis<0, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, ef, sb, weps, P, WL, WR, acc, o3, smax);
-    mixed_axis<1, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, ef, sb, weps, P, WL, WR, acc, o3, smax);
-    if constexpr (DIM == 3) mixed_axis<2, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, ef, sb, weps, P, WL, WR, acc, o3, smax);
+    mixed_axis<0, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
+    mixed_axis<1, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
+    if constexpr (DIM == 3) mixed_axis<2, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
     // ---- epilogue: the residual widened to FP64 and the FP64 stage update
     const double dt = a.ctl->dt;
     for (int c = tid; c < NC; c += NT) {

@@ -18,6 +18,8 @@
 // step runs (t < t_end, step limit, no error).
 #include "../../include/fenice_gpu.h"
 #include "hancock.cuh"
+#include "ibm.cuh"
+#include "ibm_host.h"
 #include "mixed_api.h"
 #include "stage.cuh"
 #include "viscous.cuh"
@@ -252,6 +254,12 @@ struct fvg_run {
     };
     bool timing = false;
     EvTimer t_stage, t_visc;
+    // immersed body (use_ibm): the mask, the forced-state slots and buffer, the ghost table, the deep solid cells
+    bool ibm = false;
+    int ng = 0, nd = 0;
+    unsigned char* d_mask = nullptr;
+    int *d_slot = nullptr, *d_ghost = nullptr, *d_img_cell = nullptr, *d_deep = nullptr;
+    double *d_forced = nullptr, *d_img_w = nullptr, *d_ratio = nullptr, *d_gn = nullptr;
     double* Ucur() { return cur ? Ut : U; }
 };
 
@@ -407,9 +415,41 @@ void timer_flush(fvg_run::EvTimer& t) {
     t.used = 0;
 }
 
+// The immersed body's forced states of Uin (reset = 0: for the residual that follows) or its per-step reset of Uout in
+// place (reset = 1: ImmersedBoundary::apply_solid_reset, after each step).
+cudaError_t ibm_fill(fvg_run* r, const double* Usrc, double* Uout, int reset, const int* gate) {
+    IbmArgs a{};
+    a.m = r->m;
+    a.eos = r->eos;
+    a.slip = r->cfg.use_viscous ? 0 : 1;
+    a.ng = r->ng;
+    a.nd = r->nd;
+    a.ghost = r->d_ghost;
+    a.img_cell = r->d_img_cell;
+    a.img_w = r->d_img_w;
+    a.ratio = r->d_ratio;
+    a.gn = r->d_gn;
+    a.deep = r->d_deep;
+    a.rho_ref = r->cfg.rho_in;
+    a.p_ref = r->cfg.p_out;
+    a.U = Usrc;
+    a.forced = r->d_forced;
+    a.Uout = Uout;
+    a.reset = reset;
+    a.gate = gate;
+    const int n = r->ng + r->nd;
+    const int blocks = n <= 0 ? 1 : ((n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184);
+    if (r->nvar == 5)
+        ibm_fill_kernel<5><<<blocks, 256, 0, r->stream>>>(a);
+    else
+        ibm_fill_kernel<4><<<blocks, 256, 0, r->stream>>>(a);
+    return cudaGetLastError();
+}
+
 // One residual stage of Uin: the viscous sweep (3-D viscous runs), then the inviscid stage kernel.
 cudaError_t residual_stage(fvg_run* r, const double* Uin, const double* U0, double* out, int mode, double ca, double cb, int stage, const int* gate) {
     cudaError_t e;
+    if (r->ibm && (e = ibm_fill(r, Uin, nullptr, 0, gate)) != cudaSuccess) return e;
     if (r->cfg.use_viscous) {
         timer_mark(r, r->t_visc);
         e = r->cfg.precision == FVG_PREC_MIXED ? mixed_viscous_launch(visc_args(r, Uin, r->bmv[stage], gate), r->nbv, r->stream)
@@ -440,13 +480,16 @@ cudaError_t enqueue_step(fvg_run* r) {
         double* Uin = r->Ucur();
         double* Uout = r->cur ? r->U : r->Ut;
         k_hancock_begin<<<1, 1, 0, r->stream>>>(c);
+        if (r->ibm && (e = ibm_fill(r, Uin, nullptr, 0, &c->seed))) return e;
         if ((e = r->stage.launch(stage_args(r, Uin, nullptr, r->R, kStoreR, 0, 0, nullptr, r->bm_seed, &c->seed), r->nb, r->stream))) return e;
         k_hancock_seed<<<1, 1024, 0, r->stream>>>(c, r->bm_seed, r->nb);
         k_hancock_dt<<<1, 1, 0, r->stream>>>(c);
+        if (r->ibm && (e = ibm_fill(r, Uin, nullptr, 0, act))) return e;
         timer_mark(r, r->t_stage);
         e = launch_hancock(r, hancock_args(r, Uin, Uout, kAxpy, r->bm[0], act));
         timer_mark(r, r->t_stage);
         if (e) return e;
+        if (r->ibm && (e = ibm_fill(r, Uout, Uout, 1, act))) return e;
         k_hancock_end<<<1, 1024, 0, r->stream>>>(c, r->bm[0], r->nbh);
         r->cur ^= 1;
         return cudaGetLastError();
@@ -455,6 +498,7 @@ cudaError_t enqueue_step(fvg_run* r) {
     k_stage1_dt<<<1, 1024, 0, r->stream>>>(c, r->bm[0], r->nb, r->bmv[0], nbv);
     if (ts == FVG_TS_EULER) {
         k_axpy<<<axpy_blocks(r), 256, 0, r->stream>>>(c, r->U, r->U, r->R, r->m.plane, r->m.ncells, r->nvar);
+        if (r->ibm && (e = ibm_fill(r, r->U, r->U, 1, act))) return e;
         k_end_rk<<<1, 1, 0, r->stream>>>(c, 1);
         return cudaGetLastError();
     }
@@ -462,6 +506,7 @@ cudaError_t enqueue_step(fvg_run* r) {
     if (ts == FVG_TS_SSPRK2) {
         if ((e = residual_stage(r, r->Ut, r->U, r->U, kCombine, 0.5, 0.5, 1, act))) return e;
         k_stage_max<<<1, 1024, 0, r->stream>>>(c, act, 1, r->bm[1], r->nb, r->bmv[1], nbv);
+        if (r->ibm && (e = ibm_fill(r, r->U, r->U, 1, act))) return e;
         k_end_rk<<<1, 1, 0, r->stream>>>(c, 2);
         return cudaGetLastError();
     }
@@ -469,6 +514,7 @@ cudaError_t enqueue_step(fvg_run* r) {
     k_stage_max<<<1, 1024, 0, r->stream>>>(c, act, 1, r->bm[1], r->nb, r->bmv[1], nbv);
     if ((e = residual_stage(r, r->R, r->U, r->U, kCombine, 1.0 / 3.0, 2.0 / 3.0, 2, act))) return e;
     k_stage_max<<<1, 1024, 0, r->stream>>>(c, act, 2, r->bm[2], r->nb, r->bmv[2], nbv);
+    if (r->ibm && (e = ibm_fill(r, r->U, r->U, 1, act))) return e;
     k_end_rk<<<1, 1, 0, r->stream>>>(c, 3);
     return cudaGetLastError();
 }
@@ -587,6 +633,48 @@ int fvg_create(const fvg_config* cfg, fvg_run** out) {
             run->err = "device allocation failed";
             return bail(FVG_ERR_CUDA);
         }
+    if (c.use_ibm) {
+        IbmTable t;
+        const std::string msg = build_ibm(c, t);
+        if (!msg.empty()) {
+            run->err = msg;
+            return bail(FVG_ERR_CONFIG);
+        }
+        run->ibm = true;
+        run->ng = (int)t.ghost.size();
+        run->nd = (int)t.deep.size();
+        std::vector<int> slot(run->m.ncells, -1);
+        for (int k = 0; k < run->ng; ++k) slot[t.ghost[k]] = k;
+        for (int k = 0; k < run->nd; ++k) slot[t.deep[k]] = run->ng + k;
+        std::vector<double> gn(3 * (size_t)run->ng);
+        for (int k = 0; k < run->ng; ++k) {
+            gn[3 * k] = t.gnx[k];
+            gn[3 * k + 1] = t.gny[k];
+            gn[3 * k + 2] = t.gnz[k];
+        }
+        const size_t ns = (size_t)(run->ng + run->nd) + 1, ng1 = (size_t)run->ng + 1, nd1 = (size_t)run->nd + 1;
+        bool ok = cudaMalloc(&run->d_mask, run->m.ncells) == cudaSuccess && cudaMalloc(&run->d_slot, sizeof(int) * run->m.ncells) == cudaSuccess &&
+                  cudaMalloc(&run->d_forced, sizeof(double) * 5 * ns) == cudaSuccess && cudaMalloc(&run->d_ghost, sizeof(int) * ng1) == cudaSuccess &&
+                  cudaMalloc(&run->d_img_cell, sizeof(int) * 8 * ng1) == cudaSuccess && cudaMalloc(&run->d_img_w, sizeof(double) * 8 * ng1) == cudaSuccess &&
+                  cudaMalloc(&run->d_ratio, sizeof(double) * ng1) == cudaSuccess && cudaMalloc(&run->d_gn, sizeof(double) * 3 * ng1) == cudaSuccess &&
+                  cudaMalloc(&run->d_deep, sizeof(int) * nd1) == cudaSuccess;
+        ok = ok && cudaMemcpy(run->d_mask, t.mask.data(), run->m.ncells, cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(run->d_slot, slot.data(), sizeof(int) * run->m.ncells, cudaMemcpyHostToDevice) == cudaSuccess;
+        if (ok && run->ng > 0)
+            ok = cudaMemcpy(run->d_ghost, t.ghost.data(), sizeof(int) * run->ng, cudaMemcpyHostToDevice) == cudaSuccess &&
+                 cudaMemcpy(run->d_img_cell, t.img_cell.data(), sizeof(int) * 8 * run->ng, cudaMemcpyHostToDevice) == cudaSuccess &&
+                 cudaMemcpy(run->d_img_w, t.img_w.data(), sizeof(double) * 8 * run->ng, cudaMemcpyHostToDevice) == cudaSuccess &&
+                 cudaMemcpy(run->d_ratio, t.ratio.data(), sizeof(double) * run->ng, cudaMemcpyHostToDevice) == cudaSuccess &&
+                 cudaMemcpy(run->d_gn, gn.data(), sizeof(double) * 3 * run->ng, cudaMemcpyHostToDevice) == cudaSuccess;
+        if (ok && run->nd > 0) ok = cudaMemcpy(run->d_deep, t.deep.data(), sizeof(int) * run->nd, cudaMemcpyHostToDevice) == cudaSuccess;
+        if (!ok) {
+            run->err = "device allocation of the immersed body's tables failed";
+            return bail(FVG_ERR_CUDA);
+        }
+        run->bc.solid = run->d_mask;
+        run->bc.slot = run->d_slot;
+        run->bc.forced = run->d_forced;
+    }
     cudaMemsetAsync(run->U, 0, sbytes, run->stream);
     cudaMemsetAsync(run->Ut, 0, sbytes, run->stream);
     Ctl h{};
@@ -615,6 +703,9 @@ int fvg_destroy(fvg_run* run) {
     for (double* p : {run->U, run->Ut, run->R, run->Rv, run->staging, run->bm_seed, run->bm[0], run->bm[1], run->bm[2], run->bmv[0], run->bmv[1], run->bmv[2]})
         if (p) cudaFree(p);
     if (run->ctl) cudaFree(run->ctl);
+    for (void* p : {(void*)run->d_mask, (void*)run->d_slot, (void*)run->d_forced, (void*)run->d_ghost, (void*)run->d_img_cell, (void*)run->d_img_w,
+                    (void*)run->d_ratio, (void*)run->d_gn, (void*)run->d_deep})
+        if (p) cudaFree(p);
     if (run->stream) cudaStreamDestroy(run->stream);
     delete run;
     return FVG_OK;
@@ -669,6 +760,7 @@ int fvg_residual(fvg_run* run, double predictor_half_dt, double* R, size_t ncell
         if (run->cfg.reconstruction != FVG_RECON_MUSCL || run->dim != 2 || run->cfg.use_viscous)
             return fail(run, FVG_ERR_CONFIG, "the MUSCL-Hancock predictor needs a 2-D inviscid MUSCL run");
         CK(cudaMemcpyAsync(&c->half_dt, &predictor_half_dt, sizeof(double), cudaMemcpyHostToDevice, run->stream));
+        if (run->ibm) CK(ibm_fill(run, run->Ucur(), nullptr, 0, always));
         CK(launch_hancock(run, hancock_args(run, run->Ucur(), out, kStoreR, run->bm[0], always)));
         k_stage_max<<<1, 1024, 0, run->stream>>>(c, always, 0, run->bm[0], run->nbh, run->bmv[0], 0);
     } else {
@@ -934,6 +1026,7 @@ extern "C" int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long
     const std::string v = validate(*cfg);
     if (!v.empty()) return noalloc_fail(FVG_ERR_CONFIG, v);
     if (cfg->precision != FVG_PREC_FP64) return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: the FP64 form only");
+    if (cfg->use_ibm) return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: an immersed body needs its tables on the device; use fvg_residual");
     if (cfg->use_viscous) return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: viscous runs need a residual-sized scratch array; use fvg_residual");
     const fvg_config& c = *cfg;
     const int dim = c.nz > 1 ? 3 : 2;

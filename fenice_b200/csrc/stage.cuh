@@ -57,14 +57,15 @@ template <int DIM, int RECON, int TX, int TY, int TZ> struct StageShape {
     // acc [NV][NC] the balance, 32 for the reduction
     static constexpr int P_SIZE = NV * EXT;
     static constexpr int SMEM_DOUBLES = P_SIZE + 2 * NV * NF + NV * NC + 32;
-    static constexpr size_t SMEM_BYTES = sizeof(double) * SMEM_DOUBLES;
+    static constexpr int FLAG_BYTES = (EXT + 7) / 8 * 8;   // solidity of the extended tile (WENO5-Z beside an immersed body)
+    static constexpr size_t SMEM_BYTES = sizeof(double) * SMEM_DOUBLES + FLAG_BYTES;
 };
 
 // One axis of the tile sweep of stage_kernel (the axis a template parameter, so the extents of the extended tile and of
 // the face grid are compile-time constants).
 template <int AXIS, int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT>
 __device__ __forceinline__ void stage_axis(const StageArgs& a, double* __restrict__ P, double* __restrict__ WL, double* __restrict__ WR,
-                                           double* __restrict__ acc, const int o3[3], double& smax) {
+                                           double* __restrict__ acc, unsigned char* __restrict__ Sf, const int o3[3], double& smax) {
     using S = StageShape<DIM, RECON, TX, TY, TZ>;
     constexpr int NV = S::NV, H = S::H, NC = S::NC;
     constexpr int axis = AXIS;
@@ -81,6 +82,8 @@ __device__ __forceinline__ void stage_axis(const StageArgs& a, double* __restric
             int l3[3] = {e % E[0], (e / E[0]) % E[1], e / (E[0] * E[1])};
             l3[axis] -= H;
             const St<double, NV> u = stencil_cons<DIM, NV>(m, a.bc, a.eos, a.U, o3[0] + l3[0], o3[1] + l3[1], o3[2] + l3[2]);
+            if constexpr (RECON == kWeno5)
+                if (a.bc.solid) Sf[e] = stencil_solid<DIM>(m, a.bc, o3[0] + l3[0], o3[1] + l3[1], o3[2] + l3[2]);
             if constexpr (RECON == kFirstOrder) {
 #pragma unroll
                 for (int q = 0; q < NV; ++q) P[q * S::EXT + e] = u[q];
@@ -112,8 +115,17 @@ __device__ __forceinline__ void stage_axis(const StageArgs& a, double* __restric
                     wr = weno3z(c[3 * sstride], c[2 * sstride], c[sstride], a.weno_eps);
                 } else {
                     const double c0 = c[0], c1 = c[sstride], c2 = c[2 * sstride], c3 = c[3 * sstride], c4 = c[4 * sstride], c5 = c[5 * sstride];
-                    wl = weno5z(c0, c1, c2, c3, c4, a.weno_eps);
-                    wr = weno5z(c5, c4, c3, c2, c1, a.weno_eps);
+                    bool four = false;   // a solid cell among the six: the four-cell WENO3-Z stencil (weno_line_states, Schemes.cpp:815-831)
+                    if (a.bc.solid)
+#pragma unroll
+                        for (int s6 = 0; s6 < 6; ++s6) four = four || Sf[base + s6 * sstride] != 0;
+                    if (four) {
+                        wl = weno3z(c1, c2, c3, a.weno_eps);
+                        wr = weno3z(c4, c3, c2, a.weno_eps);
+                    } else {
+                        wl = weno5z(c0, c1, c2, c3, c4, a.weno_eps);
+                        wr = weno5z(c5, c4, c3, c2, c1, a.weno_eps);
+                    }
                 }
                 WL[q * S::NF + f] = wl;
                 WR[q * S::NF + f] = wr;
@@ -190,13 +202,14 @@ __device__ __forceinline__ void stage_axis(const StageArgs& a, double* __restric
 template <int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT>
 __global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
     using S = StageShape<DIM, RECON, TX, TY, TZ>;
-    constexpr int NV = S::NV, H = S::H, NC = S::NC;
+    constexpr int NV = S::NV, NC = S::NC;
     extern __shared__ double smem[];
     double* P = smem;                       // [NV][EXT]
     double* WL = P + S::P_SIZE;             // [NV][NF]
     double* WR = WL + NV * S::NF;           // [NV][NF]
     double* acc = WR + NV * S::NF;          // [NV][NC]
     double* red = acc + NV * NC;            // [32]
+    unsigned char* Sf = reinterpret_cast<unsigned char*>(red + 32);   // [EXT]
     if (!*a.gate) return;
 
     const Mesh& m = a.m;
@@ -204,12 +217,11 @@ __global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
     const int b = blockIdx.x;
     const int t0 = b % a.tiles[0], t1 = (b / a.tiles[0]) % a.tiles[1], t2 = b / (a.tiles[0] * a.tiles[1]);
     const int o3[3] = {t0 * TX, t1 * TY, t2 * TZ};
-    const int n3[3] = {m.nx, m.ny, m.nz};
     double smax = 0.0;
 
-    stage_axis<0, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, P, WL, WR, acc, o3, smax);
-    stage_axis<1, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, P, WL, WR, acc, o3, smax);
-    if constexpr (DIM == 3) stage_axis<2, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, P, WL, WR, acc, o3, smax);
+    stage_axis<0, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, P, WL, WR, acc, Sf, o3, smax);
+    stage_axis<1, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, P, WL, WR, acc, Sf, o3, smax);
+    if constexpr (DIM == 3) stage_axis<2, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, P, WL, WR, acc, Sf, o3, smax);
     // ---- epilogue: the residual and the stage update
     const double dt = a.ctl->dt;
     for (int c = tid; c < NC; c += NT) {

@@ -56,7 +56,7 @@ __device__ __forceinline__ St<double, 5> viscous_ghost_3d(const ViscArgs& a, int
 }
 
 __device__ __forceinline__ St<double, 5> cell_at(const ViscArgs& a, int i, int j, int k) {
-    return read_cell<5>(a.U, a.m.plane, ((long long)k * a.m.ny + j) * a.m.nx + i);
+    return read_state<5>(a.bc, a.U, a.m.plane, ((long long)k * a.m.ny + j) * a.m.nx + i);
 }
 
 // The padded entry beyond one side along axis d (padded_3d, Boundaries.cpp:621-700): the opposite layer of a periodic

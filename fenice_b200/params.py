@@ -20,6 +20,7 @@ DEFAULTS = {
     "riemann_solver": "HLLC", "reconstruction": "none", "muscl_limiter": "Van Leer", "weno_epsilon": 1e-6,
     "boundary_order": 2, "time_scheme": "auto", "cfl": 0.5, "shock_blend": 0.2, "dt_max": 0.0, "t_end": 0.005,
     "max_steps": 0,
+    "use_ibm": False, "ibm_shape": "Cylinder", "ibm_radius": 0.1, "ibm_cx": 0.5, "ibm_cy": 0.5, "ibm_cz": 0.5, "ibm_curvature": False,
 }
 
 BC_NAMES = {"wall": 0, "inviscid wall (slip)": 0, "no_slip": 1, "viscous wall (no-slip)": 1, "moving_wall": 2, "moving wall": 2,
@@ -45,7 +46,9 @@ class FvgConfig(ctypes.Structure):
                 ("boundary_order", ctypes.c_int), ("time_scheme", ctypes.c_int),
                 ("cfl", ctypes.c_double), ("dt_max", ctypes.c_double),
                 ("use_viscous", ctypes.c_int), ("mu", ctypes.c_double), ("pr", ctypes.c_double),
-                ("precision", ctypes.c_int), ("device", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("device", ctypes.c_int),
+                ("use_ibm", ctypes.c_int), ("ibm_shape", ctypes.c_int), ("ibm_radius", ctypes.c_double), ("ibm_cx", ctypes.c_double),
+                ("ibm_cy", ctypes.c_double), ("ibm_cz", ctypes.c_double), ("ibm_curvature", ctypes.c_int)]
 
 
 def _flag(v):
@@ -99,6 +102,13 @@ def to_config(params, precision=0, device=0):
     c.mu, c.pr = float(p["mu"]), float(p["pr"])
     c.precision = int(precision)
     c.device = int(device)
+    c.use_ibm = 1 if _flag(p["use_ibm"]) else 0
+    shape = str(p["ibm_shape"]).strip().lower()
+    if c.use_ibm and shape not in ("cylinder", "sphere"):
+        raise ValueError(f"Unknown IBM shape: '{p['ibm_shape']}' (the device path supports Cylinder and Sphere)")
+    c.ibm_shape = 1 if shape == "sphere" else 0
+    c.ibm_radius, c.ibm_cx, c.ibm_cy, c.ibm_cz = float(p["ibm_radius"]), float(p["ibm_cx"]), float(p["ibm_cy"]), float(p["ibm_cz"])
+    c.ibm_curvature = 1 if _flag(p["ibm_curvature"]) else 0
     return c
 
 

@@ -69,6 +69,10 @@ typedef struct fvg_config {
     double mu, pr;               /* [physics] mu, pr */
     int precision;               /* FVG_PREC_FP64: the reference's arithmetic, bit for bit; FVG_PREC_MIXED: FP32 stencil */
     int device;                  /* CUDA device ordinal */
+    int use_ibm;                 /* [ibm] use_ibm: a static immersed body with the sharp ghost-cell wall (slip when inviscid) */
+    int ibm_shape;               /* [ibm] ibm_shape: 0 Cylinder (a circle in 2-D, infinite along z in 3-D), 1 Sphere (3-D) */
+    double ibm_radius, ibm_cx, ibm_cy, ibm_cz; /* [ibm] */
+    int ibm_curvature;           /* [ibm] ibm_curvature (must be 0 on the device) */
 } fvg_config;
 
 typedef struct fvg_run fvg_run;

@@ -105,3 +105,36 @@ def case_field(params, seed):
         W[:, 3] = 1.0 + 0.1 * np.cos(np.arange(U.shape[0]))
         U = prim_to_cons(W, gamma=gamma, p_inf=float(params["p_inf"]), stiffened=True)
     return U
+
+
+# immersed-body cases: (name, params, initial primitive state, perturbation seed or None, n_steps)
+CYL = dict(Lx=8.0, Ly=12.0, use_ibm=True, ibm_shape="Cylinder", ibm_radius=0.5, ibm_cx=3.0, ibm_cy=6.0, rho_in=1.4, p_out=1.0, u_in=2.0,
+           bc_xmin="vel_inlet", bc_xmax="transmissive", bc_ymin="transmissive", bc_ymax="transmissive")
+IBM_CASES = [
+    ("cyl_hancock_mc", dict(nx=80, ny=120, reconstruction="muscl", muscl_limiter="MC", time_scheme="MUSCL-Hancock", **CYL), (1.4, 2.0, 0.0, 1.0), 41, 12),
+    ("cyl_weno5_rk3", dict(nx=64, ny=96, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", cfl=0.4, **CYL), (1.4, 2.0, 0.0, 1.0), 42, 6),
+    ("cyl_minmod_rk2_order1", dict(nx=48, ny=72, reconstruction="muscl", muscl_limiter="Minmod", time_scheme="SSP Runge-Kutta 2",
+                                   boundary_order=1, **CYL), (1.4, 2.0, 0.0, 1.0), 43, 6),
+    ("sphere3d_weno5_rk3", dict(nx=20, ny=18, nz=22, Lx=1.0, Ly=1.0, Lz=1.0, use_ibm=True, ibm_shape="Sphere", ibm_radius=0.22, ibm_cx=0.45,
+                                ibm_cy=0.5, ibm_cz=0.52, rho_in=1.0, p_out=1.0, u_in=0.5, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3",
+                                **bcs("vel_inlet", "transmissive", "transmissive", "transmissive", z=("transmissive", "transmissive"))),
+     (1.0, 0.5, 0.0, 1.0), 44, 3),
+    ("cyl3d_viscous_noslip", dict(nx=24, ny=20, nz=6, Lx=1.2, Ly=1.0, Lz=0.3, use_ibm=True, ibm_shape="Cylinder", ibm_radius=0.2, ibm_cx=0.4,
+                                  ibm_cy=0.5, rho_in=1.0, p_out=1.0, u_in=0.4, use_viscous=True, mu=0.01, reconstruction="muscl",
+                                  muscl_limiter="Van Leer", time_scheme="SSP Runge-Kutta 2",
+                                  **bcs("vel_inlet", "outlet", "wall", "wall", z=("periodic", "periodic"))), (1.0, 0.4, 0.0, 1.0), 45, 3),
+]
+
+
+def ibm_field(params, W0, seed):
+    """A uniform primitive state W0 with a small seeded perturbation (cells of 5 doubles; rho w = 0 on a 2-D mesh)."""
+    nz = int(params.get("nz", 1))
+    U = smooth_field(int(params["nx"]), int(params["ny"]), nz, seed=seed, amp=0.05)
+    W = np.zeros_like(U)
+    W[:, 0] = W0[0] * U[:, 0]
+    W[:, 1] = W0[1] + U[:, 1] / U[:, 0] - 0.3
+    W[:, 2] = W0[2] + U[:, 2] / U[:, 0] + 0.2
+    W[:, 3] = W0[3] * (1.0 + 0.1 * (U[:, 0] - 1.0))
+    if nz > 1:
+        W[:, 4] = U[:, 4] / U[:, 0] - 0.1
+    return prim_to_cons(W)
