@@ -64,6 +64,15 @@ static fvg_config to_fvg(const fv::SimParams& p) {
     c.pr = p.pr;
     c.precision = FVG_PREC_FP64;
     c.device = 0;
+    c.use_ibm = p.use_ibm ? 1 : 0;
+    std::string shape = p.ibm_shape;
+    for (auto& ch : shape) ch = static_cast<char>(std::tolower(static_cast<unsigned char>(ch)));
+    c.ibm_shape = shape == "sphere" ? 1 : 0;
+    c.ibm_radius = p.ibm_radius;
+    c.ibm_cx = p.ibm_cx;
+    c.ibm_cy = p.ibm_cy;
+    c.ibm_cz = p.ibm_cz;
+    c.ibm_curvature = p.ibm_curvature ? 1 : 0;
     return c;
 }
 
@@ -74,7 +83,8 @@ int main(int argc, char** argv) {
     if (!mkdtemp(tmpl)) return 2;
     const fs::path dir = tmpl;
     std::ofstream(dir / "case.toml") << "[case]\nname = \"dropin\"\n[initial]\n"
-                                     << (which == "vortex" ? "profile = \"isentropic_vortex\"\n"
+                                     << (which == "cylinder" ? "state = { rho = 1.4, u = 2.0, v = 0.0, p = 1.0 }\n"
+                                         : which == "vortex" ? "profile = \"isentropic_vortex\"\n"
                                          : which == "tgv"  ? "profile = \"taylor_green_3d\"\n"
                                                            : "state = { rho = 1.0, u = 0.1, v = -0.2, p = 1.0 }\n[[initial.region]]\nshape = \"box\"\n"
                                                              "min = [0.0, 0.0]\nmax = [0.5, 0.5]\nstate = { rho = 0.5, u = 0.3, v = 0.1, p = 0.4 }\n");
@@ -86,6 +96,12 @@ int main(int argc, char** argv) {
         for (auto kv : {std::pair<const char*, const char*>{"nx", "128"}, {"ny", "128"}, {"Lx", "10"}, {"Ly", "10"}, {"reconstruction", "muscl"},
                         {"muscl_limiter", "Van Leer"}, {"time_scheme", "MUSCL-Hancock"}, {"bc_xmin", "periodic"}, {"bc_xmax", "periodic"},
                         {"bc_ymin", "periodic"}, {"bc_ymax", "periodic"}})
+            P.set(kv.first, kv.second);
+    } else if (which == "cylinder") {
+        for (auto kv : {std::pair<const char*, const char*>{"nx", "160"}, {"ny", "240"}, {"Lx", "8"}, {"Ly", "12"}, {"reconstruction", "muscl"},
+                        {"muscl_limiter", "MC"}, {"time_scheme", "MUSCL-Hancock"}, {"bc_xmin", "vel_inlet"}, {"bc_xmax", "transmissive"},
+                        {"bc_ymin", "transmissive"}, {"bc_ymax", "transmissive"}, {"u_in", "2.0"}, {"rho_in", "1.4"}, {"p_out", "1.0"},
+                        {"use_ibm", "true"}, {"ibm_shape", "Cylinder"}, {"ibm_radius", "0.5"}, {"ibm_cx", "3.0"}, {"ibm_cy", "6.0"}})
             P.set(kv.first, kv.second);
     } else if (which == "tgv") {
         for (auto kv : {std::pair<const char*, const char*>{"nx", "32"}, {"ny", "32"}, {"nz", "32"}, {"Lx", "6.283185307179586"},
