@@ -162,6 +162,17 @@ def allmax(x, world):
     return float(t.item())
 
 
+def allsum(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], device="cuda")
+    dist.all_reduce(t)
+    return float(t.item())
+
+
 def barrier(world):
     if world > 1:
         import torch.distributed as dist
@@ -218,6 +229,126 @@ def l1_errors(U, Uref):
         d = np.abs(U[:, q] - Uref[:, q])
         out[name] = {"l1_rel": float(d.sum()) / scale if scale else 0.0,
                      "linf_rel": float(d.max()) / float(np.abs(Uref[:, q]).max()) if scale else 0.0}
+    return out
+
+
+BATCH_T_END = 0.15
+BYTES_PER_CELL_STAGE_2D = (2 + 3 + 3) / 3 * 4 * 8   # SSP-RK3 on a 2-D mesh (4 state planes)
+
+
+BATCH_WORKLOAD = ("512 seeded shock tubes, nx log-uniform in [128, 8192] x 1, rho ~ U[0.1, 1], p ~ U[0.05, 1], u ~ U[-1, 1], "
+                  "WENO5-Z + HLLC + SSP-RK3, CFL 0.4, transmissive, to t = 0.15")
+
+
+def cpu_batch_rate(budget_s):
+    """The reference solver (oracle/_ref) on the host cores over the shock tubes in order, one Simulation each, until
+    budget_s seconds of work: cell-stages per second."""
+    from fenice_b200 import initial
+    from oracle.oracle import Reference
+
+    params, states, _ = initial.shock_tubes(512, seed=0)
+    work, wall, done = 0, 0.0, 0
+    for p, U in zip(params, states):
+        ref = Reference(p, initial_state=(1, 0, 0, 1, 0))
+        ref.set_state(U)
+        t0 = time.perf_counter()
+        n = len(ref.steps(1000000, BATCH_T_END)[0])
+        wall += time.perf_counter() - t0
+        work += n * 3 * p["nx"]
+        done += 1
+        if wall > budget_s:
+            break
+    return work / wall, wall, f"the first {done} of the 512 tubes, each run to t = 0.15 ({work} cell-stages in {wall:.1f} s)"
+
+
+def batch_timed(params, states, precision, schedule, local, timing=False):
+    """One whole batch run to t = 0.15 on a fresh batch, timed with CUDA events on the batch's stream."""
+    import torch
+
+    from fenice_b200 import Batch
+
+    b = Batch(params, states, precision=precision, device=local)
+    b.set_schedule(*schedule)
+    if timing:
+        b.set_timing(True)
+    ext = torch.cuda.ExternalStream(b.stream(), device=torch.device("cuda", local))
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(ext)
+    work = b.run(BATCH_T_END)
+    end.record(ext)
+    torch.cuda.synchronize()
+    return b, start.elapsed_time(end), work
+
+
+def batch_arm(args, world, rank, local):
+    """The batched uneven workload: 512 seeded shock tubes (nx log-uniform in [128, 8192], WENO5-Z + HLLC + SSP-RK3,
+    CFL 0.4) to t = 0.15, all problems of a GPU in one persistent launch per stage under CUDA graphs. With N GPUs the
+    problems are split by cost (no exchange); the time is the slowest GPU's."""
+    import torch
+
+    from fenice_b200 import Batch, initial
+    from fenice_b200.runtime import split_batch
+
+    params, states, _ = initial.shock_tubes(512, seed=0)
+    mine = split_batch(params, world)[rank]
+    params = [params[i] for i in mine]
+    states = [states[i] for i in mine]
+    out = {}
+    for prec, name in ((0, "fp64"), (1, "mixed")):
+        warm = Batch(params, states, precision=prec, device=local)
+        shape, cps, stage_ms = warm.autotune()
+        warm.run(1e30, max_steps=max(args.warmup, 3))
+        warm.close()
+        barrier(world)
+        with Clocks(local) as clk:
+            b, ms, work = batch_timed(params, states, prec, (shape, cps), local)
+        U = b.state()
+        b.close()
+        ms = allmax(ms, world)
+        work_all = allsum(work, world)
+        bt, _, _ = batch_timed(params, states, prec, (shape, cps), local, timing=True)
+        tm = bt.timing()
+        bt.close()
+        sched = {"tile": [[64, 1], [128, 1], [256, 1], [16, 15]][shape], "ctas_per_sm": cps, "autotune_stage_ms": stage_ms}
+        mixed_schedule = (shape, cps)
+        stage_avg = tm["stage_ms"] / max(tm["stage_launches"], 1)
+        # algorithmic bytes of one stage launch, averaged over the run: the cells of the running problems per launch
+        alg = BYTES_PER_CELL_STAGE_2D * work / max(tm["stage_launches"], 1)
+        peak, peak_kind = measured_peak()
+        achieved = alg / (stage_avg * 1e-3) / 1e9
+        out[name] = {"value": work_all / (ms * 1e-3), "ms": ms, "cell_stages": work_all, "schedule": sched, "clocks": clk.summary(),
+                     "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                                  "traffic": None, "peak_source": f"hbm_gbs of MEASURED_PEAKS.json ({peak_kind})",
+                                  "kernel": f"batch_{'mixed' if prec else 'stage'}_kernel<WENO5, HLLC> (persistent, all problems)",
+                                  "stage_launch_ms": round(stage_avg, 4), "stage_launches": tm["stage_launches"],
+                                  "stage_share_of_run": round(tm["stage_ms"] / ms, 4),
+                                  "note": "the three state pools (about 32 MB each) stay in L2: the bound is the FP64 / FP32 pipe, not HBM"}}
+        out[name + "_state"] = U
+    U64, Um = out.pop("fp64_state"), out.pop("mixed_state")
+    offs = np.concatenate([[0], np.cumsum([p["nx"] for p in params])])
+    l1 = [np.abs(Um[a:b_, 0] - U64[a:b_, 0]).sum() / np.abs(U64[a:b_, 0]).sum() for a, b_ in zip(offs[:-1], offs[1:])]
+    out["accuracy"] = {"vs": "the FP64 batch (the reference's arithmetic)", "l1_rho_worst": float(max(l1)), "l1_rho_median": float(np.median(l1)),
+                       "l1_rho_bar": 1e-4, "within_bar": bool(max(l1) <= 1e-4)}
+    out["speedup_of_mixed"] = out["mixed"]["value"] / out["fp64"]["value"]
+    # end to end through the public API (mixed form): upload from pinned host memory, the whole run, download
+    if args.e2e_steps > 0:
+        host = torch.empty((int(offs[-1]), 5), dtype=torch.float64, pin_memory=True).numpy()
+        host[:] = np.concatenate(states)
+        b = Batch(params, None, precision=1, device=local)
+        b.set_schedule(*mixed_schedule)
+        barrier(world)
+        t0 = time.perf_counter()
+        b.set_state(host)
+        work = b.run(BATCH_T_END)
+        host[:] = b.state()
+        wall = allmax(time.perf_counter() - t0, world)
+        b.close()
+        out["e2e"] = {"value": allsum(work, world) / wall, "unit": UNIT,
+                      "h2d_bytes_per_step": int(offs[-1]) * 40, "d2h_bytes_per_step": int(offs[-1]) * 40,
+                      "timing": "host wall clock around upload + whole run + download (one step = the whole batch to t = 0.15)"}
+    out["problems"] = len(params)
+    out["cells"] = int(offs[-1])
     return out
 
 
@@ -285,14 +416,26 @@ def main():
     ap.add_argument("--size", type=int, default=256, help="cells per axis (256: the benchmark workload)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-baseline", type=int, default=1, help="time the reference on the host cores (rank 0, N = 1)")
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch"],
+                    help="tgv: the 3-D Taylor-Green vortex (default); batch: 512 shock tubes in one persistent launch per stage")
+    ap.add_argument("--batch", type=int, default=1, help="with --workload tgv at N = 1: add the batched workload's figures")
     args = ap.parse_args()
     world, rank, local = (1, 0, 0) if args.impl == "reference" and int(os.environ.get("WORLD_SIZE", "1")) == 1 else dist_setup()
     threads = len(os.sched_getaffinity(0))
     if args.impl == "reference":
         if rank != 0:
             return
-        warm, timed = min(args.warmup, 1), max(1, min(args.steps, 3))
         os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+        if args.workload == "batch":
+            rate, wall, sample = cpu_batch_rate(20.0)
+            line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": 1e3 * wall,
+                    "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "impl": "reference",
+                    "data": "synthetic (seeded shock tubes)", "config": {"workload": BATCH_WORKLOAD},
+                    "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+                    "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            print(json.dumps(line), flush=True)
+            return
+        warm, timed = min(args.warmup, 1), max(1, min(args.steps, 3))
         rate, wall, done = cpu_reference_rate(args.size, warm, timed)
         sample = f"{done} SSP-RK3 step(s) of the {args.size}^3 mesh after {warm} untimed, {threads} OpenMP threads"
         line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": done, "warmup": warm,
@@ -304,7 +447,32 @@ def main():
                 "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
+    if args.workload == "batch":
+        b = batch_arm(args, world, rank, local)
+        m = b["mixed"]
+        line = {"metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world, "steps": 1, "warmup": args.warmup,
+                "ms_per_step": m["ms"], "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                "dtype": "f32 stencil / f64 state (mixed form); plain form f64", "data": "synthetic (seeded shock tubes)",
+                "config": {"workload": BATCH_WORKLOAD + "; value: the mixed-precision batch; fp64: the reference's arithmetic",
+                           "problems": b["problems"], "cells": b["cells"], "parallelism": f"problems split by cost over {world} GPUs" if world > 1 else "single GPU",
+                           "l2": "the state pools fit in L2 (no flush; one step is the whole run)"},
+                "roofline": m["roofline"], "clocks": m["clocks"], "e2e": b.get("e2e"), "accuracy": b["accuracy"], "fp64": b["fp64"],
+                "speedup_of_mixed": b["speedup_of_mixed"], "gpu_launches": None}
+        if rank == 0 and world == 1 and args.cpu_baseline:
+            os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+            rate, wall, sample = cpu_batch_rate(12.0)
+            line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
     line = gpu_arm(args, world, rank, local)
+    if world == 1 and args.batch:
+        line["batch"] = batch_arm(args, world, rank, local)
+        line["batch"]["workload"] = BATCH_WORKLOAD
     if rank == 0 and world == 1 and args.cpu_baseline:
         os.environ.setdefault("OMP_NUM_THREADS", str(threads))
         try:

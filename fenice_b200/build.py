@@ -7,6 +7,7 @@ flags are part of the numerics: --fmad=false keeps every multiply and add separa
 with -ffp-contract=off), and double division and square root are IEEE-rounded, so the FP64 kernels give the
 reference's bits.
 """
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -17,8 +18,8 @@ SRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfenice_gpu.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["runtime.cu", "mixed.cu"]
-HEADERS = ["physics.cuh", "grid.cuh", "stage.cuh", "viscous.cuh", "hancock.cuh", "mixed.cuh", "mixed_api.h"]
+SOURCES = ["runtime.cu", "mixed.cu", "batch.cu", "batch_mixed.cu"]
+HEADERS = ["physics.cuh", "grid.cuh", "stage.cuh", "viscous.cuh", "hancock.cuh", "mixed.cuh", "mixed_api.h", "batch.cuh", "batch_api.h", "host_common.h", "ibm.cuh", "ibm_host.h"]
 
 COMMON_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -31,6 +32,8 @@ COMMON_FLAGS = [
 UNIT_FLAGS = {
     "runtime.cu": ["--fmad=false", "-prec-div=true", "-prec-sqrt=true"],
     "mixed.cu": ["--use_fast_math"],
+    "batch.cu": ["--fmad=false", "-prec-div=true", "-prec-sqrt=true"],
+    "batch_mixed.cu": ["--use_fast_math"],
 }
 
 
@@ -58,11 +61,12 @@ def build(force=False, verbose=False, extra=()):
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
-    for f in SOURCES:
-        o = os.path.join(objdir, f.replace(".cu", ".o"))
-        _run([NVCC] + COMMON_FLAGS + UNIT_FLAGS[f] + list(extra) + ["-c", os.path.join(SRC, f), "-o", o], verbose)
-        objs.append(o)
+    objs = [os.path.join(objdir, f.replace(".cu", ".o")) for f in SOURCES]
+    cmds = [[NVCC] + COMMON_FLAGS + UNIT_FLAGS[f] + list(extra) + ["-c", os.path.join(SRC, f), "-o", o] for f, o in zip(SOURCES, objs)]
+    # the translation units compile in parallel
+    with concurrent.futures.ThreadPoolExecutor(max_workers=len(cmds)) as pool:
+        for fut in [pool.submit(_run, c, verbose) for c in cmds]:
+            fut.result()
     _run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "--cudart", "static", "-shared", "-o", LIB] + objs, verbose)
     return LIB
 

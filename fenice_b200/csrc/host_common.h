@@ -1,0 +1,15 @@
+// Host-side helpers of the single runs (runtime.cu) that the batched runs (batch.cu) share.
+#pragma once
+
+#include "../../include/fenice_gpu.h"
+
+#include <string>
+
+namespace fvg {
+// why a configuration cannot run on the device ("" when it can)
+std::string config_error(const fvg_config& c);
+// the halo kind (kHalo*) of each side for a reconstruction `depth` cells deep
+void config_halo_kinds(const fvg_config& c, int depth, int kinds[6]);
+// the message fvg_create_error() returns (this thread's)
+std::string* create_error_slot();
+}   // namespace fvg

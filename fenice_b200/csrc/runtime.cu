@@ -19,6 +19,7 @@
 #include "../../include/fenice_gpu.h"
 #include "hancock.cuh"
 #include "ibm.cuh"
+#include "host_common.h"
 #include "ibm_host.h"
 #include "mixed_api.h"
 #include "stage.cuh"
@@ -526,6 +527,11 @@ int read_ctl(fvg_run* run, Ctl* h) {
 }
 
 }   // namespace
+
+// configuration checks shared with the batched runs (batch.cu)
+std::string fvg::config_error(const fvg_config& c) { return validate(c); }
+void fvg::config_halo_kinds(const fvg_config& c, int depth, int kinds[6]) { halo_kinds(c, depth, kinds); }
+std::string* fvg::create_error_slot() { return &g_create_error; }
 
 // ------------------------------------------------------------------------------------------------ C ABI
 extern "C" {

@@ -29,7 +29,10 @@ EXPORTS = ["fvg_abi_version", "fvg_create", "fvg_destroy", "fvg_last_error", "fv
            "fvg_download_state", "fvg_residual", "fvg_step", "fvg_run_until", "fvg_get_time", "fvg_set_time",
            "fvg_get_lagged_speed", "fvg_set_lagged_speed", "fvg_dt_length", "fvg_device_state", "fvg_stream",
            "fvg_synchronize", "fvg_face_flux_batch", "fvg_set_timing", "fvg_get_timing",
-           "fvg_residual_noalloc"]
+           "fvg_residual_noalloc",
+           "fvg_batch_create", "fvg_batch_destroy", "fvg_batch_last_error", "fvg_batch_cells", "fvg_batch_upload",
+           "fvg_batch_download", "fvg_batch_run", "fvg_batch_problem", "fvg_batch_autotune", "fvg_batch_set_schedule",
+           "fvg_batch_get_schedule", "fvg_batch_stream", "fvg_batch_set_timing", "fvg_batch_get_timing"]
 
 _lib = None
 
@@ -68,6 +71,22 @@ def load_library(path=LIB_PATH):
     lib.fvg_set_timing.argtypes = [c_p, ctypes.c_int]
     ll = ctypes.POINTER(ctypes.c_longlong)
     lib.fvg_get_timing.argtypes = [c_p, dp, ll, dp, ll]
+    ip = ctypes.POINTER(ctypes.c_int)
+    lib.fvg_batch_create.argtypes = [ctypes.POINTER(P.FvgConfig), ctypes.c_int, ctypes.POINTER(c_p)]
+    lib.fvg_batch_destroy.argtypes = [c_p]
+    lib.fvg_batch_last_error.argtypes = [c_p]
+    lib.fvg_batch_last_error.restype = ctypes.c_char_p
+    lib.fvg_batch_cells.argtypes = [c_p, ll]
+    lib.fvg_batch_upload.argtypes = [c_p, dp, ctypes.c_size_t]
+    lib.fvg_batch_download.argtypes = [c_p, dp, ctypes.c_size_t]
+    lib.fvg_batch_run.argtypes = [c_p, ctypes.c_double, ctypes.c_int, ll]
+    lib.fvg_batch_problem.argtypes = [c_p, ctypes.c_int, dp, ip, ip]
+    lib.fvg_batch_autotune.argtypes = [c_p, ip, ip, dp]
+    lib.fvg_batch_set_schedule.argtypes = [c_p, ctypes.c_int, ctypes.c_int]
+    lib.fvg_batch_get_schedule.argtypes = [c_p, ip, ip, ip, ip]
+    lib.fvg_batch_stream.argtypes = [c_p, ctypes.POINTER(c_p)]
+    lib.fvg_batch_set_timing.argtypes = [c_p, ctypes.c_int]
+    lib.fvg_batch_get_timing.argtypes = [c_p, dp, ll]
     _lib = lib
     return lib
 
@@ -202,3 +221,127 @@ class Run:
         self._check(self.lib.fvg_face_flux_batch(self.h, _dp(UL), _dp(UR), ax.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n, _dp(F), _dp(S)),
                     "face_flux_batch")
         return F, S
+
+
+BatchProblem = namedtuple("BatchProblem", ["t", "steps", "status"])
+
+
+def batch_cost(params):
+    """Relative cost of a problem: cells x steps, with steps proportional to 1 / (cfl L), L = min(dx, dy)."""
+    p = P.resolve(params)
+    nx, ny = int(p["nx"]), int(p["ny"])
+    L = min(float(p["Lx"]) / nx, float(p["Ly"]) / ny)
+    return nx * ny / (float(p["cfl"]) * L)
+
+
+def split_batch(params_list, parts):
+    """Problem indices for each of `parts` GPUs: longest-processing-time-first by batch_cost, so the most loaded GPU
+    carries as little as the greedy rule gets it (the batch has no exchange between problems)."""
+    cost = [batch_cost(p) for p in params_list]
+    load = [0.0] * parts
+    out = [[] for _ in range(parts)]
+    for i in sorted(range(len(cost)), key=lambda k: (-cost[k], k)):
+        r = min(range(parts), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += cost[i]
+    return [sorted(o) for o in out]
+
+
+class Batch:
+    """Independent 2-D problems of uneven sizes advanced together on one GPU (fvg_batch_*): one persistent launch per
+    Runge-Kutta stage for all of them, each problem with its own clock, dt and step count, each getting the bits its
+    single ``Run`` gives. ``params_list`` holds one parameter dict per problem (reference keys); the problems share the
+    scheme. States are (sum of cells, 5) float64 arrays: problem 0's cells, then problem 1's, ..."""
+
+    def __init__(self, params_list, states=None, precision=0, device=0):
+        self.lib = load_library()
+        self.params = [P.resolve(p) for p in params_list]
+        n = len(self.params)
+        cfgs = (P.FvgConfig * n)(*[P.to_config(p, precision=precision, device=device) for p in self.params])
+        self.cfgs = cfgs
+        h = ctypes.c_void_p()
+        rc = self.lib.fvg_batch_create(cfgs, n, ctypes.byref(h))
+        if rc != FVG_OK:
+            msg = self.lib.fvg_create_error().decode()
+            raise (ValueError if rc == FVG_ERR_CONFIG else RuntimeError)(f"fvg_batch_create: {msg}")
+        self.h = h
+        self.n = n
+        self.cells = [c.nx * c.ny for c in cfgs]
+        self.offsets = np.concatenate([[0], np.cumsum(self.cells)]).astype(np.int64)
+        self.ncells = int(self.offsets[-1])
+        self.stages = P.STAGES[cfgs[0].time_scheme]
+        if states is not None:
+            self.set_state(np.concatenate(states) if isinstance(states, (list, tuple)) else states)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.fvg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc == FVG_OK:
+            return
+        msg = self.lib.fvg_batch_last_error(self.h).decode()
+        if rc in (FVG_ERR_CONFIG, FVG_ERR_ARGUMENT, FVG_ERR_STATE):
+            raise ValueError(f"{what}: {msg}")
+        raise RuntimeError(f"{what}: {msg}")
+
+    def set_state(self, U):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        if U.shape != (self.ncells, 5):
+            raise ValueError(f"state must be ({self.ncells}, 5), got {U.shape}")
+        self._check(self.lib.fvg_batch_upload(self.h, _dp(U), self.ncells), "upload")
+
+    def state(self):
+        U = np.empty((self.ncells, 5))
+        self._check(self.lib.fvg_batch_download(self.h, _dp(U), self.ncells), "download")
+        return U
+
+    def split(self, U):
+        """The per-problem views of a batch state array."""
+        return [U[self.offsets[p]:self.offsets[p + 1]] for p in range(self.n)]
+
+    def run(self, t_end, max_steps=0, check=True):
+        """Every problem to t_end (or max_steps steps); returns the cell-stages done. A diverged problem raises
+        RuntimeError after the others finished (check=False: no raise; see problem(i).status)."""
+        w = ctypes.c_longlong()
+        rc = self.lib.fvg_batch_run(self.h, float(t_end), int(max_steps), ctypes.byref(w))
+        if check or rc != FVG_ERR_DIVERGED:
+            self._check(rc, "run")
+        return w.value
+
+    def problem(self, i):
+        t, s, st = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.fvg_batch_problem(self.h, int(i), ctypes.byref(t), ctypes.byref(s), ctypes.byref(st)), "problem")
+        return BatchProblem(t.value, s.value, st.value)
+
+    def autotune(self):
+        """Picks the tile shape and persistent grid (fvg_batch_autotune); returns (shape, ctas_per_sm, stage_ms)."""
+        s, c, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        self._check(self.lib.fvg_batch_autotune(self.h, ctypes.byref(s), ctypes.byref(c), ctypes.byref(ms)), "autotune")
+        return s.value, c.value, ms.value
+
+    def set_schedule(self, shape, ctas_per_sm=0):
+        self._check(self.lib.fvg_batch_set_schedule(self.h, int(shape), int(ctas_per_sm)), "set_schedule")
+
+    def schedule(self):
+        """{shape, tile_x, tile_y, grid} (shape -1: not chosen yet)"""
+        v = [ctypes.c_int() for _ in range(4)]
+        self._check(self.lib.fvg_batch_get_schedule(self.h, *[ctypes.byref(x) for x in v]), "get_schedule")
+        return dict(zip(["shape", "tile_x", "tile_y", "grid"], [x.value for x in v]))
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        self._check(self.lib.fvg_batch_stream(self.h, ctypes.byref(s)), "stream")
+        return s.value
+
+    def set_timing(self, on=True):
+        self._check(self.lib.fvg_batch_set_timing(self.h, 1 if on else 0), "set_timing")
+
+    def timing(self):
+        a, b = ctypes.c_double(), ctypes.c_longlong()
+        self._check(self.lib.fvg_batch_get_timing(self.h, ctypes.byref(a), ctypes.byref(b)), "get_timing")
+        return {"stage_ms": a.value, "stage_launches": b.value}

@@ -144,6 +144,41 @@ int fvg_face_flux_batch(fvg_run* run, const double* UL, const double* UR, const 
  * and must be serialised by the caller. On failure, fvg_create_error() returns this thread's message. */
 int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long long plane, double* R, double* smax, void* stream);
 
+/* ---- Batched independent problems (no counterpart in the reference, which runs one Simulation per process).
+ *
+ * n 2-D problems (nz = 1) of uneven sizes advance together, each with its own clock, dt and step count, as if each
+ * were a run of its own: every problem's states, dt and wave speeds are the bits fvg_create + fvg_run_until give it.
+ * The problems share the scheme (reconstruction, Riemann solver, time scheme Euler / SSP-RK2 / SSP-RK3, precision,
+ * device) and may differ in everything else of fvg_config that a 2-D inviscid run without an immersed body uses
+ * (mesh, lengths, gas, boundary conditions, limiter, cfl, dt_max). Each Runge-Kutta stage of all problems is one
+ * persistent kernel launch over the tiles of the problems still running; a step's launches are captured in a CUDA graph.
+ * States cross the ABI as one array: problem 0's cells, then problem 1's, ... (each in the single-run layout). */
+typedef struct fvg_batch fvg_batch;
+int fvg_batch_create(const fvg_config* cfgs, int n, fvg_batch** out);   /* failures: fvg_create_error() */
+int fvg_batch_destroy(fvg_batch* b);
+const char* fvg_batch_last_error(const fvg_batch* b);
+/* the cells of all problems (the length of the state arrays below, in cells of 5 doubles) */
+int fvg_batch_cells(const fvg_batch* b, long long* ncells);
+int fvg_batch_upload(fvg_batch* b, const double* U, size_t ncells);
+int fvg_batch_download(fvg_batch* b, double* U, size_t ncells);
+/* Every problem steps from t = 0 until t >= t_end or max_steps steps (max_steps <= 0: no limit). *cell_stages (may be
+ * NULL) gets the work done: the sum over problems of cells x stages per step x steps. A problem whose solution
+ * diverges stops (its status 1) while the others run on; the call then returns FVG_ERR_DIVERGED. Without a schedule
+ * set, the first call runs fvg_batch_autotune. */
+int fvg_batch_run(fvg_batch* b, double t_end, int max_steps, long long* cell_stages);
+/* problem i after a run: its time, steps taken and status (0 ok, 1 diverged) */
+int fvg_batch_problem(const fvg_batch* b, int i, double* t, int* steps, int* status);
+/* Autotuner: times one stage of every problem for each tile shape the library has (64x1, 128x1, 256x1, 16x15 cells)
+ * and each persistent grid (1 .. the CTAs an SM holds, per SM) and keeps the fastest; returns the choice and its
+ * stage time in ms. fvg_batch_set_schedule sets one by hand (ctas_per_sm 0: as many as an SM holds). */
+int fvg_batch_autotune(fvg_batch* b, int* shape, int* ctas_per_sm, double* stage_ms);
+int fvg_batch_set_schedule(fvg_batch* b, int shape, int ctas_per_sm);
+int fvg_batch_get_schedule(const fvg_batch* b, int* shape, int* tile_x, int* tile_y, int* grid);
+int fvg_batch_stream(fvg_batch* b, void** stream);
+/* Kernel timing of the batched stage kernel, as fvg_set_timing / fvg_get_timing for a single run. */
+int fvg_batch_set_timing(fvg_batch* b, int on);
+int fvg_batch_get_timing(const fvg_batch* b, double* stage_ms, long long* stage_launches);
+
 #ifdef __cplusplus
 }
 #endif

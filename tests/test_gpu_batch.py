@@ -1,0 +1,149 @@
+"""Batched independent problems on the GPU (fvg_batch_*): every problem of a batch gets the bits of its own single run
+(states, time, step count), whatever tile shape and persistent grid the schedule uses; the seeded shock-tube batch (512
+problems, nx log-uniform in [128, 8192], WENO5-Z + HLLC + SSP-RK3 to t = 0.15) against the exact Riemann solution; the
+reference run alongside on two tubes (when oracle/_ref is built); and the mixed-precision batch within the L1 bar."""
+import numpy as np
+import pytest
+
+from fenice_b200 import Batch, Run, initial
+from oracle.exact_riemann import riemann
+from oracle.oracle import Reference, ref_available
+
+pytestmark = pytest.mark.gpu
+
+T_END = 0.15
+
+
+def bits_equal(a, b):
+    return np.array_equal(np.ascontiguousarray(a).view(np.uint64), np.ascontiguousarray(b).view(np.uint64))
+
+
+def single(params, U, precision=0):
+    run = Run(params, U=U, precision=precision)
+    steps = run.run(T_END)
+    return run.state(), run.t, steps
+
+
+@pytest.fixture(scope="module")
+def small():
+    """24 tubes, nx in [128, 1024]."""
+    return initial.shock_tubes(24, seed=11, nx_max=1024)
+
+
+@pytest.mark.parametrize("shape", [0, 1, 2, 3])
+def test_batch_matches_single_runs_bit_for_bit(small, shape):
+    params, states, _ = small
+    b = Batch(params, states)
+    b.set_schedule(shape, 0 if shape != 1 else 1)
+    work = b.run(T_END)
+    out = b.split(b.state())
+    total = 0
+    for p, (prm, U0) in enumerate(zip(params, states)):
+        U, t, steps = single(prm, U0)
+        pb = b.problem(p)
+        assert pb.status == 0 and pb.steps == steps and pb.t == t, (p, pb, steps, t)
+        assert bits_equal(out[p], U), p
+        total += steps * 3 * prm["nx"]
+    assert work == total
+
+
+def test_autotuner_picks_a_schedule_and_runs_continue(small):
+    params, states, _ = small
+    b = Batch(params, states)
+    shape, cps, ms = b.autotune()
+    sch = b.schedule()
+    assert sch["shape"] == shape and 0 <= shape < 4 and cps >= 1 and ms > 0
+    assert sch["grid"] % cps == 0
+    # a second call continues every problem's clock, as fvg_run_until does for a single run
+    b.run(T_END / 2)
+    b.run(T_END)
+    run = Run(params[0], U=states[0])
+    run.run(T_END / 2)
+    run.run(T_END)
+    assert b.problem(0).t == run.t == T_END
+    assert bits_equal(b.split(b.state())[0], run.state())
+
+
+def test_max_steps_and_per_problem_clocks(small):
+    params, states, _ = small
+    b = Batch(params, states)
+    b.run(T_END, max_steps=7)
+    for p in range(b.n):
+        assert b.problem(p).steps == 7
+    run = Run(params[3], U=states[3])
+    run.run(T_END, max_steps=7)
+    assert b.problem(3).t == run.t
+    assert bits_equal(b.split(b.state())[3], run.state())
+
+
+@pytest.fixture(scope="module")
+def c4():
+    params, states, lr = initial.shock_tubes(512, seed=0)
+    b = Batch(params, states)
+    b.autotune()
+    work = b.run(T_END)
+    return params, states, lr, b, b.split(b.state()), work
+
+
+def test_c4_shock_tubes_against_the_exact_solution(c4):
+    params, states, lr, b, out, work = c4
+    errs = []
+    for p, (prm, U, (left, right)) in enumerate(zip(params, out, lr)):
+        assert b.problem(p).t == T_END and b.problem(p).status == 0
+        nx = prm["nx"]
+        x = (np.arange(nx) + 0.5) / nx
+        rho, _, _ = riemann(x, T_END, left, right)
+        errs.append(np.abs(U[:, 0] - rho).mean() / np.abs(rho).mean())
+    errs = np.array(errs)
+    nx = np.array([p["nx"] for p in params])
+    print(f"\nC4: {work} cell-stages; L1(rho) vs exact: median {np.median(errs):.2e}, max {errs.max():.2e} (nx {nx[errs.argmax()]}); "
+          f"max L1 sqrt(nx) {(errs * np.sqrt(nx)).max():.3f}")
+    # the error sits at the discontinuities and the rarefaction corners; a contact spreads over a width that shrinks
+    # more slowly than 1 / nx, so the bound is on L1 sqrt(nx)
+    assert np.all(errs * np.sqrt(nx) < 1.0), (errs * np.sqrt(nx)).max()
+    assert errs.max() < 0.05 and np.median(errs) < 5e-3
+
+
+def test_c4_sample_matches_single_runs(c4):
+    params, states, lr, b, out, work = c4
+    nx = np.array([p["nx"] for p in params])
+    pick = sorted(set(np.random.default_rng(5).choice(len(params), 12, replace=False).tolist()) | {int(nx.argmax()), int(nx.argmin())})
+    for p in pick:
+        U, t, steps = single(params[p], states[p])
+        assert b.problem(p).steps == steps and b.problem(p).t == t
+        assert bits_equal(out[p], U), p
+
+
+@pytest.mark.skipif(not ref_available(), reason="the reference is not compiled (oracle/_ref)")
+def test_tubes_against_the_reference():
+    params, states, _ = initial.shock_tubes(2, seed=3, nx_max=400)
+    b = Batch(params, states)
+    b.run(T_END)
+    out = b.split(b.state())
+    for p in range(2):
+        ref = Reference(params[p], initial_state=(1, 0, 0, 1, 0))
+        ref.set_state(states[p])
+        dts, _ = ref.steps(100000, T_END)
+        assert b.problem(p).steps == len(dts)
+        assert bits_equal(out[p], ref.state()), p
+
+
+def test_mixed_batch(small):
+    params, states, _ = small
+    bm = Batch(params, states, precision=1)
+    bm.run(T_END)
+    b64 = Batch(params, states)
+    b64.run(T_END)
+    Um, U64 = bm.split(bm.state()), b64.split(b64.state())
+    worst = 0.0
+    for p in range(len(params)):
+        l1 = np.abs(Um[p][:, 0] - U64[p][:, 0]).sum() / np.abs(U64[p][:, 0]).sum()
+        worst = max(worst, l1)
+    print(f"\nmixed batch vs FP64 batch: worst L1(rho) {worst:.2e}")
+    assert worst <= 1e-4
+    # the mixed batch against the mixed single run of one problem
+    run = Run(params[5], U=states[5], precision=1)
+    run.run(T_END)
+    d = np.abs(Um[5] - run.state()).max()
+    print(f"mixed batch vs mixed single run, problem 5: max |diff| {d:.2e}")
+    assert d <= 1e-6 * np.abs(run.state()).max()
