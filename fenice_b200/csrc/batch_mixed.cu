@@ -7,6 +7,48 @@
 namespace fvg {
 namespace {
 
+// the thin y sweep of batch.cuh in the mixed form: the boundary-face states in FP64 (side_states), their primitives
+// rounded to FP32, the Riemann solver and the balance in FP32 (as mixed_axis does for boundary faces)
+template <int RIEMANN>
+__device__ __forceinline__ float thin_face_mixed(const StageArgs& a, const Eos<float>& ef, float sb, int side, int i, St<float, 4>& F) {
+    St<double, 4> UL, UR;
+    side_states<4>(a.m, a.bc, a.eos, a.U, side, i, 0, 0, UL, UR);
+    const St<double, 4> dl = c2p(a.eos, UL), dr = c2p(a.eos, UR);
+    St<float, 4> wl, wr;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        wl[q] = (float)dl[q];
+        wr[q] = (float)dr[q];
+    }
+    return face_flux_prim<RIEMANN>(ef, sb, wl, wr, 1, F);
+}
+
+template <int RIEMANN, int TX, int NT>
+__device__ __forceinline__ void thin_y_mixed(const StageArgs& a, const Eos<float>& ef, float sb, float* __restrict__ acc, const int o3[3], float& smax) {
+    const Mesh& m = a.m;
+    const float A = (float)m.area[1];
+    const bool same = copy_side(a.bc.type[2]) && copy_side(a.bc.type[3]);
+    for (int c = threadIdx.x; c < TX; c += NT) {
+        const int i = o3[0] + c;
+        if (i >= m.nx) continue;
+        St<float, 4> Fb, Ft;
+        const float s_b = thin_face_mixed<RIEMANN>(a, ef, sb, 2, i, Fb);
+        float s_t = s_b;
+        if (same)
+            Ft = Fb;
+        else
+            s_t = thin_face_mixed<RIEMANN>(a, ef, sb, 3, i, Ft);
+        if (s_b > smax) smax = s_b;
+        if (s_t > smax) smax = s_t;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float d = (Ft[q] - Fb[q]) * A;
+            acc[q * TX + c] = acc[q * TX + c] - d;
+        }
+    }
+    __syncthreads();
+}
+
 template <int RECON, int RIEMANN, int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT) batch_mixed_kernel(const BatchArgs b) {
     using S = MixedShape<2, RECON, TX, TY, 1>;
@@ -32,7 +74,12 @@ __global__ void __launch_bounds__(NT) batch_mixed_kernel(const BatchArgs b) {
         const int o3[3] = {(it.tile % tx) * TX, (it.tile / tx) * TY, 0};
         float smax = 0.0f;
         mixed_axis<0, 2, RECON, RIEMANN, TX, TY, 1, NT>(sa, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
-        mixed_axis<1, 2, RECON, RIEMANN, TX, TY, 1, NT>(sa, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
+        bool thin = false;
+        if constexpr (TY == 1) thin = thin_y(m, sa.bc);
+        if (thin)
+            thin_y_mixed<RIEMANN, TX, NT>(sa, ef, sb, acc, o3, smax);
+        else
+            mixed_axis<1, 2, RECON, RIEMANN, TX, TY, 1, NT>(sa, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
         const double dt = b.ctl[it.prob].dt;
         for (int c = tid; c < NC; c += NT) {
             const int i = o3[0] + c % TX, j = o3[1] + c / TX;
