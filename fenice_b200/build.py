@@ -18,8 +18,8 @@ SRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfenice_gpu.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["runtime.cu", "mixed.cu", "batch.cu", "batch_mixed.cu"]
-HEADERS = ["physics.cuh", "grid.cuh", "stage.cuh", "viscous.cuh", "hancock.cuh", "mixed.cuh", "mixed_api.h", "batch.cuh", "batch_api.h", "host_common.h", "ibm.cuh", "ibm_host.h"]
+SOURCES = ["runtime.cu", "mixed.cu", "batch.cu", "batch_mixed.cu", "sensor.cu"]
+HEADERS = ["physics.cuh", "grid.cuh", "stage.cuh", "viscous.cuh", "hancock.cuh", "mixed.cuh", "mixed_api.h", "batch.cuh", "batch_api.h", "host_common.h", "ibm.cuh", "ibm_host.h", "sensor.cuh"]
 
 COMMON_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -34,6 +34,7 @@ UNIT_FLAGS = {
     "mixed.cu": ["--use_fast_math"],
     "batch.cu": ["--fmad=false", "-prec-div=true", "-prec-sqrt=true"],
     "batch_mixed.cu": ["--use_fast_math"],
+    "sensor.cu": ["--use_fast_math"],
 }
 
 

@@ -23,6 +23,20 @@ template <int DIM, int RECON, int RIEMANN> struct MixedK {
     }
 };
 
+// the WENO5-Z kernels gated by the learned sensor
+template <int DIM, int RIEMANN> struct GatedK {
+    using T = MTile<DIM>;
+    using S = MixedShape<DIM, kWeno5, T::X, T::Y, T::Z>;
+    static cudaError_t prepare() {
+        return cudaFuncSetAttribute(mixed_stage_kernel<DIM, kWeno5, RIEMANN, T::X, T::Y, T::Z, T::NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)S::GATED_BYTES);
+    }
+    static cudaError_t launch(const StageArgs& a, int nblocks, cudaStream_t s) {
+        mixed_stage_kernel<DIM, kWeno5, RIEMANN, T::X, T::Y, T::Z, T::NT, true><<<nblocks, T::NT, S::GATED_BYTES, s>>>(a);
+        return cudaGetLastError();
+    }
+};
+
 template <int DIM, int RECON> MixedStage pick_r(int riemann) {
     if (riemann == kLowMach) return {MixedK<DIM, RECON, kLowMach>::prepare, MixedK<DIM, RECON, kLowMach>::launch};
     return {MixedK<DIM, RECON, kHLLC>::prepare, MixedK<DIM, RECON, kHLLC>::launch};
@@ -38,6 +52,13 @@ template <int DIM> MixedStage pick(int recon, int riemann) {
 }   // namespace
 
 MixedStage mixed_stage(int dim, int recon, int riemann) { return dim == 3 ? pick<3>(recon, riemann) : pick<2>(recon, riemann); }
+
+MixedStage mixed_stage_gated(int dim, int riemann) {
+    if (dim == 3) return riemann == kLowMach ? MixedStage{GatedK<3, kLowMach>::prepare, GatedK<3, kLowMach>::launch}
+                                             : MixedStage{GatedK<3, kHLLC>::prepare, GatedK<3, kHLLC>::launch};
+    return riemann == kLowMach ? MixedStage{GatedK<2, kLowMach>::prepare, GatedK<2, kLowMach>::launch}
+                               : MixedStage{GatedK<2, kHLLC>::prepare, GatedK<2, kHLLC>::launch};
+}
 
 cudaError_t mixed_viscous_prepare() {
     return cudaFuncSetAttribute(mixed_viscous_kernel<8, 8, 8, 192>, cudaFuncAttributeMaxDynamicSharedMemorySize,

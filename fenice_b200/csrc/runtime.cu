@@ -22,6 +22,7 @@
 #include "host_common.h"
 #include "ibm_host.h"
 #include "mixed_api.h"
+#include "sensor.cuh"
 #include "stage.cuh"
 #include "viscous.cuh"
 
@@ -261,6 +262,10 @@ struct fvg_run {
     unsigned char* d_mask = nullptr;
     int *d_slot = nullptr, *d_ghost = nullptr, *d_img_cell = nullptr, *d_deep = nullptr;
     double *d_forced = nullptr, *d_img_w = nullptr, *d_ratio = nullptr, *d_gn = nullptr;
+    // the learned sensor (fvg_set_sensor): its weights (a copy), the logit threshold, the counters
+    void* sens = nullptr;
+    float sens_theta = 0.0f;
+    unsigned long long* sens_count = nullptr;
     double* Ucur() { return cur ? Ut : U; }
 };
 
@@ -348,6 +353,9 @@ StageArgs stage_args(fvg_run* r, const double* Uin, const double* U0, double* ou
     a.ctl = r->ctl;
     a.gate = gate;
     for (int d = 0; d < 3; ++d) a.tiles[d] = r->tiles[d];
+    a.sens = static_cast<const SensorW*>(r->sens);
+    a.sens_theta = r->sens_theta;
+    a.sens_count = r->sens_count;
     return a;
 }
 
@@ -532,6 +540,19 @@ int read_ctl(fvg_run* run, Ctl* h) {
 std::string fvg::config_error(const fvg_config& c) { return validate(c); }
 void fvg::config_halo_kinds(const fvg_config& c, int depth, int kinds[6]) { halo_kinds(c, depth, kinds); }
 std::string* fvg::create_error_slot() { return &g_create_error; }
+bool fvg::run_view(fvg_run* run, RunView* v) {
+    if (!run || !v) return false;
+    v->m = run->m;
+    v->bc = run->bc;
+    v->eos = run->eos;
+    v->U = run->Ucur();
+    v->stream = run->stream;
+    v->dim = run->dim;
+    v->nvar = run->nvar;
+    v->device = run->cfg.device;
+    v->weno_eps = run->cfg.weno_epsilon;
+    return true;
+}
 
 // ------------------------------------------------------------------------------------------------ C ABI
 extern "C" {
@@ -709,6 +730,8 @@ int fvg_destroy(fvg_run* run) {
     for (double* p : {run->U, run->Ut, run->R, run->Rv, run->staging, run->bm_seed, run->bm[0], run->bm[1], run->bm[2], run->bmv[0], run->bmv[1], run->bmv[2]})
         if (p) cudaFree(p);
     if (run->ctl) cudaFree(run->ctl);
+    if (run->sens) cudaFree(run->sens);
+    if (run->sens_count) cudaFree(run->sens_count);
     for (void* p : {(void*)run->d_mask, (void*)run->d_slot, (void*)run->d_forced, (void*)run->d_ghost, (void*)run->d_img_cell, (void*)run->d_img_w,
                     (void*)run->d_ratio, (void*)run->d_gn, (void*)run->d_deep})
         if (p) cudaFree(p);
@@ -948,6 +971,55 @@ int fvg_get_timing(const fvg_run* run, double* stage_ms, long long* stage_launch
     if (stage_launches) *stage_launches = run->t_stage.n;
     if (viscous_ms) *viscous_ms = run->t_visc.ms;
     if (viscous_launches) *viscous_launches = run->t_visc.n;
+    return FVG_OK;
+}
+
+int fvg_set_sensor(fvg_run* run, const void* weights, float threshold) {
+    if (!run) return FVG_ERR_ARGUMENT;
+    CK(cudaSetDevice(run->cfg.device));
+    CK(cudaStreamSynchronize(run->stream));
+    for (int g = 0; g < 2; ++g)
+        if (run->graph[g]) {
+            cudaGraphExecDestroy(run->graph[g]);
+            run->graph[g] = nullptr;
+        }
+    if (!weights) {   // back to plain WENO5-Z
+        if (!run->sens) return FVG_OK;
+        const MixedStage ms = mixed_stage(run->dim, run->cfg.reconstruction, run->cfg.riemann);
+        run->stage.prepare = ms.prepare;
+        run->stage.launch = ms.launch;
+        if (run->sens) cudaFree(run->sens);
+        run->sens = nullptr;
+        return FVG_OK;
+    }
+    if (run->cfg.precision != FVG_PREC_MIXED || run->cfg.reconstruction != FVG_RECON_WENO5)
+        return fail(run, FVG_ERR_CONFIG, "the sensor gates the mixed-precision WENO5-Z form");
+    if (run->ibm) return fail(run, FVG_ERR_CONFIG, "the sensor is not built for runs with an immersed body");
+    if (!run->sens) CK(cudaMalloc(&run->sens, sizeof(SensorW)));
+    if (!run->sens_count) {
+        CK(cudaMalloc(&run->sens_count, 2 * sizeof(unsigned long long)));
+        CK(cudaMemset(run->sens_count, 0, 2 * sizeof(unsigned long long)));
+    }
+    CK(cudaMemcpy(run->sens, weights, sizeof(SensorW), cudaMemcpyDefault));
+    const MixedStage ms = mixed_stage_gated(run->dim, run->cfg.riemann);
+    if (ms.prepare() != cudaSuccess) return fail(run, FVG_ERR_CUDA, "kernel set-up failed (shared-memory limit)");
+    run->stage.prepare = ms.prepare;
+    run->stage.launch = ms.launch;
+    run->sens_theta = threshold;
+    return FVG_OK;
+}
+
+int fvg_get_sensor_counts(fvg_run* run, long long* linear, long long* evaluated, int reset) {
+    if (!run) return FVG_ERR_ARGUMENT;
+    unsigned long long h[2] = {0, 0};
+    if (run->sens_count) {
+        CK(cudaSetDevice(run->cfg.device));
+        CK(cudaStreamSynchronize(run->stream));
+        CK(cudaMemcpy(h, run->sens_count, sizeof(h), cudaMemcpyDeviceToHost));
+        if (reset) CK(cudaMemset(run->sens_count, 0, sizeof(h)));
+    }
+    if (linear) *linear = (long long)h[0];
+    if (evaluated) *evaluated = (long long)h[1];
     return FVG_OK;
 }
 

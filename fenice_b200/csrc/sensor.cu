@@ -1,0 +1,430 @@
+// The troubled-cell sensor's kernels and their C ABI (include/fenice_gpu.h: fvg_sensor_*): training data from a run's
+// state, the network's forward and backward passes on the tensor cores, the optimiser step, inference. Built with fast
+// single-precision math, as the mixed-precision stage kernels that evaluate the network inside their tiles.
+#include "../../include/fenice_gpu.h"
+#include "grid.cuh"
+#include "host_common.h"
+#include "sensor.cuh"
+
+#include <cuda_runtime.h>
+
+using namespace fvg;
+
+namespace {
+
+// ------------------------------------------------------------------------------------------------ training data
+__device__ __forceinline__ unsigned hash32(unsigned long long x, unsigned seed) {
+    unsigned h = (unsigned)(x ^ (x >> 32)) * 0x9E3779B1u ^ seed * 0x85EBCA77u;
+    h ^= h >> 15;
+    h *= 0x2C1B3C6Du;
+    h ^= h >> 12;
+    h *= 0x297A2D39u;
+    h ^= h >> 15;
+    return h;
+}
+
+// Features and label statistic of every (cell, axis) of a state. mode 0: all, at index cell * DIM + axis; mode 1: the
+// troubled ones (departure > tau) and every keep_div-th other one (by a hash), appended at an atomic counter up to cap.
+// stats[0] += troubled, stats[1] += all.
+template <int DIM, int NV>
+__global__ void k_sensor_extract(Mesh m, Bc bc, Eos<double> eos, const double* __restrict__ U, double weno_eps, int mode, int keep_div, unsigned seed,
+                                 float tau, float* __restrict__ X, float* __restrict__ dep, int* count, long long cap,
+                                 unsigned long long* stats) {
+    const long long n = m.ncells * DIM;
+    unsigned long long troubled = 0, total = 0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const long long c = e / DIM;
+        const int axis = (int)(e % DIM);
+        const int i = (int)(c % m.nx), j = (int)((c / m.nx) % m.ny), k = (int)(c / ((long long)m.nx * m.ny));
+        double w5[5][NV];
+#pragma unroll
+        for (int s = 0; s < 5; ++s) {
+            const int d = s - 2;
+            const St<double, NV> u = stencil_cons<DIM, NV>(m, bc, eos, U, i + (axis == 0 ? d : 0), j + (axis == 1 ? d : 0), k + (axis == 2 ? d : 0));
+            const St<double, NV> w = c2p(eos, u);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) w5[s][q] = w[q];
+        }
+        float f[kSensF];
+        double D = 0.0;
+#pragma unroll
+        for (int sq = 0; sq < kSensQ; ++sq) {
+            const int var = sensor_var<NV>(sq, axis);
+            float v[5];
+#pragma unroll
+            for (int s = 0; s < 5; ++s) v[s] = var >= 0 ? (float)w5[s][var < 0 ? 0 : var] : 0.0f;
+            sensor_quantity_features(v, f + 5 * sq);
+            if (var >= 0) {
+                double cv[5];
+#pragma unroll
+                for (int s = 0; s < 5; ++s) cv[s] = w5[s][var];
+                D = fmax(D, weno5z_departure(cv[0], cv[1], cv[2], cv[3], cv[4], weno_eps));
+                D = fmax(D, weno5z_departure(cv[4], cv[3], cv[2], cv[1], cv[0], weno_eps));
+            }
+        }
+        const bool bad = D > (double)tau;
+        troubled += bad;
+        total += 1;
+        long long slot = e;
+        if (mode == 1) {
+            if (!bad && (keep_div <= 1 ? false : (hash32((unsigned long long)e, seed) % (unsigned)keep_div) != 0)) continue;
+            slot = atomicAdd(count, 1);
+            if (slot >= cap) continue;
+        }
+        float4* xo = reinterpret_cast<float4*>(X + slot * kSensK);
+#pragma unroll
+        for (int q = 0; q < kSensK / 4; ++q) {
+            float4 v;
+            v.x = 4 * q + 0 < kSensF ? f[4 * q + 0] : 0.0f;
+            v.y = 4 * q + 1 < kSensF ? f[4 * q + 1] : 0.0f;
+            v.z = 4 * q + 2 < kSensF ? f[4 * q + 2] : 0.0f;
+            v.w = 4 * q + 3 < kSensF ? f[4 * q + 3] : 0.0f;
+            xo[q] = v;
+        }
+        dep[slot] = (float)D;
+    }
+    if (stats) {
+        atomicAdd(stats, troubled);
+        atomicAdd(stats + 1, total);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------ training
+constexpr int kLd = 40;   // row stride (bf16) of the per-warp 16 x 32 tiles in shared memory (rows on distinct banks)
+
+// A 16 x 16 row-major A fragment whose element (m, k) is T[k][m0 + m] of a tile T (rows = k): the transpose of a tile.
+__device__ __forceinline__ void load_at_frag(const __nv_bfloat16* T, int m0, uint32_t (&a)[4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    a[0] = pack_bf16_raw(T[(2 * t) * kLd + m0 + g], T[(2 * t + 1) * kLd + m0 + g]);
+    a[1] = pack_bf16_raw(T[(2 * t) * kLd + m0 + g + 8], T[(2 * t + 1) * kLd + m0 + g + 8]);
+    a[2] = pack_bf16_raw(T[(2 * t + 8) * kLd + m0 + g], T[(2 * t + 9) * kLd + m0 + g]);
+    a[3] = pack_bf16_raw(T[(2 * t + 8) * kLd + m0 + g + 8], T[(2 * t + 9) * kLd + m0 + g + 8]);
+}
+// A 16 x 8 col B fragment whose element (k, n) is T[k][n0 + n].
+__device__ __forceinline__ void load_b_frag(const __nv_bfloat16* T, int n0, uint32_t (&b)[2]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    b[0] = pack_bf16_raw(T[(2 * t) * kLd + n0 + g], T[(2 * t + 1) * kLd + n0 + g]);
+    b[1] = pack_bf16_raw(T[(2 * t + 8) * kLd + n0 + g], T[(2 * t + 9) * kLd + n0 + g]);
+}
+// acc[mt][nt] += L^T R over the 16 rows of two tiles: (32 x 16) x (16 x 32) on the tensor cores.
+__device__ __forceinline__ void outer_acc(const __nv_bfloat16* L, const __nv_bfloat16* R, float (&acc)[2][4][4]) {
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+        uint32_t a[4];
+        load_at_frag(L, 16 * mt, a);
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            uint32_t b[2];
+            load_b_frag(R, 8 * nt, b);
+            mma16816(acc[mt][nt], a, b);
+        }
+    }
+}
+// store a C-layout 16 x 32 tile (rows g, g + 8 of the four n-tiles) to shared memory as bf16
+__device__ __forceinline__ void store_c_tile(__nv_bfloat16* T, const float (&v)[4][4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+        *reinterpret_cast<uint32_t*>(T + g * kLd + 8 * nt + 2 * t) = pack_bf16(v[nt][0], v[nt][1]);
+        *reinterpret_cast<uint32_t*>(T + (g + 8) * kLd + 8 * nt + 2 * t) = pack_bf16(v[nt][2], v[nt][3]);
+    }
+}
+__device__ __forceinline__ float group_sum(float v) {   // over the 8 groups (lanes with the same t)
+    v += __shfl_xor_sync(0xffffffffu, v, 4);
+    v += __shfl_xor_sync(0xffffffffu, v, 8);
+    v += __shfl_xor_sync(0xffffffffu, v, 16);
+    return v;
+}
+
+// Gradients of the mean class-weighted binary cross-entropy (weight wpos on troubled samples) over n samples, added
+// to grad (a SensorP of float32) and the loss sum to *loss. Each warp takes 16 samples at a time: forward on the
+// tensor cores, the backward products (hidden gradients x weights, and the weight gradients as sums over the samples
+// of outer products) on the tensor cores too, bfloat16 operands and float32 sums.
+__global__ void __launch_bounds__(256) k_sensor_grad(const SensorW* __restrict__ wg, const float* __restrict__ X, const float* __restrict__ y, long long n,
+                                                     float wpos, float inv_n, float* __restrict__ grad, float* __restrict__ loss) {
+    __shared__ SensorW w;
+    __shared__ float gs[kSensParams];
+    __shared__ __align__(16) __nv_bfloat16 tiles[8][3][16 * kLd];
+    {
+        const int* src = reinterpret_cast<const int*>(wg);
+        int* dst = reinterpret_cast<int*>(&w);
+        for (int i = threadIdx.x; i < (int)(sizeof(SensorW) / 4); i += blockDim.x) dst[i] = src[i];
+        for (int i = threadIdx.x; i < kSensParams; i += blockDim.x) gs[i] = 0.0f;
+    }
+    __syncthreads();
+    SensorP& G = *reinterpret_cast<SensorP*>(gs);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    __nv_bfloat16* Xs = tiles[warp][0];
+    __nv_bfloat16* H1s = tiles[warp][1];
+    __nv_bfloat16* D2s = tiles[warp][2];
+    float gW1[2][4][4] = {}, gW2[2][4][4] = {};
+    float gb1[4][2] = {}, gb2[4][2] = {}, gw3[4][2] = {};
+    float gb3 = 0.0f, lsum = 0.0f;
+    const long long chunks = (n + 15) / 16;
+    for (long long ch = (long long)blockIdx.x * 8 + warp; ch < chunks; ch += (long long)gridDim.x * 8) {
+        const long long r0 = ch * 16;
+        for (int idx = lane; idx < 16 * kSensK; idx += 32) {
+            const int r = idx / kSensK, col = idx % kSensK;
+            Xs[r * kLd + col] = __float2bfloat16_rn(r0 + r < n ? X[(r0 + r) * kSensK + col] : 0.0f);
+        }
+        __syncwarp();
+        // ---- forward
+        uint32_t a[2][4];
+        float h1[4][4], h2[4][4];
+        load_a_frags(Xs, kLd, a);
+        dense32(a, w.W1, h1);
+        relu_to_a(h1, w.b1, a);
+        store_c_tile(H1s, h1);
+        dense32(a, w.W2, h2);
+        relu_to_a(h2, w.b2, a);
+        float zl = 0.0f, zh = 0.0f;
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            const float w0 = w.w3[8 * nt + 2 * t], w1 = w.w3[8 * nt + 2 * t + 1];
+            zl += h2[nt][0] * w0 + h2[nt][1] * w1;
+            zh += h2[nt][2] * w0 + h2[nt][3] * w1;
+        }
+        zl += __shfl_xor_sync(0xffffffffu, zl, 1);
+        zl += __shfl_xor_sync(0xffffffffu, zl, 2);
+        zh += __shfl_xor_sync(0xffffffffu, zh, 1);
+        zh += __shfl_xor_sync(0xffffffffu, zh, 2);
+        zl += w.b3;
+        zh += w.b3;
+        // ---- loss and the logit gradients of rows g and g + 8
+        float dzl = 0.0f, dzh = 0.0f;
+        {
+            const long long rl = r0 + g, rh = r0 + g + 8;
+            const float yl = rl < n ? y[rl] : 0.0f, yh = rh < n ? y[rh] : 0.0f;
+            const float wl = rl < n ? (yl > 0.5f ? wpos : 1.0f) : 0.0f, wh = rh < n ? (yh > 0.5f ? wpos : 1.0f) : 0.0f;
+            const float spl = fmaxf(zl, 0.0f) + log1pf(__expf(-fabsf(zl))), sph = fmaxf(zh, 0.0f) + log1pf(__expf(-fabsf(zh)));
+            dzl = wl * (1.0f / (1.0f + __expf(-zl)) - yl) * inv_n;
+            dzh = wh * (1.0f / (1.0f + __expf(-zh)) - yh) * inv_n;
+            if (t == 0) {
+                lsum += wl * (spl - yl * zl) + wh * (sph - yh * zh);
+                gb3 += dzl + dzh;
+            }
+        }
+        // ---- backward: dh2 = dz w3 (z2 > 0), dh1 = (dh2 W2) (z1 > 0)
+        float d2[4][4];
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+#pragma unroll
+            for (int jj = 0; jj < 2; ++jj) {
+                const float w3v = w.w3[8 * nt + 2 * t + jj];
+                gw3[nt][jj] += dzl * h2[nt][jj] + dzh * h2[nt][jj + 2];
+                d2[nt][jj] = h2[nt][jj] > 0.0f ? dzl * w3v : 0.0f;
+                d2[nt][jj + 2] = h2[nt][jj + 2] > 0.0f ? dzh * w3v : 0.0f;
+                gb2[nt][jj] += d2[nt][jj] + d2[nt][jj + 2];
+            }
+        }
+        store_c_tile(D2s, d2);
+        uint32_t ad[2][4];
+#pragma unroll
+        for (int s2 = 0; s2 < 2; ++s2) {
+            ad[s2][0] = pack_bf16(d2[2 * s2][0], d2[2 * s2][1]);
+            ad[s2][1] = pack_bf16(d2[2 * s2][2], d2[2 * s2][3]);
+            ad[s2][2] = pack_bf16(d2[2 * s2 + 1][0], d2[2 * s2 + 1][1]);
+            ad[s2][3] = pack_bf16(d2[2 * s2 + 1][2], d2[2 * s2 + 1][3]);
+        }
+        float d1[4][4];
+        dense32(ad, w.W2T, d1);
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) d1[nt][q] = h1[nt][q] > 0.0f ? d1[nt][q] : 0.0f;
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            gb1[nt][0] += d1[nt][0] + d1[nt][2];
+            gb1[nt][1] += d1[nt][1] + d1[nt][3];
+        }
+        __syncwarp();
+        // ---- weight gradients: dW2 += dh2^T h1, then dW1 += dh1^T x (dh1 takes the slot of h1)
+        outer_acc(D2s, H1s, gW2);
+        __syncwarp();
+        store_c_tile(H1s, d1);
+        __syncwarp();
+        outer_acc(H1s, Xs, gW1);
+        __syncwarp();
+    }
+    // ---- the warp's sums into the block's, then the block's into grad
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            const int o = 16 * mt + g, i = 8 * nt + 2 * t;
+            atomicAdd(&G.W1[o * kSensK + i], gW1[mt][nt][0]);
+            atomicAdd(&G.W1[o * kSensK + i + 1], gW1[mt][nt][1]);
+            atomicAdd(&G.W1[(o + 8) * kSensK + i], gW1[mt][nt][2]);
+            atomicAdd(&G.W1[(o + 8) * kSensK + i + 1], gW1[mt][nt][3]);
+            atomicAdd(&G.W2[o * kSensH + i], gW2[mt][nt][0]);
+            atomicAdd(&G.W2[o * kSensH + i + 1], gW2[mt][nt][1]);
+            atomicAdd(&G.W2[(o + 8) * kSensH + i], gW2[mt][nt][2]);
+            atomicAdd(&G.W2[(o + 8) * kSensH + i + 1], gW2[mt][nt][3]);
+        }
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+        for (int jj = 0; jj < 2; ++jj) {
+            const float v1 = group_sum(gb1[nt][jj]), v2 = group_sum(gb2[nt][jj]), v3 = group_sum(gw3[nt][jj]);
+            if (g == 0) {
+                atomicAdd(&G.b1[8 * nt + 2 * t + jj], v1);
+                atomicAdd(&G.b2[8 * nt + 2 * t + jj], v2);
+                atomicAdd(&G.w3[8 * nt + 2 * t + jj], v3);
+            }
+        }
+    gb3 = group_sum(gb3);
+    lsum = group_sum(lsum);
+    gb3 += __shfl_xor_sync(0xffffffffu, gb3, 1);
+    gb3 += __shfl_xor_sync(0xffffffffu, gb3, 2);
+    lsum += __shfl_xor_sync(0xffffffffu, lsum, 1);
+    lsum += __shfl_xor_sync(0xffffffffu, lsum, 2);
+    if (lane == 0) {
+        atomicAdd(&G.b3, gb3);
+        atomicAdd(loss, lsum);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kSensParams; i += blockDim.x)
+        if (gs[i] != 0.0f) atomicAdd(&grad[i], gs[i]);
+}
+
+// The device weights (bfloat16 copies, the transposed second layer) of float32 master parameters.
+__device__ void pack_weights(const SensorP& P, SensorW* out) {
+    for (int i = threadIdx.x; i < kSensH * kSensK; i += blockDim.x) out->W1[i] = __float2bfloat16_rn((i % kSensK) < kSensF ? P.W1[i] : 0.0f);
+    for (int i = threadIdx.x; i < kSensH * kSensH; i += blockDim.x) {
+        out->W2[i] = __float2bfloat16_rn(P.W2[i]);
+        out->W2T[(i % kSensH) * kSensH + i / kSensH] = __float2bfloat16_rn(P.W2[i]);
+    }
+    for (int i = threadIdx.x; i < kSensH; i += blockDim.x) {
+        out->b1[i] = P.b1[i];
+        out->b2[i] = P.b2[i];
+        out->w3[i] = round_bf16(P.w3[i]);
+    }
+    if (threadIdx.x == 0) out->b3 = P.b3;
+}
+
+__global__ void k_sensor_pack(const SensorP* P, SensorW* out) { pack_weights(*P, out); }
+
+// One Adam step on the master parameters from grad (then cleared), and their device weights. One CTA.
+__global__ void k_sensor_adam(float* P, float* m, float* v, float* grad, int step, float lr, float b1, float b2, float eps, SensorW* out) {
+    const float c1 = 1.0f / (1.0f - powf(b1, (float)step)), c2 = 1.0f / (1.0f - powf(b2, (float)step));
+    for (int i = threadIdx.x; i < kSensParams; i += blockDim.x) {
+        const float gi = grad[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi, vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        float p = P[i] - lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+        if (i < kSensH * kSensK && (i % kSensK) >= kSensF) p = 0.0f;   // the padding inputs keep zero weights
+        P[i] = p;
+        grad[i] = 0.0f;
+    }
+    __syncthreads();
+    pack_weights(*reinterpret_cast<const SensorP*>(P), out);
+}
+
+// Logits of n feature rows.
+__global__ void __launch_bounds__(256) k_sensor_infer(const SensorW* __restrict__ wg, const float* __restrict__ X, long long n, float* __restrict__ logits) {
+    __shared__ SensorW w;
+    __shared__ __align__(16) __nv_bfloat16 tiles[8][16 * kLd];
+    {
+        const int* src = reinterpret_cast<const int*>(wg);
+        int* dst = reinterpret_cast<int*>(&w);
+        for (int i = threadIdx.x; i < (int)(sizeof(SensorW) / 4); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    __nv_bfloat16* Xs = tiles[warp];
+    const long long chunks = (n + 15) / 16;
+    for (long long ch = (long long)blockIdx.x * 8 + warp; ch < chunks; ch += (long long)gridDim.x * 8) {
+        const long long r0 = ch * 16;
+        for (int idx = lane; idx < 16 * kSensK; idx += 32) {
+            const int r = idx / kSensK, col = idx % kSensK;
+            Xs[r * kLd + col] = __float2bfloat16_rn(r0 + r < n ? X[(r0 + r) * kSensK + col] : 0.0f);
+        }
+        __syncwarp();
+        float lo, hi;
+        sensor_logits(w, Xs, kLd, lo, hi);
+        if (t == 0) {
+            if (r0 + g < n) logits[r0 + g] = lo;
+            if (r0 + g + 8 < n) logits[r0 + g + 8] = hi;
+        }
+        __syncwarp();
+    }
+}
+
+int grid_for(long long rows) {
+    const long long chunks = (rows + 15) / 16, b = (chunks + 7) / 8;
+    return (int)(b < 1 ? 1 : (b > 148 * 4 ? 148 * 4 : b));
+}
+
+}   // namespace
+
+// ------------------------------------------------------------------------------------------------ C ABI
+namespace {
+int serr(int code, const char* msg) {
+    *create_error_slot() = msg;
+    return code;
+}
+#define SK(call)                                                                                \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess) return serr(FVG_ERR_CUDA, cudaGetErrorString(e_));               \
+    } while (0)
+}   // namespace
+
+extern "C" {
+
+int fvg_sensor_sizes(int* n_params, int* weights_bytes, int* n_inputs) {
+    if (n_params) *n_params = kSensParams;
+    if (weights_bytes) *weights_bytes = (int)sizeof(SensorW);
+    if (n_inputs) *n_inputs = kSensK;
+    return FVG_OK;
+}
+
+int fvg_sensor_extract(fvg_run* run, int mode, int keep_div, unsigned seed, float tau, float* X, float* departure, int* count, long long capacity,
+                       unsigned long long* stats) {
+    RunView v;
+    if (!run_view(run, &v) || !X || !departure || (mode == 1 && !count)) return serr(FVG_ERR_ARGUMENT, "null argument");
+    if (mode != 0 && mode != 1) return serr(FVG_ERR_ARGUMENT, "mode must be 0 (all) or 1 (sampled)");
+    if (mode == 0 && capacity < v.m.ncells * v.dim) return serr(FVG_ERR_ARGUMENT, "capacity below cells x axes");
+    SK(cudaSetDevice(v.device));
+    const long long n = v.m.ncells * v.dim;
+    const int blocks = (int)((n + 255) / 256 < 148 * 8 ? (n + 255) / 256 : 148 * 8);
+    if (v.dim == 3)
+        k_sensor_extract<3, 5><<<blocks, 256, 0, v.stream>>>(v.m, v.bc, v.eos, v.U, v.weno_eps, mode, keep_div, seed, tau, X, departure, count, capacity, stats);
+    else
+        k_sensor_extract<2, 4><<<blocks, 256, 0, v.stream>>>(v.m, v.bc, v.eos, v.U, v.weno_eps, mode, keep_div, seed, tau, X, departure, count, capacity, stats);
+    SK(cudaGetLastError());
+    SK(cudaStreamSynchronize(v.stream));
+    return FVG_OK;
+}
+
+int fvg_sensor_grad(const void* weights, const float* X, const float* y, long long n, float wpos, float* grad, float* loss, void* stream) {
+    if (!weights || !X || !y || !grad || !loss || n < 1) return serr(FVG_ERR_ARGUMENT, "null argument or no samples");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_sensor_grad<<<grid_for(n), 256, 0, s>>>(static_cast<const SensorW*>(weights), X, y, n, wpos, 1.0f / (float)n, grad, loss);
+    SK(cudaGetLastError());
+    return FVG_OK;
+}
+
+int fvg_sensor_adam(float* params, float* m, float* v, float* grad, int step, float lr, float beta1, float beta2, float eps, void* weights, void* stream) {
+    if (!params || !m || !v || !grad || !weights || step < 1) return serr(FVG_ERR_ARGUMENT, "null argument or step < 1");
+    k_sensor_adam<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(params, m, v, grad, step, lr, beta1, beta2, eps, static_cast<SensorW*>(weights));
+    SK(cudaGetLastError());
+    return FVG_OK;
+}
+
+int fvg_sensor_pack(const float* params, void* weights, void* stream) {
+    if (!params || !weights) return serr(FVG_ERR_ARGUMENT, "null argument");
+    k_sensor_pack<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(reinterpret_cast<const SensorP*>(params), static_cast<SensorW*>(weights));
+    SK(cudaGetLastError());
+    return FVG_OK;
+}
+
+int fvg_sensor_infer(const void* weights, const float* X, long long n, float* logits, void* stream) {
+    if (!weights || !X || !logits || n < 1) return serr(FVG_ERR_ARGUMENT, "null argument or no samples");
+    k_sensor_infer<<<grid_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const SensorW*>(weights), X, n, logits);
+    SK(cudaGetLastError());
+    return FVG_OK;
+}
+
+}   // extern "C"

@@ -1,0 +1,182 @@
+// The learned troubled-cell sensor: a small MLP that reads a cell's 5-cell stencil along a sweep axis and decides whether
+// the cell's two WENO5-Z reconstructions along that axis may take the linear fifth-order upwind values instead.
+//
+// Inputs (per cell and axis): the 5 cells c-2 .. c+2 along the axis, 5 primitive quantities each (rho, the normal
+// velocity, the two tangential velocities (the second is 0 on a 2-D mesh), p). Per quantity, with r the root mean square
+// of its 5 values (1 when all are 0): the centre v0 / r and the four differences (v_k - v0) / r, each scaled by 200 and
+// clamped to [-16, 16] (relative jumps above 8 % look alike: such a cell is troubled anyway). 25 features, padded with
+// zeros to the 32 of two tensor-core k-steps.
+// Network: 32 -> 32 (ReLU) -> 32 (ReLU) -> 1 logit; weights and hidden activations in bfloat16, sums in float32
+// (mma.sync m16n8k16 bf16 with f32 accumulators, one warp per 16 cells). The cell is smooth (linear reconstruction)
+// when the logit is below a threshold chosen for a low miss rate; otherwise, and for every cell the network is not sure
+// about, WENO5-Z stays.
+// Label (what the network learns): the largest departure |omega_k - d_k| of the WENO-Z nonlinear weights from the linear
+// ones d = (0.1, 0.6, 0.3) over the quantities and the cell's two reconstructions (weno5z, cpp/src/Schemes.cpp:328-353),
+// above a label threshold.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+namespace fvg {
+
+constexpr int kSensQ = 5;             // quantities per stencil cell
+constexpr int kSensF = 5 * kSensQ;    // features
+constexpr int kSensK = 32;            // padded input width
+constexpr int kSensH = 32;            // hidden width
+constexpr float kSensScale = 200.0f, kSensClamp = 16.0f;
+
+// Device weights of the network as the kernels read them.
+struct SensorW {
+    __nv_bfloat16 W1[kSensH * kSensK];    // [out][in], inputs kSensF .. kSensK-1 zero
+    __nv_bfloat16 W2[kSensH * kSensH];    // [out][in]
+    float b1[kSensH], b2[kSensH];
+    float w3[kSensH];                     // bfloat16-rounded
+    float b3;
+    float pad[3];
+    __nv_bfloat16 W2T[kSensH * kSensH];   // [in][out] (the backward pass's operand; inference copies what precedes it)
+};
+constexpr int kSensInferBytes = 2 * kSensH * kSensK + 2 * kSensH * kSensH + 4 * (3 * kSensH + 4);
+
+// Float32 master parameters (training): the layout of the gradients too.
+struct SensorP {
+    float W1[kSensH * kSensK];
+    float b1[kSensH];
+    float W2[kSensH * kSensH];
+    float b2[kSensH];
+    float w3[kSensH];
+    float b3;
+};
+constexpr int kSensParams = sizeof(SensorP) / sizeof(float);
+
+__device__ __forceinline__ float sens_clamp(float x) { return fminf(fmaxf(kSensScale * x, -kSensClamp), kSensClamp); }
+
+// The five features of one quantity from its values at c-2 .. c+2 (f[2] the centre entry).
+__device__ __forceinline__ void sensor_quantity_features(const float v[5], float f[5]) {
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) s += v[k] * v[k];
+    const float r = s > 0.0f ? sqrtf(0.2f * s) : 1.0f;
+    const float ir = 1.0f / r, v0 = v[2];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) f[k] = sens_clamp(k == 2 ? v0 * ir : (v[k] - v0) * ir);
+}
+
+// Index of sensor quantity sq (rho, u_n, u_t1, u_t2, p) among the primitive variables [rho, u, v, p(, w)] for a sweep
+// along `axis`; -1 for a velocity the mesh does not have (w on a 2-D mesh).
+template <int NV> __device__ __forceinline__ int sensor_var(int sq, int axis) {
+    if (sq == 0) return 0;
+    if (sq == 4) return 3;
+    const int k = (sq - 1 + axis) % 3;   // velocity component: axis 0 (u, v, w), axis 1 (v, w, u), axis 2 (w, u, v)
+    return k == 0 ? 1 : (k == 1 ? 2 : (NV == 5 ? 4 : -1));
+}
+
+// WENO-Z weights' departure from the linear ones for the value right of c2 from c0 .. c4 (double precision, the
+// reference's weno5z weights).
+__device__ __forceinline__ double weno5z_departure(double c0, double c1, double c2, double c3, double c4, double eps_rel) {
+    const double eps = eps_rel * (c0 * c0 + c1 * c1 + c2 * c2 + c3 * c3 + c4 * c4) * 0.2 + 1e-300;
+    const double s0 = c0 - 2.0 * c1 + c2, t0 = c0 - 4.0 * c1 + 3.0 * c2;
+    const double s1 = c1 - 2.0 * c2 + c3, t1 = c1 - c3;
+    const double s2 = c2 - 2.0 * c3 + c4, t2 = 3.0 * c2 - 4.0 * c3 + c4;
+    const double b0 = (13.0 / 12.0) * s0 * s0 + 0.25 * t0 * t0;
+    const double b1 = (13.0 / 12.0) * s1 * s1 + 0.25 * t1 * t1;
+    const double b2 = (13.0 / 12.0) * s2 * s2 + 0.25 * t2 * t2;
+    const double tau = fabs(b0 - b2);
+    const double a0 = 0.1 * (1.0 + tau / (b0 + eps)), a1 = 0.6 * (1.0 + tau / (b1 + eps)), a2 = 0.3 * (1.0 + tau / (b2 + eps));
+    const double is = 1.0 / (a0 + a1 + a2);
+    return fmax(fabs(a0 * is - 0.1), fmax(fabs(a1 * is - 0.6), fabs(a2 * is - 0.3)));
+}
+
+// ------------------------------------------------------------------------------------------------ tensor-core MLP
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+__device__ __forceinline__ uint32_t pack_bf16_raw(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+__device__ __forceinline__ float round_bf16(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+// D += A B with A 16x16 (row), B 16x8 (col), bf16 operands, f32 accumulators (PTX mma.sync.m16n8k16).
+__device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// The A fragments (two k-steps) of 16 rows x 32 bf16 stored row-major with a row stride of `ld` elements.
+__device__ __forceinline__ void load_a_frags(const __nv_bfloat16* X, int ld, uint32_t (&a)[2][4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        const int k = 16 * s + 2 * t;
+        a[s][0] = *reinterpret_cast<const uint32_t*>(X + g * ld + k);
+        a[s][1] = *reinterpret_cast<const uint32_t*>(X + (g + 8) * ld + k);
+        a[s][2] = *reinterpret_cast<const uint32_t*>(X + g * ld + k + 8);
+        a[s][3] = *reinterpret_cast<const uint32_t*>(X + (g + 8) * ld + k + 8);
+    }
+}
+
+// One dense layer on the tensor cores: acc[nt] (n-tile nt = outputs 8 nt .. 8 nt + 7) = A W^T, W [32 out][32 in] bf16.
+__device__ __forceinline__ void dense32(const uint32_t (&a)[2][4], const __nv_bfloat16* W, float (&acc)[4][4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+        acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.0f;
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const uint32_t* wp = reinterpret_cast<const uint32_t*>(W + (8 * nt + g) * 32 + 16 * s + 2 * t);
+            const uint32_t b[2] = {wp[0], wp[4]};   // k = 16 s + 2 t (+1) and + 8
+            mma16816(acc[nt], a[s], b);
+        }
+    }
+}
+
+// Bias, ReLU and bfloat16 rounding of a layer's accumulators, repacked as the next layer's A fragments (the C fragment
+// of n-tiles 2s, 2s+1 is the A fragment of k-step s); acc keeps the rounded activations.
+__device__ __forceinline__ void relu_to_a(float (&acc)[4][4], const float* bias, uint32_t (&a)[2][4]) {
+    const int t = (threadIdx.x & 31) & 3;
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+        const float b0 = bias[8 * nt + 2 * t], b1v = bias[8 * nt + 2 * t + 1];
+        acc[nt][0] = round_bf16(fmaxf(acc[nt][0] + b0, 0.0f));
+        acc[nt][1] = round_bf16(fmaxf(acc[nt][1] + b1v, 0.0f));
+        acc[nt][2] = round_bf16(fmaxf(acc[nt][2] + b0, 0.0f));
+        acc[nt][3] = round_bf16(fmaxf(acc[nt][3] + b1v, 0.0f));
+    }
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        a[s][0] = pack_bf16(acc[2 * s][0], acc[2 * s][1]);
+        a[s][1] = pack_bf16(acc[2 * s][2], acc[2 * s][3]);
+        a[s][2] = pack_bf16(acc[2 * s + 1][0], acc[2 * s + 1][1]);
+        a[s][3] = pack_bf16(acc[2 * s + 1][2], acc[2 * s + 1][3]);
+    }
+}
+
+// Logits of the 16 rows of a warp's feature tile X (bf16, 16 x 32, row stride ld): lo = row g, hi = row g + 8 (g = lane / 4),
+// the same in the four lanes of a group.
+__device__ __forceinline__ void sensor_logits(const SensorW& w, const __nv_bfloat16* X, int ld, float& lo, float& hi) {
+    uint32_t a[2][4];
+    float acc[4][4];
+    load_a_frags(X, ld, a);
+    dense32(a, w.W1, acc);
+    relu_to_a(acc, w.b1, a);
+    dense32(a, w.W2, acc);
+    relu_to_a(acc, w.b2, a);
+    const int t = (threadIdx.x & 31) & 3;
+    float s0 = 0.0f, s1 = 0.0f;
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+        const float w0 = w.w3[8 * nt + 2 * t], w1 = w.w3[8 * nt + 2 * t + 1];
+        s0 += acc[nt][0] * w0 + acc[nt][1] * w1;
+        s1 += acc[nt][2] * w0 + acc[nt][3] * w1;
+    }
+    s0 += __shfl_xor_sync(0xffffffffu, s0, 1);
+    s0 += __shfl_xor_sync(0xffffffffu, s0, 2);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, 2);
+    lo = s0 + w.b3;
+    hi = s1 + w.b3;
+}
+
+}   // namespace fvg

@@ -41,6 +41,11 @@ struct StageArgs {
     const Ctl* ctl;             // dt
     const int* gate;            // the kernel does nothing unless *gate (the control block's `active` or `seed`)
     int tiles[3];               // tiles per axis
+    // the learned troubled-cell sensor (mixed-precision WENO5-Z kernels with the sensor only): its device weights, the
+    // logit threshold below which a cell's reconstructions are linear, and counters (cell-axes linear, evaluated)
+    const struct SensorW* sens;
+    float sens_theta;
+    unsigned long long* sens_count;
 };
 
 template <int DIM, int RECON, int TX, int TY, int TZ> struct StageShape {

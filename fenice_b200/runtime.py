@@ -32,7 +32,9 @@ EXPORTS = ["fvg_abi_version", "fvg_create", "fvg_destroy", "fvg_last_error", "fv
            "fvg_residual_noalloc",
            "fvg_batch_create", "fvg_batch_destroy", "fvg_batch_last_error", "fvg_batch_cells", "fvg_batch_upload",
            "fvg_batch_download", "fvg_batch_run", "fvg_batch_problem", "fvg_batch_autotune", "fvg_batch_set_schedule",
-           "fvg_batch_get_schedule", "fvg_batch_stream", "fvg_batch_set_timing", "fvg_batch_get_timing"]
+           "fvg_batch_get_schedule", "fvg_batch_stream", "fvg_batch_set_timing", "fvg_batch_get_timing",
+           "fvg_sensor_sizes", "fvg_sensor_extract", "fvg_sensor_grad", "fvg_sensor_adam", "fvg_sensor_pack", "fvg_sensor_infer",
+           "fvg_set_sensor", "fvg_get_sensor_counts"]
 
 _lib = None
 
@@ -87,6 +89,14 @@ def load_library(path=LIB_PATH):
     lib.fvg_batch_stream.argtypes = [c_p, ctypes.POINTER(c_p)]
     lib.fvg_batch_set_timing.argtypes = [c_p, ctypes.c_int]
     lib.fvg_batch_get_timing.argtypes = [c_p, dp, ll]
+    lib.fvg_sensor_sizes.argtypes = [ip, ip, ip]
+    lib.fvg_sensor_extract.argtypes = [c_p, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_float, c_p, c_p, c_p, ctypes.c_longlong, c_p]
+    lib.fvg_sensor_grad.argtypes = [c_p, c_p, c_p, ctypes.c_longlong, ctypes.c_float, c_p, c_p, c_p]
+    lib.fvg_sensor_adam.argtypes = [c_p, c_p, c_p, c_p, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, c_p, c_p]
+    lib.fvg_sensor_pack.argtypes = [c_p, c_p, c_p]
+    lib.fvg_sensor_infer.argtypes = [c_p, c_p, ctypes.c_longlong, c_p, c_p]
+    lib.fvg_set_sensor.argtypes = [c_p, c_p, ctypes.c_float]
+    lib.fvg_get_sensor_counts.argtypes = [c_p, ll, ll, ctypes.c_int]
     _lib = lib
     return lib
 
@@ -210,6 +220,17 @@ class Run:
         a, b, c, d = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_double(), ctypes.c_longlong()
         self._check(self.lib.fvg_get_timing(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d)), "get_timing")
         return {"stage_ms": a.value, "stage_launches": b.value, "viscous_ms": c.value, "viscous_launches": d.value}
+
+    def set_sensor(self, sensor, threshold=0.0):
+        """Gate the WENO5-Z reconstructions (mixed precision) with a trained ``fenice_b200.sensor.Sensor`` (None: off)."""
+        ptr = None if sensor is None else sensor.weights_ptr()
+        self._check(self.lib.fvg_set_sensor(self.h, ptr, float(threshold)), "set_sensor")
+
+    def sensor_counts(self, reset=False):
+        """(cell-axis evaluations that went linear, all evaluations) since the last reset."""
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(self.lib.fvg_get_sensor_counts(self.h, ctypes.byref(a), ctypes.byref(b), 1 if reset else 0), "sensor_counts")
+        return a.value, b.value
 
     def face_flux_batch(self, UL, UR, axis):
         UL = np.ascontiguousarray(UL, dtype=np.float64)

@@ -144,6 +144,37 @@ int fvg_face_flux_batch(fvg_run* run, const double* UL, const double* UR, const 
  * and must be serialised by the caller. On failure, fvg_create_error() returns this thread's message. */
 int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long long plane, double* R, double* smax, void* stream);
 
+/* ---- The learned troubled-cell sensor (no counterpart in the reference, whose WENO5-Z reconstruction, weno5z and
+ * weno_line_states, cpp/src/Schemes.cpp:328-353 and 793-835, has no gate).
+ *
+ * A 32 -> 32 -> 32 -> 1 MLP reads a cell's 5-cell stencil along a sweep axis (25 features: rho, normal and tangential
+ * velocities, p) and decides whether the cell's two reconstructions along that axis take the linear fifth-order upwind
+ * values (logit below the threshold) or WENO5-Z. Weights and activations are bfloat16 on the tensor cores with float32
+ * sums. The label it learns: the cell's WENO-Z nonlinear weights depart from the linear ones (0.1, 0.6, 0.3) by more
+ * than a threshold tau. Training runs on the GPU through these calls, on device buffers the caller owns:
+ *   fvg_sensor_extract  features (32 floats per sample) and the departure of every (cell, axis) of a run's state
+ *                       (mode 0, at index cell * dim + axis) or of the troubled ones and every keep_div-th other one
+ *                       (mode 1, appended at the device counter *count up to capacity); stats (device, may be NULL):
+ *                       [troubled, all] added
+ *   fvg_sensor_grad     gradients (added to grad, fvg_sensor_sizes' n_params floats) and loss sum (added to *loss) of
+ *                       the mean class-weighted cross-entropy (weight wpos on y = 1) over n samples
+ *   fvg_sensor_adam     one Adam step of the float32 parameters (grad is cleared) and their device weights
+ *   fvg_sensor_pack     device weights of float32 parameters; fvg_sensor_infer: logits of n feature rows
+ * Parameter layout (floats): W1[32][32] (inputs 25..31 unused), b1[32], W2[32][32], b2[32], w3[32], b3.
+ * fvg_set_sensor gates a mixed-precision WENO5-Z run with device weights (copied; NULL: plain WENO5-Z again);
+ * fvg_get_sensor_counts returns the (cell, axis) evaluations that went linear and all evaluations since the last reset.
+ * Failures of the calls without a run handle: fvg_create_error(). */
+int fvg_sensor_sizes(int* n_params, int* weights_bytes, int* n_inputs);
+int fvg_sensor_extract(fvg_run* run, int mode, int keep_div, unsigned seed, float tau, float* X, float* departure, int* count,
+                       long long capacity, unsigned long long* stats);
+int fvg_sensor_grad(const void* weights, const float* X, const float* y, long long n, float wpos, float* grad, float* loss, void* stream);
+int fvg_sensor_adam(float* params, float* m, float* v, float* grad, int step, float lr, float beta1, float beta2, float eps, void* weights,
+                    void* stream);
+int fvg_sensor_pack(const float* params, void* weights, void* stream);
+int fvg_sensor_infer(const void* weights, const float* X, long long n, float* logits, void* stream);
+int fvg_set_sensor(fvg_run* run, const void* weights, float threshold);
+int fvg_get_sensor_counts(fvg_run* run, long long* linear, long long* evaluated, int reset);
+
 /* ---- Batched independent problems (no counterpart in the reference, which runs one Simulation per process).
  *
  * n 2-D problems (nz = 1) of uneven sizes advance together, each with its own clock, dt and step count, as if each

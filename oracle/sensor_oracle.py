@@ -1,0 +1,116 @@
+"""Test infrastructure (the oracle), not part of the product: a numpy restatement of the troubled-cell sensor's inputs,
+labels and network, the check of the GPU sensor kernels (fenice_b200/csrc/sensor.cuh).
+
+* stencil_features(Q5): the 25 features of one (cell, axis): the 5 cells c-2 .. c+2 along the axis, 5 primitive
+  quantities each (rho, normal velocity, the two tangential velocities (0 on a 2-D mesh), p). Per quantity, with r the
+  root mean square of its 5 values (1 when all are 0), the centre value v0 / r and the four differences (v_k - v0) / r,
+  each scaled by 200 and clamped to [-16, 16]; quantity-major, padded with zeros to 32 inputs.
+* departure(Q5): the label statistic: over the 5 quantities and both WENO5-Z reconstructions centred on the cell (the
+  value at its right face from c-2 .. c+2 and at its left face from c+2 .. c-2), the largest |omega_k - d_k| of the
+  WENO-Z weights (the reference's weno5z, cpp/src/Schemes.cpp:328-353) against the linear ones d = (0.1, 0.6, 0.3). A cell
+  is troubled along the axis when it exceeds the label threshold.
+* mlp_forward / mlp_loss_grad: 32 -> 32 -> 32 -> 1 with ReLU, the product's arithmetic emulated: inputs, weights and
+  hidden activations rounded to bfloat16 where the kernels feed them to the tensor cores, sums and biases in float32 (here
+  float64 on the rounded operands), loss the mean class-weighted binary cross-entropy with logits.
+"""
+import numpy as np
+
+D_LIN = np.array([0.1, 0.6, 0.3])
+NF, NK, NH = 25, 32, 32
+
+
+def bf16(a):
+    """Round to bfloat16 (round to nearest even), returned as float32."""
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    u = a.view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32)
+
+
+def g(x):
+    return np.clip(np.float32(200.0) * x, -16.0, 16.0).astype(np.float32)
+
+
+def axis_quantities(W, axis):
+    """(..., 5, 5) stencil of primitive cells [rho, u, v, p, w] along `axis` -> [rho, u_n, u_t1, u_t2, p]."""
+    W = np.asarray(W, dtype=np.float64)
+    u, v, w = W[..., 1], W[..., 2], W[..., 4]
+    n, t1, t2 = [(u, v, w), (v, w, u), (w, u, v)][axis]
+    return np.stack([W[..., 0], n, t1, t2, W[..., 3]], axis=-1)
+
+
+def stencil_features(Q5):
+    """(n, 5, 5) stencil quantities -> (n, 32) features (quantity-major: 5 entries per quantity, positions c-2 .. c+2
+    with the centre entry v0 / r; columns 25 .. 31 zero)."""
+    Q5 = np.asarray(Q5, dtype=np.float32)
+    r = np.sqrt(np.float32(0.2) * np.sum(Q5 * Q5, axis=1))
+    r = np.where(r > 0, r, np.float32(1.0)).astype(np.float32)
+    ir = (np.float32(1.0) / r).astype(np.float32)
+    v0 = Q5[:, 2, :]
+    d = (Q5 - v0[:, None, :]) * ir[:, None, :]
+    d[:, 2, :] = v0 * ir
+    out = np.zeros((len(Q5), NK), dtype=np.float32)
+    out[:, :NF] = g(np.transpose(d, (0, 2, 1)).reshape(len(Q5), NF))
+    return out
+
+
+def weno5z_weights(c, eps_rel=1e-6):
+    """WENO-Z weights of the value at the face right of c[:, 2] from c[:, 0..4] (float64)."""
+    c0, c1, c2, c3, c4 = (c[:, k] for k in range(5))
+    eps = eps_rel * (c0 * c0 + c1 * c1 + c2 * c2 + c3 * c3 + c4 * c4) * 0.2 + 1e-300
+    s0, t0 = c0 - 2 * c1 + c2, c0 - 4 * c1 + 3 * c2
+    s1, t1 = c1 - 2 * c2 + c3, c1 - c3
+    s2, t2 = c2 - 2 * c3 + c4, 3 * c2 - 4 * c3 + c4
+    b0 = 13 / 12 * s0 * s0 + 0.25 * t0 * t0
+    b1 = 13 / 12 * s1 * s1 + 0.25 * t1 * t1
+    b2 = 13 / 12 * s2 * s2 + 0.25 * t2 * t2
+    tau = np.abs(b0 - b2)
+    a = np.stack([0.1 * (1 + tau / (b0 + eps)), 0.6 * (1 + tau / (b1 + eps)), 0.3 * (1 + tau / (b2 + eps))], axis=1)
+    return a / a.sum(axis=1, keepdims=True)
+
+
+def departure(Q5, eps_rel=1e-6):
+    """(n, 5, 5) -> (n,) the largest departure of the WENO-Z weights from the linear ones."""
+    Q5 = np.asarray(Q5, dtype=np.float64)
+    out = np.zeros(len(Q5))
+    for q in range(Q5.shape[2]):
+        c = Q5[:, :, q]
+        for cc in (c, c[:, ::-1]):
+            out = np.maximum(out, np.abs(weno5z_weights(cc, eps_rel) - D_LIN).max(axis=1))
+    return out
+
+
+def mlp_forward(X, P):
+    """Logits of (n, 32) features; P = dict(W1 (32, 32), b1 (32,), W2 (32, 32), b2, w3 (32,), b3 ()). Returns the
+    logits and the intermediates mlp_backward needs."""
+    Xb = bf16(X).astype(np.float64)
+    W1, W2, w3 = (bf16(P[k]).astype(np.float64) for k in ("W1", "W2", "w3"))
+    z1 = Xb @ W1.T + P["b1"]
+    h1 = bf16(np.maximum(z1, 0)).astype(np.float64)
+    z2 = h1 @ W2.T + P["b2"]
+    h2 = bf16(np.maximum(z2, 0)).astype(np.float64)
+    z = h2 @ w3 + float(P["b3"])
+    return z, (Xb, z1, h1, z2, h2, W1, W2, w3)
+
+
+def mlp_loss_grad(X, y, wpos, P):
+    """Mean class-weighted BCE with logits (weight wpos on y = 1, 1 on y = 0) and its gradients. The backward pass
+    rounds the back-propagated hidden gradients to bfloat16 where the kernels do (before the weight-gradient and
+    input-gradient products)."""
+    z, (Xb, z1, h1, z2, h2, W1, W2, w3) = mlp_forward(X, P)
+    n = len(z)
+    y = np.asarray(y, dtype=np.float64)
+    w = np.where(y > 0.5, wpos, 1.0)
+    sp = np.logaddexp(0, -np.abs(z)) + np.maximum(z, 0)   # softplus(z)
+    loss = float(np.mean(w * (sp - y * z)))
+    dz = w * (1 / (1 + np.exp(-z)) - y) / n
+    G = {"w3": h2.T @ dz, "b3": dz.sum()}
+    dh2 = np.outer(dz, w3) * (z2 > 0)
+    dh2b = bf16(dh2).astype(np.float64)
+    G["W2"] = dh2b.T @ h1
+    G["b2"] = dh2.sum(axis=0)
+    dh1 = (dh2b @ W2) * (z1 > 0)
+    dh1b = bf16(dh1).astype(np.float64)
+    G["W1"] = dh1b.T @ Xb
+    G["b1"] = dh1.sum(axis=0)
+    return loss, G

@@ -1,0 +1,116 @@
+"""The learned troubled-cell sensor on the GPU against its CPU oracle (oracle/sensor_oracle.py): the tensor-core
+forward pass (logits), the backward pass (every gradient), the training data (features and WENO-Z departures of a run's
+state), and that Adam on the GPU kernels learns the label."""
+import numpy as np
+import pytest
+
+from fenice_b200 import Run, initial
+from oracle import sensor_oracle as SO
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def sensor(seed=0):
+    from fenice_b200.sensor import Sensor
+
+    return Sensor(seed=seed)
+
+
+def random_params(seed):
+    rng = np.random.default_rng(seed)
+    P = {"W1": rng.normal(0, 0.4, (32, 32)), "b1": rng.normal(0, 0.2, 32), "W2": rng.normal(0, 0.3, (32, 32)), "b2": rng.normal(0, 0.2, 32),
+         "w3": rng.normal(0, 0.3, 32), "b3": 0.1}
+    P["W1"][:, 25:] = 0.0
+    return P
+
+
+def random_features(n, seed):
+    rng = np.random.default_rng(seed)
+    X = np.zeros((n, 32), dtype=np.float32)
+    X[:, :25] = np.clip(rng.normal(0, 4, (n, 25)), -16, 16)
+    return X
+
+
+def test_forward_matches_oracle():
+    from fenice_b200.sensor import Sensor
+
+    P = random_params(1)
+    s = Sensor(params=P)
+    X = random_features(4099, 2)
+    z = s.logits(torch.tensor(X, device="cuda")).cpu().numpy()
+    zr, _ = SO.mlp_forward(X, P)
+    close = np.isclose(z, zr, rtol=1e-3, atol=2e-3)
+    print(f"\nforward: max |dz| {np.abs(z - zr).max():.2e}, {close.mean():.4f} within tolerance")
+    assert close.mean() > 0.995
+
+
+def test_gradients_match_oracle():
+    from fenice_b200.sensor import Sensor
+
+    P = random_params(3)
+    s = Sensor(params=P)
+    n = 3001
+    X = random_features(n, 4)
+    y = (np.random.default_rng(5).random(n) < 0.3).astype(np.float32)
+    loss, g = s.grad(torch.tensor(X, device="cuda"), torch.tensor(y, device="cuda"), wpos=3.0)
+    G = Sensor.unflatten(g.cpu().numpy().astype(np.float64))
+    lr, Gr = SO.mlp_loss_grad(X, y, 3.0, P)
+    assert abs(loss - lr) <= 1e-3 * abs(lr)
+    for k in ("W1", "b1", "W2", "b2", "w3", "b3"):
+        a, b = np.asarray(G[k]), np.asarray(Gr[k])
+        if k == "W1":
+            a, b = a[:, :25], b[:, :25]
+        rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+        print(f"grad {k}: relative error {rel:.2e}")
+        assert rel < 1e-2, k
+
+
+def stencils(W, n, axis):
+    """(n*n, 5, 5) stencils along `axis` of interior-padded primitive cells (only interior cells are compared)."""
+    Wg = W.reshape(n, n, 5)
+    out = np.zeros((n, n, 5, 5))
+    for k in range(-2, 3):
+        out[:, :, k + 2] = np.roll(Wg, -k, axis=1 - axis)
+    return out.reshape(n * n, 5, 5)
+
+
+def test_training_data_matches_oracle():
+    from fenice_b200.sensor import Sensor
+
+    n = 48
+    run = Run(initial.quadrant_params(n), U=initial.riemann_quadrants(n, 9))
+    run.run(0.05)
+    U = run.state()
+    s = Sensor()
+    X, D, stats = s.samples(run, mode=0)
+    X, D = X.cpu().numpy().reshape(n * n, 2, 32), D.cpu().numpy().reshape(n * n, 2)
+    g = 1.4
+    W = np.zeros((n * n, 5))
+    W[:, 0] = U[:, 0]
+    W[:, 1], W[:, 2] = U[:, 1] / U[:, 0], U[:, 2] / U[:, 0]
+    W[:, 3] = (g - 1) * (U[:, 3] - 0.5 * (U[:, 1] ** 2 + U[:, 2] ** 2) / U[:, 0])
+    inner = np.zeros((n, n), bool)
+    inner[2:-2, 2:-2] = True
+    inner = inner.ravel()
+    for axis in (0, 1):
+        Q = SO.axis_quantities(stencils(W, n, axis), axis)
+        Xr, Dr = SO.stencil_features(Q), SO.departure(Q)
+        assert np.allclose(X[inner, axis], Xr[inner], rtol=1e-4, atol=2e-3), np.abs(X[inner, axis] - Xr[inner]).max()
+        assert np.allclose(D[inner, axis], Dr[inner], rtol=1e-4, atol=1e-6), np.abs(D[inner, axis] - Dr[inner]).max()
+    assert stats[1] == n * n * 2 and stats[0] == int((D > 0.01).sum())
+
+
+def test_adam_on_the_gpu_learns_the_label():
+    from fenice_b200.sensor import Sensor, quadrant_training_data
+
+    s = Sensor(seed=7)
+    X, D = quadrant_training_data(s, seeds=[1, 2, 3], n=128, t_end=0.2, snapshots=3)
+    y = (D > 0.01).float()
+    before = s.grad(X, y, wpos=1.0)[0]
+    losses = s.train(X, y, epochs=6, batch=4096, lr=3e-3)
+    after = s.grad(X, y, wpos=1.0)[0]
+    acc = ((s.logits(X) > 0).float() == y).float().mean().item()
+    print(f"\n{len(X)} samples, troubled {y.mean().item():.3f}; loss {before:.4f} -> {after:.4f} (epochs {[round(v, 4) for v in losses]}); "
+          f"accuracy {acc:.4f}")
+    assert after < 0.5 * before and acc > 0.9
