@@ -180,7 +180,15 @@ def barrier(world):
         dist.barrier()
 
 
-def timed_run(params, U0, precision, args, world, local):
+def load_sensor(local):
+    """The trained sensor (fenice_b200/sensor_weights.npz, written by python -m fenice_b200.train_sensor) and its threshold."""
+    from fenice_b200.sensor import Sensor
+
+    s = Sensor.load(os.path.join(ROOT, "fenice_b200", "sensor_weights.npz"), device=local)
+    return s, float(s.meta["threshold"])
+
+
+def timed_run(params, U0, precision, args, world, local, sensor=None):
     """W untimed steps, then K steps timed with CUDA events on the run's stream (and around every stage / viscous
     launch), the SM clock sampled meanwhile; returns the run, the device milliseconds (max over ranks), the kernel
     timings and the clock summary."""
@@ -189,6 +197,8 @@ def timed_run(params, U0, precision, args, world, local):
     from fenice_b200 import Run
 
     run = Run(params, U=U0, precision=precision, device=local)
+    if sensor is not None:
+        run.set_sensor(sensor[0], sensor[1])
     ext = torch.cuda.ExternalStream(run.stream(), device=torch.device("cuda", local))
     if args.warmup:
         run.run(1e30, max_steps=args.warmup)
@@ -352,6 +362,51 @@ def batch_arm(args, world, rank, local):
     return out
 
 
+QUAD_WORKLOAD = ("seeded four-quadrant Riemann problem (held-out seed {seed}), {n}^2 cells of [0,1]^2, rho, p ~ U[0.1, 2], u, v ~ U[-1, 1], "
+                 "WENO5-Z + HLLC + SSP-RK3, CFL 0.4, transmissive, to t = 0.25")
+
+
+def quad_arm(args, world, rank, local):
+    """The four-quadrant workload: one whole run to t = 0.25 per form (plain FP64, mixed, mixed + learned sensor), each
+    timed with CUDA events on its stream; L1 of the mixed forms against the plain FP64 run."""
+    import torch
+
+    from fenice_b200 import Run, initial
+
+    n, seed = args.size, args.seed
+    params, U0 = initial.quadrant_params(n), initial.riemann_quadrants(n, seed)
+    sensor = load_sensor(local)
+    out, states = {}, {}
+    for name, prec, sens in (("plain_fp64", 0, None), ("mixed", 1, None), ("mixed_learned", 1, sensor)):
+        warm = Run(params, U=U0, precision=prec, device=local)
+        if sens:
+            warm.set_sensor(*sens)
+        warm.run(1e30, max_steps=max(args.warmup, 3))
+        warm.close()
+        run = Run(params, U=U0, precision=prec, device=local)
+        if sens:
+            run.set_sensor(*sens)
+        ext = torch.cuda.ExternalStream(run.stream(), device=torch.device("cuda", local))
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        with Clocks(local) as clk:
+            start.record(ext)
+            steps = run.run(0.25)
+            end.record(ext)
+            run.synchronize()
+        ms = allmax(start.elapsed_time(end), world)
+        states[name] = run.state()
+        out[name] = {"value": world * n * n * 3 * steps / (ms * 1e-3), "ms": ms, "steps": steps, "clocks": clk.summary()}
+        if sens:
+            lin, ev = run.sensor_counts()
+            out[name]["linear_share_of_tile_axes"] = lin / max(ev, 1)
+        run.close()
+    for name in ("mixed", "mixed_learned"):
+        out[name]["l1_rho_vs_fp64"] = float(np.abs(states[name][:, 0] - states["plain_fp64"][:, 0]).sum() / np.abs(states["plain_fp64"][:, 0]).sum())
+    out["l1_rho_learned_vs_mixed"] = float(np.abs(states["mixed_learned"][:, 0] - states["mixed"][:, 0]).sum() / np.abs(states["mixed"][:, 0]).sum())
+    return out
+
+
 def gpu_arm(args, world, rank, local):
     import torch
 
@@ -364,10 +419,18 @@ def gpu_arm(args, world, rank, local):
     U_plain = plain.state()
     plain.close()
     mixed, ms_m, tm_m, clk_m = timed_run(params, U0, 1, args, world, local)
-    errs = l1_errors(mixed.state(), U_plain)
+    errs_m = l1_errors(mixed.state(), U_plain)
+    mixed.close()
+    # the mixed form gated by the learned sensor (the metric's form)
+    sensor = load_sensor(local)
+    learned, ms_l, tm_l, clk_l = timed_run(params, U0, 1, args, world, local, sensor=sensor)
+    errs = l1_errors(learned.state(), U_plain)
+    lin, ev = learned.sensor_counts()
     del U_plain
-    value = world * cells * STAGES * args.steps / (ms_m * 1e-3)
+    value = world * cells * STAGES * args.steps / (ms_l * 1e-3)
+    value_m = world * cells * STAGES * args.steps / (ms_m * 1e-3)
     value_p = world * cells * STAGES * args.steps / (ms_p * 1e-3)
+    mixed = learned
 
     # end to end through the public API (mixed form): per step the state goes host (pinned) -> device, one step, back
     e2e = None
@@ -385,25 +448,35 @@ def gpu_arm(args, world, rank, local):
                "d2h_bytes_per_step": cells * 5 * 8, "steps": args.e2e_steps, "timing": "host wall clock around upload + step + download"}
     mixed.close()
 
+    rl_l = roofline_of(tm_l, ms_l, cells, "mixed_stage_kernel<3, WENO5, LowMach, gated> (FP32 reconstruction (linear or WENO5-Z per tile) + "
+                       "Riemann + balance, FP64 RK update)", ncu_traffic(n, "mixed_stage_kernel_weno5_3d.json"))
     rl_m = roofline_of(tm_m, ms_m, cells, "mixed_stage_kernel<3, WENO5, LowMach> (FP32 reconstruction + Riemann + balance, FP64 RK update)",
                        ncu_traffic(n, "mixed_stage_kernel_weno5_3d.json"))
     rl_p = roofline_of(tm_p, ms_p, cells, "stage_kernel<3, WENO5, LowMach> (FP64, the reference's arithmetic)",
                        ncu_traffic(n, "stage_kernel_weno5_3d.json"))
-    launches = 2 * (args.steps * 11 + 1)   # per RK3 step: 3 viscous + 3 stage + dt + axpy + 2 stage maxima + end; one begin per run
+    # per RK3 step: 3 viscous + 3 stage + dt + axpy + 2 stage maxima + end; one begin per run; the gated run adds the
+    # sensor's refresh (network, 3 dilation passes, tile reduction) to every step (the kernels return at once off the
+    # refresh steps)
+    launches = 3 * (args.steps * 11 + 1) + args.steps * 5
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_m / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 stencil / f64 state (mixed form); plain form f64",
+            "dtype": "f32 stencil / f64 state (mixed form) with bf16 sensor; plain form f64",
             "data": "synthetic (Taylor-Green initial state computed in numpy)",
             "config": {"workload": f"Taylor-Green vortex 3-D {n}^3, WENO5-Z + low-Mach HLLC + SSP-RK3, viscous Re 1600 Pr 0.71, CFL 0.5; "
-                                   "value: the mixed-precision form (no learned sensor yet); plain_fp64: the reference's arithmetic",
+                                   "value: the mixed-precision form gated by the learned sensor; mixed: without the sensor; "
+                                   "plain_fp64: the reference's arithmetic",
                        "cells": cells, "stages_per_step": STAGES,
                        "parallelism": f"replicas{world}" if world > 1 else "single GPU",
                        "l2": f"inputs larger than L2 ({cells * 40 / 1e6:.0f} MB per state field), no flush"},
-            "accuracy": {"vs": f"plain FP64 form after {args.warmup + args.steps} steps from the same state", "fields": errs,
+            "accuracy": {"vs": f"plain FP64 form after {args.warmup + args.steps} steps from the same state (the value's form)", "fields": errs,
                          "l1_rho_bar": 1e-4, "l1_rho_within_bar": errs["rho"]["l1_rel"] <= 1e-4},
             "plain_fp64": {"value": value_p, "ms_per_step": ms_p / args.steps, "roofline": rl_p, "clocks": clk_p,
-                           "speedup_of_mixed": value / value_p},
-            "roofline": rl_m, "e2e": e2e, "gpu_launches": launches, "clocks": clk_m}
+                           "speedup_of_value": value / value_p},
+            "mixed": {"value": value_m, "ms_per_step": ms_m / args.steps, "roofline": rl_m, "clocks": clk_m, "speedup_vs_plain": value_m / value_p,
+                      "accuracy_l1_rho": errs_m["rho"]["l1_rel"]},
+            "sensor": {"threshold": sensor[1], "tile_axes_linear": lin, "tile_axes": ev, "linear_share": lin / max(ev, 1),
+                       "refresh_every_steps": 5, "speedup_vs_mixed": value / value_m},
+            "roofline": rl_l, "e2e": e2e, "gpu_launches": launches, "clocks": clk_l}
     return line
 
 
@@ -416,8 +489,10 @@ def main():
     ap.add_argument("--size", type=int, default=256, help="cells per axis (256: the benchmark workload)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-baseline", type=int, default=1, help="time the reference on the host cores (rank 0, N = 1)")
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch"],
-                    help="tgv: the 3-D Taylor-Green vortex (default); batch: 512 shock tubes in one persistent launch per stage")
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "quadrants"],
+                    help="tgv: the 3-D Taylor-Green vortex (default); batch: 512 shock tubes in one persistent launch per stage; "
+                         "quadrants: a seeded four-quadrant Riemann problem (--size cells per axis, default 2048 for it)")
+    ap.add_argument("--seed", type=int, default=2048, help="seed of the quadrants workload")
     ap.add_argument("--batch", type=int, default=1, help="with --workload tgv at N = 1: add the batched workload's figures")
     args = ap.parse_args()
     world, rank, local = (1, 0, 0) if args.impl == "reference" and int(os.environ.get("WORLD_SIZE", "1")) == 1 else dist_setup()
@@ -446,6 +521,24 @@ def main():
                 "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
                 "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
+        return
+    if args.workload == "quadrants":
+        if args.size == 256:
+            args.size = 2048
+        q = quad_arm(args, world, rank, local)
+        m = q["mixed_learned"]
+        line = {"metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world, "steps": m["steps"], "warmup": args.warmup,
+                "ms_per_step": m["ms"] / m["steps"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 stencil / f64 state with bf16 sensor (value); plain form f64", "data": "synthetic (seeded quadrant states)",
+                "config": {"workload": QUAD_WORKLOAD.format(seed=args.seed, n=args.size) + "; value: mixed + learned sensor",
+                           "cells": args.size ** 2, "l2": "inputs larger than L2 from 2048^2 on (134 MB per state), no flush"},
+                "clocks": m["clocks"], "forms": q, "e2e": None, "gpu_launches": None}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
         return
     if args.workload == "batch":
         b = batch_arm(args, world, rank, local)

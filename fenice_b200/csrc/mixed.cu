@@ -29,10 +29,10 @@ template <int DIM, int RIEMANN> struct GatedK {
     using S = MixedShape<DIM, kWeno5, T::X, T::Y, T::Z>;
     static cudaError_t prepare() {
         return cudaFuncSetAttribute(mixed_stage_kernel<DIM, kWeno5, RIEMANN, T::X, T::Y, T::Z, T::NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)S::GATED_BYTES);
+                                    (int)S::SMEM_BYTES);
     }
     static cudaError_t launch(const StageArgs& a, int nblocks, cudaStream_t s) {
-        mixed_stage_kernel<DIM, kWeno5, RIEMANN, T::X, T::Y, T::Z, T::NT, true><<<nblocks, T::NT, S::GATED_BYTES, s>>>(a);
+        mixed_stage_kernel<DIM, kWeno5, RIEMANN, T::X, T::Y, T::Z, T::NT, true><<<nblocks, T::NT, S::SMEM_BYTES, s>>>(a);
         return cudaGetLastError();
     }
 };

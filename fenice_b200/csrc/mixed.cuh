@@ -14,7 +14,6 @@
 #pragma once
 
 #include "grid.cuh"
-#include "sensor.cuh"
 #include "stage.cuh"
 #include "viscous.cuh"
 
@@ -50,8 +49,6 @@ __device__ __forceinline__ float face_flux_prim(const Eos<float>& e, float shock
     return hllc_core(WL, WR, p2c(e, WL), p2c(e, WR), inv_L, inv_R, c_L, c_R, axis, shock_blend, F);
 }
 
-template <int TX, int TY, int TZ> __host__ __device__ constexpr int T3g(int a) { return a == 0 ? TX : (a == 1 ? TY : TZ); }
-
 // the fifth-order upwind value right of c2 from c0 .. c4: 0.1 p0 + 0.6 p1 + 0.3 p2 of the three candidate stencils
 __device__ __forceinline__ float lin5(float c0, float c1, float c2, float c3, float c4) {
     return (2.0f * c0 - 13.0f * c1 + 47.0f * c2 + 27.0f * c3 - 3.0f * c4) * (1.0f / 60.0f);
@@ -71,27 +68,15 @@ template <int DIM, int RECON, int TX, int TY, int TZ> struct MixedShape {
     static constexpr int SMEM_FLOATS = NV * EXT + 2 * NV * NF + NV * NC + 64;
     static constexpr int FLAG_BYTES = (EXT + 7) / 8 * 8;   // solidity of the extended tile (WENO5-Z beside an immersed body)
     static constexpr size_t SMEM_BYTES = sizeof(float) * SMEM_FLOATS + FLAG_BYTES;
-    // with the sensor: its weights (the inference part) after the rest
-    static constexpr size_t GATE_OFF = (SMEM_BYTES + 15) / 16 * 16;
-    static constexpr size_t GATED_BYTES = GATE_OFF + (kSensInferBytes + 15) / 16 * 16;
 };
-
-// The sensor's part of a gated sweep (GATED): after the load, the network decides for every cell whose two reconstructions
-// along the axis the tile needs (extended positions 2 .. T + 3 along it) whether they are linear (Gf = 0) or WENO5-Z
-// (Gf = 1). Each warp takes 16 cells at a time: their features into its bf16 tile, the logits on the tensor cores.
-struct GateSmem {
-    const SensorW* w;         // the weights (the inference part), in shared memory
-    __nv_bfloat16* tile;      // per warp 16 x kSensLd features, over the face-value buffers (free until the reconstruction)
-    unsigned char* Gf;        // per extended position (the solidity flags' buffer: a gated run has no immersed body)
-    unsigned nlin, neval;     // this thread's counts
-};
-constexpr int kSensLd = 40;
 
 // One axis of the tile sweep of mixed_stage_kernel (compile-time extents).
+// GATED (WENO5-Z with the learned sensor): the tile's flag for this axis (one byte per tile and axis, from the sensor's
+// last refresh) makes every reconstruction of the sweep linear (0) or WENO5-Z (1); the branch is uniform over the CTA.
 template <int AXIS, int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT, bool GATED = false>
 __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>& ef, float sb, float weps, float* __restrict__ P,
                                            float* __restrict__ WL, float* __restrict__ WR, float* __restrict__ acc, unsigned char* __restrict__ Sf,
-                                           const int o3[3], float& smax, GateSmem* gate = nullptr) {
+                                           const int o3[3], float& smax) {
     using S = MixedShape<DIM, RECON, TX, TY, TZ>;
     constexpr int NV = S::NV, H = S::H, NC = S::NC;
     constexpr int axis = AXIS;
@@ -114,61 +99,8 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
         }
         __syncthreads();
         const int sstride = axis == 0 ? 1 : (axis == 1 ? E[0] : E[0] * E[1]);
-        if constexpr (GATED) {
-            static_assert(RECON == kWeno5, "the sensor gates WENO5-Z");
-            constexpr int La = T3g<TX, TY, TZ>(AXIS) + 2, O0 = AXIS == 0 ? 1 : 0, O1 = AXIS == 2 ? 1 : 2;
-            constexpr int nS = La * (nE / E[AXIS]);
-            // as many warps as the face-value buffers (WL, WR: free until the reconstruction) hold feature tiles of
-            constexpr int NWS = (NT / 32) < (2 * NV * S::NF * 4) / (16 * kSensLd * 2) ? (NT / 32) : (2 * NV * S::NF * 4) / (16 * kSensLd * 2);
-            static_assert(NWS >= 1, "a feature tile fits in the face-value buffers");
-            const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
-            __nv_bfloat16* X = gate->tile + warp * 16 * kSensLd;
-            for (int ch = warp; warp < NWS && ch * 16 < nS; ch += NWS) {
-                for (int it2 = lane; it2 < 16 * kSensQ; it2 += 32) {
-                    const int row = it2 / kSensQ, sq = it2 % kSensQ, j = ch * 16 + row;
-                    float f[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-                    const int var = sensor_var<NV>(sq, AXIS);
-                    if (j < nS && var >= 0) {
-                        int l3[3];
-                        const int r = j / La;
-                        l3[AXIS] = 2 + j % La;
-                        l3[O0] = r % E[O0];
-                        l3[O1] = r / E[O0];
-                        const int e = (l3[2] * E[1] + l3[1]) * E[0] + l3[0];
-                        float v[5];
-#pragma unroll
-                        for (int k = 0; k < 5; ++k) v[k] = P[var * S::EXT + e + (k - 2) * sstride];
-                        sensor_quantity_features(v, f);
-                    }
-#pragma unroll
-                    for (int k = 0; k < 5; ++k) X[row * kSensLd + 5 * sq + k] = __float2bfloat16_rn(f[k]);
-                }
-                // the padding inputs: zeros (the buffer holds the previous sweep's fluxes)
-                for (int z = lane; z < 16 * (kSensK - kSensF); z += 32) X[(z / (kSensK - kSensF)) * kSensLd + kSensF + z % (kSensK - kSensF)] = __float2bfloat16_rn(0.0f);
-                __syncwarp();
-                float lo, hi;
-                sensor_logits(*gate->w, X, kSensLd, lo, hi);
-                if (t == 0) {
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int j = ch * 16 + g + 8 * h;
-                        if (j >= nS) continue;
-                        const float z = h ? hi : lo;
-                        int l3[3];
-                        const int r = j / La;
-                        l3[AXIS] = 2 + j % La;
-                        l3[O0] = r % E[O0];
-                        l3[O1] = r / E[O0];
-                        const bool weno = !(z < a.sens_theta);
-                        gate->Gf[(l3[2] * E[1] + l3[1]) * E[0] + l3[0]] = weno ? 1 : 0;
-                        gate->nlin += weno ? 0u : 1u;
-                        gate->neval += 1u;
-                    }
-                }
-                __syncwarp();
-            }
-            __syncthreads();
-        }
+        bool tile_linear = false;
+        if constexpr (GATED) tile_linear = a.sens_flags[AXIS * a.tiles[0] * a.tiles[1] * a.tiles[2] + blockIdx.x] == 0;
         // ---- 2. face values
         for (int it = tid; it < nF * NV; it += NT) {
             const int f = it % nF, q = it / nF;
@@ -193,11 +125,11 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
                 if (four) {
                     wl = weno3z(c1, c2, c3, weps);
                     wr = weno3z(c4, c3, c2, weps);
-                } else if constexpr (GATED) {
-                    // linear fifth-order upwind values where the sensor passed the cell (the WENO-Z weights at their
+                } else if (tile_linear) {
+                    // linear fifth-order upwind values where the sensor passed the tile (the WENO-Z weights at their
                     // linear values 0.1, 0.6, 0.3)
-                    wl = gate->Gf[base + 2 * sstride] ? weno5z(c0, c1, c2, c3, c4, weps) : lin5(c0, c1, c2, c3, c4);
-                    wr = gate->Gf[base + 3 * sstride] ? weno5z(c5, c4, c3, c2, c1, weps) : lin5(c5, c4, c3, c2, c1);
+                    wl = lin5(c0, c1, c2, c3, c4);
+                    wr = lin5(c5, c4, c3, c2, c1);
                 } else {
                     wl = weno5z(c0, c1, c2, c3, c4, weps);
                     wr = weno5z(c5, c4, c3, c2, c1, weps);
@@ -284,21 +216,9 @@ __global__ void __launch_bounds__(NT) mixed_stage_kernel(const StageArgs a) {
     const int tid = threadIdx.x, b = blockIdx.x;
     const int o3[3] = {(b % a.tiles[0]) * TX, ((b / a.tiles[0]) % a.tiles[1]) * TY, (b / (a.tiles[0] * a.tiles[1])) * TZ};
     float smax = 0.0f;
-    GateSmem gs{};
-    if constexpr (GATED) {
-        SensorW* ws = reinterpret_cast<SensorW*>(reinterpret_cast<unsigned char*>(smem_d) + S::GATE_OFF);
-        const int* src = reinterpret_cast<const int*>(a.sens);
-        int* dst = reinterpret_cast<int*>(ws);
-        for (int i = tid; i < kSensInferBytes / 4; i += NT) dst[i] = src[i];
-        gs.w = ws;
-        gs.tile = reinterpret_cast<__nv_bfloat16*>(WL);
-        gs.Gf = Sf;
-        __syncthreads();
-    }
-
-    mixed_axis<0, DIM, RECON, RIEMANN, TX, TY, TZ, NT, GATED>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax, &gs);
-    mixed_axis<1, DIM, RECON, RIEMANN, TX, TY, TZ, NT, GATED>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax, &gs);
-    if constexpr (DIM == 3) mixed_axis<2, DIM, RECON, RIEMANN, TX, TY, TZ, NT, GATED>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax, &gs);
+    mixed_axis<0, DIM, RECON, RIEMANN, TX, TY, TZ, NT, GATED>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
+    mixed_axis<1, DIM, RECON, RIEMANN, TX, TY, TZ, NT, GATED>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
+    if constexpr (DIM == 3) mixed_axis<2, DIM, RECON, RIEMANN, TX, TY, TZ, NT, GATED>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
     // ---- epilogue: the residual widened to FP64 and the FP64 stage update
     const double dt = a.ctl->dt;
     for (int c = tid; c < NC; c += NT) {
@@ -323,18 +243,6 @@ __global__ void __launch_bounds__(NT) mixed_stage_kernel(const StageArgs a) {
     }
     const double bm = block_max<NT>((double)smax, red);
     if (tid == 0) a.blockmax[b] = bm;
-    if constexpr (GATED) {
-        unsigned nl = gs.nlin, ne = gs.neval;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            nl += __shfl_xor_sync(0xffffffffu, nl, o);
-            ne += __shfl_xor_sync(0xffffffffu, ne, o);
-        }
-        if ((tid & 31) == 0 && a.sens_count) {
-            atomicAdd(a.sens_count, (unsigned long long)nl);
-            atomicAdd(a.sens_count + 1, (unsigned long long)ne);
-        }
-    }
 }
 
 template <int TX, int TY, int TZ> struct MixedViscShape {

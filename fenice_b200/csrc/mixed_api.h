@@ -16,7 +16,7 @@ struct MixedStage {
 // launch geometry is the FP64 stage kernel's (3-D: 8x8x8 tiles, 192 threads; 2-D: 16x15 tiles, 256 threads)
 MixedStage mixed_stage(int dim, int recon, int riemann);
 // the mixed WENO5-Z stage kernel with the learned troubled-cell sensor choosing linear or WENO5-Z reconstructions
-// (StageArgs::sens, sens_theta, sens_count)
+// (StageArgs::sens_flags)
 MixedStage mixed_stage_gated(int dim, int riemann);
 cudaError_t mixed_viscous_prepare();
 cudaError_t mixed_viscous_launch(const ViscArgs& a, int nblocks, cudaStream_t s);

@@ -23,6 +23,7 @@
 #include "ibm_host.h"
 #include "mixed_api.h"
 #include "sensor.cuh"
+#include "sensor_api.h"
 #include "stage.cuh"
 #include "viscous.cuh"
 
@@ -262,9 +263,13 @@ struct fvg_run {
     unsigned char* d_mask = nullptr;
     int *d_slot = nullptr, *d_ghost = nullptr, *d_img_cell = nullptr, *d_deep = nullptr;
     double *d_forced = nullptr, *d_img_w = nullptr, *d_ratio = nullptr, *d_gn = nullptr;
-    // the learned sensor (fvg_set_sensor): its weights (a copy), the logit threshold, the counters
+    // the learned sensor (fvg_set_sensor): its weights (a copy), the logit threshold, the refresh period and dilation,
+    // the two flag buffers (the result in sens_result), the counters
     void* sens = nullptr;
     float sens_theta = 0.0f;
+    int sens_every = 5, sens_radius = 4;
+    unsigned char* sens_flags[2] = {nullptr, nullptr};
+    unsigned char* sens_tiles = nullptr;   // per axis and stage tile
     unsigned long long* sens_count = nullptr;
     double* Ucur() { return cur ? Ut : U; }
 };
@@ -353,9 +358,7 @@ StageArgs stage_args(fvg_run* r, const double* Uin, const double* U0, double* ou
     a.ctl = r->ctl;
     a.gate = gate;
     for (int d = 0; d < 3; ++d) a.tiles[d] = r->tiles[d];
-    a.sens = static_cast<const SensorW*>(r->sens);
-    a.sens_theta = r->sens_theta;
-    a.sens_count = r->sens_count;
+    a.sens_flags = r->sens ? r->sens_tiles : nullptr;
     return a;
 }
 
@@ -472,6 +475,16 @@ cudaError_t residual_stage(fvg_run* r, const double* Uin, const double* U0, doub
     return e;
 }
 
+// The sensor's refresh of the gate (a gated run only): at the steps where ctl->steps % sens_every == 0 (ctl null: now).
+cudaError_t refresh_gate(fvg_run* r, const double* Uin, const Ctl* ctl) {
+    if (!r->sens) return cudaSuccess;
+    int per[3];
+    for (int d = 0; d < 3; ++d) per[d] = r->cfg.bc[2 * d] == FVG_BC_PERIODIC && r->cfg.bc[2 * d + 1] == FVG_BC_PERIODIC;
+    const int tile[3] = {r->dim == 3 ? Tile<3>::X : Tile<2>::X, r->dim == 3 ? Tile<3>::Y : Tile<2>::Y, r->dim == 3 ? Tile<3>::Z : 1};
+    return sensor_refresh(r->m, r->bc, r->eos, r->dim, Uin, r->sens, r->sens_theta, r->sens_radius, per, r->sens_flags[0], r->sens_flags[1], tile,
+                          r->tiles, r->sens_tiles, ctl, r->sens_every, r->sens_count, r->stream);
+}
+
 int axpy_blocks(const fvg_run* r) {
     const long long n = r->m.ncells * r->nvar;
     long long b = (n + 255) / 256;
@@ -503,6 +516,7 @@ cudaError_t enqueue_step(fvg_run* r) {
         r->cur ^= 1;
         return cudaGetLastError();
     }
+    if ((e = refresh_gate(r, r->U, c))) return e;
     if ((e = residual_stage(r, r->U, nullptr, r->R, kStoreR, 0, 0, 0, act))) return e;
     k_stage1_dt<<<1, 1024, 0, r->stream>>>(c, r->bm[0], r->nb, r->bmv[0], nbv);
     if (ts == FVG_TS_EULER) {
@@ -732,6 +746,9 @@ int fvg_destroy(fvg_run* run) {
     if (run->ctl) cudaFree(run->ctl);
     if (run->sens) cudaFree(run->sens);
     if (run->sens_count) cudaFree(run->sens_count);
+    for (unsigned char* f : run->sens_flags)
+        if (f) cudaFree(f);
+    if (run->sens_tiles) cudaFree(run->sens_tiles);
     for (void* p : {(void*)run->d_mask, (void*)run->d_slot, (void*)run->d_forced, (void*)run->d_ghost, (void*)run->d_img_cell, (void*)run->d_img_w,
                     (void*)run->d_ratio, (void*)run->d_gn, (void*)run->d_deep})
         if (p) cudaFree(p);
@@ -793,6 +810,7 @@ int fvg_residual(fvg_run* run, double predictor_half_dt, double* R, size_t ncell
         CK(launch_hancock(run, hancock_args(run, run->Ucur(), out, kStoreR, run->bm[0], always)));
         k_stage_max<<<1, 1024, 0, run->stream>>>(c, always, 0, run->bm[0], run->nbh, run->bmv[0], 0);
     } else {
+        CK(refresh_gate(run, run->Ucur(), nullptr));
         CK(residual_stage(run, run->Ucur(), nullptr, out, kStoreR, 0, 0, 0, always));
         k_stage_max<<<1, 1024, 0, run->stream>>>(c, always, 0, run->bm[0], run->nb, run->bmv[0], run->cfg.use_viscous ? run->nbv : 0);
     }
@@ -974,7 +992,7 @@ int fvg_get_timing(const fvg_run* run, double* stage_ms, long long* stage_launch
     return FVG_OK;
 }
 
-int fvg_set_sensor(fvg_run* run, const void* weights, float threshold) {
+int fvg_set_sensor(fvg_run* run, const void* weights, float threshold, int every, int radius) {
     if (!run) return FVG_ERR_ARGUMENT;
     CK(cudaSetDevice(run->cfg.device));
     CK(cudaStreamSynchronize(run->stream));
@@ -988,14 +1006,20 @@ int fvg_set_sensor(fvg_run* run, const void* weights, float threshold) {
         const MixedStage ms = mixed_stage(run->dim, run->cfg.reconstruction, run->cfg.riemann);
         run->stage.prepare = ms.prepare;
         run->stage.launch = ms.launch;
-        if (run->sens) cudaFree(run->sens);
+        cudaFree(run->sens);
         run->sens = nullptr;
         return FVG_OK;
     }
     if (run->cfg.precision != FVG_PREC_MIXED || run->cfg.reconstruction != FVG_RECON_WENO5)
         return fail(run, FVG_ERR_CONFIG, "the sensor gates the mixed-precision WENO5-Z form");
     if (run->ibm) return fail(run, FVG_ERR_CONFIG, "the sensor is not built for runs with an immersed body");
+    if (every <= 0) every = 5;
+    if (radius < 0) radius = (int)std::ceil(run->cfg.cfl * every) + 1;
+    const size_t fbytes = (size_t)run->m.plane * run->dim;
     if (!run->sens) CK(cudaMalloc(&run->sens, sizeof(SensorW)));
+    for (unsigned char*& f : run->sens_flags)
+        if (!f) CK(cudaMalloc(&f, fbytes));
+    if (!run->sens_tiles) CK(cudaMalloc(&run->sens_tiles, (size_t)run->nb * run->dim));
     if (!run->sens_count) {
         CK(cudaMalloc(&run->sens_count, 2 * sizeof(unsigned long long)));
         CK(cudaMemset(run->sens_count, 0, 2 * sizeof(unsigned long long)));
@@ -1006,6 +1030,8 @@ int fvg_set_sensor(fvg_run* run, const void* weights, float threshold) {
     run->stage.prepare = ms.prepare;
     run->stage.launch = ms.launch;
     run->sens_theta = threshold;
+    run->sens_every = every;
+    run->sens_radius = radius;
     return FVG_OK;
 }
 

@@ -5,6 +5,7 @@
 #include "grid.cuh"
 #include "host_common.h"
 #include "sensor.cuh"
+#include "sensor_api.h"
 
 #include <cuda_runtime.h>
 
@@ -351,12 +352,195 @@ __global__ void __launch_bounds__(256) k_sensor_infer(const SensorW* __restrict_
     }
 }
 
+// ------------------------------------------------------------------------------------------------ the gate
+__device__ __forceinline__ bool refresh_due(const Ctl* ctl, int every) { return !ctl || (ctl->active && ctl->steps % every == 0); }
+
+// The network's flags of every (cell, axis) of a state: each warp takes 32 rows (row = cell * DIM + axis) at a time, one
+// lane's features per row into two 16-row bf16 tiles, then the logits on the tensor cores.
+template <int DIM, int NV>
+__global__ void __launch_bounds__(256) k_sensor_flags(Mesh m, Bc bc, Eos<double> eos, const double* __restrict__ U, const SensorW* __restrict__ wg,
+                                                      float theta, unsigned char* __restrict__ flags, const Ctl* ctl, int every) {
+    if (!refresh_due(ctl, every)) return;
+    __shared__ SensorW w;
+    __shared__ __align__(16) __nv_bfloat16 tiles[8][32 * kLd];
+    {
+        const int* src = reinterpret_cast<const int*>(wg);
+        int* dst = reinterpret_cast<int*>(&w);
+        for (int i = threadIdx.x; i < kSensInferBytes / 4; i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    __nv_bfloat16* Xs = tiles[warp];
+    const long long rows = m.ncells * DIM, groups = (rows + 31) / 32;
+    for (long long gi = (long long)blockIdx.x * 8 + warp; gi < groups; gi += (long long)gridDim.x * 8) {
+        const long long row = gi * 32 + lane;
+        float f[kSensK];
+#pragma unroll
+        for (int k = 0; k < kSensK; ++k) f[k] = 0.0f;
+        if (row < rows) {
+            const long long c = row / DIM;
+            const int axis = (int)(row % DIM);
+            const int i = (int)(c % m.nx), j = (int)((c / m.nx) % m.ny), k = (int)(c / ((long long)m.nx * m.ny));
+            float q5[5][kSensQ];
+#pragma unroll
+            for (int s5 = 0; s5 < 5; ++s5) {
+                const int d = s5 - 2;
+                const St<double, NV> wv = c2p(eos, stencil_cons<DIM, NV>(m, bc, eos, U, i + (axis == 0 ? d : 0), j + (axis == 1 ? d : 0), k + (axis == 2 ? d : 0)));
+#pragma unroll
+                for (int sq = 0; sq < kSensQ; ++sq) {
+                    const int var = sensor_var<NV>(sq, axis);
+                    q5[s5][sq] = var >= 0 ? (float)wv[var < 0 ? 0 : var] : 0.0f;
+                }
+            }
+#pragma unroll
+            for (int sq = 0; sq < kSensQ; ++sq) {
+                const float v[5] = {q5[0][sq], q5[1][sq], q5[2][sq], q5[3][sq], q5[4][sq]};
+                sensor_quantity_features(v, f + 5 * sq);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kSensK; k += 2)
+            *reinterpret_cast<uint32_t*>(Xs + lane * kLd + k) = pack_bf16(f[k], f[k + 1]);
+        __syncwarp();
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            float lo, hi;
+            sensor_logits(w, Xs + half * 16 * kLd, kLd, lo, hi);
+            if (t == 0) {
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const long long r = gi * 32 + half * 16 + g + 8 * h;
+                    if (r >= rows) continue;
+                    const float z = h ? hi : lo;
+                    flags[(r % DIM) * m.plane + r / DIM] = z < theta ? 0 : 1;
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// One pass of the dilation: out = the largest flag within `radius` cells along axis d (every axis plane); the last pass
+// counts the linear (cell, axis) pairs.
+template <int DIM>
+__global__ void k_sensor_dilate(Mesh m, const unsigned char* __restrict__ in, unsigned char* __restrict__ out, int d, int radius, int periodic,
+                                const Ctl* ctl, int every, unsigned long long* counts) {
+    if (!refresh_due(ctl, every)) return;
+    const int n3[3] = {m.nx, m.ny, m.nz};
+    const long long stride = d == 0 ? 1 : (d == 1 ? (long long)m.nx : (long long)m.nx * m.ny);
+    unsigned long long lin = 0, all = 0;
+    const long long n = m.ncells * DIM;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int a = (int)(e / m.ncells);
+        const long long c = e % m.ncells;
+        const int p = (int)(d == 0 ? c % m.nx : (d == 1 ? (c / m.nx) % m.ny : c / ((long long)m.nx * m.ny)));
+        const unsigned char* src = in + a * m.plane;
+        unsigned char v = 0;
+        for (int o = -radius; o <= radius && !v; ++o) {
+            int q = p + o;
+            if (q < 0 || q >= n3[d]) {
+                if (!periodic) continue;
+                q = ((q % n3[d]) + n3[d]) % n3[d];
+            }
+            v = src[c + (long long)(q - p) * stride];
+        }
+        out[a * m.plane + c] = v;
+        if (counts) {
+            lin += v ? 0 : 1;
+            all += 1;
+        }
+    }
+    if (counts) {
+        atomicAdd(counts, lin);
+        atomicAdd(counts + 1, all);
+    }
+}
+
+// The tile flags of the stage kernels: tile b is linear along axis a (0) when no cell whose reconstructions along a it
+// needs (the tile extended by one cell along a) is flagged; a tile whose extension leaves the mesh across a side that is
+// not periodic stays WENO5-Z. One warp per (axis, tile); counts += [linear, all] tile-axes.
+template <int DIM>
+__global__ void k_sensor_tiles(Mesh m, const unsigned char* __restrict__ flags, int TX, int TY, int TZ, int t0, int t1, int t2, int per0, int per1,
+                               int per2, unsigned char* __restrict__ out, const Ctl* ctl, int every, unsigned long long* counts) {
+    if (!refresh_due(ctl, every)) return;
+    const int lane = threadIdx.x & 31;
+    const long long ntiles = (long long)t0 * t1 * t2, total = DIM * ntiles;
+    const int n3[3] = {m.nx, m.ny, m.nz}, T[3] = {TX, TY, TZ}, per[3] = {per0, per1, per2};
+    unsigned long long lin = 0, all = 0;
+    for (long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; w < total; w += ((long long)gridDim.x * blockDim.x) >> 5) {
+        const int a = (int)(w / ntiles);
+        const long long b = w % ntiles;
+        const int o[3] = {(int)(b % t0) * TX, (int)((b / t0) % t1) * TY, (int)(b / ((long long)t0 * t1)) * TZ};
+        int lo[3], hi[3];   // the cell range, inclusive
+        bool edge = false;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = o[d];
+            hi[d] = o[d] + T[d] - 1 < n3[d] - 1 ? o[d] + T[d] - 1 : n3[d] - 1;
+        }
+        lo[a] -= 1;
+        hi[a] += 1;
+        if (!per[a] && (lo[a] < 0 || hi[a] > n3[a] - 1)) edge = true;
+        const int e0 = hi[0] - lo[0] + 1, e1 = hi[1] - lo[1] + 1, e2 = hi[2] - lo[2] + 1;
+        const int cnt = e0 * e1 * e2;
+        bool any = edge;
+        for (int k = lane; k < cnt && !edge; k += 32) {
+            int p3[3] = {lo[0] + k % e0, lo[1] + (k / e0) % e1, lo[2] + k / (e0 * e1)};
+            p3[a] = ((p3[a] % n3[a]) + n3[a]) % n3[a];
+            any = any || flags[a * m.plane + ((long long)p3[2] * m.ny + p3[1]) * m.nx + p3[0]] != 0;
+        }
+        any = __any_sync(0xffffffffu, any);
+        if (lane == 0) {
+            out[w] = any ? 1 : 0;
+            lin += any ? 0 : 1;
+            all += 1;
+        }
+    }
+    if (counts && lane == 0 && all) {
+        atomicAdd(counts, lin);
+        atomicAdd(counts + 1, all);
+    }
+}
+
 int grid_for(long long rows) {
     const long long chunks = (rows + 15) / 16, b = (chunks + 7) / 8;
     return (int)(b < 1 ? 1 : (b > 148 * 4 ? 148 * 4 : b));
 }
 
 }   // namespace
+
+cudaError_t fvg::sensor_refresh(const Mesh& m, const Bc& bc, const Eos<double>& eos, int dim, const double* U, const void* weights, float theta,
+                                int radius, const int periodic[3], unsigned char* flags0, unsigned char* flags1, const int tile[3],
+                                const int tiles[3], unsigned char* tile_flags, const Ctl* ctl, int every, unsigned long long* counts,
+                                cudaStream_t s) {
+    const long long groups = (m.ncells * dim + 31) / 32;
+    const int fb = (int)((groups + 7) / 8 < 148 * 8 ? (groups + 7) / 8 : 148 * 8);
+    const SensorW* w = static_cast<const SensorW*>(weights);
+    if (dim == 3)
+        k_sensor_flags<3, 5><<<fb, 256, 0, s>>>(m, bc, eos, U, w, theta, flags0, ctl, every);
+    else
+        k_sensor_flags<2, 4><<<fb, 256, 0, s>>>(m, bc, eos, U, w, theta, flags0, ctl, every);
+    const long long n = m.ncells * dim;
+    const int db = (int)((n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16);
+    unsigned char* bufs[2] = {flags0, flags1};
+    int cur = 0;
+    for (int d = 0; d < dim; ++d) {
+        if (dim == 3)
+            k_sensor_dilate<3><<<db, 256, 0, s>>>(m, bufs[cur], bufs[cur ^ 1], d, radius, periodic[d], ctl, every, nullptr);
+        else
+            k_sensor_dilate<2><<<db, 256, 0, s>>>(m, bufs[cur], bufs[cur ^ 1], d, radius, periodic[d], ctl, every, nullptr);
+        cur ^= 1;
+    }
+    const long long nt = (long long)tiles[0] * tiles[1] * tiles[2] * dim;
+    const int tb = (int)((nt * 32 + 255) / 256 < 148 * 16 ? (nt * 32 + 255) / 256 : 148 * 16);
+    if (dim == 3)
+        k_sensor_tiles<3><<<tb, 256, 0, s>>>(m, bufs[cur], tile[0], tile[1], tile[2], tiles[0], tiles[1], tiles[2], periodic[0], periodic[1], periodic[2],
+                                             tile_flags, ctl, every, counts);
+    else
+        k_sensor_tiles<2><<<tb, 256, 0, s>>>(m, bufs[cur], tile[0], tile[1], 1, tiles[0], tiles[1], 1, periodic[0], periodic[1], 0, tile_flags, ctl,
+                                             every, counts);
+    return cudaGetLastError();
+}
 
 // ------------------------------------------------------------------------------------------------ C ABI
 namespace {

@@ -2,10 +2,10 @@
 // the cell's two WENO5-Z reconstructions along that axis may take the linear fifth-order upwind values instead.
 //
 // Inputs (per cell and axis): the 5 cells c-2 .. c+2 along the axis, 5 primitive quantities each (rho, the normal
-// velocity, the two tangential velocities (the second is 0 on a 2-D mesh), p). Per quantity, with r the root mean square
-// of its 5 values (1 when all are 0): the centre v0 / r and the four differences (v_k - v0) / r, each scaled by 200 and
-// clamped to [-16, 16] (relative jumps above 8 % look alike: such a cell is troubled anyway). 25 features, padded with
-// zeros to the 32 of two tensor-core k-steps.
+// velocity, the two tangential velocities (the second is 0 on a 2-D mesh), p). Per quantity: the stencil's shape (the
+// four differences v_k - v0 over the largest of them) and its amplitude (log2(1 + 1e4 M / r) / 4, M that largest
+// difference, r the root mean square of the 5 values). 25 features, padded with zeros to the 32 of two tensor-core
+// k-steps.
 // Network: 32 -> 32 (ReLU) -> 32 (ReLU) -> 1 logit; weights and hidden activations in bfloat16, sums in float32
 // (mma.sync m16n8k16 bf16 with f32 accumulators, one warp per 16 cells). The cell is smooth (linear reconstruction)
 // when the logit is below a threshold chosen for a low miss rate; otherwise, and for every cell the network is not sure
@@ -24,7 +24,6 @@ constexpr int kSensQ = 5;             // quantities per stencil cell
 constexpr int kSensF = 5 * kSensQ;    // features
 constexpr int kSensK = 32;            // padded input width
 constexpr int kSensH = 32;            // hidden width
-constexpr float kSensScale = 200.0f, kSensClamp = 16.0f;
 
 // Device weights of the network as the kernels read them.
 struct SensorW {
@@ -49,17 +48,23 @@ struct SensorP {
 };
 constexpr int kSensParams = sizeof(SensorP) / sizeof(float);
 
-__device__ __forceinline__ float sens_clamp(float x) { return fminf(fmaxf(kSensScale * x, -kSensClamp), kSensClamp); }
-
-// The five features of one quantity from its values at c-2 .. c+2 (f[2] the centre entry).
+// The five features of one quantity from its values at c-2 .. c+2: the shape of the stencil, (v_k - v0) / M for the four
+// neighbours with M = max_k |v_k - v0| (0 when the stencil is flat), and its amplitude against the quantity's size,
+// log2(1 + 1e4 M / r) / 4 with r the root mean square of the five values (WENO-Z compares the smoothness indicators with
+// an epsilon of 1e-6 r^2, so jumps of order 1e-3 r separate the two regimes). f[2] is the amplitude.
 __device__ __forceinline__ void sensor_quantity_features(const float v[5], float f[5]) {
-    float s = 0.0f;
+    float s = 0.0f, M = 0.0f;
+    const float v0 = v[2];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) s += v[k] * v[k];
+    for (int k = 0; k < 5; ++k) {
+        s += v[k] * v[k];
+        M = fmaxf(M, fabsf(v[k] - v0));
+    }
     const float r = s > 0.0f ? sqrtf(0.2f * s) : 1.0f;
-    const float ir = 1.0f / r, v0 = v[2];
+    const float iM = M > 0.0f ? 1.0f / M : 0.0f;
 #pragma unroll
-    for (int k = 0; k < 5; ++k) f[k] = sens_clamp(k == 2 ? v0 * ir : (v[k] - v0) * ir);
+    for (int k = 0; k < 5; ++k) f[k] = (v[k] - v0) * iM;
+    f[2] = 0.25f * __log2f(1.0f + 1e4f * M / r);
 }
 
 // Index of sensor quantity sq (rho, u_n, u_t1, u_t2, p) among the primitive variables [rho, u, v, p(, w)] for a sweep

@@ -41,11 +41,9 @@ struct StageArgs {
     const Ctl* ctl;             // dt
     const int* gate;            // the kernel does nothing unless *gate (the control block's `active` or `seed`)
     int tiles[3];               // tiles per axis
-    // the learned troubled-cell sensor (mixed-precision WENO5-Z kernels with the sensor only): its device weights, the
-    // logit threshold below which a cell's reconstructions are linear, and counters (cell-axes linear, evaluated)
-    const struct SensorW* sens;
-    float sens_theta;
-    unsigned long long* sens_count;
+    // the learned troubled-cell sensor's tile flags (mixed-precision WENO5-Z kernels with the sensor only): one byte per
+    // axis and tile (axis-major), 1 where the tile's reconstructions along the axis stay WENO5-Z, 0 where they are linear
+    const unsigned char* sens_flags;
 };
 
 template <int DIM, int RECON, int TX, int TY, int TZ> struct StageShape {

@@ -6,6 +6,8 @@ reference's cell order ((k ny + j) nx + i), evaluated at cell centres.
 * ``riemann_quadrants``: four constant states split at (0.5, 0.5) of [0,1]^2, drawn from a seeded PCG64 in NE, NW, SW,
   SE order with rho, p ~ U[0.1, 2], u, v ~ U[-1, 1] (a case file with a background state and three box regions,
   CaseFile.hpp:110-111, describes the same field).
+* ``riemann_octants``: the 3-D analogue, eight constant states split at (0.5, 0.5, 0.5) of [0,1]^3 (training data of
+  the learned sensor).
 * ``shock_tubes``: a batch of seeded 1-D shock tubes on nx x 1 meshes, nx log-uniform in [128, 8192], interface at
   x = 0.5, rho ~ U[0.1, 1], p ~ U[0.05, 1], u ~ U[-1, 1] on each side.
 """
@@ -67,6 +69,26 @@ def quadrant_params(n):
     """WENO5-Z + HLLC + SSP-RK3, CFL 0.4, transmissive sides, [0, 1]^2 (run to t = 0.25)."""
     return dict(nx=n, ny=n, Lx=1.0, Ly=1.0, gamma=1.4, reconstruction="weno5", riemann_solver="HLLC", time_scheme="SSP Runge-Kutta 3",
                 cfl=0.4, bc_xmin="transmissive", bc_xmax="transmissive", bc_ymin="transmissive", bc_ymax="transmissive")
+
+
+def riemann_octants(n, seed, gamma=1.4):
+    """Eight constant states (rho, p ~ U[0.1, 2], u, v, w ~ U[-1, 1], drawn in octant order x fastest) on n^3 cells of
+    [0, 1]^3."""
+    rng = np.random.default_rng(seed)
+    st = [(rng.uniform(0.1, 2), rng.uniform(-1, 1), rng.uniform(-1, 1), rng.uniform(0.1, 2), rng.uniform(-1, 1)) for _ in range(8)]
+    c = (np.arange(n) + 0.5) / n
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    o = ((x >= 0.5).astype(int) + 2 * (y >= 0.5) + 4 * (z >= 0.5)).ravel()
+    W = np.zeros((n ** 3, 5))
+    for k, w in enumerate(st):
+        W[o == k] = w
+    return prim_to_cons(W, gamma)
+
+
+def octant_params(n):
+    """WENO5-Z + HLLC + SSP-RK3, CFL 0.4, transmissive sides, [0, 1]^3."""
+    p = dict(quadrant_params(n), nz=n, Lz=1.0, bc_zmin="transmissive", bc_zmax="transmissive")
+    return p
 
 
 def shock_tubes(n=512, seed=0, nx_min=128, nx_max=8192, gamma=1.4):

@@ -95,7 +95,7 @@ def load_library(path=LIB_PATH):
     lib.fvg_sensor_adam.argtypes = [c_p, c_p, c_p, c_p, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, c_p, c_p]
     lib.fvg_sensor_pack.argtypes = [c_p, c_p, c_p]
     lib.fvg_sensor_infer.argtypes = [c_p, c_p, ctypes.c_longlong, c_p, c_p]
-    lib.fvg_set_sensor.argtypes = [c_p, c_p, ctypes.c_float]
+    lib.fvg_set_sensor.argtypes = [c_p, c_p, ctypes.c_float, ctypes.c_int, ctypes.c_int]
     lib.fvg_get_sensor_counts.argtypes = [c_p, ll, ll, ctypes.c_int]
     _lib = lib
     return lib
@@ -221,10 +221,11 @@ class Run:
         self._check(self.lib.fvg_get_timing(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d)), "get_timing")
         return {"stage_ms": a.value, "stage_launches": b.value, "viscous_ms": c.value, "viscous_launches": d.value}
 
-    def set_sensor(self, sensor, threshold=0.0):
-        """Gate the WENO5-Z reconstructions (mixed precision) with a trained ``fenice_b200.sensor.Sensor`` (None: off)."""
+    def set_sensor(self, sensor, threshold=0.0, every=0, radius=-1):
+        """Gate the WENO5-Z reconstructions (mixed precision) with a trained ``fenice_b200.sensor.Sensor`` (None: off),
+        refreshed every `every` steps and grown by `radius` cells (defaults: 5 steps, ceil(cfl every) + 1 cells)."""
         ptr = None if sensor is None else sensor.weights_ptr()
-        self._check(self.lib.fvg_set_sensor(self.h, ptr, float(threshold)), "set_sensor")
+        self._check(self.lib.fvg_set_sensor(self.h, ptr, float(threshold), int(every), int(radius)), "set_sensor")
 
     def sensor_counts(self, reset=False):
         """(cell-axis evaluations that went linear, all evaluations) since the last reset."""

@@ -168,13 +168,17 @@ def choose_threshold(logits, troubled, miss=0.002):
 
 def quadrant_training_data(sensor, seeds, n=512, t_end=0.25, snapshots=5, tau=TAU, keep_div=8, precision=0):
     """Samples of seeded four-quadrant problems run with plain WENO5-Z (FP64: the reference's arithmetic), taken at
-    `snapshots` evenly spaced times up to t_end."""
+    `snapshots` evenly spaced times up to t_end (up to the divergence of a problem whose seeded states make WENO5-Z lose
+    positivity, as the reference does without its positivity fallback)."""
     torch = sensor.torch
     Xs, Ds = [], []
     for s in seeds:
         run = Run(initial.quadrant_params(n), U=initial.riemann_quadrants(n, s), precision=precision, device=sensor.dev.index)
         for k in range(1, snapshots + 1):
-            run.run(t_end * k / snapshots)
+            try:
+                run.run(t_end * k / snapshots)
+            except RuntimeError:   # the seeded states can make WENO5-Z lose positivity: the snapshots so far stay
+                break
             X, D, _ = sensor.samples(run, tau, keep_div, seed=1000 * s + k, capacity=run.ncells * 2)
             Xs.append(X.clone())
             Ds.append(D.clone())
@@ -200,4 +204,22 @@ def taylor_green_training_data(sensor, n=64, steps=200, snapshots=5, tau=TAU, ke
         Xs.append(X.clone())
         Ds.append(D.clone())
     run.close()
+    return torch.cat(Xs), torch.cat(Ds)
+
+
+def octant_training_data(sensor, seeds, n=64, t_end=0.2, snapshots=4, tau=TAU, keep_div=8, precision=0):
+    """Samples of seeded eight-octant problems (3-D) run with plain WENO5-Z, as quadrant_training_data."""
+    torch = sensor.torch
+    Xs, Ds = [], []
+    for s in seeds:
+        run = Run(initial.octant_params(n), U=initial.riemann_octants(n, s), precision=precision, device=sensor.dev.index)
+        for k in range(1, snapshots + 1):
+            try:
+                run.run(t_end * k / snapshots)
+            except RuntimeError:
+                break
+            X, D, _ = sensor.samples(run, tau, keep_div, seed=5000 + 1000 * s + k, capacity=run.ncells * 3)
+            Xs.append(X.clone())
+            Ds.append(D.clone())
+        run.close()
     return torch.cat(Xs), torch.cat(Ds)

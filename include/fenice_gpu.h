@@ -161,8 +161,12 @@ int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long long plane
  *   fvg_sensor_adam     one Adam step of the float32 parameters (grad is cleared) and their device weights
  *   fvg_sensor_pack     device weights of float32 parameters; fvg_sensor_infer: logits of n feature rows
  * Parameter layout (floats): W1[32][32] (inputs 25..31 unused), b1[32], W2[32][32], b2[32], w3[32], b3.
- * fvg_set_sensor gates a mixed-precision WENO5-Z run with device weights (copied; NULL: plain WENO5-Z again);
- * fvg_get_sensor_counts returns the (cell, axis) evaluations that went linear and all evaluations since the last reset.
+ * fvg_set_sensor gates a mixed-precision WENO5-Z run with device weights (copied; NULL: plain WENO5-Z again): every
+ * `every` steps (<= 0: 5) a kernel evaluates the network on every (cell, axis) of the state, the troubled set is grown by
+ * `radius` cells along every axis (< 0: ceil(cfl every) + 1, the distance a wave travels until the next refresh, plus
+ * one) and reduced to the stage kernels' tiles: a tile whose cells are all untroubled along an axis takes the linear
+ * reconstruction for every face of that sweep. fvg_get_sensor_counts returns the (tile, axis) pairs the refreshes
+ * passed to the linear reconstruction and all pairs, since the last reset.
  * Failures of the calls without a run handle: fvg_create_error(). */
 int fvg_sensor_sizes(int* n_params, int* weights_bytes, int* n_inputs);
 int fvg_sensor_extract(fvg_run* run, int mode, int keep_div, unsigned seed, float tau, float* X, float* departure, int* count,
@@ -172,7 +176,7 @@ int fvg_sensor_adam(float* params, float* m, float* v, float* grad, int step, fl
                     void* stream);
 int fvg_sensor_pack(const float* params, void* weights, void* stream);
 int fvg_sensor_infer(const void* weights, const float* X, long long n, float* logits, void* stream);
-int fvg_set_sensor(fvg_run* run, const void* weights, float threshold);
+int fvg_set_sensor(fvg_run* run, const void* weights, float threshold, int every, int radius);
 int fvg_get_sensor_counts(fvg_run* run, long long* linear, long long* evaluated, int reset);
 
 /* ---- Batched independent problems (no counterpart in the reference, which runs one Simulation per process).

@@ -2,9 +2,10 @@
 labels and network, the check of the GPU sensor kernels (fenice_b200/csrc/sensor.cuh).
 
 * stencil_features(Q5): the 25 features of one (cell, axis): the 5 cells c-2 .. c+2 along the axis, 5 primitive
-  quantities each (rho, normal velocity, the two tangential velocities (0 on a 2-D mesh), p). Per quantity, with r the
-  root mean square of its 5 values (1 when all are 0), the centre value v0 / r and the four differences (v_k - v0) / r,
-  each scaled by 200 and clamped to [-16, 16]; quantity-major, padded with zeros to 32 inputs.
+  quantities each (rho, normal velocity, the two tangential velocities (0 on a 2-D mesh), p). Per quantity, with
+  M = max_k |v_k - v0| and r the root mean square of the 5 values (1 when all are 0): the shape (v_k - v0) / M of the
+  four neighbours (0 when M = 0) and, in the centre slot, the amplitude log2(1 + 1e4 M / r) / 4; quantity-major, padded
+  with zeros to 32 inputs.
 * departure(Q5): the label statistic: over the 5 quantities and both WENO5-Z reconstructions centred on the cell (the
   value at its right face from c-2 .. c+2 and at its left face from c+2 .. c-2), the largest |omega_k - d_k| of the
   WENO-Z weights (the reference's weno5z, cpp/src/Schemes.cpp:328-353) against the linear ones d = (0.1, 0.6, 0.3). A cell
@@ -27,10 +28,6 @@ def bf16(a):
     return r.astype(np.uint32).view(np.float32)
 
 
-def g(x):
-    return np.clip(np.float32(200.0) * x, -16.0, 16.0).astype(np.float32)
-
-
 def axis_quantities(W, axis):
     """(..., 5, 5) stencil of primitive cells [rho, u, v, p, w] along `axis` -> [rho, u_n, u_t1, u_t2, p]."""
     W = np.asarray(W, dtype=np.float64)
@@ -41,16 +38,17 @@ def axis_quantities(W, axis):
 
 def stencil_features(Q5):
     """(n, 5, 5) stencil quantities -> (n, 32) features (quantity-major: 5 entries per quantity, positions c-2 .. c+2
-    with the centre entry v0 / r; columns 25 .. 31 zero)."""
+    with the amplitude in the centre entry; columns 25 .. 31 zero)."""
     Q5 = np.asarray(Q5, dtype=np.float32)
     r = np.sqrt(np.float32(0.2) * np.sum(Q5 * Q5, axis=1))
     r = np.where(r > 0, r, np.float32(1.0)).astype(np.float32)
-    ir = (np.float32(1.0) / r).astype(np.float32)
-    v0 = Q5[:, 2, :]
-    d = (Q5 - v0[:, None, :]) * ir[:, None, :]
-    d[:, 2, :] = v0 * ir
+    d = Q5 - Q5[:, 2:3, :]
+    M = np.abs(d).max(axis=1)
+    iM = np.where(M > 0, np.float32(1.0) / np.where(M > 0, M, 1), 0).astype(np.float32)
+    f = d * iM[:, None, :]
+    f[:, 2, :] = 0.25 * np.log2(1.0 + 1e4 * M / r)
     out = np.zeros((len(Q5), NK), dtype=np.float32)
-    out[:, :NF] = g(np.transpose(d, (0, 2, 1)).reshape(len(Q5), NF))
+    out[:, :NF] = np.transpose(f, (0, 2, 1)).reshape(len(Q5), NF)
     return out
 
 
