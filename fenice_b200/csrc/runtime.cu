@@ -491,8 +491,9 @@ int axpy_blocks(const fvg_run* r) {
     return (int)(b < 148 * 16 ? b : 148 * 16);
 }
 
-// The launches of one time step on the run's stream (no host synchronisation).
-cudaError_t enqueue_step(fvg_run* r) {
+// The launches of one time step on the run's stream (no host synchronisation). refresh = false leaves out the sensor's
+// refresh (a graph of sens_every steps keeps it in its first step only).
+cudaError_t enqueue_step(fvg_run* r, bool refresh = true) {
     cudaError_t e;
     Ctl* c = r->ctl;
     const int* act = &c->active;
@@ -516,7 +517,7 @@ cudaError_t enqueue_step(fvg_run* r) {
         r->cur ^= 1;
         return cudaGetLastError();
     }
-    if ((e = refresh_gate(r, r->U, c))) return e;
+    if (refresh && (e = refresh_gate(r, r->U, c))) return e;
     if ((e = residual_stage(r, r->U, nullptr, r->R, kStoreR, 0, 0, 0, act))) return e;
     k_stage1_dt<<<1, 1024, 0, r->stream>>>(c, r->bm[0], r->nb, r->bmv[0], nbv);
     if (ts == FVG_TS_EULER) {
@@ -863,13 +864,18 @@ static int run_steps(fvg_run* run, double t_end, int max_steps, int use_graph, i
         // every enqueue flipped the ping-pong; only the steps that ran moved the state
         if (hancock) run->cur = (cur0 + done) & 1;
     } else {
-        // a graph of two steps (the MUSCL-Hancock ping-pong returns to its buffer after two)
+        // a graph of two steps (the MUSCL-Hancock ping-pong returns to its buffer after two), or, with the sensor, of
+        // sens_every steps with its refresh in the first (the step count of a run call starts at 0, and a graph
+        // advances it by sens_every while the run is active, so the first step of every graph is a refresh step)
         cudaGraphExec_t& graph = run->graph[run->cur];
         if (!graph) {
             const int cur0 = run->cur;
+            const int per_graph = run->sens ? run->sens_every : 2;
             cudaGraph_t g;
             CK(cudaStreamBeginCapture(run->stream, cudaStreamCaptureModeThreadLocal));
-            cudaError_t e1 = enqueue_step(run), e2 = enqueue_step(run);
+            cudaError_t e1 = cudaSuccess;
+            for (int k = 0; k < per_graph && e1 == cudaSuccess; ++k) e1 = enqueue_step(run, k == 0);
+            cudaError_t e2 = cudaSuccess;
             cudaError_t e3 = cudaStreamEndCapture(run->stream, &g);
             run->cur = cur0;
             if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)

@@ -355,65 +355,64 @@ __global__ void __launch_bounds__(256) k_sensor_infer(const SensorW* __restrict_
 // ------------------------------------------------------------------------------------------------ the gate
 __device__ __forceinline__ bool refresh_due(const Ctl* ctl, int every) { return !ctl || (ctl->active && ctl->steps % every == 0); }
 
-// The network's flags of every (cell, axis) of a state: each warp takes 32 rows (row = cell * DIM + axis) at a time, one
-// lane's features per row into two 16-row bf16 tiles, then the logits on the tensor cores.
-template <int DIM, int NV>
-__global__ void __launch_bounds__(256) k_sensor_flags(Mesh m, Bc bc, Eos<double> eos, const double* __restrict__ U, const SensorW* __restrict__ wg,
-                                                      float theta, unsigned char* __restrict__ flags, const Ctl* ctl, int every) {
+// The network's flags of every (cell, axis), tiled: a CTA takes a BX x BY (x BZ) block of cells, recovers the
+// primitive state of the block and a 2-cell halo once per cell into shared memory (float), then its warps take 16
+// (cell, axis) rows at a time: features of the row's 5-cell stencil into the warp's bf16 tile (one lane per row and
+// quantity), logits on the tensor cores.
+template <int DIM, int NV, int BX, int BY, int BZ>
+__global__ void __launch_bounds__(256) k_sensor_flags_t(Mesh m, Bc bc, Eos<double> eos, const double* __restrict__ U, const SensorW* __restrict__ wg,
+                                                        float theta, unsigned char* __restrict__ flags, const Ctl* ctl, int every, int nb0, int nb1) {
     if (!refresh_due(ctl, every)) return;
-    __shared__ SensorW w;
-    __shared__ __align__(16) __nv_bfloat16 tiles[8][32 * kLd];
+    constexpr int EX = BX + 4, EY = BY + 4, EZ = DIM == 3 ? BZ + 4 : 1, BOX = EX * EY * EZ, NC = BX * BY * BZ, ROWS = NC * DIM;
+    __shared__ __align__(16) unsigned char wbuf[kSensInferBytes];
+    __shared__ float P[NV * BOX];
+    __shared__ __align__(16) __nv_bfloat16 tiles[8][16 * kLd];
+    const SensorW& w = *reinterpret_cast<const SensorW*>(wbuf);
     {
         const int* src = reinterpret_cast<const int*>(wg);
-        int* dst = reinterpret_cast<int*>(&w);
+        int* dst = reinterpret_cast<int*>(wbuf);
         for (int i = threadIdx.x; i < kSensInferBytes / 4; i += blockDim.x) dst[i] = src[i];
+        for (int i = threadIdx.x; i < 8 * 16; i += blockDim.x)
+            for (int k = kSensF; k < kSensK; ++k) tiles[i / 16][(i % 16) * kLd + k] = __float2bfloat16_rn(0.0f);
+    }
+    const int b = blockIdx.x;
+    const int o0 = (b % nb0) * BX, o1 = ((b / nb0) % nb1) * BY, o2 = DIM == 3 ? (b / (nb0 * nb1)) * BZ : 0;
+    for (int e = threadIdx.x; e < BOX; e += blockDim.x) {
+        const int i = o0 + e % EX - 2, j = o1 + (e / EX) % EY - 2, k = DIM == 3 ? o2 + e / (EX * EY) - 2 : 0;
+        const St<double, NV> wv = c2p(eos, stencil_cons<DIM, NV>(m, bc, eos, U, i, j, k));
+#pragma unroll
+        for (int q = 0; q < NV; ++q) P[q * BOX + e] = (float)wv[q];
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     __nv_bfloat16* Xs = tiles[warp];
-    const long long rows = m.ncells * DIM, groups = (rows + 31) / 32;
-    for (long long gi = (long long)blockIdx.x * 8 + warp; gi < groups; gi += (long long)gridDim.x * 8) {
-        const long long row = gi * 32 + lane;
-        float f[kSensK];
+    for (int ch = warp; ch * 16 < ROWS; ch += 8) {
+        for (int it = lane; it < 16 * kSensQ; it += 32) {
+            const int row = it / kSensQ, sq = it % kSensQ, r = ch * 16 + row;
+            const int c = r / DIM, axis = r % DIM;
+            const int var = sensor_var<NV>(sq, axis);
+            float f[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+            if (var >= 0) {
+                const int e = ((DIM == 3 ? c / (BX * BY) + 2 : 0) * EY + (c / BX) % BY + 2) * EX + c % BX + 2;
+                const int st = axis == 0 ? 1 : (axis == 1 ? EX : EX * EY);
+                float v[5];
 #pragma unroll
-        for (int k = 0; k < kSensK; ++k) f[k] = 0.0f;
-        if (row < rows) {
-            const long long c = row / DIM;
-            const int axis = (int)(row % DIM);
-            const int i = (int)(c % m.nx), j = (int)((c / m.nx) % m.ny), k = (int)(c / ((long long)m.nx * m.ny));
-            float q5[5][kSensQ];
-#pragma unroll
-            for (int s5 = 0; s5 < 5; ++s5) {
-                const int d = s5 - 2;
-                const St<double, NV> wv = c2p(eos, stencil_cons<DIM, NV>(m, bc, eos, U, i + (axis == 0 ? d : 0), j + (axis == 1 ? d : 0), k + (axis == 2 ? d : 0)));
-#pragma unroll
-                for (int sq = 0; sq < kSensQ; ++sq) {
-                    const int var = sensor_var<NV>(sq, axis);
-                    q5[s5][sq] = var >= 0 ? (float)wv[var < 0 ? 0 : var] : 0.0f;
-                }
+                for (int k = 0; k < 5; ++k) v[k] = P[var * BOX + e + (k - 2) * st];
+                sensor_quantity_features(v, f);
             }
 #pragma unroll
-            for (int sq = 0; sq < kSensQ; ++sq) {
-                const float v[5] = {q5[0][sq], q5[1][sq], q5[2][sq], q5[3][sq], q5[4][sq]};
-                sensor_quantity_features(v, f + 5 * sq);
-            }
+            for (int k = 0; k < 5; ++k) Xs[row * kLd + 5 * sq + k] = __float2bfloat16_rn(f[k]);
         }
-#pragma unroll
-        for (int k = 0; k < kSensK; k += 2)
-            *reinterpret_cast<uint32_t*>(Xs + lane * kLd + k) = pack_bf16(f[k], f[k + 1]);
         __syncwarp();
+        float lo, hi;
+        sensor_logits(w, Xs, kLd, lo, hi);
+        if (t == 0) {
 #pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            float lo, hi;
-            sensor_logits(w, Xs + half * 16 * kLd, kLd, lo, hi);
-            if (t == 0) {
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const long long r = gi * 32 + half * 16 + g + 8 * h;
-                    if (r >= rows) continue;
-                    const float z = h ? hi : lo;
-                    flags[(r % DIM) * m.plane + r / DIM] = z < theta ? 0 : 1;
-                }
+            for (int h = 0; h < 2; ++h) {
+                const int r = ch * 16 + g + 8 * h, c = r / DIM, axis = r % DIM;
+                const int i = o0 + c % BX, j = o1 + (c / BX) % BY, k = DIM == 3 ? o2 + c / (BX * BY) : 0;
+                if (i >= m.nx || j >= m.ny || k >= m.nz) continue;
+                flags[axis * m.plane + ((long long)k * m.ny + j) * m.nx + i] = (h ? hi : lo) < theta ? 0 : 1;
             }
         }
         __syncwarp();
@@ -513,13 +512,14 @@ cudaError_t fvg::sensor_refresh(const Mesh& m, const Bc& bc, const Eos<double>& 
                                 int radius, const int periodic[3], unsigned char* flags0, unsigned char* flags1, const int tile[3],
                                 const int tiles[3], unsigned char* tile_flags, const Ctl* ctl, int every, unsigned long long* counts,
                                 cudaStream_t s) {
-    const long long groups = (m.ncells * dim + 31) / 32;
-    const int fb = (int)((groups + 7) / 8 < 148 * 8 ? (groups + 7) / 8 : 148 * 8);
     const SensorW* w = static_cast<const SensorW*>(weights);
-    if (dim == 3)
-        k_sensor_flags<3, 5><<<fb, 256, 0, s>>>(m, bc, eos, U, w, theta, flags0, ctl, every);
-    else
-        k_sensor_flags<2, 4><<<fb, 256, 0, s>>>(m, bc, eos, U, w, theta, flags0, ctl, every);
+    if (dim == 3) {
+        const int b0 = (m.nx + 7) / 8, b1 = (m.ny + 7) / 8, b2 = (m.nz + 3) / 4;
+        k_sensor_flags_t<3, 5, 8, 8, 4><<<b0 * b1 * b2, 256, 0, s>>>(m, bc, eos, U, w, theta, flags0, ctl, every, b0, b1);
+    } else {
+        const int b0 = (m.nx + 31) / 32, b1 = (m.ny + 7) / 8;
+        k_sensor_flags_t<2, 4, 32, 8, 1><<<b0 * b1, 256, 0, s>>>(m, bc, eos, U, w, theta, flags0, ctl, every, b0, b1);
+    }
     const long long n = m.ncells * dim;
     const int db = (int)((n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16);
     unsigned char* bufs[2] = {flags0, flags1};
