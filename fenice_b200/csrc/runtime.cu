@@ -252,6 +252,7 @@ struct fvg_run {
     struct EvTimer {
         std::vector<cudaEvent_t> ev;
         size_t used = 0;
+        std::vector<size_t> step_start;   // ev index at the start of each step enqueued since the last flush
         double ms = 0.0;
         long long n = 0;
     };
@@ -415,9 +416,12 @@ void timer_mark(fvg_run* r, fvg_run::EvTimer& t) {
     cudaEventRecord(t.ev[t.used++], r->stream);
 }
 
-// after a stream synchronisation: add up the recorded (start, end) pairs
-void timer_flush(fvg_run::EvTimer& t) {
-    for (size_t k = 0; k + 1 < t.used; k += 2) {
+// after a stream synchronisation: add up the recorded (start, end) pairs of the first `steps` steps enqueued since the
+// last flush (the steps that ran; the gated launches of steps past the end are not counted)
+void timer_flush(fvg_run::EvTimer& t, long long steps = -1) {
+    const size_t end = (steps >= 0 && (size_t)steps < t.step_start.size()) ? t.step_start[steps] : t.used;
+    t.step_start.clear();
+    for (size_t k = 0; k + 1 < end; k += 2) {
         float ms = 0.0f;
         if (cudaEventElapsedTime(&ms, t.ev[k], t.ev[k + 1]) == cudaSuccess) {
             t.ms += ms;
@@ -848,15 +852,18 @@ static int run_steps(fvg_run* run, double t_end, int max_steps, int use_graph, i
     } else if (run->timing) {
         // timed: the same launches, one step at a time, events around the kernels
         const int cur0 = run->cur;
-        int chunk = 4;
+        int chunk = 4, before = 0;
         while (true) {
             for (int k = 0; k < chunk; ++k) {
+                run->t_stage.step_start.push_back(run->t_stage.used);
+                run->t_visc.step_start.push_back(run->t_visc.used);
                 cudaError_t e = enqueue_step(run);
                 if (e != cudaSuccess) return fail(run, FVG_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
             }
             if ((rc = read_ctl(run, &h))) return rc;
-            timer_flush(run->t_stage);
-            timer_flush(run->t_visc);
+            timer_flush(run->t_stage, h.steps - before);
+            timer_flush(run->t_visc, h.steps - before);
+            before = h.steps;
             if (!h.active) break;
             if (chunk < 64) chunk *= 2;
         }
