@@ -407,6 +407,70 @@ def quad_arm(args, world, rank, local):
     return out
 
 
+CYL_WORKLOAD = ("Mach 2 flow over a cylinder (diameter 1, sharp ghost-cell immersed boundary, slip wall) in an 8 x 12 box, {nx} x {ny}, "
+                "inflow rho 1.4, p 1, Mach 2, transmissive elsewhere, from the free stream, {steps} steps; plain: MUSCL (MC) + HLLC + "
+                "MUSCL-Hancock; mixed: WENO5-Z + HLLC + SSP-RK3 (FP32 stencil, FP64 state)")
+
+
+def cyl_arm(args, world, rank, local):
+    """The Mach 2 cylinder: plain FP64, mixed and mixed + sensor runs of `steps` steps from the free stream at nx x ny, each
+    timed with CUDA events; bow-shock stand-off and Cd of each; the reference (CPU) at a quarter of the resolution to the
+    plain run's final time, its stand-off and Cd."""
+    import torch
+
+    from fenice_b200 import Run
+    from fenice_b200 import diagnostics as D
+
+    nx, ny, steps = args.cyl_nx, args.cyl_nx * 3 // 2, args.cyl_steps
+    sensor = load_sensor(local)
+    out = {}
+    t_final = None
+    for name, form, prec, sens in (("plain_fp64", "plain", 0, None), ("mixed", "mixed", 1, None), ("mixed_learned", "mixed", 1, sensor)):
+        params = D.cylinder_params(nx, ny, form)
+        run = Run(params, U=D.free_stream(params), precision=prec, device=local)
+        if sens:
+            run.set_sensor(*sens)
+        run.run(1e30, max_steps=3)   # warm-up (graph capture, first refresh)
+        run.close()
+        run = Run(params, U=D.free_stream(params), precision=prec, device=local)
+        if sens:
+            run.set_sensor(*sens)
+        ext = torch.cuda.ExternalStream(run.stream(), device=torch.device("cuda", local))
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        with Clocks(local) as clk:
+            start.record(ext)
+            done = run.run(1e30, max_steps=steps)
+            end.record(ext)
+            run.synchronize()
+        ms = allmax(start.elapsed_time(end), world)
+        stages = 1 if form == "plain" else 3
+        loads = run.ibm_loads()
+        U = run.state()
+        out[name] = {"value": world * nx * ny * stages * done / (ms * 1e-3), "ms": ms, "steps": done, "t": run.t, "stages_per_step": stages,
+                     "standoff_over_diameter": D.bow_shock_standoff(U, params), "Cd": loads["Cd"], "Cl": loads["Cl"], "clocks": clk.summary()}
+        if sens:
+            lin, ev = run.sensor_counts()
+            out[name]["linear_share_of_tile_axes"] = lin / max(ev, 1)
+        if name == "plain_fp64":
+            t_final = run.t
+        run.close()
+    if args.cpu_baseline and rank == 0:
+        from oracle.oracle import Reference
+
+        q = D.cylinder_params(nx // 4, ny // 4, "plain")
+        ref = Reference(q, initial_state=(D.RHO_IN, q["u_in"], 0.0, D.P_IN))
+        t0 = time.perf_counter()
+        n = len(ref.steps(10 ** 7, t_final)[0])
+        wall = time.perf_counter() - t0
+        f = ref.ibm_loads()
+        qA = 0.5 * D.RHO_IN * q["u_in"] ** 2 * 1.0
+        out["reference_cpu_quarter_resolution"] = {"nx": nx // 4, "ny": ny // 4, "steps": n, "t": ref.t, "wall_s": wall,
+                                                    "value": (nx // 4) * (ny // 4) * n / wall, "standoff_over_diameter": D.bow_shock_standoff(ref.state(), q),
+                                                    "Cd": f[0] / qA, "threads": len(os.sched_getaffinity(0))}
+    return out
+
+
 def gpu_arm(args, world, rank, local):
     import torch
 
@@ -489,10 +553,12 @@ def main():
     ap.add_argument("--size", type=int, default=256, help="cells per axis (256: the benchmark workload)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-baseline", type=int, default=1, help="time the reference on the host cores (rank 0, N = 1)")
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "quadrants"],
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "quadrants", "cylinder"],
                     help="tgv: the 3-D Taylor-Green vortex (default); batch: 512 shock tubes in one persistent launch per stage; "
                          "quadrants: a seeded four-quadrant Riemann problem (--size cells per axis, default 2048 for it)")
     ap.add_argument("--seed", type=int, default=2048, help="seed of the quadrants workload")
+    ap.add_argument("--cyl-nx", type=int, default=1600, help="cylinder workload: cells along x (y: 3/2 of it)")
+    ap.add_argument("--cyl-steps", type=int, default=20000, help="cylinder workload: steps of each GPU form")
     ap.add_argument("--batch", type=int, default=1, help="with --workload tgv at N = 1: add the batched workload's figures")
     args = ap.parse_args()
     world, rank, local = (1, 0, 0) if args.impl == "reference" and int(os.environ.get("WORLD_SIZE", "1")) == 1 else dist_setup()
@@ -521,6 +587,26 @@ def main():
                 "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
                 "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
+        return
+    if args.workload == "cylinder":
+        cy = cyl_arm(args, world, rank, local)
+        m = cy["mixed_learned"]
+        line = {"metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world, "steps": m["steps"], "warmup": 3,
+                "ms_per_step": m["ms"] / m["steps"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 stencil / f64 state with bf16 sensor (value); plain form f64", "data": "synthetic (uniform inflow)",
+                "config": {"workload": CYL_WORKLOAD.format(nx=args.cyl_nx, ny=args.cyl_nx * 3 // 2, steps=args.cyl_steps) + "; value: mixed + learned sensor",
+                           "cells": args.cyl_nx * (args.cyl_nx * 3 // 2)},
+                "clocks": m["clocks"], "forms": cy, "e2e": None, "gpu_launches": None}
+        if "reference_cpu_quarter_resolution" in cy:
+            r = cy["reference_cpu_quarter_resolution"]
+            line["cpu_baseline"] = {"value": r["value"], "unit": "cell-updates/s", "cores": r["threads"], "kind": "reference",
+                                    "sample": f"the plain form at {r['nx']} x {r['ny']} to the GPU plain run's final time ({r['steps']} steps)"}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
         return
     if args.workload == "quadrants":
         if args.size == 256:

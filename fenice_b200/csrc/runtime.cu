@@ -172,6 +172,25 @@ __global__ void k_face_flux(Eos<double> e, double shock_blend, const double* UL,
     }
 }
 
+// Simulation::ibm_loads (cpp/src/SimulationRun.cpp:134-155): {Fx, Fy, Mz} = the momentum residual of the solid cells times
+// the cell volume, summed in cell order (one thread: the reference's order, so the bits), Mz about (cx, cy).
+__global__ void k_ibm_loads(const double* R, long long plane, const int* cells, int n, double vol, int nx, int ny, double dx, double dy, double cx,
+                            double cy, double* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double fx = 0.0, fy = 0.0, mz = 0.0;
+    for (int k = 0; k < n; ++k) {
+        const int c = cells[k];
+        const double ex = R[plane + c] * vol, ey = R[2 * plane + c] * vol;
+        fx += ex;
+        fy += ey;
+        const double xc = ((c % nx) + 0.5) * dx + 0.0, yc = (((c / nx) % ny) + 0.5) * dy + 0.0;
+        mz += (xc - cx) * ey - (yc - cy) * ex;
+    }
+    out[0] = fx;
+    out[1] = fy;
+    out[2] = mz;
+}
+
 // ------------------------------------------------------------------------------------------------ kernel dispatch
 template <int DIM> struct Tile;
 template <> struct Tile<3> { static constexpr int X = 8, Y = 8, Z = 8, NT = 192; };
@@ -263,6 +282,9 @@ struct fvg_run {
     int ng = 0, nd = 0;
     unsigned char* d_mask = nullptr;
     int *d_slot = nullptr, *d_ghost = nullptr, *d_img_cell = nullptr, *d_deep = nullptr;
+    int* d_solid = nullptr;   // the solid cells in cell order (the loads' sum)
+    int nsolid = 0;
+    double* d_loads = nullptr;
     double *d_forced = nullptr, *d_img_w = nullptr, *d_ratio = nullptr, *d_gn = nullptr;
     // the learned sensor (fvg_set_sensor): its weights (a copy), the logit threshold, the refresh period and dilation,
     // the two flag buffers (the result in sens_result), the counters
@@ -717,6 +739,15 @@ int fvg_create(const fvg_config* cfg, fvg_run** out) {
             run->err = "device allocation of the immersed body's tables failed";
             return bail(FVG_ERR_CUDA);
         }
+        std::vector<int> solid_cells;
+        for (long long c = 0; c < run->m.ncells; ++c)
+            if (t.mask[c]) solid_cells.push_back((int)c);
+        run->nsolid = (int)solid_cells.size();
+        if (cudaMalloc(&run->d_solid, sizeof(int) * (solid_cells.size() + 1)) != cudaSuccess || cudaMalloc(&run->d_loads, sizeof(double) * 3) != cudaSuccess ||
+            (run->nsolid > 0 && cudaMemcpy(run->d_solid, solid_cells.data(), sizeof(int) * run->nsolid, cudaMemcpyHostToDevice) != cudaSuccess)) {
+            run->err = "device allocation of the immersed body's tables failed";
+            return bail(FVG_ERR_CUDA);
+        }
         run->bc.solid = run->d_mask;
         run->bc.slot = run->d_slot;
         run->bc.forced = run->d_forced;
@@ -755,7 +786,7 @@ int fvg_destroy(fvg_run* run) {
         if (f) cudaFree(f);
     if (run->sens_tiles) cudaFree(run->sens_tiles);
     for (void* p : {(void*)run->d_mask, (void*)run->d_slot, (void*)run->d_forced, (void*)run->d_ghost, (void*)run->d_img_cell, (void*)run->d_img_w,
-                    (void*)run->d_ratio, (void*)run->d_gn, (void*)run->d_deep})
+                    (void*)run->d_ratio, (void*)run->d_gn, (void*)run->d_deep, (void*)run->d_solid, (void*)run->d_loads})
         if (p) cudaFree(p);
     if (run->stream) cudaStreamDestroy(run->stream);
     delete run;
@@ -1025,7 +1056,6 @@ int fvg_set_sensor(fvg_run* run, const void* weights, float threshold, int every
     }
     if (run->cfg.precision != FVG_PREC_MIXED || run->cfg.reconstruction != FVG_RECON_WENO5)
         return fail(run, FVG_ERR_CONFIG, "the sensor gates the mixed-precision WENO5-Z form");
-    if (run->ibm) return fail(run, FVG_ERR_CONFIG, "the sensor is not built for runs with an immersed body");
     if (every <= 0) every = 5;
     if (radius < 0) radius = (int)std::ceil(run->cfg.cfl * every) + 1;
     const size_t fbytes = (size_t)run->m.plane * run->dim;
@@ -1059,6 +1089,37 @@ int fvg_get_sensor_counts(fvg_run* run, long long* linear, long long* evaluated,
     }
     if (linear) *linear = (long long)h[0];
     if (evaluated) *evaluated = (long long)h[1];
+    return FVG_OK;
+}
+
+int fvg_ibm_loads(fvg_run* run, double* loads) {
+    if (!run || !loads) return FVG_ERR_ARGUMENT;
+    if (!run->ibm) return fail(run, FVG_ERR_CONFIG, "the run has no immersed body");
+    CK(cudaSetDevice(run->cfg.device));
+    // the residual of the current state (after a step the scheme's predictor is off: the plain residual, as the monitor's)
+    const int* always = &run->ctl->always;
+    double* out = run->cur ? run->U : run->Ut;
+    CK(refresh_gate(run, run->Ucur(), nullptr));
+    CK(residual_stage(run, run->Ucur(), nullptr, out, kStoreR, 0, 0, 0, always));
+    const fvg_config& c = run->cfg;
+    const double vol = run->dim == 3 ? run->m.dx * run->m.dy * run->m.dz : run->m.dx * run->m.dy;
+    k_ibm_loads<<<1, 32, 0, run->stream>>>(out, run->m.plane, run->d_solid, run->nsolid, vol, run->m.nx, run->m.ny, run->m.dx, run->m.dy, c.ibm_cx,
+                                           c.ibm_cy, run->d_loads);
+    CK(cudaGetLastError());
+    double h[3];
+    CK(cudaMemcpyAsync(h, run->d_loads, sizeof(h), cudaMemcpyDeviceToHost, run->stream));
+    CK(cudaStreamSynchronize(run->stream));
+    // the monitor's coefficients (cpp/src/SimulationRun.cpp:94-103): on q A, A = the diameter (2-D, per unit depth), pi r^2
+    // (sphere) or diameter x Lz (3-D cylinder); Cm about (ibm_cx, ibm_cy), nose-up positive
+    const double L = 2.0 * c.ibm_radius;
+    const double A = run->dim == 2 ? L : (c.ibm_shape == 1 ? 3.14159265358979323846 * c.ibm_radius * c.ibm_radius : L * c.Lz);
+    const double qA = 0.5 * c.rho_in * c.u_in * c.u_in * A;
+    loads[0] = h[0];
+    loads[1] = h[1];
+    loads[2] = h[2];
+    loads[3] = qA > 0 ? h[0] / qA : 0.0;
+    loads[4] = qA > 0 ? h[1] / qA : 0.0;
+    loads[5] = qA > 0 ? -h[2] / (qA * L) : 0.0;
     return FVG_OK;
 }
 

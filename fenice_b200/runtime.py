@@ -34,7 +34,7 @@ EXPORTS = ["fvg_abi_version", "fvg_create", "fvg_destroy", "fvg_last_error", "fv
            "fvg_batch_download", "fvg_batch_run", "fvg_batch_problem", "fvg_batch_autotune", "fvg_batch_set_schedule",
            "fvg_batch_get_schedule", "fvg_batch_stream", "fvg_batch_set_timing", "fvg_batch_get_timing",
            "fvg_sensor_sizes", "fvg_sensor_extract", "fvg_sensor_grad", "fvg_sensor_adam", "fvg_sensor_pack", "fvg_sensor_infer",
-           "fvg_set_sensor", "fvg_get_sensor_counts"]
+           "fvg_set_sensor", "fvg_get_sensor_counts", "fvg_ibm_loads"]
 
 _lib = None
 
@@ -97,6 +97,7 @@ def load_library(path=LIB_PATH):
     lib.fvg_sensor_infer.argtypes = [c_p, c_p, ctypes.c_longlong, c_p, c_p]
     lib.fvg_set_sensor.argtypes = [c_p, c_p, ctypes.c_float, ctypes.c_int, ctypes.c_int]
     lib.fvg_get_sensor_counts.argtypes = [c_p, ll, ll, ctypes.c_int]
+    lib.fvg_ibm_loads.argtypes = [c_p, dp]
     _lib = lib
     return lib
 
@@ -220,6 +221,13 @@ class Run:
         a, b, c, d = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_double(), ctypes.c_longlong()
         self._check(self.lib.fvg_get_timing(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d)), "get_timing")
         return {"stage_ms": a.value, "stage_launches": b.value, "viscous_ms": c.value, "viscous_launches": d.value}
+
+    def ibm_loads(self):
+        """{Fx, Fy, Mz, Cd, Cl, Cm} of the immersed body from a residual of the current state (Simulation::ibm_loads and
+        the monitor's coefficients)."""
+        v = (ctypes.c_double * 6)()
+        self._check(self.lib.fvg_ibm_loads(self.h, v), "ibm_loads")
+        return dict(zip(["Fx", "Fy", "Mz", "Cd", "Cl", "Cm"], list(v)))
 
     def set_sensor(self, sensor, threshold=0.0, every=0, radius=-1):
         """Gate the WENO5-Z reconstructions (mixed precision) with a trained ``fenice_b200.sensor.Sensor`` (None: off),

@@ -122,6 +122,12 @@ int fvg_synchronize(fvg_run* run);
 int fvg_set_timing(fvg_run* run, int on);
 int fvg_get_timing(const fvg_run* run, double* stage_ms, long long* stage_launches, double* viscous_ms, long long* viscous_launches);
 
+/* The immersed body's loads from a residual of the current state (Simulation::ibm_loads, cpp/src/SimulationRun.cpp:134-155,
+ * and the monitor's coefficients, :94-103): loads[6] = {Fx, Fy, Mz, Cd, Cl, Cm}; F the momentum residual of the solid
+ * cells times the cell volume (summed in cell order: the reference's bits), Mz about (ibm_cx, ibm_cy), the coefficients
+ * on 1/2 rho_in u_in^2 A (A = the diameter in 2-D, pi r^2 for a sphere, diameter x Lz for a 3-D cylinder). */
+int fvg_ibm_loads(fvg_run* run, double* loads);
+
 /* Face fluxes of n face pairs (UL, UR: n x 5 doubles, axis: n ints) on the device with the run's EOS and Riemann
  * solver (RiemannSolver::face_flux, cpp/src/Schemes.cpp:202-229): F (n x 5) and the wave speeds (n). */
 int fvg_face_flux_batch(fvg_run* run, const double* UL, const double* UR, const int* axis, size_t n, double* F, double* smax);

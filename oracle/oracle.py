@@ -227,6 +227,7 @@ class Reference:
                                          P(ctypes.c_double)]
             lib.ref_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, P(ctypes.c_double), P(ctypes.c_double)]
             lib.ref_solid_mask.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+            lib.ref_ibm_loads.argtypes = [ctypes.c_void_p, P(ctypes.c_double)]
             cls._lib = lib
         return cls._lib
 
@@ -299,3 +300,10 @@ class Reference:
         if n < 0:
             return None
         return np.frombuffer(m.raw, dtype=np.int8).copy()
+
+    def ibm_loads(self):
+        """{Fx, Fy, Mz} of the immersed body from a residual of the current state (Simulation::ibm_loads)."""
+        v = (ctypes.c_double * 3)()
+        if self.lib().ref_ibm_loads(self.h, v) != 0:
+            raise RuntimeError("reference ibm_loads failed: " + self.lib().ref_error().decode())
+        return list(v)

@@ -206,4 +206,25 @@ int ref_solid_mask(void* h, char* mask) {
     return n;
 }
 
+// The immersed body's loads {Fx, Fy, Mz} of the current state, as the monitor takes them (Simulation::ibm_loads on a
+// residual of U with the predictor off); returns -1 without a body or on an error.
+int ref_ibm_loads(void* h, double* loads) {
+    auto* r = static_cast<RefRun*>(h);
+    if (!r->sim.p.use_ibm || !r->sim.ibm) return -1;
+    try {
+        fv::Field R;
+        r->sim.scheme->stage_time = r->sim.t;
+        r->sim.scheme->predictor_half_dt = 0.0;
+        r->sim.residual(r->sim.U, R);
+        const std::array<double, 3> f = r->sim.ibm_loads(r->sim.mesh, *r->sim.ibm, r->sim.U, R);
+        loads[0] = f[0];
+        loads[1] = f[1];
+        loads[2] = f[2];
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
 }   // extern "C"

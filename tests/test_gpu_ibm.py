@@ -4,6 +4,7 @@ WENO5-Z / SSP-RK3 (the narrow stencil beside the body) and boundary_order 1, a 3
 no-slip walls), and a longer Mach 2 cylinder run against the reference run alongside (when oracle/_ref is built)."""
 import json
 import math
+import os
 
 import numpy as np
 import pytest
@@ -79,3 +80,31 @@ def test_mach2_cylinder_against_reference():
     ref.steps(150, 1e30)
     assert bits_equal(run.state(), ref.state()), describe(run.state(), ref.state())
     assert run.t == ref.t
+    # the monitor's loads (Simulation::ibm_loads of a residual of the state): the same sums in the same order
+    loads, ref_loads = run.ibm_loads(), ref.ibm_loads()
+    print(f"\nloads after 150 steps: {loads}")
+    assert [loads["Fx"], loads["Fy"], loads["Mz"]] == ref_loads
+
+
+def test_sensor_gate_with_the_immersed_body():
+    """The learned gate on a mixed WENO5-Z cylinder run: the narrow stencil beside the body keeps its WENO3-Z; a gate
+    that never passes a tile gives the plain mixed run's state."""
+    from fenice_b200 import diagnostics as D
+    from fenice_b200.sensor import Sensor
+
+    params = D.cylinder_params(160, 240, form="mixed")
+    U0 = D.free_stream(params)
+    plain = Run(params, U=U0, precision=1)
+    plain.run(1e30, max_steps=30)
+    s = Sensor.load(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "fenice_b200", "sensor_weights.npz"))
+    never = Run(params, U=U0, precision=1)
+    never.set_sensor(s, -1e30)
+    never.run(1e30, max_steps=30)
+    assert np.abs(never.state() - plain.state()).max() <= 1e-5 * np.abs(plain.state()).max()
+    gated = Run(params, U=U0, precision=1)
+    gated.set_sensor(s, float(s.meta["threshold"]))
+    gated.run(1e30, max_steps=30)
+    lin, ev = gated.sensor_counts()
+    l1 = np.abs(gated.state()[:, 0] - plain.state()[:, 0]).sum() / np.abs(plain.state()[:, 0]).sum()
+    print(f"\ncylinder, sensor gate: {lin}/{ev} tile-axes linear, L1(rho) vs plain mixed {l1:.2e}")
+    assert ev > 0 and l1 < 1e-2
