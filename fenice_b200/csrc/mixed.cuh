@@ -13,6 +13,8 @@
 // two are the same; the tests state the L1 / Linf distance of this form from the FP64 oracle per field and per case.
 #pragma once
 
+#include <type_traits>
+
 #include "grid.cuh"
 #include "stage.cuh"
 #include "viscous.cuh"
@@ -251,8 +253,9 @@ template <int TX, int TY, int TZ> struct MixedViscShape {
     static constexpr int cmax(int x, int y) { return x > y ? x : y; }
     static constexpr int NE = cmax(cmax((TX + 2) * TY * TZ, TX * (TY + 2) * TZ), TX * TY * (TZ + 2));
     static constexpr int NF = cmax(cmax((TX + 1) * TY * TZ, TX * (TY + 1) * TZ), TX * TY * (TZ + 1));
-    // red [32 doubles], floats: B [5][NB] conservative box, Wb [4][NB] (u, v, w, T), G [4][NE], F [4][NF], acc [5][NC]
-    static constexpr int SMEM_FLOATS = 64 + 9 * NB + 4 * NE + 4 * NF + 5 * NC;
+    // red [32 doubles], floats: B [6][NB] box (rho, rho u, rho v, rho w, T, 1 / rho), G [4][NE], F [4][NF], acc [4][NC]
+    // (the momentum and energy balances; the mass balance is 0): 4 CTAs of the 8x8x8 tile fit on an SM
+    static constexpr int SMEM_FLOATS = 64 + 6 * NB + 4 * NE + 4 * NF + 4 * NC;
     static constexpr size_t SMEM_BYTES = sizeof(float) * SMEM_FLOATS;
 };
 
@@ -264,11 +267,10 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
     constexpr int NC = S::NC, BX = S::BX, BY = S::BY, NB = S::NB;
     extern __shared__ double smem_d[];
     double* red = smem_d;
-    float* B = reinterpret_cast<float*>(smem_d + 32);   // [5][NB]
-    float* Wb = B + 5 * NB;                              // [4][NB]: u, v, w, T
-    float* G = Wb + 4 * NB;                              // [4][NE]
+    float* B = reinterpret_cast<float*>(smem_d + 32);   // [6][NB]: rho, rho u, rho v, rho w, T, 1 / rho
+    float* G = B + 6 * NB;                               // [4][NE]
     float* Fv = G + 4 * S::NE;                           // [4][NF]
-    float* acc = Fv + 4 * S::NF;                         // [5][NC]
+    float* acc = Fv + 4 * S::NF;                         // [4][NC]: rho u, rho v, rho E, rho w
     if (!*a.gate) return;
     const Mesh& m = a.m;
     const int tid = threadIdx.x, b = blockIdx.x;
@@ -276,10 +278,14 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
     const int n3[3] = {m.nx, m.ny, m.nz};
     const float h[3] = {(float)m.dx, (float)m.dy, (float)m.dz};
     const float mu = (float)a.mu, kc = (float)a.k_cond;
-    const int* mom = kViscMom;
-    const auto& GA = kViscGA;
-    const auto& GB = kViscGB;
+    // the (a, b) of the four velocity-gradient entries of each axis's faces, in the reference's CrossGhosts order
+    // (cpp/src/Physics.cpp:653-667); compile-time tables, constant indices in the unrolled sweeps
+    constexpr int GA[3][4] = {{0, 1, 2, 0}, {0, 1, 2, 1}, {0, 1, 2, 2}};
+    constexpr int GB[3][4] = {{1, 1, 2, 2}, {0, 0, 2, 2}, {0, 1, 0, 1}};
     auto bidx = [&](int i, int j, int k) { return ((k + 1) * BY + (j + 1)) * BX + (i + 1); };
+    // velocity component x (u, v, w) and temperature of box position p
+    auto vel = [&](int x, int p) { return B[(1 + x) * NB + p] * B[5 * NB + p]; };
+    auto tmp = [&](int p) { return B[4 * NB + p]; };
 
     for (int e = tid; e < NB; e += NT) {
         int g[3] = {o3[0] + e % BX - 1, o3[1] + (e / BX) % BY - 1, o3[2] + e / (BX * BY) - 1};
@@ -290,34 +296,34 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
         for (int x = 0; x < 3; ++x) g[x] = g[x] < -1 ? -1 : (g[x] > n3[x] ? n3[x] : g[x]);
         const St<double, 5> u = padded_cons(a, g[0], g[1], g[2]);
         const St<double, 5> w = c2p(a.eos, u);
-#pragma unroll
-        for (int q = 0; q < 5; ++q) B[q * NB + e] = (float)u[q];
-        Wb[0 * NB + e] = (float)w[1];
-        Wb[1 * NB + e] = (float)w[2];
-        Wb[2 * NB + e] = (float)w[4];
-        Wb[3 * NB + e] = (float)(w[3] / w[0]);
+        B[0 * NB + e] = (float)u[0];
+        B[1 * NB + e] = (float)u[1];
+        B[2 * NB + e] = (float)u[2];
+        B[3 * NB + e] = (float)u[4];
+        B[4 * NB + e] = (float)(w[3] / w[0]);
+        B[5 * NB + e] = 1.0f / vmax((float)u[0], Num<float>::eos_eps);
     }
     __syncthreads();
 
-#pragma unroll 1
-    for (int d = 0; d < 3; ++d) {
-        int E[3] = {TX, TY, TZ}, Fd[3] = {TX, TY, TZ};
-        E[d] += 2;
-        Fd[d] += 1;
+    // one sweep per axis, the axis a compile-time constant (every small index array stays in registers)
+    auto sweep = [&](auto axis_c) {
+        constexpr int d = decltype(axis_c)::value;
+        constexpr int E[3] = {TX + (d == 0 ? 2 : 0), TY + (d == 1 ? 2 : 0), TZ + (d == 2 ? 2 : 0)};
+        constexpr int Fd[3] = {TX + (d == 0), TY + (d == 1), TZ + (d == 2)};
         const int nE = E[0] * E[1] * E[2], nF = Fd[0] * Fd[1] * Fd[2];
         for (int e = tid; e < nE; e += NT) {
             int l[3] = {e % E[0], (e / E[0]) % E[1], e / (E[0] * E[1])};
             l[d] -= 1;
             const int p = bidx(l[0], l[1], l[2]);
-            const float inv_rho = 1.0f / vmax(B[p], Num<float>::eos_eps);
+            const float inv_rho = B[5 * NB + p];
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
                 const int ga = GA[d][s], gb = GB[d][s];
                 const int off = gb == 0 ? 1 : (gb == 1 ? BX : BX * BY);
                 const float inv2h = 0.5f / h[gb];
-                const float gq = (B[mom[ga] * NB + p + off] - B[mom[ga] * NB + p - off]) * inv2h;
+                const float gq = (B[(1 + ga) * NB + p + off] - B[(1 + ga) * NB + p - off]) * inv2h;
                 const float g0 = (B[p + off] - B[p - off]) * inv2h;
-                G[s * S::NE + e] = (gq - Wb[ga * NB + p] * g0) * inv_rho;
+                G[s * S::NE + e] = (gq - vel(ga, p) * g0) * inv_rho;
             }
         }
         __syncthreads();
@@ -350,8 +356,8 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
                         const int ga = GA[d][s], gb = GB[d][s];
                         const int pg = lo ? pL : pR, pc = lo ? pR : pL;
                         const int off = gb == 0 ? 1 : (gb == 1 ? BX : BX * BY);
-                        const float fp = 0.5f * (Wb[ga * NB + pg + off] + Wb[ga * NB + pc + off]);
-                        const float fm = 0.5f * (Wb[ga * NB + pg - off] + Wb[ga * NB + pc - off]);
+                        const float fp = 0.5f * (vel(ga, pg + off) + vel(ga, pc + off));
+                        const float fm = 0.5f * (vel(ga, pg - off) + vel(ga, pc - off));
                         Gc[s] = (fp - fm) * (0.5f / h[gb]);
                     } else {
                         Gc[s] = 0.5f * (G[s * S::NE + xL] + G[s * S::NE + xR]);
@@ -360,11 +366,11 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
                 float Gn[3], vf[3];
 #pragma unroll
                 for (int x = 0; x < 3; ++x) {
-                    const float vl = Wb[x * NB + pL], vr = Wb[x * NB + pR];
+                    const float vl = vel(x, pL), vr = vel(x, pR);
                     Gn[x] = (vr - vl) * inv_h;
                     vf[x] = 0.5f * (vl + vr);
                 }
-                const float dT = (Wb[3 * NB + pR] - Wb[3 * NB + pL]) * inv_h;
+                const float dT = (tmp(pR) - tmp(pL)) * inv_h;
                 float tau[3];
                 if (d == 0) {
                     tau[0] = mu * ((4.0f / 3.0f) * Gn[0] - (2.0f / 3.0f) * (Gc[1] + Gc[2]));
@@ -393,13 +399,16 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
             const int fl = (c3[2] * Fd[1] + c3[1]) * Fd[0] + c3[0];
             const int fr = fl + (d == 0 ? 1 : (d == 1 ? Fd[0] : Fd[0] * Fd[1]));
 #pragma unroll
-            for (int q = 0; q < 5; ++q) {
-                const float dif = q == 0 ? 0.0f : Fv[(q - 1) * S::NF + fr] - Fv[(q - 1) * S::NF + fl];
+            for (int q = 0; q < 4; ++q) {
+                const float dif = Fv[q * S::NF + fr] - Fv[q * S::NF + fl];
                 acc[q * NC + c] = d == 0 ? dif : acc[q * NC + c] + dif;
             }
         }
         __syncthreads();
-    }
+        };
+    sweep(std::integral_constant<int, 0>{});
+    sweep(std::integral_constant<int, 1>{});
+    sweep(std::integral_constant<int, 2>{});
     double smax = 0.0;
     const float gm1 = (float)(a.eos.gamma - 1.0);
     for (int c = tid; c < NC; c += NT) {
@@ -407,13 +416,14 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
         const int g3[3] = {o3[0] + c3[0], o3[1] + c3[1], o3[2] + c3[2]};
         if (g3[0] >= m.nx || g3[1] >= m.ny || g3[2] >= m.nz) continue;
         const long long cell = ((long long)g3[2] * m.ny + g3[1]) * m.nx + g3[0];
+        a.Rv[cell] = 0.0;   // no mass flux: (double)(0.0f) * inv_cell
 #pragma unroll
-        for (int q = 0; q < 5; ++q) a.Rv[q * m.plane + cell] = (double)acc[q * NC + c] * m.inv_cell;
+        for (int q = 1; q < 5; ++q) a.Rv[q * m.plane + cell] = (double)acc[(q - 1) * NC + c] * m.inv_cell;
         const int p = bidx(c3[0], c3[1], c3[2]);
         const float rho = vmax(B[p], Num<float>::eos_eps);
-        const float T = Wb[3 * NB + p];
+        const float T = tmp(p);
         const float nu_eff = vmax((4.0f / 3.0f) * (mu / rho), (kc * gm1) / rho) + 1e-12f;
-        const float vm = vmax(vmax(fabsf(Wb[p]), fabsf(Wb[NB + p])), fabsf(Wb[2 * NB + p]));
+        const float vm = vmax(vmax(fabsf(vel(0, p)), fabsf(vel(1, p))), fabsf(vel(2, p)));
         // sound speed from T = p / rho: c = sqrt(gamma (p + p_inf) / rho)
         const float cs = sqrtf((float)a.eos.gamma * (T + (float)a.eos.p_inf / rho));
         const double s = (double)(vm + cs + 2.0f * (float)a.L * (float)a.inv_h2 * nu_eff);

@@ -14,6 +14,8 @@
 // (ViscousBound.hpp: max |u_a| + c + 2 L sum(1/h^2) max(4/3 mu/rho, k (gamma-1)/rho) + 1e-12).
 #pragma once
 
+#include <type_traits>
+
 #include "grid.cuh"
 
 namespace fvg {
@@ -109,12 +111,6 @@ __device__ __forceinline__ St<double, 5> padded_cons(const ViscArgs& a, int i, i
     return cell_at(a, p[0], p[1], p[2]);
 }
 
-// the momentum slots of the velocity components, and the (a, b) of the four gradient entries the faces of axis d read, in
-// the reference's CrossGhosts order (cpp/src/Physics.cpp:653-667)
-__constant__ int kViscMom[3] = {1, 2, 4};
-__constant__ int kViscGA[3][4] = {{0, 1, 2, 0}, {0, 1, 2, 1}, {0, 1, 2, 2}};
-__constant__ int kViscGB[3][4] = {{1, 1, 2, 2}, {0, 0, 2, 2}, {0, 1, 0, 1}};
-
 // velocity component a (0, 1, 2) of a primitive state, without indexing the state by a run-time value
 __device__ __forceinline__ double velc(const St<double, 5>& w, int a) { return a == 0 ? w[1] : (a == 1 ? w[2] : w[4]); }
 
@@ -145,9 +141,12 @@ __global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
     const int o3[3] = {(b % a.tiles[0]) * TX, ((b / a.tiles[0]) % a.tiles[1]) * TY, (b / (a.tiles[0] * a.tiles[1])) * TZ};
     const int n3[3] = {m.nx, m.ny, m.nz};
     const double h[3] = {m.dx, m.dy, m.dz};
-    const int* mom = kViscMom;
-    const auto& GA = kViscGA;
-    const auto& GB = kViscGB;
+    // the momentum slots of the velocity components, and the (a, b) of the four gradient entries the faces of axis d read,
+    // in the reference's CrossGhosts order (cpp/src/Physics.cpp:653-667); compile-time tables, constant indices in the
+    // unrolled sweeps
+    constexpr int mom[3] = {1, 2, 4};
+    constexpr int GA[3][4] = {{0, 1, 2, 0}, {0, 1, 2, 1}, {0, 1, 2, 2}};
+    constexpr int GB[3][4] = {{1, 1, 2, 2}, {0, 0, 2, 2}, {0, 1, 0, 1}};
     // box position (tile-relative cell index -1 .. T per axis) -> shared-memory index
     auto bidx = [&](int i, int j, int k) { return ((k + 1) * BY + (j + 1)) * BX + (i + 1); };
     auto cons = [&](int p) {
@@ -174,11 +173,11 @@ __global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
     }
     __syncthreads();
 
-#pragma unroll 1
-    for (int d = 0; d < 3; ++d) {
-        int E[3] = {TX, TY, TZ}, Fd[3] = {TX, TY, TZ};
-        E[d] += 2;
-        Fd[d] += 1;
+// one sweep per axis, the axis a compile-time constant (every small index array stays in registers)
+    auto sweep = [&](auto axis_c) {
+        constexpr int d = decltype(axis_c)::value;
+        constexpr int E[3] = {TX + (d == 0 ? 2 : 0), TY + (d == 1 ? 2 : 0), TZ + (d == 2 ? 2 : 0)};
+        constexpr int Fd[3] = {TX + (d == 0), TY + (d == 1), TZ + (d == 2)};
         const int nE = E[0] * E[1] * E[2], nF = Fd[0] * Fd[1] * Fd[2];
         // ---- 1. the four gradient entries of the cells of the tile extended along d (meaningless at a ghost position)
         for (int e = tid; e < nE; e += NT) {
@@ -288,7 +287,10 @@ __global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
             }
         }
         __syncthreads();
-    }
+    };
+    sweep(std::integral_constant<int, 0>{});
+    sweep(std::integral_constant<int, 1>{});
+    sweep(std::integral_constant<int, 2>{});
     // ---- residual and speed bound
     double smax = 0.0;
     for (int c = tid; c < NC; c += NT) {
