@@ -236,6 +236,16 @@ cudaError_t launch_viscous(const ViscArgs& a, int nblocks, cudaStream_t s) {
     viscous_kernel<8, 8, 8, 192><<<nblocks, 192, ViscShape<8, 8, 8>::SMEM_BYTES, s>>>(a);
     return cudaGetLastError();
 }
+// the 2-D sweep: 16 x 16 tiles, 256 threads (the mixed form uses it too: the FP32 viscous kernel is 3-D only)
+constexpr int kVisc2T = 16;
+cudaError_t prepare_viscous2d() {
+    return cudaFuncSetAttribute(viscous2d_kernel<kVisc2T, kVisc2T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)Visc2Shape<kVisc2T, kVisc2T>::SMEM_BYTES);
+}
+cudaError_t launch_viscous2d(const ViscArgs& a, int nblocks, cudaStream_t s) {
+    viscous2d_kernel<kVisc2T, kVisc2T, 256><<<nblocks, 256, Visc2Shape<kVisc2T, kVisc2T>::SMEM_BYTES, s>>>(a);
+    return cudaGetLastError();
+}
 
 template <int RIEMANN> cudaError_t prepare_hancock_t() {
     return cudaFuncSetAttribute(hancock_kernel<RIEMANN, 16, 16, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HancockShape<16, 16>::SMEM_BYTES);
@@ -338,7 +348,6 @@ std::string validate(const fvg_config& c) {
         if (c.nz > 1) return "MUSCL-Hancock is built for 2-D meshes only";
         if (c.use_viscous) return "MUSCL-Hancock with viscous fluxes is not supported on the device";
     }
-    if (c.use_viscous && c.nz == 1) return "the 2-D viscous sweep is not supported on the device (3-D only)";
     if (!(c.cfl > 0)) return "cfl must be > 0";
     return "";
 }
@@ -394,7 +403,9 @@ ViscArgs visc_args(fvg_run* r, const double* Uin, double* bmv, const int* gate) 
     a.mu = r->cfg.mu;
     a.k_cond = r->cfg.mu * g / (r->cfg.pr * (g - 1.0));   // TransportLaw (Core.hpp:194-197)
     a.L = r->L;
-    a.inv_h2 = 1.0 / (r->m.dx * r->m.dx) + 1.0 / (r->m.dy * r->m.dy) + 1.0 / (r->m.dz * r->m.dz);
+    a.inv_h2 = r->dim == 3 ? 1.0 / (r->m.dx * r->m.dx) + 1.0 / (r->m.dy * r->m.dy) + 1.0 / (r->m.dz * r->m.dz)   // inv_h2_3d
+                           : 1.0 / (r->m.dx * r->m.dx) + 1.0 / (r->m.dy * r->m.dy);                               // inv_h2_2d
+    a.nvar = r->nvar;
     a.u_in = r->cfg.u_in;
     a.v_in = r->cfg.v_in;
     a.bface2 = r->cfg.boundary_order == 2;
@@ -490,8 +501,9 @@ cudaError_t residual_stage(fvg_run* r, const double* Uin, const double* U0, doub
     if (r->ibm && (e = ibm_fill(r, Uin, nullptr, 0, gate)) != cudaSuccess) return e;
     if (r->cfg.use_viscous) {
         timer_mark(r, r->t_visc);
-        e = r->cfg.precision == FVG_PREC_MIXED ? mixed_viscous_launch(visc_args(r, Uin, r->bmv[stage], gate), r->nbv, r->stream)
-                                               : launch_viscous(visc_args(r, Uin, r->bmv[stage], gate), r->nbv, r->stream);
+        e = r->dim == 2 ? launch_viscous2d(visc_args(r, Uin, r->bmv[stage], gate), r->nbv, r->stream)
+            : r->cfg.precision == FVG_PREC_MIXED ? mixed_viscous_launch(visc_args(r, Uin, r->bmv[stage], gate), r->nbv, r->stream)
+                                                 : launch_viscous(visc_args(r, Uin, r->bmv[stage], gate), r->nbv, r->stream);
         timer_mark(r, r->t_visc);
         if (e != cudaSuccess) return e;
     }
@@ -662,9 +674,10 @@ int fvg_create(const fvg_config* cfg, fvg_run** out) {
     run->tiles[1] = (c.ny + TY - 1) / TY;
     run->tiles[2] = (c.nz + TZ - 1) / TZ;
     run->nb = run->tiles[0] * run->tiles[1] * run->tiles[2];
-    run->ntiles_v[0] = (c.nx + 7) / 8;
-    run->ntiles_v[1] = (c.ny + 7) / 8;
-    run->ntiles_v[2] = (c.nz + 7) / 8;
+    const int vt = run->dim == 3 ? 8 : kVisc2T;   // viscous tiles: 8^3, or 16 x 16 in 2-D
+    run->ntiles_v[0] = (c.nx + vt - 1) / vt;
+    run->ntiles_v[1] = (c.ny + vt - 1) / vt;
+    run->ntiles_v[2] = run->dim == 3 ? (c.nz + 7) / 8 : 1;
     run->nbv = run->ntiles_v[0] * run->ntiles_v[1] * run->ntiles_v[2];
     run->ntiles_h[0] = (c.nx + 15) / 16;
     run->ntiles_h[1] = (c.ny + 15) / 16;
@@ -681,7 +694,7 @@ int fvg_create(const fvg_config* cfg, fvg_run** out) {
         }
     }
     // the seed residual of MUSCL-Hancock and every residual use the stage kernel; the viscous and predictor kernels as needed
-    if (run->stage.prepare() != cudaSuccess || (c.use_viscous && prepare_viscous() != cudaSuccess) ||
+    if (run->stage.prepare() != cudaSuccess || (c.use_viscous && (run->dim == 3 ? prepare_viscous() : prepare_viscous2d()) != cudaSuccess) ||
         (run->dim == 2 && c.reconstruction == FVG_RECON_MUSCL &&
          (c.riemann == FVG_RIEMANN_LOWMACH ? prepare_hancock_t<kLowMach>() : prepare_hancock_t<kHLLC>()) != cudaSuccess)) {
         run->err = "kernel set-up failed (shared-memory limit)";

@@ -28,6 +28,7 @@ struct ViscArgs {
     double u_in, v_in;
     int bface2;        // boundary_order == 2
     int periodic[3];   // both sides of the axis periodic
+    int nvar;          // state planes: 4 on a 2-D mesh (rho w is +0 there), 5 in 3-D
     const double* U;
     double* Rv;
     double* blockmax;
@@ -58,7 +59,14 @@ __device__ __forceinline__ St<double, 5> viscous_ghost_3d(const ViscArgs& a, int
 }
 
 __device__ __forceinline__ St<double, 5> cell_at(const ViscArgs& a, int i, int j, int k) {
-    return read_state<5>(a.bc, a.U, a.m.plane, ((long long)k * a.m.ny + j) * a.m.nx + i);
+    const long long c = ((long long)k * a.m.ny + j) * a.m.nx + i;
+    if (a.nvar == 5) return read_state<5>(a.bc, a.U, a.m.plane, c);
+    const St<double, 4> u4 = read_state<4>(a.bc, a.U, a.m.plane, c);
+    St<double, 5> u;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) u[s] = u4[s];
+    u[4] = 0.0;
+    return u;
 }
 
 // The padded entry beyond one side along axis d (padded_3d, Boundaries.cpp:621-700): the opposite layer of a periodic
@@ -305,6 +313,183 @@ __global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
         const double nu_eff = vmax((4.0 / 3.0) * (a.mu / rho), (a.k_cond * (a.eos.gamma - 1.0)) / rho) + 1e-12;
         const double vm = vmax(vmax(fabs(w[1]), fabs(w[2])), fabs(w[4]));
         const double s = vm + sound_speed(a.eos, w[3], rho) + 2.0 * a.L * a.inv_h2 * nu_eff;
+        if (s > smax) smax = s;
+    }
+    const double bm = block_max<NT>(smax, red);
+    if (tid == 0) a.blockmax[b] = bm;
+}
+
+}   // namespace fvg
+
+namespace fvg {
+
+// ---------------------------------------------------------------------------------------------- 2-D viscous sweep
+// NavierStokes::viscous_residual_rows (cpp/src/Physics.cpp:229-479) on a TX x TY tile: the padded frame of the 2-D mesh
+// (get_padded_frame + fix_frame_corners, cpp/src/Boundaries.cpp:402-630: the zero-gradient copy with the wall momentum
+// rules, the same entries padded_cons gives a one-cell-high 3-D mesh; a periodic side wrapped) staged for the tile and
+// two cells around it; then, for the tile and one cell around it, the cell quantities of a row (u, v, T and the four
+// velocity derivatives (d(rho u_a)/dx_b - u_a d(rho)/dx_b) / rho from central differences over 2h); then the x and y face
+// fluxes with the reference's choice of cells at the mesh sides (a side that is not periodic averages the derivative of
+// the boundary cell with itself, or, with boundary_order 2, takes the tangential derivative of the face-averaged frame);
+// then the balance ((0 + (Fr - Fl)) + (Ft - Fb)) / area and the speed bound max(|u|, |v|) + c + 2 L (1/dx^2 + 1/dy^2) nu_eff.
+template <int TX, int TY> struct Visc2Shape {
+    static constexpr int BX = TX + 4, BY = TY + 4, NB = BX * BY;   // conservative box: the tile +- 2
+    static constexpr int QX = TX + 2, QY = TY + 2, NQ = QX * QY;   // cell quantities: the tile +- 1
+    static constexpr int NFX = (TX + 1) * TY, NFY = TX * (TY + 1);
+    // doubles: B [4][NB], Q [7][NQ] (u, v, T, du/dx, du/dy, dv/dx, dv/dy), FX [3][NFX], FY [3][NFY], 32 for the reduction
+    static constexpr int SMEM_DOUBLES = 4 * NB + 7 * NQ + 3 * NFX + 3 * NFY + 32;
+    static constexpr size_t SMEM_BYTES = sizeof(double) * SMEM_DOUBLES;
+};
+
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) viscous2d_kernel(const ViscArgs a) {
+    using S = Visc2Shape<TX, TY>;
+    constexpr int BX = S::BX, NB = S::NB, QX = S::QX, NQ = S::NQ;
+    constexpr double MU_DIAG = 4.0 / 3.0, MU_OFF = 2.0 / 3.0;
+    extern __shared__ double smem[];
+    double* B = smem;                 // [4][NB]
+    double* Q = B + 4 * NB;           // [7][NQ]
+    double* FX = Q + 7 * NQ;          // [3][NFX]
+    double* FY = FX + 3 * S::NFX;     // [3][NFY]
+    double* red = FY + 3 * S::NFY;
+    if (!*a.gate) return;
+    const Mesh& m = a.m;
+    const int tid = threadIdx.x, b = blockIdx.x;
+    const int ox = (b % a.tiles[0]) * TX, oy = (b / a.tiles[0]) * TY;
+    const int nx = m.nx, ny = m.ny;
+    const double dx = m.dx, dy = m.dy, mu = a.mu, kc = a.k_cond;
+    const bool px = a.periodic[0] != 0, py = a.periodic[1] != 0;
+    // box position (tile-relative -2 .. T+1) and quantity position (-1 .. T)
+    auto bidx = [&](int i, int j) { return (j + 2) * BX + (i + 2); };
+    auto qidx = [&](int i, int j) { return (j + 1) * QX + (i + 1); };
+    auto q = [&](int s, int i, int j) { return Q[s * NQ + qidx(i, j)]; };
+
+    // ---- the padded state of the tile +- 2 (the frame beyond the mesh, a periodic side wrapped first)
+    for (int e = tid; e < NB; e += NT) {
+        int g[2] = {ox + e % BX - 2, oy + e / BX - 2};
+        if (px && (g[0] < 0 || g[0] >= nx)) g[0] = ((g[0] % nx) + nx) % nx;
+        if (py && (g[1] < 0 || g[1] >= ny)) g[1] = ((g[1] % ny) + ny) % ny;
+        g[0] = g[0] < -1 ? -1 : (g[0] > nx ? nx : g[0]);
+        g[1] = g[1] < -1 ? -1 : (g[1] > ny ? ny : g[1]);
+        const St<double, 5> u = padded_cons(a, g[0], g[1], 0);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) B[s * NB + e] = u[s];
+    }
+    __syncthreads();
+    // ---- cell quantities of the tile +- 1 (the expressions of fill / scalar_cells)
+    for (int e = tid; e < NQ; e += NT) {
+        const int i = e % QX - 1, j = e / QX - 1;
+        const int p = bidx(i, j);
+        St<double, 5> c;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) c[s] = B[s * NB + p];
+        c[4] = 0.0;
+        const St<double, 5> w = c2p(a.eos, c);
+        const double rho = w[0], u = w[1], v = w[2];
+        const int pe = p + 1, pw = p - 1, pn = p + BX, ps = p - BX;
+        const double drx = (B[pe] - B[pw]) / (2.0 * dx), dry = (B[pn] - B[ps]) / (2.0 * dy);
+        const double gx1 = (B[NB + pe] - B[NB + pw]) / (2.0 * dx), gy1 = (B[NB + pn] - B[NB + ps]) / (2.0 * dy);
+        const double gx2 = (B[2 * NB + pe] - B[2 * NB + pw]) / (2.0 * dx), gy2 = (B[2 * NB + pn] - B[2 * NB + ps]) / (2.0 * dy);
+        Q[0 * NQ + e] = u;
+        Q[1 * NQ + e] = v;
+        Q[2 * NQ + e] = w[3] / rho;
+        Q[3 * NQ + e] = (gx1 - u * drx) / rho;
+        Q[4 * NQ + e] = (gy1 - u * dry) / rho;
+        Q[5 * NQ + e] = (gx2 - v * drx) / rho;
+        Q[6 * NQ + e] = (gy2 - v * dry) / rho;
+    }
+    __syncthreads();
+    // ---- x faces of the tile's rows (xflux): face il between quantity positions il-1 and il
+    for (int f = tid; f < S::NFX; f += NT) {
+        const int il = f % (TX + 1), jl = f / (TX + 1);
+        const int i = ox + il, j = oy + jl;
+        double out[3] = {0.0, 0.0, 0.0};
+        if (i <= nx && j < ny) {
+            const bool lo = i == 0, hi = i == nx;
+            const double uL = q(0, il - 1, jl), uR = q(0, il, jl);
+            const double vL = q(1, il - 1, jl), vR = q(1, il, jl);
+            const double TL = q(2, il - 1, jl), TR = q(2, il, jl);
+            const double u_f = 0.5 * (uL + uR), v_f = 0.5 * (vL + vR);
+            const double du_dx = (uR - uL) / dx, dv_dx = (vR - vL) / dx, dT_dx = (TR - TL) / dx;
+            // the cells whose tangential derivatives the face averages: the two neighbours; at a side that is not
+            // periodic, the boundary cell twice
+            const int xl = (lo && !px) ? il : il - 1, xr = (hi && !px) ? il - 1 : il;
+            double du_dy = 0.5 * (q(4, xl, jl) + q(4, xr, jl));
+            double dv_dy = 0.5 * (q(6, xl, jl) + q(6, xr, jl));
+            if (a.bface2 && (lo || hi) && !px) {
+                const int ig = lo ? il - 1 : il, ic = lo ? il : il - 1;   // the frame column and the boundary cell's column
+                const double fu_p = 0.5 * (q(0, ig, jl + 1) + q(0, ic, jl + 1)), fu_m = 0.5 * (q(0, ig, jl - 1) + q(0, ic, jl - 1));
+                const double fv_p = 0.5 * (q(1, ig, jl + 1) + q(1, ic, jl + 1)), fv_m = 0.5 * (q(1, ig, jl - 1) + q(1, ic, jl - 1));
+                du_dy = (fu_p - fu_m) / (2.0 * dy);
+                dv_dy = (fv_p - fv_m) / (2.0 * dy);
+            }
+            const double tau_xx = mu * (MU_DIAG * du_dx - MU_OFF * dv_dy);
+            const double tau_xy = mu * (du_dy + dv_dx);
+            const double q_x = -kc * dT_dx;
+            out[0] = tau_xx * dy;
+            out[1] = tau_xy * dy;
+            out[2] = (u_f * tau_xx + v_f * tau_xy - q_x) * dy;
+        }
+#pragma unroll
+        for (int s = 0; s < 3; ++s) FX[s * S::NFX + f] = out[s];
+    }
+    // ---- y faces of the tile's columns (yflux): face jl between quantity rows jl-1 and jl
+    for (int f = tid; f < S::NFY; f += NT) {
+        const int il = f % TX, jl = f / TX;
+        const int i = ox + il, j = oy + jl;
+        double out[3] = {0.0, 0.0, 0.0};
+        if (i < nx && j <= ny) {
+            const bool lo = j == 0, hi = j == ny;
+            const double uB = q(0, il, jl - 1), uT = q(0, il, jl);
+            const double vB = q(1, il, jl - 1), vT = q(1, il, jl);
+            const double TB = q(2, il, jl - 1), TT = q(2, il, jl);
+            const double u_f = 0.5 * (uB + uT), v_f = 0.5 * (vB + vT);
+            const double dv_dy = (vT - vB) / dy, du_dy = (uT - uB) / dy, dT_dy = (TT - TB) / dy;
+            const int yb = (lo && !py) ? jl : jl - 1, yt = (hi && !py) ? jl - 1 : jl;
+            double du_dx = 0.5 * (q(3, il, yb) + q(3, il, yt));
+            double dv_dx = 0.5 * (q(5, il, yb) + q(5, il, yt));
+            if (a.bface2 && (lo || hi) && !py) {
+                const int jg = lo ? jl - 1 : jl, jc = lo ? jl : jl - 1;   // the frame row and the boundary cell's row
+                const double fu_p = 0.5 * (q(0, il + 1, jg) + q(0, il + 1, jc)), fu_m = 0.5 * (q(0, il - 1, jg) + q(0, il - 1, jc));
+                const double fv_p = 0.5 * (q(1, il + 1, jg) + q(1, il + 1, jc)), fv_m = 0.5 * (q(1, il - 1, jg) + q(1, il - 1, jc));
+                du_dx = (fu_p - fu_m) / (2.0 * dx);
+                dv_dx = (fv_p - fv_m) / (2.0 * dx);
+            }
+            const double tau_yy = mu * (MU_DIAG * dv_dy - MU_OFF * du_dx);
+            const double tau_yx = mu * (du_dy + dv_dx);
+            const double q_y = -kc * dT_dy;
+            out[0] = tau_yx * dx;
+            out[1] = tau_yy * dx;
+            out[2] = (u_f * tau_yx + v_f * tau_yy - q_y) * dx;
+        }
+#pragma unroll
+        for (int s = 0; s < 3; ++s) FY[s * S::NFY + f] = out[s];
+    }
+    __syncthreads();
+    // ---- balance, residual and speed bound
+    const double inv_area = m.inv_cell;
+    const double zero_slot = ((0.0 + (0.0 - 0.0)) + (0.0 - 0.0)) * inv_area;
+    double smax = 0.0;
+    for (int c = tid; c < TX * TY; c += NT) {
+        const int il = c % TX, jl = c / TX;
+        const int i = ox + il, j = oy + jl;
+        if (i >= nx || j >= ny) continue;
+        const long long cell = (long long)j * nx + i;
+        const int fl = jl * (TX + 1) + il, fb = jl * TX + il;
+        a.Rv[cell] = zero_slot;
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+            const double bal = ((0.0 + (FX[s * S::NFX + fl + 1] - FX[s * S::NFX + fl])) + (FY[s * S::NFY + fb + TX] - FY[s * S::NFY + fb])) * inv_area;
+            a.Rv[(s + 1) * m.plane + cell] = bal;
+        }
+        St<double, 5> cc;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) cc[s] = B[s * NB + bidx(il, jl)];
+        cc[4] = 0.0;
+        const St<double, 5> w = c2p(a.eos, cc);
+        const double rho = w[0];
+        const double nu_eff = vmax((4.0 / 3.0) * (a.mu / rho), (a.k_cond * (a.eos.gamma - 1.0)) / rho) + 1e-12;
+        const double s = vmax(fabs(w[1]), fabs(w[2])) + sound_speed(a.eos, w[3], rho) + 2.0 * a.L * a.inv_h2 * nu_eff;
         if (s > smax) smax = s;
     }
     const double bm = block_max<NT>(smax, red);

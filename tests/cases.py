@@ -138,3 +138,24 @@ def ibm_field(params, W0, seed):
     if nz > 1:
         W[:, 4] = U[:, 4] / U[:, 0] - 0.1
     return prim_to_cons(W)
+
+
+# 2-D viscous cases (NavierStokes::viscous_residual_rows): (name, params, seed, steps); a residual of the seeded field,
+# then `steps` steps, written by tests/golden/make_golden.py into visc2d.npz
+V2 = dict(use_viscous=True, mu=0.02, pr=0.72)
+VISC2D_CASES = [
+    ("v2_periodic_weno5_rk3", dict(nx=48, ny=40, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", **V2,
+                                   **bcs("periodic", "periodic", "periodic", "periodic")), 61, 4),
+    ("v2_noslip_muscl_rk2", dict(nx=40, ny=36, reconstruction="muscl", muscl_limiter="Van Leer", time_scheme="SSP Runge-Kutta 2", **V2,
+                                 **bcs("no_slip", "no_slip", "no_slip", "no_slip")), 62, 4),
+    ("v2_lid_weno3_rk3", dict(nx=36, ny=36, reconstruction="weno3", time_scheme="SSP Runge-Kutta 3", u_in=1.0, **V2,
+                              **bcs("no_slip", "no_slip", "no_slip", "moving_wall")), 63, 4),
+    ("v2_lid_order1", dict(nx=36, ny=34, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", u_in=0.7, v_in=0.2, boundary_order=1, **V2,
+                           **bcs("moving_wall", "wall", "no_slip", "moving_wall")), 64, 3),
+    ("v2_channel_inlet", dict(nx=50, ny=30, reconstruction="muscl", muscl_limiter="MC", time_scheme="SSP Runge-Kutta 3", u_in=0.5, p_out=1.0,
+                              **V2, **bcs("vel_inlet", "outlet", "wall", "no_slip")), 65, 4),
+    ("v2_xperiodic_walls", dict(nx=44, ny=32, reconstruction="weno5", time_scheme="Explicit Euler", cfl=0.3, **V2,
+                                **bcs("periodic", "periodic", "no_slip", "wall")), 66, 3),
+    ("v2_yperiodic_first_order", dict(nx=30, ny=40, reconstruction="none", time_scheme="Explicit Euler", **V2,
+                                      **bcs("transmissive", "no_slip", "periodic", "periodic")), 67, 3),
+]

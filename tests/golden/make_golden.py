@@ -7,8 +7,11 @@ the seeded inputs of tests/cases.py and stores, per case, the parameters, the in
   residuals.npz  one residual R(U) and its wave speed (Simulation::residual, with the MUSCL-Hancock predictor where the
                  case has a half step)
   steps.npz      the state after n steps of the serial time loop, with each step's dt and wave speed
+  ibm.npz        immersed-body cases: the forced field, a residual, then a few steps
+  visc2d.npz     2-D viscous cases (NavierStokes::viscous_residual_rows): a residual, then a few steps
   riemann.json   the reference's bench_riemann fingerprints over one pass of its 65536 state pairs
                  (oracle/_ref/bench_riemann 65536)
+Sections can be named on the command line (residuals steps ibm visc2d riemann); default: all.
 The fixtures are test data: nothing of the product reads them.
 """
 import json
@@ -27,7 +30,31 @@ from oracle.oracle import Reference  # noqa: E402
 import cases  # noqa: E402
 
 
-def main():
+def visc2d():
+    out = {}
+    for name, params, seed, n in cases.VISC2D_CASES:
+        U = cases.case_field(params, seed)
+        ref = Reference(params, initial_state=(1, 0, 0, 1, 0))
+        R, s = ref.residual(U)
+        out[f"{name}/params"] = np.array(json.dumps(params))
+        out[f"{name}/U0"] = U
+        out[f"{name}/R"] = R
+        out[f"{name}/smax"] = np.array(s)
+        ref.set_state(U)
+        dts, sms = ref.steps(n, 1e30)
+        out[f"{name}/U"] = ref.state()
+        out[f"{name}/dts"] = dts
+        out[f"{name}/smaxs"] = sms
+        out[f"{name}/t"] = np.array(ref.t)
+        print(f"visc2d {name}: smax {s:.6g}, {len(dts)} steps")
+    np.savez_compressed(os.path.join(HERE, "visc2d.npz"), **out)
+
+
+def main(sections=("residuals", "steps", "ibm", "visc2d", "riemann")):
+    if "visc2d" in sections:
+        visc2d()
+    if not {"residuals", "steps", "ibm", "riemann"} & set(sections):
+        return
     res = {}
     for name, params, seed, half in cases.RESIDUAL_CASES:
         U = cases.case_field(params, seed)
@@ -90,4 +117,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]) or ("residuals", "steps", "ibm", "visc2d", "riemann"))

@@ -43,7 +43,7 @@ def create_code(params):
     (dict(bc_xmax="nonreflecting"), "non-reflecting"),
     (dict(bc_xmin="periodic", bc_xmax="wall"), "periodic"),
     (dict(reconstruction="weno5", time_scheme="MUSCL-Hancock"), "MUSCL-Hancock"),
-    (dict(use_viscous=True), "2-D viscous"),
+    (dict(use_viscous=True, reconstruction="muscl", time_scheme="MUSCL-Hancock"), "viscous"),
     (dict(boundary_order=3), "boundary_order"),
     (dict(cfl=0.0), "cfl"),
 ])
