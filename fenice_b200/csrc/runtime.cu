@@ -408,7 +408,7 @@ ViscArgs visc_args(fvg_run* r, const double* Uin, double* bmv, const int* gate) 
     a.nvar = r->nvar;
     a.u_in = r->cfg.u_in;
     a.v_in = r->cfg.v_in;
-    a.bface2 = r->cfg.boundary_order == 2;
+    a.bface2 = r->cfg.boundary_order == 2 && r->cfg.reconstruction != FVG_RECON_NONE;   // Params.cpp:470: first order keeps order 1
     for (int d = 0; d < 3; ++d) a.periodic[d] = r->cfg.bc[2 * d] == FVG_BC_PERIODIC && r->cfg.bc[2 * d + 1] == FVG_BC_PERIODIC;
     a.U = Uin;
     a.Rv = r->Rv;

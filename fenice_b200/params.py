@@ -6,7 +6,7 @@ take the reference's defaults. Names are parsed as the reference parses them (ca
 parse_riemann / parse_limiter / parse_reconstruction, cpp/src/Schemes.cpp:77-102; parse_bc,
 cpp/src/Boundaries.cpp:15-27; parse_time_scheme, cpp/src/TimeScheme.cpp:73-80) and an unknown name raises ValueError,
 as the reference raises std::invalid_argument. ``time_scheme = "auto"`` resolves as in SimParams::from
-(cpp/src/Params.cpp:360-363).
+(cpp/src/Params.cpp:360-363), and boundary_order 2 falls back to 1 without a reconstruction (Params.cpp:470).
 """
 import ctypes
 import tomllib
@@ -76,6 +76,9 @@ def resolve(params):
     if str(p["time_scheme"]).strip().lower() == "auto":
         rec = str(p["reconstruction"]).strip().lower()
         p["time_scheme"] = "Explicit Euler" if rec != "muscl" else ("SSP Runge-Kutta 2" if _flag(p["use_viscous"]) else "MUSCL-Hancock")
+    # a first-order run keeps first-order boundaries (Params.cpp:470)
+    if int(p["boundary_order"]) == 2 and str(p["reconstruction"]).strip().lower() == "none":
+        p["boundary_order"] = 1
     return p
 
 
