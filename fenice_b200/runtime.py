@@ -147,8 +147,12 @@ class Run:
             raise ValueError(f"state must be ({self.ncells}, 5), got {U.shape}")
         self._check(self.lib.fvg_upload_state(self.h, _dp(U), self.ncells), "upload")
 
-    def state(self):
-        U = np.empty((self.ncells, 5))
+    def state(self, out=None):
+        """The state (a new array, or `out`: a C-contiguous float64 (ncells, 5) array, e.g. a view of pinned memory, which
+        the device then writes directly)."""
+        U = np.empty((self.ncells, 5)) if out is None else out
+        if U.shape != (self.ncells, 5) or U.dtype != np.float64 or not U.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of shape (ncells, 5)")
         self._check(self.lib.fvg_download_state(self.h, _dp(U), self.ncells), "download")
         return U
 
@@ -325,8 +329,10 @@ class Batch:
             raise ValueError(f"state must be ({self.ncells}, 5), got {U.shape}")
         self._check(self.lib.fvg_batch_upload(self.h, _dp(U), self.ncells), "upload")
 
-    def state(self):
-        U = np.empty((self.ncells, 5))
+    def state(self, out=None):
+        U = np.empty((self.ncells, 5)) if out is None else out
+        if U.shape != (self.ncells, 5) or U.dtype != np.float64 or not U.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of shape (ncells, 5)")
         self._check(self.lib.fvg_batch_download(self.h, _dp(U), self.ncells), "download")
         return U
 
