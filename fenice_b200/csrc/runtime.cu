@@ -247,11 +247,18 @@ cudaError_t launch_viscous2d(const ViscArgs& a, int nblocks, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-template <int RIEMANN> cudaError_t prepare_hancock_t() {
+// MUSCL-Hancock tiles: 16 x 16 in 2-D, 8 x 8 x 4 in 3-D (93 KB of shared memory: two CTAs per SM)
+template <int RIEMANN> cudaError_t prepare_hancock_t(int dim) {
+    if (dim == 3)
+        return cudaFuncSetAttribute(hancock3d_kernel<RIEMANN, 8, 8, 4, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)Hancock3Shape<8, 8, 4>::SMEM_BYTES);
     return cudaFuncSetAttribute(hancock_kernel<RIEMANN, 16, 16, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HancockShape<16, 16>::SMEM_BYTES);
 }
-template <int RIEMANN> cudaError_t launch_hancock_t(const HancockArgs& a, int nblocks, cudaStream_t s) {
-    hancock_kernel<RIEMANN, 16, 16, 256><<<nblocks, 256, HancockShape<16, 16>::SMEM_BYTES, s>>>(a);
+template <int RIEMANN> cudaError_t launch_hancock_t(int dim, const HancockArgs& a, int nblocks, cudaStream_t s) {
+    if (dim == 3)
+        hancock3d_kernel<RIEMANN, 8, 8, 4, 256><<<nblocks, 256, Hancock3Shape<8, 8, 4>::SMEM_BYTES, s>>>(a);
+    else
+        hancock_kernel<RIEMANN, 16, 16, 256><<<nblocks, 256, HancockShape<16, 16>::SMEM_BYTES, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -345,7 +352,6 @@ std::string validate(const fvg_config& c) {
             return "a periodic axis needs both of its sides periodic";
     if (c.time_scheme == FVG_TS_HANCOCK) {
         if (c.reconstruction != FVG_RECON_MUSCL) return "MUSCL-Hancock needs reconstruction = muscl";
-        if (c.nz > 1) return "MUSCL-Hancock is built for 2-D meshes only";
         if (c.use_viscous) return "MUSCL-Hancock with viscous fluxes is not supported on the device";
     }
     if (!(c.cfl > 0)) return "cfl must be > 0";
@@ -436,7 +442,8 @@ HancockArgs hancock_args(fvg_run* r, const double* Uin, double* out, int mode, d
 }
 
 cudaError_t launch_hancock(fvg_run* r, const HancockArgs& a) {
-    return r->cfg.riemann == FVG_RIEMANN_LOWMACH ? launch_hancock_t<kLowMach>(a, r->nbh, r->stream) : launch_hancock_t<kHLLC>(a, r->nbh, r->stream);
+    return r->cfg.riemann == FVG_RIEMANN_LOWMACH ? launch_hancock_t<kLowMach>(r->dim, a, r->nbh, r->stream)
+                                                 : launch_hancock_t<kHLLC>(r->dim, a, r->nbh, r->stream);
 }
 
 void timer_mark(fvg_run* r, fvg_run::EvTimer& t) {
@@ -679,10 +686,11 @@ int fvg_create(const fvg_config* cfg, fvg_run** out) {
     run->ntiles_v[1] = (c.ny + vt - 1) / vt;
     run->ntiles_v[2] = run->dim == 3 ? (c.nz + 7) / 8 : 1;
     run->nbv = run->ntiles_v[0] * run->ntiles_v[1] * run->ntiles_v[2];
-    run->ntiles_h[0] = (c.nx + 15) / 16;
-    run->ntiles_h[1] = (c.ny + 15) / 16;
-    run->ntiles_h[2] = 1;
-    run->nbh = run->ntiles_h[0] * run->ntiles_h[1];
+    const int hx = run->dim == 3 ? 8 : 16, hz = run->dim == 3 ? 4 : 1;   // MUSCL-Hancock tiles
+    run->ntiles_h[0] = (c.nx + hx - 1) / hx;
+    run->ntiles_h[1] = (c.ny + hx - 1) / hx;
+    run->ntiles_h[2] = (c.nz + hz - 1) / hz;
+    run->nbh = run->ntiles_h[0] * run->ntiles_h[1] * run->ntiles_h[2];
     run->stage = run->dim == 3 ? stage_launcher<3>(c.reconstruction, c.riemann) : stage_launcher<2>(c.reconstruction, c.riemann);
     if (c.precision == FVG_PREC_MIXED) {
         const MixedStage ms = mixed_stage(run->dim, c.reconstruction, c.riemann);
@@ -695,8 +703,8 @@ int fvg_create(const fvg_config* cfg, fvg_run** out) {
     }
     // the seed residual of MUSCL-Hancock and every residual use the stage kernel; the viscous and predictor kernels as needed
     if (run->stage.prepare() != cudaSuccess || (c.use_viscous && (run->dim == 3 ? prepare_viscous() : prepare_viscous2d()) != cudaSuccess) ||
-        (run->dim == 2 && c.reconstruction == FVG_RECON_MUSCL &&
-         (c.riemann == FVG_RIEMANN_LOWMACH ? prepare_hancock_t<kLowMach>() : prepare_hancock_t<kHLLC>()) != cudaSuccess)) {
+        (c.reconstruction == FVG_RECON_MUSCL &&
+         (c.riemann == FVG_RIEMANN_LOWMACH ? prepare_hancock_t<kLowMach>(run->dim) : prepare_hancock_t<kHLLC>(run->dim)) != cudaSuccess)) {
         run->err = "kernel set-up failed (shared-memory limit)";
         return bail(FVG_ERR_CUDA);
     }
@@ -852,8 +860,8 @@ int fvg_residual(fvg_run* run, double predictor_half_dt, double* R, size_t ncell
     const int* always = &c->always;
     double* out = run->cur ? run->U : run->Ut;   // a buffer that is not the state
     if (predictor_half_dt > 0.0) {
-        if (run->cfg.reconstruction != FVG_RECON_MUSCL || run->dim != 2 || run->cfg.use_viscous)
-            return fail(run, FVG_ERR_CONFIG, "the MUSCL-Hancock predictor needs a 2-D inviscid MUSCL run");
+        if (run->cfg.reconstruction != FVG_RECON_MUSCL || run->cfg.use_viscous)
+            return fail(run, FVG_ERR_CONFIG, "the MUSCL-Hancock predictor needs an inviscid MUSCL run");
         CK(cudaMemcpyAsync(&c->half_dt, &predictor_half_dt, sizeof(double), cudaMemcpyHostToDevice, run->stream));
         if (run->ibm) CK(ibm_fill(run, run->Ucur(), nullptr, 0, always));
         CK(launch_hancock(run, hancock_args(run, run->Ucur(), out, kStoreR, run->bm[0], always)));

@@ -159,3 +159,19 @@ VISC2D_CASES = [
     ("v2_yperiodic_first_order", dict(nx=30, ny=40, reconstruction="none", time_scheme="Explicit Euler", **V2,
                                       **bcs("transmissive", "no_slip", "periodic", "periodic")), 67, 3),
 ]
+
+# 3-D MUSCL-Hancock (MusclReconstruction::hancock_residual_3d): residuals with the predictor of half a step
+# (name, params, seed, predictor_half_dt), then steps of the MUSCL-Hancock scheme (name, params, seed, n_steps); sizes that
+# leave partial 8 x 8 x 4 tiles, every limiter, periodic, slab and first-order (no halo) sides, walls on every axis
+HANCOCK3D_RESIDUAL_CASES = [
+    ("h3_vl_periodic", dict(nx=12, ny=10, nz=9, reconstruction="muscl", muscl_limiter="Van Leer", **bcs("periodic", "periodic", "periodic", "periodic")), 31, 0.004),
+    ("h3_mc_walls", dict(nx=10, ny=11, nz=7, reconstruction="muscl", muscl_limiter="MC", **bcs("wall", "transmissive", "no_slip", "vel_inlet", z=("outlet", "moving_wall")), u_in=0.3, v_in=-0.2, p_out=0.95), 32, 0.003),
+    ("h3_minmod_order1", dict(nx=9, ny=12, nz=10, reconstruction="muscl", muscl_limiter="Minmod", boundary_order=1, **bcs("no_slip", "outlet", "periodic", "periodic", z=("wall", "transmissive"))), 33, 0.005),
+    ("h3_koren_lowmach", dict(nx=17, ny=9, nz=6, reconstruction="muscl", muscl_limiter="Koren", riemann_solver="lowmach", **bcs("periodic", "periodic", "wall", "wall", z=("transmissive", "transmissive"))), 34, 0.004),
+    ("h3_mc_order1_walls", dict(nx=11, ny=9, nz=13, reconstruction="muscl", muscl_limiter="MC", boundary_order=1, **bcs("moving_wall", "wall", "transmissive", "no_slip", z=("vel_inlet", "outlet")), u_in=0.4), 35, 0.003),
+]
+HANCOCK3D_STEP_CASES = [
+    ("h3s_vl_periodic", dict(nx=12, ny=11, nz=10, reconstruction="muscl", muscl_limiter="Van Leer", time_scheme="MUSCL-Hancock", **bcs("periodic", "periodic", "periodic", "periodic")), 36, 5),
+    ("h3s_mc_inlet", dict(nx=11, ny=10, nz=9, reconstruction="muscl", muscl_limiter="MC", time_scheme="MUSCL-Hancock", **bcs("vel_inlet", "transmissive", "wall", "no_slip", z=("periodic", "periodic")), u_in=0.8), 37, 5),
+    ("h3s_minmod_order1", dict(nx=10, ny=9, nz=11, reconstruction="muscl", muscl_limiter="Minmod", boundary_order=1, time_scheme="MUSCL-Hancock", **bcs("wall", "outlet", "transmissive", "moving_wall", z=("no_slip", "transmissive")), u_in=0.2), 38, 4),
+]

@@ -9,9 +9,10 @@ the seeded inputs of tests/cases.py and stores, per case, the parameters, the in
   steps.npz      the state after n steps of the serial time loop, with each step's dt and wave speed
   ibm.npz        immersed-body cases: the forced field, a residual, then a few steps
   visc2d.npz     2-D viscous cases (NavierStokes::viscous_residual_rows): a residual, then a few steps
+  hancock3d.npz  3-D MUSCL-Hancock (MusclReconstruction::hancock_residual_3d): residuals with the predictor, then steps
   riemann.json   the reference's bench_riemann fingerprints over one pass of its 65536 state pairs
                  (oracle/_ref/bench_riemann 65536)
-Sections can be named on the command line (residuals steps ibm visc2d riemann); default: all.
+Sections can be named on the command line (residuals steps ibm visc2d hancock3d riemann); default: all.
 The fixtures are test data: nothing of the product reads them.
 """
 import json
@@ -50,9 +51,38 @@ def visc2d():
     np.savez_compressed(os.path.join(HERE, "visc2d.npz"), **out)
 
 
-def main(sections=("residuals", "steps", "ibm", "visc2d", "riemann")):
+def hancock3d():
+    out = {}
+    for name, params, seed, half in cases.HANCOCK3D_RESIDUAL_CASES:
+        U = cases.case_field(params, seed)
+        ref = Reference(params, initial_state=(1, 0, 0, 1, 0))
+        R, s = ref.residual(U, predictor_half_dt=half)
+        out[f"{name}/params"] = np.array(json.dumps(params))
+        out[f"{name}/U"] = U
+        out[f"{name}/R"] = R
+        out[f"{name}/smax"] = np.array(s)
+        out[f"{name}/half_dt"] = np.array(half)
+        print(f"hancock3d residual {name}: smax {s:.6g}")
+    for name, params, seed, n in cases.HANCOCK3D_STEP_CASES:
+        U = cases.case_field(params, seed)
+        ref = Reference(params, initial_state=(1, 0, 0, 1, 0))
+        ref.set_state(U)
+        dts, sms = ref.steps(n, 1e30)
+        out[f"{name}/params"] = np.array(json.dumps(params))
+        out[f"{name}/U0"] = U
+        out[f"{name}/U"] = ref.state()
+        out[f"{name}/dts"] = dts
+        out[f"{name}/smaxs"] = sms
+        out[f"{name}/t"] = np.array(ref.t)
+        print(f"hancock3d steps {name}: {len(dts)} steps, t = {ref.t:.6g}")
+    np.savez_compressed(os.path.join(HERE, "hancock3d.npz"), **out)
+
+
+def main(sections=("residuals", "steps", "ibm", "visc2d", "hancock3d", "riemann")):
     if "visc2d" in sections:
         visc2d()
+    if "hancock3d" in sections:
+        hancock3d()
     if not {"residuals", "steps", "ibm", "riemann"} & set(sections):
         return
     res = {}
@@ -117,4 +147,4 @@ def main(sections=("residuals", "steps", "ibm", "visc2d", "riemann")):
 
 
 if __name__ == "__main__":
-    main(tuple(sys.argv[1:]) or ("residuals", "steps", "ibm", "visc2d", "riemann"))
+    main(tuple(sys.argv[1:]) or ("residuals", "steps", "ibm", "visc2d", "hancock3d", "riemann"))

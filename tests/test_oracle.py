@@ -43,6 +43,30 @@ def test_oracle_steps_match_golden(orc, golden, case):
     assert t == float(g[f"{name}/t"])
 
 
+@pytest.fixture(scope="module")
+def h3():
+    return np.load(os.path.join(HERE, "golden", "hancock3d.npz"))
+
+
+@pytest.mark.parametrize("case", cases.HANCOCK3D_RESIDUAL_CASES, ids=[c[0] for c in cases.HANCOCK3D_RESIDUAL_CASES])
+def test_oracle_hancock3d_residual_matches_golden(orc, h3, case):
+    name = case[0]
+    params = json.loads(str(h3[f"{name}/params"]))
+    R, s = orc.residual(params, h3[f"{name}/U"], float(h3[f"{name}/half_dt"]))
+    assert bits_equal(R, h3[f"{name}/R"]), np.abs(R - h3[f"{name}/R"]).max()
+    assert s == float(h3[f"{name}/smax"])
+
+
+@pytest.mark.parametrize("case", cases.HANCOCK3D_STEP_CASES, ids=[c[0] for c in cases.HANCOCK3D_STEP_CASES])
+def test_oracle_hancock3d_steps_match_golden(orc, h3, case):
+    name, _, _, n = case
+    params = json.loads(str(h3[f"{name}/params"]))
+    U, t, dts, sms, _ = orc.run(params, h3[f"{name}/U0"], n)
+    assert bits_equal(dts, h3[f"{name}/dts"])
+    assert bits_equal(U, h3[f"{name}/U"])
+    assert t == float(h3[f"{name}/t"])
+
+
 def test_oracle_riemann_fingerprints(orc):
     with open(os.path.join(HERE, "golden", "riemann.json")) as f:
         h = json.load(f)["hashes"]
