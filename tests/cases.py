@@ -119,6 +119,10 @@ IBM_CASES = [
                                 ibm_cy=0.5, ibm_cz=0.52, rho_in=1.0, p_out=1.0, u_in=0.5, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3",
                                 **bcs("vel_inlet", "transmissive", "transmissive", "transmissive", z=("transmissive", "transmissive"))),
      (1.0, 0.5, 0.0, 1.0), 44, 3),
+    ("sphere3d_hancock_mc", dict(nx=21, ny=18, nz=19, Lx=1.0, Ly=1.0, Lz=1.0, use_ibm=True, ibm_shape="Sphere", ibm_radius=0.24, ibm_cx=0.45,
+                                 ibm_cy=0.5, ibm_cz=0.48, rho_in=1.0, p_out=1.0, u_in=0.6, reconstruction="muscl", muscl_limiter="MC",
+                                 time_scheme="MUSCL-Hancock", **bcs("vel_inlet", "transmissive", "wall", "transmissive", z=("periodic", "periodic"))),
+     (1.0, 0.6, 0.0, 1.0), 46, 5),
     ("cyl3d_viscous_noslip", dict(nx=24, ny=20, nz=6, Lx=1.2, Ly=1.0, Lz=0.3, use_ibm=True, ibm_shape="Cylinder", ibm_radius=0.2, ibm_cx=0.4,
                                   ibm_cy=0.5, rho_in=1.0, p_out=1.0, u_in=0.4, use_viscous=True, mu=0.01, reconstruction="muscl",
                                   muscl_limiter="Van Leer", time_scheme="SSP Runge-Kutta 2",

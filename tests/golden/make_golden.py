@@ -83,8 +83,17 @@ def main(sections=("residuals", "steps", "ibm", "visc2d", "hancock3d", "riemann"
         visc2d()
     if "hancock3d" in sections:
         hancock3d()
-    if not {"residuals", "steps", "ibm", "riemann"} & set(sections):
-        return
+    if "residuals" in sections:
+        residuals()
+    if "steps" in sections:
+        steps()
+    if "ibm" in sections:
+        ibm()
+    if "riemann" in sections:
+        riemann()
+
+
+def residuals():
     res = {}
     for name, params, seed, half in cases.RESIDUAL_CASES:
         U = cases.case_field(params, seed)
@@ -98,6 +107,8 @@ def main(sections=("residuals", "steps", "ibm", "visc2d", "hancock3d", "riemann"
         print(f"residual {name}: smax {s:.6g}")
     np.savez_compressed(os.path.join(HERE, "residuals.npz"), **res)
 
+
+def steps():
     st = {}
     for name, params, seed, n in cases.STEP_CASES:
         U = cases.case_field(params, seed)
@@ -113,6 +124,8 @@ def main(sections=("residuals", "steps", "ibm", "visc2d", "hancock3d", "riemann"
         print(f"steps {name}: {len(dts)} steps, t = {ref.t:.6g}")
     np.savez_compressed(os.path.join(HERE, "steps.npz"), **st)
 
+
+def ibm():
     ib = {}
     for name, params, W0, seed, n in cases.IBM_CASES:
         ref = Reference(params, initial_state=W0)
@@ -135,6 +148,8 @@ def main(sections=("residuals", "steps", "ibm", "visc2d", "hancock3d", "riemann"
         print(f"ibm {name}: {int(ib[f'{name}/mask'].sum())} solid cells, {len(dts)} steps")
     np.savez_compressed(os.path.join(HERE, "ibm.npz"), **ib)
 
+
+def riemann():
     out = subprocess.run([os.path.join(ROOT, "oracle", "_ref", "bench_riemann"), "65536"], capture_output=True, text=True, check=True).stdout
     hashes = {}
     for line in out.splitlines():
