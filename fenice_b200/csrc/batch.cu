@@ -258,7 +258,8 @@ std::string batch_config_error(const fvg_config* cfgs, int n) {
         const std::string e = config_error(c);
         if (!e.empty()) return "problem " + std::to_string(p) + ": " + e;
         if (c.nz != 1) return "problem " + std::to_string(p) + ": batched problems are 2-D (nz = 1)";
-        if (c.use_viscous || c.use_ibm) return "problem " + std::to_string(p) + ": batched problems are inviscid and without an immersed body";
+        if (c.use_viscous || c.use_ibm || c.use_bodyforce)
+            return "problem " + std::to_string(p) + ": batched problems are inviscid, without an immersed body or a body force";
         if (c.time_scheme == FVG_TS_HANCOCK) return "problem " + std::to_string(p) + ": batched problems use Euler, SSP-RK2 or SSP-RK3";
         if (c.reconstruction != a.reconstruction || c.riemann != a.riemann || c.time_scheme != a.time_scheme || c.precision != a.precision ||
             c.device != a.device)

@@ -50,6 +50,9 @@ struct Bc {
     const unsigned char* solid;
     const int* slot;
     const double* forced;
+    // the constant body force (gz = 0 on a 2-D mesh), on when grav_on
+    double grav[3];
+    int grav_on;
 };
 
 // BoundaryManager::ghost_state (cpp/src/Boundaries.cpp:106-153) for the sides a device run supports (every type but
@@ -116,6 +119,21 @@ template <int NV> __device__ __forceinline__ St<double, NV> read_state(const Bc&
         }
     }
     return read_cell<NV>(U, plane, c);
+}
+
+// ConstantBodyForce::add_to (cpp/src/Physics.cpp:832-844) for one cell of state u, into r in its order:
+// r1 += rho gx, r2 += rho gy, r3 += m_x gx + m_y gy, then with gz != 0 (a 3-D mesh) r3 += m_z gz and r4 += rho gz.
+template <int NV> __device__ __forceinline__ void add_body_force(const Bc& bc, const St<double, NV>& u, St<double, NV>& r) {
+    const double gx = bc.grav[0], gy = bc.grav[1], gz = bc.grav[2];
+    r[1] = r[1] + u[0] * gx;
+    r[2] = r[2] + u[0] * gy;
+    r[3] = r[3] + (u[1] * gx + u[2] * gy);
+    if constexpr (NV == 5) {
+        if (gz != 0.0) {
+            r[3] = r[3] + u[4] * gz;
+            r[4] = r[4] + u[0] * gz;
+        }
+    }
 }
 
 // The conservative state at cell position (i, j, k) of the reconstruction stencil, which may lie outside the mesh along

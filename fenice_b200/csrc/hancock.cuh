@@ -29,6 +29,7 @@ struct HancockArgs {
     int limiter;
     int mode;          // kStoreR or kAxpy
     const double* U;
+    const double* Rv;  // the viscous residual of U (null: inviscid); it joins the balance, not the predictor
     double* out;
     double* blockmax;
     const Ctl* ctl;    // dt and half_dt
@@ -61,6 +62,16 @@ __device__ __forceinline__ St<double, 4> euler_flux2(const Eos<double>& e, const
 __device__ __forceinline__ bool admissible(const Eos<double>& e, const St<double, 4>& U) {
     if (!(U[0] > Num<double>::eos_eps)) return false;
     return 0.5 * (U[1] * U[1] + U[2] * U[2] + 0.0 * 0.0) < U[0] * (U[3] - e.p_inf);
+}
+
+// The source field of a MUSCL-Hancock residual (Simulation::assemble, cpp/src/Simulation.cpp:975-980): zero, then the
+// body force added; the predictor takes d - half_dt src, the balance R + src after the viscous term (:1043-1047).
+template <int NV> __device__ __forceinline__ St<double, NV> body_source(const Bc& bc, const St<double, NV>& u) {
+    St<double, NV> src;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) src[q] = 0.0;
+    add_body_force<NV>(bc, u, src);
+    return src;
 }
 
 template <int RIEMANN, int TX, int TY, int NT>
@@ -142,6 +153,11 @@ __global__ void __launch_bounds__(NT) hancock_kernel(const HancockArgs a) {
                 St<double, 4> d;
 #pragma unroll
                 for (int q = 0; q < 4; ++q) d[q] = hx * (fxr[q] - fxl[q]) + hy * (fyt[q] - fyb[q]);
+                if (a.bc.grav_on) {   // the body force joins the predictor: d - half_dt src
+                    const St<double, 4> src = body_source<4>(a.bc, read_state<4>(a.bc, a.U, m.plane, (long long)cj * nx + ci));
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) d[q] = d[q] - half_dt * src[q];
+                }
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {
                     if (sd & (1 << s)) continue;
@@ -224,11 +240,21 @@ __global__ void __launch_bounds__(NT) hancock_kernel(const HancockArgs a) {
         const int gi = ox + c % TX, gj = oy + c / TX;
         if (gi >= nx || gj >= ny) continue;
         const long long cell = (long long)gj * nx + gi;
+        St<double, 4> r;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const double r = acc[q * NC + c] * m.inv_cell;
+            r[q] = acc[q * NC + c] * m.inv_cell;
+            if (a.Rv) r[q] = r[q] + a.Rv[q * m.plane + cell];
+        }
+        if (a.bc.grav_on) {
+            const St<double, 4> src = body_source<4>(a.bc, read_state<4>(a.bc, a.U, m.plane, cell));
+#pragma unroll
+            for (int q = 0; q < 4; ++q) r[q] = r[q] + src[q];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
             const long long x = q * m.plane + cell;
-            a.out[x] = a.mode == 0 ? r : a.U[x] + dt * r;
+            a.out[x] = a.mode == 0 ? r[q] : a.U[x] + dt * r[q];
         }
     }
     const double bm = block_max<NT>(smax, red);
@@ -375,6 +401,11 @@ __global__ void __launch_bounds__(NT) hancock3d_kernel(const HancockArgs a) {
                 const St<double, 5> fzf = euler_flux3(e, st[4], 2), fzk = euler_flux3(e, st[5], 2);
 #pragma unroll
                 for (int q = 0; q < 5; ++q) d[q] = (hx * (fxr[q] - fxl[q]) + hy * (fyt[q] - fyb[q])) + hz * (fzk[q] - fzf[q]);
+                if (a.bc.grav_on) {
+                    const St<double, 5> src = body_source<5>(a.bc, read_state<5>(a.bc, a.U, m.plane, cell_of(c3[0], c3[1], c3[2])));
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) d[q] = d[q] - half_dt * src[q];
+                }
                 f = 64;
                 if (sol) {   // solid_side_mask (Schemes.cpp:2890-2905), no wrap-around
                     auto sd = [&](int i, int j, int k) { return i >= 0 && i < n3[0] && j >= 0 && j < n3[1] && k >= 0 && k < n3[2] && sol[cell_of(i, j, k)]; };
@@ -470,11 +501,21 @@ __global__ void __launch_bounds__(NT) hancock3d_kernel(const HancockArgs a) {
         const int g3[3] = {o3[0] + c % TX, o3[1] + (c / TX) % TY, o3[2] + c / (TX * TY)};
         if (g3[0] >= m.nx || g3[1] >= m.ny || g3[2] >= m.nz) continue;
         const long long cell = cell_of(g3[0], g3[1], g3[2]);
+        St<double, 5> r;
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
-            const double r = acc[q * NC + c] * m.inv_cell;
+            r[q] = acc[q * NC + c] * m.inv_cell;
+            if (a.Rv) r[q] = r[q] + a.Rv[q * m.plane + cell];
+        }
+        if (a.bc.grav_on) {
+            const St<double, 5> src = body_source<5>(a.bc, read_state<5>(a.bc, a.U, m.plane, cell));
+#pragma unroll
+            for (int q = 0; q < 5; ++q) r[q] = r[q] + src[q];
+        }
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
             const long long x = q * m.plane + cell;
-            a.out[x] = a.mode == 0 ? r : a.U[x] + dt * r;
+            a.out[x] = a.mode == 0 ? r[q] : a.U[x] + dt * r[q];
         }
     }
     const double bm = block_max<NT>(smax, red);

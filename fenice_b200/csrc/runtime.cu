@@ -113,9 +113,9 @@ __global__ void k_end_rk(Ctl* c, int nstages) {
 
 // MUSCL-Hancock (MusclHancock::step, TimeScheme.cpp:296-319)
 __global__ void k_hancock_begin(Ctl* c) { c->seed = c->active && !(c->s_lag > 0.0); }
-__global__ void k_hancock_seed(Ctl* c, const double* bm, int nb) {
+__global__ void k_hancock_seed(Ctl* c, const double* bm, int nb, const double* bmv, int nbv) {
     if (!c->seed) return;
-    const double s = block_reduce_max(bm, nb, bm, 0);
+    const double s = block_reduce_max(bm, nb, bmv, nbv);
     if (threadIdx.x == 0) c->s_lag = s;
 }
 __global__ void k_hancock_dt(Ctl* c) {
@@ -126,9 +126,10 @@ __global__ void k_hancock_dt(Ctl* c) {
     c->dt = dt;
     c->half_dt = 0.5 * dt;
 }
-__global__ void k_hancock_end(Ctl* c, const double* bm, int nb) {
+// the step's speed: the Hancock residual's, max the viscous bound (Simulation.cpp:1038-1041), lagged to the next step
+__global__ void k_hancock_end(Ctl* c, const double* bm, int nb, const double* bmv, int nbv) {
     if (!c->active) return;
-    const double s = block_reduce_max(bm, nb, bm, 0);
+    const double s = block_reduce_max(bm, nb, bmv, nbv);
     if (threadIdx.x == 0) {
         c->s_lag = s;
         finish_step(c, s);
@@ -350,12 +351,19 @@ std::string validate(const fvg_config& c) {
     for (int a = 0; a < naxes; ++a)
         if ((c.bc[2 * a] == FVG_BC_PERIODIC) != (c.bc[2 * a + 1] == FVG_BC_PERIODIC))
             return "a periodic axis needs both of its sides periodic";
-    if (c.time_scheme == FVG_TS_HANCOCK) {
-        if (c.reconstruction != FVG_RECON_MUSCL) return "MUSCL-Hancock needs reconstruction = muscl";
-        if (c.use_viscous) return "MUSCL-Hancock with viscous fluxes is not supported on the device";
-    }
+    if (c.time_scheme == FVG_TS_HANCOCK && c.reconstruction != FVG_RECON_MUSCL) return "MUSCL-Hancock needs reconstruction = muscl";
+    if (c.use_bodyforce && c.precision == FVG_PREC_MIXED) return "the body force runs in the FP64 form only";
+    if (c.use_bodyforce && c.use_ibm) return "the body force with an immersed body (gravity in its ghost states) is not supported on the device";
     if (!(c.cfl > 0)) return "cfl must be > 0";
     return "";
+}
+
+// the constant body force of a configuration (Simulation::setup, cpp/src/Simulation.cpp:362-363: gz only on a 3-D mesh)
+void set_body_force(const fvg_config& c, Bc& bc) {
+    bc.grav_on = c.use_bodyforce ? 1 : 0;
+    bc.grav[0] = c.use_bodyforce ? c.gx : 0.0;
+    bc.grav[1] = c.use_bodyforce ? c.gy : 0.0;
+    bc.grav[2] = c.use_bodyforce && c.nz > 1 ? c.gz : 0.0;
 }
 
 // halo kinds of the sides for a reconstruction `depth` cells deep (Simulation.cpp:868-905, 1107-1176)
@@ -433,6 +441,7 @@ HancockArgs hancock_args(fvg_run* r, const double* Uin, double* out, int mode, d
     a.limiter = r->cfg.limiter;
     a.mode = mode;
     a.U = Uin;
+    a.Rv = r->cfg.use_viscous ? r->Rv : nullptr;
     a.out = out;
     a.blockmax = bm;
     a.ctl = r->ctl;
@@ -502,18 +511,22 @@ cudaError_t ibm_fill(fvg_run* r, const double* Usrc, double* Uout, int reset, co
     return cudaGetLastError();
 }
 
-// One residual stage of Uin: the viscous sweep (3-D viscous runs), then the inviscid stage kernel.
+// The viscous residual of Uin into Rv and its per-CTA speed bounds into bmv.
+cudaError_t launch_visc(fvg_run* r, const double* Uin, double* bmv, const int* gate, bool timed = true) {
+    if (timed) timer_mark(r, r->t_visc);
+    const cudaError_t e = r->dim == 2 ? launch_viscous2d(visc_args(r, Uin, bmv, gate), r->nbv, r->stream)
+                          : r->cfg.precision == FVG_PREC_MIXED ? mixed_viscous_launch(visc_args(r, Uin, bmv, gate), r->nbv, r->stream)
+                                                               : launch_viscous(visc_args(r, Uin, bmv, gate), r->nbv, r->stream);
+    if (timed) timer_mark(r, r->t_visc);
+    return e;
+}
+
+// One residual stage of Uin: the immersed body's forced states, the viscous sweep (viscous runs), then the inviscid
+// stage kernel.
 cudaError_t residual_stage(fvg_run* r, const double* Uin, const double* U0, double* out, int mode, double ca, double cb, int stage, const int* gate) {
     cudaError_t e;
     if (r->ibm && (e = ibm_fill(r, Uin, nullptr, 0, gate)) != cudaSuccess) return e;
-    if (r->cfg.use_viscous) {
-        timer_mark(r, r->t_visc);
-        e = r->dim == 2 ? launch_viscous2d(visc_args(r, Uin, r->bmv[stage], gate), r->nbv, r->stream)
-            : r->cfg.precision == FVG_PREC_MIXED ? mixed_viscous_launch(visc_args(r, Uin, r->bmv[stage], gate), r->nbv, r->stream)
-                                                 : launch_viscous(visc_args(r, Uin, r->bmv[stage], gate), r->nbv, r->stream);
-        timer_mark(r, r->t_visc);
-        if (e != cudaSuccess) return e;
-    }
+    if (r->cfg.use_viscous && (e = launch_visc(r, Uin, r->bmv[stage], gate)) != cudaSuccess) return e;
     timer_mark(r, r->t_stage);
     e = r->stage.launch(stage_args(r, Uin, U0, out, mode, ca, cb, r->cfg.use_viscous ? r->Rv : nullptr, r->bm[stage], gate), r->nb, r->stream);
     timer_mark(r, r->t_stage);
@@ -548,17 +561,22 @@ cudaError_t enqueue_step(fvg_run* r, bool refresh = true) {
         double* Uin = r->Ucur();
         double* Uout = r->cur ? r->U : r->Ut;
         k_hancock_begin<<<1, 1, 0, r->stream>>>(c);
+        // the seed (first step only; untimed): one plain residual for the speed, its viscous bound included
         if (r->ibm && (e = ibm_fill(r, Uin, nullptr, 0, &c->seed))) return e;
-        if ((e = r->stage.launch(stage_args(r, Uin, nullptr, r->R, kStoreR, 0, 0, nullptr, r->bm_seed, &c->seed), r->nb, r->stream))) return e;
-        k_hancock_seed<<<1, 1024, 0, r->stream>>>(c, r->bm_seed, r->nb);
+        if (r->cfg.use_viscous && (e = launch_visc(r, Uin, r->bmv[1], &c->seed, false))) return e;
+        if ((e = r->stage.launch(stage_args(r, Uin, nullptr, r->R, kStoreR, 0, 0, r->cfg.use_viscous ? r->Rv : nullptr, r->bm_seed, &c->seed), r->nb,
+                                 r->stream)))
+            return e;
+        k_hancock_seed<<<1, 1024, 0, r->stream>>>(c, r->bm_seed, r->nb, r->bmv[1], nbv);
         k_hancock_dt<<<1, 1, 0, r->stream>>>(c);
         if (r->ibm && (e = ibm_fill(r, Uin, nullptr, 0, act))) return e;
+        if (r->cfg.use_viscous && (e = launch_visc(r, Uin, r->bmv[0], act))) return e;
         timer_mark(r, r->t_stage);
         e = launch_hancock(r, hancock_args(r, Uin, Uout, kAxpy, r->bm[0], act));
         timer_mark(r, r->t_stage);
         if (e) return e;
         if (r->ibm && (e = ibm_fill(r, Uout, Uout, 1, act))) return e;
-        k_hancock_end<<<1, 1024, 0, r->stream>>>(c, r->bm[0], r->nbh);
+        k_hancock_end<<<1, 1024, 0, r->stream>>>(c, r->bm[0], r->nbh, r->bmv[0], nbv);
         r->cur ^= 1;
         return cudaGetLastError();
     }
@@ -676,6 +694,7 @@ int fvg_create(const fvg_config* cfg, fvg_run** out) {
     run->bc.u_in = c.u_in;
     run->bc.v_in = c.v_in;
     run->bc.p_out = c.p_out;
+    set_body_force(c, run->bc);
     const int TX = run->dim == 3 ? Tile<3>::X : Tile<2>::X, TY = run->dim == 3 ? Tile<3>::Y : Tile<2>::Y, TZ = run->dim == 3 ? Tile<3>::Z : 1;
     run->tiles[0] = (c.nx + TX - 1) / TX;
     run->tiles[1] = (c.ny + TY - 1) / TY;
@@ -860,12 +879,13 @@ int fvg_residual(fvg_run* run, double predictor_half_dt, double* R, size_t ncell
     const int* always = &c->always;
     double* out = run->cur ? run->U : run->Ut;   // a buffer that is not the state
     if (predictor_half_dt > 0.0) {
-        if (run->cfg.reconstruction != FVG_RECON_MUSCL || run->cfg.use_viscous)
-            return fail(run, FVG_ERR_CONFIG, "the MUSCL-Hancock predictor needs an inviscid MUSCL run");
+        if (run->cfg.reconstruction != FVG_RECON_MUSCL)
+            return fail(run, FVG_ERR_CONFIG, "the MUSCL-Hancock predictor needs a MUSCL run");
         CK(cudaMemcpyAsync(&c->half_dt, &predictor_half_dt, sizeof(double), cudaMemcpyHostToDevice, run->stream));
         if (run->ibm) CK(ibm_fill(run, run->Ucur(), nullptr, 0, always));
+        if (run->cfg.use_viscous) CK(launch_visc(run, run->Ucur(), run->bmv[0], always));
         CK(launch_hancock(run, hancock_args(run, run->Ucur(), out, kStoreR, run->bm[0], always)));
-        k_stage_max<<<1, 1024, 0, run->stream>>>(c, always, 0, run->bm[0], run->nbh, run->bmv[0], 0);
+        k_stage_max<<<1, 1024, 0, run->stream>>>(c, always, 0, run->bm[0], run->nbh, run->bmv[0], run->cfg.use_viscous ? run->nbv : 0);
     } else {
         CK(refresh_gate(run, run->Ucur(), nullptr));
         CK(residual_stage(run, run->Ucur(), nullptr, out, kStoreR, 0, 0, 0, always));
@@ -1280,6 +1300,7 @@ extern "C" int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long
     a.bc.u_in = c.u_in;
     a.bc.v_in = c.v_in;
     a.bc.p_out = c.p_out;
+    set_body_force(c, a.bc);
     a.eos.type = c.eos_type;
     a.eos.gamma = c.gamma;
     a.eos.p_inf = c.p_inf;

@@ -12,7 +12,7 @@
 //   4. balance: one thread per cell adds the face-flux difference of this axis to a shared-memory accumulator,
 //              in the reference's expression order ((0 - x) - y) - z, so the result has its bits.
 // The faces between two tiles are solved by both (the same bits; the reference's thread blocks do the same).
-// Epilogue: R = acc * (1 / volume) (+ the viscous residual of the stage), then the stage update
+// Epilogue: R = acc * (1 / volume) (+ the viscous residual of the stage, + the body force), then the stage update
 //   STORE_R:  out = R
 //   AXPY:     out = U + dt R                            (forward Euler, MUSCL-Hancock)
 //   COMBINE:  out = a U0 + b (U + dt R)                 (SSP-RK2 / RK3 stages 2 and 3)
@@ -232,18 +232,24 @@ __global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
         const int g3[3] = {o3[0] + c3[0], o3[1] + c3[1], o3[2] + c3[2]};
         if (g3[0] >= m.nx || g3[1] >= m.ny || g3[2] >= m.nz) continue;
         const long long cell = ((long long)g3[2] * m.ny + g3[1]) * m.nx + g3[0];
+        St<double, NV> r;
 #pragma unroll
         for (int q = 0; q < NV; ++q) {
-            double r = acc[q * NC + c] * m.inv_cell;
-            if (a.Rv) r = r + a.Rv[q * m.plane + cell];
+            r[q] = acc[q * NC + c] * m.inv_cell;
+            if (a.Rv) r[q] = r[q] + a.Rv[q * m.plane + cell];
+        }
+        // the body force joins after the viscous term (Simulation::assemble, cpp/src/Simulation.cpp:1038-1049)
+        if (a.bc.grav_on) add_body_force<NV>(a.bc, read_state<NV>(a.bc, a.U, m.plane, cell), r);
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
             const long long e = q * m.plane + cell;
             double o;
             if (a.mode == kStoreR)
-                o = r;
+                o = r[q];
             else if (a.mode == kAxpy)
-                o = a.U[e] + dt * r;
+                o = a.U[e] + dt * r[q];
             else
-                o = a.ca * a.U0[e] + a.cb * (a.U[e] + dt * r);
+                o = a.ca * a.U0[e] + a.cb * (a.U[e] + dt * r[q]);
             a.out[e] = o;
         }
     }

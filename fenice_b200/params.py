@@ -21,6 +21,7 @@ DEFAULTS = {
     "boundary_order": 2, "time_scheme": "auto", "cfl": 0.5, "shock_blend": 0.2, "dt_max": 0.0, "t_end": 0.005,
     "max_steps": 0,
     "use_ibm": False, "ibm_shape": "Cylinder", "ibm_radius": 0.1, "ibm_cx": 0.5, "ibm_cy": 0.5, "ibm_cz": 0.5, "ibm_curvature": False,
+    "use_bodyforce": False, "gx": 0.0, "gy": -9.81, "gz": 0.0,
 }
 
 BC_NAMES = {"wall": 0, "inviscid wall (slip)": 0, "no_slip": 1, "viscous wall (no-slip)": 1, "moving_wall": 2, "moving wall": 2,
@@ -48,7 +49,8 @@ class FvgConfig(ctypes.Structure):
                 ("use_viscous", ctypes.c_int), ("mu", ctypes.c_double), ("pr", ctypes.c_double),
                 ("precision", ctypes.c_int), ("device", ctypes.c_int),
                 ("use_ibm", ctypes.c_int), ("ibm_shape", ctypes.c_int), ("ibm_radius", ctypes.c_double), ("ibm_cx", ctypes.c_double),
-                ("ibm_cy", ctypes.c_double), ("ibm_cz", ctypes.c_double), ("ibm_curvature", ctypes.c_int)]
+                ("ibm_cy", ctypes.c_double), ("ibm_cz", ctypes.c_double), ("ibm_curvature", ctypes.c_int),
+                ("use_bodyforce", ctypes.c_int), ("gx", ctypes.c_double), ("gy", ctypes.c_double), ("gz", ctypes.c_double)]
 
 
 def _flag(v):
@@ -82,8 +84,46 @@ def resolve(params):
     return p
 
 
+def _num(v):
+    try:
+        return float(v)
+    except (TypeError, ValueError):
+        return None
+
+
+def not_on_device(params):
+    """The reference features a parameter dict switches on that the device path does not compute (None: none). They
+    are refused, never ignored: AMR, case-file source expressions (source_* evaluated per cell and stage), the
+    positivity fallback, fourth-order flux quadrature, time tables of the inlet / outlet values, reynolds (mu derived from
+    the body's length scale), and a moving or flow-driven immersed body. (Combinations the device refuses, such as the body
+force with the mixed-precision form, are refused by fvg_create with FVG_ERR_CONFIG.)"""
+    p = resolve(params)
+    if _flag(p.get("use_amr", False)):
+        return "adaptive meshes (use_amr)"
+    src = [k for k in ("source_rho", "source_mx", "source_my", "source_mz", "source_E") if _num(p.get(k, 0)) != 0.0]
+    if src:
+        return "case-file source terms (" + ", ".join(src) + ")"
+    if _flag(p.get("positivity_fallback", False)):
+        return "the positivity fallback"
+    if str(p.get("flux_quadrature", "midpoint")).strip().lower() != "midpoint":
+        return "fourth-order flux quadrature"
+    tables = [k for k in p if k.endswith("_table") and str(p[k]).strip()]
+    if tables:
+        return "time tables (" + ", ".join(tables) + ")"
+    if (_num(p.get("reynolds", 0)) or 0.0) > 0.0:
+        return "reynolds > 0 (give mu)"
+    if _flag(p["use_ibm"]):
+        moving = [k for k in ("ibm_vx", "ibm_vy", "ibm_vz", "ibm_omega", "ibm_omega_x", "ibm_omega_y", "ibm_mass") if (_num(p.get(k, 0)) or 0.0) != 0.0]
+        if moving:
+            return "a moving immersed body (" + ", ".join(moving) + ")"
+    return None
+
+
 def to_config(params, precision=0, device=0):
-    """fvg_config of a parameter dict (reference keys)."""
+    """fvg_config of a parameter dict (reference keys); ValueError for a feature the device path does not compute."""
+    why = not_on_device(params)
+    if why:
+        raise ValueError(f"not computed by the device path: {why}")
     p = resolve(params)
     c = FvgConfig()
     c.nx, c.ny, c.nz = int(p["nx"]), int(p["ny"]), int(p["nz"])
@@ -112,6 +152,8 @@ def to_config(params, precision=0, device=0):
     c.ibm_shape = 1 if shape == "sphere" else 0
     c.ibm_radius, c.ibm_cx, c.ibm_cy, c.ibm_cz = float(p["ibm_radius"]), float(p["ibm_cx"]), float(p["ibm_cy"]), float(p["ibm_cz"])
     c.ibm_curvature = 1 if _flag(p["ibm_curvature"]) else 0
+    c.use_bodyforce = 1 if _flag(p["use_bodyforce"]) else 0
+    c.gx, c.gy, c.gz = float(p["gx"]), float(p["gy"]), float(p["gz"])
     return c
 
 

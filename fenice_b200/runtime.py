@@ -37,6 +37,7 @@ EXPORTS = ["fvg_abi_version", "fvg_create", "fvg_destroy", "fvg_last_error", "fv
            "fvg_set_sensor", "fvg_get_sensor_counts", "fvg_ibm_loads"]
 
 _lib = None
+ABI_VERSION = 2   # FVG_ABI_VERSION of include/fenice_gpu.h
 
 
 def load_library(path=LIB_PATH):
@@ -50,6 +51,8 @@ def load_library(path=LIB_PATH):
     c_p = ctypes.c_void_p
     dp = ctypes.POINTER(ctypes.c_double)
     lib.fvg_abi_version.restype = ctypes.c_int
+    if lib.fvg_abi_version() != ABI_VERSION:   # fvg_config's layout is the one params.FvgConfig mirrors
+        raise RuntimeError(f"{path} has ABI version {lib.fvg_abi_version()}, this package needs {ABI_VERSION}: rebuild it")
     lib.fvg_create.argtypes = [ctypes.POINTER(P.FvgConfig), ctypes.POINTER(c_p)]
     lib.fvg_destroy.argtypes = [c_p]
     lib.fvg_last_error.argtypes = [c_p]

@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define FVG_ABI_VERSION 1
+#define FVG_ABI_VERSION 2
 
 /* status codes */
 enum {
@@ -73,6 +73,8 @@ typedef struct fvg_config {
     int ibm_shape;               /* [ibm] ibm_shape: 0 Cylinder (a circle in 2-D, infinite along z in 3-D), 1 Sphere (3-D) */
     double ibm_radius, ibm_cx, ibm_cy, ibm_cz; /* [ibm] */
     int ibm_curvature;           /* [ibm] ibm_curvature (must be 0 on the device) */
+    int use_bodyforce;           /* [physics] use_bodyforce: the constant body force (ConstantBodyForce, Physics.cpp:832-844) */
+    double gx, gy, gz;           /* [physics] gx, gy, gz (gz is not used on a 2-D mesh) */
 } fvg_config;
 
 typedef struct fvg_run fvg_run;

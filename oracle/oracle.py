@@ -88,8 +88,28 @@ class OracleConfig(ctypes.Structure):
                 ("viscous", ctypes.c_int), ("mu", ctypes.c_double), ("pr", ctypes.c_double)]
 
 
+def not_covered(p):
+    """Features the restatement does not compute (it refuses them rather than ignore them)."""
+    if _flag(p.get("use_ibm", False)):
+        return "the immersed body"
+    if _flag(p.get("use_bodyforce", False)):
+        return "the body force"
+    for k in ("source_rho", "source_mx", "source_my", "source_mz", "source_E"):
+        try:
+            if float(p.get(k, 0)) != 0.0:
+                return "source terms"
+        except (TypeError, ValueError):
+            return "source terms"
+    if _flag(p.get("use_amr", False)) or _flag(p.get("positivity_fallback", False)):
+        return "AMR / the positivity fallback"
+    return None
+
+
 def oracle_config(params):
     p = resolved(params)
+    why = not_covered(p)
+    if why:
+        raise ValueError(f"the restatement does not cover {why}")
     c = OracleConfig()
     c.nx, c.ny, c.nz = int(p["nx"]), int(p["ny"]), int(p["nz"])
     c.Lx, c.Ly, c.Lz = float(p["Lx"]), float(p["Ly"]), float(p["Lz"])

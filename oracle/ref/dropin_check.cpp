@@ -73,6 +73,10 @@ static fvg_config to_fvg(const fv::SimParams& p) {
     c.ibm_cy = p.ibm_cy;
     c.ibm_cz = p.ibm_cz;
     c.ibm_curvature = p.ibm_curvature ? 1 : 0;
+    c.use_bodyforce = p.use_bodyforce ? 1 : 0;
+    c.gx = p.gx;
+    c.gy = p.gy;
+    c.gz = p.gz;
     return c;
 }
 

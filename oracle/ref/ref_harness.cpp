@@ -66,14 +66,15 @@ extern "C" {
 const char* ref_error() { return g_error.c_str(); }
 
 // kv: "key=value" lines. Keys of the reference's parameter table, plus initial_profile (isentropic_vortex,
-// taylor_green_3d, taylor_green) or initial_state ("rho,u,v,p[,w]", a uniform field).
+// taylor_green_3d, taylor_green) or initial_state ("rho,u,v,p[,w]", a uniform field), or case (a test case name of
+// the reference or a case folder / case.toml: its defaults and its own initial condition, as `fenice --case`).
 void* ref_create(const char* kv) {
     try {
         auto* r = new RefRun();
         char tmpl[] = "/tmp/fenice_ref_XXXXXX";
         if (!mkdtemp(tmpl)) throw std::runtime_error("mkdtemp failed");
         r->dir = tmpl;
-        std::string profile, state = "1,0,0,1,0";
+        std::string profile, state = "1,0,0,1,0", case_name;
         fv::Params p = fv::baseline_defaults();
         std::stringstream ss(kv ? kv : "");
         std::string line;
@@ -88,17 +89,20 @@ void* ref_create(const char* kv) {
                 profile = v;
             else if (k == "initial_state")
                 state = v;
+            else if (k == "case")
+                case_name = v;
             else
                 over.emplace_back(k, v);
         }
-        const fs::path cf = r->dir / "case.toml";
-        {
+        std::string cf = case_name;
+        if (cf.empty()) {
+            cf = (r->dir / "case.toml").string();
             std::ofstream f(cf);
             f << case_text(profile, state);
         }
-        const fv::TestCase& tc = fv::get_test_case(cf.string());
+        const fv::TestCase& tc = fv::get_test_case(cf);
         p.merge(tc.defaults);
-        p.set("test_case", cf.string());
+        p.set("test_case", cf);
         p.set("output_root", (r->dir / "out").string());
         p.set("save_interval", "1000000000");
         for (const auto& e : over) p.set(e.first, e.second);

@@ -179,3 +179,24 @@ HANCOCK3D_STEP_CASES = [
     ("h3s_mc_inlet", dict(nx=11, ny=10, nz=9, reconstruction="muscl", muscl_limiter="MC", time_scheme="MUSCL-Hancock", **bcs("vel_inlet", "transmissive", "wall", "no_slip", z=("periodic", "periodic")), u_in=0.8), 37, 5),
     ("h3s_minmod_order1", dict(nx=10, ny=9, nz=11, reconstruction="muscl", muscl_limiter="Minmod", boundary_order=1, time_scheme="MUSCL-Hancock", **bcs("wall", "outlet", "transmissive", "moving_wall", z=("no_slip", "transmissive")), u_in=0.2), 38, 4),
 ]
+
+# the body force (ConstantBodyForce) and MUSCL-Hancock with viscous fluxes: a residual (with the predictor of half a step
+# for MUSCL-Hancock), then steps; (name, params, seed, predictor_half_dt, n_steps)
+FORCE_CASES = [
+    ("grav_muscl_rk2_2d", dict(nx=24, ny=20, reconstruction="muscl", muscl_limiter="MC", time_scheme="SSP Runge-Kutta 2", use_bodyforce=True, gx=0.3,
+                               gy=-1.2, **bcs("transmissive", "transmissive", "wall", "wall")), 51, 0.0, 4),
+    ("grav_weno5_rk3_3d", dict(nx=10, ny=9, nz=11, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", use_bodyforce=True, gx=-0.2, gy=0.5, gz=-0.9,
+                               **bcs("periodic", "periodic", "wall", "no_slip", z=("wall", "transmissive"))), 52, 0.0, 3),
+    ("grav_hancock_2d", dict(nx=22, ny=18, reconstruction="muscl", muscl_limiter="Van Leer", time_scheme="MUSCL-Hancock", use_bodyforce=True, gx=0.0,
+                             gy=-2.0, **bcs("periodic", "periodic", "wall", "wall")), 53, 0.004, 5),
+    ("grav_hancock_3d_visc", dict(nx=11, ny=10, nz=9, reconstruction="muscl", muscl_limiter="MC", time_scheme="MUSCL-Hancock", use_viscous=True, mu=0.02,
+                                  use_bodyforce=True, gx=0.4, gy=0.0, gz=-1.5, **bcs("wall", "transmissive", "periodic", "periodic", z=("no_slip", "wall"))),
+     54, 0.003, 4),
+    ("hancock_visc_2d_walls", dict(nx=20, ny=17, reconstruction="muscl", muscl_limiter="Minmod", time_scheme="MUSCL-Hancock", use_viscous=True, mu=0.03,
+                                   **bcs("no_slip", "outlet", "moving_wall", "wall"), u_in=0.3), 55, 0.004, 5),
+    ("hancock_visc_3d_order1", dict(nx=9, ny=12, nz=10, reconstruction="muscl", muscl_limiter="Koren", boundary_order=1, time_scheme="MUSCL-Hancock",
+                                    use_viscous=True, mu=0.01, riemann_solver="lowmach", **bcs("periodic", "periodic", "no_slip", "moving_wall",
+                                                                                                z=("transmissive", "wall")), u_in=0.2), 56, 0.003, 4),
+    ("grav_first_order_stiff", dict(nx=30, ny=8, reconstruction="none", time_scheme="Explicit Euler", eos_type="Stiffened Gas", gamma=4.4, p_inf=0.5,
+                                    use_bodyforce=True, gx=0.3, gy=-1.0, **bcs("transmissive", "transmissive", "wall", "wall")), 57, 0.0, 6),
+]

@@ -10,9 +10,10 @@ the seeded inputs of tests/cases.py and stores, per case, the parameters, the in
   ibm.npz        immersed-body cases: the forced field, a residual, then a few steps
   visc2d.npz     2-D viscous cases (NavierStokes::viscous_residual_rows): a residual, then a few steps
   hancock3d.npz  3-D MUSCL-Hancock (MusclReconstruction::hancock_residual_3d): residuals with the predictor, then steps
+  forces.npz     the body force (ConstantBodyForce) and MUSCL-Hancock with viscous fluxes: a residual, then steps
   riemann.json   the reference's bench_riemann fingerprints over one pass of its 65536 state pairs
                  (oracle/_ref/bench_riemann 65536)
-Sections can be named on the command line (residuals steps ibm visc2d hancock3d riemann); default: all.
+Sections can be named on the command line (residuals steps ibm visc2d hancock3d forces riemann); default: all.
 The fixtures are test data: nothing of the product reads them.
 """
 import json
@@ -78,11 +79,34 @@ def hancock3d():
     np.savez_compressed(os.path.join(HERE, "hancock3d.npz"), **out)
 
 
-def main(sections=("residuals", "steps", "ibm", "visc2d", "hancock3d", "riemann")):
+def forces():
+    out = {}
+    for name, params, seed, half, n in cases.FORCE_CASES:
+        U = cases.case_field(params, seed)
+        ref = Reference(params, initial_state=(1, 0, 0, 1, 0))
+        R, s = ref.residual(U, predictor_half_dt=half)
+        out[f"{name}/params"] = np.array(json.dumps(params))
+        out[f"{name}/U0"] = U
+        out[f"{name}/R"] = R
+        out[f"{name}/smax"] = np.array(s)
+        out[f"{name}/half_dt"] = np.array(half)
+        ref.set_state(U)
+        dts, sms = ref.steps(n, 1e30)
+        out[f"{name}/U"] = ref.state()
+        out[f"{name}/dts"] = dts
+        out[f"{name}/smaxs"] = sms
+        out[f"{name}/t"] = np.array(ref.t)
+        print(f"forces {name}: smax {s:.6g}, {len(dts)} steps")
+    np.savez_compressed(os.path.join(HERE, "forces.npz"), **out)
+
+
+def main(sections=("residuals", "steps", "ibm", "visc2d", "hancock3d", "forces", "riemann")):
     if "visc2d" in sections:
         visc2d()
     if "hancock3d" in sections:
         hancock3d()
+    if "forces" in sections:
+        forces()
     if "residuals" in sections:
         residuals()
     if "steps" in sections:
@@ -162,4 +186,4 @@ def riemann():
 
 
 if __name__ == "__main__":
-    main(tuple(sys.argv[1:]) or ("residuals", "steps", "ibm", "visc2d", "hancock3d", "riemann"))
+    main(tuple(sys.argv[1:]) or ("residuals", "steps", "ibm", "visc2d", "hancock3d", "forces", "riemann"))

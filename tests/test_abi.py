@@ -26,12 +26,13 @@ def test_library_exports_every_declared_entry_point():
     for n in names:
         assert hasattr(lib, n), n
     assert set(names) == set(RT.EXPORTS)
-    assert lib.fvg_abi_version() == 1
+    assert lib.fvg_abi_version() == 2
 
 
 def create_code(params):
     lib = RT.load_library()
-    c = P.to_config(params)
+    params = dict(params)
+    c = P.to_config(params, precision=1 if params.pop("precision_mixed", False) else 0)
     h = ctypes.c_void_p()
     rc = lib.fvg_create(ctypes.byref(c), ctypes.byref(h))
     return rc, lib.fvg_create_error().decode()
@@ -43,7 +44,8 @@ def create_code(params):
     (dict(bc_xmax="nonreflecting"), "non-reflecting"),
     (dict(bc_xmin="periodic", bc_xmax="wall"), "periodic"),
     (dict(reconstruction="weno5", time_scheme="MUSCL-Hancock"), "MUSCL-Hancock"),
-    (dict(use_viscous=True, reconstruction="muscl", time_scheme="MUSCL-Hancock"), "viscous"),
+    (dict(use_bodyforce=True, reconstruction="muscl", time_scheme="SSP Runge-Kutta 2", precision_mixed=True), "FP64 form only"),
+    (dict(use_bodyforce=True, use_ibm=True, bc_xmin="vel_inlet"), "immersed body"),
     (dict(boundary_order=3), "boundary_order"),
     (dict(cfl=0.0), "cfl"),
 ])
