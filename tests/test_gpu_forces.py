@@ -63,8 +63,8 @@ def test_force_graph_run_bit_exact(fx, case):
 def test_body_force_refusals(fx):
     p = json.loads(str(fx["grav_muscl_rk2_2d/params"]))
     U = fx["grav_muscl_rk2_2d/U0"]
-    with pytest.raises(RuntimeError, match="FP64 form only"):
+    with pytest.raises(ValueError, match="FP64 form only"):
         Run(p, U=U, precision=1)
     q = dict(p, use_ibm=True, ibm_shape="Cylinder", ibm_radius=0.2, ibm_cx=0.5, ibm_cy=0.5, bc_xmin="vel_inlet", u_in=0.5)
-    with pytest.raises(RuntimeError, match="immersed body"):
+    with pytest.raises(ValueError, match="immersed body"):
         Run(q, U=U)
