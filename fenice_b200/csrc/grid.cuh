@@ -15,8 +15,10 @@ namespace fvg {
 constexpr int kBcWall = 0, kBcNoSlip = 1, kBcMovingWall = 2, kBcVelInlet = 3, kBcMassflowInlet = 4, kBcOutlet = 5,
               kBcTransmissive = 6, kBcPeriodic = 7, kBcNonReflecting = 8;
 // what lies beyond a side for the reconstruction stencil (cpp/src/Simulation.cpp:868-905): nothing (edge
-// replication, first-order boundary faces), the periodic wrap, or the ghost slab of the boundary condition
-constexpr int kHaloNone = 0, kHaloWrap = 1, kHaloSlab = 2;
+// replication, first-order boundary faces), the periodic wrap, or the ghost slab of the boundary condition; and, for
+// one part of a slab-decomposed mesh, the neighbouring part's cells, held in ghost planes beyond the side (the state
+// arrays of a part are allocated with Bc::ext planes there, so indices -ext .. -1 and n .. n + ext - 1 are real cells)
+constexpr int kHaloNone = 0, kHaloWrap = 1, kHaloSlab = 2, kHaloPeer = 3;
 
 // Device control block of a run: the clock, the step and the wave speeds, all on the device so a step needs no
 // host round trip (and can be captured in a CUDA graph).
@@ -53,7 +55,16 @@ struct Bc {
     // the constant body force (gz = 0 on a 2-D mesh), on when grav_on
     double grav[3];
     int grav_on;
+    // planes of the neighbouring part held beyond each side (kHaloPeer sides only; 0 elsewhere)
+    int ext[6];
 };
+
+// Whether position g along an axis of n cells is a cell whose state is in the arrays (a cell of the mesh, or of a
+// neighbouring part's ghost planes beyond a kHaloPeer side), and the wrapped index of a periodic axis otherwise.
+__device__ __forceinline__ bool held(const Bc& bc, int axis, int g, int n) {
+    return (g >= 0 && g < n) || (g < 0 && bc.halo[2 * axis] == kHaloPeer && g >= -bc.ext[2 * axis]) ||
+           (g >= n && bc.halo[2 * axis + 1] == kHaloPeer && g < n + bc.ext[2 * axis + 1]);
+}
 
 // BoundaryManager::ghost_state (cpp/src/Boundaries.cpp:106-153) for the sides a device run supports (every type but
 // the mass-flow inlet and the non-reflecting outlet, which need more than one cell).
@@ -151,10 +162,12 @@ __device__ __forceinline__ St<double, NV> stencil_cons(const Mesh& m, const Bc& 
     for (int a = 0; a < DIM; ++a) {
         const bool lo = idx[a] < 0, hi = idx[a] >= n3[a];
         if (!lo && !hi) continue;
-        if (bc.halo[2 * a + (hi ? 1 : 0)] == kHaloWrap) {
+        const int kind = bc.halo[2 * a + (hi ? 1 : 0)];
+        if (kind == kHaloWrap) {
             idx[a] = ((idx[a] % n3[a]) + n3[a]) % n3[a];
             continue;
         }
+        if (kind == kHaloPeer) continue;   // the neighbouring part's cell (clamped below onto its ghost planes)
         out_axis = a;
         ++nout;
     }
@@ -171,7 +184,10 @@ __device__ __forceinline__ St<double, NV> stencil_cons(const Mesh& m, const Bc& 
         }
     }
 #pragma unroll
-    for (int a = 0; a < 3; ++a) idx[a] = idx[a] < 0 ? 0 : (idx[a] >= n3[a] ? n3[a] - 1 : idx[a]);
+    for (int a = 0; a < 3; ++a) {
+        const int lo = -bc.ext[2 * a], hi = n3[a] - 1 + bc.ext[2 * a + 1];
+        idx[a] = idx[a] < lo ? lo : (idx[a] > hi ? hi : idx[a]);
+    }
     const long long c = ((long long)idx[2] * m.ny + idx[1]) * m.nx + idx[0];
     return read_state<NV>(bc, U, m.plane, c);
 }

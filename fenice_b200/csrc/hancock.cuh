@@ -123,11 +123,11 @@ __global__ void __launch_bounds__(NT) hancock_kernel(const HancockArgs a) {
             st[2 * ax + 1] = p2c(e, wl);
             st[2 * ax] = p2c(e, wr);
         }
-        const bool in_x = gi >= 0 && gi < nx, in_y = gj >= 0 && gj < ny;
-        const bool real = (in_x || wrap_x) && (in_y || wrap_y) && gi < nx + 1 && gj < ny + 1 && gi >= -1 && gj >= -1;
+        // a real cell: of the mesh, of a periodic wrap, or of the neighbouring part beyond a part interface
+        const bool real = gi >= -1 && gi <= nx && gj >= -1 && gj <= ny && (wrap_x || held(a.bc, 0, gi, nx)) && (wrap_y || held(a.bc, 1, gj, ny));
         if (real) {
             // the mesh cell (wrapped): sides without a halo give it the round trip of its own state there
-            const int ci = (gi + nx) % nx, cj = (gj + ny) % ny;
+            const int ci = wrap_x ? (gi + nx) % nx : gi, cj = wrap_y ? (gj + ny) % ny : gj;
             const bool b0 = ci == 0 && a.bc.halo[0] == kHaloNone, b1 = ci == nx - 1 && a.bc.halo[1] == kHaloNone;
             const bool b2 = cj == 0 && a.bc.halo[2] == kHaloNone, b3 = cj == ny - 1 && a.bc.halo[3] == kHaloNone;
             if (b0 || b1 || b2 || b3) {
@@ -360,9 +360,8 @@ __global__ void __launch_bounds__(NT) hancock3d_kernel(const HancockArgs a) {
         bool real = true;
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            const bool in = g[d] >= 0 && g[d] < n3[d];
-            real = real && (in || (wrap[d] && g[d] >= -1 && g[d] <= n3[d]));
-            c3[d] = (g[d] + n3[d]) % n3[d];
+            real = real && g[d] >= -1 && g[d] <= n3[d] && (wrap[d] || held(a.bc, d, g[d], n3[d]));
+            c3[d] = wrap[d] ? (g[d] + n3[d]) % n3[d] : g[d];
         }
         if (real) {
             const int side_lo = 2 * ax, c = c3[ax];
@@ -386,9 +385,8 @@ __global__ void __launch_bounds__(NT) hancock3d_kernel(const HancockArgs a) {
             int c3[3];
 #pragma unroll
             for (int x = 0; x < 3; ++x) {
-                const bool in = g[x] >= 0 && g[x] < n3[x];
-                real = real && (in || (wrap[x] && g[x] >= -1 && g[x] <= n3[x]));
-                c3[x] = (g[x] + n3[x]) % n3[x];
+                real = real && g[x] >= -1 && g[x] <= n3[x] && (wrap[x] || held(a.bc, x, g[x], n3[x]));
+                c3[x] = wrap[x] ? (g[x] + n3[x]) % n3[x] : g[x];
             }
             const unsigned char* sol = a.bc.solid;
             const bool is_solid = real && sol && sol[cell_of(c3[0], c3[1], c3[2])];

@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
         for (int x = 0; x < 3; ++x)
             if (a.periodic[x] && (g[x] < 0 || g[x] >= n3[x])) g[x] = ((g[x] % n3[x]) + n3[x]) % n3[x];
 #pragma unroll
-        for (int x = 0; x < 3; ++x) g[x] = g[x] < -1 ? -1 : (g[x] > n3[x] ? n3[x] : g[x]);
+        for (int x = 0; x < 3; ++x) g[x] = box_clamp(a, x, g[x], n3[x]);
         const St<double, 5> u = padded_cons(a, g[0], g[1], g[2]);
         const St<double, 5> w = c2p(a.eos, u);
         B[0 * NB + e] = (float)u[0];
@@ -346,9 +346,10 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
                 int lc[3] = {f3[0], f3[1], f3[2]};
                 lc[d] -= 1;
                 const int pL = bidx(lc[0], lc[1], lc[2]), pR = pL + bstride;
-                const int xL = (lo && !a.periodic[d]) ? eR : eL;
-                const int xR = (hi && !a.periodic[d]) ? eL : eR;
-                const bool phys = a.bface2 && !a.periodic[d] && (lo || hi);
+                const bool lo_wall = lo && !a.through[2 * d], hi_wall = hi && !a.through[2 * d + 1];
+                const int xL = lo_wall ? eR : eL;
+                const int xR = hi_wall ? eL : eR;
+                const bool phys = a.bface2 && (lo_wall || hi_wall);
                 float Gc[4];
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {

@@ -136,6 +136,58 @@ __global__ void k_hancock_end(Ctl* c, const double* bm, int nb, const double* bm
     }
 }
 
+// ---- parts of a slab-decomposed mesh
+// the largest of a stage's per-CTA speeds (and viscous bounds) into a slot the hosts all-reduce (0 when the gate is off)
+__global__ void k_part_local(const int* gate, const double* bm, int nb, const double* bmv, int nbv, double* out) {
+    if (!*gate) {
+        if (threadIdx.x == 0) *out = 0.0;
+        return;
+    }
+    const double s = block_reduce_max(bm, nb, bmv, nbv);
+    if (threadIdx.x == 0) *out = s;
+}
+// stage 1 of a step with the all-reduced speed: dt as k_stage1_dt
+__global__ void k_part_dt(Ctl* c, const double* s) {
+    if (!c->active) return;
+    c->s_stage[0] = s[0];
+    double dt = c->cfl * c->L / (s[0] + kDtEps);
+    dt = vmin(dt, c->t_end - c->t);
+    if (c->dt_max > 0.0) dt = vmin(dt, c->dt_max);
+    c->dt = dt;
+}
+__global__ void k_part_stages(Ctl* c, const double* s, int from, int n) {
+    if (!c->active) return;
+    for (int k = 0; k < n; ++k) c->s_stage[from + k] = s[k];
+}
+__global__ void k_part_seed(Ctl* c, const double* s) {
+    if (c->seed) c->s_lag = s[0];
+}
+__global__ void k_part_hancock_end(Ctl* c, const double* s) {
+    if (!c->active) return;
+    c->s_lag = s[0];
+    finish_step(c, s[0]);
+}
+// the part's `depth` first and last planes of every variable into the send buffers ([nvar][depth * area] each), or the
+// receive buffers into the ghost planes before and after (an interface side only)
+__global__ void k_part_pack(const double* U, long long plane, long long area, int depth, int count, int nvar, double* lo, double* hi, int do_lo,
+                            int do_hi) {
+    const long long n = (long long)depth * area, total = n * nvar;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total; x += (long long)gridDim.x * blockDim.x) {
+        const long long q = x / n, r = x - q * n;
+        if (do_lo) lo[x] = U[q * plane + r];
+        if (do_hi) hi[x] = U[q * plane + (long long)(count - depth) * area + r];
+    }
+}
+__global__ void k_part_unpack(double* U, long long plane, long long area, int depth, int count, int nvar, const double* lo, const double* hi, int do_lo,
+                              int do_hi) {
+    const long long n = (long long)depth * area, total = n * nvar;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total; x += (long long)gridDim.x * blockDim.x) {
+        const long long q = x / n, r = x - q * n;
+        if (do_lo) U[q * plane - n + r] = lo[x];
+        if (do_hi) U[q * plane + (long long)count * area + r] = hi[x];
+    }
+}
+
 // out = a + dt b over the state planes (TimeScheme.cpp:27-59: axpy)
 __global__ void k_axpy(const Ctl* c, double* out, const double* a, const double* b, long long plane, long long n, int nvar) {
     if (!c->active) return;
@@ -312,6 +364,15 @@ struct fvg_run {
     unsigned char* sens_flags[2] = {nullptr, nullptr};
     unsigned char* sens_tiles = nullptr;   // per axis and stage tile
     unsigned long long* sens_count = nullptr;
+    // one part of a slab-decomposed mesh (fvg_create_part): the split axis (z in 3-D, y in 2-D), the part's first plane
+    // and plane count, the ghost depth, which sides are interfaces with a neighbouring part, the offset of the first
+    // interior plane in the state arrays (U, Ut, R, Rv point there), the exchange buffers (send lo / hi, recv lo / hi:
+    // depth x plane cells x nvar each) and the all-reduce slots
+    bool is_part = false;
+    int nparts = 1, part = 0, split = 2, first = 0, count = 0, depth = 0, peer[2] = {0, 0};
+    long long goff = 0, area = 0, xcount = 0;
+    double* xbuf = nullptr;
+    double* xred = nullptr;
     double* Ucur() { return cur ? Ut : U; }
 };
 
@@ -423,7 +484,11 @@ ViscArgs visc_args(fvg_run* r, const double* Uin, double* bmv, const int* gate) 
     a.u_in = r->cfg.u_in;
     a.v_in = r->cfg.v_in;
     a.bface2 = r->cfg.boundary_order == 2 && r->cfg.reconstruction != FVG_RECON_NONE;   // Params.cpp:470: first order keeps order 1
-    for (int d = 0; d < 3; ++d) a.periodic[d] = r->cfg.bc[2 * d] == FVG_BC_PERIODIC && r->cfg.bc[2 * d + 1] == FVG_BC_PERIODIC;
+    for (int d = 0; d < 3; ++d) {   // (a split periodic axis is not wrapped in a part: its ends are interfaces)
+        const bool split = r->is_part && d == r->split;
+        a.periodic[d] = r->cfg.bc[2 * d] == FVG_BC_PERIODIC && r->cfg.bc[2 * d + 1] == FVG_BC_PERIODIC && !(split && (r->peer[0] || r->peer[1]));
+        for (int h = 0; h < 2; ++h) a.through[2 * d + h] = a.periodic[d] || r->bc.halo[2 * d + h] == kHaloPeer;
+    }
     a.U = Uin;
     a.Rv = r->Rv;
     a.blockmax = bmv;
@@ -606,6 +671,146 @@ cudaError_t enqueue_step(fvg_run* r, bool refresh = true) {
     return cudaGetLastError();
 }
 
+// ---- parts of a slab-decomposed mesh: a step in phases separated by the hosts' communication
+int xblocks(const fvg_run* r) {
+    const long long b = (r->xcount + 255) / 256;
+    return (int)(b < 148 * 8 ? (b > 0 ? b : 1) : 148 * 8);
+}
+cudaError_t part_pack(fvg_run* r, const double* U) {
+    k_part_pack<<<xblocks(r), 256, 0, r->stream>>>(U, r->m.plane, r->area, r->depth, r->count, r->nvar, r->xbuf, r->xbuf + r->xcount, r->peer[0],
+                                                  r->peer[1]);
+    return cudaGetLastError();
+}
+cudaError_t part_unpack(fvg_run* r, double* U) {
+    k_part_unpack<<<xblocks(r), 256, 0, r->stream>>>(U, r->m.plane, r->area, r->depth, r->count, r->nvar, r->xbuf + 2 * r->xcount,
+                                                    r->xbuf + 3 * r->xcount, r->peer[0], r->peer[1]);
+    return cudaGetLastError();
+}
+cudaError_t part_local(fvg_run* r, const int* gate, const double* bm, int nb, const double* bmv, int nbv, int slot) {
+    k_part_local<<<1, 1024, 0, r->stream>>>(gate, bm, nb, bmv, nbv, r->xred + slot);
+    return cudaGetLastError();
+}
+
+// Phase `phase` of a step of a part (the launches of enqueue_step, cut where a stage needs its neighbours' planes or
+// the speed of every part). *comm: 0 the step is complete; 1 the hosts exchange the send / receive buffers (each part's
+// send_lo to its low neighbour's recv_hi, send_hi to its high neighbour's recv_lo); 2 they all-reduce (MAX) the first
+// *nred doubles of the reduce buffer; -1 no such phase.
+cudaError_t part_phase(fvg_run* r, int phase, int* comm, int* nred) {
+    Ctl* c = r->ctl;
+    const int* act = &c->active;
+    const int nbv = r->cfg.use_viscous ? r->nbv : 0;
+    const int ts = r->cfg.time_scheme;
+    cudaStream_t s = r->stream;
+    cudaError_t e = cudaSuccess;
+    *comm = -1;
+    *nred = 0;
+    if (ts == FVG_TS_HANCOCK) {
+        double* Uin = r->Ucur();
+        double* Uout = r->cur ? r->U : r->Ut;
+        switch (phase) {
+        case 0:   // the state's boundary planes
+            e = part_pack(r, Uin);
+            *comm = 1;
+            break;
+        case 1:   // the seed residual (first step only) and its speed
+            if ((e = part_unpack(r, Uin))) break;
+            k_hancock_begin<<<1, 1, 0, s>>>(c);
+            if (r->cfg.use_viscous && (e = launch_visc(r, Uin, r->bmv[1], &c->seed, false))) break;
+            if ((e = r->stage.launch(stage_args(r, Uin, nullptr, r->R, kStoreR, 0, 0, r->cfg.use_viscous ? r->Rv : nullptr, r->bm_seed, &c->seed), r->nb,
+                                     s)))
+                break;
+            e = part_local(r, &c->seed, r->bm_seed, r->nb, r->bmv[1], nbv, 0);
+            *comm = 2;
+            *nred = 1;
+            break;
+        case 2:   // dt from the lagged speed, the predictor and update, the speed
+            k_part_seed<<<1, 1, 0, s>>>(c, r->xred);
+            k_hancock_dt<<<1, 1, 0, s>>>(c);
+            if (r->cfg.use_viscous && (e = launch_visc(r, Uin, r->bmv[0], act))) break;
+            timer_mark(r, r->t_stage);
+            e = launch_hancock(r, hancock_args(r, Uin, Uout, kAxpy, r->bm[0], act));
+            timer_mark(r, r->t_stage);
+            if (e) break;
+            e = part_local(r, act, r->bm[0], r->nbh, r->bmv[0], nbv, 0);
+            *comm = 2;
+            *nred = 1;
+            break;
+        case 3:
+            k_part_hancock_end<<<1, 1, 0, s>>>(c, r->xred);
+            r->cur ^= 1;
+            e = cudaGetLastError();
+            *comm = 0;
+            break;
+        default: break;
+        }
+        return e;
+    }
+    switch (phase) {
+    case 0:
+        e = part_pack(r, r->U);
+        *comm = 1;
+        break;
+    case 1:   // stage 1 and its speed
+        if ((e = part_unpack(r, r->U))) break;
+        if ((e = residual_stage(r, r->U, nullptr, r->R, kStoreR, 0, 0, 0, act))) break;
+        e = part_local(r, act, r->bm[0], r->nb, r->bmv[0], nbv, 0);
+        *comm = 2;
+        *nred = 1;
+        break;
+    case 2:   // dt; Euler: the update and the end; else the first stage state and its planes
+        k_part_dt<<<1, 1, 0, s>>>(c, r->xred);
+        if (ts == FVG_TS_EULER) {
+            k_axpy<<<axpy_blocks(r), 256, 0, s>>>(c, r->U, r->U, r->R, r->m.plane, r->m.ncells, r->nvar);
+            k_end_rk<<<1, 1, 0, s>>>(c, 1);
+            e = cudaGetLastError();
+            *comm = 0;
+            break;
+        }
+        k_axpy<<<axpy_blocks(r), 256, 0, s>>>(c, r->Ut, r->U, r->R, r->m.plane, r->m.ncells, r->nvar);
+        if ((e = cudaGetLastError())) break;
+        e = part_pack(r, r->Ut);
+        *comm = 1;
+        break;
+    case 3:   // stage 2
+        if ((e = part_unpack(r, r->Ut))) break;
+        if (ts == FVG_TS_SSPRK2) {
+            if ((e = residual_stage(r, r->Ut, r->U, r->U, kCombine, 0.5, 0.5, 1, act))) break;
+            e = part_local(r, act, r->bm[1], r->nb, r->bmv[1], nbv, 0);
+            *comm = 2;
+            *nred = 1;
+            break;
+        }
+        if ((e = residual_stage(r, r->Ut, r->U, r->R, kCombine, 0.75, 0.25, 1, act))) break;
+        if ((e = part_local(r, act, r->bm[1], r->nb, r->bmv[1], nbv, 0))) break;
+        e = part_pack(r, r->R);
+        *comm = 1;
+        break;
+    case 4:
+        if (ts == FVG_TS_SSPRK2) {
+            k_part_stages<<<1, 1, 0, s>>>(c, r->xred, 1, 1);
+            k_end_rk<<<1, 1, 0, s>>>(c, 2);
+            e = cudaGetLastError();
+            *comm = 0;
+            break;
+        }
+        if ((e = part_unpack(r, r->R))) break;   // stage 3
+        if ((e = residual_stage(r, r->R, r->U, r->U, kCombine, 1.0 / 3.0, 2.0 / 3.0, 2, act))) break;
+        e = part_local(r, act, r->bm[2], r->nb, r->bmv[2], nbv, 1);
+        *comm = 2;
+        *nred = 2;
+        break;
+    case 5:
+        if (ts != FVG_TS_SSPRK3) break;
+        k_part_stages<<<1, 1, 0, s>>>(c, r->xred, 1, 2);
+        k_end_rk<<<1, 1, 0, s>>>(c, 3);
+        e = cudaGetLastError();
+        *comm = 0;
+        break;
+    default: break;
+    }
+    return e;
+}
+
 int read_ctl(fvg_run* run, Ctl* h) {
     CK(cudaMemcpyAsync(h, run->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, run->stream));
     CK(cudaStreamSynchronize(run->stream));
@@ -632,6 +837,10 @@ bool fvg::run_view(fvg_run* run, RunView* v) {
     return true;
 }
 
+namespace {
+int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_run** out);
+}
+
 // ------------------------------------------------------------------------------------------------ C ABI
 extern "C" {
 
@@ -639,7 +848,25 @@ int fvg_abi_version(void) { return FVG_ABI_VERSION; }
 const char* fvg_create_error(void) { return g_create_error.c_str(); }
 const char* fvg_last_error(const fvg_run* run) { return run ? run->err.c_str() : "null run"; }
 
-int fvg_create(const fvg_config* cfg, fvg_run** out) {
+int fvg_create(const fvg_config* cfg, fvg_run** out) { return create_run(cfg, 1, 0, false, out); }
+
+int fvg_create_part(const fvg_config* cfg, int nparts, int part, fvg_run** out) {
+    if (nparts < 1 || part < 0 || part >= nparts) {
+        g_create_error = "part must be in 0 .. nparts - 1";
+        return FVG_ERR_ARGUMENT;
+    }
+    return create_run(cfg, nparts, part, true, out);
+}
+
+}   // extern "C"
+
+namespace {
+
+// fvg_create, and part `part` of `nparts` slabs of the mesh along its slowest axis (nparts = 1 with part mode off: a
+// whole run). A part holds planes first .. first + count - 1 of the split axis (the first nsplit % nparts parts one
+// plane more), with `depth` ghost planes on each side; the mesh spacing, the step length and every other parameter are
+// the whole mesh's.
+int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_run** out) {
     if (!cfg || !out) {
         g_create_error = "null argument";
         return FVG_ERR_ARGUMENT;
@@ -650,8 +877,43 @@ int fvg_create(const fvg_config* cfg, fvg_run** out) {
         g_create_error = v;
         return FVG_ERR_CONFIG;
     }
+    const bool is_part = as_part;
+    const int split = cfg->nz > 1 ? 2 : 1;
+    const int nsplit = split == 2 ? cfg->nz : cfg->ny;
+    const int depth = cfg->reconstruction == FVG_RECON_WENO5 ? 3 : 2;
+    const int count = nsplit / nparts + (part < nsplit % nparts ? 1 : 0);
+    const int first = part * (nsplit / nparts) + (part < nsplit % nparts ? part : nsplit % nparts);
+    if (is_part) {
+        if (cfg->use_ibm) {
+            g_create_error = "a part of a decomposed mesh cannot hold an immersed body";
+            return FVG_ERR_CONFIG;
+        }
+        if (count < depth) {
+            g_create_error = "each part needs at least " + std::to_string(depth) + " planes along the split axis";
+            return FVG_ERR_CONFIG;
+        }
+        // a first-order run takes the states of a periodic side's faces through the round trip (a side without a halo);
+        // split there, those faces would be a part interface
+        if (cfg->reconstruction == FVG_RECON_NONE && cfg->bc[2 * split] == FVG_BC_PERIODIC) {
+            g_create_error = "a first-order run cannot be split along a periodic axis";
+            return FVG_ERR_CONFIG;
+        }
+    }
     auto* run = new fvg_run();
     run->cfg = *cfg;
+    if (is_part) {
+        const bool periodic = cfg->bc[2 * split] == FVG_BC_PERIODIC && cfg->bc[2 * split + 1] == FVG_BC_PERIODIC;
+        run->is_part = true;
+        run->nparts = nparts;
+        run->part = part;
+        run->split = split;
+        run->first = first;
+        run->count = count;
+        run->depth = depth;
+        run->peer[0] = part > 0 || periodic;
+        run->peer[1] = part < nparts - 1 || periodic;
+        (split == 2 ? run->cfg.nz : run->cfg.ny) = count;   // the local mesh; the spacing below is the whole mesh's
+    }
     const fvg_config& c = run->cfg;
     auto bail = [&](int code) {
         g_create_error = run->err;
@@ -670,27 +932,41 @@ int fvg_create(const fvg_config* cfg, fvg_run** out) {
     m.nz = c.nz;
     m.ncells = (long long)c.nx * c.ny * c.nz;
     m.plane = (m.ncells + 31) / 32 * 32;
-    m.dx = c.Lx / c.nx;   // generate_cartesian_mesh_3d (Core.cpp:20-40)
-    m.dy = c.Ly / c.ny;
-    m.dz = c.Lz / c.nz;
+    if (run->is_part) {   // ghost planes before and after the part's own along the split axis
+        run->area = split == 2 ? (long long)c.nx * c.ny : (long long)c.nx;
+        run->goff = (long long)depth * run->area;
+        m.plane = ((long long)(count + 2 * depth) * run->area + 31) / 32 * 32;
+        run->xcount = (long long)depth * run->area * (run->dim == 3 ? 5 : 4);
+    }
+    const fvg_config& g = *cfg;   // the whole mesh
+    m.dx = g.Lx / g.nx;   // generate_cartesian_mesh_3d (Core.cpp:20-40)
+    m.dy = g.Ly / g.ny;
+    m.dz = g.Lz / g.nz;
     if (run->dim == 3) {
         m.area[0] = m.dy * m.dz;
         m.area[1] = m.dx * m.dz;
         m.area[2] = m.dx * m.dy;
         m.inv_cell = 1.0 / (m.dx * m.dy * m.dz);
-        run->L = 2.0 / (1.0 / (c.Lx / c.nx) + 1.0 / (c.Ly / c.ny) + 1.0 / (c.Lz / c.nz));
+        run->L = 2.0 / (1.0 / (g.Lx / g.nx) + 1.0 / (g.Ly / g.ny) + 1.0 / (g.Lz / g.nz));
     } else {
         m.area[0] = m.dy;
         m.area[1] = m.dx;
         m.area[2] = 0.0;
         m.inv_cell = 1.0 / (m.dx * m.dy);
-        run->L = vmin(c.Lx / c.nx, c.Ly / c.ny);
+        run->L = vmin(g.Lx / g.nx, g.Ly / g.ny);
     }
     run->eos.type = c.eos_type;
     run->eos.gamma = c.gamma;
     run->eos.p_inf = c.p_inf;
     for (int s = 0; s < 6; ++s) run->bc.type[s] = c.bc[s];
     halo_kinds(c, c.reconstruction == FVG_RECON_WENO5 ? 3 : 2, run->bc.halo);
+    for (int h = 0; h < 2; ++h)
+        if (run->is_part && run->peer[h]) {   // an interface: the neighbour's cells, no boundary rule
+            const int side = 2 * split + h;
+            run->bc.halo[side] = kHaloPeer;
+            run->bc.type[side] = kBcPeriodic;
+            run->bc.ext[side] = depth;
+        }
     run->bc.u_in = c.u_in;
     run->bc.v_in = c.v_in;
     run->bc.p_out = c.p_out;
@@ -731,10 +1007,15 @@ int fvg_create(const fvg_config* cfg, fvg_run** out) {
     if (cudaStreamCreateWithFlags(&run->stream, cudaStreamNonBlocking) != cudaSuccess || cudaMalloc(&run->U, sbytes) != cudaSuccess ||
         cudaMalloc(&run->Ut, sbytes) != cudaSuccess || cudaMalloc(&run->R, sbytes) != cudaSuccess ||
         (c.use_viscous && cudaMalloc(&run->Rv, sbytes) != cudaSuccess) || cudaMalloc(&run->ctl, sizeof(Ctl)) != cudaSuccess ||
-        cudaMalloc(&run->bm_seed, sizeof(double) * run->nb) != cudaSuccess) {
+        cudaMalloc(&run->bm_seed, sizeof(double) * run->nb) != cudaSuccess ||
+        (run->is_part && (cudaMalloc(&run->xbuf, sizeof(double) * 4 * run->xcount) != cudaSuccess || cudaMalloc(&run->xred, sizeof(double) * 2) != cudaSuccess))) {
         run->err = "device allocation failed";
         return bail(FVG_ERR_CUDA);
     }
+    // the state arrays start with the ghost planes: U, Ut, R, Rv point at the first interior plane
+    for (double** p : {&run->U, &run->Ut, &run->R, &run->Rv})
+        if (*p) cudaMemsetAsync(*p, 0, sbytes, run->stream), *p += run->goff;
+    if (run->xred) cudaMemsetAsync(run->xred, 0, sizeof(double) * 2, run->stream);
     const int nbmax = run->nb > run->nbh ? run->nb : run->nbh;
     for (int s = 0; s < 3; ++s)
         if (cudaMalloc(&run->bm[s], sizeof(double) * nbmax) != cudaSuccess || cudaMalloc(&run->bmv[s], sizeof(double) * run->nbv) != cudaSuccess) {
@@ -792,8 +1073,6 @@ int fvg_create(const fvg_config* cfg, fvg_run** out) {
         run->bc.slot = run->d_slot;
         run->bc.forced = run->d_forced;
     }
-    cudaMemsetAsync(run->U, 0, sbytes, run->stream);
-    cudaMemsetAsync(run->Ut, 0, sbytes, run->stream);
     Ctl h{};
     h.cfl = c.cfl;
     h.L = run->L;
@@ -809,6 +1088,10 @@ int fvg_create(const fvg_config* cfg, fvg_run** out) {
     return FVG_OK;
 }
 
+}   // namespace
+
+extern "C" {
+
 int fvg_destroy(fvg_run* run) {
     if (!run) return FVG_OK;
     cudaSetDevice(run->cfg.device);
@@ -817,7 +1100,9 @@ int fvg_destroy(fvg_run* run) {
     for (cudaEvent_t e : run->t_visc.ev) cudaEventDestroy(e);
     for (int g = 0; g < 2; ++g)
         if (run->graph[g]) cudaGraphExecDestroy(run->graph[g]);
-    for (double* p : {run->U, run->Ut, run->R, run->Rv, run->staging, run->bm_seed, run->bm[0], run->bm[1], run->bm[2], run->bmv[0], run->bmv[1], run->bmv[2]})
+    for (double* p : {run->U, run->Ut, run->R, run->Rv})   // the arrays start goff doubles before the first interior plane
+        if (p) cudaFree(p - run->goff);
+    for (double* p : {run->staging, run->bm_seed, run->bm[0], run->bm[1], run->bm[2], run->bmv[0], run->bmv[1], run->bmv[2], run->xbuf, run->xred})
         if (p) cudaFree(p);
     if (run->ctl) cudaFree(run->ctl);
     if (run->sens) cudaFree(run->sens);
@@ -873,6 +1158,7 @@ int fvg_download_state(fvg_run* run, double* U, size_t ncells) {
 
 int fvg_residual(fvg_run* run, double predictor_half_dt, double* R, size_t ncells, double* smax) {
     if (!run) return FVG_ERR_ARGUMENT;
+    if (run->is_part) return fail(run, FVG_ERR_CONFIG, "a part of a decomposed mesh steps through fvg_part_phase");
     if (R && (long long)ncells != run->m.ncells) return fail(run, FVG_ERR_ARGUMENT, "ncells is not the mesh's");
     CK(cudaSetDevice(run->cfg.device));
     Ctl* c = run->ctl;
@@ -984,6 +1270,7 @@ static int run_steps(fvg_run* run, double t_end, int max_steps, int use_graph, i
 
 int fvg_step(fvg_run* run, double t_end, double* dt, double* smax) {
     if (!run) return FVG_ERR_ARGUMENT;
+    if (run->is_part) return fail(run, FVG_ERR_CONFIG, "a part of a decomposed mesh steps through fvg_part_phase");
     int n = 0;
     const int rc = run_steps(run, t_end, 1, 0, &n);
     if (rc) return rc;
@@ -997,7 +1284,68 @@ int fvg_step(fvg_run* run, double t_end, double* dt, double* smax) {
 
 int fvg_run_until(fvg_run* run, double t_end, int max_steps, int* steps) {
     if (!run) return FVG_ERR_ARGUMENT;
+    if (run->is_part) return fail(run, FVG_ERR_CONFIG, "a part of a decomposed mesh steps through fvg_part_phase");
     return run_steps(run, t_end, max_steps, 1, steps);
+}
+
+int fvg_part_info(const fvg_run* run, int* axis, int* first, int* count, int* depth, int* peer_lo, int* peer_hi) {
+    if (!run || !run->is_part) return FVG_ERR_ARGUMENT;
+    if (axis) *axis = run->split;
+    if (first) *first = run->first;
+    if (count) *count = run->count;
+    if (depth) *depth = run->depth;
+    if (peer_lo) *peer_lo = run->peer[0];
+    if (peer_hi) *peer_hi = run->peer[1];
+    return FVG_OK;
+}
+
+int fvg_part_buffers(fvg_run* run, double** send_lo, double** send_hi, double** recv_lo, double** recv_hi, long long* count, double** reduce) {
+    if (!run || !run->is_part) return FVG_ERR_ARGUMENT;
+    if (send_lo) *send_lo = run->xbuf;
+    if (send_hi) *send_hi = run->xbuf + run->xcount;
+    if (recv_lo) *recv_lo = run->xbuf + 2 * run->xcount;
+    if (recv_hi) *recv_hi = run->xbuf + 3 * run->xcount;
+    if (count) *count = run->xcount;
+    if (reduce) *reduce = run->xred;
+    return FVG_OK;
+}
+
+int fvg_part_begin(fvg_run* run, double t_end, int max_steps) {
+    if (!run) return FVG_ERR_ARGUMENT;
+    if (!run->is_part) return fail(run, FVG_ERR_CONFIG, "not a part of a decomposed mesh");
+    CK(cudaSetDevice(run->cfg.device));
+    k_begin<<<1, 1, 0, run->stream>>>(run->ctl, t_end, max_steps);
+    CK(cudaGetLastError());
+    return FVG_OK;
+}
+
+int fvg_part_phase(fvg_run* run, int phase, int* comm, int* nreduce) {
+    if (!run || !comm || !nreduce) return FVG_ERR_ARGUMENT;
+    if (!run->is_part) return fail(run, FVG_ERR_CONFIG, "not a part of a decomposed mesh");
+    CK(cudaSetDevice(run->cfg.device));
+    const cudaError_t e = part_phase(run, phase, comm, nreduce);
+    if (e != cudaSuccess) return fail(run, FVG_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    if (*comm < 0) return fail(run, FVG_ERR_ARGUMENT, "no such phase of this time scheme");
+    return FVG_OK;
+}
+
+int fvg_part_status(fvg_run* run, int* active, int* steps, double* t, double* dt, double* smax) {
+    if (!run) return FVG_ERR_ARGUMENT;
+    CK(cudaSetDevice(run->cfg.device));
+    Ctl h;
+    const int rc = read_ctl(run, &h);
+    if (rc) return rc;
+    if (active) *active = h.active;
+    if (steps) *steps = h.steps;
+    if (t) *t = h.t;
+    if (dt) *dt = h.dt;
+    if (smax) *smax = h.s_step;
+    if (h.status) {
+        char msg[256];
+        std::snprintf(msg, sizeof msg, "the solution diverged at step %d (t = %.6g, dt = %.3g, largest wave speed = %.3g)", h.steps + 1, h.t, h.dt, h.s_step);
+        return fail(run, FVG_ERR_DIVERGED, msg);
+    }
+    return FVG_OK;
 }
 
 int fvg_get_time(const fvg_run* run, double* t) {
@@ -1079,6 +1427,7 @@ int fvg_get_timing(const fvg_run* run, double* stage_ms, long long* stage_launch
 
 int fvg_set_sensor(fvg_run* run, const void* weights, float threshold, int every, int radius) {
     if (!run) return FVG_ERR_ARGUMENT;
+    if (run->is_part) return fail(run, FVG_ERR_CONFIG, "the sensor's gate is not exchanged between parts of a decomposed mesh");
     CK(cudaSetDevice(run->cfg.device));
     CK(cudaStreamSynchronize(run->stream));
     for (int g = 0; g < 2; ++g)

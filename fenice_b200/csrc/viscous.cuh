@@ -28,6 +28,7 @@ struct ViscArgs {
     double u_in, v_in;
     int bface2;        // boundary_order == 2
     int periodic[3];   // both sides of the axis periodic
+    int through[6];    // the side is periodic or a part interface (kHaloPeer): no wall rules at its faces
     int nvar;          // state planes: 4 on a 2-D mesh (rho w is +0 there), 5 in 3-D
     const double* U;
     double* Rv;
@@ -96,7 +97,7 @@ __device__ __forceinline__ St<double, 5> padded_cons(const ViscArgs& a, int i, i
     int ng = 0, ga[2] = {-1, -1};
 #pragma unroll
     for (int d = 0; d < 3; ++d)
-        if (p[d] < 0 || p[d] >= n3[d]) {
+        if (!held(a.bc, d, p[d], n3[d])) {
             if (ng < 2) ga[ng] = d;
             ++ng;
         }
@@ -115,8 +116,18 @@ __device__ __forceinline__ St<double, 5> padded_cons(const ViscArgs& a, int i, i
         return viscous_ghost_3d(a, side, face_ghost(a, e, q[0], q[1], q[2]));
     }
 #pragma unroll
-    for (int d = 0; d < 3; ++d) p[d] = p[d] < 0 ? 0 : (p[d] >= n3[d] ? n3[d] - 1 : p[d]);
+    for (int d = 0; d < 3; ++d) {
+        const int lo = -a.bc.ext[2 * d], hi = n3[d] - 1 + a.bc.ext[2 * d + 1];
+        p[d] = p[d] < lo ? lo : (p[d] > hi ? hi : p[d]);
+    }
     return cell_at(a, p[0], p[1], p[2]);
+}
+
+// The range of positions a viscous box loads along an axis: one ghost layer beyond a side, or the neighbouring part's
+// ghost planes beyond a part interface.
+__device__ __forceinline__ int box_clamp(const ViscArgs& a, int d, int g, int n) {
+    const int lo = a.bc.ext[2 * d] > 0 ? -a.bc.ext[2 * d] : -1, hi = a.bc.ext[2 * d + 1] > 0 ? n - 1 + a.bc.ext[2 * d + 1] : n;
+    return g < lo ? lo : (g > hi ? hi : g);
 }
 
 // velocity component a (0, 1, 2) of a primitive state, without indexing the state by a run-time value
@@ -174,7 +185,7 @@ __global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
             if (a.periodic[x] && (g[x] < 0 || g[x] >= n3[x])) g[x] = ((g[x] % n3[x]) + n3[x]) % n3[x];
         // a tile that overhangs the mesh: positions past the ghost layer are clamped onto it (their results are not used)
 #pragma unroll
-        for (int x = 0; x < 3; ++x) g[x] = g[x] < -1 ? -1 : (g[x] > n3[x] ? n3[x] : g[x]);
+        for (int x = 0; x < 3; ++x) g[x] = box_clamp(a, x, g[x], n3[x]);
         const St<double, 5> u = padded_cons(a, g[0], g[1], g[2]);
 #pragma unroll
         for (int q = 0; q < 5; ++q) B[q * NB + e] = u[q];
@@ -227,9 +238,10 @@ __global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
                 const double vL[3] = {wL[1], wL[2], wL[4]}, vR[3] = {wR[1], wR[2], wR[4]};
                 const double TL = wL[3] / wL[0], TR = wR[3] / wR[0];
                 // cross terms: the cells on either side; at a side that is not periodic the cell next to it (both slots)
-                const int xL = (lo && !a.periodic[d]) ? eR : eL;
-                const int xR = (hi && !a.periodic[d]) ? eL : eR;
-                const bool phys = a.bface2 && !a.periodic[d] && (lo || hi);
+                const bool lo_wall = lo && !a.through[2 * d], hi_wall = hi && !a.through[2 * d + 1];
+                const int xL = lo_wall ? eR : eL;
+                const int xR = hi_wall ? eL : eR;
+                const bool phys = a.bface2 && (lo_wall || hi_wall);
                 double Gc[4];
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {
@@ -369,8 +381,8 @@ __global__ void __launch_bounds__(NT) viscous2d_kernel(const ViscArgs a) {
         int g[2] = {ox + e % BX - 2, oy + e / BX - 2};
         if (px && (g[0] < 0 || g[0] >= nx)) g[0] = ((g[0] % nx) + nx) % nx;
         if (py && (g[1] < 0 || g[1] >= ny)) g[1] = ((g[1] % ny) + ny) % ny;
-        g[0] = g[0] < -1 ? -1 : (g[0] > nx ? nx : g[0]);
-        g[1] = g[1] < -1 ? -1 : (g[1] > ny ? ny : g[1]);
+        g[0] = box_clamp(a, 0, g[0], nx);
+        g[1] = box_clamp(a, 1, g[1], ny);
         const St<double, 5> u = padded_cons(a, g[0], g[1], 0);
 #pragma unroll
         for (int s = 0; s < 4; ++s) B[s * NB + e] = u[s];
@@ -413,10 +425,11 @@ __global__ void __launch_bounds__(NT) viscous2d_kernel(const ViscArgs a) {
             const double du_dx = (uR - uL) / dx, dv_dx = (vR - vL) / dx, dT_dx = (TR - TL) / dx;
             // the cells whose tangential derivatives the face averages: the two neighbours; at a side that is not
             // periodic, the boundary cell twice
-            const int xl = (lo && !px) ? il : il - 1, xr = (hi && !px) ? il - 1 : il;
+            const bool lo_wall = lo && !a.through[0], hi_wall = hi && !a.through[1];
+            const int xl = lo_wall ? il : il - 1, xr = hi_wall ? il - 1 : il;
             double du_dy = 0.5 * (q(4, xl, jl) + q(4, xr, jl));
             double dv_dy = 0.5 * (q(6, xl, jl) + q(6, xr, jl));
-            if (a.bface2 && (lo || hi) && !px) {
+            if (a.bface2 && (lo_wall || hi_wall)) {
                 const int ig = lo ? il - 1 : il, ic = lo ? il : il - 1;   // the frame column and the boundary cell's column
                 const double fu_p = 0.5 * (q(0, ig, jl + 1) + q(0, ic, jl + 1)), fu_m = 0.5 * (q(0, ig, jl - 1) + q(0, ic, jl - 1));
                 const double fv_p = 0.5 * (q(1, ig, jl + 1) + q(1, ic, jl + 1)), fv_m = 0.5 * (q(1, ig, jl - 1) + q(1, ic, jl - 1));
@@ -445,10 +458,11 @@ __global__ void __launch_bounds__(NT) viscous2d_kernel(const ViscArgs a) {
             const double TB = q(2, il, jl - 1), TT = q(2, il, jl);
             const double u_f = 0.5 * (uB + uT), v_f = 0.5 * (vB + vT);
             const double dv_dy = (vT - vB) / dy, du_dy = (uT - uB) / dy, dT_dy = (TT - TB) / dy;
-            const int yb = (lo && !py) ? jl : jl - 1, yt = (hi && !py) ? jl - 1 : jl;
+            const bool lo_wall = lo && !a.through[2], hi_wall = hi && !a.through[3];
+            const int yb = lo_wall ? jl : jl - 1, yt = hi_wall ? jl - 1 : jl;
             double du_dx = 0.5 * (q(3, il, yb) + q(3, il, yt));
             double dv_dx = 0.5 * (q(5, il, yb) + q(5, il, yt));
-            if (a.bface2 && (lo || hi) && !py) {
+            if (a.bface2 && (lo_wall || hi_wall)) {
                 const int jg = lo ? jl - 1 : jl, jc = lo ? jl : jl - 1;   // the frame row and the boundary cell's row
                 const double fu_p = 0.5 * (q(0, il + 1, jg) + q(0, il + 1, jc)), fu_m = 0.5 * (q(0, il - 1, jg) + q(0, il - 1, jc));
                 const double fv_p = 0.5 * (q(1, il + 1, jg) + q(1, il + 1, jc)), fv_m = 0.5 * (q(1, il - 1, jg) + q(1, il - 1, jc));

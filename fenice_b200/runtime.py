@@ -34,7 +34,8 @@ EXPORTS = ["fvg_abi_version", "fvg_create", "fvg_destroy", "fvg_last_error", "fv
            "fvg_batch_download", "fvg_batch_run", "fvg_batch_problem", "fvg_batch_autotune", "fvg_batch_set_schedule",
            "fvg_batch_get_schedule", "fvg_batch_stream", "fvg_batch_set_timing", "fvg_batch_get_timing",
            "fvg_sensor_sizes", "fvg_sensor_extract", "fvg_sensor_grad", "fvg_sensor_adam", "fvg_sensor_pack", "fvg_sensor_infer",
-           "fvg_set_sensor", "fvg_get_sensor_counts", "fvg_ibm_loads"]
+           "fvg_set_sensor", "fvg_get_sensor_counts", "fvg_ibm_loads",
+           "fvg_create_part", "fvg_part_info", "fvg_part_buffers", "fvg_part_begin", "fvg_part_phase", "fvg_part_status"]
 
 _lib = None
 ABI_VERSION = 2   # FVG_ABI_VERSION of include/fenice_gpu.h
@@ -101,6 +102,14 @@ def load_library(path=LIB_PATH):
     lib.fvg_set_sensor.argtypes = [c_p, c_p, ctypes.c_float, ctypes.c_int, ctypes.c_int]
     lib.fvg_get_sensor_counts.argtypes = [c_p, ll, ll, ctypes.c_int]
     lib.fvg_ibm_loads.argtypes = [c_p, dp]
+    ip = ctypes.POINTER(ctypes.c_int)
+    dpp = ctypes.POINTER(dp)
+    lib.fvg_create_part.argtypes = [ctypes.POINTER(P.FvgConfig), ctypes.c_int, ctypes.c_int, ctypes.POINTER(c_p)]
+    lib.fvg_part_info.argtypes = [c_p, ip, ip, ip, ip, ip, ip]
+    lib.fvg_part_buffers.argtypes = [c_p, dpp, dpp, dpp, dpp, ll, dpp]
+    lib.fvg_part_begin.argtypes = [c_p, ctypes.c_double, ctypes.c_int]
+    lib.fvg_part_phase.argtypes = [c_p, ctypes.c_int, ip, ip]
+    lib.fvg_part_status.argtypes = [c_p, ip, ip, dp, dp, dp]
     _lib = lib
     return lib
 
@@ -112,18 +121,29 @@ def _dp(a):
 class Run:
     """A run of the finite-volume path on one GPU."""
 
-    def __init__(self, params, U=None, precision=0, device=0):
+    def __init__(self, params, U=None, precision=0, device=0, part=None):
+        """part = (nparts, index): one part of the slab decomposition of the mesh (fvg_create_part; see
+        fenice_b200.slabs), whose state is its own planes."""
         self.lib = load_library()
         self.params = P.resolve(params)
         self.cfg = P.to_config(self.params, precision=precision, device=device)
         h = ctypes.c_void_p()
-        rc = self.lib.fvg_create(ctypes.byref(self.cfg), ctypes.byref(h))
+        if part is None:
+            rc = self.lib.fvg_create(ctypes.byref(self.cfg), ctypes.byref(h))
+        else:
+            rc = self.lib.fvg_create_part(ctypes.byref(self.cfg), int(part[0]), int(part[1]), ctypes.byref(h))
         if rc != FVG_OK:
             msg = self.lib.fvg_create_error().decode()
-            raise (ValueError if rc == FVG_ERR_CONFIG else RuntimeError)(f"fvg_create: {msg}")
+            raise (ValueError if rc in (FVG_ERR_CONFIG, FVG_ERR_ARGUMENT) else RuntimeError)(f"fvg_create: {msg}")
         self.h = h
         self.shape = (self.cfg.nx, self.cfg.ny, self.cfg.nz)
-        self.ncells = self.cfg.nx * self.cfg.ny * self.cfg.nz
+        if part is not None:
+            ax, first, count = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+            self.lib.fvg_part_info(h, ctypes.byref(ax), ctypes.byref(first), ctypes.byref(count), None, None, None)
+            shape = list(self.shape)
+            shape[ax.value] = count.value
+            self.shape = tuple(shape)
+        self.ncells = self.shape[0] * self.shape[1] * self.shape[2]
         self.stages = P.STAGES[self.cfg.time_scheme]
         if U is not None:
             self.set_state(U)

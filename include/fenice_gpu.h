@@ -103,6 +103,33 @@ int fvg_step(fvg_run* run, double t_end, double* dt, double* smax);
  * clock kept on the device; *steps gets the number taken. */
 int fvg_run_until(fvg_run* run, double t_end, int max_steps, int* steps);
 
+/* ---- Slab decomposition (one process, or one part, per GPU; SimulationRun.cpp:1011-1446 run_mpi and
+ * MPIDecomposition.cpp:114-242 split the mesh into strips the same way and exchange halos and the wave speed).
+ * Part `part` of `nparts` slabs of the mesh of cfg along its slowest axis (z on a 3-D mesh, y on a 2-D one): planes
+ * first .. first + count - 1 (the first nsplit % nparts parts hold one plane more), with `depth` ghost planes beyond each
+ * side that is an interface with a neighbouring part (a periodic axis joins the last part to the first). The mesh
+ * spacing and step length are the whole mesh's, so a decomposed run gives the bits of the whole run. A part's state is
+ * uploaded and downloaded with fvg_upload_state / fvg_download_state (its own cells, in the reference's order); it is
+ * advanced step by step through fvg_part_phase (fvg_step, fvg_run_until, fvg_residual and the sensor are refused).
+ * Refused configurations: an immersed body; fewer than depth (3 for WENO5, else 2) planes per part; a first-order run
+ * split along a periodic axis. */
+int fvg_create_part(const fvg_config* cfg, int nparts, int part, fvg_run** out);
+/* axis: 1 (y) or 2 (z); the part's planes; ghost depth; whether the low / high side is an interface */
+int fvg_part_info(const fvg_run* run, int* axis, int* first, int* count, int* depth, int* peer_lo, int* peer_hi);
+/* the part's device buffers: the planes it sends to its low and high neighbours and receives from them (count doubles
+ * each), and the all-reduce slots (2 doubles) */
+int fvg_part_buffers(fvg_run* run, double** send_lo, double** send_hi, double** recv_lo, double** recv_hi, long long* count, double** reduce);
+/* starts advancing toward t_end (max_steps > 0: at most that many steps), as fvg_run_until does */
+int fvg_part_begin(fvg_run* run, double t_end, int max_steps);
+/* Enqueues phase `phase` (0, 1, ...) of the current step on the run's stream. *comm says what the hosts do before the
+ * next phase, on that stream: 0 the step is complete; 1 exchange: every part's send_lo goes to its low neighbour's
+ * recv_hi and its send_hi to its high neighbour's recv_lo; 2 all-reduce (MAX, over all parts) the first *nreduce doubles
+ * of the reduce slots. Every part takes the same phases in the same order. */
+int fvg_part_phase(fvg_run* run, int phase, int* comm, int* nreduce);
+/* reads the control block (synchronises the stream): whether the run continues, its steps, t, the last dt and wave
+ * speed; FVG_ERR_DIVERGED as fvg_run_until */
+int fvg_part_status(fvg_run* run, int* active, int* steps, double* t, double* dt, double* smax);
+
 int fvg_get_time(const fvg_run* run, double* t);
 int fvg_set_time(fvg_run* run, double t);
 /* The MUSCL-Hancock lagged wave speed (the reference's checkpoint key S; 0: the next step seeds it). */
