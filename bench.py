@@ -476,6 +476,79 @@ def cyl_arm(args, world, rank, local):
     return out
 
 
+SLAB_WORKLOAD = ("Taylor-Green vortex 3-D, WENO5-Z + low-Mach HLLC + SSP-RK3, viscous Re 1600 Pr 0.71, CFL 0.5, slab-decomposed along z "
+                 "(fenice_b200.slabs): {layout}")
+
+
+def slab_arm(args, world, rank, local):
+    """The slab decomposition: at N = 1, the --size^3 mesh as --parts parts in this process on one GPU (the interface
+    planes and speeds copied between the parts' buffers), against the whole run of the same mesh, bit for bit; under
+    torchrun, one --size^3 part per rank of a mesh of N --size planes along z (halo exchange and speed all-reduce over
+    NCCL). Plain FP64 and mixed forms; each timed with CUDA events on the parts' streams over --steps steps after
+    --warmup."""
+    import hashlib
+
+    import torch
+
+    from fenice_b200 import Run, slabs
+
+    n = args.size
+    out = {}
+    for name, prec in (("plain_fp64", 0), ("mixed", 1)):
+        if world == 1:
+            params = workload(n)
+            U0 = tgv_state(n)
+            nparts = args.parts
+            parts = [slabs.Part(params, nparts, i, U=u, precision=prec, device=local) for i, u in enumerate(slabs.split_state(params, U0, nparts))]
+            ex = slabs.LocalExchange(parts)
+        else:
+            params = dict(workload(n), nz=n * world, Lz=2 * math.pi * world)
+            grid = tgv_state(n)   # every rank's part starts from the periodic Taylor-Green box (the mesh is N boxes along z)
+            parts = [slabs.Part(params, world, rank, U=grid, precision=prec, device=local)]
+            ex = slabs.DistExchange.for_part(parts[0])
+        slabs.advance(parts, ex, 1e30, args.warmup)
+        streams = [torch.cuda.ExternalStream(p.stream(), device=torch.device("cuda", local)) for p in parts]
+        torch.cuda.synchronize()
+        barrier(world)
+        start = torch.cuda.Event(enable_timing=True)
+        ends = [torch.cuda.Event(enable_timing=True) for _ in parts]
+        with Clocks(local) as clk:
+            start.record(streams[0])
+            for st in streams[1:]:
+                st.wait_event(start)
+            steps, _ = slabs.advance(parts, ex, 1e30, args.steps)
+            for e, st in zip(ends, streams):
+                e.record(st)
+            torch.cuda.synchronize()
+        ms = allmax(max(start.elapsed_time(e) for e in ends), world)
+        cells = n ** 3 * world
+        out[name] = {"value": cells * STAGES * steps / (ms * 1e-3), "ms": ms, "steps": steps, "clocks": clk.summary()}
+        if world == 1:
+            Ud = slabs.join_states(params, [p.state() for p in parts])
+            for p in parts:
+                p.close()
+            whole = Run(params, U=U0, precision=prec, device=local)
+            whole.run(1e30, max_steps=args.warmup)
+            ext = torch.cuda.ExternalStream(whole.stream(), device=torch.device("cuda", local))
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            s0.record(ext)
+            whole.run(1e30, max_steps=args.steps)
+            s1.record(ext)
+            torch.cuda.synchronize()
+            wms = s0.elapsed_time(s1)
+            Uw = whole.state()
+            whole.close()
+            out[name]["whole_run_ms"] = wms
+            out[name]["decomposition_overhead"] = ms / wms - 1.0
+            out[name]["bits_equal_whole_run"] = bool(np.array_equal(Ud.view(np.uint64), Uw.view(np.uint64)))
+            out[name]["state_sha256"] = hashlib.sha256(np.ascontiguousarray(Ud).tobytes()).hexdigest()
+        else:
+            for p in parts:
+                p.close()
+    return out
+
+
 def gpu_arm(args, world, rank, local):
     import torch
 
@@ -558,7 +631,8 @@ def main():
     ap.add_argument("--size", type=int, default=256, help="cells per axis (256: the benchmark workload)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-baseline", type=int, default=1, help="time the reference on the host cores (rank 0, N = 1)")
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "quadrants", "cylinder"],
+    ap.add_argument("--parts", type=int, default=2, help="slab workload at N = 1: parts of the mesh in one process")
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "quadrants", "cylinder", "slab"],
                     help="tgv: the 3-D Taylor-Green vortex (default); batch: 512 shock tubes in one persistent launch per stage; "
                          "quadrants: a seeded four-quadrant Riemann problem (--size cells per axis, default 2048 for it)")
     ap.add_argument("--seed", type=int, default=2048, help="seed of the quadrants workload")
@@ -606,6 +680,24 @@ def main():
             r = cy["reference_cpu"]
             line["cpu_baseline"] = {"value": r["value"], "unit": "cell-updates/s", "cores": r["threads"], "kind": "reference",
                                     "sample": f"{r['steps']} MUSCL-Hancock steps of the same mesh from the free stream after 2 untimed"}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+    if args.workload == "slab":
+        sl = slab_arm(args, world, rank, local)
+        m = sl["mixed"]
+        layout = (f"{args.size}^3 as {args.parts} parts in one process on one GPU" if world == 1
+                  else f"{args.size} x {args.size} x {args.size * world}, one {args.size}^3 part per GPU, NCCL halo exchange")
+        line = {"metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world, "steps": m["steps"], "warmup": args.warmup,
+                "ms_per_step": m["ms"] / m["steps"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 stencil / f64 state (value); plain form f64", "data": "synthetic (Taylor-Green state)",
+                "config": {"workload": SLAB_WORKLOAD.format(layout=layout) + "; value: mixed form", "cells": args.size ** 3 * world,
+                           "parallelism": f"slab decomposition z, {max(world, args.parts if world == 1 else world)} parts"},
+                "clocks": m["clocks"], "forms": sl, "e2e": None, "gpu_launches": None}
         if rank == 0:
             print(json.dumps(line), flush=True)
         if world > 1:
