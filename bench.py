@@ -601,7 +601,7 @@ def gpu_arm(args, world, rank, local):
     # refresh steps)
     launches = 3 * (args.steps * 11 + 1) + args.steps * 5
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_m / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": ms_l / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 stencil / f64 state (mixed form) with bf16 sensor; plain form f64",
             "data": "synthetic (Taylor-Green initial state computed in numpy)",
             "config": {"workload": f"Taylor-Green vortex 3-D {n}^3, WENO5-Z + low-Mach HLLC + SSP-RK3, viscous Re 1600 Pr 0.71, CFL 0.5; "
