@@ -57,6 +57,9 @@ struct Bc {
     int grav_on;
     // planes of the neighbouring part held beyond each side (kHaloPeer sides only; 0 elsewhere)
     int ext[6];
+    // mass-flow inlets: the target velocity of each side for the residual being taken (device array of 6, written from
+    // the residual's state before it; null without a mass-flow side)
+    const double* u_target;
 };
 
 // Whether position g along an axis of n cells is a cell whose state is in the arrays (a cell of the mesh, or of a
@@ -67,7 +70,7 @@ __device__ __forceinline__ bool held(const Bc& bc, int axis, int g, int n) {
 }
 
 // BoundaryManager::ghost_state (cpp/src/Boundaries.cpp:106-153) for the sides a device run supports (every type but
-// the mass-flow inlet and the non-reflecting outlet, which need more than one cell).
+// the non-reflecting outlet, which needs more than one cell; the mass-flow inlet's target comes from Bc::u_target).
 template <typename T, int NV>
 __device__ __forceinline__ St<T, NV> ghost_state(const Eos<T>& e, const Bc& bc, int side, const St<T, NV>& Ui) {
     const int type = bc.type[side];
@@ -93,6 +96,11 @@ __device__ __forceinline__ St<T, NV> ghost_state(const Eos<T>& e, const Bc& bc, 
     case kBcMovingWall:
     case kBcVelInlet:
         Wg[1] = T(2) * T(bc.u_in) - Wi[1];
+        Wg[2] = T(2) * T(bc.v_in) - Wi[2];
+        if constexpr (NV == 5) Wg[4] = -Wi[4];
+        break;
+    case kBcMassflowInlet:   // the x velocity of the side's mass-flow target, whatever the side's axis (as the reference)
+        Wg[1] = T(2) * T(bc.u_target[side]) - Wi[1];
         Wg[2] = T(2) * T(bc.v_in) - Wi[2];
         if constexpr (NV == 5) Wg[4] = -Wi[4];
         break;

@@ -136,6 +136,36 @@ __global__ void k_hancock_end(Ctl* c, const double* bm, int nb, const double* bm
     }
 }
 
+// BoundaryManager::apply_side's mass-flow target (Boundaries.cpp:284-294), one block per side: the mean over the side's
+// cells (in cell order, a sequential sum as the reference's) of cons_to_prim's density, rho_avg = max(mean, 1e-5),
+// u_target = rho_in u_in / rho_avg. Other sides return at once.
+template <int NV>
+__global__ void __launch_bounds__(1024) k_massflow(Mesh m, Bc bc, const double* U, double rho_in, double u_in, double* u_target, const int* gate) {
+    __shared__ double rho[1024];
+    const int side = blockIdx.x;
+    if (!*gate || bc.type[side] != kBcMassflowInlet) return;
+    const int axis = side >> 1, hi = side & 1;
+    const long long nx = m.nx, ny = m.ny, nz = m.nz;
+    const long long count = axis == 0 ? ny * nz : (axis == 1 ? nx * nz : nx * ny);
+    double sum = 0.0;
+    for (long long base = 0; base < count; base += blockDim.x) {
+        const long long k = base + threadIdx.x;
+        if (k < count) {   // Mesh::boundary_cell (Core.hpp:136-145)
+            const long long cell = axis == 0 ? k * nx + (hi ? nx - 1 : 0)
+                                   : axis == 1 ? ((k / nx) * ny + (hi ? ny - 1 : 0)) * nx + k % nx
+                                               : (hi ? (nz - 1) * ny * nx : 0) + k;
+            rho[threadIdx.x] = vmax(read_state<NV>(bc, U, m.plane, cell)[0], Num<double>::eos_eps);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const long long lim = count - base < blockDim.x ? count - base : blockDim.x;
+            for (long long q = 0; q < lim; ++q) sum = sum + rho[q];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) u_target[side] = (rho_in * u_in) / vmax(sum / (double)count, 1e-5);
+}
+
 // ---- parts of a slab-decomposed mesh
 // the largest of a stage's per-CTA speeds (and viscous bounds) into a slot the hosts all-reduce (0 when the gate is off)
 __global__ void k_part_local(const int* gate, const double* bm, int nb, const double* bmv, int nbv, double* out) {
@@ -368,6 +398,7 @@ struct fvg_run {
     // and plane count, the ghost depth, which sides are interfaces with a neighbouring part, the offset of the first
     // interior plane in the state arrays (U, Ut, R, Rv point there), the exchange buffers (send lo / hi, recv lo / hi:
     // depth x plane cells x nvar each) and the all-reduce slots
+    double* d_utarget = nullptr;   // mass-flow inlets: the target velocity per side (Bc::u_target)
     bool is_part = false;
     int nparts = 1, part = 0, split = 2, first = 0, count = 0, depth = 0, peer[2] = {0, 0};
     long long goff = 0, area = 0, xcount = 0;
@@ -406,7 +437,6 @@ std::string validate(const fvg_config& c) {
     const int naxes = c.nz > 1 ? 3 : 2;
     for (int s = 0; s < 2 * naxes; ++s) {
         if (c.bc[s] < 0 || c.bc[s] > FVG_BC_NONREFLECTING) return "unknown boundary type";
-        if (c.bc[s] == FVG_BC_MASSFLOWINLET) return "the mass-flow inlet is not supported on the device";
         if (c.bc[s] == FVG_BC_NONREFLECTING) return "the non-reflecting outlet is not supported on the device";
     }
     for (int a = 0; a < naxes; ++a)
@@ -576,6 +606,16 @@ cudaError_t ibm_fill(fvg_run* r, const double* Usrc, double* Uout, int reset, co
     return cudaGetLastError();
 }
 
+// The mass-flow inlets' targets of the state a residual is taken of (before the residual's kernels read a ghost).
+cudaError_t massflow_targets(fvg_run* r, const double* Uin, const int* gate) {
+    if (!r->d_utarget) return cudaSuccess;
+    if (r->nvar == 5)
+        k_massflow<5><<<6, 1024, 0, r->stream>>>(r->m, r->bc, Uin, r->cfg.rho_in, r->cfg.u_in, r->d_utarget, gate);
+    else
+        k_massflow<4><<<6, 1024, 0, r->stream>>>(r->m, r->bc, Uin, r->cfg.rho_in, r->cfg.u_in, r->d_utarget, gate);
+    return cudaGetLastError();
+}
+
 // The viscous residual of Uin into Rv and its per-CTA speed bounds into bmv.
 cudaError_t launch_visc(fvg_run* r, const double* Uin, double* bmv, const int* gate, bool timed = true) {
     if (timed) timer_mark(r, r->t_visc);
@@ -591,6 +631,7 @@ cudaError_t launch_visc(fvg_run* r, const double* Uin, double* bmv, const int* g
 cudaError_t residual_stage(fvg_run* r, const double* Uin, const double* U0, double* out, int mode, double ca, double cb, int stage, const int* gate) {
     cudaError_t e;
     if (r->ibm && (e = ibm_fill(r, Uin, nullptr, 0, gate)) != cudaSuccess) return e;
+    if ((e = massflow_targets(r, Uin, gate)) != cudaSuccess) return e;
     if (r->cfg.use_viscous && (e = launch_visc(r, Uin, r->bmv[stage], gate)) != cudaSuccess) return e;
     timer_mark(r, r->t_stage);
     e = r->stage.launch(stage_args(r, Uin, U0, out, mode, ca, cb, r->cfg.use_viscous ? r->Rv : nullptr, r->bm[stage], gate), r->nb, r->stream);
@@ -628,6 +669,7 @@ cudaError_t enqueue_step(fvg_run* r, bool refresh = true) {
         k_hancock_begin<<<1, 1, 0, r->stream>>>(c);
         // the seed (first step only; untimed): one plain residual for the speed, its viscous bound included
         if (r->ibm && (e = ibm_fill(r, Uin, nullptr, 0, &c->seed))) return e;
+        if ((e = massflow_targets(r, Uin, &c->seed))) return e;
         if (r->cfg.use_viscous && (e = launch_visc(r, Uin, r->bmv[1], &c->seed, false))) return e;
         if ((e = r->stage.launch(stage_args(r, Uin, nullptr, r->R, kStoreR, 0, 0, r->cfg.use_viscous ? r->Rv : nullptr, r->bm_seed, &c->seed), r->nb,
                                  r->stream)))
@@ -635,6 +677,7 @@ cudaError_t enqueue_step(fvg_run* r, bool refresh = true) {
         k_hancock_seed<<<1, 1024, 0, r->stream>>>(c, r->bm_seed, r->nb, r->bmv[1], nbv);
         k_hancock_dt<<<1, 1, 0, r->stream>>>(c);
         if (r->ibm && (e = ibm_fill(r, Uin, nullptr, 0, act))) return e;
+        if ((e = massflow_targets(r, Uin, act))) return e;
         if (r->cfg.use_viscous && (e = launch_visc(r, Uin, r->bmv[0], act))) return e;
         timer_mark(r, r->t_stage);
         e = launch_hancock(r, hancock_args(r, Uin, Uout, kAxpy, r->bm[0], act));
@@ -892,6 +935,11 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
             g_create_error = "each part needs at least " + std::to_string(depth) + " planes along the split axis";
             return FVG_ERR_CONFIG;
         }
+        for (int s = 0; s < 6; ++s)
+            if (cfg->bc[s] == FVG_BC_MASSFLOWINLET) {   // its target is a sequential sum over the whole side
+                g_create_error = "a decomposed mesh cannot have a mass-flow inlet";
+                return FVG_ERR_CONFIG;
+            }
         // a first-order run takes the states of a periodic side's faces through the round trip (a side without a halo);
         // split there, those faces would be a part interface
         if (cfg->reconstruction == FVG_RECON_NONE && cfg->bc[2 * split] == FVG_BC_PERIODIC) {
@@ -1016,6 +1064,15 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
     for (double** p : {&run->U, &run->Ut, &run->R, &run->Rv})
         if (*p) cudaMemsetAsync(*p, 0, sbytes, run->stream), *p += run->goff;
     if (run->xred) cudaMemsetAsync(run->xred, 0, sizeof(double) * 2, run->stream);
+    for (int s = 0; s < 2 * (run->dim == 3 ? 3 : 2); ++s)
+        if (c.bc[s] == FVG_BC_MASSFLOWINLET && !run->d_utarget) {
+            if (cudaMalloc(&run->d_utarget, sizeof(double) * 6) != cudaSuccess) {
+                run->err = "device allocation failed";
+                return bail(FVG_ERR_CUDA);
+            }
+            cudaMemsetAsync(run->d_utarget, 0, sizeof(double) * 6, run->stream);
+            run->bc.u_target = run->d_utarget;
+        }
     const int nbmax = run->nb > run->nbh ? run->nb : run->nbh;
     for (int s = 0; s < 3; ++s)
         if (cudaMalloc(&run->bm[s], sizeof(double) * nbmax) != cudaSuccess || cudaMalloc(&run->bmv[s], sizeof(double) * run->nbv) != cudaSuccess) {
@@ -1102,7 +1159,8 @@ int fvg_destroy(fvg_run* run) {
         if (run->graph[g]) cudaGraphExecDestroy(run->graph[g]);
     for (double* p : {run->U, run->Ut, run->R, run->Rv})   // the arrays start goff doubles before the first interior plane
         if (p) cudaFree(p - run->goff);
-    for (double* p : {run->staging, run->bm_seed, run->bm[0], run->bm[1], run->bm[2], run->bmv[0], run->bmv[1], run->bmv[2], run->xbuf, run->xred})
+    for (double* p : {run->staging, run->bm_seed, run->bm[0], run->bm[1], run->bm[2], run->bmv[0], run->bmv[1], run->bmv[2], run->xbuf, run->xred,
+                      run->d_utarget})
         if (p) cudaFree(p);
     if (run->ctl) cudaFree(run->ctl);
     if (run->sens) cudaFree(run->sens);
@@ -1169,6 +1227,7 @@ int fvg_residual(fvg_run* run, double predictor_half_dt, double* R, size_t ncell
             return fail(run, FVG_ERR_CONFIG, "the MUSCL-Hancock predictor needs a MUSCL run");
         CK(cudaMemcpyAsync(&c->half_dt, &predictor_half_dt, sizeof(double), cudaMemcpyHostToDevice, run->stream));
         if (run->ibm) CK(ibm_fill(run, run->Ucur(), nullptr, 0, always));
+        CK(massflow_targets(run, run->Ucur(), always));
         if (run->cfg.use_viscous) CK(launch_visc(run, run->Ucur(), run->bmv[0], always));
         CK(launch_hancock(run, hancock_args(run, run->Ucur(), out, kStoreR, run->bm[0], always)));
         k_stage_max<<<1, 1024, 0, run->stream>>>(c, always, 0, run->bm[0], run->nbh, run->bmv[0], run->cfg.use_viscous ? run->nbv : 0);
@@ -1596,6 +1655,9 @@ extern "C" int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long
     if (cfg->precision != FVG_PREC_FP64) return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: the FP64 form only");
     if (cfg->use_ibm) return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: an immersed body needs its tables on the device; use fvg_residual");
     if (cfg->use_viscous) return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: viscous runs need a residual-sized scratch array; use fvg_residual");
+    for (int s = 0; s < 6; ++s)
+        if (cfg->bc[s] == FVG_BC_MASSFLOWINLET)
+            return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: a mass-flow inlet needs its target on the device; use fvg_residual");
     const fvg_config& c = *cfg;
     const int dim = c.nz > 1 ? 3 : 2;
     const long long ncells = (long long)c.nx * c.ny * c.nz;

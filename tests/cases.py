@@ -199,4 +199,13 @@ FORCE_CASES = [
                                                                                                 z=("transmissive", "wall")), u_in=0.2), 56, 0.003, 4),
     ("grav_first_order_stiff", dict(nx=30, ny=8, reconstruction="none", time_scheme="Explicit Euler", eos_type="Stiffened Gas", gamma=4.4, p_inf=0.5,
                                     use_bodyforce=True, gx=0.3, gy=-1.0, **bcs("transmissive", "transmissive", "wall", "wall")), 57, 0.0, 6),
+    # the mass-flow inlet (its target velocity from the mean density of the side's cells, per residual)
+    ("massflow_muscl_rk2_2d", dict(nx=30, ny=16, reconstruction="muscl", muscl_limiter="MC", time_scheme="SSP Runge-Kutta 2", rho_in=1.2, u_in=0.6,
+                                   p_out=0.9, **bcs("massflow_inlet", "outlet", "wall", "wall")), 58, 0.0, 5),
+    ("massflow_hancock_order1", dict(nx=28, ny=18, reconstruction="muscl", muscl_limiter="Van Leer", time_scheme="MUSCL-Hancock", boundary_order=1,
+                                     rho_in=0.9, u_in=0.4, **bcs("massflow_inlet", "transmissive", "periodic", "periodic")), 59, 0.003, 5),
+    ("massflow_y_side_2d", dict(nx=20, ny=24, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", rho_in=1.1, u_in=0.3, v_in=0.5,
+                                **bcs("wall", "wall", "massflow_inlet", "outlet")), 60, 0.0, 4),
+    ("massflow_visc_3d", dict(nx=12, ny=10, nz=9, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", use_viscous=True, mu=0.01, rho_in=1.0,
+                              u_in=0.5, **bcs("massflow_inlet", "outlet", "no_slip", "wall", z=("periodic", "periodic"))), 61, 0.0, 3),
 ]

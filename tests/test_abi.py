@@ -40,7 +40,6 @@ def create_code(params):
 
 @pytest.mark.parametrize("params,words", [
     (dict(nx=0), "nx"),
-    (dict(bc_xmin="massflow_inlet"), "mass-flow"),
     (dict(bc_xmax="nonreflecting"), "non-reflecting"),
     (dict(bc_xmin="periodic", bc_xmax="wall"), "periodic"),
     (dict(reconstruction="weno5", time_scheme="MUSCL-Hancock"), "MUSCL-Hancock"),
