@@ -261,7 +261,8 @@ std::string batch_config_error(const fvg_config* cfgs, int n) {
         if (c.use_viscous || c.use_ibm || c.use_bodyforce)
             return "problem " + std::to_string(p) + ": batched problems are inviscid, without an immersed body or a body force";
         for (int s = 0; s < 4; ++s)
-            if (c.bc[s] == FVG_BC_MASSFLOWINLET) return "problem " + std::to_string(p) + ": batched problems have no mass-flow inlet";
+            if (c.bc[s] == FVG_BC_MASSFLOWINLET || c.bc[s] == FVG_BC_NONREFLECTING)
+                return "problem " + std::to_string(p) + ": batched problems have no mass-flow inlet or non-reflecting outlet";
         if (c.time_scheme == FVG_TS_HANCOCK) return "problem " + std::to_string(p) + ": batched problems use Euler, SSP-RK2 or SSP-RK3";
         if (c.reconstruction != a.reconstruction || c.riemann != a.riemann || c.time_scheme != a.time_scheme || c.precision != a.precision ||
             c.device != a.device)

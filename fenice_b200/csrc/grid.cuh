@@ -60,6 +60,9 @@ struct Bc {
     // mass-flow inlets: the target velocity of each side for the residual being taken (device array of 6, written from
     // the residual's state before it; null without a mass-flow side)
     const double* u_target;
+    // non-reflecting outlets: relaxation sigma, transverse weight beta (< 0: the local Mach number), the domain length
+    // and the cell size per axis
+    double nrbc_sigma, nrbc_beta, length[3], h[3];
 };
 
 // Whether position g along an axis of n cells is a cell whose state is in the arrays (a cell of the mesh, or of a
@@ -216,6 +219,77 @@ template <int DIM> __device__ __forceinline__ unsigned char stencil_solid(const 
     return (bc.solid[cc] != 0 || bc.solid[cw] != 0) ? 1 : 0;
 }
 
+// BoundaryManager::nonreflecting_ghost (cpp/src/Boundaries.cpp:155-191) of the cell (i, j, k) next to side `side`, with
+// its tangential neighbours as apply_side gathers them (Boundaries.cpp:316-355): along each other axis of more than one
+// cell, the cells on either side (wrapped on a periodic axis, a neighbouring part's across a part interface, else the cell
+// itself at an end, which halves the span). The ghost differs from the cell in the incoming acoustic characteristic only.
+template <int NV>
+__device__ __forceinline__ St<double, NV> nrbc_ghost(const Mesh& m, const Bc& bc, const Eos<double>& e, const double* __restrict__ U, int side, int i,
+                                                     int j, int k, const St<double, NV>& Ui) {
+    const int axis = side >> 1;
+    const double s = (side & 1) ? 1.0 : -1.0;
+    const int mom[3] = {1, 2, NV == 5 ? 4 : 1};
+    const St<double, NV> Wi = c2p(e, Ui);
+    St<double, NV> Wg = Wi;
+    const int qv = mom[axis];
+    const double u_out = s * Wi[qv];
+    const double c = sound_speed(e, Wi[3], Wi[0]);
+    const double M = vmin(vmax(u_out / c, -1.0), 1.0);
+    if (M >= 1.0) return p2c(e, Wg);   // supersonic outflow: nothing enters
+    const double h = bc.h[axis];
+    const double K = bc.nrbc_sigma * c * (1.0 - M * M) / bc.length[axis];
+    const double beta = bc.nrbc_beta >= 0.0 ? bc.nrbc_beta : fabs(M);
+    double T1 = 0.0;
+    if (beta < 1.0) {
+        const int n3[3] = {m.nx, m.ny, m.nz};
+        const int ijk[3] = {i, j, k};
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            if (t == axis || n3[t] == 1) continue;
+            const bool peer_lo = bc.halo[2 * t] == kHaloPeer, peer_hi = bc.halo[2 * t + 1] == kHaloPeer;
+            const bool wrap = bc.type[2 * t] == kBcPeriodic && bc.type[2 * t + 1] == kBcPeriodic && !peer_lo && !peer_hi;
+            int lo = ijk[t] - 1, hi = ijk[t] + 1;
+            double span = 2.0;
+            if (wrap) {
+                lo = (lo + n3[t]) % n3[t];
+                hi = hi % n3[t];
+            } else {
+                if (lo < 0 && !peer_lo) {
+                    lo = 0;
+                    span -= 1.0;
+                }
+                if (hi >= n3[t] && !peer_hi) {
+                    hi = n3[t] - 1;
+                    span -= 1.0;
+                }
+                if (span <= 0.0) continue;
+            }
+            int a[3] = {i, j, k}, b[3] = {i, j, k};
+            a[t] = lo;
+            b[t] = hi;
+            const St<double, NV> Wl = c2p(e, read_state<NV>(bc, U, m.plane, ((long long)a[2] * m.ny + a[1]) * m.nx + a[0]));
+            const St<double, NV> Wh = c2p(e, read_state<NV>(bc, U, m.plane, ((long long)b[2] * m.ny + b[1]) * m.nx + b[0]));
+            const double ht = span * bc.h[t];
+            const int qt = mom[t];
+            T1 += Wi[qt] * (Wh[3] - Wl[3]) / ht + Wi[0] * c * c * (Wh[qt] - Wl[qt]) / ht - Wi[0] * c * s * Wi[qt] * (Wh[qv] - Wl[qv]) / ht;
+        }
+    }
+    const double dw1 = -h * (K * (Wi[3] - bc.p_out) - (1.0 - beta) * T1) / (c - u_out);
+    Wg[3] = Wi[3] + 0.5 * dw1;
+    Wg[qv] = Wi[qv] - s * dw1 / (2.0 * Wi[0] * c);
+    Wg[0] = Wi[0] + 0.5 * dw1 / (c * c);
+    return p2c(e, Wg);
+}
+
+// The first-order ghost of the cell (i, j, k) next to a side without a halo: ghost_state, or the non-reflecting ghost.
+template <int NV>
+__device__ __forceinline__ St<double, NV> side_ghost(const Mesh& m, const Bc& bc, const Eos<double>& e, const double* __restrict__ U, int side, int i,
+                                                     int j, int k) {
+    const St<double, NV> Ui = read_state<NV>(bc, U, m.plane, ((long long)k * m.ny + j) * m.nx + i);
+    if (bc.type[side] == kBcNonReflecting) return nrbc_ghost<NV>(m, bc, e, U, side, i, j, k, Ui);
+    return ghost_state(e, bc, side, Ui);
+}
+
 // The first-order states of a boundary face whose side has no halo (BoundaryManager::apply_side,
 // cpp/src/Boundaries.cpp:277-373): the cell next to the side and its ghost (the opposite cell on a periodic side).
 template <int NV>
@@ -229,6 +303,8 @@ __device__ __forceinline__ void side_states(const Mesh& m, const Bc& bc, const E
         const int a = side >> 1, n = a == 0 ? m.nx : (a == 1 ? m.ny : m.nz);
         idx[a] = (side & 1) ? idx[a] - (n - 1) : idx[a] + (n - 1);
         Ug = read_state<NV>(bc, U, m.plane, ((long long)idx[2] * m.ny + idx[1]) * m.nx + idx[0]);
+    } else if (bc.type[side] == kBcNonReflecting) {
+        Ug = nrbc_ghost<NV>(m, bc, e, U, side, i, j, k, Ui);
     } else {
         Ug = ghost_state(e, bc, side, Ui);
     }

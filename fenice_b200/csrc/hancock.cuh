@@ -206,14 +206,14 @@ __global__ void __launch_bounds__(NT) hancock_kernel(const HancockArgs a) {
                     if (wall_lo)
                         UL = ghost_state(e, a.bc, lo_side, UR);
                     else if (a.bc.halo[lo_side] == kHaloNone)
-                        UL = round_trip(e, ghost_state(e, a.bc, lo_side, read_state<4>(a.bc, a.U, m.plane, (long long)gj * nx + gi)));
+                        UL = round_trip(e, side_ghost<4>(m, a.bc, e, a.U, lo_side, gi, gj, 0));
                 }
                 if (t == n_a) {
                     const int ci = axis == 0 ? nx - 1 : gi, cj = axis == 0 ? gj : ny - 1;
                     if (wall_hi)
                         UR = ghost_state(e, a.bc, hi_side, UL);
                     else if (a.bc.halo[hi_side] == kHaloNone)
-                        UR = round_trip(e, ghost_state(e, a.bc, hi_side, read_state<4>(a.bc, a.U, m.plane, (long long)cj * nx + ci)));
+                        UR = round_trip(e, side_ghost<4>(m, a.bc, e, a.U, hi_side, ci, cj, 0));
                 }
                 const double s = face_flux<RIEMANN>(e, a.shock_blend, UL, UR, axis, F);
                 if (s > smax) smax = s;
@@ -460,7 +460,7 @@ __global__ void __launch_bounds__(NT) hancock3d_kernel(const HancockArgs a) {
                     if (wall_lo)
                         UL = ghost_state(e, a.bc, lo_side, UR);
                     else if (a.bc.halo[lo_side] == kHaloNone)
-                        UL = round_trip(e, ghost_state(e, a.bc, lo_side, read_state<5>(a.bc, a.U, m.plane, cell_of(g3[0], g3[1], g3[2]))));
+                        UL = round_trip(e, side_ghost<5>(m, a.bc, e, a.U, lo_side, g3[0], g3[1], g3[2]));
                 }
                 if (t == n3[AX]) {
                     int c3[3] = {g3[0], g3[1], g3[2]};
@@ -468,7 +468,7 @@ __global__ void __launch_bounds__(NT) hancock3d_kernel(const HancockArgs a) {
                     if (wall_hi)
                         UR = ghost_state(e, a.bc, hi_side, UL);
                     else if (a.bc.halo[hi_side] == kHaloNone)
-                        UR = round_trip(e, ghost_state(e, a.bc, hi_side, read_state<5>(a.bc, a.U, m.plane, cell_of(c3[0], c3[1], c3[2]))));
+                        UR = round_trip(e, side_ghost<5>(m, a.bc, e, a.U, hi_side, c3[0], c3[1], c3[2]));
                 }
                 const double s = face_flux<RIEMANN>(e, a.shock_blend, UL, UR, AX, F);
                 if (s > smax) smax = s;

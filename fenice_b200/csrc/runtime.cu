@@ -437,7 +437,6 @@ std::string validate(const fvg_config& c) {
     const int naxes = c.nz > 1 ? 3 : 2;
     for (int s = 0; s < 2 * naxes; ++s) {
         if (c.bc[s] < 0 || c.bc[s] > FVG_BC_NONREFLECTING) return "unknown boundary type";
-        if (c.bc[s] == FVG_BC_NONREFLECTING) return "the non-reflecting outlet is not supported on the device";
     }
     for (int a = 0; a < naxes; ++a)
         if ((c.bc[2 * a] == FVG_BC_PERIODIC) != (c.bc[2 * a + 1] == FVG_BC_PERIODIC))
@@ -446,7 +445,21 @@ std::string validate(const fvg_config& c) {
     if (c.use_bodyforce && c.precision == FVG_PREC_MIXED) return "the body force runs in the FP64 form only";
     if (c.use_bodyforce && c.use_ibm) return "the body force with an immersed body (gravity in its ghost states) is not supported on the device";
     if (!(c.cfl > 0)) return "cfl must be > 0";
+    if (!(c.nrbc_sigma >= 0.0)) return "nrbc_sigma must be >= 0";   // Params.cpp:489-490
+    if (!(c.nrbc_beta <= 1.0)) return "nrbc_beta must be <= 1 (< 0: local Mach number)";
     return "";
+}
+
+// the non-reflecting outlet's parameters (BCParams, cpp/include/fv/Boundaries.hpp:23-29; length: the domain, h: the cells)
+void set_nrbc(const fvg_config& c, Bc& bc) {
+    bc.nrbc_sigma = c.nrbc_sigma;
+    bc.nrbc_beta = c.nrbc_beta;
+    bc.length[0] = c.Lx;
+    bc.length[1] = c.Ly;
+    bc.length[2] = c.Lz;
+    bc.h[0] = c.Lx / c.nx;
+    bc.h[1] = c.Ly / c.ny;
+    bc.h[2] = c.Lz / c.nz;
 }
 
 // the constant body force of a configuration (Simulation::setup, cpp/src/Simulation.cpp:362-363: gz only on a 3-D mesh)
@@ -1019,6 +1032,7 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
     run->bc.v_in = c.v_in;
     run->bc.p_out = c.p_out;
     set_body_force(c, run->bc);
+    set_nrbc(*cfg, run->bc);   // the whole mesh's lengths and cell sizes
     const int TX = run->dim == 3 ? Tile<3>::X : Tile<2>::X, TY = run->dim == 3 ? Tile<3>::Y : Tile<2>::Y, TZ = run->dim == 3 ? Tile<3>::Z : 1;
     run->tiles[0] = (c.nx + TX - 1) / TX;
     run->tiles[1] = (c.ny + TY - 1) / TY;
@@ -1712,6 +1726,7 @@ extern "C" int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long
     a.bc.v_in = c.v_in;
     a.bc.p_out = c.p_out;
     set_body_force(c, a.bc);
+    set_nrbc(c, a.bc);
     a.eos.type = c.eos_type;
     a.eos.gamma = c.gamma;
     a.eos.p_inf = c.p_inf;

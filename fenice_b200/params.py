@@ -21,7 +21,7 @@ DEFAULTS = {
     "boundary_order": 2, "time_scheme": "auto", "cfl": 0.5, "shock_blend": 0.2, "dt_max": 0.0, "t_end": 0.005,
     "max_steps": 0,
     "use_ibm": False, "ibm_shape": "Cylinder", "ibm_radius": 0.1, "ibm_cx": 0.5, "ibm_cy": 0.5, "ibm_cz": 0.5, "ibm_curvature": False,
-    "use_bodyforce": False, "gx": 0.0, "gy": -9.81, "gz": 0.0,
+    "use_bodyforce": False, "gx": 0.0, "gy": -9.81, "gz": 0.0, "nrbc_sigma": 0.28, "nrbc_beta": -1.0,
 }
 
 BC_NAMES = {"wall": 0, "inviscid wall (slip)": 0, "no_slip": 1, "viscous wall (no-slip)": 1, "moving_wall": 2, "moving wall": 2,
@@ -50,7 +50,8 @@ class FvgConfig(ctypes.Structure):
                 ("precision", ctypes.c_int), ("device", ctypes.c_int),
                 ("use_ibm", ctypes.c_int), ("ibm_shape", ctypes.c_int), ("ibm_radius", ctypes.c_double), ("ibm_cx", ctypes.c_double),
                 ("ibm_cy", ctypes.c_double), ("ibm_cz", ctypes.c_double), ("ibm_curvature", ctypes.c_int),
-                ("use_bodyforce", ctypes.c_int), ("gx", ctypes.c_double), ("gy", ctypes.c_double), ("gz", ctypes.c_double)]
+                ("use_bodyforce", ctypes.c_int), ("gx", ctypes.c_double), ("gy", ctypes.c_double), ("gz", ctypes.c_double),
+                ("nrbc_sigma", ctypes.c_double), ("nrbc_beta", ctypes.c_double)]
 
 
 def _flag(v):
@@ -154,6 +155,7 @@ def to_config(params, precision=0, device=0):
     c.ibm_curvature = 1 if _flag(p["ibm_curvature"]) else 0
     c.use_bodyforce = 1 if _flag(p["use_bodyforce"]) else 0
     c.gx, c.gy, c.gz = float(p["gx"]), float(p["gy"]), float(p["gz"])
+    c.nrbc_sigma, c.nrbc_beta = float(p["nrbc_sigma"]), float(p["nrbc_beta"])
     return c
 
 

@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define FVG_ABI_VERSION 2
+#define FVG_ABI_VERSION 3
 
 /* status codes */
 enum {
@@ -75,6 +75,7 @@ typedef struct fvg_config {
     int ibm_curvature;           /* [ibm] ibm_curvature (must be 0 on the device) */
     int use_bodyforce;           /* [physics] use_bodyforce: the constant body force (ConstantBodyForce, Physics.cpp:832-844) */
     double gx, gy, gz;           /* [physics] gx, gy, gz (gz is not used on a 2-D mesh) */
+    double nrbc_sigma, nrbc_beta; /* [boundaries] the non-reflecting outlet's relaxation (0.28) and transverse weight (-1: local Mach) */
 } fvg_config;
 
 typedef struct fvg_run fvg_run;

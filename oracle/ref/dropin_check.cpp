@@ -77,6 +77,8 @@ static fvg_config to_fvg(const fv::SimParams& p) {
     c.gx = p.gx;
     c.gy = p.gy;
     c.gz = p.gz;
+    c.nrbc_sigma = p.nrbc_sigma;
+    c.nrbc_beta = p.nrbc_beta;
     return c;
 }
 

@@ -208,4 +208,12 @@ FORCE_CASES = [
                                 **bcs("wall", "wall", "massflow_inlet", "outlet")), 60, 0.0, 4),
     ("massflow_visc_3d", dict(nx=12, ny=10, nz=9, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", use_viscous=True, mu=0.01, rho_in=1.0,
                               u_in=0.5, **bcs("massflow_inlet", "outlet", "no_slip", "wall", z=("periodic", "periodic"))), 61, 0.0, 3),
+    # the non-reflecting outlet (the characteristic ghost with the transverse terms of the side's tangential neighbours:
+    # wrapped, one-sided at a wall end, across both other axes in 3-D)
+    ("nrbc_muscl_rk2_2d", dict(nx=30, ny=20, reconstruction="muscl", muscl_limiter="MC", time_scheme="SSP Runge-Kutta 2", p_out=0.95,
+                               **bcs("transmissive", "nonreflecting", "periodic", "periodic")), 62, 0.0, 5),
+    ("nrbc_hancock_walls_2d", dict(nx=26, ny=18, reconstruction="muscl", muscl_limiter="Van Leer", time_scheme="MUSCL-Hancock", u_in=0.5, nrbc_beta=0.3,
+                                   **bcs("vel_inlet", "nonreflecting", "wall", "wall")), 63, 0.003, 5),
+    ("nrbc_weno5_visc_3d", dict(nx=12, ny=10, nz=9, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", use_viscous=True, mu=0.01, nrbc_sigma=0.5,
+                                **bcs("transmissive", "nonreflecting", "no_slip", "wall", z=("nonreflecting", "nonreflecting"))), 64, 0.0, 3),
 ]

@@ -12,8 +12,6 @@ TOL = 1e-8   # cpp/tests/regression.py: --tol default
 NOT_ON_DEVICE = {
     "mms_unsteady_hancock": "source terms",
     "mms_walls_b2": "source terms",
-    "vortex_nrbc": "non-reflecting outlet",
-    "tgv3d_nrbc": "non-reflecting outlet",
 }
 
 

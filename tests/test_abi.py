@@ -26,7 +26,7 @@ def test_library_exports_every_declared_entry_point():
     for n in names:
         assert hasattr(lib, n), n
     assert set(names) == set(RT.EXPORTS)
-    assert lib.fvg_abi_version() == 2
+    assert lib.fvg_abi_version() == 3
 
 
 def create_code(params):
@@ -40,7 +40,6 @@ def create_code(params):
 
 @pytest.mark.parametrize("params,words", [
     (dict(nx=0), "nx"),
-    (dict(bc_xmax="nonreflecting"), "non-reflecting"),
     (dict(bc_xmin="periodic", bc_xmax="wall"), "periodic"),
     (dict(reconstruction="weno5", time_scheme="MUSCL-Hancock"), "MUSCL-Hancock"),
     (dict(use_bodyforce=True, reconstruction="muscl", time_scheme="SSP Runge-Kutta 2", precision_mixed=True), "FP64 form only"),

@@ -35,6 +35,9 @@ SLAB_CASES = [
      69, 4, (1, 2, 3), 0),
     ("mixed_w5_rk3_visc_3d", dict(nx=20, ny=16, nz=18, reconstruction="weno5", riemann_solver="lowmach", time_scheme="SSP Runge-Kutta 3",
                                   use_viscous=True, mu=0.01, **TGV), 70, 4, (2, 3), 1),
+    # non-reflecting outlets: on x, whose tangential z neighbours cross the part interfaces, and at the low z end
+    ("nrbc_w5_rk3_visc_3d", dict(nx=12, ny=10, nz=13, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", use_viscous=True, mu=0.01,
+                                 **B("transmissive", "nonreflecting", "periodic", "periodic", z=("nonreflecting", "wall"))), 71, 3, (2, 3), 0),
 ]
 
 
@@ -76,6 +79,8 @@ def test_decomposed_run_to_t_end():
     (dict(nx=16, ny=12, reconstruction="none", time_scheme="Explicit Euler", **B("periodic", "periodic", "periodic", "periodic")), 2, "periodic axis"),
     (dict(nx=32, ny=24, Lx=4.0, Ly=3.0, use_ibm=True, ibm_radius=0.3, ibm_cx=1.0, ibm_cy=1.5, reconstruction="muscl", u_in=0.5,
           **B("vel_inlet", "transmissive", "wall", "wall")), 2, "immersed body"),
+    (dict(nx=32, ny=24, reconstruction="muscl", time_scheme="SSP Runge-Kutta 2", u_in=0.5, **B("massflow_inlet", "outlet", "wall", "wall")), 2,
+     "mass-flow inlet"),
 ])
 def test_part_refusals(params, nparts, words):
     with pytest.raises(ValueError, match=words):
