@@ -258,7 +258,7 @@ std::string batch_config_error(const fvg_config* cfgs, int n) {
         const std::string e = config_error(c);
         if (!e.empty()) return "problem " + std::to_string(p) + ": " + e;
         if (c.nz != 1) return "problem " + std::to_string(p) + ": batched problems are 2-D (nz = 1)";
-        if (c.use_viscous || c.use_ibm || c.use_bodyforce)
+        if (c.use_viscous || c.use_ibm || c.use_bodyforce || c.positivity_fallback)
             return "problem " + std::to_string(p) + ": batched problems are inviscid, without an immersed body or a body force";
         for (int s = 0; s < 4; ++s)
             if (c.bc[s] == FVG_BC_MASSFLOWINLET || c.bc[s] == FVG_BC_NONREFLECTING)

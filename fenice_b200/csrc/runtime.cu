@@ -229,6 +229,48 @@ __global__ void k_axpy(const Ctl* c, double* out, const double* a, const double*
     }
 }
 
+// ---- positivity_fallback (Simulation.cpp:545-584, TimeScheme.cpp:86-90)
+// axpy gated by a repair flag (the control block's dt)
+__global__ void k_axpy_gated(const int* gate, const Ctl* c, double* out, const double* a, const double* b, long long plane, long long n, int nvar) {
+    if (!*gate) return;
+    const double dt = c->dt;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n * nvar; e += (long long)gridDim.x * blockDim.x) {
+        const long long q = e / n, i = e % n;
+        const long long x = q * plane + i;
+        out[x] = a[x] + dt * b[x];
+    }
+}
+// the accepted candidate into the state
+__global__ void k_copy_planes(const Ctl* c, double* out, const double* in, long long plane, long long n, int nvar) {
+    if (!c->active) return;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n * nvar; e += (long long)gridDim.x * blockDim.x) {
+        const long long q = e / n, i = e % n;
+        out[q * plane + i] = in[q * plane + i];
+    }
+}
+// the guard's mark: a cell of the candidate without density (rho > 0 fails, NaN included) or pressure (p + p_inf > 0
+// fails, from the internal energy E - |m|^2 / (2 rho)) that is not flagged yet is flagged, and *grew set
+template <int NV>
+__global__ void k_fb_mark(const Ctl* c, Eos<double> e, const double* U, long long plane, long long n, unsigned char* flags, int* grew) {
+    if (!c->active) return;
+    const double p_inf = e.type == kIdeal ? 0.0 : e.p_inf;
+    int mine = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double rho = U[i];
+        bool bad = !(rho > 0.0);
+        if (!bad) {
+            const double m1 = U[plane + i], m2 = U[2 * plane + i], m3 = NV == 5 ? U[4 * plane + i] : 0.0;
+            const double ke = 0.5 * (m1 * m1 + m2 * m2 + m3 * m3) / rho;
+            bad = !(pressure(e, U[3 * plane + i] - ke) + p_inf > 0.0);
+        }
+        if (bad && !flags[i]) {
+            flags[i] = 1;
+            mine = 1;
+        }
+    }
+    if (__syncthreads_or(mine) && threadIdx.x == 0) atomicExch(grew, 1);
+}
+
 // reference layout (cells of 5 doubles) <-> state planes; a 2-D mesh carries no rho w (it must be zero)
 __global__ void k_aos_to_planes(const double* aos, double* U, long long plane, long long n, int nvar, int* bad) {
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
@@ -399,6 +441,8 @@ struct fvg_run {
     // interior plane in the state arrays (U, Ut, R, Rv point there), the exchange buffers (send lo / hi, recv lo / hi:
     // depth x plane cells x nvar each) and the all-reduce slots
     double* d_utarget = nullptr;   // mass-flow inlets: the target velocity per side (Bc::u_target)
+    unsigned char* fb_flags = nullptr;   // positivity_fallback: the cells flagged in the current stage
+    int* fb_grew = nullptr;              // and whether the last mark flagged a new one (the repeat's gate)
     bool is_part = false;
     int nparts = 1, part = 0, split = 2, first = 0, count = 0, depth = 0, peer[2] = {0, 0};
     long long goff = 0, area = 0, xcount = 0;
@@ -441,8 +485,19 @@ std::string validate(const fvg_config& c) {
     for (int a = 0; a < naxes; ++a)
         if ((c.bc[2 * a] == FVG_BC_PERIODIC) != (c.bc[2 * a + 1] == FVG_BC_PERIODIC))
             return "a periodic axis needs both of its sides periodic";
-    if (c.time_scheme == FVG_TS_HANCOCK && c.reconstruction != FVG_RECON_MUSCL) return "MUSCL-Hancock needs reconstruction = muscl";
+    if (c.time_scheme == FVG_TS_HANCOCK && c.reconstruction != FVG_RECON_MUSCL) return "time_scheme = MUSCL-Hancock needs reconstruction = muscl";
+    if ((c.reconstruction == FVG_RECON_WENO3 || c.reconstruction == FVG_RECON_WENO5) && c.time_scheme == FVG_TS_SSPRK2)   // Params.cpp:444-446
+        return std::string("reconstruction = ") + (c.reconstruction == FVG_RECON_WENO3 ? "weno3" : "weno5") +
+               " is not used with SSP Runge-Kutta 2 (use SSP Runge-Kutta 3)";
+    if (!(c.weno_epsilon >= 0.0)) return "weno_epsilon must be >= 0";
+    if (!(c.dt_max >= 0.0) || !std::isfinite(c.dt_max)) return "dt_max must be finite and >= 0 (0: off)";
+    if (c.use_viscous && (!(c.mu >= 0.0) || !(c.pr > 0.0))) return "mu must be >= 0 and pr > 0 with use_viscous";
     if (c.use_bodyforce && c.precision == FVG_PREC_MIXED) return "the body force runs in the FP64 form only";
+    if (c.positivity_fallback) {   // Params.cpp:464-467
+        if (c.reconstruction != FVG_RECON_WENO3 && c.reconstruction != FVG_RECON_WENO5)
+            return "positivity_fallback needs reconstruction = weno3 or weno5 (the other schemes keep their reconstructed states between the cells)";
+        if (c.precision != FVG_PREC_FP64) return "positivity_fallback runs in the FP64 form only";
+    }
     if (c.use_bodyforce && c.use_ibm) return "the body force with an immersed body (gravity in its ghost states) is not supported on the device";
     if (!(c.cfl > 0)) return "cfl must be > 0";
     if (!(c.nrbc_sigma >= 0.0)) return "nrbc_sigma must be >= 0";   // Params.cpp:489-490
@@ -641,13 +696,16 @@ cudaError_t launch_visc(fvg_run* r, const double* Uin, double* bmv, const int* g
 
 // One residual stage of Uin: the immersed body's forced states, the viscous sweep (viscous runs), then the inviscid
 // stage kernel.
-cudaError_t residual_stage(fvg_run* r, const double* Uin, const double* U0, double* out, int mode, double ca, double cb, int stage, const int* gate) {
+cudaError_t residual_stage(fvg_run* r, const double* Uin, const double* U0, double* out, int mode, double ca, double cb, int stage, const int* gate,
+                           const unsigned char* fb = nullptr) {
     cudaError_t e;
     if (r->ibm && (e = ibm_fill(r, Uin, nullptr, 0, gate)) != cudaSuccess) return e;
     if ((e = massflow_targets(r, Uin, gate)) != cudaSuccess) return e;
     if (r->cfg.use_viscous && (e = launch_visc(r, Uin, r->bmv[stage], gate)) != cudaSuccess) return e;
     timer_mark(r, r->t_stage);
-    e = r->stage.launch(stage_args(r, Uin, U0, out, mode, ca, cb, r->cfg.use_viscous ? r->Rv : nullptr, r->bm[stage], gate), r->nb, r->stream);
+    StageArgs sa = stage_args(r, Uin, U0, out, mode, ca, cb, r->cfg.use_viscous ? r->Rv : nullptr, r->bm[stage], gate);
+    sa.fb = fb;
+    e = r->stage.launch(sa, r->nb, r->stream);
     timer_mark(r, r->t_stage);
     return e;
 }
@@ -668,9 +726,74 @@ int axpy_blocks(const fvg_run* r) {
     return (int)(b < 148 * 16 ? b : 148 * 16);
 }
 
+// positivity_fallback: TimeScheme::repair (TimeScheme.cpp:86-90) on the device. Up to kMaxRepairs = 8 times: mark the
+// candidate (new cells without density or pressure join the stage's flagged set and raise fb_grew); if one did, `again`
+// recomputes the candidate with first-order faces around the set (gated by fb_grew). Then the set is emptied. The
+// repeats' wave speeds are not used (the stage's speed is its first residual's).
+template <typename F> cudaError_t fb_repair(fvg_run* r, const double* cand, F again) {
+    cudaError_t e;
+    for (int it = 0; it < 8; ++it) {
+        if ((e = cudaMemsetAsync(r->fb_grew, 0, sizeof(int), r->stream))) return e;
+        if (r->nvar == 5)
+            k_fb_mark<5><<<axpy_blocks(r), 256, 0, r->stream>>>(r->ctl, r->eos, cand, r->m.plane, r->m.ncells, r->fb_flags, r->fb_grew);
+        else
+            k_fb_mark<4><<<axpy_blocks(r), 256, 0, r->stream>>>(r->ctl, r->eos, cand, r->m.plane, r->m.ncells, r->fb_flags, r->fb_grew);
+        if ((e = cudaGetLastError())) return e;
+        if ((e = again())) return e;
+    }
+    return cudaMemsetAsync(r->fb_flags, 0, r->m.ncells, r->stream);
+}
+
+// A Runge-Kutta / Euler step with the guard (TimeScheme.cpp:110-290 with guard_): every stage writes its candidate into a
+// buffer that is not one of its inputs (Ut, R, Ut), so a repeat recomputes it from the same inputs; the accepted
+// candidate is then copied into U. Without repairs the bits are those of the unguarded step.
+cudaError_t enqueue_step_fb(fvg_run* r) {
+    cudaError_t e;
+    Ctl* c = r->ctl;
+    const int* act = &c->active;
+    const int* rep = r->fb_grew;
+    const int nbv = r->cfg.use_viscous ? r->nbv : 0;
+    const int ts = r->cfg.time_scheme;
+    const long long pl = r->m.plane, n = r->m.ncells;
+    const int nv = r->nvar;
+    cudaStream_t s = r->stream;
+    // stage 1: candidate Ut = U + dt R
+    if ((e = residual_stage(r, r->U, nullptr, r->R, kStoreR, 0, 0, 0, act))) return e;
+    k_stage1_dt<<<1, 1024, 0, s>>>(c, r->bm[0], r->nb, r->bmv[0], nbv);
+    k_axpy<<<axpy_blocks(r), 256, 0, s>>>(c, r->Ut, r->U, r->R, pl, n, nv);
+    if ((e = fb_repair(r, r->Ut, [&] {
+             cudaError_t e2 = residual_stage(r, r->U, nullptr, r->R, kStoreR, 0, 0, 0, rep, r->fb_flags);
+             if (e2) return e2;
+             k_axpy_gated<<<axpy_blocks(r), 256, 0, s>>>(rep, c, r->Ut, r->U, r->R, pl, n, nv);
+             return cudaGetLastError();
+         })))
+        return e;
+    const double* accepted = r->Ut;
+    if (ts == FVG_TS_SSPRK2) {   // stage 2: candidate R = 1/2 U + 1/2 (Ut + dt R(Ut))
+        if ((e = residual_stage(r, r->Ut, r->U, r->R, kCombine, 0.5, 0.5, 1, act))) return e;
+        k_stage_max<<<1, 1024, 0, s>>>(c, act, 1, r->bm[1], r->nb, r->bmv[1], nbv);
+        if ((e = fb_repair(r, r->R, [&] { return residual_stage(r, r->Ut, r->U, r->R, kCombine, 0.5, 0.5, 1, rep, r->fb_flags); }))) return e;
+        accepted = r->R;
+    } else if (ts == FVG_TS_SSPRK3) {   // stage 2 into R, stage 3 into Ut
+        if ((e = residual_stage(r, r->Ut, r->U, r->R, kCombine, 0.75, 0.25, 1, act))) return e;
+        k_stage_max<<<1, 1024, 0, s>>>(c, act, 1, r->bm[1], r->nb, r->bmv[1], nbv);
+        if ((e = fb_repair(r, r->R, [&] { return residual_stage(r, r->Ut, r->U, r->R, kCombine, 0.75, 0.25, 1, rep, r->fb_flags); }))) return e;
+        if ((e = residual_stage(r, r->R, r->U, r->Ut, kCombine, 1.0 / 3.0, 2.0 / 3.0, 2, act))) return e;
+        k_stage_max<<<1, 1024, 0, s>>>(c, act, 2, r->bm[2], r->nb, r->bmv[2], nbv);
+        if ((e = fb_repair(r, r->Ut, [&] { return residual_stage(r, r->R, r->U, r->Ut, kCombine, 1.0 / 3.0, 2.0 / 3.0, 2, rep, r->fb_flags); })))
+            return e;
+        accepted = r->Ut;
+    }
+    k_copy_planes<<<axpy_blocks(r), 256, 0, s>>>(c, r->U, accepted, pl, n, nv);
+    if (r->ibm && (e = ibm_fill(r, r->U, r->U, 1, act))) return e;
+    k_end_rk<<<1, 1, 0, s>>>(c, ts == FVG_TS_EULER ? 1 : (ts == FVG_TS_SSPRK2 ? 2 : 3));
+    return cudaGetLastError();
+}
+
 // The launches of one time step on the run's stream (no host synchronisation). refresh = false leaves out the sensor's
 // refresh (a graph of sens_every steps keeps it in its first step only).
 cudaError_t enqueue_step(fvg_run* r, bool refresh = true) {
+    if (r->fb_flags) return enqueue_step_fb(r);
     cudaError_t e;
     Ctl* c = r->ctl;
     const int* act = &c->active;
@@ -948,6 +1071,10 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
             g_create_error = "each part needs at least " + std::to_string(depth) + " planes along the split axis";
             return FVG_ERR_CONFIG;
         }
+        if (cfg->positivity_fallback) {   // the flags of the neighbours' cells would have to be exchanged too
+            g_create_error = "a decomposed mesh cannot use positivity_fallback";
+            return FVG_ERR_CONFIG;
+        }
         for (int s = 0; s < 6; ++s)
             if (cfg->bc[s] == FVG_BC_MASSFLOWINLET) {   // its target is a sequential sum over the whole side
                 g_create_error = "a decomposed mesh cannot have a mass-flow inlet";
@@ -1078,6 +1205,13 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
     for (double** p : {&run->U, &run->Ut, &run->R, &run->Rv})
         if (*p) cudaMemsetAsync(*p, 0, sbytes, run->stream), *p += run->goff;
     if (run->xred) cudaMemsetAsync(run->xred, 0, sizeof(double) * 2, run->stream);
+    if (c.positivity_fallback) {
+        if (cudaMalloc(&run->fb_flags, run->m.ncells) != cudaSuccess || cudaMalloc(&run->fb_grew, sizeof(int)) != cudaSuccess) {
+            run->err = "device allocation failed";
+            return bail(FVG_ERR_CUDA);
+        }
+        cudaMemsetAsync(run->fb_flags, 0, run->m.ncells, run->stream);
+    }
     for (int s = 0; s < 2 * (run->dim == 3 ? 3 : 2); ++s)
         if (c.bc[s] == FVG_BC_MASSFLOWINLET && !run->d_utarget) {
             if (cudaMalloc(&run->d_utarget, sizeof(double) * 6) != cudaSuccess) {
@@ -1177,6 +1311,8 @@ int fvg_destroy(fvg_run* run) {
                       run->d_utarget})
         if (p) cudaFree(p);
     if (run->ctl) cudaFree(run->ctl);
+    if (run->fb_flags) cudaFree(run->fb_flags);
+    if (run->fb_grew) cudaFree(run->fb_grew);
     if (run->sens) cudaFree(run->sens);
     if (run->sens_count) cudaFree(run->sens_count);
     for (unsigned char* f : run->sens_flags)

@@ -44,7 +44,23 @@ struct StageArgs {
     // the learned troubled-cell sensor's tile flags (mixed-precision WENO5-Z kernels with the sensor only): one byte per
     // axis and tile (axis-major), 1 where the tile's reconstructions along the axis stay WENO5-Z, 0 where they are linear
     const unsigned char* sens_flags;
+    // positivity_fallback: the cells flagged in this stage (null: none); a face next to one takes the cells' states
+    const unsigned char* fb;
 };
+
+// positivity_fallback's flag of a stencil position (Schemes.cpp:548-557): the cell's; across a periodic seam the wrapped
+// cell's; beyond any other side none (a ghost layer is never flagged).
+template <int DIM> __device__ __forceinline__ bool fb_flagged(const Mesh& m, const Bc& bc, const unsigned char* fb, int i, int j, int k) {
+    int p[3] = {i, j, k};
+    const int n3[3] = {m.nx, m.ny, m.nz};
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+        if (p[a] >= 0 && p[a] < n3[a]) continue;
+        if (bc.halo[2 * a + (p[a] < 0 ? 0 : 1)] != kHaloWrap) return false;
+        p[a] = p[a] < 0 ? p[a] + n3[a] : p[a] - n3[a];
+    }
+    return fb[((long long)p[2] * m.ny + p[1]) * m.nx + p[0]] != 0;
+}
 
 template <int DIM, int RECON, int TX, int TY, int TZ> struct StageShape {
     static constexpr int NV = DIM == 3 ? 5 : 4;
@@ -169,14 +185,22 @@ __device__ __forceinline__ void stage_axis(const StageArgs& a, double* __restric
                         UR[q] = P[q * S::EXT + base + sstride];
                     }
                 } else {
-                    St<double, NV> wl, wr;
+                    int lc[3] = {g3[0], g3[1], g3[2]};
+                    lc[axis] -= 1;
+                    if (a.fb && (fb_flagged<DIM>(m, a.bc, a.fb, lc[0], lc[1], lc[2]) || fb_flagged<DIM>(m, a.bc, a.fb, g3[0], g3[1], g3[2]))) {
+                        // next to a flagged cell: the two cells' states (the ghost of a side's halo beyond it)
+                        UL = stencil_cons<DIM, NV>(m, a.bc, a.eos, a.U, lc[0], lc[1], lc[2]);
+                        UR = stencil_cons<DIM, NV>(m, a.bc, a.eos, a.U, g3[0], g3[1], g3[2]);
+                    } else {
+                        St<double, NV> wl, wr;
 #pragma unroll
-                    for (int q = 0; q < NV; ++q) {
-                        wl[q] = WL[q * S::NF + f];
-                        wr[q] = WR[q * S::NF + f];
+                        for (int q = 0; q < NV; ++q) {
+                            wl[q] = WL[q * S::NF + f];
+                            wr[q] = WR[q * S::NF + f];
+                        }
+                        UL = p2c(a.eos, wl);
+                        UR = p2c(a.eos, wr);
                     }
-                    UL = p2c(a.eos, wl);
-                    UR = p2c(a.eos, wr);
                 }
                 const double s = face_flux<RIEMANN>(a.eos, a.shock_blend, UL, UR, axis, F);
                 if (s > smax) smax = s;

@@ -21,7 +21,7 @@ DEFAULTS = {
     "boundary_order": 2, "time_scheme": "auto", "cfl": 0.5, "shock_blend": 0.2, "dt_max": 0.0, "t_end": 0.005,
     "max_steps": 0,
     "use_ibm": False, "ibm_shape": "Cylinder", "ibm_radius": 0.1, "ibm_cx": 0.5, "ibm_cy": 0.5, "ibm_cz": 0.5, "ibm_curvature": False,
-    "use_bodyforce": False, "gx": 0.0, "gy": -9.81, "gz": 0.0, "nrbc_sigma": 0.28, "nrbc_beta": -1.0,
+    "use_bodyforce": False, "gx": 0.0, "gy": -9.81, "gz": 0.0, "nrbc_sigma": 0.28, "nrbc_beta": -1.0, "positivity_fallback": False,
 }
 
 BC_NAMES = {"wall": 0, "inviscid wall (slip)": 0, "no_slip": 1, "viscous wall (no-slip)": 1, "moving_wall": 2, "moving wall": 2,
@@ -51,7 +51,7 @@ class FvgConfig(ctypes.Structure):
                 ("use_ibm", ctypes.c_int), ("ibm_shape", ctypes.c_int), ("ibm_radius", ctypes.c_double), ("ibm_cx", ctypes.c_double),
                 ("ibm_cy", ctypes.c_double), ("ibm_cz", ctypes.c_double), ("ibm_curvature", ctypes.c_int),
                 ("use_bodyforce", ctypes.c_int), ("gx", ctypes.c_double), ("gy", ctypes.c_double), ("gz", ctypes.c_double),
-                ("nrbc_sigma", ctypes.c_double), ("nrbc_beta", ctypes.c_double)]
+                ("nrbc_sigma", ctypes.c_double), ("nrbc_beta", ctypes.c_double), ("positivity_fallback", ctypes.c_int)]
 
 
 def _flag(v):
@@ -94,8 +94,8 @@ def _num(v):
 
 def not_on_device(params):
     """The reference features a parameter dict switches on that the device path does not compute (None: none). They
-    are refused, never ignored: AMR, case-file source expressions (source_* evaluated per cell and stage), the
-    positivity fallback, fourth-order flux quadrature, time tables of the inlet / outlet values, reynolds (mu derived from
+    are refused, never ignored: AMR, case-file source expressions (source_* evaluated per cell and stage),
+    fourth-order flux quadrature, time tables of the inlet / outlet values, reynolds (mu derived from
     the body's length scale), and a moving or flow-driven immersed body. (Combinations the device refuses, such as the body
 force with the mixed-precision form, are refused by fvg_create with FVG_ERR_CONFIG.)"""
     p = resolve(params)
@@ -104,8 +104,6 @@ force with the mixed-precision form, are refused by fvg_create with FVG_ERR_CONF
     src = [k for k in ("source_rho", "source_mx", "source_my", "source_mz", "source_E") if _num(p.get(k, 0)) != 0.0]
     if src:
         return "case-file source terms (" + ", ".join(src) + ")"
-    if _flag(p.get("positivity_fallback", False)):
-        return "the positivity fallback"
     if str(p.get("flux_quadrature", "midpoint")).strip().lower() != "midpoint":
         return "fourth-order flux quadrature"
     tables = [k for k in p if k.endswith("_table") and str(p[k]).strip()]
@@ -156,6 +154,7 @@ def to_config(params, precision=0, device=0):
     c.use_bodyforce = 1 if _flag(p["use_bodyforce"]) else 0
     c.gx, c.gy, c.gz = float(p["gx"]), float(p["gy"]), float(p["gz"])
     c.nrbc_sigma, c.nrbc_beta = float(p["nrbc_sigma"]), float(p["nrbc_beta"])
+    c.positivity_fallback = 1 if _flag(p["positivity_fallback"]) else 0
     return c
 
 

@@ -38,7 +38,7 @@ EXPORTS = ["fvg_abi_version", "fvg_create", "fvg_destroy", "fvg_last_error", "fv
            "fvg_create_part", "fvg_part_info", "fvg_part_buffers", "fvg_part_begin", "fvg_part_phase", "fvg_part_status"]
 
 _lib = None
-ABI_VERSION = 3   # FVG_ABI_VERSION of include/fenice_gpu.h
+ABI_VERSION = 4   # FVG_ABI_VERSION of include/fenice_gpu.h
 
 
 def load_library(path=LIB_PATH):

@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define FVG_ABI_VERSION 3
+#define FVG_ABI_VERSION 4
 
 /* status codes */
 enum {
@@ -76,6 +76,8 @@ typedef struct fvg_config {
     int use_bodyforce;           /* [physics] use_bodyforce: the constant body force (ConstantBodyForce, Physics.cpp:832-844) */
     double gx, gy, gz;           /* [physics] gx, gy, gz (gz is not used on a 2-D mesh) */
     double nrbc_sigma, nrbc_beta; /* [boundaries] the non-reflecting outlet's relaxation (0.28) and transverse weight (-1: local Mach) */
+    int positivity_fallback;     /* [numerics] positivity_fallback: a stage that leaves a cell without density or pressure is
+                                    repeated with first-order faces around it (WENO3-Z / WENO5-Z, FP64) */
 } fvg_config;
 
 typedef struct fvg_run fvg_run;

@@ -79,6 +79,7 @@ static fvg_config to_fvg(const fv::SimParams& p) {
     c.gz = p.gz;
     c.nrbc_sigma = p.nrbc_sigma;
     c.nrbc_beta = p.nrbc_beta;
+    c.positivity_fallback = p.positivity_fallback ? 1 : 0;
     return c;
 }
 

@@ -217,3 +217,42 @@ FORCE_CASES = [
     ("nrbc_weno5_visc_3d", dict(nx=12, ny=10, nz=9, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", use_viscous=True, mu=0.01, nrbc_sigma=0.5,
                                 **bcs("transmissive", "nonreflecting", "no_slip", "wall", z=("nonreflecting", "nonreflecting"))), 64, 0.0, 3),
 ]
+
+
+# positivity_fallback (a stage that leaves a cell without density or pressure is repeated with first-order faces around
+# it): (name, params, initial state (name, arguments), n_steps). The first two need repairs (the reference diverges
+# without the guard); the last two have none (the guarded run has the unguarded bits).
+def double_rarefaction(nx, ny, u0, p):
+    x = (np.tile(np.arange(nx), ny) + 0.5) / nx
+    W = np.zeros((nx * ny, 5))
+    W[:, 0] = 1.0
+    W[:, 3] = p
+    W[:, 1] = np.where(x < 0.5, -u0, u0)
+    return prim_to_cons(W)
+
+
+def blast(nx, ny, nz, p_in, p_out=1e-3):
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    x, y, z = (i.ravel() + 0.5) / nx, (j.ravel() + 0.5) / ny, (k.ravel() + 0.5) / max(nz, 1)
+    r2 = (x - 0.5) ** 2 + (y - 0.5) ** 2 + ((z - 0.5) ** 2 if nz > 1 else 0.0)
+    W = np.zeros((nx * ny * nz, 5))
+    W[:, 0] = 1.0
+    W[:, 3] = np.where(r2 < 0.01, p_in, p_out)
+    return prim_to_cons(W)
+
+
+FALLBACK_CASES = [
+    ("fb_double_rarefaction_w5", dict(nx=64, ny=4, Ly=1 / 16, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", positivity_fallback=True,
+                                      **bcs("transmissive", "transmissive", "periodic", "periodic")), ("double_rarefaction", (64, 4, 3.5, 0.1)), 40),
+    ("fb_blast_w5_3d", dict(nx=16, ny=16, nz=16, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", cfl=0.6, positivity_fallback=True,
+                            **bcs("periodic", "periodic", "periodic", "periodic")), ("blast", (16, 16, 16, 1e5)), 10),
+    ("fb_none_w3_euler", dict(nx=64, ny=4, Ly=1 / 16, reconstruction="weno3", time_scheme="Explicit Euler", cfl=0.3, positivity_fallback=True,
+                              **bcs("transmissive", "wall", "periodic", "periodic")), ("double_rarefaction", (64, 4, 2.0, 0.4)), 30),
+    ("fb_none_w5_rk3_walls", dict(nx=40, ny=40, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", cfl=0.5, positivity_fallback=True,
+                                  **bcs("wall", "wall", "wall", "wall")), ("blast", (40, 40, 1, 1e3)), 12),
+]
+
+
+def fallback_state(spec):
+    name, args = spec
+    return double_rarefaction(*args) if name == "double_rarefaction" else blast(*args)

@@ -11,9 +11,11 @@ the seeded inputs of tests/cases.py and stores, per case, the parameters, the in
   visc2d.npz     2-D viscous cases (NavierStokes::viscous_residual_rows): a residual, then a few steps
   hancock3d.npz  3-D MUSCL-Hancock (MusclReconstruction::hancock_residual_3d): residuals with the predictor, then steps
   forces.npz     the body force (ConstantBodyForce) and MUSCL-Hancock with viscous fluxes: a residual, then steps
+  fallback.npz   positivity_fallback: steps of problems that need repairs (and of two that need none), with and without the
+                 guard (the unguarded reference diverges on the first two)
   riemann.json   the reference's bench_riemann fingerprints over one pass of its 65536 state pairs
                  (oracle/_ref/bench_riemann 65536)
-Sections can be named on the command line (residuals steps ibm visc2d hancock3d forces riemann); default: all.
+Sections can be named on the command line (residuals steps ibm visc2d hancock3d forces fallback riemann); default: all.
 The fixtures are test data: nothing of the product reads them.
 """
 import json
@@ -100,13 +102,40 @@ def forces():
     np.savez_compressed(os.path.join(HERE, "forces.npz"), **out)
 
 
-def main(sections=("residuals", "steps", "ibm", "visc2d", "hancock3d", "forces", "riemann")):
+def fallback():
+    out = {}
+    for name, params, spec, n in cases.FALLBACK_CASES:
+        U = cases.fallback_state(spec)
+        ref = Reference(params, initial_state=(1, 0, 0, 1, 0))
+        ref.set_state(U)
+        dts, sms = ref.steps(n, 1e30)
+        out[f"{name}/params"] = np.array(json.dumps(params))
+        out[f"{name}/U0"] = U
+        out[f"{name}/U"] = ref.state()
+        out[f"{name}/dts"] = dts
+        out[f"{name}/smaxs"] = sms
+        out[f"{name}/t"] = np.array(ref.t)
+        plain = Reference(dict(params, positivity_fallback=False), initial_state=(1, 0, 0, 1, 0))
+        plain.set_state(U)
+        try:
+            plain.steps(n, 1e30)
+            unguarded = "same" if np.array_equal(plain.state().view(np.uint64), ref.state().view(np.uint64)) else "differs"
+        except RuntimeError:
+            unguarded = "diverges"
+        out[f"{name}/unguarded"] = np.array(unguarded)
+        print(f"fallback {name}: {len(dts)} steps, t = {ref.t:.6g}; without the guard the reference {unguarded}")
+    np.savez_compressed(os.path.join(HERE, "fallback.npz"), **out)
+
+
+def main(sections=("residuals", "steps", "ibm", "visc2d", "hancock3d", "forces", "fallback", "riemann")):
     if "visc2d" in sections:
         visc2d()
     if "hancock3d" in sections:
         hancock3d()
     if "forces" in sections:
         forces()
+    if "fallback" in sections:
+        fallback()
     if "residuals" in sections:
         residuals()
     if "steps" in sections:
@@ -186,4 +215,4 @@ def riemann():
 
 
 if __name__ == "__main__":
-    main(tuple(sys.argv[1:]) or ("residuals", "steps", "ibm", "visc2d", "hancock3d", "forces", "riemann"))
+    main(tuple(sys.argv[1:]) or ("residuals", "steps", "ibm", "visc2d", "hancock3d", "forces", "fallback", "riemann"))
