@@ -67,6 +67,8 @@ __device__ __forceinline__ void batch_item_args(const BatchArgs& b, const BatchP
     sa.blockmax = nullptr;
     sa.ctl = nullptr;
     sa.gate = nullptr;
+    sa.sens_flags = nullptr;   // (shared memory is not initialised: every pointer a stage sweep may test is set here)
+    sa.fb = nullptr;
 }
 
 // a problem's stage maximum: the reference's rule `if (s > local) local = s` (a NaN or a zero never enters)
