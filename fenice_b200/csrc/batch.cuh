@@ -101,7 +101,7 @@ __device__ __forceinline__ void thin_y_fp64(const StageArgs& a, double* __restri
         const int i = o3[0] + c;
         if (i >= m.nx) continue;
         St<double, 4> UL, UR, Fb, Ft;
-        side_states<4>(m, a.bc, a.eos, a.U, 2, i, 0, 0, UL, UR);
+        side_states<4, false>(m, a.bc, a.eos, a.U, 2, i, 0, 0, UL, UR);
         if constexpr (RECON != kFirstOrder) {
             UL = round_trip(a.eos, UL);
             UR = round_trip(a.eos, UR);
@@ -111,7 +111,7 @@ __device__ __forceinline__ void thin_y_fp64(const StageArgs& a, double* __restri
         if (same) {
             Ft = Fb;
         } else {
-            side_states<4>(m, a.bc, a.eos, a.U, 3, i, 0, 0, UL, UR);
+            side_states<4, false>(m, a.bc, a.eos, a.U, 3, i, 0, 0, UL, UR);
             if constexpr (RECON != kFirstOrder) {
                 UL = round_trip(a.eos, UL);
                 UR = round_trip(a.eos, UR);
@@ -152,13 +152,13 @@ __global__ void __launch_bounds__(NT) batch_stage_kernel(const BatchArgs b) {
         const int tx = (m.nx + TX - 1) / TX;
         const int o3[3] = {(it.tile % tx) * TX, (it.tile / tx) * TY, 0};
         double smax = 0.0;
-        stage_axis<0, 2, RECON, RIEMANN, TX, TY, 1, NT>(sa, P, WL, WR, acc, Sf, o3, smax);
+        stage_axis<0, 2, RECON, RIEMANN, TX, TY, 1, NT, false>(sa, P, WL, WR, acc, Sf, o3, smax);
         bool thin = false;
         if constexpr (TY == 1) thin = thin_y(m, sa.bc);
         if (thin)
             thin_y_fp64<RECON, RIEMANN, TX, NT>(sa, acc, o3, smax);
         else
-            stage_axis<1, 2, RECON, RIEMANN, TX, TY, 1, NT>(sa, P, WL, WR, acc, Sf, o3, smax);
+            stage_axis<1, 2, RECON, RIEMANN, TX, TY, 1, NT, false>(sa, P, WL, WR, acc, Sf, o3, smax);
         const double dt = b.ctl[it.prob].dt;
         for (int c = tid; c < NC; c += NT) {
             const int i = o3[0] + c % TX, j = o3[1] + c / TX;

@@ -12,7 +12,7 @@ namespace {
 template <int RIEMANN>
 __device__ __forceinline__ float thin_face_mixed(const StageArgs& a, const Eos<float>& ef, float sb, int side, int i, St<float, 4>& F) {
     St<double, 4> UL, UR;
-    side_states<4>(a.m, a.bc, a.eos, a.U, side, i, 0, 0, UL, UR);
+    side_states<4, false>(a.m, a.bc, a.eos, a.U, side, i, 0, 0, UL, UR);
     const St<double, 4> dl = c2p(a.eos, UL), dr = c2p(a.eos, UR);
     St<float, 4> wl, wr;
 #pragma unroll
@@ -73,13 +73,13 @@ __global__ void __launch_bounds__(NT) batch_mixed_kernel(const BatchArgs b) {
         const int tx = (m.nx + TX - 1) / TX;
         const int o3[3] = {(it.tile % tx) * TX, (it.tile / tx) * TY, 0};
         float smax = 0.0f;
-        mixed_axis<0, 2, RECON, RIEMANN, TX, TY, 1, NT>(sa, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
+        mixed_axis<0, 2, RECON, RIEMANN, TX, TY, 1, NT, false, false>(sa, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
         bool thin = false;
         if constexpr (TY == 1) thin = thin_y(m, sa.bc);
         if (thin)
             thin_y_mixed<RIEMANN, TX, NT>(sa, ef, sb, acc, o3, smax);
         else
-            mixed_axis<1, 2, RECON, RIEMANN, TX, TY, 1, NT>(sa, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
+            mixed_axis<1, 2, RECON, RIEMANN, TX, TY, 1, NT, false, false>(sa, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
         const double dt = b.ctl[it.prob].dt;
         for (int c = tid; c < NC; c += NT) {
             const int i = o3[0] + c % TX, j = o3[1] + c / TX;

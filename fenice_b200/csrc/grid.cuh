@@ -67,7 +67,8 @@ struct Bc {
 
 // Whether position g along an axis of n cells is a cell whose state is in the arrays (a cell of the mesh, or of a
 // neighbouring part's ghost planes beyond a kHaloPeer side), and the wrapped index of a periodic axis otherwise.
-__device__ __forceinline__ bool held(const Bc& bc, int axis, int g, int n) {
+template <bool FULL = true> __device__ __forceinline__ bool held(const Bc& bc, int axis, int g, int n) {
+    if constexpr (!FULL) return g >= 0 && g < n;
     return (g >= 0 && g < n) || (g < 0 && bc.halo[2 * axis] == kHaloPeer && g >= -bc.ext[2 * axis]) ||
            (g >= n && bc.halo[2 * axis + 1] == kHaloPeer && g < n + bc.ext[2 * axis + 1]);
 }
@@ -163,7 +164,10 @@ template <int NV> __device__ __forceinline__ void add_body_force(const Bc& bc, c
 // layer l beyond the side is ghost_state of the interior cell l cells from it), or edge replication (pad_primitives,
 // cpp/src/Schemes.cpp:915-969). Positions outside along two axes (never on a stencil of a face of the mesh) and those of a
 // tile that overhangs the mesh are clamped, so every read is inside the state arrays.
-template <int DIM, int NV>
+//
+// FULL = false: a run without part interfaces (no kHaloPeer side), for the hot kernels (the interface test and the
+// ghost-plane clamp compiled out).
+template <int DIM, int NV, bool FULL = true>
 __device__ __forceinline__ St<double, NV> stencil_cons(const Mesh& m, const Bc& bc, const Eos<double>& e, const double* __restrict__ U, int i, int j,
                                                        int k) {
     int idx[3] = {i, j, k};
@@ -178,7 +182,7 @@ __device__ __forceinline__ St<double, NV> stencil_cons(const Mesh& m, const Bc& 
             idx[a] = ((idx[a] % n3[a]) + n3[a]) % n3[a];
             continue;
         }
-        if (kind == kHaloPeer) continue;   // the neighbouring part's cell (clamped below onto its ghost planes)
+        if (FULL && kind == kHaloPeer) continue;   // the neighbouring part's cell (clamped below onto its ghost planes)
         out_axis = a;
         ++nout;
     }
@@ -196,7 +200,7 @@ __device__ __forceinline__ St<double, NV> stencil_cons(const Mesh& m, const Bc& 
     }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const int lo = -bc.ext[2 * a], hi = n3[a] - 1 + bc.ext[2 * a + 1];
+        const int lo = FULL ? -bc.ext[2 * a] : 0, hi = FULL ? n3[a] - 1 + bc.ext[2 * a + 1] : n3[a] - 1;
         idx[a] = idx[a] < lo ? lo : (idx[a] > hi ? hi : idx[a]);
     }
     const long long c = ((long long)idx[2] * m.ny + idx[1]) * m.nx + idx[0];
@@ -282,17 +286,18 @@ __device__ __forceinline__ St<double, NV> nrbc_ghost(const Mesh& m, const Bc& bc
 }
 
 // The first-order ghost of the cell (i, j, k) next to a side without a halo: ghost_state, or the non-reflecting ghost.
-template <int NV>
+template <int NV, bool FULL = true>
 __device__ __forceinline__ St<double, NV> side_ghost(const Mesh& m, const Bc& bc, const Eos<double>& e, const double* __restrict__ U, int side, int i,
                                                      int j, int k) {
     const St<double, NV> Ui = read_state<NV>(bc, U, m.plane, ((long long)k * m.ny + j) * m.nx + i);
-    if (bc.type[side] == kBcNonReflecting) return nrbc_ghost<NV>(m, bc, e, U, side, i, j, k, Ui);
+    if (FULL && bc.type[side] == kBcNonReflecting) return nrbc_ghost<NV>(m, bc, e, U, side, i, j, k, Ui);
     return ghost_state(e, bc, side, Ui);
 }
 
 // The first-order states of a boundary face whose side has no halo (BoundaryManager::apply_side,
 // cpp/src/Boundaries.cpp:277-373): the cell next to the side and its ghost (the opposite cell on a periodic side).
-template <int NV>
+// (FULL = false: a run without non-reflecting sides, the characteristic ghost compiled out)
+template <int NV, bool FULL = true>
 __device__ __forceinline__ void side_states(const Mesh& m, const Bc& bc, const Eos<double>& e, const double* __restrict__ U, int side, int i, int j, int k,
                                             St<double, NV>& UL, St<double, NV>& UR) {
     const long long c = ((long long)k * m.ny + j) * m.nx + i;
@@ -303,7 +308,7 @@ __device__ __forceinline__ void side_states(const Mesh& m, const Bc& bc, const E
         const int a = side >> 1, n = a == 0 ? m.nx : (a == 1 ? m.ny : m.nz);
         idx[a] = (side & 1) ? idx[a] - (n - 1) : idx[a] + (n - 1);
         Ug = read_state<NV>(bc, U, m.plane, ((long long)idx[2] * m.ny + idx[1]) * m.nx + idx[0]);
-    } else if (bc.type[side] == kBcNonReflecting) {
+    } else if (FULL && bc.type[side] == kBcNonReflecting) {
         Ug = nrbc_ghost<NV>(m, bc, e, U, side, i, j, k, Ui);
     } else {
         Ug = ghost_state(e, bc, side, Ui);

@@ -74,7 +74,8 @@ template <int NV> __device__ __forceinline__ St<double, NV> body_source(const Bc
     return src;
 }
 
-template <int RIEMANN, int TX, int TY, int NT>
+// FULL = false: a run without part interfaces, non-reflecting sides or the body force (their code compiled out)
+template <int RIEMANN, int TX, int TY, int NT, bool FULL = true>
 __global__ void __launch_bounds__(NT) hancock_kernel(const HancockArgs a) {
     using S = HancockShape<TX, TY>;
     constexpr int PX = S::PX, PY = S::PY, BX = S::BX, BY = S::BY, NB = BX * BY, NP = PX * PY, NC = TX * TY;
@@ -96,7 +97,7 @@ __global__ void __launch_bounds__(NT) hancock_kernel(const HancockArgs a) {
     // ---- 1. primitive box: cells ox-2 .. ox+TX+1, oy-2 .. oy+TY+1
     for (int p = tid; p < NP; p += NT) {
         const int i = ox + p % PX - 2, j = oy + p / PX - 2;
-        const St<double, 4> w = c2p(e, stencil_cons<2, 4>(m, a.bc, e, a.U, i, j, 0));
+        const St<double, 4> w = c2p(e, stencil_cons<2, 4, FULL>(m, a.bc, e, a.U, i, j, 0));
 #pragma unroll
         for (int q = 0; q < 4; ++q) P[q * NP + p] = w[q];
     }
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(NT) hancock_kernel(const HancockArgs a) {
             st[2 * ax] = p2c(e, wr);
         }
         // a real cell: of the mesh, of a periodic wrap, or of the neighbouring part beyond a part interface
-        const bool real = gi >= -1 && gi <= nx && gj >= -1 && gj <= ny && (wrap_x || held(a.bc, 0, gi, nx)) && (wrap_y || held(a.bc, 1, gj, ny));
+        const bool real = gi >= -1 && gi <= nx && gj >= -1 && gj <= ny && (wrap_x || held<FULL>(a.bc, 0, gi, nx)) && (wrap_y || held<FULL>(a.bc, 1, gj, ny));
         if (real) {
             // the mesh cell (wrapped): sides without a halo give it the round trip of its own state there
             const int ci = wrap_x ? (gi + nx) % nx : gi, cj = wrap_y ? (gj + ny) % ny : gj;
@@ -153,7 +154,7 @@ __global__ void __launch_bounds__(NT) hancock_kernel(const HancockArgs a) {
                 St<double, 4> d;
 #pragma unroll
                 for (int q = 0; q < 4; ++q) d[q] = hx * (fxr[q] - fxl[q]) + hy * (fyt[q] - fyb[q]);
-                if (a.bc.grav_on) {   // the body force joins the predictor: d - half_dt src
+                if (FULL && a.bc.grav_on) {   // the body force joins the predictor: d - half_dt src
                     const St<double, 4> src = body_source<4>(a.bc, read_state<4>(a.bc, a.U, m.plane, (long long)cj * nx + ci));
 #pragma unroll
                     for (int q = 0; q < 4; ++q) d[q] = d[q] - half_dt * src[q];
@@ -206,14 +207,14 @@ __global__ void __launch_bounds__(NT) hancock_kernel(const HancockArgs a) {
                     if (wall_lo)
                         UL = ghost_state(e, a.bc, lo_side, UR);
                     else if (a.bc.halo[lo_side] == kHaloNone)
-                        UL = round_trip(e, side_ghost<4>(m, a.bc, e, a.U, lo_side, gi, gj, 0));
+                        UL = round_trip(e, side_ghost<4, FULL>(m, a.bc, e, a.U, lo_side, gi, gj, 0));
                 }
                 if (t == n_a) {
                     const int ci = axis == 0 ? nx - 1 : gi, cj = axis == 0 ? gj : ny - 1;
                     if (wall_hi)
                         UR = ghost_state(e, a.bc, hi_side, UL);
                     else if (a.bc.halo[hi_side] == kHaloNone)
-                        UR = round_trip(e, side_ghost<4>(m, a.bc, e, a.U, hi_side, ci, cj, 0));
+                        UR = round_trip(e, side_ghost<4, FULL>(m, a.bc, e, a.U, hi_side, ci, cj, 0));
                 }
                 const double s = face_flux<RIEMANN>(e, a.shock_blend, UL, UR, axis, F);
                 if (s > smax) smax = s;
@@ -246,7 +247,7 @@ __global__ void __launch_bounds__(NT) hancock_kernel(const HancockArgs a) {
             r[q] = acc[q * NC + c] * m.inv_cell;
             if (a.Rv) r[q] = r[q] + a.Rv[q * m.plane + cell];
         }
-        if (a.bc.grav_on) {
+        if (FULL && a.bc.grav_on) {
             const St<double, 4> src = body_source<4>(a.bc, read_state<4>(a.bc, a.U, m.plane, cell));
 #pragma unroll
             for (int q = 0; q < 4; ++q) r[q] = r[q] + src[q];
@@ -308,7 +309,7 @@ __device__ __forceinline__ bool admissible3(const Eos<double>& e, const St<doubl
     return 0.5 * (U[1] * U[1] + U[2] * U[2] + U[4] * U[4]) < U[0] * (U[3] - e.p_inf);
 }
 
-template <int RIEMANN, int TX, int TY, int TZ, int NT>
+template <int RIEMANN, int TX, int TY, int TZ, int NT, bool FULL = true>
 __global__ void __launch_bounds__(NT) hancock3d_kernel(const HancockArgs a) {
     using S = Hancock3Shape<TX, TY, TZ>;
     constexpr int PX = S::PX, PY = S::PY, NP = S::NP, DX = S::DX, DY = S::DY, ND = S::ND, NC = S::NC;
@@ -335,7 +336,7 @@ __global__ void __launch_bounds__(NT) hancock3d_kernel(const HancockArgs a) {
     // ---- 1. primitive box
     for (int p = tid; p < NP; p += NT) {
         const int i = o3[0] + p % PX - 2, j = o3[1] + (p / PX) % PY - 2, k = o3[2] + p / (PX * PY) - 2;
-        const St<double, 5> w = c2p(e, stencil_cons<3, 5>(m, a.bc, e, a.U, i, j, k));
+        const St<double, 5> w = c2p(e, stencil_cons<3, 5, FULL>(m, a.bc, e, a.U, i, j, k));
 #pragma unroll
         for (int q = 0; q < 5; ++q) P[q * NP + p] = w[q];
     }
@@ -360,7 +361,7 @@ __global__ void __launch_bounds__(NT) hancock3d_kernel(const HancockArgs a) {
         bool real = true;
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            real = real && g[d] >= -1 && g[d] <= n3[d] && (wrap[d] || held(a.bc, d, g[d], n3[d]));
+            real = real && g[d] >= -1 && g[d] <= n3[d] && (wrap[d] || held<FULL>(a.bc, d, g[d], n3[d]));
             c3[d] = wrap[d] ? (g[d] + n3[d]) % n3[d] : g[d];
         }
         if (real) {
@@ -385,7 +386,7 @@ __global__ void __launch_bounds__(NT) hancock3d_kernel(const HancockArgs a) {
             int c3[3];
 #pragma unroll
             for (int x = 0; x < 3; ++x) {
-                real = real && g[x] >= -1 && g[x] <= n3[x] && (wrap[x] || held(a.bc, x, g[x], n3[x]));
+                real = real && g[x] >= -1 && g[x] <= n3[x] && (wrap[x] || held<FULL>(a.bc, x, g[x], n3[x]));
                 c3[x] = wrap[x] ? (g[x] + n3[x]) % n3[x] : g[x];
             }
             const unsigned char* sol = a.bc.solid;
@@ -399,7 +400,7 @@ __global__ void __launch_bounds__(NT) hancock3d_kernel(const HancockArgs a) {
                 const St<double, 5> fzf = euler_flux3(e, st[4], 2), fzk = euler_flux3(e, st[5], 2);
 #pragma unroll
                 for (int q = 0; q < 5; ++q) d[q] = (hx * (fxr[q] - fxl[q]) + hy * (fyt[q] - fyb[q])) + hz * (fzk[q] - fzf[q]);
-                if (a.bc.grav_on) {
+                if (FULL && a.bc.grav_on) {
                     const St<double, 5> src = body_source<5>(a.bc, read_state<5>(a.bc, a.U, m.plane, cell_of(c3[0], c3[1], c3[2])));
 #pragma unroll
                     for (int q = 0; q < 5; ++q) d[q] = d[q] - half_dt * src[q];
@@ -460,7 +461,7 @@ __global__ void __launch_bounds__(NT) hancock3d_kernel(const HancockArgs a) {
                     if (wall_lo)
                         UL = ghost_state(e, a.bc, lo_side, UR);
                     else if (a.bc.halo[lo_side] == kHaloNone)
-                        UL = round_trip(e, side_ghost<5>(m, a.bc, e, a.U, lo_side, g3[0], g3[1], g3[2]));
+                        UL = round_trip(e, side_ghost<5, FULL>(m, a.bc, e, a.U, lo_side, g3[0], g3[1], g3[2]));
                 }
                 if (t == n3[AX]) {
                     int c3[3] = {g3[0], g3[1], g3[2]};
@@ -468,7 +469,7 @@ __global__ void __launch_bounds__(NT) hancock3d_kernel(const HancockArgs a) {
                     if (wall_hi)
                         UR = ghost_state(e, a.bc, hi_side, UL);
                     else if (a.bc.halo[hi_side] == kHaloNone)
-                        UR = round_trip(e, side_ghost<5>(m, a.bc, e, a.U, hi_side, c3[0], c3[1], c3[2]));
+                        UR = round_trip(e, side_ghost<5, FULL>(m, a.bc, e, a.U, hi_side, c3[0], c3[1], c3[2]));
                 }
                 const double s = face_flux<RIEMANN>(e, a.shock_blend, UL, UR, AX, F);
                 if (s > smax) smax = s;
@@ -505,7 +506,7 @@ __global__ void __launch_bounds__(NT) hancock3d_kernel(const HancockArgs a) {
             r[q] = acc[q * NC + c] * m.inv_cell;
             if (a.Rv) r[q] = r[q] + a.Rv[q * m.plane + cell];
         }
-        if (a.bc.grav_on) {
+        if (FULL && a.bc.grav_on) {
             const St<double, 5> src = body_source<5>(a.bc, read_state<5>(a.bc, a.U, m.plane, cell));
 #pragma unroll
             for (int q = 0; q < 5; ++q) r[q] = r[q] + src[q];

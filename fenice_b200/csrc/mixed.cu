@@ -10,54 +10,60 @@ template <int DIM> struct MTile;
 template <> struct MTile<3> { static constexpr int X = 8, Y = 8, Z = 8, NT = 192; };
 template <> struct MTile<2> { static constexpr int X = 16, Y = 15, Z = 1, NT = 256; };
 
-template <int DIM, int RECON, int RIEMANN> struct MixedK {
+template <int DIM, int RECON, int RIEMANN, bool FULL> struct MixedK {
     using T = MTile<DIM>;
     using S = MixedShape<DIM, RECON, T::X, T::Y, T::Z>;
     static cudaError_t prepare() {
-        return cudaFuncSetAttribute(mixed_stage_kernel<DIM, RECON, RIEMANN, T::X, T::Y, T::Z, T::NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)S::SMEM_BYTES);
+        return cudaFuncSetAttribute(mixed_stage_kernel<DIM, RECON, RIEMANN, T::X, T::Y, T::Z, T::NT, false, FULL>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM_BYTES);
     }
     static cudaError_t launch(const StageArgs& a, int nblocks, cudaStream_t s) {
-        mixed_stage_kernel<DIM, RECON, RIEMANN, T::X, T::Y, T::Z, T::NT><<<nblocks, T::NT, S::SMEM_BYTES, s>>>(a);
+        mixed_stage_kernel<DIM, RECON, RIEMANN, T::X, T::Y, T::Z, T::NT, false, FULL><<<nblocks, T::NT, S::SMEM_BYTES, s>>>(a);
         return cudaGetLastError();
     }
 };
 
 // the WENO5-Z kernels gated by the learned sensor
-template <int DIM, int RIEMANN> struct GatedK {
+template <int DIM, int RIEMANN, bool FULL> struct GatedK {
     using T = MTile<DIM>;
     using S = MixedShape<DIM, kWeno5, T::X, T::Y, T::Z>;
     static cudaError_t prepare() {
-        return cudaFuncSetAttribute(mixed_stage_kernel<DIM, kWeno5, RIEMANN, T::X, T::Y, T::Z, T::NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)S::SMEM_BYTES);
+        return cudaFuncSetAttribute(mixed_stage_kernel<DIM, kWeno5, RIEMANN, T::X, T::Y, T::Z, T::NT, true, FULL>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM_BYTES);
     }
     static cudaError_t launch(const StageArgs& a, int nblocks, cudaStream_t s) {
-        mixed_stage_kernel<DIM, kWeno5, RIEMANN, T::X, T::Y, T::Z, T::NT, true><<<nblocks, T::NT, S::SMEM_BYTES, s>>>(a);
+        mixed_stage_kernel<DIM, kWeno5, RIEMANN, T::X, T::Y, T::Z, T::NT, true, FULL><<<nblocks, T::NT, S::SMEM_BYTES, s>>>(a);
         return cudaGetLastError();
     }
 };
 
-template <int DIM, int RECON> MixedStage pick_r(int riemann) {
-    if (riemann == kLowMach) return {MixedK<DIM, RECON, kLowMach>::prepare, MixedK<DIM, RECON, kLowMach>::launch};
-    return {MixedK<DIM, RECON, kHLLC>::prepare, MixedK<DIM, RECON, kHLLC>::launch};
+template <int DIM, int RECON, bool FULL> MixedStage pick_r(int riemann) {
+    if (riemann == kLowMach) return {MixedK<DIM, RECON, kLowMach, FULL>::prepare, MixedK<DIM, RECON, kLowMach, FULL>::launch};
+    return {MixedK<DIM, RECON, kHLLC, FULL>::prepare, MixedK<DIM, RECON, kHLLC, FULL>::launch};
 }
-template <int DIM> MixedStage pick(int recon, int riemann) {
+template <int DIM, bool FULL> MixedStage pick(int recon, int riemann) {
     switch (recon) {
-    case kMuscl: return pick_r<DIM, kMuscl>(riemann);
-    case kWeno3: return pick_r<DIM, kWeno3>(riemann);
-    default: return pick_r<DIM, kWeno5>(riemann);
+    case kMuscl: return pick_r<DIM, kMuscl, FULL>(riemann);
+    case kWeno3: return pick_r<DIM, kWeno3, FULL>(riemann);
+    default: return pick_r<DIM, kWeno5, FULL>(riemann);
     }
+}
+template <int DIM, bool FULL> MixedStage pick_gated(int riemann) {
+    return riemann == kLowMach ? MixedStage{GatedK<DIM, kLowMach, FULL>::prepare, GatedK<DIM, kLowMach, FULL>::launch}
+                               : MixedStage{GatedK<DIM, kHLLC, FULL>::prepare, GatedK<DIM, kHLLC, FULL>::launch};
 }
 
 }   // namespace
 
-MixedStage mixed_stage(int dim, int recon, int riemann) { return dim == 3 ? pick<3>(recon, riemann) : pick<2>(recon, riemann); }
+// full: the kernels with the code of part interfaces and non-reflecting sides; else the lean instantiation
+MixedStage mixed_stage(int dim, int recon, int riemann, bool full) {
+    if (dim == 3) return full ? pick<3, true>(recon, riemann) : pick<3, false>(recon, riemann);
+    return full ? pick<2, true>(recon, riemann) : pick<2, false>(recon, riemann);
+}
 
-MixedStage mixed_stage_gated(int dim, int riemann) {
-    if (dim == 3) return riemann == kLowMach ? MixedStage{GatedK<3, kLowMach>::prepare, GatedK<3, kLowMach>::launch}
-                                             : MixedStage{GatedK<3, kHLLC>::prepare, GatedK<3, kHLLC>::launch};
-    return riemann == kLowMach ? MixedStage{GatedK<2, kLowMach>::prepare, GatedK<2, kLowMach>::launch}
-                               : MixedStage{GatedK<2, kHLLC>::prepare, GatedK<2, kHLLC>::launch};
+MixedStage mixed_stage_gated(int dim, int riemann, bool full) {
+    if (dim == 3) return full ? pick_gated<3, true>(riemann) : pick_gated<3, false>(riemann);
+    return full ? pick_gated<2, true>(riemann) : pick_gated<2, false>(riemann);
 }
 
 cudaError_t mixed_viscous_prepare() {

@@ -75,7 +75,7 @@ template <int DIM, int RECON, int TX, int TY, int TZ> struct MixedShape {
 // One axis of the tile sweep of mixed_stage_kernel (compile-time extents).
 // GATED (WENO5-Z with the learned sensor): the tile's flag for this axis (one byte per tile and axis, from the sensor's
 // last refresh) makes every reconstruction of the sweep linear (0) or WENO5-Z (1); the branch is uniform over the CTA.
-template <int AXIS, int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT, bool GATED = false>
+template <int AXIS, int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT, bool GATED = false, bool FULL = true>
 __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>& ef, float sb, float weps, float* __restrict__ P,
                                            float* __restrict__ WL, float* __restrict__ WR, float* __restrict__ acc, unsigned char* __restrict__ Sf,
                                            const int o3[3], float& smax) {
@@ -93,7 +93,7 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
         for (int e = tid; e < nE; e += NT) {
             int l3[3] = {e % E[0], (e / E[0]) % E[1], e / (E[0] * E[1])};
             l3[axis] -= H;
-            const St<double, NV> w = c2p(a.eos, stencil_cons<DIM, NV>(m, a.bc, a.eos, a.U, o3[0] + l3[0], o3[1] + l3[1], o3[2] + l3[2]));
+            const St<double, NV> w = c2p(a.eos, stencil_cons<DIM, NV, FULL>(m, a.bc, a.eos, a.U, o3[0] + l3[0], o3[1] + l3[1], o3[2] + l3[2]));
             if constexpr (RECON == kWeno5)
                 if (a.bc.solid) Sf[e] = stencil_solid<DIM>(m, a.bc, o3[0] + l3[0], o3[1] + l3[1], o3[2] + l3[2]);
 #pragma unroll
@@ -161,7 +161,7 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
                     int c3[3] = {g3[0], g3[1], g3[2]};
                     if (hi_face) c3[axis] = na - 1;
                     St<double, NV> UL, UR;
-                    side_states<NV>(m, a.bc, a.eos, a.U, lo_face ? lo_side : hi_side, c3[0], c3[1], c3[2], UL, UR);
+                    side_states<NV, FULL>(m, a.bc, a.eos, a.U, lo_face ? lo_side : hi_side, c3[0], c3[1], c3[2], UL, UR);
                     const St<double, NV> dl = c2p(a.eos, UL), dr = c2p(a.eos, UR);
 #pragma unroll
                     for (int q = 0; q < NV; ++q) {
@@ -200,7 +200,8 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
 
 // The mixed-precision stage kernel: the tile sweep of stage_kernel (same phases, same launch geometry) with FP32 stencil
 // arithmetic; see the file comment for what stays FP64.
-template <int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT, bool GATED = false>
+// FULL = false: a run without part interfaces or non-reflecting sides (their code compiled out of the hot loop)
+template <int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT, bool GATED = false, bool FULL = true>
 __global__ void __launch_bounds__(NT) mixed_stage_kernel(const StageArgs a) {
     using S = MixedShape<DIM, RECON, TX, TY, TZ>;
     constexpr int NV = S::NV, NC = S::NC;
@@ -218,9 +219,9 @@ __global__ void __launch_bounds__(NT) mixed_stage_kernel(const StageArgs a) {
     const int tid = threadIdx.x, b = blockIdx.x;
     const int o3[3] = {(b % a.tiles[0]) * TX, ((b / a.tiles[0]) % a.tiles[1]) * TY, (b / (a.tiles[0] * a.tiles[1])) * TZ};
     float smax = 0.0f;
-    mixed_axis<0, DIM, RECON, RIEMANN, TX, TY, TZ, NT, GATED>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
-    mixed_axis<1, DIM, RECON, RIEMANN, TX, TY, TZ, NT, GATED>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
-    if constexpr (DIM == 3) mixed_axis<2, DIM, RECON, RIEMANN, TX, TY, TZ, NT, GATED>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
+    mixed_axis<0, DIM, RECON, RIEMANN, TX, TY, TZ, NT, GATED, FULL>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
+    mixed_axis<1, DIM, RECON, RIEMANN, TX, TY, TZ, NT, GATED, FULL>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
+    if constexpr (DIM == 3) mixed_axis<2, DIM, RECON, RIEMANN, TX, TY, TZ, NT, GATED, FULL>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
     // ---- epilogue: the residual widened to FP64 and the FP64 stage update
     const double dt = a.ctl->dt;
     for (int c = tid; c < NC; c += NT) {

@@ -14,10 +14,10 @@ struct MixedStage {
 };
 // the mixed stage kernel for a 2-D or 3-D mesh, a reconstruction (MUSCL, WENO3-Z, WENO5-Z) and a Riemann solver; the
 // launch geometry is the FP64 stage kernel's (3-D: 8x8x8 tiles, 192 threads; 2-D: 16x15 tiles, 256 threads)
-MixedStage mixed_stage(int dim, int recon, int riemann);
+MixedStage mixed_stage(int dim, int recon, int riemann, bool full);
 // the mixed WENO5-Z stage kernel with the learned troubled-cell sensor choosing linear or WENO5-Z reconstructions
 // (StageArgs::sens_flags)
-MixedStage mixed_stage_gated(int dim, int riemann);
+MixedStage mixed_stage_gated(int dim, int riemann, bool full);
 cudaError_t mixed_viscous_prepare();
 cudaError_t mixed_viscous_launch(const ViscArgs& a, int nblocks, cudaStream_t s);
 }   // namespace fvg

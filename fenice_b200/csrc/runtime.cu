@@ -322,15 +322,15 @@ template <> struct Tile<3> { static constexpr int X = 8, Y = 8, Z = 8, NT = 192;
 template <> struct Tile<2> { static constexpr int X = 16, Y = 15, Z = 1, NT = 256; };
 
 // Each kernel gets its shared-memory limit raised once, when a run is created (never during a graph capture).
-template <int DIM, int RECON, int RIEMANN> struct StageK {
+template <int DIM, int RECON, int RIEMANN, bool FULL> struct StageK {
     using Tl = Tile<DIM>;
     using S = StageShape<DIM, RECON, Tl::X, Tl::Y, Tl::Z>;
     static cudaError_t prepare() {
-        return cudaFuncSetAttribute(stage_kernel<DIM, RECON, RIEMANN, Tl::X, Tl::Y, Tl::Z, Tl::NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        return cudaFuncSetAttribute(stage_kernel<DIM, RECON, RIEMANN, Tl::X, Tl::Y, Tl::Z, Tl::NT, FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)S::SMEM_BYTES);
     }
     static cudaError_t launch(const StageArgs& a, int nblocks, cudaStream_t s) {
-        stage_kernel<DIM, RECON, RIEMANN, Tl::X, Tl::Y, Tl::Z, Tl::NT><<<nblocks, Tl::NT, S::SMEM_BYTES, s>>>(a);
+        stage_kernel<DIM, RECON, RIEMANN, Tl::X, Tl::Y, Tl::Z, Tl::NT, FULL><<<nblocks, Tl::NT, S::SMEM_BYTES, s>>>(a);
         return cudaGetLastError();
     }
 };
@@ -340,18 +340,24 @@ struct StageLauncher {
     cudaError_t (*launch)(const StageArgs&, int, cudaStream_t) = nullptr;
 };
 
-template <int DIM, int RECON> StageLauncher stage_launcher_r(int riemann) {
-    if (riemann == kLowMach) return {StageK<DIM, RECON, kLowMach>::prepare, StageK<DIM, RECON, kLowMach>::launch};
-    return {StageK<DIM, RECON, kHLLC>::prepare, StageK<DIM, RECON, kHLLC>::launch};
+template <int DIM, int RECON, bool FULL> StageLauncher stage_launcher_r(int riemann) {
+    if (riemann == kLowMach) return {StageK<DIM, RECON, kLowMach, FULL>::prepare, StageK<DIM, RECON, kLowMach, FULL>::launch};
+    return {StageK<DIM, RECON, kHLLC, FULL>::prepare, StageK<DIM, RECON, kHLLC, FULL>::launch};
 }
 
-template <int DIM> StageLauncher stage_launcher(int recon, int riemann) {
+template <int DIM, bool FULL> StageLauncher stage_launcher_f(int recon, int riemann) {
     switch (recon) {
-    case kFirstOrder: return stage_launcher_r<DIM, kFirstOrder>(riemann);
-    case kMuscl: return stage_launcher_r<DIM, kMuscl>(riemann);
-    case kWeno3: return stage_launcher_r<DIM, kWeno3>(riemann);
-    default: return stage_launcher_r<DIM, kWeno5>(riemann);
+    case kFirstOrder: return stage_launcher_r<DIM, kFirstOrder, FULL>(riemann);
+    case kMuscl: return stage_launcher_r<DIM, kMuscl, FULL>(riemann);
+    case kWeno3: return stage_launcher_r<DIM, kWeno3, FULL>(riemann);
+    default: return stage_launcher_r<DIM, kWeno5, FULL>(riemann);
     }
+}
+
+// full: the run has a part interface, a non-reflecting side, the positivity fallback or the body force (the stage
+// kernels with their code); else the lean instantiation
+template <int DIM> StageLauncher stage_launcher(int recon, int riemann, bool full) {
+    return full ? stage_launcher_f<DIM, true>(recon, riemann) : stage_launcher_f<DIM, false>(recon, riemann);
 }
 
 cudaError_t prepare_viscous() {
@@ -372,19 +378,24 @@ cudaError_t launch_viscous2d(const ViscArgs& a, int nblocks, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-// MUSCL-Hancock tiles: 16 x 16 in 2-D, 8 x 8 x 4 in 3-D (93 KB of shared memory: two CTAs per SM)
-template <int RIEMANN> cudaError_t prepare_hancock_t(int dim) {
+// MUSCL-Hancock tiles: 16 x 16 in 2-D, 8 x 8 x 4 in 3-D (93 KB of shared memory: two CTAs per SM); FULL as the stage kernels
+template <int RIEMANN, bool FULL> cudaError_t prepare_hancock_t(int dim) {
     if (dim == 3)
-        return cudaFuncSetAttribute(hancock3d_kernel<RIEMANN, 8, 8, 4, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        return cudaFuncSetAttribute(hancock3d_kernel<RIEMANN, 8, 8, 4, 256, FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)Hancock3Shape<8, 8, 4>::SMEM_BYTES);
-    return cudaFuncSetAttribute(hancock_kernel<RIEMANN, 16, 16, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HancockShape<16, 16>::SMEM_BYTES);
+    return cudaFuncSetAttribute(hancock_kernel<RIEMANN, 16, 16, 256, FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)HancockShape<16, 16>::SMEM_BYTES);
 }
-template <int RIEMANN> cudaError_t launch_hancock_t(int dim, const HancockArgs& a, int nblocks, cudaStream_t s) {
+template <int RIEMANN, bool FULL> cudaError_t launch_hancock_t(int dim, const HancockArgs& a, int nblocks, cudaStream_t s) {
     if (dim == 3)
-        hancock3d_kernel<RIEMANN, 8, 8, 4, 256><<<nblocks, 256, Hancock3Shape<8, 8, 4>::SMEM_BYTES, s>>>(a);
+        hancock3d_kernel<RIEMANN, 8, 8, 4, 256, FULL><<<nblocks, 256, Hancock3Shape<8, 8, 4>::SMEM_BYTES, s>>>(a);
     else
-        hancock_kernel<RIEMANN, 16, 16, 256><<<nblocks, 256, HancockShape<16, 16>::SMEM_BYTES, s>>>(a);
+        hancock_kernel<RIEMANN, 16, 16, 256, FULL><<<nblocks, 256, HancockShape<16, 16>::SMEM_BYTES, s>>>(a);
     return cudaGetLastError();
+}
+cudaError_t prepare_hancock(int riemann, bool full, int dim) {
+    if (riemann == kLowMach) return full ? prepare_hancock_t<kLowMach, true>(dim) : prepare_hancock_t<kLowMach, false>(dim);
+    return full ? prepare_hancock_t<kHLLC, true>(dim) : prepare_hancock_t<kHLLC, false>(dim);
 }
 
 }   // namespace
@@ -443,6 +454,7 @@ struct fvg_run {
     double* d_utarget = nullptr;   // mass-flow inlets: the target velocity per side (Bc::u_target)
     unsigned char* fb_flags = nullptr;   // positivity_fallback: the cells flagged in the current stage
     int* fb_grew = nullptr;              // and whether the last mark flagged a new one (the repeat's gate)
+    bool full = false;   // the kernels with the code of part interfaces, NRBC, the fallback, the body force
     bool is_part = false;
     int nparts = 1, part = 0, split = 2, first = 0, count = 0, depth = 0, peer[2] = {0, 0};
     long long goff = 0, area = 0, xcount = 0;
@@ -614,8 +626,9 @@ HancockArgs hancock_args(fvg_run* r, const double* Uin, double* out, int mode, d
 }
 
 cudaError_t launch_hancock(fvg_run* r, const HancockArgs& a) {
-    return r->cfg.riemann == FVG_RIEMANN_LOWMACH ? launch_hancock_t<kLowMach>(r->dim, a, r->nbh, r->stream)
-                                                 : launch_hancock_t<kHLLC>(r->dim, a, r->nbh, r->stream);
+    if (r->cfg.riemann == FVG_RIEMANN_LOWMACH)
+        return r->full ? launch_hancock_t<kLowMach, true>(r->dim, a, r->nbh, r->stream) : launch_hancock_t<kLowMach, false>(r->dim, a, r->nbh, r->stream);
+    return r->full ? launch_hancock_t<kHLLC, true>(r->dim, a, r->nbh, r->stream) : launch_hancock_t<kHLLC, false>(r->dim, a, r->nbh, r->stream);
 }
 
 void timer_mark(fvg_run* r, fvg_run::EvTimer& t) {
@@ -1175,9 +1188,12 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
     run->ntiles_h[1] = (c.ny + hx - 1) / hx;
     run->ntiles_h[2] = (c.nz + hz - 1) / hz;
     run->nbh = run->ntiles_h[0] * run->ntiles_h[1] * run->ntiles_h[2];
-    run->stage = run->dim == 3 ? stage_launcher<3>(c.reconstruction, c.riemann) : stage_launcher<2>(c.reconstruction, c.riemann);
+    bool full = run->is_part || c.positivity_fallback || c.use_bodyforce;
+    for (int s = 0; s < 6; ++s) full = full || c.bc[s] == FVG_BC_NONREFLECTING;
+    run->full = full;
+    run->stage = run->dim == 3 ? stage_launcher<3>(c.reconstruction, c.riemann, full) : stage_launcher<2>(c.reconstruction, c.riemann, full);
     if (c.precision == FVG_PREC_MIXED) {
-        const MixedStage ms = mixed_stage(run->dim, c.reconstruction, c.riemann);
+        const MixedStage ms = mixed_stage(run->dim, c.reconstruction, c.riemann, full);
         run->stage.prepare = ms.prepare;
         run->stage.launch = ms.launch;
         if (c.use_viscous && mixed_viscous_prepare() != cudaSuccess) {
@@ -1187,8 +1203,7 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
     }
     // the seed residual of MUSCL-Hancock and every residual use the stage kernel; the viscous and predictor kernels as needed
     if (run->stage.prepare() != cudaSuccess || (c.use_viscous && (run->dim == 3 ? prepare_viscous() : prepare_viscous2d()) != cudaSuccess) ||
-        (c.reconstruction == FVG_RECON_MUSCL &&
-         (c.riemann == FVG_RIEMANN_LOWMACH ? prepare_hancock_t<kLowMach>(run->dim) : prepare_hancock_t<kHLLC>(run->dim)) != cudaSuccess)) {
+        (c.reconstruction == FVG_RECON_MUSCL && prepare_hancock(c.riemann == FVG_RIEMANN_LOWMACH ? kLowMach : kHLLC, full, run->dim) != cudaSuccess)) {
         run->err = "kernel set-up failed (shared-memory limit)";
         return bail(FVG_ERR_CUDA);
     }
@@ -1646,7 +1661,7 @@ int fvg_set_sensor(fvg_run* run, const void* weights, float threshold, int every
         }
     if (!weights) {   // back to plain WENO5-Z
         if (!run->sens) return FVG_OK;
-        const MixedStage ms = mixed_stage(run->dim, run->cfg.reconstruction, run->cfg.riemann);
+        const MixedStage ms = mixed_stage(run->dim, run->cfg.reconstruction, run->cfg.riemann, run->full);
         run->stage.prepare = ms.prepare;
         run->stage.launch = ms.launch;
         cudaFree(run->sens);
@@ -1667,7 +1682,7 @@ int fvg_set_sensor(fvg_run* run, const void* weights, float threshold, int every
         CK(cudaMemset(run->sens_count, 0, 2 * sizeof(unsigned long long)));
     }
     CK(cudaMemcpy(run->sens, weights, sizeof(SensorW), cudaMemcpyDefault));
-    const MixedStage ms = mixed_stage_gated(run->dim, run->cfg.riemann);
+    const MixedStage ms = mixed_stage_gated(run->dim, run->cfg.riemann, run->full);
     if (ms.prepare() != cudaSuccess) return fail(run, FVG_ERR_CUDA, "kernel set-up failed (shared-memory limit)");
     run->stage.prepare = ms.prepare;
     run->stage.launch = ms.launch;
@@ -1823,7 +1838,9 @@ extern "C" int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return noalloc_fail(FVG_ERR_CUDA, "no current CUDA device");
     NoAllocDevice& d = g_noalloc_dev[dev];
-    const StageLauncher launcher = dim == 3 ? stage_launcher<3>(c.reconstruction, c.riemann) : stage_launcher<2>(c.reconstruction, c.riemann);
+    bool full = c.positivity_fallback || c.use_bodyforce;   // (the residual of a whole mesh: no part interface)
+    for (int s = 0; s < 6; ++s) full = full || c.bc[s] == FVG_BC_NONREFLECTING;
+    const StageLauncher launcher = dim == 3 ? stage_launcher<3>(c.reconstruction, c.riemann, full) : stage_launcher<2>(c.reconstruction, c.riemann, full);
     if (!d.ready) {
         // once per device, with that device current: the device address of the scratch array (the host-side name is not one)
         void* p = nullptr;

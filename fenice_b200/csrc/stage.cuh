@@ -82,7 +82,7 @@ template <int DIM, int RECON, int TX, int TY, int TZ> struct StageShape {
 
 // One axis of the tile sweep of stage_kernel (the axis a template parameter, so the extents of the extended tile and of
 // the face grid are compile-time constants).
-template <int AXIS, int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT>
+template <int AXIS, int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT, bool FULL = true>
 __device__ __forceinline__ void stage_axis(const StageArgs& a, double* __restrict__ P, double* __restrict__ WL, double* __restrict__ WR,
                                            double* __restrict__ acc, unsigned char* __restrict__ Sf, const int o3[3], double& smax) {
     using S = StageShape<DIM, RECON, TX, TY, TZ>;
@@ -100,7 +100,7 @@ __device__ __forceinline__ void stage_axis(const StageArgs& a, double* __restric
         for (int e = tid; e < nE; e += NT) {
             int l3[3] = {e % E[0], (e / E[0]) % E[1], e / (E[0] * E[1])};
             l3[axis] -= H;
-            const St<double, NV> u = stencil_cons<DIM, NV>(m, a.bc, a.eos, a.U, o3[0] + l3[0], o3[1] + l3[1], o3[2] + l3[2]);
+            const St<double, NV> u = stencil_cons<DIM, NV, FULL>(m, a.bc, a.eos, a.U, o3[0] + l3[0], o3[1] + l3[1], o3[2] + l3[2]);
             if constexpr (RECON == kWeno5)
                 if (a.bc.solid) Sf[e] = stencil_solid<DIM>(m, a.bc, o3[0] + l3[0], o3[1] + l3[1], o3[2] + l3[2]);
             if constexpr (RECON == kFirstOrder) {
@@ -171,7 +171,7 @@ __device__ __forceinline__ void stage_axis(const StageArgs& a, double* __restric
                 if (lo_face || hi_face) {
                     int c3[3] = {g3[0], g3[1], g3[2]};
                     if (hi_face) c3[axis] = na - 1;
-                    side_states<NV>(m, a.bc, a.eos, a.U, lo_face ? lo_side : hi_side, c3[0], c3[1], c3[2], UL, UR);
+                    side_states<NV, FULL>(m, a.bc, a.eos, a.U, lo_face ? lo_side : hi_side, c3[0], c3[1], c3[2], UL, UR);
                     if constexpr (RECON != kFirstOrder) {
                         UL = round_trip(a.eos, UL);
                         UR = round_trip(a.eos, UR);
@@ -187,7 +187,7 @@ __device__ __forceinline__ void stage_axis(const StageArgs& a, double* __restric
                 } else {
                     int lc[3] = {g3[0], g3[1], g3[2]};
                     lc[axis] -= 1;
-                    if (a.fb && (fb_flagged<DIM>(m, a.bc, a.fb, lc[0], lc[1], lc[2]) || fb_flagged<DIM>(m, a.bc, a.fb, g3[0], g3[1], g3[2]))) {
+                    if (FULL && a.fb && (fb_flagged<DIM>(m, a.bc, a.fb, lc[0], lc[1], lc[2]) || fb_flagged<DIM>(m, a.bc, a.fb, g3[0], g3[1], g3[2]))) {
                         // next to a flagged cell: the two cells' states (the ghost of a side's halo beyond it)
                         UL = stencil_cons<DIM, NV>(m, a.bc, a.eos, a.U, lc[0], lc[1], lc[2]);
                         UR = stencil_cons<DIM, NV>(m, a.bc, a.eos, a.U, g3[0], g3[1], g3[2]);
@@ -226,7 +226,9 @@ __device__ __forceinline__ void stage_axis(const StageArgs& a, double* __restric
         }
 }
 
-template <int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT>
+// FULL = false: a run without part interfaces, non-reflecting sides, the positivity fallback or the body force (their
+// code compiled out of the hot loop: a branch never taken still costs the others registers and instruction fetch).
+template <int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT, bool FULL = true>
 __global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
     using S = StageShape<DIM, RECON, TX, TY, TZ>;
     constexpr int NV = S::NV, NC = S::NC;
@@ -246,9 +248,9 @@ __global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
     const int o3[3] = {t0 * TX, t1 * TY, t2 * TZ};
     double smax = 0.0;
 
-    stage_axis<0, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, P, WL, WR, acc, Sf, o3, smax);
-    stage_axis<1, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, P, WL, WR, acc, Sf, o3, smax);
-    if constexpr (DIM == 3) stage_axis<2, DIM, RECON, RIEMANN, TX, TY, TZ, NT>(a, P, WL, WR, acc, Sf, o3, smax);
+    stage_axis<0, DIM, RECON, RIEMANN, TX, TY, TZ, NT, FULL>(a, P, WL, WR, acc, Sf, o3, smax);
+    stage_axis<1, DIM, RECON, RIEMANN, TX, TY, TZ, NT, FULL>(a, P, WL, WR, acc, Sf, o3, smax);
+    if constexpr (DIM == 3) stage_axis<2, DIM, RECON, RIEMANN, TX, TY, TZ, NT, FULL>(a, P, WL, WR, acc, Sf, o3, smax);
     // ---- epilogue: the residual and the stage update
     const double dt = a.ctl->dt;
     for (int c = tid; c < NC; c += NT) {
@@ -263,7 +265,8 @@ __global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
             if (a.Rv) r[q] = r[q] + a.Rv[q * m.plane + cell];
         }
         // the body force joins after the viscous term (Simulation::assemble, cpp/src/Simulation.cpp:1038-1049)
-        if (a.bc.grav_on) add_body_force<NV>(a.bc, read_state<NV>(a.bc, a.U, m.plane, cell), r);
+        if constexpr (FULL)
+            if (a.bc.grav_on) add_body_force<NV>(a.bc, read_state<NV>(a.bc, a.U, m.plane, cell), r);
 #pragma unroll
         for (int q = 0; q < NV; ++q) {
             const long long e = q * m.plane + cell;
