@@ -18,8 +18,8 @@ SRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfenice_gpu.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["runtime.cu", "mixed.cu", "batch.cu", "batch_mixed.cu", "sensor.cu"]
-HEADERS = ["physics.cuh", "grid.cuh", "stage.cuh", "viscous.cuh", "hancock.cuh", "mixed.cuh", "mixed_api.h", "batch.cuh", "batch_api.h", "host_common.h", "ibm.cuh", "ibm_host.h", "sensor.cuh", "sensor_api.h"]
+SOURCES = ["runtime.cu", "mixed.cu", "batch.cu", "batch_mixed.cu", "sensor.cu", "expr.cu"]
+HEADERS = ["physics.cuh", "grid.cuh", "stage.cuh", "viscous.cuh", "hancock.cuh", "mixed.cuh", "mixed_api.h", "batch.cuh", "batch_api.h", "host_common.h", "ibm.cuh", "ibm_host.h", "sensor.cuh", "sensor_api.h", "expr.h", "expr.cuh"]
 
 COMMON_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -35,6 +35,7 @@ UNIT_FLAGS = {
     "batch.cu": ["--fmad=false", "-prec-div=true", "-prec-sqrt=true"],
     "batch_mixed.cu": ["--use_fast_math"],
     "sensor.cu": ["--use_fast_math"],
+    "expr.cu": ["--fmad=false", "-prec-div=true", "-prec-sqrt=true"],
 }
 
 

@@ -28,11 +28,13 @@ struct Ctl {
     double s_step;      // largest wave speed of the current step
     double s_stage[3];  // wave speed of each stage of the step
     double half_dt;     // MUSCL-Hancock: half the step the predictor advances the face states by
+    double stage_t;     // the time of the residual being taken (TimeScheme::stage_time)
     int active;         // this step runs (t < t_end, steps < max_steps, no error)
     int seed;           // MUSCL-Hancock: this step first takes one plain residual for the wave speed
     int always;         // 1: the gate of calls outside the time loop
     int steps, max_steps;
-    int status;         // 0 ok; 1 the solution diverged (non-finite speed or dt, or t no longer advances)
+    int status;         // 0 ok; 1 the solution diverged (non-finite speed or dt, or t no longer advances); 3 a
+                        // time-dependent boundary value was not finite, or rho_in or p_out not positive, at a stage time
 };
 
 struct Mesh {
@@ -63,7 +65,17 @@ struct Bc {
     // non-reflecting outlets: relaxation sigma, transverse weight beta (< 0: the local Mach number), the domain length
     // and the cell size per axis
     double nrbc_sigma, nrbc_beta, length[3], h[3];
+    // time-dependent boundary values [u_in, v_in, rho_in, p_out] at the stage time of the residual being taken (device
+    // array of 4, written before it); null when they are the constants above
+    const double* tv;
+    // the case's source terms S (planes in the state's layout, the state's ghost planes included) added to the
+    // residual; null without
+    const double* src;
 };
+
+__device__ __forceinline__ double bc_u_in(const Bc& bc) { return bc.tv ? bc.tv[0] : bc.u_in; }
+__device__ __forceinline__ double bc_v_in(const Bc& bc) { return bc.tv ? bc.tv[1] : bc.v_in; }
+__device__ __forceinline__ double bc_p_out(const Bc& bc) { return bc.tv ? bc.tv[3] : bc.p_out; }
 
 // Whether position g along an axis of n cells is a cell whose state is in the arrays (a cell of the mesh, or of a
 // neighbouring part's ghost planes beyond a kHaloPeer side), and the wrapped index of a periodic axis otherwise.
@@ -99,13 +111,13 @@ __device__ __forceinline__ St<T, NV> ghost_state(const Eos<T>& e, const Bc& bc, 
         break;
     case kBcMovingWall:
     case kBcVelInlet:
-        Wg[1] = T(2) * T(bc.u_in) - Wi[1];
-        Wg[2] = T(2) * T(bc.v_in) - Wi[2];
+        Wg[1] = T(2) * T(bc_u_in(bc)) - Wi[1];
+        Wg[2] = T(2) * T(bc_v_in(bc)) - Wi[2];
         if constexpr (NV == 5) Wg[4] = -Wi[4];
         break;
     case kBcMassflowInlet:   // the x velocity of the side's mass-flow target, whatever the side's axis (as the reference)
         Wg[1] = T(2) * T(bc.u_target[side]) - Wi[1];
-        Wg[2] = T(2) * T(bc.v_in) - Wi[2];
+        Wg[2] = T(2) * T(bc_v_in(bc)) - Wi[2];
         if constexpr (NV == 5) Wg[4] = -Wi[4];
         break;
     case kBcOutlet: {
@@ -114,7 +126,7 @@ __device__ __forceinline__ St<T, NV> ghost_state(const Eos<T>& e, const Bc& bc, 
         Wg[1] = outflow ? Wi[1] : T(0);
         Wg[2] = outflow ? Wi[2] : T(0);
         if constexpr (NV == 5) Wg[4] = outflow ? Wi[4] : T(0);
-        Wg[3] = vmax(T(bc.p_out), T(1e-5));
+        Wg[3] = vmax(T(bc_p_out(bc)), T(1e-5));
         break;
     }
     default: break;
@@ -146,6 +158,12 @@ template <int NV> __device__ __forceinline__ St<double, NV> read_state(const Bc&
 
 // ConstantBodyForce::add_to (cpp/src/Physics.cpp:832-844) for one cell of state u, into r in its order:
 // r1 += rho gx, r2 += rho gy, r3 += m_x gx + m_y gy, then with gz != 0 (a 3-D mesh) r3 += m_z gz and r4 += rho gz.
+// RhsSourceTerms' expression source (Simulation.cpp:397-412, add_source): r[q] += S[q] of the cell.
+template <int NV> __device__ __forceinline__ void add_source(const Bc& bc, long long plane, long long cell, St<double, NV>& r) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) r[q] = r[q] + bc.src[q * plane + cell];
+}
+
 template <int NV> __device__ __forceinline__ void add_body_force(const Bc& bc, const St<double, NV>& u, St<double, NV>& r) {
     const double gx = bc.grav[0], gy = bc.grav[1], gz = bc.grav[2];
     r[1] = r[1] + u[0] * gx;
@@ -278,7 +296,7 @@ __device__ __forceinline__ St<double, NV> nrbc_ghost(const Mesh& m, const Bc& bc
             T1 += Wi[qt] * (Wh[3] - Wl[3]) / ht + Wi[0] * c * c * (Wh[qt] - Wl[qt]) / ht - Wi[0] * c * s * Wi[qt] * (Wh[qv] - Wl[qv]) / ht;
         }
     }
-    const double dw1 = -h * (K * (Wi[3] - bc.p_out) - (1.0 - beta) * T1) / (c - u_out);
+    const double dw1 = -h * (K * (Wi[3] - bc_p_out(bc)) - (1.0 - beta) * T1) / (c - u_out);
     Wg[3] = Wi[3] + 0.5 * dw1;
     Wg[qv] = Wi[qv] - s * dw1 / (2.0 * Wi[0] * c);
     Wg[0] = Wi[0] + 0.5 * dw1 / (c * c);

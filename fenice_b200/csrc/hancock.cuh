@@ -65,12 +65,14 @@ __device__ __forceinline__ bool admissible(const Eos<double>& e, const St<double
 }
 
 // The source field of a MUSCL-Hancock residual (Simulation::assemble, cpp/src/Simulation.cpp:975-980): zero, then the
-// body force added; the predictor takes d - half_dt src, the balance R + src after the viscous term (:1043-1047).
-template <int NV> __device__ __forceinline__ St<double, NV> body_source(const Bc& bc, const St<double, NV>& u) {
+// body force and the case's source terms added (RhsSourceTerms::apply_uniform); the predictor takes d - half_dt src, the
+// balance R + src after the viscous term (:1043-1047).
+template <int NV> __device__ __forceinline__ St<double, NV> body_source(const Bc& bc, const double* U, long long plane, long long cell) {
     St<double, NV> src;
 #pragma unroll
     for (int q = 0; q < NV; ++q) src[q] = 0.0;
-    add_body_force<NV>(bc, u, src);
+    if (bc.grav_on) add_body_force<NV>(bc, read_state<NV>(bc, U, plane, cell), src);
+    if (bc.src) add_source<NV>(bc, plane, cell, src);
     return src;
 }
 
@@ -154,8 +156,8 @@ __global__ void __launch_bounds__(NT) hancock_kernel(const HancockArgs a) {
                 St<double, 4> d;
 #pragma unroll
                 for (int q = 0; q < 4; ++q) d[q] = hx * (fxr[q] - fxl[q]) + hy * (fyt[q] - fyb[q]);
-                if (FULL && a.bc.grav_on) {   // the body force joins the predictor: d - half_dt src
-                    const St<double, 4> src = body_source<4>(a.bc, read_state<4>(a.bc, a.U, m.plane, (long long)cj * nx + ci));
+                if (FULL && (a.bc.grav_on || a.bc.src)) {   // the body force and the sources join the predictor: d - half_dt src
+                    const St<double, 4> src = body_source<4>(a.bc, a.U, m.plane, (long long)cj * nx + ci);
 #pragma unroll
                     for (int q = 0; q < 4; ++q) d[q] = d[q] - half_dt * src[q];
                 }
@@ -247,8 +249,8 @@ __global__ void __launch_bounds__(NT) hancock_kernel(const HancockArgs a) {
             r[q] = acc[q * NC + c] * m.inv_cell;
             if (a.Rv) r[q] = r[q] + a.Rv[q * m.plane + cell];
         }
-        if (FULL && a.bc.grav_on) {
-            const St<double, 4> src = body_source<4>(a.bc, read_state<4>(a.bc, a.U, m.plane, cell));
+        if (FULL && (a.bc.grav_on || a.bc.src)) {
+            const St<double, 4> src = body_source<4>(a.bc, a.U, m.plane, cell);
 #pragma unroll
             for (int q = 0; q < 4; ++q) r[q] = r[q] + src[q];
         }
@@ -400,8 +402,8 @@ __global__ void __launch_bounds__(NT) hancock3d_kernel(const HancockArgs a) {
                 const St<double, 5> fzf = euler_flux3(e, st[4], 2), fzk = euler_flux3(e, st[5], 2);
 #pragma unroll
                 for (int q = 0; q < 5; ++q) d[q] = (hx * (fxr[q] - fxl[q]) + hy * (fyt[q] - fyb[q])) + hz * (fzk[q] - fzf[q]);
-                if (FULL && a.bc.grav_on) {
-                    const St<double, 5> src = body_source<5>(a.bc, read_state<5>(a.bc, a.U, m.plane, cell_of(c3[0], c3[1], c3[2])));
+                if (FULL && (a.bc.grav_on || a.bc.src)) {
+                    const St<double, 5> src = body_source<5>(a.bc, a.U, m.plane, cell_of(c3[0], c3[1], c3[2]));
 #pragma unroll
                     for (int q = 0; q < 5; ++q) d[q] = d[q] - half_dt * src[q];
                 }
@@ -506,8 +508,8 @@ __global__ void __launch_bounds__(NT) hancock3d_kernel(const HancockArgs a) {
             r[q] = acc[q * NC + c] * m.inv_cell;
             if (a.Rv) r[q] = r[q] + a.Rv[q * m.plane + cell];
         }
-        if (FULL && a.bc.grav_on) {
-            const St<double, 5> src = body_source<5>(a.bc, read_state<5>(a.bc, a.U, m.plane, cell));
+        if (FULL && (a.bc.grav_on || a.bc.src)) {
+            const St<double, 5> src = body_source<5>(a.bc, a.U, m.plane, cell);
 #pragma unroll
             for (int q = 0; q < 5; ++q) r[q] = r[q] + src[q];
         }

@@ -10,6 +10,8 @@
 namespace fvg {
 // why a configuration cannot run on the device ("" when it can)
 std::string config_error(const fvg_config& c);
+// whether it has case-file source terms or time-dependent boundary values
+bool config_has_expressions(const fvg_config& c);
 // the halo kind (kHalo*) of each side for a reconstruction `depth` cells deep
 void config_halo_kinds(const fvg_config& c, int depth, int kinds[6]);
 // the message fvg_create_error() returns (this thread's)

@@ -17,6 +17,7 @@
 // "end" reduces the later stages, applies check_progress, advances t and the step count and decides whether the next
 // step runs (t < t_end, step limit, no error).
 #include "../../include/fenice_gpu.h"
+#include "expr.cuh"
 #include "hancock.cuh"
 #include "ibm.cuh"
 #include "host_common.h"
@@ -27,10 +28,14 @@
 #include "stage.cuh"
 #include "viscous.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 using namespace fvg;
@@ -163,7 +168,64 @@ __global__ void __launch_bounds__(1024) k_massflow(Mesh m, Bc bc, const double* 
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) u_target[side] = (rho_in * u_in) / vmax(sum / (double)count, 1e-5);
+    if (threadIdx.x == 0) {
+        const double rin = bc.tv ? bc.tv[2] : rho_in, uin = bc.tv ? bc.tv[0] : u_in;   // at the stage time when they vary
+        u_target[side] = (rin * uin) / vmax(sum / (double)count, 1e-5);
+    }
+}
+
+// ---- case-file expressions (expr.h): the programs of a run on the device
+struct ExprArgs {
+    const expr::Op* code;
+    const double* pool;
+    int src[5];   // entries of source_rho, source_mx, source_my, source_E, source_mz
+    int bnd[4];   // entries of u_in, v_in, rho_in, p_out as functions of t (-1: constant)
+};
+
+// TimeScheme::stage_time of the residual about to be taken (kind 0: t, 1: t + dt, 2: t + 0.5 dt, 3: `at`, 4: t +
+// half_dt; TimeScheme.cpp:111-306), and Simulation::update_boundary_values at that time (Simulation.cpp:170-185): the
+// time-dependent values into tv (x = y = z = 0, as compile_time_expression binds them). A value that is not finite, or
+// rho_in or p_out not positive, stops the run (status 3; the reference throws).
+__global__ void k_stage_values(Ctl* c, const int* gate, int kind, double at, ExprArgs x, double* tv) {
+    if (!*gate) return;
+    const double t = kind == 0 ? c->t : kind == 1 ? c->t + c->dt : kind == 2 ? c->t + 0.5 * c->dt : kind == 3 ? at : c->t + c->half_dt;
+    c->stage_t = t;
+    if (!tv) return;
+    bool ok = true;
+    for (int k = 0; k < 4; ++k)
+        if (x.bnd[k] >= 0) {
+            const double v = expr::run(x.code, x.pool, x.bnd[k], 0.0, 0.0, 0.0, t);
+            tv[k] = v;
+            ok = ok && isfinite(v);
+        }
+    if (!ok || !(tv[2] > 0.0) || !(tv[3] > 0.0)) {
+        c->status = 3;
+        c->active = 0;
+    }
+}
+
+// evaluate_source (cpp/src/CaseFile.cpp:879-890) on the device: the five source expressions at the cell centres
+// ((i + 1/2) dx, ...; z = 0 on a 2-D mesh; Mesh::xc, cpp/include/fv/Core.hpp:98-102) and the stage time, into planes
+// in the state's layout. A part's own planes along the split axis and `lo` / `hi` ghost planes beyond them, at their
+// places in the whole mesh of nsplit planes (wrapped across a periodic end).
+template <int NV>
+__global__ void k_source_field(Mesh m, ExprArgs x, const Ctl* c, const int* gate, int split, int first, int lo, int hi, int nsplit, double* S) {
+    if (!*gate) return;
+    const double t = c->stage_t;
+    const long long nloc = split == 2 ? m.nz : m.ny;
+    const long long area = split == 2 ? (long long)m.nx * m.ny : m.nx;
+    const long long total = (nloc + lo + hi) * area;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const long long pl = e / area - lo, rem = e % area;
+        long long gp = first + pl;
+        if (gp < 0) gp += nsplit;
+        else if (gp >= nsplit) gp -= nsplit;
+        const long long i = split == 2 ? rem % m.nx : rem, j = split == 2 ? rem / m.nx : gp, k = split == 2 ? gp : 0;
+        const double xc = ((double)i + 0.5) * m.dx, yc = ((double)j + 0.5) * m.dy, zc = NV == 5 ? ((double)k + 0.5) * m.dz : 0.0;
+        const long long cell = pl * area + rem;
+#pragma unroll 1
+        for (int q = 0; q < NV; ++q) S[q * m.plane + cell] = expr::run(x.code, x.pool, x.src[q], xc, yc, zc, t);
+    }
 }
 
 // ---- parts of a slab-decomposed mesh
@@ -460,6 +522,17 @@ struct fvg_run {
     long long goff = 0, area = 0, xcount = 0;
     double* xbuf = nullptr;
     double* xred = nullptr;
+    int nsplit = 1;   // planes of the whole mesh along the split axis
+    // case-file expressions (fvg_config source / boundary_*): the programs on the device, the source field (planes in the
+    // state's layout with its ghost planes; d_src is the allocation) and the time-dependent boundary values (d_tv: 4)
+    ExprArgs xa{};
+    expr::Op* d_code = nullptr;
+    double* d_pool = nullptr;
+    bool src_on = false, src_unsteady = false, tv_on = false;
+    double* d_src = nullptr;
+    double* d_tv = nullptr;
+    double res_time = NAN;   // fvg_set_stage_time (NaN: the run's time)
+    int res_kind = -1;       // the stage-time kind residual_stage takes (-1: its stage index)
     double* Ucur() { return cur ? Ut : U; }
 };
 
@@ -475,6 +548,26 @@ int fail(fvg_run* r, int code, const std::string& msg) {
         cudaError_t e_ = (call);                                                                  \
         if (e_ != cudaSuccess) return fail(run, FVG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
+
+// Whether a configuration has case-file source terms (a value that is not a whole number equal to 0: Params.cpp:280-286)
+// or time-dependent boundary values (an expression that is not a whole number, or a time table).
+bool has_expressions(const fvg_config& c) {
+    for (int q = 0; q < 5; ++q)
+        if (c.source[q]) {
+            char* end = nullptr;
+            const double d = std::strtod(c.source[q], &end);
+            if (!(end && *end == '\0' && d == 0.0)) return true;
+        }
+    for (int k = 0; k < 4; ++k) {
+        if (c.boundary_table[k] && c.boundary_table_rows[k] > 0) return true;
+        if (c.boundary_expr[k] && *c.boundary_expr[k]) {
+            char* end = nullptr;
+            std::strtod(c.boundary_expr[k], &end);
+            if (!(end && end != c.boundary_expr[k] && *end == '\0')) return true;
+        }
+    }
+    return false;
+}
 
 std::string validate(const fvg_config& c) {
     if (c.nx < 1 || c.ny < 1 || c.nz < 1) return "nx, ny, nz must be >= 1";
@@ -505,6 +598,9 @@ std::string validate(const fvg_config& c) {
     if (!(c.dt_max >= 0.0) || !std::isfinite(c.dt_max)) return "dt_max must be finite and >= 0 (0: off)";
     if (c.use_viscous && (!(c.mu >= 0.0) || !(c.pr > 0.0))) return "mu must be >= 0 and pr > 0 with use_viscous";
     if (c.use_bodyforce && c.precision == FVG_PREC_MIXED) return "the body force runs in the FP64 form only";
+    if (has_expressions(c) && c.precision == FVG_PREC_MIXED)
+        return "case-file source terms and time-dependent boundary values run in the FP64 form only";
+    if (c.nparams < 0 || (c.nparams > 0 && (!c.param_names || !c.param_values))) return "param_names / param_values missing";
     if (c.positivity_fallback) {   // Params.cpp:464-467
         if (c.reconstruction != FVG_RECON_WENO3 && c.reconstruction != FVG_RECON_WENO5)
             return "positivity_fallback needs reconstruction = weno3 or weno5 (the other schemes keep their reconstructed states between the cells)";
@@ -512,6 +608,10 @@ std::string validate(const fvg_config& c) {
     }
     if (c.use_bodyforce && c.use_ibm) return "the body force with an immersed body (gravity in its ghost states) is not supported on the device";
     if (!(c.cfl > 0)) return "cfl must be > 0";
+    // load_boundary_functions (Simulation.cpp:152-153); time-dependent ones are checked at t = 0 when compiled
+    const bool rho_fn = (c.boundary_expr[2] && *c.boundary_expr[2]) || (c.boundary_table[2] && c.boundary_table_rows[2] > 0);
+    const bool p_fn = (c.boundary_expr[3] && *c.boundary_expr[3]) || (c.boundary_table[3] && c.boundary_table_rows[3] > 0);
+    if ((!rho_fn && !(c.rho_in > 0.0)) || (!p_fn && !(c.p_out > 0.0))) return "rho_in and p_out must be positive";
     if (!(c.nrbc_sigma >= 0.0)) return "nrbc_sigma must be >= 0";   // Params.cpp:489-490
     if (!(c.nrbc_beta <= 1.0)) return "nrbc_beta must be <= 1 (< 0: local Mach number)";
     return "";
@@ -707,11 +807,38 @@ cudaError_t launch_visc(fvg_run* r, const double* Uin, double* bmv, const int* g
     return e;
 }
 
+// The source field's planes of a run: its own planes and, for a part, the ghost planes beyond its interfaces.
+void source_planes(const fvg_run* r, int* split, int* first, int* lo, int* hi) {
+    *split = r->is_part ? r->split : (r->dim == 3 ? 2 : 1);
+    *first = r->is_part ? r->first : 0;
+    *lo = r->is_part && r->peer[0] ? r->depth : 0;
+    *hi = r->is_part && r->peer[1] ? r->depth : 0;
+}
+
+// Before a residual whose stage time is of `kind` (k_stage_values): the stage time, the time-dependent boundary values
+// and an unsteady source field.
+cudaError_t stage_values(fvg_run* r, int kind, const int* gate) {
+    if (!r->tv_on && !r->src_unsteady) return cudaSuccess;
+    k_stage_values<<<1, 1, 0, r->stream>>>(r->ctl, gate, kind, r->res_time, r->xa, r->tv_on ? r->d_tv : nullptr);
+    if (r->src_unsteady) {
+        int split, first, lo, hi;
+        source_planes(r, &split, &first, &lo, &hi);
+        const long long n = ((split == 2 ? r->m.nz : r->m.ny) + lo + hi) * (split == 2 ? (long long)r->m.nx * r->m.ny : r->m.nx);
+        const int blocks = (int)std::min<long long>((n + 127) / 128, 148 * 8);
+        if (r->nvar == 5)
+            k_source_field<5><<<blocks, 128, 0, r->stream>>>(r->m, r->xa, r->ctl, gate, split, first, lo, hi, r->nsplit, r->d_src + r->goff);
+        else
+            k_source_field<4><<<blocks, 128, 0, r->stream>>>(r->m, r->xa, r->ctl, gate, split, first, lo, hi, r->nsplit, r->d_src + r->goff);
+    }
+    return cudaGetLastError();
+}
+
 // One residual stage of Uin: the immersed body's forced states, the viscous sweep (viscous runs), then the inviscid
 // stage kernel.
 cudaError_t residual_stage(fvg_run* r, const double* Uin, const double* U0, double* out, int mode, double ca, double cb, int stage, const int* gate,
                            const unsigned char* fb = nullptr) {
     cudaError_t e;
+    if ((e = stage_values(r, r->res_kind >= 0 ? r->res_kind : stage, gate)) != cudaSuccess) return e;
     if (r->ibm && (e = ibm_fill(r, Uin, nullptr, 0, gate)) != cudaSuccess) return e;
     if ((e = massflow_targets(r, Uin, gate)) != cudaSuccess) return e;
     if (r->cfg.use_viscous && (e = launch_visc(r, Uin, r->bmv[stage], gate)) != cudaSuccess) return e;
@@ -817,6 +944,7 @@ cudaError_t enqueue_step(fvg_run* r, bool refresh = true) {
         double* Uout = r->cur ? r->U : r->Ut;
         k_hancock_begin<<<1, 1, 0, r->stream>>>(c);
         // the seed (first step only; untimed): one plain residual for the speed, its viscous bound included
+        if ((e = stage_values(r, 0, &c->seed))) return e;
         if (r->ibm && (e = ibm_fill(r, Uin, nullptr, 0, &c->seed))) return e;
         if ((e = massflow_targets(r, Uin, &c->seed))) return e;
         if (r->cfg.use_viscous && (e = launch_visc(r, Uin, r->bmv[1], &c->seed, false))) return e;
@@ -825,6 +953,7 @@ cudaError_t enqueue_step(fvg_run* r, bool refresh = true) {
             return e;
         k_hancock_seed<<<1, 1024, 0, r->stream>>>(c, r->bm_seed, r->nb, r->bmv[1], nbv);
         k_hancock_dt<<<1, 1, 0, r->stream>>>(c);
+        if ((e = stage_values(r, 2, act))) return e;   // t + dt / 2: the sources centred in the step
         if (r->ibm && (e = ibm_fill(r, Uin, nullptr, 0, act))) return e;
         if ((e = massflow_targets(r, Uin, act))) return e;
         if (r->cfg.use_viscous && (e = launch_visc(r, Uin, r->bmv[0], act))) return e;
@@ -907,6 +1036,7 @@ cudaError_t part_phase(fvg_run* r, int phase, int* comm, int* nred) {
         case 1:   // the seed residual (first step only) and its speed
             if ((e = part_unpack(r, Uin))) break;
             k_hancock_begin<<<1, 1, 0, s>>>(c);
+            if ((e = stage_values(r, 0, &c->seed))) break;
             if (r->cfg.use_viscous && (e = launch_visc(r, Uin, r->bmv[1], &c->seed, false))) break;
             if ((e = r->stage.launch(stage_args(r, Uin, nullptr, r->R, kStoreR, 0, 0, r->cfg.use_viscous ? r->Rv : nullptr, r->bm_seed, &c->seed), r->nb,
                                      s)))
@@ -918,6 +1048,7 @@ cudaError_t part_phase(fvg_run* r, int phase, int* comm, int* nred) {
         case 2:   // dt from the lagged speed, the predictor and update, the speed
             k_part_seed<<<1, 1, 0, s>>>(c, r->xred);
             k_hancock_dt<<<1, 1, 0, s>>>(c);
+            if ((e = stage_values(r, 2, act))) break;
             if (r->cfg.use_viscous && (e = launch_visc(r, Uin, r->bmv[0], act))) break;
             timer_mark(r, r->t_stage);
             e = launch_hancock(r, hancock_args(r, Uin, Uout, kAxpy, r->bm[0], act));
@@ -1013,6 +1144,7 @@ int read_ctl(fvg_run* run, Ctl* h) {
 
 // configuration checks shared with the batched runs (batch.cu)
 std::string fvg::config_error(const fvg_config& c) { return validate(c); }
+bool fvg::config_has_expressions(const fvg_config& c) { return has_expressions(c); }
 void fvg::config_halo_kinds(const fvg_config& c, int depth, int kinds[6]) { halo_kinds(c, depth, kinds); }
 std::string* fvg::create_error_slot() { return &g_create_error; }
 bool fvg::run_view(fvg_run* run, RunView* v) {
@@ -1053,6 +1185,122 @@ int fvg_create_part(const fvg_config* cfg, int nparts, int part, fvg_run** out) 
 }   // extern "C"
 
 namespace {
+
+// The case-file expressions of a run (Simulation::setup and load_boundary_functions, cpp/src/Simulation.cpp:118-168,
+// 372-412): compiles the source terms (when one is not a whole number equal to 0) and the boundary values given as
+// expressions of t or time tables, replaces u_in, v_in, rho_in, p_out by their values at t = 0, and notes which vary.
+// Throws std::exception with the reference's message for what it refuses.
+void compile_expressions(fvg_run* run, const fvg_config& whole, expr::Program& p) {
+    for (int i = 0; i < whole.nparams; ++i) p.bind(whole.param_names[i] ? whole.param_names[i] : "", whole.param_values[i]);
+    p.bind("Lx", whole.Lx);   // the mesh is authoritative for the domain (CaseFile.cpp:323-329)
+    p.bind("Ly", whole.Ly);
+    p.bind("Lz", whole.Lz);
+    p.bind("nx", whole.nx);
+    p.bind("ny", whole.ny);
+    p.bind("nz", whole.nz);
+    static const char* const skeys[5] = {"source_rho", "source_mx", "source_my", "source_E", "source_mz"};
+    bool use = false;
+    for (int q = 0; q < 5; ++q) {
+        const char* v = whole.source[q] ? whole.source[q] : "0";
+        char* end = nullptr;
+        const double d = std::strtod(v, &end);
+        if (!(end && *end == '\0' && d == 0.0)) use = true;
+    }
+    for (int q = 0; q < 5; ++q) run->xa.src[q] = -1;
+    if (use) {
+        for (int q = 0; q < 5; ++q) {
+            run->xa.src[q] = p.add(whole.source[q] ? whole.source[q] : "0", skeys[q]);
+            if (p.reads(run->xa.src[q], expr::kVarT)) run->src_unsteady = true;
+        }
+        run->src_on = true;
+        double c0 = 0.0;
+        if (whole.nz <= 1 && !(p.constant(run->xa.src[4], &c0) && c0 == 0.0))
+            throw std::invalid_argument("source_mz must be 0 on a 2-D mesh (rho w is held at 0 there)");
+    }
+    static const char* const bkeys[4] = {"u_in", "v_in", "rho_in", "p_out"};
+    double* vals[4] = {&run->cfg.u_in, &run->cfg.v_in, &run->cfg.rho_in, &run->cfg.p_out};
+    bool any = false;
+    for (int k = 0; k < 4; ++k) {
+        run->xa.bnd[k] = -1;
+        const char* ex = whole.boundary_expr[k];
+        const bool has_ex = ex && *ex;
+        char* end = nullptr;
+        const double num = has_ex ? std::strtod(ex, &end) : 0.0;
+        const bool numeric = has_ex && end != ex && *end == '\0';
+        const std::string key = bkeys[k];
+        int entry = -1;
+        if (whole.boundary_table[k] && whole.boundary_table_rows[k] > 0) {
+            if (has_ex && !numeric) throw std::invalid_argument(key + " expression and " + key + "_table cannot both be set");
+            entry = p.add_table(whole.boundary_table[k], whole.boundary_table_rows[k], key + "_table");
+        } else if (has_ex) {
+            if (numeric) *vals[k] = num;
+            else entry = p.add(ex, key);
+        }
+        if (entry < 0) continue;
+        any = true;
+        const double v0 = p.eval(entry, 0.0, 0.0, 0.0, 0.0);
+        if (!std::isfinite(v0)) throw std::runtime_error(key + ": time expression evaluated to a non-finite value");
+        *vals[k] = v0;
+        if (p.reads(entry, expr::kVarT)) {
+            run->xa.bnd[k] = entry;
+            run->tv_on = true;
+        }
+    }
+    if (any && (!(run->cfg.rho_in > 0.0) || !(run->cfg.p_out > 0.0)))
+        throw std::invalid_argument("time-dependent rho_in and p_out must be positive at t=0");
+}
+
+// The programs on the device, the boundary values' array and the source field (a steady one evaluated here on the
+// host, with the C library's functions as the reference evaluates it: its bits; an unsteady one is evaluated on the
+// device before every residual).
+int upload_expressions(fvg_run* run, const expr::Program& p) {
+    if (!run->src_on && !run->tv_on) return FVG_OK;
+    if (cudaMalloc(&run->d_code, sizeof(expr::Op) * p.code.size()) != cudaSuccess ||
+        cudaMalloc(&run->d_pool, sizeof(double) * (p.pool.size() + 1)) != cudaSuccess || cudaMalloc(&run->d_tv, sizeof(double) * 4) != cudaSuccess)
+        return fail(run, FVG_ERR_CUDA, "device allocation failed");
+    const double tv0[4] = {run->cfg.u_in, run->cfg.v_in, run->cfg.rho_in, run->cfg.p_out};
+    if (cudaMemcpy(run->d_code, p.code.data(), sizeof(expr::Op) * p.code.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        (!p.pool.empty() && cudaMemcpy(run->d_pool, p.pool.data(), sizeof(double) * p.pool.size(), cudaMemcpyHostToDevice) != cudaSuccess) ||
+        cudaMemcpy(run->d_tv, tv0, sizeof(tv0), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(run, FVG_ERR_CUDA, "copy of the expression programs failed");
+    run->xa.code = run->d_code;
+    run->xa.pool = run->d_pool;
+    if (run->tv_on) run->bc.tv = run->d_tv;
+    if (!run->src_on) return FVG_OK;
+    const size_t sbytes = sizeof(double) * run->m.plane * run->nvar;
+    if (cudaMalloc(&run->d_src, sbytes) != cudaSuccess) return fail(run, FVG_ERR_CUDA, "device allocation failed");
+    run->bc.src = run->d_src + run->goff;
+    if (run->src_unsteady) return cudaMemset(run->d_src, 0, sbytes) == cudaSuccess ? FVG_OK : fail(run, FVG_ERR_CUDA, "cudaMemset failed");
+    int split, first, lo, hi;
+    source_planes(run, &split, &first, &lo, &hi);
+    const Mesh& m = run->m;
+    const long long nloc = split == 2 ? m.nz : m.ny, area = split == 2 ? (long long)m.nx * m.ny : m.nx;
+    std::vector<double> S((size_t)m.plane * run->nvar, 0.0);
+    const long long total = (nloc + lo + hi) * area;
+    const int nv = run->nvar;
+    auto work = [&](long long from, long long to) {   // the cells of k_source_field, the same coordinates
+        for (long long e = from; e < to; ++e) {
+            const long long pl = e / area - lo, rem = e % area;
+            long long gp = first + pl;
+            if (gp < 0) gp += run->nsplit;
+            else if (gp >= run->nsplit) gp -= run->nsplit;
+            const long long i = split == 2 ? rem % m.nx : rem, j = split == 2 ? rem / m.nx : gp, k = split == 2 ? gp : 0;
+            const double xc = ((double)i + 0.5) * m.dx, yc = ((double)j + 0.5) * m.dy, zc = nv == 5 ? ((double)k + 0.5) * m.dz : 0.0;
+            const long long cell = run->goff + pl * area + rem;
+            for (int q = 0; q < nv; ++q) S[(size_t)q * m.plane + cell] = p.eval(run->xa.src[q], xc, yc, zc, 0.0);
+        }
+    };
+    const int nthreads = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    if (total < (1 << 16) || nthreads == 1) {
+        work(0, total);
+    } else {
+        std::vector<std::thread> pool;
+        for (int w = 0; w < nthreads; ++w) pool.emplace_back(work, total * w / nthreads, total * (w + 1) / nthreads);
+        for (std::thread& t : pool) t.join();
+    }
+    if (cudaMemcpy(run->d_src, S.data(), sbytes, cudaMemcpyHostToDevice) != cudaSuccess) return fail(run, FVG_ERR_CUDA, "copy of the source field failed");
+    return FVG_OK;
+}
 
 // fvg_create, and part `part` of `nparts` slabs of the mesh along its slowest axis (nparts = 1 with part mode off: a
 // whole run). A part holds planes first .. first + count - 1 of the split axis (the first nsplit % nparts parts one
@@ -1121,6 +1369,23 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
         fvg_destroy(run);
         return code;
     };
+    run->nsplit = nsplit;
+    expr::Program prog;
+    try {
+        compile_expressions(run, *cfg, prog);
+    } catch (const std::exception& ex) {
+        run->err = ex.what();
+        return bail(FVG_ERR_CONFIG);
+    }
+    for (int q = 0; q < 5; ++q) run->cfg.source[q] = nullptr;   // (the caller's memory is not kept)
+    for (int k = 0; k < 4; ++k) {
+        run->cfg.boundary_expr[k] = nullptr;
+        run->cfg.boundary_table[k] = nullptr;
+        run->cfg.boundary_table_rows[k] = 0;
+    }
+    run->cfg.param_names = nullptr;
+    run->cfg.param_values = nullptr;
+    run->cfg.nparams = 0;
     if (cudaSetDevice(c.device) != cudaSuccess) {
         run->err = "cudaSetDevice failed (no CUDA device?)";
         return bail(FVG_ERR_CUDA);
@@ -1188,7 +1453,7 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
     run->ntiles_h[1] = (c.ny + hx - 1) / hx;
     run->ntiles_h[2] = (c.nz + hz - 1) / hz;
     run->nbh = run->ntiles_h[0] * run->ntiles_h[1] * run->ntiles_h[2];
-    bool full = run->is_part || c.positivity_fallback || c.use_bodyforce;
+    bool full = run->is_part || c.positivity_fallback || c.use_bodyforce || run->src_on;
     for (int s = 0; s < 6; ++s) full = full || c.bc[s] == FVG_BC_NONREFLECTING;
     run->full = full;
     run->stage = run->dim == 3 ? stage_launcher<3>(c.reconstruction, c.riemann, full) : stage_launcher<2>(c.reconstruction, c.riemann, full);
@@ -1236,6 +1501,7 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
             cudaMemsetAsync(run->d_utarget, 0, sizeof(double) * 6, run->stream);
             run->bc.u_target = run->d_utarget;
         }
+    if (const int rc = upload_expressions(run, prog)) return bail(rc);
     const int nbmax = run->nb > run->nbh ? run->nb : run->nbh;
     for (int s = 0; s < 3; ++s)
         if (cudaMalloc(&run->bm[s], sizeof(double) * nbmax) != cudaSuccess || cudaMalloc(&run->bmv[s], sizeof(double) * run->nbv) != cudaSuccess) {
@@ -1323,9 +1589,10 @@ int fvg_destroy(fvg_run* run) {
     for (double* p : {run->U, run->Ut, run->R, run->Rv})   // the arrays start goff doubles before the first interior plane
         if (p) cudaFree(p - run->goff);
     for (double* p : {run->staging, run->bm_seed, run->bm[0], run->bm[1], run->bm[2], run->bmv[0], run->bmv[1], run->bmv[2], run->xbuf, run->xred,
-                      run->d_utarget})
+                      run->d_utarget, run->d_pool, run->d_src, run->d_tv})
         if (p) cudaFree(p);
     if (run->ctl) cudaFree(run->ctl);
+    if (run->d_code) cudaFree(run->d_code);
     if (run->fb_flags) cudaFree(run->fb_flags);
     if (run->fb_grew) cudaFree(run->fb_grew);
     if (run->sens) cudaFree(run->sens);
@@ -1387,10 +1654,14 @@ int fvg_residual(fvg_run* run, double predictor_half_dt, double* R, size_t ncell
     Ctl* c = run->ctl;
     const int* always = &c->always;
     double* out = run->cur ? run->U : run->Ut;   // a buffer that is not the state
+    CK(cudaMemsetAsync(&c->status, 0, sizeof(int), run->stream));
+    // the stage time: fvg_set_stage_time's, else t (plus half the step for the MUSCL-Hancock predictor)
+    const int kind = !std::isnan(run->res_time) ? 3 : (predictor_half_dt > 0.0 ? 4 : 0);
     if (predictor_half_dt > 0.0) {
         if (run->cfg.reconstruction != FVG_RECON_MUSCL)
             return fail(run, FVG_ERR_CONFIG, "the MUSCL-Hancock predictor needs a MUSCL run");
         CK(cudaMemcpyAsync(&c->half_dt, &predictor_half_dt, sizeof(double), cudaMemcpyHostToDevice, run->stream));
+        CK(stage_values(run, kind, always));
         if (run->ibm) CK(ibm_fill(run, run->Ucur(), nullptr, 0, always));
         CK(massflow_targets(run, run->Ucur(), always));
         if (run->cfg.use_viscous) CK(launch_visc(run, run->Ucur(), run->bmv[0], always));
@@ -1398,13 +1669,21 @@ int fvg_residual(fvg_run* run, double predictor_half_dt, double* R, size_t ncell
         k_stage_max<<<1, 1024, 0, run->stream>>>(c, always, 0, run->bm[0], run->nbh, run->bmv[0], run->cfg.use_viscous ? run->nbv : 0);
     } else {
         CK(refresh_gate(run, run->Ucur(), nullptr));
-        CK(residual_stage(run, run->Ucur(), nullptr, out, kStoreR, 0, 0, 0, always));
+        run->res_kind = kind;
+        const cudaError_t e = residual_stage(run, run->Ucur(), nullptr, out, kStoreR, 0, 0, 0, always);
+        run->res_kind = -1;
+        CK(e);
         k_stage_max<<<1, 1024, 0, run->stream>>>(c, always, 0, run->bm[0], run->nb, run->bmv[0], run->cfg.use_viscous ? run->nbv : 0);
     }
     CK(cudaGetLastError());
     Ctl h;
     int rc = read_ctl(run, &h);
     if (rc) return rc;
+    if (h.status == 3) {
+        char msg[256];
+        std::snprintf(msg, sizeof msg, "time-dependent boundary values: not finite, or rho_in or p_out not positive, at t = %.17g", h.stage_t);
+        return fail(run, FVG_ERR_BOUNDARY, msg);
+    }
     if (smax) *smax = h.s_stage[0];
     if (R) {
         if ((rc = ensure_staging(run))) return rc;
@@ -1483,6 +1762,12 @@ static int run_steps(fvg_run* run, double t_end, int max_steps, int use_graph, i
         if (hancock && (done & 1)) run->cur ^= 1;
     }
     if (steps) *steps = done;
+    if (h.status == 3) {
+        char msg[256];
+        std::snprintf(msg, sizeof msg, "time-dependent boundary values: not finite, or rho_in or p_out not positive, at t = %.17g (step %d)", h.stage_t,
+                      done + 1);
+        return fail(run, FVG_ERR_BOUNDARY, msg);
+    }
     if (h.status) {
         char msg[256];
         std::snprintf(msg, sizeof msg, "the solution diverged at step %d (t = %.6g, dt = %.3g, largest wave speed = %.3g)", done + 1, h.t, h.dt,
@@ -1564,6 +1849,12 @@ int fvg_part_status(fvg_run* run, int* active, int* steps, double* t, double* dt
     if (t) *t = h.t;
     if (dt) *dt = h.dt;
     if (smax) *smax = h.s_step;
+    if (h.status == 3) {
+        char msg[256];
+        std::snprintf(msg, sizeof msg, "time-dependent boundary values: not finite, or rho_in or p_out not positive, at t = %.17g (step %d)", h.stage_t,
+                      h.steps + 1);
+        return fail(run, FVG_ERR_BOUNDARY, msg);
+    }
     if (h.status) {
         char msg[256];
         std::snprintf(msg, sizeof msg, "the solution diverged at step %d (t = %.6g, dt = %.3g, largest wave speed = %.3g)", h.steps + 1, h.t, h.dt, h.s_step);
@@ -1586,6 +1877,12 @@ int fvg_set_time(fvg_run* run, double t) {
     if (!run) return FVG_ERR_ARGUMENT;
     CK(cudaMemcpyAsync(&run->ctl->t, &t, sizeof(double), cudaMemcpyHostToDevice, run->stream));
     CK(cudaStreamSynchronize(run->stream));
+    return FVG_OK;
+}
+
+int fvg_set_stage_time(fvg_run* run, double t) {
+    if (!run) return FVG_ERR_ARGUMENT;
+    run->res_time = t;
     return FVG_OK;
 }
 
@@ -1820,6 +2117,8 @@ extern "C" int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long
     if (cfg->precision != FVG_PREC_FP64) return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: the FP64 form only");
     if (cfg->use_ibm) return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: an immersed body needs its tables on the device; use fvg_residual");
     if (cfg->use_viscous) return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: viscous runs need a residual-sized scratch array; use fvg_residual");
+    if (has_expressions(*cfg))
+        return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: source terms and time-dependent boundary values need their programs on the device; use fvg_residual");
     for (int s = 0; s < 6; ++s)
         if (cfg->bc[s] == FVG_BC_MASSFLOWINLET)
             return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: a mass-flow inlet needs its target on the device; use fvg_residual");

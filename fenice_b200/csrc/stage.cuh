@@ -264,9 +264,12 @@ __global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
             r[q] = acc[q * NC + c] * m.inv_cell;
             if (a.Rv) r[q] = r[q] + a.Rv[q * m.plane + cell];
         }
-        // the body force joins after the viscous term (Simulation::assemble, cpp/src/Simulation.cpp:1038-1049)
-        if constexpr (FULL)
+        // the body force, then the case's source terms, join after the viscous term (Simulation::assemble,
+        // cpp/src/Simulation.cpp:1038-1049; RhsSourceTerms in the order Simulation::setup adds them, :372-412)
+        if constexpr (FULL) {
             if (a.bc.grav_on) add_body_force<NV>(a.bc, read_state<NV>(a.bc, a.U, m.plane, cell), r);
+            if (a.bc.src) add_source<NV>(a.bc, m.plane, cell, r);
+        }
 #pragma unroll
         for (int q = 0; q < NV; ++q) {
             const long long e = q * m.plane + cell;

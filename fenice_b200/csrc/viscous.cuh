@@ -50,7 +50,7 @@ __device__ __forceinline__ St<double, 5> viscous_ghost_3d(const ViscArgs& a, int
     } else if (type == kBcWall) {
         gh[mom[d]] = -c[mom[d]];
     } else if (type == kBcMovingWall) {
-        const double uw[3] = {a.u_in, a.v_in, 0.0};
+        const double uw[3] = {a.bc.tv ? a.bc.tv[0] : a.u_in, a.bc.tv ? a.bc.tv[1] : a.v_in, 0.0};
 #pragma unroll
         for (int t = 0; t < 3; ++t) gh[mom[t]] = (t == d) ? -c[mom[t]] : 2.0 * c[0] * uw[t] - c[mom[t]];
         if (a.bface2)   // match_kinetic_energy (Boundaries.cpp:197-200)

@@ -51,7 +51,13 @@ class FvgConfig(ctypes.Structure):
                 ("use_ibm", ctypes.c_int), ("ibm_shape", ctypes.c_int), ("ibm_radius", ctypes.c_double), ("ibm_cx", ctypes.c_double),
                 ("ibm_cy", ctypes.c_double), ("ibm_cz", ctypes.c_double), ("ibm_curvature", ctypes.c_int),
                 ("use_bodyforce", ctypes.c_int), ("gx", ctypes.c_double), ("gy", ctypes.c_double), ("gz", ctypes.c_double),
-                ("nrbc_sigma", ctypes.c_double), ("nrbc_beta", ctypes.c_double), ("positivity_fallback", ctypes.c_int)]
+                ("nrbc_sigma", ctypes.c_double), ("nrbc_beta", ctypes.c_double), ("positivity_fallback", ctypes.c_int),
+                ("source", ctypes.c_char_p * 5), ("boundary_expr", ctypes.c_char_p * 4),
+                ("boundary_table", ctypes.POINTER(ctypes.c_double) * 4), ("boundary_table_rows", ctypes.c_int * 4),
+                ("param_names", ctypes.POINTER(ctypes.c_char_p)), ("param_values", ctypes.POINTER(ctypes.c_double)), ("nparams", ctypes.c_int)]
+
+SOURCE_KEYS = ("source_rho", "source_mx", "source_my", "source_E", "source_mz")   # the state's slot order
+BOUNDARY_KEYS = ("u_in", "v_in", "rho_in", "p_out")
 
 
 def _flag(v):
@@ -94,28 +100,77 @@ def _num(v):
 
 def not_on_device(params):
     """The reference features a parameter dict switches on that the device path does not compute (None: none). They
-    are refused, never ignored: AMR, case-file source expressions (source_* evaluated per cell and stage),
-    fourth-order flux quadrature, time tables of the inlet / outlet values, reynolds (mu derived from
-    the body's length scale), and a moving or flow-driven immersed body. (Combinations the device refuses, such as the body
-force with the mixed-precision form, are refused by fvg_create with FVG_ERR_CONFIG.)"""
+    are refused, never ignored: AMR, fourth-order flux quadrature and a moving or flow-driven immersed body. (Combinations
+    the device refuses, such as the body force with the mixed-precision form, are refused by fvg_create with
+    FVG_ERR_CONFIG.)"""
     p = resolve(params)
     if _flag(p.get("use_amr", False)):
         return "adaptive meshes (use_amr)"
-    src = [k for k in ("source_rho", "source_mx", "source_my", "source_mz", "source_E") if _num(p.get(k, 0)) != 0.0]
-    if src:
-        return "case-file source terms (" + ", ".join(src) + ")"
     if str(p.get("flux_quadrature", "midpoint")).strip().lower() != "midpoint":
         return "fourth-order flux quadrature"
-    tables = [k for k in p if k.endswith("_table") and str(p[k]).strip()]
-    if tables:
-        return "time tables (" + ", ".join(tables) + ")"
-    if (_num(p.get("reynolds", 0)) or 0.0) > 0.0:
-        return "reynolds > 0 (give mu)"
     if _flag(p["use_ibm"]):
         moving = [k for k in ("ibm_vx", "ibm_vy", "ibm_vz", "ibm_omega", "ibm_omega_x", "ibm_omega_y", "ibm_mass") if (_num(p.get(k, 0)) or 0.0) != 0.0]
         if moving:
             return "a moving immersed body (" + ", ".join(moving) + ")"
     return None
+
+
+def read_time_table(path):
+    """The rows (t, value) of a boundary time table (read_time_table, cpp/src/SimulationInternal.hpp:62-99): one row per
+    line, comma- or space-separated, '#' comments and blank lines skipped, an optional 't,value' / 'time,value' header
+    before the first row, a UTF-8 byte-order mark dropped; finite values, strictly increasing times, at least two rows."""
+    rows = []
+    with open(path, "rb") as f:
+        text = f.read()
+    if text.startswith(b"\xef\xbb\xbf"):
+        text = text[3:]
+    for n, raw in enumerate(text.decode().split("\n"), 1):
+        line = raw.strip(" \t\r")
+        if not line or line.startswith("#"):
+            continue
+        parts = line.replace(",", " ").split()
+        try:
+            t, v = float(parts[0]), float(parts[1])
+        except (ValueError, IndexError):
+            if not rows and len(parts) == 2 and parts[0].lower() in ("t", "time") and parts[1].lower() == "value":
+                continue
+            raise ValueError(f"{path}:{n} must contain t,value") from None
+        if len(parts) > 2:
+            raise ValueError(f"{path}:{n} has more than two columns")
+        if not (abs(t) < float("inf") and abs(v) < float("inf")):
+            raise ValueError(f"{path}:{n} values must be finite")
+        if rows and not t > rows[-1][0]:
+            raise ValueError(f"{path}: times must be strictly increasing")
+        rows.append((t, v))
+    if len(rows) < 2:
+        raise ValueError(f"{path} must contain at least two (t,value) rows")
+    return rows
+
+
+def _bound_names(p):
+    """The names the reference's Evaluator binds besides x, y, z, t: every numeric run parameter (Lx .. nz are bound again
+    from the mesh by the library)."""
+    out = []
+    for k, v in p.items():
+        if k in ("x", "y", "z", "t") or isinstance(v, bool):
+            continue
+        n = _num(v)
+        if n is not None:
+            out.append((str(k), n))
+    return out
+
+
+def _initial_boundary_value(p, key):
+    """u_in / v_in / rho_in / p_out at t = 0 (load_boundary_functions, cpp/src/Simulation.cpp:145-153)."""
+    table = str(p.get(key + "_table", "") or "").strip()
+    if table:
+        return read_time_table(table)[0][1]
+    v = _num(p[key])
+    if v is not None:
+        return v
+    from .runtime import eval_expression
+
+    return float(eval_expression(str(p[key]), _bound_names(p) + [(k, float(p[k])) for k in ("Lx", "Ly", "Lz", "nx", "ny", "nz")], [0.0], [0.0], [0.0], 0.0)[0])
 
 
 def to_config(params, precision=0, device=0):
@@ -131,7 +186,38 @@ def to_config(params, precision=0, device=0):
     c.gamma, c.p_inf = float(p["gamma"]), float(p["p_inf"])
     for s, key in enumerate(("bc_xmin", "bc_xmax", "bc_ymin", "bc_ymax", "bc_zmin", "bc_zmax")):
         c.bc[s] = _pick(BC_NAMES, p[key], "boundary condition type")
-    c.u_in, c.v_in, c.rho_in, c.p_out = float(p["u_in"]), float(p["v_in"]), float(p["rho_in"]), float(p["p_out"])
+    # u_in, v_in, rho_in, p_out: numbers, expressions of t or time tables (load_boundary_functions, Simulation.cpp:118-168)
+    keep = []
+    for k, key in enumerate(BOUNDARY_KEYS):
+        v = _num(p[key])
+        setattr(c, key, v if v is not None else (1.0 if key in ("rho_in", "p_out") else 0.0))
+        if v is None:
+            c.boundary_expr[k] = str(p[key]).encode()
+        table = str(p.get(key + "_table", "") or "").strip()
+        if table:
+            if v is None:
+                raise ValueError(f"{key} expression and {key}_table cannot both be set")
+            rows = (ctypes.c_double * (2 * len(read_time_table(table))))(*[x for r in read_time_table(table) for x in r])
+            keep.append(rows)
+            c.boundary_table[k] = ctypes.cast(rows, ctypes.POINTER(ctypes.c_double))
+            c.boundary_table_rows[k] = len(rows) // 2
+    # reynolds > 0: mu from the body's length scale and the inflow at t = 0 (Simulation.cpp:154-167)
+    if (_num(p.get("reynolds", 0)) or 0.0) > 0.0:
+        rho0, u0 = _initial_boundary_value(p, "rho_in"), _initial_boundary_value(p, "u_in")
+        if not (rho0 > 0.0 and u0 > 0.0):
+            raise ValueError("reynolds needs positive u_in and rho_in at t=0 (including boundary tables)")
+        p = dict(p, mu=rho0 * u0 * (2.0 * float(p["ibm_radius"])) / float(p["reynolds"]))
+    for q, key in enumerate(SOURCE_KEYS):
+        c.source[q] = str(p.get(key, "0")).encode()
+    names = _bound_names(p)
+    c.nparams = len(names)
+    if names:
+        cn = (ctypes.c_char_p * len(names))(*[k.encode() for k, _ in names])
+        cv = (ctypes.c_double * len(names))(*[v for _, v in names])
+        keep += [cn, cv]
+        c.param_names = ctypes.cast(cn, ctypes.POINTER(ctypes.c_char_p))
+        c.param_values = ctypes.cast(cv, ctypes.POINTER(ctypes.c_double))
+    c._keep = keep   # the arrays the pointers above point into live as long as the configuration
     c.riemann = _pick(RIEMANN_NAMES, p["riemann_solver"], "Riemann solver")
     c.shock_blend = float(p["shock_blend"])
     c.reconstruction = _pick(RECON_NAMES, p["reconstruction"], "reconstruction")
@@ -155,6 +241,7 @@ def to_config(params, precision=0, device=0):
     c.gx, c.gy, c.gz = float(p["gx"]), float(p["gy"]), float(p["gz"])
     c.nrbc_sigma, c.nrbc_beta = float(p["nrbc_sigma"]), float(p["nrbc_beta"])
     c.positivity_fallback = 1 if _flag(p["positivity_fallback"]) else 0
+    c.mu = float(p["mu"])   # (derived from reynolds above when given)
     return c
 
 
@@ -172,4 +259,12 @@ def load_case(path, overrides=None):
             if not isinstance(v, (dict, list)):
                 params[k] = v
     params.update(overrides or {})
+    # a boundary time table is looked for next to the case file, then in the current folder (Simulation.cpp:128-139)
+    import os
+
+    for k, v in list(params.items()):
+        if k.endswith("_table") and isinstance(v, str) and v.strip() and not os.path.isabs(v.strip()):
+            beside = os.path.join(os.path.dirname(os.path.abspath(path)), v.strip())
+            if os.path.exists(beside):
+                params[k] = beside
     return params, doc.get("initial", {})

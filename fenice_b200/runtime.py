@@ -20,13 +20,13 @@ from . import params as P
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfenice_gpu.so")
 
-FVG_OK, FVG_ERR_CONFIG, FVG_ERR_ARGUMENT, FVG_ERR_CUDA, FVG_ERR_DIVERGED, FVG_ERR_STATE = range(6)
+FVG_OK, FVG_ERR_CONFIG, FVG_ERR_ARGUMENT, FVG_ERR_CUDA, FVG_ERR_DIVERGED, FVG_ERR_STATE, FVG_ERR_BOUNDARY = range(7)
 
 StepResult = namedtuple("StepResult", ["dt", "s_max"])
 
 # every entry point of include/fenice_gpu.h
 EXPORTS = ["fvg_abi_version", "fvg_create", "fvg_destroy", "fvg_last_error", "fvg_create_error", "fvg_upload_state",
-           "fvg_download_state", "fvg_residual", "fvg_step", "fvg_run_until", "fvg_get_time", "fvg_set_time",
+           "fvg_download_state", "fvg_residual", "fvg_step", "fvg_run_until", "fvg_get_time", "fvg_set_time", "fvg_set_stage_time",
            "fvg_get_lagged_speed", "fvg_set_lagged_speed", "fvg_dt_length", "fvg_device_state", "fvg_stream",
            "fvg_synchronize", "fvg_face_flux_batch", "fvg_set_timing", "fvg_get_timing",
            "fvg_residual_noalloc",
@@ -35,10 +35,11 @@ EXPORTS = ["fvg_abi_version", "fvg_create", "fvg_destroy", "fvg_last_error", "fv
            "fvg_batch_get_schedule", "fvg_batch_stream", "fvg_batch_set_timing", "fvg_batch_get_timing",
            "fvg_sensor_sizes", "fvg_sensor_extract", "fvg_sensor_grad", "fvg_sensor_adam", "fvg_sensor_pack", "fvg_sensor_infer",
            "fvg_set_sensor", "fvg_get_sensor_counts", "fvg_ibm_loads",
-           "fvg_create_part", "fvg_part_info", "fvg_part_buffers", "fvg_part_begin", "fvg_part_phase", "fvg_part_status"]
+           "fvg_create_part", "fvg_part_info", "fvg_part_buffers", "fvg_part_begin", "fvg_part_phase", "fvg_part_status",
+           "fvg_expr_eval"]
 
 _lib = None
-ABI_VERSION = 4   # FVG_ABI_VERSION of include/fenice_gpu.h
+ABI_VERSION = 5   # FVG_ABI_VERSION of include/fenice_gpu.h
 
 
 def load_library(path=LIB_PATH):
@@ -66,6 +67,7 @@ def load_library(path=LIB_PATH):
     lib.fvg_run_until.argtypes = [c_p, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.fvg_get_time.argtypes = [c_p, dp]
     lib.fvg_set_time.argtypes = [c_p, ctypes.c_double]
+    lib.fvg_set_stage_time.argtypes = [c_p, ctypes.c_double]
     lib.fvg_get_lagged_speed.argtypes = [c_p, dp]
     lib.fvg_set_lagged_speed.argtypes = [c_p, ctypes.c_double]
     lib.fvg_dt_length.argtypes = [c_p, dp]
@@ -110,8 +112,28 @@ def load_library(path=LIB_PATH):
     lib.fvg_part_begin.argtypes = [c_p, ctypes.c_double, ctypes.c_int]
     lib.fvg_part_phase.argtypes = [c_p, ctypes.c_int, ip, ip]
     lib.fvg_part_status.argtypes = [c_p, ip, ip, dp, dp, dp]
+    lib.fvg_expr_eval.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_char_p), dp, ctypes.c_int, dp, dp, dp, ctypes.c_double, ctypes.c_size_t, dp,
+                                  ctypes.c_char_p, ctypes.c_size_t]
     _lib = lib
     return lib
+
+
+def eval_expression(src, names, x, y, z, t=0.0):
+    """A case-file expression evaluated on the host by the library's compiler (fvg_expr_eval: the reference's grammar
+    and the C library's functions) at the points (x, y, z) and time t. `names`: a dict or (name, value) pairs bound
+    after x, y, z, t (later ones replace earlier ones). ValueError for an expression the grammar refuses."""
+    lib = load_library()
+    pairs = list(names.items()) if isinstance(names, dict) else list(names)
+    n = len(x)
+    arrs = [np.ascontiguousarray(np.broadcast_to(np.asarray(a, dtype=np.float64), (n,))) for a in (x, y, z)]
+    out = np.empty(n)
+    cn = (ctypes.c_char_p * max(1, len(pairs)))(*[k.encode() for k, _ in pairs])
+    cv = np.array([float(v) for _, v in pairs] or [0.0])
+    err = ctypes.create_string_buffer(512)
+    rc = lib.fvg_expr_eval(str(src).encode(), cn, _dp(cv), len(pairs), _dp(arrs[0]), _dp(arrs[1]), _dp(arrs[2]), float(t), n, _dp(out), err, 512)
+    if rc != 0:
+        raise ValueError(err.value.decode())
+    return out
 
 
 def _dp(a):
@@ -188,6 +210,11 @@ class Run:
         self._check(self.lib.fvg_residual(self.h, float(predictor_half_dt), _dp(R) if want_R else None, self.ncells if want_R else 0,
                                           ctypes.byref(s)), "residual")
         return R, s.value
+
+    def set_stage_time(self, t=float("nan")):
+        """The time at which the next residual() evaluates time-dependent source terms and boundary values
+        (TimeScheme::stage_time); NaN: the run's time (plus predictor_half_dt for a MUSCL-Hancock residual)."""
+        self._check(self.lib.fvg_set_stage_time(self.h, float(t)), "stage time")
 
     def step(self, t_end):
         dt, s = ctypes.c_double(), ctypes.c_double()

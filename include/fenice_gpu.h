@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define FVG_ABI_VERSION 4
+#define FVG_ABI_VERSION 5
 
 /* status codes */
 enum {
@@ -35,7 +35,9 @@ enum {
     FVG_ERR_ARGUMENT = 2,    /* bad pointer or size */
     FVG_ERR_CUDA = 3,        /* a CUDA call failed (no device, out of memory, launch failure) */
     FVG_ERR_DIVERGED = 4,    /* non-finite wave speed or time step, or t no longer advances (check_progress) */
-    FVG_ERR_STATE = 5        /* the state is not valid for the mesh (e.g. rho w != 0 on a 2-D mesh) */
+    FVG_ERR_STATE = 5,       /* the state is not valid for the mesh (e.g. rho w != 0 on a 2-D mesh) */
+    FVG_ERR_BOUNDARY = 6     /* a time-dependent boundary value was not finite, or rho_in or p_out not positive, at a
+                                stage time (Simulation::update_boundary_values, cpp/src/Simulation.cpp:170-185) */
 };
 
 /* enumerations, in the reference's order */
@@ -78,6 +80,23 @@ typedef struct fvg_config {
     double nrbc_sigma, nrbc_beta; /* [boundaries] the non-reflecting outlet's relaxation (0.28) and transverse weight (-1: local Mach) */
     int positivity_fallback;     /* [numerics] positivity_fallback: a stage that leaves a cell without density or pressure is
                                     repeated with first-order faces around it (WENO3-Z / WENO5-Z, FP64) */
+    /* Case-file expressions, in the reference's expression grammar (TinyExpr with right-to-left ^; a whole number is
+     * read with strtod). They may use x, y, z (cell centres), t, the parameters param_names / param_values (bound in
+     * order, a later name replacing an earlier one, as the reference's Evaluator binds every numeric run parameter,
+     * cpp/src/CaseFile.cpp:299-333) and then Lx, Ly, Lz, nx, ny, nz of the mesh. FP64 form only. */
+    const char* source[5];       /* [source] source_rho, source_mx, source_my, source_E, source_mz (NULL: "0"): the source
+                                    terms added to R after the viscous term and the body force (RhsSourceTerms,
+                                    cpp/include/fv/Physics.hpp:21-47, cpp/src/Simulation.cpp:397-412); evaluated once at
+                                    t = 0, or at every stage time when one of them reads t (source_unsteady). source_mz
+                                    must be 0 on a 2-D mesh. */
+    const char* boundary_expr[4];      /* u_in, v_in, rho_in, p_out as expressions of t (NULL: the constants above) */
+    const double* boundary_table[4];   /* or as time tables ([boundaries] u_in_table ...): boundary_table_rows[k] rows of
+                                          (t, value), linear between rows, constant outside (read_time_table /
+                                          table_value, cpp/src/SimulationInternal.hpp:62-111) */
+    int boundary_table_rows[4];
+    const char* const* param_names;
+    const double* param_values;
+    int nparams;
 } fvg_config;
 
 typedef struct fvg_run fvg_run;
@@ -135,6 +154,15 @@ int fvg_part_status(fvg_run* run, int* active, int* steps, double* t, double* dt
 
 int fvg_get_time(const fvg_run* run, double* t);
 int fvg_set_time(fvg_run* run, double t);
+/* The time at which the next fvg_residual calls evaluate time-dependent source terms and boundary values
+ * (TimeScheme::stage_time, cpp/include/fv/TimeScheme.hpp:88); NaN (the default): the run's time t, plus
+ * predictor_half_dt for a MUSCL-Hancock residual. The time loop (fvg_step, fvg_run_until, parts) sets its own. */
+int fvg_set_stage_time(fvg_run* run, double t);
+/* Evaluates one case-file expression on the host (the C library's functions, the reference's values bit for bit) at n
+ * points (x, y, z may be NULL: 0) and time t, with the names bound as in fvg_config. Returns FVG_OK, or FVG_ERR_CONFIG
+ * with the reason in err (errlen bytes) for an expression the grammar refuses. */
+int fvg_expr_eval(const char* expr, const char* const* names, const double* values, int nnames, const double* x, const double* y,
+                  const double* z, double t, size_t n, double* out, char* err, size_t errlen);
 /* The MUSCL-Hancock lagged wave speed (the reference's checkpoint key S; 0: the next step seeds it). */
 int fvg_get_lagged_speed(const fvg_run* run, double* s);
 int fvg_set_lagged_speed(fvg_run* run, double s);

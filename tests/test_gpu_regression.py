@@ -1,8 +1,9 @@
 """The reference's own regression fixtures (its cpp/tests/reference/*.npz, with their inputs, in
 tests/golden/regression.npz) run through the device path: every case the device computes reaches the reference's step
 count and its final state within the reference's bar (relative difference per variable below 1e-8,
-cpp/tests/regression.py), and equals bit for bit the reference compiled from its sources (the fixture's U_here); every
-case that needs a feature the device does not compute is refused before anything runs."""
+cpp/tests/regression.py), and equals bit for bit the reference compiled from its sources (the fixture's U_here), except
+a case whose source terms read t: evaluated on the device with CUDA's functions at every stage, its state is within
+1e-12 (relative, per variable) of the reference's."""
 import numpy as np
 import pytest
 
@@ -25,10 +26,14 @@ def test_device_reproduces_reference_regression_state(name):
     d = rc.rel_diff(U, FX[f"{name}/U"])
     here = FX[f"{name}/U_here"]
     exact = rc.bits_equal(U[:, : here.shape[1]], here)
+    d_here = rc.rel_diff(U, here)
     print(f"\n{name}: {steps} steps, relative difference from the stored state {d:.3g}, "
-          f"bit-exact vs the reference compiled here: {exact}")
+          f"bit-exact vs the reference compiled here: {exact} (relative difference {d_here:.3g})")
     assert d < rc.TOL
-    assert exact
+    if name in rc.DEVICE_MATH:
+        assert d_here < rc.DEVICE_MATH_TOL
+    else:
+        assert exact
 
 
 @pytest.mark.parametrize("name", sorted(rc.NOT_ON_DEVICE))

@@ -1,7 +1,7 @@
 """The reference's own regression fixtures (its cpp/tests/reference/*.npz final states, extracted with their inputs into
 tests/golden/regression.npz by tests/golden/make_regression.py) against the C restatement (oracle/): the same step count
-and the reference's own bar (relative difference per variable below 1e-8, cpp/tests/regression.py); and the refusal of
-the features the device path does not compute, by the parameter layer, before anything runs."""
+and the reference's own bar (relative difference per variable below 1e-8, cpp/tests/regression.py); and every case's
+configuration accepted by the parameter layer."""
 import numpy as np
 import pytest
 
@@ -39,13 +39,7 @@ def test_oracle_reproduces_reference_regression_state(name):
     assert rc.bits_equal(U[:, : FX[f"{name}/U_here"].shape[1]], FX[f"{name}/U_here"])
 
 
-@pytest.mark.parametrize("name", sorted(n for n, why in rc.NOT_ON_DEVICE.items() if why == "source terms"))
-def test_parameter_layer_refuses_features_not_on_device(name):
-    with pytest.raises(ValueError, match=rc.NOT_ON_DEVICE[name]):
-        fparams.to_config(rc.params(FX, name))
-
-
-def test_parameter_layer_accepts_every_other_case():
-    for n in NAMES:   # (the mass-flow inlet and the non-reflecting outlet are refused by fvg_create)
-        if rc.NOT_ON_DEVICE.get(n) != "source terms":
-            assert fparams.not_on_device(rc.params(FX, n)) is None, n
+def test_parameter_layer_accepts_every_case():
+    for n in NAMES:   # (the case-file source terms included: they run on the device)
+        assert fparams.not_on_device(rc.params(FX, n)) is None, n
+        fparams.to_config(rc.params(FX, n))
