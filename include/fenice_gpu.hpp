@@ -9,6 +9,7 @@
 // (e.g. the reference's std::vector<std::array<double, 5>>).
 #pragma once
 
+#include <limits>
 #include <stdexcept>
 #include <string>
 
@@ -81,6 +82,8 @@ public:
         return t;
     }
     void set_time(double t) { check(fvg_set_time(h_, t), "time", fvg_last_error(h_)); }
+    // the time the next residual evaluates time-dependent sources and boundary values at (NaN: the run's time)
+    void set_stage_time(double t) { check(fvg_set_stage_time(h_, t), "stage time", fvg_last_error(h_)); }
 
 private:
     fvg_run* h_ = nullptr;
@@ -88,16 +91,19 @@ private:
 };
 
 // The residual seam of the reference (`ResidualFn`): usable wherever a `std::function<double(const Field&, Field&)>` is,
-// e.g. as the `res` argument of the reference's TimeScheme::step. `predictor_half_dt` is read at each call, so a caller
-// that drives MUSCL-Hancock sets it from its scheme's predictor_half_dt before the call.
+// e.g. as the `res` argument of the reference's TimeScheme::step. `predictor_half_dt` and `stage_time` are read at each
+// call, so a caller sets them from its scheme's predictor_half_dt and stage_time before the call (stage_time NaN: the
+// run's time).
 template <class Field> class GpuResidual {
 public:
     explicit GpuResidual(GpuRun& run) : run_(run) {}
     double operator()(const Field& U, Field& R) {
         run_.upload(U);
+        run_.set_stage_time(stage_time);
         return run_.residual(R, predictor_half_dt);
     }
     double predictor_half_dt = 0.0;
+    double stage_time = std::numeric_limits<double>::quiet_NaN();
 
 private:
     GpuRun& run_;

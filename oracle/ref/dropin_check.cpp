@@ -16,6 +16,7 @@
 #include "fenice_gpu.hpp"
 
 #include <cstdio>
+#include <vector>
 #include <cstring>
 #include <filesystem>
 #include <fstream>
@@ -80,10 +81,45 @@ static fvg_config to_fvg(const fv::SimParams& p) {
     c.nrbc_sigma = p.nrbc_sigma;
     c.nrbc_beta = p.nrbc_beta;
     c.positivity_fallback = p.positivity_fallback ? 1 : 0;
+    // case-file expressions: the source terms, boundary values given as expressions of t, and every numeric parameter
+    // bound by name (the strings live in `keep` until fvg_create has compiled them)
+    static std::vector<std::string> keep;
+    static std::vector<const char*> names;
+    static std::vector<double> values;
+    keep.clear();
+    keep.reserve(64 + p.source.values().size());
+    static const char* const skeys[5] = {"source_rho", "source_mx", "source_my", "source_E", "source_mz"};
+    for (int q = 0; q < 5; ++q) c.source[q] = keep.emplace_back(p.source.str(skeys[q], "0")).c_str();
+    static const char* const bkeys[4] = {"u_in", "v_in", "rho_in", "p_out"};
+    for (int k = 0; k < 4; ++k) {
+        const std::string raw = p.source.str(bkeys[k], k >= 2 ? "1.0" : "0.0");
+        char* end = nullptr;
+        std::strtod(raw.c_str(), &end);
+        if (!(end && end != raw.c_str() && *end == '\0')) c.boundary_expr[k] = keep.emplace_back(raw).c_str();
+    }
+    names.clear();
+    values.clear();
+    for (const auto& [k, v] : p.source.values()) {
+        char* end = nullptr;
+        const double d = std::strtod(v.c_str(), &end);
+        while (end && (*end == ' ' || *end == '\t')) ++end;
+        if (!v.empty() && end && *end == '\0') {
+            names.push_back(keep.emplace_back(k).c_str());
+            values.push_back(d);
+        }
+    }
+    c.param_names = names.data();
+    c.param_values = values.data();
+    c.nparams = (int)names.size();
     return c;
 }
 
 int main(int argc, char** argv) {
+    if (fvg_abi_version() != FVG_ABI_VERSION) {   // fvg_config's layout must be the one this file was compiled with
+        std::fprintf(stderr, "libfenice_gpu.so has ABI %d, this check was built for %d: rebuild it (make -C oracle/ref dropin)\n",
+                     fvg_abi_version(), FVG_ABI_VERSION);
+        return 2;
+    }
     const std::string which = argc > 1 ? argv[1] : "vortex";
     const int nsteps = argc > 2 ? std::atoi(argv[2]) : 10;
     char tmpl[] = "/tmp/fenice_dropin_XXXXXX";
@@ -116,6 +152,19 @@ int main(int argc, char** argv) {
                         {"time_scheme", "SSP Runge-Kutta 3"}, {"use_viscous", "true"}, {"mu", "6.25e-4"}, {"pr", "0.71"}, {"bc_xmin", "periodic"},
                         {"bc_xmax", "periodic"}, {"bc_ymin", "periodic"}, {"bc_ymax", "periodic"}})
             P.set(kv.first, kv.second);
+    } else if (which == "sources") {   // unsteady sources and boundary values of t (arithmetic: the same bits on the device)
+        for (auto kv : {std::pair<const char*, const char*>{"nx", "64"}, {"ny", "48"}, {"Lx", "2"}, {"Ly", "1"}, {"reconstruction", "muscl"},
+                        {"muscl_limiter", "MC"}, {"time_scheme", "MUSCL-Hancock"}, {"bc_xmin", "vel_inlet"}, {"bc_xmax", "outlet"},
+                        {"bc_ymin", "periodic"}, {"bc_ymax", "periodic"}, {"u_in", "0.3 + 0.5*t"}, {"v_in", "0.05*t"}, {"p_out", "1 - 0.1*t"},
+                        {"source_rho", "0.01*(x - 0.5)*(y - 0.25)*(1 + t)"}, {"source_mx", "0.02*x*x - 0.01*t"}, {"source_my", "-0.03*y*t"},
+                        {"source_E", "0.05*(x + y)*(1 - 2*t) + gamma*0.001"}})
+            P.set(kv.first, kv.second);
+    } else if (which == "sources_rk3") {   // steady sources with transcendental functions (evaluated once on the host)
+        for (auto kv : {std::pair<const char*, const char*>{"nx", "48"}, {"ny", "48"}, {"reconstruction", "weno5"}, {"time_scheme", "SSP Runge-Kutta 3"},
+                        {"bc_xmin", "periodic"}, {"bc_xmax", "periodic"}, {"bc_ymin", "periodic"}, {"bc_ymax", "periodic"},
+                        {"source_rho", "0.1*sin(2*pi*x)*cos(2*pi*y)"}, {"source_mx", "0.05*exp(-x)"}, {"source_my", "0.02*log(1 + y)"},
+                        {"source_E", "0.2*tanh(x - y)"}})
+            P.set(kv.first, kv.second);
     } else {
         for (auto kv : {std::pair<const char*, const char*>{"nx", "96"}, {"ny", "96"}, {"reconstruction", "weno5"}, {"time_scheme", "SSP Runge-Kutta 3"},
                         {"cfl", "0.4"}, {"bc_xmin", "transmissive"}, {"bc_xmax", "transmissive"}, {"bc_ymin", "transmissive"},
@@ -132,6 +181,7 @@ int main(int argc, char** argv) {
     fvg::GpuResidual<fv::Field> gpu(run);
     const fv::ResidualFn gpu_res = [&](const fv::Field& U, fv::Field& R) {
         gpu.predictor_half_dt = host.scheme->predictor_half_dt;
+        gpu.stage_time = host.scheme->stage_time;
         return gpu(U, R);
     };
     const fv::ResidualFn ref_res = [&](const fv::Field& U, fv::Field& R) { return ref.residual(U, R); };
