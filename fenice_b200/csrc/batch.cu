@@ -264,6 +264,7 @@ std::string batch_config_error(const fvg_config* cfgs, int n) {
             if (c.bc[s] == FVG_BC_MASSFLOWINLET || c.bc[s] == FVG_BC_NONREFLECTING)
                 return "problem " + std::to_string(p) + ": batched problems have no mass-flow inlet or non-reflecting outlet";
         if (c.time_scheme == FVG_TS_HANCOCK) return "problem " + std::to_string(p) + ": batched problems use Euler, SSP-RK2 or SSP-RK3";
+        if (c.flux_quadrature != 0) return "problem " + std::to_string(p) + ": batched problems use the midpoint flux quadrature";
         if (config_has_expressions(c))
             return "problem " + std::to_string(p) + ": batched problems have no case-file source terms or time-dependent boundary values";
         if (c.reconstruction != a.reconstruction || c.riemann != a.riemann || c.time_scheme != a.time_scheme || c.precision != a.precision ||

@@ -18,6 +18,7 @@
 // step runs (t < t_end, step limit, no error).
 #include "../../include/fenice_gpu.h"
 #include "expr.cuh"
+#include "fourth.cuh"
 #include "hancock.cuh"
 #include "ibm.cuh"
 #include "host_common.h"
@@ -531,6 +532,10 @@ struct fvg_run {
     bool src_on = false, src_unsteady = false, tv_on = false;
     double* d_src = nullptr;
     double* d_tv = nullptr;
+    // flux_quadrature = fourth: the face arrays of the face passes (fourth.cuh; one allocation, d_fourth)
+    bool fourth = false;
+    FourthArgs fa{};
+    void* d_fourth = nullptr;
     double res_time = NAN;   // fvg_set_stage_time (NaN: the run's time)
     int res_kind = -1;       // the stage-time kind residual_stage takes (-1: its stage index)
     double* Ucur() { return cur ? Ut : U; }
@@ -601,6 +606,13 @@ std::string validate(const fvg_config& c) {
     if (has_expressions(c) && c.precision == FVG_PREC_MIXED)
         return "case-file source terms and time-dependent boundary values run in the FP64 form only";
     if (c.nparams < 0 || (c.nparams > 0 && (!c.param_names || !c.param_values))) return "param_names / param_values missing";
+    if (c.flux_quadrature != 0 && c.flux_quadrature != 1) return "flux_quadrature must be midpoint (0) or fourth (1)";
+    if (c.flux_quadrature == 1) {   // Params.cpp:450-456
+        if (c.reconstruction != FVG_RECON_WENO3 && c.reconstruction != FVG_RECON_WENO5) return "flux_quadrature = fourth needs reconstruction = weno3 or weno5";
+        if (c.use_ibm) return "flux_quadrature = fourth is not available with an immersed body yet";
+        if (c.positivity_fallback) return "positivity_fallback needs flux_quadrature = midpoint";
+        if (c.precision != FVG_PREC_FP64) return "flux_quadrature = fourth runs in the FP64 form only";
+    }
     if (c.positivity_fallback) {   // Params.cpp:464-467
         if (c.reconstruction != FVG_RECON_WENO3 && c.reconstruction != FVG_RECON_WENO5)
             return "positivity_fallback needs reconstruction = weno3 or weno5 (the other schemes keep their reconstructed states between the cells)";
@@ -807,6 +819,50 @@ cudaError_t launch_visc(fvg_run* r, const double* Uin, double* bmv, const int* g
     return e;
 }
 
+// The residual stage of flux_quadrature = fourth: the face passes of fourth.cuh with the stage's arguments.
+template <int DIM, int RIEMANN> cudaError_t fourth_stage_t(fvg_run* r, const StageArgs& sa) {
+    constexpr int NV = DIM == 3 ? 5 : 4;
+    FourthArgs a = r->fa;
+    a.m = sa.m;
+    a.bc = sa.bc;
+    a.eos = sa.eos;
+    a.U = sa.U;
+    a.mode = sa.mode;
+    a.ca = sa.ca;
+    a.cb = sa.cb;
+    a.U0 = sa.U0;
+    a.out = sa.out;
+    a.Rv = sa.Rv;
+    a.blockmax = sa.blockmax;
+    a.ctl = sa.ctl;
+    a.gate = sa.gate;
+    auto grid = [](long long n) { return (int)std::min<long long>((n + 255) / 256, 148 * 16); };
+    cudaStream_t s = r->stream;
+    if (r->cfg.reconstruction == FVG_RECON_WENO5) {
+        k4_recon<DIM, NV, 0, true><<<grid(a.nf[0]), 256, 0, s>>>(a);
+        k4_recon<DIM, NV, 1, true><<<grid(a.nf[1]), 256, 0, s>>>(a);
+        if constexpr (DIM == 3) k4_recon<DIM, NV, 2, true><<<grid(a.nf[2]), 256, 0, s>>>(a);
+    } else {
+        k4_recon<DIM, NV, 0, false><<<grid(a.nf[0]), 256, 0, s>>>(a);
+        k4_recon<DIM, NV, 1, false><<<grid(a.nf[1]), 256, 0, s>>>(a);
+        if constexpr (DIM == 3) k4_recon<DIM, NV, 2, false><<<grid(a.nf[2]), 256, 0, s>>>(a);
+    }
+    k4_point<DIM, NV, 0><<<grid(a.nf[0]), 256, 0, s>>>(a);
+    k4_point<DIM, NV, 1><<<grid(a.nf[1]), 256, 0, s>>>(a);
+    if constexpr (DIM == 3) k4_point<DIM, NV, 2><<<grid(a.nf[2]), 256, 0, s>>>(a);
+    k4_flux<DIM, NV, RIEMANN><<<r->nb, 256, 0, s>>>(a);   // (one CTA per stage tile: the speeds go where the stage kernel's go)
+    k4_correct<DIM, NV, RIEMANN, 0><<<grid(a.nf[0]), 256, 0, s>>>(a);
+    k4_correct<DIM, NV, RIEMANN, 1><<<grid(a.nf[1]), 256, 0, s>>>(a);
+    if constexpr (DIM == 3) k4_correct<DIM, NV, RIEMANN, 2><<<grid(a.nf[2]), 256, 0, s>>>(a);
+    k4_balance<DIM, NV><<<grid(r->m.ncells), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t fourth_stage(fvg_run* r, const StageArgs& sa) {
+    if (r->dim == 3) return r->cfg.riemann == FVG_RIEMANN_LOWMACH ? fourth_stage_t<3, kLowMach>(r, sa) : fourth_stage_t<3, kHLLC>(r, sa);
+    return r->cfg.riemann == FVG_RIEMANN_LOWMACH ? fourth_stage_t<2, kLowMach>(r, sa) : fourth_stage_t<2, kHLLC>(r, sa);
+}
+
 // The source field's planes of a run: its own planes and, for a part, the ghost planes beyond its interfaces.
 void source_planes(const fvg_run* r, int* split, int* first, int* lo, int* hi) {
     *split = r->is_part ? r->split : (r->dim == 3 ? 2 : 1);
@@ -845,7 +901,7 @@ cudaError_t residual_stage(fvg_run* r, const double* Uin, const double* U0, doub
     timer_mark(r, r->t_stage);
     StageArgs sa = stage_args(r, Uin, U0, out, mode, ca, cb, r->cfg.use_viscous ? r->Rv : nullptr, r->bm[stage], gate);
     sa.fb = fb;
-    e = r->stage.launch(sa, r->nb, r->stream);
+    e = r->fourth ? fourth_stage(r, sa) : r->stage.launch(sa, r->nb, r->stream);
     timer_mark(r, r->t_stage);
     return e;
 }
@@ -1332,6 +1388,10 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
             g_create_error = "each part needs at least " + std::to_string(depth) + " planes along the split axis";
             return FVG_ERR_CONFIG;
         }
+        if (cfg->flux_quadrature == 1) {   // Params.cpp:454
+            g_create_error = "flux_quadrature = fourth is serial yet (its corrections read faces two cells across a part interface)";
+            return FVG_ERR_CONFIG;
+        }
         if (cfg->positivity_fallback) {   // the flags of the neighbours' cells would have to be exchanged too
             g_create_error = "a decomposed mesh cannot use positivity_fallback";
             return FVG_ERR_CONFIG;
@@ -1502,6 +1562,41 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
             run->bc.u_target = run->d_utarget;
         }
     if (const int rc = upload_expressions(run, prog)) return bail(rc);
+    if (c.flux_quadrature == 1) {   // the face arrays: per axis 6 x nvar doubles and 3 flag bytes per face
+        run->fourth = true;
+        FourthArgs& fa = run->fa;
+        fa.shock_blend = c.shock_blend;
+        fa.weno_eps = c.weno_epsilon;
+        size_t bytes = 0;
+        for (int a = 0; a < run->dim; ++a) {
+            fa.periodic[a] = c.bc[2 * a] == FVG_BC_PERIODIC && c.bc[2 * a + 1] == FVG_BC_PERIODIC;
+            fa.nf[a] = (long long)(c.nx + (a == 0)) * (c.ny + (a == 1)) * (c.nz + (a == 2));
+            bytes += (size_t)fa.nf[a] * (6 * run->nvar * sizeof(double) + 3);
+        }
+        bytes += 256 * 9 * 3;
+        if (cudaMalloc(&run->d_fourth, bytes) != cudaSuccess) {
+            run->err = "device allocation of the fourth-order face arrays failed";
+            return bail(FVG_ERR_CUDA);
+        }
+        char* p = static_cast<char*>(run->d_fourth);
+        auto take = [&](size_t n) {
+            char* q = p;
+            p += (n + 255) / 256 * 256;
+            return q;
+        };
+        for (int a = 0; a < run->dim; ++a) {
+            const size_t nd = (size_t)fa.nf[a] * run->nvar * sizeof(double);
+            fa.UL[a] = reinterpret_cast<double*>(take(nd));
+            fa.UR[a] = reinterpret_cast<double*>(take(nd));
+            fa.AL[a] = reinterpret_cast<double*>(take(nd));
+            fa.AR[a] = reinterpret_cast<double*>(take(nd));
+            fa.Fp[a] = reinterpret_cast<double*>(take(nd));
+            fa.F[a] = reinterpret_cast<double*>(take(nd));
+            fa.good[a] = reinterpret_cast<unsigned char*>(take(fa.nf[a]));
+            fa.pt[a] = reinterpret_cast<unsigned char*>(take(fa.nf[a]));
+            fa.full[a] = reinterpret_cast<unsigned char*>(take(fa.nf[a]));
+        }
+    }
     const int nbmax = run->nb > run->nbh ? run->nb : run->nbh;
     for (int s = 0; s < 3; ++s)
         if (cudaMalloc(&run->bm[s], sizeof(double) * nbmax) != cudaSuccess || cudaMalloc(&run->bmv[s], sizeof(double) * run->nbv) != cudaSuccess) {
@@ -1593,6 +1688,7 @@ int fvg_destroy(fvg_run* run) {
         if (p) cudaFree(p);
     if (run->ctl) cudaFree(run->ctl);
     if (run->d_code) cudaFree(run->d_code);
+    if (run->d_fourth) cudaFree(run->d_fourth);
     if (run->fb_flags) cudaFree(run->fb_flags);
     if (run->fb_grew) cudaFree(run->fb_grew);
     if (run->sens) cudaFree(run->sens);
@@ -2117,6 +2213,7 @@ extern "C" int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long
     if (cfg->precision != FVG_PREC_FP64) return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: the FP64 form only");
     if (cfg->use_ibm) return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: an immersed body needs its tables on the device; use fvg_residual");
     if (cfg->use_viscous) return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: viscous runs need a residual-sized scratch array; use fvg_residual");
+    if (cfg->flux_quadrature == 1) return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: flux_quadrature = fourth needs its face arrays; use fvg_residual");
     if (has_expressions(*cfg))
         return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: source terms and time-dependent boundary values need their programs on the device; use fvg_residual");
     for (int s = 0; s < 6; ++s)

@@ -54,7 +54,8 @@ class FvgConfig(ctypes.Structure):
                 ("nrbc_sigma", ctypes.c_double), ("nrbc_beta", ctypes.c_double), ("positivity_fallback", ctypes.c_int),
                 ("source", ctypes.c_char_p * 5), ("boundary_expr", ctypes.c_char_p * 4),
                 ("boundary_table", ctypes.POINTER(ctypes.c_double) * 4), ("boundary_table_rows", ctypes.c_int * 4),
-                ("param_names", ctypes.POINTER(ctypes.c_char_p)), ("param_values", ctypes.POINTER(ctypes.c_double)), ("nparams", ctypes.c_int)]
+                ("param_names", ctypes.POINTER(ctypes.c_char_p)), ("param_values", ctypes.POINTER(ctypes.c_double)), ("nparams", ctypes.c_int),
+                ("flux_quadrature", ctypes.c_int)]
 
 SOURCE_KEYS = ("source_rho", "source_mx", "source_my", "source_E", "source_mz")   # the state's slot order
 BOUNDARY_KEYS = ("u_in", "v_in", "rho_in", "p_out")
@@ -100,14 +101,12 @@ def _num(v):
 
 def not_on_device(params):
     """The reference features a parameter dict switches on that the device path does not compute (None: none). They
-    are refused, never ignored: AMR, fourth-order flux quadrature and a moving or flow-driven immersed body. (Combinations
+    are refused, never ignored: AMR and a moving or flow-driven immersed body. (Combinations
     the device refuses, such as the body force with the mixed-precision form, are refused by fvg_create with
     FVG_ERR_CONFIG.)"""
     p = resolve(params)
     if _flag(p.get("use_amr", False)):
         return "adaptive meshes (use_amr)"
-    if str(p.get("flux_quadrature", "midpoint")).strip().lower() != "midpoint":
-        return "fourth-order flux quadrature"
     if _flag(p["use_ibm"]):
         moving = [k for k in ("ibm_vx", "ibm_vy", "ibm_vz", "ibm_omega", "ibm_omega_x", "ibm_omega_y", "ibm_mass") if (_num(p.get(k, 0)) or 0.0) != 0.0]
         if moving:
@@ -241,6 +240,10 @@ def to_config(params, precision=0, device=0):
     c.gx, c.gy, c.gz = float(p["gx"]), float(p["gy"]), float(p["gz"])
     c.nrbc_sigma, c.nrbc_beta = float(p["nrbc_sigma"]), float(p["nrbc_beta"])
     c.positivity_fallback = 1 if _flag(p["positivity_fallback"]) else 0
+    quad = str(p.get("flux_quadrature", "midpoint")).strip().lower()
+    if quad not in ("midpoint", "fourth"):   # Params.cpp:448-449
+        raise ValueError(f"flux_quadrature must be midpoint or fourth; got '{quad}'")
+    c.flux_quadrature = 1 if quad == "fourth" else 0
     c.mu = float(p["mu"])   # (derived from reynolds above when given)
     return c
 

@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define FVG_ABI_VERSION 5
+#define FVG_ABI_VERSION 6
 
 /* status codes */
 enum {
@@ -97,6 +97,9 @@ typedef struct fvg_config {
     const char* const* param_names;
     const double* param_values;
     int nparams;
+    int flux_quadrature;         /* [numerics] flux_quadrature: 0 midpoint, 1 fourth (WENO3-Z / WENO5-Z of the conserved
+                                    averages, point values at the face centres and the transverse flux correction,
+                                    cpp/src/Schemes.cpp:1202-1350, 1954-2133; FP64, whole meshes without an immersed body) */
 } fvg_config;
 
 typedef struct fvg_run fvg_run;

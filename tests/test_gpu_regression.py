@@ -34,9 +34,3 @@ def test_device_reproduces_reference_regression_state(name):
         assert d_here < rc.DEVICE_MATH_TOL
     else:
         assert exact
-
-
-@pytest.mark.parametrize("name", sorted(rc.NOT_ON_DEVICE))
-def test_device_refuses_features_it_does_not_compute(name):
-    with pytest.raises((ValueError, RuntimeError)):
-        Run(rc.params(FX, name), U=FX[f"{name}/U0"])
