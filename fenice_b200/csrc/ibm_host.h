@@ -19,6 +19,7 @@ struct IbmTable {
     std::vector<int> img_cell;         // 8 per ghost: the image point's interpolation cells (the first four in 2-D / extruded bodies)
     std::vector<double> img_w;         // 8 per ghost: their weights (0 for a solid cell; renormalised)
     std::vector<double> ratio, gnx, gny, gnz;   // per ghost: distance ghost-wall / distance image-wall, and the wall normal
+    std::vector<double> gwx, gwy, gwz;          // per ghost: its wall point (the wall velocity of a moving body is taken there)
     std::vector<int> deep;             // the other solid cells
     int fallback = 0;                  // ghosts with no fluid around any image point (nearest fluid cell, ratio 0)
 };
@@ -92,16 +93,14 @@ inline bool make_probe3(const IbmGeom& m, const std::vector<unsigned char>& mask
     return true;
 }
 
-// The mask and the ghost table of a static body on the whole mesh; returns "" or an error message.
-inline std::string build_ibm(const fvg_config& c, IbmTable& t) {
+// The body's geometry on the mesh of a configuration, its centre at (cx, cy, cz) (a moving body: its placement plus the
+// displacement of its pose, ImmersedBoundary::place_geometry, cpp/src/Physics.cpp:1162-1194).
+inline IbmGeom ibm_geom(const fvg_config& c, double cx, double cy, double cz) {
     IbmGeom m;
-    const bool d3 = c.nz > 1;
-    if (c.ibm_shape != 0 && c.ibm_shape != 1) return "ibm_shape: Cylinder or Sphere only on the device";
-    if (c.ibm_curvature) return "ibm_curvature is not supported on the device";
-    m.ball = d3 && c.ibm_shape == 1;
-    m.cx = c.ibm_cx;
-    m.cy = c.ibm_cy;
-    m.cz = c.ibm_cz;
+    m.ball = c.nz > 1 && c.ibm_shape == 1;
+    m.cx = cx;
+    m.cy = cy;
+    m.cz = cz;
     m.r = c.ibm_radius;
     m.nx = c.nx;
     m.ny = c.ny;
@@ -109,6 +108,21 @@ inline std::string build_ibm(const fvg_config& c, IbmTable& t) {
     m.dx = c.Lx / c.nx;
     m.dy = c.Ly / c.ny;
     m.dz = c.Lz / c.nz;
+    return m;
+}
+
+inline std::string build_ibm_geom(const IbmGeom& m, IbmTable& t);
+
+// The mask and the ghost table of a static body on the whole mesh; returns "" or an error message.
+inline std::string build_ibm(const fvg_config& c, IbmTable& t) {
+    if (c.ibm_shape != 0 && c.ibm_shape != 1) return "ibm_shape: Cylinder or Sphere only on the device";
+    if (c.ibm_curvature) return "ibm_curvature is not supported on the device";
+    return build_ibm_geom(ibm_geom(c, c.ibm_cx, c.ibm_cy, c.ibm_cz), t);
+}
+
+// The mask and the ghost table of the body of geometry m (ImmersedBoundary::build_ghosts, Physics.cpp:1397-1537).
+inline std::string build_ibm_geom(const IbmGeom& m, IbmTable& t) {
+    const bool d3 = m.nz > 1;
     if (m.nx < 2 || m.ny < 2 || (m.ball && m.nz < 2)) return "the immersed body needs at least two cells per axis";
     const size_t n = static_cast<size_t>(m.nx) * m.ny * m.nz;
     t = IbmTable();
@@ -194,11 +208,102 @@ inline std::string build_ibm(const fvg_config& c, IbmTable& t) {
                 t.gnx.push_back(gx);
                 t.gny.push_back(gy);
                 t.gnz.push_back(gz);
+                t.gwx.push_back(wx);
+                t.gwy.push_back(wy);
+                t.gwz.push_back(m.ball ? wz : z);   // (a cylinder's wall point is at the cell's z)
                 is_ghost[m.cell(i, j, k)] = 1;
             }
     for (size_t cc = 0; cc < n; ++cc)
         if (t.mask[cc] && !is_ghost[cc]) t.deep.push_back(static_cast<int>(cc));
     return "";
+}
+
+// The cells a moving body has left, to be given the state of the wall layer (ImmersedBoundary::build_fresh,
+// Physics.cpp:1230-1290): per cell the image probe on the normal through its closest wall point (reading settled fluid
+// only: the fresh cells count as solid meanwhile), the ratio of the distances, and the wall velocity at the wall point.
+struct FreshTable {
+    std::vector<int> cell, img_cell;
+    std::vector<double> img_w, ratio, wvel;   // img: 8 per cell; wvel: 3 per cell
+};
+
+template <class WallVelocity>
+inline void build_fresh(const IbmGeom& m, std::vector<unsigned char>& mask, const std::vector<int>& cells, WallVelocity vel, FreshTable& f) {
+    f = FreshTable();
+    for (const int c : cells) mask[c] = 1;
+    const bool d3 = m.nz > 1;
+    const double hh = d3 ? dmax_(dmax_(m.dx, m.dy), m.dz) : dmax_(m.dx, m.dy);
+    for (const int c : cells) {
+        const int i = c % m.nx, j = (c / m.nx) % m.ny, k = c / (m.nx * m.ny);
+        const double x = m.xc(i), y = m.yc(j), z = m.zc(k);
+        double wx, wy, wz = 0.0, gx, gy, gz = 0.0, dg;
+        if (d3) {   // closest_wall_point3
+            if (m.ball) {
+                const double ex = x - m.cx, ey = y - m.cy, ez = z - m.cz, d = std::sqrt(ex * ex + ey * ey + ez * ez);
+                gx = d > 0.0 ? ex / d : 1.0;
+                gy = d > 0.0 ? ey / d : 0.0;
+                gz = d > 0.0 ? ez / d : 0.0;
+                wx = m.cx + m.r * gx;
+                wy = m.cy + m.r * gy;
+                wz = m.cz + m.r * gz;
+            } else {
+                const double ex = x - m.cx, ey = y - m.cy, d = std::sqrt(ex * ex + ey * ey);
+                gx = d > 0.0 ? ex / d : 1.0;
+                gy = d > 0.0 ? ey / d : 0.0;
+                wx = m.cx + m.r * gx;
+                wy = m.cy + m.r * gy;
+                wz = z;
+            }
+            dg = std::sqrt((x - wx) * (x - wx) + (y - wy) * (y - wy) + (z - wz) * (z - wz));
+        } else {    // closest_wall_point
+            const double ex = x - m.cx, ey = y - m.cy, d = std::sqrt(ex * ex + ey * ey);
+            gx = d > 0.0 ? ex / d : 1.0;
+            gy = d > 0.0 ? ey / d : 0.0;
+            wx = m.cx + m.r * gx;
+            wy = m.cy + m.r * gy;
+            dg = std::hypot(x - wx, y - wy);
+        }
+        double wv[3];
+        vel(wx, wy, wz, wv);
+        int cell[8];
+        double w[8];
+        bool found = false;
+        double d = 0.0;
+        for (d = dmax_(dg + hh, 1.5 * hh); d <= 4.0 * hh + dg + 1e-12; d += 0.5 * hh) {
+            found = d3 ? make_probe3(m, mask, wx + d * gx, wy + d * gy, wz + d * gz, cell, w) : make_probe(m, mask, wx + d * gx, wy + d * gy, k, cell, w);
+            if (found) break;
+        }
+        double ratio;
+        if (found) {
+            ratio = dg / d;
+        } else {   // the nearest settled fluid cell of the two-cell neighbourhood, at the wall velocity
+            double best = 1e300;
+            int cn = c;
+            for (int dk = d3 ? -2 : 0; dk <= (d3 ? 2 : 0); ++dk)
+                for (int dj = -2; dj <= 2; ++dj)
+                    for (int di = -2; di <= 2; ++di) {
+                        const int ii = i + di, jj = j + dj, kk = k + dk;
+                        if (ii < 0 || ii >= m.nx || jj < 0 || jj >= m.ny || kk < 0 || kk >= m.nz || mask[m.cell(ii, jj, kk)]) continue;
+                        const double d2 = static_cast<double>(di * di + dj * dj + dk * dk);
+                        if (d2 < best) {
+                            best = d2;
+                            cn = static_cast<int>(m.cell(ii, jj, kk));
+                        }
+                    }
+            for (int q = 0; q < 8; ++q) {
+                cell[q] = cn;
+                w[q] = q == 0 ? 1.0 : 0.0;
+            }
+            ratio = 0.0;
+        }
+        f.cell.push_back(c);
+        for (int q = 0; q < 8; ++q) {
+            f.img_cell.push_back(cell[q]);
+            f.img_w.push_back(w[q]);
+        }
+        f.ratio.push_back(ratio);
+        for (int q = 0; q < 3; ++q) f.wvel.push_back(wv[q]);
+    }
+    for (const int c : cells) mask[c] = 0;
 }
 
 }   // namespace fvg

@@ -532,6 +532,15 @@ struct fvg_run {
     bool src_on = false, src_unsteady = false, tv_on = false;
     double* d_src = nullptr;
     double* d_tv = nullptr;
+    // a moving immersed body (prescribed motion): the pose (displacement and velocities), the pose the geometry was built
+    // at, the host tables of that geometry, the wall velocities on the device (per ghost / deep cell)
+    struct Pose {
+        double x = 0.0, y = 0.0, z = 0.0, w = 0.0, angle = 0.0, u = 0.0, v = 0.0, omega = 0.0, omega_x = 0.0, omega_y = 0.0;
+    };
+    bool moving = false;
+    Pose pose, built;
+    IbmTable tab;
+    double *d_gvel = nullptr, *d_dvel = nullptr;
     // flux_quadrature = fourth: the face arrays of the face passes (fourth.cuh; one allocation, d_fourth)
     bool fourth = false;
     FourthArgs fa{};
@@ -620,6 +629,16 @@ std::string validate(const fvg_config& c) {
     }
     if (c.use_bodyforce && c.use_ibm) return "the body force with an immersed body (gravity in its ghost states) is not supported on the device";
     if (!(c.cfl > 0)) return "cfl must be > 0";
+    if (c.use_ibm) {   // a prescribed motion (Params.cpp:505-516)
+        const bool moving = c.ibm_vx != 0.0 || c.ibm_vy != 0.0 || c.ibm_vz != 0.0 || c.ibm_omega != 0.0 || c.ibm_omega_x != 0.0 || c.ibm_omega_y != 0.0;
+        if ((c.ibm_omega_from > 0.0 || c.ibm_omega_until > 0.0) && c.ibm_omega == 0.0 && c.ibm_omega_x == 0.0 && c.ibm_omega_y == 0.0)
+            return "ibm_omega_from / ibm_omega_until need a rotation (ibm_omega)";
+        if (c.ibm_omega_until > 0.0 && c.ibm_omega_until <= c.ibm_omega_from) return "ibm_omega_until must be later than ibm_omega_from";
+        if (moving && c.ibm_curvature) return "ibm_curvature is not available for a moving body";
+        if (moving && c.nz > 1 && c.ibm_shape != 1) return "a moving body in 3-D is a sphere (for now)";
+        if (c.nz == 1 && (c.ibm_omega_x != 0.0 || c.ibm_omega_y != 0.0)) return "ibm_omega_x and ibm_omega_y need a 3-D mesh (nz > 1)";
+        if (moving && c.nz == 1 && c.ibm_vz != 0.0) return "ibm_vz needs a 3-D mesh (nz > 1)";
+    }
     // load_boundary_functions (Simulation.cpp:152-153); time-dependent ones are checked at t = 0 when compiled
     const bool rho_fn = (c.boundary_expr[2] && *c.boundary_expr[2]) || (c.boundary_table[2] && c.boundary_table_rows[2] > 0);
     const bool p_fn = (c.boundary_expr[3] && *c.boundary_expr[3]) || (c.boundary_table[3] && c.boundary_table_rows[3] > 0);
@@ -785,6 +804,8 @@ cudaError_t ibm_fill(fvg_run* r, const double* Usrc, double* Uout, int reset, co
     a.deep = r->d_deep;
     a.rho_ref = r->cfg.rho_in;
     a.p_ref = r->cfg.p_out;
+    a.gvel = r->moving ? r->d_gvel : nullptr;
+    a.dvel = r->moving ? r->d_dvel : nullptr;
     a.U = Usrc;
     a.forced = r->d_forced;
     a.Uout = Uout;
@@ -1358,6 +1379,177 @@ int upload_expressions(fvg_run* run, const expr::Program& p) {
     return FVG_OK;
 }
 
+// ImmersedBoundary::body_velocity (cpp/src/Physics.cpp:1128-1139): the velocity of the rigid body at (x, y, z), with the
+// velocities of the pose and the pivot where the geometry was built.
+void body_velocity(const fvg_run* r, double x, double y, double z, double v[3]) {
+    const fvg_run::Pose& p = r->pose;
+    const double px = r->cfg.ibm_cx + r->built.x, py = r->cfg.ibm_cy + r->built.y;
+    v[0] = p.u - p.omega * (y - py);
+    v[1] = p.v + p.omega * (x - px);
+    v[2] = p.w;
+    if (p.omega_x != 0.0 || p.omega_y != 0.0) {
+        const double pz = r->cfg.ibm_cz + r->built.z, rx = x - px, ry = y - py, rz = z - pz;
+        v[0] += p.omega_y * rz;
+        v[1] -= p.omega_x * rz;
+        v[2] += p.omega_x * ry - p.omega_y * rx;
+    }
+}
+
+// The wall velocity of every ghost (at its wall point) and the velocity of every deep cell (at its centre) of a moving
+// body, from the current pose (refresh_wall_velocity; the deep cells' of fill_ghosts_part).
+int upload_velocities(fvg_run* r) {
+    const IbmTable& t = r->tab;
+    const int ng = (int)t.ghost.size(), nd = (int)t.deep.size();
+    std::vector<double> gv(3 * (size_t)ng + 3), dv(3 * (size_t)nd + 3);
+    for (int k = 0; k < ng; ++k) body_velocity(r, t.gwx[k], t.gwy[k], r->dim == 3 ? t.gwz[k] : 0.0, &gv[3 * k]);
+    const double dx = r->m.dx, dy = r->m.dy, dz = r->m.dz;
+    for (int k = 0; k < nd; ++k) {
+        const int c = t.deep[k], i = c % r->m.nx, j = (c / r->m.nx) % r->m.ny, kk = c / (r->m.nx * r->m.ny);
+        body_velocity(r, (i + 0.5) * dx + 0.0, (j + 0.5) * dy + 0.0, r->dim == 3 ? (kk + 0.5) * dz + 0.0 : 0.0, &dv[3 * k]);
+    }
+    if (cudaMemcpy(r->d_gvel, gv.data(), sizeof(double) * gv.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(r->d_dvel, dv.data(), sizeof(double) * dv.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(r, FVG_ERR_CUDA, "copy of the wall velocities failed");
+    return FVG_OK;
+}
+
+// The immersed body's tables (run->tab) on the device: the mask, the forced-state slots, the ghost and deep cells with
+// their image points, the solid cells of the loads and, for a moving body, the velocities. The arrays of an earlier
+// geometry are replaced.
+int upload_ibm(fvg_run* run) {
+    for (void** p : {(void**)&run->d_slot, (void**)&run->d_forced, (void**)&run->d_ghost, (void**)&run->d_img_cell, (void**)&run->d_img_w,
+                     (void**)&run->d_ratio, (void**)&run->d_gn, (void**)&run->d_deep, (void**)&run->d_solid, (void**)&run->d_gvel,
+                     (void**)&run->d_dvel})
+        if (*p) {
+            cudaFree(*p);
+            *p = nullptr;
+        }
+    const IbmTable& t = run->tab;
+    run->ng = (int)t.ghost.size();
+    run->nd = (int)t.deep.size();
+    std::vector<int> slot(run->m.ncells, -1);
+    for (int k = 0; k < run->ng; ++k) slot[t.ghost[k]] = k;
+    for (int k = 0; k < run->nd; ++k) slot[t.deep[k]] = run->ng + k;
+    std::vector<double> gn(3 * (size_t)run->ng);
+    for (int k = 0; k < run->ng; ++k) {
+        gn[3 * k] = t.gnx[k];
+        gn[3 * k + 1] = t.gny[k];
+        gn[3 * k + 2] = t.gnz[k];
+    }
+    const size_t ns = (size_t)(run->ng + run->nd) + 1, ng1 = (size_t)run->ng + 1, nd1 = (size_t)run->nd + 1;
+    bool ok = (run->d_mask || cudaMalloc(&run->d_mask, run->m.ncells) == cudaSuccess) &&
+              cudaMalloc(&run->d_slot, sizeof(int) * run->m.ncells) == cudaSuccess && cudaMalloc(&run->d_forced, sizeof(double) * 5 * ns) == cudaSuccess &&
+              cudaMalloc(&run->d_ghost, sizeof(int) * ng1) == cudaSuccess && cudaMalloc(&run->d_img_cell, sizeof(int) * 8 * ng1) == cudaSuccess &&
+              cudaMalloc(&run->d_img_w, sizeof(double) * 8 * ng1) == cudaSuccess && cudaMalloc(&run->d_ratio, sizeof(double) * ng1) == cudaSuccess &&
+              cudaMalloc(&run->d_gn, sizeof(double) * 3 * ng1) == cudaSuccess && cudaMalloc(&run->d_deep, sizeof(int) * nd1) == cudaSuccess &&
+              (!run->moving || (cudaMalloc(&run->d_gvel, sizeof(double) * 3 * ng1) == cudaSuccess &&
+                                cudaMalloc(&run->d_dvel, sizeof(double) * 3 * nd1) == cudaSuccess));
+    ok = ok && cudaMemcpy(run->d_mask, t.mask.data(), run->m.ncells, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(run->d_slot, slot.data(), sizeof(int) * run->m.ncells, cudaMemcpyHostToDevice) == cudaSuccess;
+    if (ok && run->ng > 0)
+        ok = cudaMemcpy(run->d_ghost, t.ghost.data(), sizeof(int) * run->ng, cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(run->d_img_cell, t.img_cell.data(), sizeof(int) * 8 * run->ng, cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(run->d_img_w, t.img_w.data(), sizeof(double) * 8 * run->ng, cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(run->d_ratio, t.ratio.data(), sizeof(double) * run->ng, cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(run->d_gn, gn.data(), sizeof(double) * 3 * run->ng, cudaMemcpyHostToDevice) == cudaSuccess;
+    if (ok && run->nd > 0) ok = cudaMemcpy(run->d_deep, t.deep.data(), sizeof(int) * run->nd, cudaMemcpyHostToDevice) == cudaSuccess;
+    if (!ok) return fail(run, FVG_ERR_CUDA, "device allocation of the immersed body's tables failed");
+    std::vector<int> solid_cells;
+    for (long long c = 0; c < run->m.ncells; ++c)
+        if (t.mask[c]) solid_cells.push_back((int)c);
+    run->nsolid = (int)solid_cells.size();
+    if (cudaMalloc(&run->d_solid, sizeof(int) * (solid_cells.size() + 1)) != cudaSuccess ||
+        (!run->d_loads && cudaMalloc(&run->d_loads, sizeof(double) * 3) != cudaSuccess) ||
+        (run->nsolid > 0 && cudaMemcpy(run->d_solid, solid_cells.data(), sizeof(int) * run->nsolid, cudaMemcpyHostToDevice) != cudaSuccess))
+        return fail(run, FVG_ERR_CUDA, "device allocation of the immersed body's tables failed");
+    run->bc.solid = run->d_mask;
+    run->bc.slot = run->d_slot;
+    run->bc.forced = run->d_forced;
+    return run->moving ? upload_velocities(run) : FVG_OK;
+}
+
+// Simulation::prescribed_pose (cpp/src/SimulationRun.cpp:193-214) at time t.
+fvg_run::Pose prescribed_pose(const fvg_config& c, double t) {
+    fvg_run::Pose p;
+    p.x = c.ibm_vx * t;
+    p.y = c.ibm_vy * t;
+    p.z = c.ibm_vz * t;
+    p.w = c.ibm_vz;
+    p.angle = c.ibm_omega * t;
+    p.u = c.ibm_vx;
+    p.v = c.ibm_vy;
+    p.omega = c.ibm_omega;
+    p.omega_x = c.ibm_omega_x;
+    p.omega_y = c.ibm_omega_y;
+    if (c.ibm_omega_from > 0.0 || c.ibm_omega_until > 0.0) {   // the rotation runs between two times, the angle held outside
+        const double t_off = c.ibm_omega_until > 0.0 ? c.ibm_omega_until : t;
+        p.angle = c.ibm_omega * (vmin(vmax(t, c.ibm_omega_from), vmax(t_off, c.ibm_omega_from)) - c.ibm_omega_from);
+        const bool on = t >= c.ibm_omega_from && (c.ibm_omega_until <= 0.0 || t < c.ibm_omega_until);
+        p.omega = on ? c.ibm_omega : 0.0;
+        p.omega_x = on ? c.ibm_omega_x : 0.0;
+        p.omega_y = on ? c.ibm_omega_y : 0.0;
+    }
+    return p;
+}
+
+// The body at the start of a step at time t (place_body and ImmersedBoundary::move_to, SimulationRun.cpp:379-384 and
+// Physics.cpp:1310-1334): the geometry follows the pose in steps of a quarter cell (then the ghost table is built again
+// and the cells the body left take the wall layer's state, fill_fresh); in between only the wall velocities change.
+int place_body(fvg_run* r, double t) {
+    const fvg_run::Pose pose = prescribed_pose(r->cfg, t);
+    const double h = r->dim == 3 ? vmin(vmin(r->m.dx, r->m.dy), r->m.dz) : vmin(r->m.dx, r->m.dy);
+    const double shift = vmax(vmax(fabs(pose.x - r->built.x), fabs(pose.y - r->built.y)), fabs(pose.z - r->built.z));
+    r->pose = pose;
+    if (shift <= 0.25 * h) return upload_velocities(r);
+    const std::vector<unsigned char> old_mask = r->tab.mask;
+    r->built = pose;
+    const IbmGeom g = ibm_geom(r->cfg, r->cfg.ibm_cx + pose.x, r->cfg.ibm_cy + pose.y, r->cfg.ibm_cz + pose.z);
+    IbmTable tb;
+    const std::string msg = build_ibm_geom(g, tb);
+    if (!msg.empty()) return fail(r, FVG_ERR_CONFIG, msg);
+    std::vector<int> cells;   // fresh: solid before, fluid now
+    for (size_t c = 0; c < tb.mask.size(); ++c)
+        if (old_mask[c] && !tb.mask[c]) cells.push_back((int)c);
+    FreshTable f;
+    build_fresh(g, tb.mask, cells, [&](double x, double y, double z, double* v) { body_velocity(r, x, y, z, v); }, f);
+    r->tab = std::move(tb);
+    if (cudaStreamSynchronize(r->stream) != cudaSuccess) return fail(r, FVG_ERR_CUDA, "synchronisation failed");
+    if (const int rc = upload_ibm(r)) return rc;
+    const int n = (int)f.cell.size();
+    if (n == 0) return FVG_OK;
+    int *dc = nullptr, *di = nullptr;
+    double *dw = nullptr, *dr = nullptr, *dv = nullptr;
+    bool ok = cudaMalloc(&dc, sizeof(int) * n) == cudaSuccess && cudaMalloc(&di, sizeof(int) * 8 * n) == cudaSuccess &&
+              cudaMalloc(&dw, sizeof(double) * 8 * n) == cudaSuccess && cudaMalloc(&dr, sizeof(double) * n) == cudaSuccess &&
+              cudaMalloc(&dv, sizeof(double) * 3 * n) == cudaSuccess;
+    ok = ok && cudaMemcpy(dc, f.cell.data(), sizeof(int) * n, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(di, f.img_cell.data(), sizeof(int) * 8 * n, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(dw, f.img_w.data(), sizeof(double) * 8 * n, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(dr, f.ratio.data(), sizeof(double) * n, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(dv, f.wvel.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice) == cudaSuccess;
+    if (ok) {
+        FreshArgs a{};
+        a.m = r->m;
+        a.eos = r->eos;
+        a.n = n;
+        a.cell = dc;
+        a.img_cell = di;
+        a.img_w = dw;
+        a.ratio = dr;
+        a.wvel = dv;
+        a.U = r->Ucur();
+        const int blocks = (n + 255) / 256;
+        if (r->nvar == 5)
+            fresh_fill_kernel<5><<<blocks, 256, 0, r->stream>>>(a);
+        else
+            fresh_fill_kernel<4><<<blocks, 256, 0, r->stream>>>(a);
+        ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(r->stream) == cudaSuccess;
+    }
+    for (void* p : {(void*)dc, (void*)di, (void*)dw, (void*)dr, (void*)dv})
+        if (p) cudaFree(p);
+    return ok ? FVG_OK : fail(r, FVG_ERR_CUDA, "the fill of the cells the body left failed");
+}
+
 // fvg_create, and part `part` of `nparts` slabs of the mesh along its slowest axis (nparts = 1 with part mode off: a
 // whole run). A part holds planes first .. first + count - 1 of the split axis (the first nsplit % nparts parts one
 // plane more), with `depth` ghost planes on each side; the mesh spacing, the step length and every other parameter are
@@ -1604,55 +1796,14 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
             return bail(FVG_ERR_CUDA);
         }
     if (c.use_ibm) {
-        IbmTable t;
-        const std::string msg = build_ibm(c, t);
+        const std::string msg = build_ibm(c, run->tab);
         if (!msg.empty()) {
             run->err = msg;
             return bail(FVG_ERR_CONFIG);
         }
         run->ibm = true;
-        run->ng = (int)t.ghost.size();
-        run->nd = (int)t.deep.size();
-        std::vector<int> slot(run->m.ncells, -1);
-        for (int k = 0; k < run->ng; ++k) slot[t.ghost[k]] = k;
-        for (int k = 0; k < run->nd; ++k) slot[t.deep[k]] = run->ng + k;
-        std::vector<double> gn(3 * (size_t)run->ng);
-        for (int k = 0; k < run->ng; ++k) {
-            gn[3 * k] = t.gnx[k];
-            gn[3 * k + 1] = t.gny[k];
-            gn[3 * k + 2] = t.gnz[k];
-        }
-        const size_t ns = (size_t)(run->ng + run->nd) + 1, ng1 = (size_t)run->ng + 1, nd1 = (size_t)run->nd + 1;
-        bool ok = cudaMalloc(&run->d_mask, run->m.ncells) == cudaSuccess && cudaMalloc(&run->d_slot, sizeof(int) * run->m.ncells) == cudaSuccess &&
-                  cudaMalloc(&run->d_forced, sizeof(double) * 5 * ns) == cudaSuccess && cudaMalloc(&run->d_ghost, sizeof(int) * ng1) == cudaSuccess &&
-                  cudaMalloc(&run->d_img_cell, sizeof(int) * 8 * ng1) == cudaSuccess && cudaMalloc(&run->d_img_w, sizeof(double) * 8 * ng1) == cudaSuccess &&
-                  cudaMalloc(&run->d_ratio, sizeof(double) * ng1) == cudaSuccess && cudaMalloc(&run->d_gn, sizeof(double) * 3 * ng1) == cudaSuccess &&
-                  cudaMalloc(&run->d_deep, sizeof(int) * nd1) == cudaSuccess;
-        ok = ok && cudaMemcpy(run->d_mask, t.mask.data(), run->m.ncells, cudaMemcpyHostToDevice) == cudaSuccess &&
-             cudaMemcpy(run->d_slot, slot.data(), sizeof(int) * run->m.ncells, cudaMemcpyHostToDevice) == cudaSuccess;
-        if (ok && run->ng > 0)
-            ok = cudaMemcpy(run->d_ghost, t.ghost.data(), sizeof(int) * run->ng, cudaMemcpyHostToDevice) == cudaSuccess &&
-                 cudaMemcpy(run->d_img_cell, t.img_cell.data(), sizeof(int) * 8 * run->ng, cudaMemcpyHostToDevice) == cudaSuccess &&
-                 cudaMemcpy(run->d_img_w, t.img_w.data(), sizeof(double) * 8 * run->ng, cudaMemcpyHostToDevice) == cudaSuccess &&
-                 cudaMemcpy(run->d_ratio, t.ratio.data(), sizeof(double) * run->ng, cudaMemcpyHostToDevice) == cudaSuccess &&
-                 cudaMemcpy(run->d_gn, gn.data(), sizeof(double) * 3 * run->ng, cudaMemcpyHostToDevice) == cudaSuccess;
-        if (ok && run->nd > 0) ok = cudaMemcpy(run->d_deep, t.deep.data(), sizeof(int) * run->nd, cudaMemcpyHostToDevice) == cudaSuccess;
-        if (!ok) {
-            run->err = "device allocation of the immersed body's tables failed";
-            return bail(FVG_ERR_CUDA);
-        }
-        std::vector<int> solid_cells;
-        for (long long c = 0; c < run->m.ncells; ++c)
-            if (t.mask[c]) solid_cells.push_back((int)c);
-        run->nsolid = (int)solid_cells.size();
-        if (cudaMalloc(&run->d_solid, sizeof(int) * (solid_cells.size() + 1)) != cudaSuccess || cudaMalloc(&run->d_loads, sizeof(double) * 3) != cudaSuccess ||
-            (run->nsolid > 0 && cudaMemcpy(run->d_solid, solid_cells.data(), sizeof(int) * run->nsolid, cudaMemcpyHostToDevice) != cudaSuccess)) {
-            run->err = "device allocation of the immersed body's tables failed";
-            return bail(FVG_ERR_CUDA);
-        }
-        run->bc.solid = run->d_mask;
-        run->bc.slot = run->d_slot;
-        run->bc.forced = run->d_forced;
+        run->moving = c.ibm_vx != 0.0 || c.ibm_vy != 0.0 || c.ibm_vz != 0.0 || c.ibm_omega != 0.0 || c.ibm_omega_x != 0.0 || c.ibm_omega_y != 0.0;
+        if (const int rc = upload_ibm(run)) return bail(rc);
     }
     Ctl h{};
     h.cfl = c.cfl;
@@ -1697,7 +1848,8 @@ int fvg_destroy(fvg_run* run) {
         if (f) cudaFree(f);
     if (run->sens_tiles) cudaFree(run->sens_tiles);
     for (void* p : {(void*)run->d_mask, (void*)run->d_slot, (void*)run->d_forced, (void*)run->d_ghost, (void*)run->d_img_cell, (void*)run->d_img_w,
-                    (void*)run->d_ratio, (void*)run->d_gn, (void*)run->d_deep, (void*)run->d_solid, (void*)run->d_loads})
+                    (void*)run->d_ratio, (void*)run->d_gn, (void*)run->d_deep, (void*)run->d_solid, (void*)run->d_loads, (void*)run->d_gvel,
+                    (void*)run->d_dvel})
         if (p) cudaFree(p);
     if (run->stream) cudaStreamDestroy(run->stream);
     delete run;
@@ -1799,7 +1951,33 @@ static int run_steps(fvg_run* run, double t_end, int max_steps, int use_graph, i
     int rc;
     const bool hancock = run->cfg.time_scheme == FVG_TS_HANCOCK;
     int done = 0;
-    if (!use_graph) {
+    if (run->moving) {
+        // a moving body: step by step, the body placed at the start of each step from the device's clock, the distance
+        // it travelled checked after it (at most one cell per step, SimulationRun.cpp:449-458)
+        while (true) {
+            if ((rc = read_ctl(run, &h))) return rc;
+            if (!h.active) break;
+            if ((rc = place_body(run, h.t))) return rc;
+            cudaError_t e = enqueue_step(run);
+            if (e != cudaSuccess) return fail(run, FVG_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+            Ctl h2;
+            if ((rc = read_ctl(run, &h2))) return rc;
+            if (h2.steps == h.steps) {   // the step did not run: the state stayed where it was
+                if (hancock) run->cur ^= 1;
+                h = h2;
+                break;
+            }
+            const fvg_config& c = run->cfg;
+            double travel = h2.dt * vmax(fabs(c.ibm_vx) / run->m.dx, fabs(c.ibm_vy) / run->m.dy);
+            if (run->dim == 3) travel = vmax(travel, h2.dt * fabs(c.ibm_vz) / run->m.dz);
+            if (travel > 1.0) {
+                if (steps) *steps = h2.steps;
+                return fail(run, FVG_ERR_DIVERGED, "the moving body travelled more than one cell in a step (lower the CFL number)");
+            }
+            h = h2;
+        }
+        done = h.steps;
+    } else if (!use_graph) {
         // one step at a time (fvg_step)
         cudaError_t e = enqueue_step(run);
         if (e != cudaSuccess) return fail(run, FVG_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
@@ -2110,8 +2288,10 @@ int fvg_ibm_loads(fvg_run* run, double* loads) {
     CK(residual_stage(run, run->Ucur(), nullptr, out, kStoreR, 0, 0, 0, always));
     const fvg_config& c = run->cfg;
     const double vol = run->dim == 3 ? run->m.dx * run->m.dy * run->m.dz : run->m.dx * run->m.dy;
-    k_ibm_loads<<<1, 32, 0, run->stream>>>(out, run->m.plane, run->d_solid, run->nsolid, vol, run->m.nx, run->m.ny, run->m.dx, run->m.dy, c.ibm_cx,
-                                           c.ibm_cy, run->d_loads);
+    // (the moment centre follows a moving body, SimulationRun.cpp:140-141)
+    k_ibm_loads<<<1, 32, 0, run->stream>>>(out, run->m.plane, run->d_solid, run->nsolid, vol, run->m.nx, run->m.ny, run->m.dx, run->m.dy,
+                                           run->moving ? c.ibm_cx + run->pose.x : c.ibm_cx, run->moving ? c.ibm_cy + run->pose.y : c.ibm_cy,
+                                           run->d_loads);
     CK(cudaGetLastError());
     double h[3];
     CK(cudaMemcpyAsync(h, run->d_loads, sizeof(h), cudaMemcpyDeviceToHost, run->stream));

@@ -55,7 +55,10 @@ class FvgConfig(ctypes.Structure):
                 ("source", ctypes.c_char_p * 5), ("boundary_expr", ctypes.c_char_p * 4),
                 ("boundary_table", ctypes.POINTER(ctypes.c_double) * 4), ("boundary_table_rows", ctypes.c_int * 4),
                 ("param_names", ctypes.POINTER(ctypes.c_char_p)), ("param_values", ctypes.POINTER(ctypes.c_double)), ("nparams", ctypes.c_int),
-                ("flux_quadrature", ctypes.c_int)]
+                ("flux_quadrature", ctypes.c_int),
+                ("ibm_vx", ctypes.c_double), ("ibm_vy", ctypes.c_double), ("ibm_vz", ctypes.c_double),
+                ("ibm_omega", ctypes.c_double), ("ibm_omega_x", ctypes.c_double), ("ibm_omega_y", ctypes.c_double),
+                ("ibm_omega_from", ctypes.c_double), ("ibm_omega_until", ctypes.c_double)]
 
 SOURCE_KEYS = ("source_rho", "source_mx", "source_my", "source_E", "source_mz")   # the state's slot order
 BOUNDARY_KEYS = ("u_in", "v_in", "rho_in", "p_out")
@@ -101,16 +104,16 @@ def _num(v):
 
 def not_on_device(params):
     """The reference features a parameter dict switches on that the device path does not compute (None: none). They
-    are refused, never ignored: AMR and a moving or flow-driven immersed body. (Combinations
+    are refused, never ignored: AMR and an immersed body driven by the flow (a prescribed motion is computed). (Combinations
     the device refuses, such as the body force with the mixed-precision form, are refused by fvg_create with
     FVG_ERR_CONFIG.)"""
     p = resolve(params)
     if _flag(p.get("use_amr", False)):
         return "adaptive meshes (use_amr)"
     if _flag(p["use_ibm"]):
-        moving = [k for k in ("ibm_vx", "ibm_vy", "ibm_vz", "ibm_omega", "ibm_omega_x", "ibm_omega_y", "ibm_mass") if (_num(p.get(k, 0)) or 0.0) != 0.0]
-        if moving:
-            return "a moving immersed body (" + ", ".join(moving) + ")"
+        driven = [k for k in ("ibm_mass", "ibm_inertia") if (_num(p.get(k, 0)) or 0.0) != 0.0]
+        if driven:
+            return "an immersed body driven by the flow (" + ", ".join(driven) + ")"
     return None
 
 
@@ -245,6 +248,8 @@ def to_config(params, precision=0, device=0):
         raise ValueError(f"flux_quadrature must be midpoint or fourth; got '{quad}'")
     c.flux_quadrature = 1 if quad == "fourth" else 0
     c.mu = float(p["mu"])   # (derived from reynolds above when given)
+    for k in ("ibm_vx", "ibm_vy", "ibm_vz", "ibm_omega", "ibm_omega_x", "ibm_omega_y", "ibm_omega_from", "ibm_omega_until"):
+        setattr(c, k, float(p.get(k, 0.0)) if c.use_ibm else 0.0)
     return c
 
 

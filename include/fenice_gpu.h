@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define FVG_ABI_VERSION 6
+#define FVG_ABI_VERSION 7
 
 /* status codes */
 enum {
@@ -100,6 +100,13 @@ typedef struct fvg_config {
     int flux_quadrature;         /* [numerics] flux_quadrature: 0 midpoint, 1 fourth (WENO3-Z / WENO5-Z of the conserved
                                     averages, point values at the face centres and the transverse flux correction,
                                     cpp/src/Schemes.cpp:1202-1350, 1954-2133; FP64, whole meshes without an immersed body) */
+    /* [ibm] a prescribed motion of the body (Simulation::prescribed_pose, cpp/src/SimulationRun.cpp:193-214; a circle in
+     * 2-D, a sphere in 3-D): constant velocity (ibm_vz: 3-D), angular velocity about z (2-D) or x and y (a sphere), and
+     * the window of the rotation (0: always). The geometry follows the pose in steps of a quarter cell, the cells the
+     * body leaves take the wall layer's state, the ghost states see the wall velocity (Physics.cpp:1128-1336, 1581-1637). */
+    double ibm_vx, ibm_vy, ibm_vz;
+    double ibm_omega, ibm_omega_x, ibm_omega_y;
+    double ibm_omega_from, ibm_omega_until;
 } fvg_config;
 
 typedef struct fvg_run fvg_run;
