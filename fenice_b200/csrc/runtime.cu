@@ -380,6 +380,40 @@ __global__ void k_ibm_loads(const double* R, long long plane, const int* cells, 
 }
 
 // ------------------------------------------------------------------------------------------------ kernel dispatch
+// Simulation::ibm_load_terms + sum_load_terms (cpp/src/SimulationRun.cpp:312-350) of the first stage's residual R: per
+// solid cell (in cell order, one thread: the reference's sums) the momentum residual times the cell volume, its moment
+// about the pivot, and in 3-D the z component and the moments about x and y; out = {fx, fy, mz, fz, mx, my}.
+__global__ void k_body_loads(const int* gate, const double* R, long long plane, const int* cells, int n, double vol, int nx, int ny, double dx,
+                             double dy, double dz, int three_d, double px, double py, double pz, double* out) {
+    if (!*gate || threadIdx.x != 0) return;
+    double fx = 0.0, fy = 0.0, mz = 0.0, fz = 0.0, mx = 0.0, my = 0.0;
+    for (int q = 0; q < n; ++q) {
+        const long long c = cells[q];
+        const double ex = R[plane + c] * vol, ey = R[2 * plane + c] * vol;
+        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+        const double xc = (i + 0.5) * dx + 0.0, yc = (j + 0.5) * dy + 0.0;
+        double ez = 0.0, tx = 0.0, ty = 0.0;
+        if (three_d) {
+            ez = R[4 * plane + c] * vol;
+            const double x = xc - px, y = yc - py, z = (k + 0.5) * dz + 0.0 - pz;
+            tx = y * ez - z * ey;
+            ty = z * ex - x * ez;
+        }
+        fx += ex;
+        fy += ey;
+        mz += (xc - px) * ey - (yc - py) * ex;
+        fz += ez;
+        mx += tx;
+        my += ty;
+    }
+    out[0] = fx;
+    out[1] = fy;
+    out[2] = mz;
+    out[3] = fz;
+    out[4] = mx;
+    out[5] = my;
+}
+
 template <int DIM> struct Tile;
 template <> struct Tile<3> { static constexpr int X = 8, Y = 8, Z = 8, NT = 192; };
 template <> struct Tile<2> { static constexpr int X = 16, Y = 15, Z = 1, NT = 256; };
@@ -537,8 +571,16 @@ struct fvg_run {
     struct Pose {
         double x = 0.0, y = 0.0, z = 0.0, w = 0.0, angle = 0.0, u = 0.0, v = 0.0, omega = 0.0, omega_x = 0.0, omega_y = 0.0;
     };
-    bool moving = false;
+    bool moving = false, dynamic = false;
     Pose pose, built;
+    // a body driven by the flow (Simulation::BodyDynamics): its state, the centre of mass from the pivot, the loads of the
+    // first stage of the step on the device (6: fx, fy, mz, fz, mx, my)
+    struct Body {
+        double x = 0, y = 0, u = 0, v = 0, z = 0, w = 0, az = 0, ax = 0, ay = 0, dt = 0, fx = 0, fy = 0, fz = 0;
+        double th = 0, om = 0, aom = 0, mx = 0, my = 0, mz = 0, omx = 0, omy = 0, aomx = 0, aomy = 0;
+    } body;
+    double cm0[2] = {0.0, 0.0};
+    double* d_bload = nullptr;
     IbmTable tab;
     double *d_gvel = nullptr, *d_dvel = nullptr;
     // flux_quadrature = fourth: the face arrays of the face passes (fourth.cuh; one allocation, d_fourth)
@@ -638,6 +680,35 @@ std::string validate(const fvg_config& c) {
         if (moving && c.nz > 1 && c.ibm_shape != 1) return "a moving body in 3-D is a sphere (for now)";
         if (c.nz == 1 && (c.ibm_omega_x != 0.0 || c.ibm_omega_y != 0.0)) return "ibm_omega_x and ibm_omega_y need a 3-D mesh (nz > 1)";
         if (moving && c.nz == 1 && c.ibm_vz != 0.0) return "ibm_vz needs a 3-D mesh (nz > 1)";
+        // a body driven by the flow (Params.cpp:517-546)
+        const bool trans = c.ibm_mass > 0.0, rot = c.ibm_inertia > 0.0;
+        if (!(c.ibm_mass >= 0.0) || !(c.ibm_stiff_x >= 0.0) || !(c.ibm_stiff_y >= 0.0) || !(c.ibm_stiff_z >= 0.0) || !(c.ibm_damp_x >= 0.0) ||
+            !(c.ibm_damp_y >= 0.0) || !(c.ibm_damp_z >= 0.0))
+            return "ibm_mass, ibm_stiff_x/y/z and ibm_damp_x/y/z must be >= 0";
+        if (!(c.ibm_inertia >= 0.0) || !(c.ibm_stiff_theta >= 0.0) || !(c.ibm_damp_theta >= 0.0))
+            return "ibm_inertia, ibm_stiff_theta and ibm_damp_theta must be >= 0";
+        if (!trans && (c.ibm_stiff_x != 0.0 || c.ibm_stiff_y != 0.0 || c.ibm_stiff_z != 0.0 || c.ibm_damp_x != 0.0 || c.ibm_damp_y != 0.0 || c.ibm_damp_z != 0.0))
+            return "ibm_stiff_* and ibm_damp_* act on a body driven by the flow: set ibm_mass > 0";
+        if (!rot && (c.ibm_stiff_theta != 0.0 || c.ibm_damp_theta != 0.0))
+            return "ibm_stiff_theta and ibm_damp_theta act on a body whose rotation is driven by the flow: set ibm_inertia > 0";
+        if (c.ibm_cm_given) {
+            if (c.nz > 1) return "ibm_cm_x / ibm_cm_y are 2-D (a sphere turns about its centre)";
+            if (!trans || !rot) return "ibm_cm_x / ibm_cm_y act on a body whose translation and rotation are both driven: set ibm_mass > 0 and ibm_inertia > 0";
+            if (!(c.ibm_inertia > c.ibm_mass * (c.ibm_cm_x * c.ibm_cm_x + c.ibm_cm_y * c.ibm_cm_y)))
+                return "ibm_inertia is the moment of inertia about the pivot: it must exceed ibm_mass times the squared distance of the centre of mass from it";
+        }
+        if (trans || rot) {
+            if (!rot && (c.ibm_omega != 0.0 || c.ibm_omega_x != 0.0 || c.ibm_omega_y != 0.0))
+                return "a body driven by the flow translates only unless its rotation is driven too (ibm_omega must be 0, or set ibm_inertia > 0)";
+            if (rot) {
+                if (c.nz > 1 && c.ibm_stiff_theta != 0.0) return "ibm_stiff_theta: a sphere has no angle to pull back (use ibm_damp_theta)";
+                if (c.ibm_omega_from > 0.0 || c.ibm_omega_until > 0.0) return "ibm_omega_from / ibm_omega_until act on a prescribed rotation, not on a driven one";
+                if (!trans && (c.ibm_vx != 0.0 || c.ibm_vy != 0.0 || c.ibm_vz != 0.0))
+                    return "a driven rotation with a prescribed translation is not available: the body is pinned at its placement";
+            }
+            if (c.time_scheme == FVG_TS_HANCOCK) return "a body driven by the flow needs a Runge-Kutta or Euler time scheme (its loads come from the first stage)";
+            if (c.positivity_fallback) return "a body driven by the flow with positivity_fallback is not supported on the device";
+        }
     }
     // load_boundary_functions (Simulation.cpp:152-153); time-dependent ones are checked at t = 0 when compiled
     const bool rho_fn = (c.boundary_expr[2] && *c.boundary_expr[2]) || (c.boundary_table[2] && c.boundary_table_rows[2] > 0);
@@ -1046,6 +1117,12 @@ cudaError_t enqueue_step(fvg_run* r, bool refresh = true) {
     if (refresh && (e = refresh_gate(r, r->U, c))) return e;
     if ((e = residual_stage(r, r->U, nullptr, r->R, kStoreR, 0, 0, 0, act))) return e;
     k_stage1_dt<<<1, 1024, 0, r->stream>>>(c, r->bm[0], r->nb, r->bmv[0], nbv);
+    if (r->dynamic) {   // a body driven by the flow: the loads of this first stage, about the pivot of the step
+        const double vol = r->dim == 3 ? r->m.dx * r->m.dy * r->m.dz : r->m.dx * r->m.dy;
+        k_body_loads<<<1, 32, 0, r->stream>>>(act, r->R, r->m.plane, r->d_solid, r->nsolid, vol, r->m.nx, r->m.ny, r->m.dx, r->m.dy, r->m.dz,
+                                              r->dim == 3, r->cfg.ibm_cx + r->body.x, r->cfg.ibm_cy + r->body.y, r->cfg.ibm_cz + r->body.z,
+                                              r->d_bload);
+    }
     if (ts == FVG_TS_EULER) {
         k_axpy<<<axpy_blocks(r), 256, 0, r->stream>>>(c, r->U, r->U, r->R, r->m.plane, r->m.ncells, r->nvar);
         if (r->ibm && (e = ibm_fill(r, r->U, r->U, 1, act))) return e;
@@ -1492,11 +1569,108 @@ fvg_run::Pose prescribed_pose(const fvg_config& c, double t) {
     return p;
 }
 
+// Simulation::body_pose (SimulationRun.cpp:216-230): the prescribed pose, or the state of a body driven by the flow.
+fvg_run::Pose body_pose(const fvg_run* r, double t) {
+    if (!r->dynamic) return prescribed_pose(r->cfg, t);
+    fvg_run::Pose p;
+    const fvg_run::Body& b = r->body;
+    p.x = b.x;
+    p.y = b.y;
+    p.u = b.u;
+    p.v = b.v;
+    p.z = b.z;
+    p.w = b.w;
+    p.angle = b.th;
+    p.omega = b.om;
+    p.omega_x = b.omx;
+    p.omega_y = b.omy;
+    return p;
+}
+
+// Simulation::coupled_accelerations (SimulationRun.cpp:236-248): the pivot's accelerations and the angular one of a
+// body whose centre of mass is off its pivot (no gravity: the device has no body force with an immersed body).
+void coupled_accelerations(const fvg_run* r, double acc[3]) {
+    const fvg_run::Body& b = r->body;
+    const fvg_config& p = r->cfg;
+    const double c = std::cos(b.th), s = std::sin(b.th);
+    const double rx = r->cm0[0] * c - r->cm0[1] * s, ry = r->cm0[0] * s + r->cm0[1] * c;
+    const double fx = b.fx - p.ibm_stiff_x * b.x - p.ibm_damp_x * b.u, fy = b.fy - p.ibm_stiff_y * b.y - p.ibm_damp_y * b.v;
+    const double mp = b.mz - p.ibm_stiff_theta * b.th - p.ibm_damp_theta * b.om;
+    const double icm = p.ibm_inertia - p.ibm_mass * (rx * rx + ry * ry);
+    const double alpha = (mp - (rx * fy - ry * fx)) / icm;
+    const double gx = 0.0, gy = 0.0;
+    acc[0] = fx / p.ibm_mass + gx + alpha * ry + b.om * b.om * rx;
+    acc[1] = fy / p.ibm_mass + gy - alpha * rx + b.om * b.om * ry;
+    acc[2] = alpha;
+}
+
+// Simulation::advance_body (SimulationRun.cpp:250-310): the body's velocities by Adams-Bashforth 2 for a variable step
+// (an Euler step after a much shorter one), its displacement and angle by the trapezoid rule, from the loads of the step.
+void advance_body(fvg_run* r, double dt) {
+    fvg_run::Body& b = r->body;
+    const fvg_config& p = r->cfg;
+    const bool coupled = p.ibm_cm_x != 0.0 || p.ibm_cm_y != 0.0;
+    double acc[3] = {0.0, 0.0, 0.0};
+    if (coupled) coupled_accelerations(r, acc);
+    if (p.ibm_inertia > 0.0) {
+        const bool ab = b.dt > 0.0 && dt <= 2.0 * b.dt;
+        const double rr = ab ? dt / b.dt : 0.0;
+        const auto advance = [&](double om, double prev, double a) { return ab ? om + dt * ((1.0 + 0.5 * rr) * a - 0.5 * rr * prev) : om + dt * a; };
+        const double a = coupled ? acc[2] : (b.mz - p.ibm_stiff_theta * b.th - p.ibm_damp_theta * b.om) / p.ibm_inertia;
+        const double om1 = advance(b.om, b.aom, a);
+        if (p.nz > 1) {
+            const double ax = (b.mx - p.ibm_damp_theta * b.omx) / p.ibm_inertia, ay = (b.my - p.ibm_damp_theta * b.omy) / p.ibm_inertia;
+            const double omx1 = advance(b.omx, b.aomx, ax), omy1 = advance(b.omy, b.aomy, ay);
+            b.omx = omx1;
+            b.omy = omy1;
+            b.aomx = ax;
+            b.aomy = ay;
+        } else {
+            b.th += 0.5 * dt * (b.om + om1);
+        }
+        b.om = om1;
+        b.aom = a;
+    }
+    if (!(p.ibm_mass > 0.0)) {
+        b.dt = dt;
+        return;
+    }
+    const double gx = 0.0, gy = 0.0;
+    const double ax = coupled ? acc[0] : (b.fx - p.ibm_stiff_x * b.x - p.ibm_damp_x * b.u) / p.ibm_mass + gx;
+    const double ay = coupled ? acc[1] : (b.fy - p.ibm_stiff_y * b.y - p.ibm_damp_y * b.v) / p.ibm_mass + gy;
+    const bool d3 = p.nz > 1;
+    const double gz = 0.0;
+    const double az = d3 ? (b.fz - p.ibm_stiff_z * b.z - p.ibm_damp_z * b.w) / p.ibm_mass + gz : 0.0;
+    double u1, v1, w1 = 0.0;
+    if (b.dt > 0.0 && dt <= 2.0 * b.dt) {
+        const double rr = dt / b.dt;
+        u1 = b.u + dt * ((1.0 + 0.5 * rr) * ax - 0.5 * rr * b.ax);
+        v1 = b.v + dt * ((1.0 + 0.5 * rr) * ay - 0.5 * rr * b.ay);
+        if (d3) w1 = b.w + dt * ((1.0 + 0.5 * rr) * az - 0.5 * rr * b.az);
+    } else {
+        u1 = b.u + dt * ax;
+        v1 = b.v + dt * ay;
+        if (d3) w1 = b.w + dt * az;
+    }
+    b.x += 0.5 * dt * (b.u + u1);
+    b.y += 0.5 * dt * (b.v + v1);
+    b.u = u1;
+    b.v = v1;
+    b.ax = ax;
+    b.ay = ay;
+    if (d3) {
+        b.z += 0.5 * dt * (b.w + w1);
+        b.w = w1;
+        b.az = az;
+    }
+    b.dt = dt;
+}
+
 // The body at the start of a step at time t (place_body and ImmersedBoundary::move_to, SimulationRun.cpp:379-384 and
 // Physics.cpp:1310-1334): the geometry follows the pose in steps of a quarter cell (then the ghost table is built again
 // and the cells the body left take the wall layer's state, fill_fresh); in between only the wall velocities change.
 int place_body(fvg_run* r, double t) {
-    const fvg_run::Pose pose = prescribed_pose(r->cfg, t);
+    const fvg_run::Pose pose = body_pose(r, t);
     const double h = r->dim == 3 ? vmin(vmin(r->m.dx, r->m.dy), r->m.dz) : vmin(r->m.dx, r->m.dy);
     const double shift = vmax(vmax(fabs(pose.x - r->built.x), fabs(pose.y - r->built.y)), fabs(pose.z - r->built.z));
     r->pose = pose;
@@ -1802,7 +1976,30 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
             return bail(FVG_ERR_CONFIG);
         }
         run->ibm = true;
-        run->moving = c.ibm_vx != 0.0 || c.ibm_vy != 0.0 || c.ibm_vz != 0.0 || c.ibm_omega != 0.0 || c.ibm_omega_x != 0.0 || c.ibm_omega_y != 0.0;
+        run->dynamic = c.ibm_mass > 0.0 || c.ibm_inertia > 0.0;
+        run->moving = run->dynamic || c.ibm_vx != 0.0 || c.ibm_vy != 0.0 || c.ibm_vz != 0.0 || c.ibm_omega != 0.0 || c.ibm_omega_x != 0.0 ||
+                      c.ibm_omega_y != 0.0;
+        if (run->dynamic) {   // it starts at its placement with the velocities given (Simulation.cpp:301-312)
+            if (c.ibm_mass > 0.0) {
+                run->body.u = c.ibm_vx;
+                run->body.v = c.ibm_vy;
+                run->body.w = c.ibm_vz;
+            }
+            if (c.ibm_inertia > 0.0) {
+                run->body.om = c.ibm_omega;
+                run->body.omx = c.ibm_omega_x;
+                run->body.omy = c.ibm_omega_y;
+            }
+            if (c.ibm_cm_x != 0.0 || c.ibm_cm_y != 0.0) {   // body frame to mesh axes (a circle is placed unturned)
+                const double ca = std::cos(0.0), sa = std::sin(0.0);
+                run->cm0[0] = c.ibm_cm_x * ca + c.ibm_cm_y * sa;
+                run->cm0[1] = -c.ibm_cm_x * sa + c.ibm_cm_y * ca;
+            }
+            if (cudaMalloc(&run->d_bload, sizeof(double) * 6) != cudaSuccess || cudaMemset(run->d_bload, 0, sizeof(double) * 6) != cudaSuccess) {
+                run->err = "device allocation failed";
+                return bail(FVG_ERR_CUDA);
+            }
+        }
         if (const int rc = upload_ibm(run)) return bail(rc);
     }
     Ctl h{};
@@ -1849,7 +2046,7 @@ int fvg_destroy(fvg_run* run) {
     if (run->sens_tiles) cudaFree(run->sens_tiles);
     for (void* p : {(void*)run->d_mask, (void*)run->d_slot, (void*)run->d_forced, (void*)run->d_ghost, (void*)run->d_img_cell, (void*)run->d_img_w,
                     (void*)run->d_ratio, (void*)run->d_gn, (void*)run->d_deep, (void*)run->d_solid, (void*)run->d_loads, (void*)run->d_gvel,
-                    (void*)run->d_dvel})
+                    (void*)run->d_dvel, (void*)run->d_bload})
         if (p) cudaFree(p);
     if (run->stream) cudaStreamDestroy(run->stream);
     delete run;
@@ -1968,11 +2165,24 @@ static int run_steps(fvg_run* run, double t_end, int max_steps, int use_graph, i
                 break;
             }
             const fvg_config& c = run->cfg;
-            double travel = h2.dt * vmax(fabs(c.ibm_vx) / run->m.dx, fabs(c.ibm_vy) / run->m.dy);
-            if (run->dim == 3) travel = vmax(travel, h2.dt * fabs(c.ibm_vz) / run->m.dz);
-            if (travel > 1.0) {
+            const double wv[3] = {run->dynamic ? run->body.u : c.ibm_vx, run->dynamic ? run->body.v : c.ibm_vy, run->dynamic ? run->body.w : c.ibm_vz};
+            double travel = h2.dt * vmax(fabs(wv[0]) / run->m.dx, fabs(wv[1]) / run->m.dy);
+            if (run->dim == 3) travel = vmax(travel, h2.dt * fabs(wv[2]) / run->m.dz);
+            if (travel > 1.0) {   // (a circle or a sphere reaches no farther by turning: its rotation adds nothing here)
                 if (steps) *steps = h2.steps;
                 return fail(run, FVG_ERR_DIVERGED, "the moving body travelled more than one cell in a step (lower the CFL number)");
+            }
+            if (run->dynamic) {   // the loads of the step's first stage move the body on
+                double L[6];
+                CK(cudaMemcpy(L, run->d_bload, sizeof(L), cudaMemcpyDeviceToHost));
+                fvg_run::Body& b = run->body;
+                b.fx = L[0];
+                b.fy = L[1];
+                b.mz = L[2];
+                b.fz = L[3];
+                b.mx = L[4];
+                b.my = L[5];
+                advance_body(run, h2.dt);
             }
             h = h2;
         }

@@ -58,7 +58,16 @@ class FvgConfig(ctypes.Structure):
                 ("flux_quadrature", ctypes.c_int),
                 ("ibm_vx", ctypes.c_double), ("ibm_vy", ctypes.c_double), ("ibm_vz", ctypes.c_double),
                 ("ibm_omega", ctypes.c_double), ("ibm_omega_x", ctypes.c_double), ("ibm_omega_y", ctypes.c_double),
-                ("ibm_omega_from", ctypes.c_double), ("ibm_omega_until", ctypes.c_double)]
+                ("ibm_omega_from", ctypes.c_double), ("ibm_omega_until", ctypes.c_double),
+                ("ibm_mass", ctypes.c_double), ("ibm_inertia", ctypes.c_double),
+                ("ibm_stiff_x", ctypes.c_double), ("ibm_stiff_y", ctypes.c_double), ("ibm_stiff_z", ctypes.c_double),
+                ("ibm_damp_x", ctypes.c_double), ("ibm_damp_y", ctypes.c_double), ("ibm_damp_z", ctypes.c_double),
+                ("ibm_stiff_theta", ctypes.c_double), ("ibm_damp_theta", ctypes.c_double),
+                ("ibm_cm_x", ctypes.c_double), ("ibm_cm_y", ctypes.c_double), ("ibm_cm_given", ctypes.c_int)]
+
+BODY_KEYS = ("ibm_vx", "ibm_vy", "ibm_vz", "ibm_omega", "ibm_omega_x", "ibm_omega_y", "ibm_omega_from", "ibm_omega_until", "ibm_mass",
+             "ibm_inertia", "ibm_stiff_x", "ibm_stiff_y", "ibm_stiff_z", "ibm_damp_x", "ibm_damp_y", "ibm_damp_z", "ibm_stiff_theta",
+             "ibm_damp_theta")
 
 SOURCE_KEYS = ("source_rho", "source_mx", "source_my", "source_E", "source_mz")   # the state's slot order
 BOUNDARY_KEYS = ("u_in", "v_in", "rho_in", "p_out")
@@ -104,16 +113,12 @@ def _num(v):
 
 def not_on_device(params):
     """The reference features a parameter dict switches on that the device path does not compute (None: none). They
-    are refused, never ignored: AMR and an immersed body driven by the flow (a prescribed motion is computed). (Combinations
+    are refused, never ignored: AMR. (Combinations
     the device refuses, such as the body force with the mixed-precision form, are refused by fvg_create with
     FVG_ERR_CONFIG.)"""
     p = resolve(params)
     if _flag(p.get("use_amr", False)):
         return "adaptive meshes (use_amr)"
-    if _flag(p["use_ibm"]):
-        driven = [k for k in ("ibm_mass", "ibm_inertia") if (_num(p.get(k, 0)) or 0.0) != 0.0]
-        if driven:
-            return "an immersed body driven by the flow (" + ", ".join(driven) + ")"
     return None
 
 
@@ -248,8 +253,14 @@ def to_config(params, precision=0, device=0):
         raise ValueError(f"flux_quadrature must be midpoint or fourth; got '{quad}'")
     c.flux_quadrature = 1 if quad == "fourth" else 0
     c.mu = float(p["mu"])   # (derived from reynolds above when given)
-    for k in ("ibm_vx", "ibm_vy", "ibm_vz", "ibm_omega", "ibm_omega_x", "ibm_omega_y", "ibm_omega_from", "ibm_omega_until"):
+    for k in BODY_KEYS:
         setattr(c, k, float(p.get(k, 0.0)) if c.use_ibm else 0.0)
+    # the centre of mass off the pivot: both keys given (Params.cpp:334-338)
+    cmx, cmy = str(p.get("ibm_cm_x", "")).strip(), str(p.get("ibm_cm_y", "")).strip()
+    if bool(cmx) != bool(cmy):
+        raise ValueError("ibm_cm_x and ibm_cm_y go together")
+    c.ibm_cm_given = 1 if (cmx and cmy and c.use_ibm) else 0
+    c.ibm_cm_x, c.ibm_cm_y = (float(cmx), float(cmy)) if c.ibm_cm_given else (0.0, 0.0)
     return c
 
 

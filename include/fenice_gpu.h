@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define FVG_ABI_VERSION 7
+#define FVG_ABI_VERSION 8
 
 /* status codes */
 enum {
@@ -107,6 +107,14 @@ typedef struct fvg_config {
     double ibm_vx, ibm_vy, ibm_vz;
     double ibm_omega, ibm_omega_x, ibm_omega_y;
     double ibm_omega_from, ibm_omega_until;
+    /* [ibm] a body driven by the flow (Simulation::advance_body, cpp/src/SimulationRun.cpp:232-310): ibm_mass > 0 frees
+     * its translation, ibm_inertia > 0 (about the pivot, ibm_cx, ibm_cy) its rotation; springs and dampers at the pivot;
+     * the centre of mass off the pivot (2-D, ibm_cm_given). The loads are those of the first stage of each step; ibm_vx ..
+     * ibm_omega_y are then the initial velocities. Runge-Kutta and Euler schemes only (as the reference). */
+    double ibm_mass, ibm_inertia;
+    double ibm_stiff_x, ibm_stiff_y, ibm_stiff_z, ibm_damp_x, ibm_damp_y, ibm_damp_z, ibm_stiff_theta, ibm_damp_theta;
+    double ibm_cm_x, ibm_cm_y;
+    int ibm_cm_given;
 } fvg_config;
 
 typedef struct fvg_run fvg_run;

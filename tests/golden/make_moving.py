@@ -40,6 +40,23 @@ requires_3d = true
 state = { rho = "1.0 + 0.05*z", u = 0.1, v = 0.0, w = 0.0, p = 1.0 }
 """
 
+PUSH2D = """[case]
+name = "pushed body"
+description = "a body in a pressure gradient"
+
+[initial]
+state = { rho = "1.0 + 0.1*y", u = 0.05, v = 0.0, p = "1.0 + 0.3*x - 0.1*y" }
+"""
+
+PUSH3D = """[case]
+name = "pushed sphere"
+description = "a sphere in a pressure gradient"
+requires_3d = true
+
+[initial]
+state = { rho = 1.0, u = 0.0, v = 0.05, w = 0.0, p = "1.0 + 0.2*x + 0.1*z" }
+"""
+
 IBM = dict(use_ibm="true", ibm_shape="Cylinder")
 
 CASES = {
@@ -65,6 +82,24 @@ CASES = {
                                              bc_xmax="transmissive", bc_ymin="wall", bc_ymax="wall", bc_zmin="periodic", bc_zmax="periodic",
                                              ibm_shape="Sphere", use_ibm="true", ibm_radius=0.2, ibm_cx=0.45, ibm_cy=0.5, ibm_cz=0.4,
                                              ibm_vy=0.25, ibm_omega_y=2.0, cfl=0.4), 16),
+    # bodies driven by the flow: the loads of each step's first stage, Adams-Bashforth 2 for the velocities
+    "circle_free_rk2_2d": (PUSH2D, dict(nx=60, ny=40, Lx=3.0, Ly=2.0, reconstruction="muscl", muscl_limiter="Van Leer", time_scheme="SSP Runge-Kutta 2",
+                                        bc_xmin="transmissive", bc_xmax="transmissive", bc_ymin="wall", bc_ymax="wall", ibm_radius=0.3,
+                                        ibm_cx=1.5, ibm_cy=1.0, ibm_mass=0.2, ibm_vx=0.1, cfl=0.5, **IBM), 40),
+    "circle_springs_spin_viscous_2d": (PUSH2D, dict(nx=48, ny=40, Lx=1.2, Ly=1.0, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3",
+                                                    use_viscous="true", mu=0.02, bc_xmin="transmissive", bc_xmax="transmissive",
+                                                    bc_ymin="no_slip", bc_ymax="no_slip", ibm_radius=0.2, ibm_cx=0.6, ibm_cy=0.5, ibm_mass=0.05,
+                                                    ibm_stiff_x=5.0, ibm_damp_y=0.5, ibm_inertia=0.002, ibm_damp_theta=0.001, ibm_omega=0.5,
+                                                    cfl=0.4, **IBM), 30),
+    "circle_cm_offset_2d": (PUSH2D, dict(nx=50, ny=40, Lx=1.5, Ly=1.2, reconstruction="muscl", muscl_limiter="MC", time_scheme="SSP Runge-Kutta 2",
+                                         use_viscous="true", mu=0.01, bc_xmin="transmissive", bc_xmax="transmissive", bc_ymin="wall", bc_ymax="wall",
+                                         ibm_radius=0.25, ibm_cx=0.75, ibm_cy=0.6, ibm_mass=0.1, ibm_inertia=0.01, ibm_cm_x=0.05, ibm_cm_y=-0.02,
+                                         ibm_stiff_theta=0.5, cfl=0.4, **IBM), 30),
+    "sphere_free_3d": (PUSH3D, dict(nx=20, ny=20, nz=20, Lx=1.0, Ly=1.0, Lz=1.0, reconstruction="muscl", muscl_limiter="Van Leer",
+                                    time_scheme="SSP Runge-Kutta 3", use_viscous="true", mu=0.01, bc_xmin="transmissive", bc_xmax="transmissive",
+                                    bc_ymin="periodic", bc_ymax="periodic", bc_zmin="wall", bc_zmax="wall", ibm_shape="Sphere", use_ibm="true",
+                                    ibm_radius=0.2, ibm_cx=0.5, ibm_cy=0.5, ibm_cz=0.5, ibm_mass=0.02, ibm_inertia=0.0005, ibm_stiff_z=2.0,
+                                    ibm_damp_theta=0.0001, ibm_omega_x=0.3, cfl=0.5), 14),
     # the body outruns the ghost table: the reference stops
     "circle_too_fast_2d": (FLOW2D, dict(nx=30, ny=20, Lx=3.0, Ly=2.0, reconstruction="muscl", time_scheme="SSP Runge-Kutta 2",
                                         bc_xmin="transmissive", bc_xmax="transmissive", bc_ymin="wall", bc_ymax="wall", ibm_radius=0.3,
