@@ -24,6 +24,11 @@ struct IbmArgs {
     // (ImmersedBoundary::body_velocity); null for a static body
     const double* gvel;
     const double* dvel;
+    // gravity (the body force): the ghost pressure carries the hydrostatic difference from the image point (per ghost its
+    // span, ghost-wall + wall-image); hydro = 0 without
+    int hydro;
+    double grav[3];
+    const double* span;
     const double* U;          // the state the ghost cells are filled from
     double* forced;           // force: [5 (ng + nd)] the forced states, by slot (ghosts first, then the deep cells)
     double* Uout;             // reset: the state written in place (may be U)
@@ -49,6 +54,9 @@ template <int NV> __global__ void ibm_fill_kernel(const IbmArgs a) {
                 for (int v = 0; v < NV; ++v) W[v] += w * Wq[v];
             }
             const double nx = a.gn[3 * k], ny = a.gn[3 * k + 1], nz = a.gn[3 * k + 2], ratio = a.ratio[k];
+            // the hydrostatic pressure from the image point to the ghost cell (Physics.cpp:1592); W[3] is the pressure in both
+            // layouts
+            if (a.hydro) W[3] -= W[0] * a.span[k] * (a.grav[0] * nx + a.grav[1] * ny + (NV == 5 ? a.grav[2] * nz : 0.0));
             // in 2-D the reference's velocity index 4 is the z component, here the last of 4 is the pressure
             const double wz = NV == 5 ? W[4] : 0.0;
             const double un = NV == 5 ? W[1] * nx + W[2] * ny + wz * nz : W[1] * nx + W[2] * ny;

@@ -20,6 +20,7 @@ struct IbmTable {
     std::vector<double> img_w;         // 8 per ghost: their weights (0 for a solid cell; renormalised)
     std::vector<double> ratio, gnx, gny, gnz;   // per ghost: distance ghost-wall / distance image-wall, and the wall normal
     std::vector<double> gwx, gwy, gwz;          // per ghost: its wall point (the wall velocity of a moving body is taken there)
+    std::vector<double> span;                   // per ghost: distance ghost-wall + wall-image (the hydrostatic correction's; 0 in a fallback)
     std::vector<int> deep;             // the other solid cells
     int fallback = 0;                  // ghosts with no fluid around any image point (nearest fluid cell, ratio 0)
 };
@@ -205,6 +206,7 @@ inline std::string build_ibm_geom(const IbmGeom& m, IbmTable& t) {
                     t.img_w.push_back(w[q]);
                 }
                 t.ratio.push_back(ratio);
+                t.span.push_back(found ? dg + di : 0.0);
                 t.gnx.push_back(gx);
                 t.gny.push_back(gy);
                 t.gnz.push_back(gz);

@@ -362,13 +362,18 @@ __global__ void k_face_flux(Eos<double> e, double shock_blend, const double* UL,
 
 // Simulation::ibm_loads (cpp/src/SimulationRun.cpp:134-155): {Fx, Fy, Mz} = the momentum residual of the solid cells times
 // the cell volume, summed in cell order (one thread: the reference's order, so the bits), Mz about (cx, cy).
-__global__ void k_ibm_loads(const double* R, long long plane, const int* cells, int n, double vol, int nx, int ny, double dx, double dy, double cx,
-                            double cy, double* out) {
+__global__ void k_ibm_loads(const double* R, const double* U, long long plane, const int* cells, int n, double vol, int nx, int ny, double dx,
+                            double dy, double cx, double cy, double gx, double gy, int grav, double* out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double fx = 0.0, fy = 0.0, mz = 0.0;
     for (int k = 0; k < n; ++k) {
         const int c = cells[k];
-        const double ex = R[plane + c] * vol, ey = R[2 * plane + c] * vol;
+        double rx = R[plane + c], ry = R[2 * plane + c];
+        if (grav) {   // the weight is not a load
+            rx -= U[c] * gx;
+            ry -= U[c] * gy;
+        }
+        const double ex = rx * vol, ey = ry * vol;
         fx += ex;
         fy += ey;
         const double xc = ((c % nx) + 0.5) * dx + 0.0, yc = (((c / nx) % ny) + 0.5) * dy + 0.0;
@@ -383,18 +388,26 @@ __global__ void k_ibm_loads(const double* R, long long plane, const int* cells, 
 // Simulation::ibm_load_terms + sum_load_terms (cpp/src/SimulationRun.cpp:312-350) of the first stage's residual R: per
 // solid cell (in cell order, one thread: the reference's sums) the momentum residual times the cell volume, its moment
 // about the pivot, and in 3-D the z component and the moments about x and y; out = {fx, fy, mz, fz, mx, my}.
-__global__ void k_body_loads(const int* gate, const double* R, long long plane, const int* cells, int n, double vol, int nx, int ny, double dx,
-                             double dy, double dz, int three_d, double px, double py, double pz, double* out) {
+__global__ void k_body_loads(const int* gate, const double* R, const double* U, long long plane, const int* cells, int n, double vol, int nx, int ny,
+                             double dx, double dy, double dz, int three_d, double px, double py, double pz, int grav, double gx, double gy, double gz,
+                             double* out) {
     if (!*gate || threadIdx.x != 0) return;
     double fx = 0.0, fy = 0.0, mz = 0.0, fz = 0.0, mx = 0.0, my = 0.0;
     for (int q = 0; q < n; ++q) {
         const long long c = cells[q];
-        const double ex = R[plane + c] * vol, ey = R[2 * plane + c] * vol;
+        double rx = R[plane + c], ry = R[2 * plane + c];
+        if (grav) {   // the weight is not a load
+            rx -= U[c] * gx;
+            ry -= U[c] * gy;
+        }
+        const double ex = rx * vol, ey = ry * vol;
         const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
         const double xc = (i + 0.5) * dx + 0.0, yc = (j + 0.5) * dy + 0.0;
         double ez = 0.0, tx = 0.0, ty = 0.0;
         if (three_d) {
-            ez = R[4 * plane + c] * vol;
+            double rz = R[4 * plane + c];
+            if (grav) rz -= U[c] * gz;
+            ez = rz * vol;
             const double x = xc - px, y = yc - py, z = (k + 0.5) * dz + 0.0 - pz;
             tx = y * ez - z * ey;
             ty = z * ex - x * ez;
@@ -535,7 +548,7 @@ struct fvg_run {
     int* d_solid = nullptr;   // the solid cells in cell order (the loads' sum)
     int nsolid = 0;
     double* d_loads = nullptr;
-    double *d_forced = nullptr, *d_img_w = nullptr, *d_ratio = nullptr, *d_gn = nullptr;
+    double *d_forced = nullptr, *d_img_w = nullptr, *d_ratio = nullptr, *d_gn = nullptr, *d_span = nullptr;
     // the learned sensor (fvg_set_sensor): its weights (a copy), the logit threshold, the refresh period and dilation,
     // the two flag buffers (the result in sens_result), the counters
     void* sens = nullptr;
@@ -669,7 +682,6 @@ std::string validate(const fvg_config& c) {
             return "positivity_fallback needs reconstruction = weno3 or weno5 (the other schemes keep their reconstructed states between the cells)";
         if (c.precision != FVG_PREC_FP64) return "positivity_fallback runs in the FP64 form only";
     }
-    if (c.use_bodyforce && c.use_ibm) return "the body force with an immersed body (gravity in its ghost states) is not supported on the device";
     if (!(c.cfl > 0)) return "cfl must be > 0";
     if (c.use_ibm) {   // a prescribed motion (Params.cpp:505-516)
         const bool moving = c.ibm_vx != 0.0 || c.ibm_vy != 0.0 || c.ibm_vz != 0.0 || c.ibm_omega != 0.0 || c.ibm_omega_x != 0.0 || c.ibm_omega_y != 0.0;
@@ -877,6 +889,9 @@ cudaError_t ibm_fill(fvg_run* r, const double* Usrc, double* Uout, int reset, co
     a.p_ref = r->cfg.p_out;
     a.gvel = r->moving ? r->d_gvel : nullptr;
     a.dvel = r->moving ? r->d_dvel : nullptr;
+    a.hydro = r->bc.grav_on && (r->bc.grav[0] != 0.0 || r->bc.grav[1] != 0.0 || r->bc.grav[2] != 0.0);   // set_gravity
+    for (int d = 0; d < 3; ++d) a.grav[d] = r->bc.grav[d];
+    a.span = r->d_span;
     a.U = Usrc;
     a.forced = r->d_forced;
     a.Uout = Uout;
@@ -1119,9 +1134,9 @@ cudaError_t enqueue_step(fvg_run* r, bool refresh = true) {
     k_stage1_dt<<<1, 1024, 0, r->stream>>>(c, r->bm[0], r->nb, r->bmv[0], nbv);
     if (r->dynamic) {   // a body driven by the flow: the loads of this first stage, about the pivot of the step
         const double vol = r->dim == 3 ? r->m.dx * r->m.dy * r->m.dz : r->m.dx * r->m.dy;
-        k_body_loads<<<1, 32, 0, r->stream>>>(act, r->R, r->m.plane, r->d_solid, r->nsolid, vol, r->m.nx, r->m.ny, r->m.dx, r->m.dy, r->m.dz,
+        k_body_loads<<<1, 32, 0, r->stream>>>(act, r->R, r->U, r->m.plane, r->d_solid, r->nsolid, vol, r->m.nx, r->m.ny, r->m.dx, r->m.dy, r->m.dz,
                                               r->dim == 3, r->cfg.ibm_cx + r->body.x, r->cfg.ibm_cy + r->body.y, r->cfg.ibm_cz + r->body.z,
-                                              r->d_bload);
+                                              r->bc.grav_on, r->bc.grav[0], r->bc.grav[1], r->bc.grav[2], r->d_bload);
     }
     if (ts == FVG_TS_EULER) {
         k_axpy<<<axpy_blocks(r), 256, 0, r->stream>>>(c, r->U, r->U, r->R, r->m.plane, r->m.ncells, r->nvar);
@@ -1496,7 +1511,7 @@ int upload_velocities(fvg_run* r) {
 int upload_ibm(fvg_run* run) {
     for (void** p : {(void**)&run->d_slot, (void**)&run->d_forced, (void**)&run->d_ghost, (void**)&run->d_img_cell, (void**)&run->d_img_w,
                      (void**)&run->d_ratio, (void**)&run->d_gn, (void**)&run->d_deep, (void**)&run->d_solid, (void**)&run->d_gvel,
-                     (void**)&run->d_dvel})
+                     (void**)&run->d_dvel, (void**)&run->d_span})
         if (*p) {
             cudaFree(*p);
             *p = nullptr;
@@ -1519,6 +1534,7 @@ int upload_ibm(fvg_run* run) {
               cudaMalloc(&run->d_ghost, sizeof(int) * ng1) == cudaSuccess && cudaMalloc(&run->d_img_cell, sizeof(int) * 8 * ng1) == cudaSuccess &&
               cudaMalloc(&run->d_img_w, sizeof(double) * 8 * ng1) == cudaSuccess && cudaMalloc(&run->d_ratio, sizeof(double) * ng1) == cudaSuccess &&
               cudaMalloc(&run->d_gn, sizeof(double) * 3 * ng1) == cudaSuccess && cudaMalloc(&run->d_deep, sizeof(int) * nd1) == cudaSuccess &&
+              cudaMalloc(&run->d_span, sizeof(double) * ng1) == cudaSuccess &&
               (!run->moving || (cudaMalloc(&run->d_gvel, sizeof(double) * 3 * ng1) == cudaSuccess &&
                                 cudaMalloc(&run->d_dvel, sizeof(double) * 3 * nd1) == cudaSuccess));
     ok = ok && cudaMemcpy(run->d_mask, t.mask.data(), run->m.ncells, cudaMemcpyHostToDevice) == cudaSuccess &&
@@ -1528,7 +1544,8 @@ int upload_ibm(fvg_run* run) {
              cudaMemcpy(run->d_img_cell, t.img_cell.data(), sizeof(int) * 8 * run->ng, cudaMemcpyHostToDevice) == cudaSuccess &&
              cudaMemcpy(run->d_img_w, t.img_w.data(), sizeof(double) * 8 * run->ng, cudaMemcpyHostToDevice) == cudaSuccess &&
              cudaMemcpy(run->d_ratio, t.ratio.data(), sizeof(double) * run->ng, cudaMemcpyHostToDevice) == cudaSuccess &&
-             cudaMemcpy(run->d_gn, gn.data(), sizeof(double) * 3 * run->ng, cudaMemcpyHostToDevice) == cudaSuccess;
+             cudaMemcpy(run->d_gn, gn.data(), sizeof(double) * 3 * run->ng, cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(run->d_span, t.span.data(), sizeof(double) * run->ng, cudaMemcpyHostToDevice) == cudaSuccess;
     if (ok && run->nd > 0) ok = cudaMemcpy(run->d_deep, t.deep.data(), sizeof(int) * run->nd, cudaMemcpyHostToDevice) == cudaSuccess;
     if (!ok) return fail(run, FVG_ERR_CUDA, "device allocation of the immersed body's tables failed");
     std::vector<int> solid_cells;
@@ -1588,7 +1605,7 @@ fvg_run::Pose body_pose(const fvg_run* r, double t) {
 }
 
 // Simulation::coupled_accelerations (SimulationRun.cpp:236-248): the pivot's accelerations and the angular one of a
-// body whose centre of mass is off its pivot (no gravity: the device has no body force with an immersed body).
+// body whose centre of mass is off its pivot (gravity: the body force's).
 void coupled_accelerations(const fvg_run* r, double acc[3]) {
     const fvg_run::Body& b = r->body;
     const fvg_config& p = r->cfg;
@@ -1598,7 +1615,7 @@ void coupled_accelerations(const fvg_run* r, double acc[3]) {
     const double mp = b.mz - p.ibm_stiff_theta * b.th - p.ibm_damp_theta * b.om;
     const double icm = p.ibm_inertia - p.ibm_mass * (rx * rx + ry * ry);
     const double alpha = (mp - (rx * fy - ry * fx)) / icm;
-    const double gx = 0.0, gy = 0.0;
+    const double gx = p.use_bodyforce ? p.gx : 0.0, gy = p.use_bodyforce ? p.gy : 0.0;
     acc[0] = fx / p.ibm_mass + gx + alpha * ry + b.om * b.om * rx;
     acc[1] = fy / p.ibm_mass + gy - alpha * rx + b.om * b.om * ry;
     acc[2] = alpha;
@@ -1635,11 +1652,11 @@ void advance_body(fvg_run* r, double dt) {
         b.dt = dt;
         return;
     }
-    const double gx = 0.0, gy = 0.0;
+    const double gx = p.use_bodyforce ? p.gx : 0.0, gy = p.use_bodyforce ? p.gy : 0.0;
     const double ax = coupled ? acc[0] : (b.fx - p.ibm_stiff_x * b.x - p.ibm_damp_x * b.u) / p.ibm_mass + gx;
     const double ay = coupled ? acc[1] : (b.fy - p.ibm_stiff_y * b.y - p.ibm_damp_y * b.v) / p.ibm_mass + gy;
     const bool d3 = p.nz > 1;
-    const double gz = 0.0;
+    const double gz = p.use_bodyforce && d3 ? p.gz : 0.0;
     const double az = d3 ? (b.fz - p.ibm_stiff_z * b.z - p.ibm_damp_z * b.w) / p.ibm_mass + gz : 0.0;
     double u1, v1, w1 = 0.0;
     if (b.dt > 0.0 && dt <= 2.0 * b.dt) {
@@ -2046,7 +2063,7 @@ int fvg_destroy(fvg_run* run) {
     if (run->sens_tiles) cudaFree(run->sens_tiles);
     for (void* p : {(void*)run->d_mask, (void*)run->d_slot, (void*)run->d_forced, (void*)run->d_ghost, (void*)run->d_img_cell, (void*)run->d_img_w,
                     (void*)run->d_ratio, (void*)run->d_gn, (void*)run->d_deep, (void*)run->d_solid, (void*)run->d_loads, (void*)run->d_gvel,
-                    (void*)run->d_dvel, (void*)run->d_bload})
+                    (void*)run->d_dvel, (void*)run->d_bload, (void*)run->d_span})
         if (p) cudaFree(p);
     if (run->stream) cudaStreamDestroy(run->stream);
     delete run;
@@ -2499,9 +2516,9 @@ int fvg_ibm_loads(fvg_run* run, double* loads) {
     const fvg_config& c = run->cfg;
     const double vol = run->dim == 3 ? run->m.dx * run->m.dy * run->m.dz : run->m.dx * run->m.dy;
     // (the moment centre follows a moving body, SimulationRun.cpp:140-141)
-    k_ibm_loads<<<1, 32, 0, run->stream>>>(out, run->m.plane, run->d_solid, run->nsolid, vol, run->m.nx, run->m.ny, run->m.dx, run->m.dy,
-                                           run->moving ? c.ibm_cx + run->pose.x : c.ibm_cx, run->moving ? c.ibm_cy + run->pose.y : c.ibm_cy,
-                                           run->d_loads);
+    k_ibm_loads<<<1, 32, 0, run->stream>>>(out, run->Ucur(), run->m.plane, run->d_solid, run->nsolid, vol, run->m.nx, run->m.ny, run->m.dx,
+                                           run->m.dy, run->moving ? c.ibm_cx + run->pose.x : c.ibm_cx, run->moving ? c.ibm_cy + run->pose.y : c.ibm_cy,
+                                           run->bc.grav[0], run->bc.grav[1], run->bc.grav_on, run->d_loads);
     CK(cudaGetLastError());
     double h[3];
     CK(cudaMemcpyAsync(h, run->d_loads, sizeof(h), cudaMemcpyDeviceToHost, run->stream));

@@ -100,6 +100,18 @@ CASES = {
                                     bc_ymin="periodic", bc_ymax="periodic", bc_zmin="wall", bc_zmax="wall", ibm_shape="Sphere", use_ibm="true",
                                     ibm_radius=0.2, ibm_cx=0.5, ibm_cy=0.5, ibm_cz=0.5, ibm_mass=0.02, ibm_inertia=0.0005, ibm_stiff_z=2.0,
                                     ibm_damp_theta=0.0001, ibm_omega_x=0.3, cfl=0.5), 14),
+    # gravity (the body force): hydrostatic ghost pressures, loads net of the weight, a falling body
+    "cylinder_gravity_static_2d": (PUSH2D, dict(nx=40, ny=40, Lx=1.0, Ly=1.0, reconstruction="muscl", muscl_limiter="Van Leer",
+                                                time_scheme="MUSCL-Hancock", bc_xmin="wall", bc_xmax="wall", bc_ymin="wall", bc_ymax="wall",
+                                                ibm_radius=0.2, ibm_cx=0.5, ibm_cy=0.45, use_bodyforce="true", gx=0.3, gy=-2.0, cfl=0.5, **IBM), 30),
+    "circle_falling_viscous_2d": (PUSH2D, dict(nx=40, ny=48, Lx=1.0, Ly=1.2, reconstruction="muscl", muscl_limiter="MC", time_scheme="SSP Runge-Kutta 2",
+                                               use_viscous="true", mu=0.01, bc_xmin="no_slip", bc_xmax="no_slip", bc_ymin="wall", bc_ymax="wall",
+                                               ibm_radius=0.15, ibm_cx=0.5, ibm_cy=0.7, ibm_mass=0.1, ibm_inertia=0.001, use_bodyforce="true",
+                                               gx=0.0, gy=-3.0, cfl=0.4, **IBM), 30),
+    "sphere_gravity_weno3_3d": (PUSH3D, dict(nx=18, ny=16, nz=16, Lx=1.0, Ly=1.0, Lz=1.0, reconstruction="weno3", time_scheme="SSP Runge-Kutta 3",
+                                             bc_xmin="wall", bc_xmax="wall", bc_ymin="periodic", bc_ymax="periodic", bc_zmin="wall", bc_zmax="wall",
+                                             ibm_shape="Sphere", use_ibm="true", ibm_radius=0.2, ibm_cx=0.5, ibm_cy=0.5, ibm_cz=0.55, ibm_mass=0.05,
+                                             use_bodyforce="true", gx=0.1, gy=0.0, gz=-1.5, cfl=0.5), 12),
     # the body outruns the ghost table: the reference stops
     "circle_too_fast_2d": (FLOW2D, dict(nx=30, ny=20, Lx=3.0, Ly=2.0, reconstruction="muscl", time_scheme="SSP Runge-Kutta 2",
                                         bc_xmin="transmissive", bc_xmax="transmissive", bc_ymin="wall", bc_ymax="wall", ibm_radius=0.3,

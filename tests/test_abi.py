@@ -43,7 +43,7 @@ def create_code(params):
     (dict(bc_xmin="periodic", bc_xmax="wall"), "periodic"),
     (dict(reconstruction="weno5", time_scheme="MUSCL-Hancock"), "MUSCL-Hancock"),
     (dict(use_bodyforce=True, reconstruction="muscl", time_scheme="SSP Runge-Kutta 2", precision_mixed=True), "FP64 form only"),
-    (dict(use_bodyforce=True, use_ibm=True, bc_xmin="vel_inlet"), "immersed body"),
+    (dict(use_ibm=True, ibm_shape="Cylinder", ibm_radius=0.1, flux_quadrature="fourth", reconstruction="weno5", time_scheme="rk3"), "immersed body"),
     (dict(boundary_order=3), "boundary_order"),
     (dict(cfl=0.0), "cfl"),
 ])

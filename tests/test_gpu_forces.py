@@ -65,6 +65,3 @@ def test_body_force_refusals(fx):
     U = fx["grav_muscl_rk2_2d/U0"]
     with pytest.raises(ValueError, match="FP64 form only"):
         Run(p, U=U, precision=1)
-    q = dict(p, use_ibm=True, ibm_shape="Cylinder", ibm_radius=0.2, ibm_cx=0.5, ibm_cy=0.5, bc_xmin="vel_inlet", u_in=0.5)
-    with pytest.raises(ValueError, match="immersed body"):
-        Run(q, U=U)

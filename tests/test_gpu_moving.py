@@ -1,7 +1,8 @@
 """An immersed body in prescribed motion on the device against the reference's own time loop (tests/golden/moving.npz,
 written by tests/golden/make_moving.py with the reference's command-line solver): a translating circle, a circle that
 spins within a time window (viscous, no-slip), a translating and turning circle under MUSCL-Hancock, and translating and
-spinning spheres (WENO5-Z and viscous MUSCL), and bodies driven by the flow (free, on springs and dampers, spinning, with the centre of mass off the pivot; a free sphere), bit for bit after their steps: the geometry rebuilt every quarter cell, the
+spinning spheres (WENO5-Z and viscous MUSCL), and bodies driven by the flow (free, on springs and dampers, spinning, with the centre of mass off the pivot; a free sphere) and bodies under gravity (hydrostatic ghost pressures, loads net
+of the weight, a falling circle and sphere), bit for bit after their steps: the geometry rebuilt every quarter cell, the
 cells the body left filled from the wall layer, the ghost and deep cells at the wall's velocity. A body that travels more
 than a cell in a step stops the run, as the reference's."""
 import json
