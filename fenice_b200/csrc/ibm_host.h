@@ -25,16 +25,49 @@ struct IbmTable {
     int fallback = 0;                  // ghosts with no fluid around any image point (nearest fluid cell, ratio 0)
 };
 
+inline double dmax_(double a, double b) { return (a < b) ? b : a; }
+inline double dmin_(double a, double b) { return (b < a) ? b : a; }
+
+// Polygon2D::contains (cpp/src/Geometry.cpp:30-38): the even-odd rule
+inline bool poly_contains(const std::vector<double>& P, double x, double y) {
+    bool in = false;
+    const size_t n = P.size() / 2;
+    for (size_t i = 0, j = n - 1; i < n; j = i++) {
+        const double xi = P[2 * i], yi = P[2 * i + 1], xj = P[2 * j], yj = P[2 * j + 1];
+        if ((yi > y) != (yj > y) && x < (xj - xi) * (y - yi) / (yj - yi) + xi) in = !in;
+    }
+    return in;
+}
+
 struct IbmGeom {
-    bool ball;   // a sphere in 3-D; otherwise a circle (2-D) or a cylinder along z (3-D)
-    double cx, cy, cz, r;
-    int nx, ny, nz;
-    double dx, dy, dz;
+    bool ball = false;   // a sphere in 3-D; otherwise a circle (2-D) or a cylinder along z (3-D) ...
+    bool poly = false;   // ... or a polygon section (an airfoil; extruded along z in 3-D)
+    double cx = 0, cy = 0, cz = 0, r = 0;
+    std::vector<double> pts;                    // the polygon's vertices (x, y) where it is placed
+    double px0 = 0, px1 = 0, py0 = 0, py1 = 0;  // and its bounding box
+    int nx = 0, ny = 0, nz = 0;
+    double dx = 0, dy = 0, dz = 0;
     size_t cell(int i, int j, int k) const { return (static_cast<size_t>(k) * ny + j) * nx + i; }
     double xc(int i) const { return (i + 0.5) * dx + 0.0; }
     double yc(int j) const { return (j + 0.5) * dy + 0.0; }
     double zc(int k) const { return (k + 0.5) * dz + 0.0; }
+    void set_polygon(std::vector<double> p) {   // the bounding box as ImmersedBoundary's polygon constructor takes it
+        pts = std::move(p);
+        double x0 = 1e300, x1 = -1e300, y0 = 1e300, y1 = -1e300;
+        for (size_t q = 0; q < pts.size() / 2; ++q) {
+            x0 = dmin_(x0, pts[2 * q]);
+            x1 = dmax_(x1, pts[2 * q]);
+            y0 = dmin_(y0, pts[2 * q + 1]);
+            y1 = dmax_(y1, pts[2 * q + 1]);
+        }
+        px0 = x0;
+        px1 = x1;
+        py0 = y0;
+        py1 = y1;
+    }
+    // ImmersedBoundary::solid_at (cpp/src/Physics.cpp:892-907)
     bool solid_at(double x, double y, double z) const {
+        if (poly) return !(x < px0 || x > px1 || y < py0 || y > py1 || !poly_contains(pts, x, y));
         if (ball) {
             const double dxc = x - cx, dyc = y - cy;
             const double r2 = dxc * dxc + dyc * dyc + (z - cz) * (z - cz);
@@ -44,10 +77,53 @@ struct IbmGeom {
         const double r2 = dxc * dxc + dyc * dyc;
         return std::sqrt(r2) <= r;
     }
+    // ImmersedBoundary::closest_wall_point (Physics.cpp:989-1034): the wall point nearest to (x, y) and the outward normal
+    void closest_wall_point(double x, double y, double& wx, double& wy, double& gx, double& gy) const {
+        if (!poly) {
+            const double ex = x - cx, ey = y - cy, d = std::sqrt(ex * ex + ey * ey);
+            gx = d > 0.0 ? ex / d : 1.0;
+            gy = d > 0.0 ? ey / d : 0.0;
+            wx = cx + r * gx;
+            wy = cy + r * gy;
+            return;
+        }
+        const size_t n = pts.size() / 2;
+        double best = 1e300;
+        size_t seg = 0;
+        wx = wy = 0.0;
+        for (size_t k = 0; k < n; ++k) {
+            const double ax = pts[2 * k], ay = pts[2 * k + 1], bx = pts[2 * ((k + 1) % n)], by = pts[2 * ((k + 1) % n) + 1];
+            const double ox = dmax_(dmax_(dmin_(ax, bx) - x, x - dmax_(ax, bx)), 0.0);
+            const double oy = dmax_(dmax_(dmin_(ay, by) - y, y - dmax_(ay, by)), 0.0);
+            if (ox * ox + oy * oy > best * (1.0 + 1e-9)) continue;   // cannot win
+            const double ex = bx - ax, ey = by - ay, l2 = ex * ex + ey * ey;
+            double t = l2 > 0.0 ? ((x - ax) * ex + (y - ay) * ey) / l2 : 0.0;
+            t = dmin_(1.0, dmax_(0.0, t));
+            const double qx = ax + t * ex, qy = ay + t * ey, d2 = (x - qx) * (x - qx) + (y - qy) * (y - qy);
+            if (d2 < best) {
+                best = d2;
+                wx = qx;
+                wy = qy;
+                seg = k;
+            }
+        }
+        const double d = std::sqrt(best);
+        const bool inside = poly_contains(pts, x, y);
+        if (d > 1e-12) {   // outward: from the point to the wall if it is inside, from the wall to the point if outside
+            gx = (inside ? wx - x : x - wx) / d;
+            gy = (inside ? wy - y : y - wy) / d;
+            return;
+        }
+        const double ax = pts[2 * seg], ay = pts[2 * seg + 1], bx = pts[2 * ((seg + 1) % n)], by = pts[2 * ((seg + 1) % n) + 1];
+        const double ex = bx - ax, ey = by - ay, l = std::sqrt(ex * ex + ey * ey);   // on the wall: the segment normal, pointing out
+        gx = ey / l;
+        gy = -ex / l;
+        if (poly_contains(pts, wx + 1e-6 * l * gx, wy + 1e-6 * l * gy)) {
+            gx = -gx;
+            gy = -gy;
+        }
+    }
 };
-
-inline double dmax_(double a, double b) { return (a < b) ? b : a; }
-inline double dmin_(double a, double b) { return (b < a) ? b : a; }
 
 // bilinear probe in the four cell centres around (x, y) of layer k; solid cells weigh 0, the rest renormalised (make_probe)
 inline bool make_probe(const IbmGeom& m, const std::vector<unsigned char>& mask, double x, double y, int layer, int* cell, double* w) {
@@ -94,11 +170,33 @@ inline bool make_probe3(const IbmGeom& m, const std::vector<unsigned char>& mask
     return true;
 }
 
+// place_airfoil (cpp/src/Geometry.cpp:143-152): the unit section of the configuration (leading edge at the origin, chord 1)
+// scaled to ibm_chord, its quarter chord at (ibm_cx, ibm_cy), turned clockwise by ibm_aoa degrees (nose up).
+inline std::vector<double> place_section(const fvg_config& c, std::string& err) {
+    std::vector<double> out;
+    if (!c.ibm_section || c.ibm_section_points < 3) {
+        err = "an airfoil section needs at least 3 points (ibm_section)";
+        return out;
+    }
+    if (!(c.ibm_chord > 0.0)) {
+        err = "ibm_chord must be > 0";
+        return out;
+    }
+    const double a = c.ibm_aoa * 3.14159265358979323846 / 180.0, ca = std::cos(a), sa = std::sin(a);
+    for (int q = 0; q < c.ibm_section_points; ++q) {
+        const double x = (c.ibm_section[2 * q] - 0.25) * c.ibm_chord, y = c.ibm_section[2 * q + 1] * c.ibm_chord;
+        out.push_back(c.ibm_cx + x * ca + y * sa);
+        out.push_back(c.ibm_cy - x * sa + y * ca);
+    }
+    return out;
+}
+
 // The body's geometry on the mesh of a configuration, its centre at (cx, cy, cz) (a moving body: its placement plus the
 // displacement of its pose, ImmersedBoundary::place_geometry, cpp/src/Physics.cpp:1162-1194).
 inline IbmGeom ibm_geom(const fvg_config& c, double cx, double cy, double cz) {
     IbmGeom m;
     m.ball = c.nz > 1 && c.ibm_shape == 1;
+    m.poly = c.ibm_shape == 2;
     m.cx = cx;
     m.cy = cy;
     m.cz = cz;
@@ -116,9 +214,15 @@ inline std::string build_ibm_geom(const IbmGeom& m, IbmTable& t);
 
 // The mask and the ghost table of a static body on the whole mesh; returns "" or an error message.
 inline std::string build_ibm(const fvg_config& c, IbmTable& t) {
-    if (c.ibm_shape != 0 && c.ibm_shape != 1) return "ibm_shape: Cylinder or Sphere only on the device";
+    if (c.ibm_shape < 0 || c.ibm_shape > 2) return "ibm_shape: Cylinder, Sphere or a section (airfoil) on the device";
     if (c.ibm_curvature) return "ibm_curvature is not supported on the device";
-    return build_ibm_geom(ibm_geom(c, c.ibm_cx, c.ibm_cy, c.ibm_cz), t);
+    IbmGeom g = ibm_geom(c, c.ibm_cx, c.ibm_cy, c.ibm_cz);
+    if (g.poly) {
+        std::string err;
+        g.set_polygon(place_section(c, err));
+        if (!err.empty()) return err;
+    }
+    return build_ibm_geom(g, t);
 }
 
 // The mask and the ghost table of the body of geometry m (ImmersedBoundary::build_ghosts, Physics.cpp:1397-1537).
@@ -128,9 +232,17 @@ inline std::string build_ibm_geom(const IbmGeom& m, IbmTable& t) {
     const size_t n = static_cast<size_t>(m.nx) * m.ny * m.nz;
     t = IbmTable();
     t.mask.assign(n, 0);
-    for (int k = 0; k < m.nz; ++k)
+    if (m.poly) {   // a section: the same in every layer
         for (int j = 0; j < m.ny; ++j)
-            for (int i = 0; i < m.nx; ++i) t.mask[m.cell(i, j, k)] = m.solid_at(m.xc(i), m.yc(j), m.zc(k)) ? 1 : 0;
+            for (int i = 0; i < m.nx; ++i) {
+                if (!m.solid_at(m.xc(i), m.yc(j), 0.0)) continue;
+                for (int k = 0; k < m.nz; ++k) t.mask[m.cell(i, j, k)] = 1;
+            }
+    } else {
+        for (int k = 0; k < m.nz; ++k)
+            for (int j = 0; j < m.ny; ++j)
+                for (int i = 0; i < m.nx; ++i) t.mask[m.cell(i, j, k)] = m.solid_at(m.xc(i), m.yc(j), m.zc(k)) ? 1 : 0;
+    }
     const double h = m.ball ? std::max({m.dx, m.dy, m.dz}) : std::max(m.dx, m.dy);
     const int dkmax = d3 ? 2 : 0;
     const auto solid = [&](int i, int j, int k) { return t.mask[m.cell(i, j, k)] != 0; };
@@ -157,12 +269,8 @@ inline std::string build_ibm_geom(const IbmGeom& m, IbmTable& t) {
                     wx = m.cx + m.r * gx;
                     wy = m.cy + m.r * gy;
                     wz = m.cz + m.r * gz;
-                } else {        // closest_wall_point
-                    const double ex = x - m.cx, ey = y - m.cy, d = std::sqrt(ex * ex + ey * ey);
-                    gx = d > 0.0 ? ex / d : 1.0;
-                    gy = d > 0.0 ? ey / d : 0.0;
-                    wx = m.cx + m.r * gx;
-                    wy = m.cy + m.r * gy;
+                } else {
+                    m.closest_wall_point(x, y, wx, wy, gx, gy);
                 }
                 const double ez = m.ball ? z - wz : 0.0;
                 const double dg = std::sqrt((x - wx) * (x - wx) + (y - wy) * (y - wy) + ez * ez);
@@ -212,7 +320,7 @@ inline std::string build_ibm_geom(const IbmGeom& m, IbmTable& t) {
                 t.gnz.push_back(gz);
                 t.gwx.push_back(wx);
                 t.gwy.push_back(wy);
-                t.gwz.push_back(m.ball ? wz : z);   // (a cylinder's wall point is at the cell's z)
+                t.gwz.push_back(wz);
                 is_ghost[m.cell(i, j, k)] = 1;
             }
     for (size_t cc = 0; cc < n; ++cc)
@@ -247,21 +355,13 @@ inline void build_fresh(const IbmGeom& m, std::vector<unsigned char>& mask, cons
                 wx = m.cx + m.r * gx;
                 wy = m.cy + m.r * gy;
                 wz = m.cz + m.r * gz;
-            } else {
-                const double ex = x - m.cx, ey = y - m.cy, d = std::sqrt(ex * ex + ey * ey);
-                gx = d > 0.0 ? ex / d : 1.0;
-                gy = d > 0.0 ? ey / d : 0.0;
-                wx = m.cx + m.r * gx;
-                wy = m.cy + m.r * gy;
+            } else {   // a cylinder or a section extruded along z
+                m.closest_wall_point(x, y, wx, wy, gx, gy);
                 wz = z;
             }
             dg = std::sqrt((x - wx) * (x - wx) + (y - wy) * (y - wy) + (z - wz) * (z - wz));
-        } else {    // closest_wall_point
-            const double ex = x - m.cx, ey = y - m.cy, d = std::sqrt(ex * ex + ey * ey);
-            gx = d > 0.0 ? ex / d : 1.0;
-            gy = d > 0.0 ? ey / d : 0.0;
-            wx = m.cx + m.r * gx;
-            wy = m.cy + m.r * gy;
+        } else {
+            m.closest_wall_point(x, y, wx, wy, gx, gy);
             dg = std::hypot(x - wx, y - wy);
         }
         double wv[3];

@@ -594,6 +594,10 @@ struct fvg_run {
     } body;
     double cm0[2] = {0.0, 0.0};
     double* d_bload = nullptr;
+    // a section body: its vertices where it was placed at t = 0 (the reference the poses turn about the pivot), and how far
+    // a vertex lies from the pivot (ImmersedBoundary::enable_motion's reach)
+    std::vector<double> ref_poly;
+    double reach = 0.0;
     IbmTable tab;
     double *d_gvel = nullptr, *d_dvel = nullptr;
     // flux_quadrature = fourth: the face arrays of the face passes (fourth.cuh; one allocation, d_fourth)
@@ -690,6 +694,8 @@ std::string validate(const fvg_config& c) {
         if (c.ibm_omega_until > 0.0 && c.ibm_omega_until <= c.ibm_omega_from) return "ibm_omega_until must be later than ibm_omega_from";
         if (moving && c.ibm_curvature) return "ibm_curvature is not available for a moving body";
         if (moving && c.nz > 1 && c.ibm_shape != 1) return "a moving body in 3-D is a sphere (for now)";
+        if (c.ibm_shape == 2 && c.ibm_mass > 0.0 && c.ibm_inertia > 0.0 && !c.ibm_cm_given)
+            return "a body that translates and turns about its pivot needs the centre of mass: set ibm_cm_x and ibm_cm_y, its offset from the pivot (0 0: at the pivot)";
         if (c.nz == 1 && (c.ibm_omega_x != 0.0 || c.ibm_omega_y != 0.0)) return "ibm_omega_x and ibm_omega_y need a 3-D mesh (nz > 1)";
         if (moving && c.nz == 1 && c.ibm_vz != 0.0) return "ibm_vz needs a 3-D mesh (nz > 1)";
         // a body driven by the flow (Params.cpp:517-546)
@@ -1689,12 +1695,24 @@ void advance_body(fvg_run* r, double dt) {
 int place_body(fvg_run* r, double t) {
     const fvg_run::Pose pose = body_pose(r, t);
     const double h = r->dim == 3 ? vmin(vmin(r->m.dx, r->m.dy), r->m.dz) : vmin(r->m.dx, r->m.dy);
-    const double shift = vmax(vmax(fabs(pose.x - r->built.x), fabs(pose.y - r->built.y)), fabs(pose.z - r->built.z));
+    const bool poly = r->cfg.ibm_shape == 2;
+    const double shift = vmax(vmax(vmax(fabs(pose.x - r->built.x), fabs(pose.y - r->built.y)), fabs(pose.z - r->built.z)),
+                              poly ? fabs(pose.angle - r->built.angle) * r->reach : 0.0);
     r->pose = pose;
     if (shift <= 0.25 * h) return upload_velocities(r);
     const std::vector<unsigned char> old_mask = r->tab.mask;
     r->built = pose;
-    const IbmGeom g = ibm_geom(r->cfg, r->cfg.ibm_cx + pose.x, r->cfg.ibm_cy + pose.y, r->cfg.ibm_cz + pose.z);
+    IbmGeom g = ibm_geom(r->cfg, r->cfg.ibm_cx + pose.x, r->cfg.ibm_cy + pose.y, r->cfg.ibm_cz + pose.z);
+    if (poly) {   // the section turned about the pivot by the pose's angle and moved by its displacement
+        const double ca = std::cos(pose.angle), sa = std::sin(pose.angle), px = r->cfg.ibm_cx, py = r->cfg.ibm_cy;
+        std::vector<double> pts(r->ref_poly.size());
+        for (size_t q = 0; q < pts.size() / 2; ++q) {
+            const double rx = r->ref_poly[2 * q] - px, ry = r->ref_poly[2 * q + 1] - py;
+            pts[2 * q] = px + pose.x + ca * rx - sa * ry;
+            pts[2 * q + 1] = py + pose.y + sa * rx + ca * ry;
+        }
+        g.set_polygon(std::move(pts));
+    }
     IbmTable tb;
     const std::string msg = build_ibm_geom(g, tb);
     if (!msg.empty()) return fail(r, FVG_ERR_CONFIG, msg);
@@ -1993,6 +2011,13 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
             return bail(FVG_ERR_CONFIG);
         }
         run->ibm = true;
+        if (c.ibm_shape == 2) {   // (enable_motion: the reach of the section about the pivot)
+            std::string err;
+            run->ref_poly = place_section(c, err);
+            for (size_t q = 0; q < run->ref_poly.size() / 2; ++q)
+                run->reach = vmax(run->reach, std::hypot(run->ref_poly[2 * q] - c.ibm_cx, run->ref_poly[2 * q + 1] - c.ibm_cy));
+            run->cfg.ibm_section = nullptr;   // (the caller's memory is not kept)
+        }
         run->dynamic = c.ibm_mass > 0.0 || c.ibm_inertia > 0.0;
         run->moving = run->dynamic || c.ibm_vx != 0.0 || c.ibm_vy != 0.0 || c.ibm_vz != 0.0 || c.ibm_omega != 0.0 || c.ibm_omega_x != 0.0 ||
                       c.ibm_omega_y != 0.0;
@@ -2007,8 +2032,8 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
                 run->body.omx = c.ibm_omega_x;
                 run->body.omy = c.ibm_omega_y;
             }
-            if (c.ibm_cm_x != 0.0 || c.ibm_cm_y != 0.0) {   // body frame to mesh axes (a circle is placed unturned)
-                const double ca = std::cos(0.0), sa = std::sin(0.0);
+            if (c.ibm_cm_x != 0.0 || c.ibm_cm_y != 0.0) {   // body frame to mesh axes: a section is placed turned by ibm_aoa, nose up
+                const double a = c.ibm_shape == 2 ? c.ibm_aoa * std::acos(-1.0) / 180.0 : 0.0, ca = std::cos(a), sa = std::sin(a);
                 run->cm0[0] = c.ibm_cm_x * ca + c.ibm_cm_y * sa;
                 run->cm0[1] = -c.ibm_cm_x * sa + c.ibm_cm_y * ca;
             }
@@ -2185,7 +2210,11 @@ static int run_steps(fvg_run* run, double t_end, int max_steps, int use_graph, i
             const double wv[3] = {run->dynamic ? run->body.u : c.ibm_vx, run->dynamic ? run->body.v : c.ibm_vy, run->dynamic ? run->body.w : c.ibm_vz};
             double travel = h2.dt * vmax(fabs(wv[0]) / run->m.dx, fabs(wv[1]) / run->m.dy);
             if (run->dim == 3) travel = vmax(travel, h2.dt * fabs(wv[2]) / run->m.dz);
-            if (travel > 1.0) {   // (a circle or a sphere reaches no farther by turning: its rotation adds nothing here)
+            if (c.ibm_inertia > 0.0) {   // a driven rotation: how far the section's farthest vertex moves (0 for a circle or sphere)
+                const double turn = h2.dt * fabs(run->body.om) * run->reach / vmin(run->m.dx, run->m.dy);
+                travel = (c.ibm_cm_x != 0.0 || c.ibm_cm_y != 0.0) ? travel + turn : vmax(travel, turn);
+            }
+            if (travel > 1.0) {
                 if (steps) *steps = h2.steps;
                 return fail(run, FVG_ERR_DIVERGED, "the moving body travelled more than one cell in a step (lower the CFL number)");
             }
@@ -2525,7 +2554,7 @@ int fvg_ibm_loads(fvg_run* run, double* loads) {
     CK(cudaStreamSynchronize(run->stream));
     // the monitor's coefficients (cpp/src/SimulationRun.cpp:94-103): on q A, A = the diameter (2-D, per unit depth), pi r^2
     // (sphere) or diameter x Lz (3-D cylinder); Cm about (ibm_cx, ibm_cy), nose-up positive
-    const double L = 2.0 * c.ibm_radius;
+    const double L = c.ibm_shape == 2 ? c.ibm_chord : 2.0 * c.ibm_radius;   // the chord of a section, else the diameter
     const double A = run->dim == 2 ? L : (c.ibm_shape == 1 ? 3.14159265358979323846 * c.ibm_radius * c.ibm_radius : L * c.Lz);
     const double qA = 0.5 * c.rho_in * c.u_in * c.u_in * A;
     loads[0] = h[0];

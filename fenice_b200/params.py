@@ -11,6 +11,8 @@ as the reference raises std::invalid_argument. ``time_scheme = "auto"`` resolves
 import ctypes
 import tomllib
 
+from . import airfoil
+
 DEFAULTS = {
     "Lx": 1.0, "Ly": 1.0, "Lz": 1.0, "nx": 100, "ny": 100, "nz": 1,
     "eos_type": "Ideal Gas", "gamma": 1.4, "p_inf": 0.0,
@@ -63,7 +65,9 @@ class FvgConfig(ctypes.Structure):
                 ("ibm_stiff_x", ctypes.c_double), ("ibm_stiff_y", ctypes.c_double), ("ibm_stiff_z", ctypes.c_double),
                 ("ibm_damp_x", ctypes.c_double), ("ibm_damp_y", ctypes.c_double), ("ibm_damp_z", ctypes.c_double),
                 ("ibm_stiff_theta", ctypes.c_double), ("ibm_damp_theta", ctypes.c_double),
-                ("ibm_cm_x", ctypes.c_double), ("ibm_cm_y", ctypes.c_double), ("ibm_cm_given", ctypes.c_int)]
+                ("ibm_cm_x", ctypes.c_double), ("ibm_cm_y", ctypes.c_double), ("ibm_cm_given", ctypes.c_int),
+                ("ibm_section", ctypes.POINTER(ctypes.c_double)), ("ibm_section_points", ctypes.c_int),
+                ("ibm_chord", ctypes.c_double), ("ibm_aoa", ctypes.c_double)]
 
 BODY_KEYS = ("ibm_vx", "ibm_vy", "ibm_vz", "ibm_omega", "ibm_omega_x", "ibm_omega_y", "ibm_omega_from", "ibm_omega_until", "ibm_mass",
              "ibm_inertia", "ibm_stiff_x", "ibm_stiff_y", "ibm_stiff_z", "ibm_damp_x", "ibm_damp_y", "ibm_damp_z", "ibm_stiff_theta",
@@ -239,9 +243,23 @@ def to_config(params, precision=0, device=0):
     c.device = int(device)
     c.use_ibm = 1 if _flag(p["use_ibm"]) else 0
     shape = str(p["ibm_shape"]).strip().lower()
-    if c.use_ibm and shape not in ("cylinder", "sphere"):
-        raise ValueError(f"Unknown IBM shape: '{p['ibm_shape']}' (the device path supports Cylinder and Sphere)")
-    c.ibm_shape = 1 if shape == "sphere" else 0
+    digits = airfoil.naca_digits(p["ibm_shape"])
+    if shape not in ("cylinder", "sphere", "airfoil") and not digits:   # Params.cpp:497-501
+        raise ValueError(f"Unknown ibm_shape: '{p['ibm_shape']}' (use Cylinder, Sphere, Airfoil or NACA dddd)")
+    c.ibm_shape = 1 if shape == "sphere" else (2 if (shape == "airfoil" or digits) else 0)
+    c.ibm_chord, c.ibm_aoa = float(p.get("ibm_chord", 1.0)), float(p.get("ibm_aoa", 0.0))
+    if c.use_ibm and c.ibm_shape == 2:   # the unit section: a NACA 4-digit one, or a coordinate file (ibm_file)
+        if digits:
+            section = airfoil.naca4(digits)
+        else:
+            path = str(p.get("ibm_file", "") or "").strip()
+            if not path:
+                raise ValueError("ibm_shape = Airfoil needs ibm_file (a Selig or Lednicer coordinate file)")
+            section = airfoil.load_airfoil(path)
+        arr = (ctypes.c_double * (2 * len(section)))(*[v for q in section for v in q])
+        c._section = arr
+        c.ibm_section = ctypes.cast(arr, ctypes.POINTER(ctypes.c_double))
+        c.ibm_section_points = len(section)
     c.ibm_radius, c.ibm_cx, c.ibm_cy, c.ibm_cz = float(p["ibm_radius"]), float(p["ibm_cx"]), float(p["ibm_cy"]), float(p["ibm_cz"])
     c.ibm_curvature = 1 if _flag(p["ibm_curvature"]) else 0
     c.use_bodyforce = 1 if _flag(p["use_bodyforce"]) else 0
@@ -282,7 +300,7 @@ def load_case(path, overrides=None):
     import os
 
     for k, v in list(params.items()):
-        if k.endswith("_table") and isinstance(v, str) and v.strip() and not os.path.isabs(v.strip()):
+        if (k.endswith("_table") or k == "ibm_file") and isinstance(v, str) and v.strip() and not os.path.isabs(v.strip()):
             beside = os.path.join(os.path.dirname(os.path.abspath(path)), v.strip())
             if os.path.exists(beside):
                 params[k] = beside

@@ -39,7 +39,7 @@ EXPORTS = ["fvg_abi_version", "fvg_create", "fvg_destroy", "fvg_last_error", "fv
            "fvg_expr_eval"]
 
 _lib = None
-ABI_VERSION = 8   # FVG_ABI_VERSION of include/fenice_gpu.h
+ABI_VERSION = 9   # FVG_ABI_VERSION of include/fenice_gpu.h
 
 
 def load_library(path=LIB_PATH):

@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define FVG_ABI_VERSION 8
+#define FVG_ABI_VERSION 9
 
 /* status codes */
 enum {
@@ -72,7 +72,8 @@ typedef struct fvg_config {
     int precision;               /* FVG_PREC_FP64: the reference's arithmetic, bit for bit; FVG_PREC_MIXED: FP32 stencil */
     int device;                  /* CUDA device ordinal */
     int use_ibm;                 /* [ibm] use_ibm: a static immersed body with the sharp ghost-cell wall (slip when inviscid) */
-    int ibm_shape;               /* [ibm] ibm_shape: 0 Cylinder (a circle in 2-D, infinite along z in 3-D), 1 Sphere (3-D) */
+    int ibm_shape;               /* [ibm] ibm_shape: 0 Cylinder (a circle in 2-D, infinite along z in 3-D), 1 Sphere (3-D),
+                                    2 a section (NACAxxxx / airfoil: ibm_section below; extruded along z in 3-D) */
     double ibm_radius, ibm_cx, ibm_cy, ibm_cz; /* [ibm] */
     int ibm_curvature;           /* [ibm] ibm_curvature (must be 0 on the device) */
     int use_bodyforce;           /* [physics] use_bodyforce: the constant body force (ConstantBodyForce, Physics.cpp:832-844) */
@@ -115,6 +116,12 @@ typedef struct fvg_config {
     double ibm_stiff_x, ibm_stiff_y, ibm_stiff_z, ibm_damp_x, ibm_damp_y, ibm_damp_z, ibm_stiff_theta, ibm_damp_theta;
     double ibm_cm_x, ibm_cm_y;
     int ibm_cm_given;
+    /* [ibm] a section body (ibm_shape 2): the unit section's vertices (x, y pairs: leading edge at the origin, chord 1 along
+     * x, as naca4 / load_airfoil give it, cpp/src/Geometry.cpp:40-141), placed by place_airfoil with its quarter chord at
+     * (ibm_cx, ibm_cy), scaled to ibm_chord and turned by ibm_aoa degrees, nose up */
+    const double* ibm_section;
+    int ibm_section_points;
+    double ibm_chord, ibm_aoa;
 } fvg_config;
 
 typedef struct fvg_run fvg_run;

@@ -6,7 +6,8 @@ Each case is a case file of ours run by the reference's command-line solver (ora
 places the body at the start of every step, rebuilds its ghost table when it has moved a quarter cell, fills the cells it
 left and checks how far it travelled) for a number of steps, with `dump_state` for the final state. The initial state is
 the reference's own set-up of the same case (oracle/ref/ref_harness.cpp, `case` key). A case whose body travels more
-than a cell in a step records the reference's error. tests/golden/moving.npz is test data: nothing of the product reads it.
+than a cell in a step records the reference's error. A section read from a file refers to it as "@section.dat" (its text is
+stored in the fixture). tests/golden/moving.npz is test data: nothing of the product reads it.
 """
 import json
 import os
@@ -58,6 +59,29 @@ state = { rho = 1.0, u = 0.0, v = 0.05, w = 0.0, p = "1.0 + 0.2*x + 0.1*z" }
 """
 
 IBM = dict(use_ibm="true", ibm_shape="Cylinder")
+
+STREAM2D = """[case]
+name = "airfoil in a stream"
+description = "a section in a uniform stream"
+
+[initial]
+state = { rho = 1.0, u = 0.5, v = 0.0, p = 1.0 }
+"""
+
+STREAM3D = """[case]
+name = "extruded airfoil"
+description = "an extruded section in a uniform stream"
+requires_3d = true
+
+[initial]
+state = { rho = 1.0, u = 0.5, v = 0.0, w = 0.0, p = 1.0 }
+"""
+
+# a Selig file of our own: a diamond section with a rounded nose, for the file reader (name line, then x y rows)
+SECTION_FILE = "diamond-ish section\n" + "\n".join(f"{x:.6f} {y:.6f}" for x, y in (
+    (1.0, 0.0), (0.75, 0.03), (0.5, 0.06), (0.25, 0.05), (0.1, 0.035), (0.03, 0.02), (0.0, 0.0), (0.03, -0.02), (0.1, -0.035), (0.25, -0.05),
+    (0.5, -0.06), (0.75, -0.03), (1.0, 0.0))) + "\n"
+INLET = dict(bc_xmin="vel_inlet", bc_xmax="outlet", bc_ymin="transmissive", bc_ymax="transmissive", u_in=0.5, rho_in=1.0, p_out=1.0)
 
 CASES = {
     "circle_translating_rk2_2d": (FLOW2D, dict(nx=60, ny=40, Lx=3.0, Ly=2.0, reconstruction="muscl", muscl_limiter="Van Leer",
@@ -112,6 +136,25 @@ CASES = {
                                              bc_xmin="wall", bc_xmax="wall", bc_ymin="periodic", bc_ymax="periodic", bc_zmin="wall", bc_zmax="wall",
                                              ibm_shape="Sphere", use_ibm="true", ibm_radius=0.2, ibm_cx=0.5, ibm_cy=0.5, ibm_cz=0.55, ibm_mass=0.05,
                                              use_bodyforce="true", gx=0.1, gy=0.0, gz=-1.5, cfl=0.5), 12),
+    # sections: NACA 4-digit and a coordinate file, static, pitching, flutter-like, extruded
+    "naca0012_static_rk2_2d": (STREAM2D, dict(nx=64, ny=48, Lx=2.0, Ly=1.5, reconstruction="muscl", muscl_limiter="Van Leer",
+                                              time_scheme="SSP Runge-Kutta 2", use_ibm="true", ibm_shape="NACA 0012", ibm_chord=0.8, ibm_aoa=5.0,
+                                              ibm_cx=0.8, ibm_cy=0.75, cfl=0.5, **INLET), 30),
+    "naca2412_pitching_viscous_2d": (STREAM2D, dict(nx=60, ny=50, Lx=1.5, Ly=1.25, reconstruction="muscl", muscl_limiter="MC",
+                                                    time_scheme="SSP Runge-Kutta 2", use_viscous="true", mu=0.005, use_ibm="true",
+                                                    ibm_shape="NACA2412", ibm_chord=0.6, ibm_aoa=-3.0, ibm_cx=0.6, ibm_cy=0.62, ibm_omega=2.0,
+                                                    cfl=0.4, **INLET), 30),
+    "section_file_hancock_2d": (STREAM2D, dict(nx=56, ny=40, Lx=1.4, Ly=1.0, reconstruction="muscl", muscl_limiter="MC", time_scheme="MUSCL-Hancock",
+                                               use_ibm="true", ibm_shape="Airfoil", ibm_file="@section.dat", ibm_chord=0.7, ibm_aoa=8.0,
+                                               ibm_cx=0.55, ibm_cy=0.5, cfl=0.5, **INLET), 25),
+    "naca0015_free_pitch_heave_2d": (STREAM2D, dict(nx=60, ny=48, Lx=1.5, Ly=1.2, reconstruction="muscl", muscl_limiter="Van Leer",
+                                                    time_scheme="SSP Runge-Kutta 2", use_viscous="true", mu=0.005, use_ibm="true",
+                                                    ibm_shape="NACA 0015", ibm_chord=0.5, ibm_aoa=6.0, ibm_cx=0.6, ibm_cy=0.6, ibm_mass=0.05,
+                                                    ibm_inertia=0.002, ibm_cm_x=0.05, ibm_cm_y=0.0, ibm_stiff_y=2.0, ibm_stiff_theta=0.05,
+                                                    cfl=0.4, **INLET), 30),
+    "naca0012_extruded_weno5_3d": (STREAM3D, dict(nx=40, ny=32, nz=4, Lx=1.6, Ly=1.2, Lz=0.2, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3",
+                                                  use_ibm="true", ibm_shape="NACA 0012", ibm_chord=0.6, ibm_aoa=4.0, ibm_cx=0.6, ibm_cy=0.6,
+                                                  bc_zmin="periodic", bc_zmax="periodic", cfl=0.5, **INLET), 8),
     # the body outruns the ghost table: the reference stops
     "circle_too_fast_2d": (FLOW2D, dict(nx=30, ny=20, Lx=3.0, Ly=2.0, reconstruction="muscl", time_scheme="SSP Runge-Kutta 2",
                                         bc_xmin="transmissive", bc_xmax="transmissive", bc_ymin="wall", bc_ymax="wall", ibm_radius=0.3,
@@ -122,7 +165,11 @@ CASES = {
 def main():
     out = {}
     tmp = tempfile.mkdtemp(prefix="fvg_moving_")
+    section = os.path.join(tmp, "section.dat")
+    with open(section, "w") as f:
+        f.write(SECTION_FILE)
     for name, (text, params, nsteps) in CASES.items():
+        params = {k: (section if v == "@section.dat" else v) for k, v in params.items()}
         case = os.path.join(tmp, name)
         os.makedirs(case)
         path = os.path.join(case, "case.toml")
@@ -133,7 +180,8 @@ def main():
         sets = dict(params, t_end=1e9, max_steps=nsteps, save_interval=1000000000, output_root=os.path.join(case, "out"), dump_state=dump)
         cmd = [FENICE, "--case", path, "--no-logo", "--threads", "4"] + sum([["--set", f"{k}={v}"] for k, v in sets.items()], [])
         r = subprocess.run(cmd, capture_output=True, text=True)
-        out[f"{name}/params"] = np.array(json.dumps(dict(params, t_end=1e9)))
+        stored = {k: ("@section.dat" if v == section else v) for k, v in dict(params, t_end=1e9).items()}
+        out[f"{name}/params"] = np.array(json.dumps(stored))
         out[f"{name}/U0"] = U0
         out[f"{name}/steps"] = np.array(nsteps)
         if r.returncode != 0:
@@ -146,6 +194,7 @@ def main():
             out[f"{name}/t"] = np.array(float(z["t"]))
             out[f"{name}/step"] = np.array(int(z["step"]))
             print(f"{name}: {int(z['step'])} steps to t = {float(z['t']):.6g}")
+    out["file/section.dat"] = np.array(SECTION_FILE)
     np.savez_compressed(os.path.join(HERE, "moving.npz"), **out)
 
 

@@ -26,7 +26,7 @@ def test_library_exports_every_declared_entry_point():
     for n in names:
         assert hasattr(lib, n), n
     assert set(names) == set(RT.EXPORTS)
-    assert lib.fvg_abi_version() == 8
+    assert lib.fvg_abi_version() == 9
 
 
 def create_code(params):
