@@ -57,6 +57,7 @@ __device__ __forceinline__ void batch_item_args(const BatchArgs& b, const BatchP
     sa.shock_blend = pr.shock_blend;
     sa.weno_eps = pr.weno_eps;
     sa.limiter = pr.limiter;
+    sa.b0 = 0;
     sa.mode = b.mode;
     sa.ca = b.ca;
     sa.cb = b.cb;

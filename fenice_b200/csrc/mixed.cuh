@@ -102,7 +102,7 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
         __syncthreads();
         const int sstride = axis == 0 ? 1 : (axis == 1 ? E[0] : E[0] * E[1]);
         bool tile_linear = false;
-        if constexpr (GATED) tile_linear = a.sens_flags[AXIS * a.tiles[0] * a.tiles[1] * a.tiles[2] + blockIdx.x] == 0;
+        if constexpr (GATED) tile_linear = a.sens_flags[AXIS * a.tiles[0] * a.tiles[1] * a.tiles[2] + blockIdx.x + a.b0] == 0;
         // ---- 2. face values
         for (int it = tid; it < nF * NV; it += NT) {
             const int f = it % nF, q = it / nF;
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(NT) mixed_stage_kernel(const StageArgs a) {
     const Mesh& m = a.m;
     const Eos<float> ef{a.eos.type, (float)a.eos.gamma, (float)a.eos.p_inf};
     const float sb = (float)a.shock_blend, weps = (float)a.weno_eps;
-    const int tid = threadIdx.x, b = blockIdx.x;
+    const int tid = threadIdx.x, b = blockIdx.x + a.b0;
     const int o3[3] = {(b % a.tiles[0]) * TX, ((b / a.tiles[0]) % a.tiles[1]) * TY, (b / (a.tiles[0] * a.tiles[1])) * TZ};
     float smax = 0.0f;
     mixed_axis<0, DIM, RECON, RIEMANN, TX, TY, TZ, NT, GATED, FULL>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax);
@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
     float* acc = Fv + 4 * S::NF;                         // [4][NC]: rho u, rho v, rho E, rho w
     if (!*a.gate) return;
     const Mesh& m = a.m;
-    const int tid = threadIdx.x, b = blockIdx.x;
+    const int tid = threadIdx.x, b = blockIdx.x + a.b0;
     const int o3[3] = {(b % a.tiles[0]) * TX, ((b / a.tiles[0]) % a.tiles[1]) * TY, (b / (a.tiles[0] * a.tiles[1])) * TZ};
     const int n3[3] = {m.nx, m.ny, m.nz};
     const float h[3] = {(float)m.dx, (float)m.dy, (float)m.dz};

@@ -604,6 +604,11 @@ struct fvg_run {
     bool fourth = false;
     FourthArgs fa{};
     void* d_fourth = nullptr;
+    // fvg_step_host: the copy stream, the events of the slabs' uploads and downloads, and the steps it took with the
+    // sensor on (the sensor's refresh cadence across calls)
+    cudaStream_t xfer = nullptr;
+    std::vector<cudaEvent_t> ev_host;
+    long long host_steps = 0;
     double res_time = NAN;   // fvg_set_stage_time (NaN: the run's time)
     int res_kind = -1;       // the stage-time kind residual_stage takes (-1: its stage index)
     double* Ucur() { return cur ? Ut : U; }
@@ -2090,6 +2095,8 @@ int fvg_destroy(fvg_run* run) {
                     (void*)run->d_ratio, (void*)run->d_gn, (void*)run->d_deep, (void*)run->d_solid, (void*)run->d_loads, (void*)run->d_gvel,
                     (void*)run->d_dvel, (void*)run->d_bload, (void*)run->d_span})
         if (p) cudaFree(p);
+    for (cudaEvent_t e : run->ev_host) cudaEventDestroy(e);
+    if (run->xfer) cudaStreamDestroy(run->xfer);
     if (run->stream) cudaStreamDestroy(run->stream);
     delete run;
     return FVG_OK;
@@ -2178,6 +2185,23 @@ int fvg_residual(fvg_run* run, double predictor_half_dt, double* R, size_t ncell
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(R, run->staging, sizeof(double) * 5 * ncells, cudaMemcpyDeviceToHost, run->stream));
         CK(cudaStreamSynchronize(run->stream));
+    }
+    return FVG_OK;
+}
+
+// The control block's verdict after `done` steps: a time-dependent boundary value out of range, or a diverged step.
+static int ctl_status(fvg_run* run, const Ctl& h, int done) {
+    if (h.status == 3) {
+        char msg[256];
+        std::snprintf(msg, sizeof msg, "time-dependent boundary values: not finite, or rho_in or p_out not positive, at t = %.17g (step %d)", h.stage_t,
+                      done + 1);
+        return fail(run, FVG_ERR_BOUNDARY, msg);
+    }
+    if (h.status) {
+        char msg[256];
+        std::snprintf(msg, sizeof msg, "the solution diverged at step %d (t = %.6g, dt = %.3g, largest wave speed = %.3g)", done + 1, h.t, h.dt,
+                      h.s_step);
+        return fail(run, FVG_ERR_DIVERGED, msg);
     }
     return FVG_OK;
 }
@@ -2292,19 +2316,7 @@ static int run_steps(fvg_run* run, double t_end, int max_steps, int use_graph, i
         if (hancock && (done & 1)) run->cur ^= 1;
     }
     if (steps) *steps = done;
-    if (h.status == 3) {
-        char msg[256];
-        std::snprintf(msg, sizeof msg, "time-dependent boundary values: not finite, or rho_in or p_out not positive, at t = %.17g (step %d)", h.stage_t,
-                      done + 1);
-        return fail(run, FVG_ERR_BOUNDARY, msg);
-    }
-    if (h.status) {
-        char msg[256];
-        std::snprintf(msg, sizeof msg, "the solution diverged at step %d (t = %.6g, dt = %.3g, largest wave speed = %.3g)", done + 1, h.t, h.dt,
-                      h.s_step);
-        return fail(run, FVG_ERR_DIVERGED, msg);
-    }
-    return FVG_OK;
+    return ctl_status(run, h, done);
 }
 
 int fvg_step(fvg_run* run, double t_end, double* dt, double* smax) {
@@ -2325,6 +2337,229 @@ int fvg_run_until(fvg_run* run, double t_end, int max_steps, int* steps) {
     if (!run) return FVG_ERR_ARGUMENT;
     if (run->is_part) return fail(run, FVG_ERR_CONFIG, "a part of a decomposed mesh steps through fvg_part_phase");
     return run_steps(run, t_end, max_steps, 1, steps);
+}
+
+// ---- one step of a state held in host memory (fvg_step_host)
+//
+// The state crosses the host link in slabs of planes along the slowest axis (z in 3-D, y in 2-D) on a copy stream. The
+// first stage runs tile plane by tile plane as soon as the slabs its cells and their halo read have arrived; the last stage
+// runs slab by slab and each finished slab is read back while the next is computed. The launches are those of fvg_step
+// (same kernels, same arguments, each over a range of tiles), so the result is bit-identical to upload + fvg_step +
+// download.
+
+namespace {
+
+constexpr int kHostSlabs = 16;   // slabs of the state per step at most (events: one per slab and direction)
+constexpr int kHostHalo = 3;     // the deepest read beyond a tile along the split axis (WENO5-Z); the viscous sweep reads 1-2
+
+struct HostSlabs {
+    int ax = 2, N = 1;     // the split axis and its cells
+    long long pc = 1;      // cells of one plane across it (the slab of planes [a, b) is cells [a pc, b pc))
+    int planes = 1, n = 1; // planes per slab, slabs
+    bool periodic = false;
+    int ord[kHostSlabs] = {}, pos[kHostSlabs] = {};   // upload order, and each slab's place in it
+};
+
+HostSlabs host_slabs(const fvg_run* r) {
+    HostSlabs s;
+    s.ax = r->dim == 3 ? 2 : 1;
+    s.N = s.ax == 2 ? r->m.nz : r->m.ny;
+    s.pc = s.ax == 2 ? (long long)r->m.nx * r->m.ny : r->m.nx;
+    const int align = r->dim == 3 ? Tile<3>::Z : 1;
+    s.planes = (s.N + kHostSlabs - 1) / kHostSlabs;
+    s.planes = std::max(8, (s.planes + align - 1) / align * align);
+    s.n = (s.N + s.planes - 1) / s.planes;
+    s.periodic = r->cfg.bc[2 * s.ax] == FVG_BC_PERIODIC && r->cfg.bc[2 * s.ax + 1] == FVG_BC_PERIODIC;
+    // a periodic axis: the last slab first, so that the first tile plane (which wraps onto it) can start early
+    for (int p = 0; p < s.n; ++p) s.ord[p] = s.periodic && s.n > 1 ? (p + s.n - 1) % s.n : p;
+    for (int p = 0; p < s.n; ++p) s.pos[s.ord[p]] = p;
+    return s;
+}
+
+// The upload place after which tile plane j of a kernel with tiles T planes high has every cell it reads: planes
+// [jT - H, (j + 1) T + H), wrapped on a periodic axis, else clamped to the mesh (ghost slabs mirror cells inside it).
+int slab_need(const HostSlabs& s, int T, int j) {
+    int p = 0;
+    for (int y = j * T - kHostHalo; y < std::min((j + 1) * T, s.N) + kHostHalo; ++y) {
+        const int yy = s.periodic ? ((y % s.N) + s.N) % s.N : std::min(std::max(y, 0), s.N - 1);
+        p = std::max(p, s.pos[yy / s.planes]);
+    }
+    return p;
+}
+
+// Runs whose residual reads only cells near each tile: no immersed body (its image points), mass-flow inlet (a whole-side
+// sum), positivity fallback (repeats), fourth-order quadrature (face passes); Runge-Kutta and Euler steps.
+bool host_pipelined(const fvg_run* r) {
+    const int ts = r->cfg.time_scheme;
+    return (ts == FVG_TS_EULER || ts == FVG_TS_SSPRK2 || ts == FVG_TS_SSPRK3) && !r->fb_flags && !r->ibm && !r->moving && !r->fourth && !r->is_part &&
+           !r->d_utarget;
+}
+
+}   // namespace
+
+int fvg_step_host(fvg_run* run, const double* U_in, double* U_out, size_t ncells, double t_end, double* dt, double* smax) {
+    if (!run || !U_in || !U_out) return FVG_ERR_ARGUMENT;
+    if (run->is_part) return fail(run, FVG_ERR_CONFIG, "a part of a decomposed mesh steps through fvg_part_phase");
+    if ((long long)ncells != run->m.ncells) return fail(run, FVG_ERR_ARGUMENT, "ncells is not the mesh's");
+    if (!host_pipelined(run)) {   // the same three calls without the overlap
+        int rc = fvg_upload_state(run, U_in, ncells);
+        if (!rc) rc = fvg_step(run, t_end, dt, smax);
+        if (!rc) rc = fvg_download_state(run, U_out, ncells);
+        return rc;
+    }
+    CK(cudaSetDevice(run->cfg.device));
+    int rc = ensure_staging(run);
+    if (rc) return rc;
+    if (!run->xfer) CK(cudaStreamCreateWithFlags(&run->xfer, cudaStreamNonBlocking));
+    if (run->ev_host.empty()) {
+        run->ev_host.resize(2 * kHostSlabs + 1);
+        for (cudaEvent_t& e : run->ev_host) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    cudaEvent_t *ev_up = run->ev_host.data(), *ev_down = ev_up + kHostSlabs, ev_start = ev_up[2 * kHostSlabs];
+    const HostSlabs s = host_slabs(run);
+    cudaStream_t cs = run->stream, xs = run->xfer;
+    Ctl* c = run->ctl;
+    const int* act = &c->active;
+    const long long pl = run->m.plane;
+    const int nv = run->nvar, dim = run->dim, ts = run->cfg.time_scheme;
+    const bool visc = run->cfg.use_viscous;
+    const int nbv = visc ? run->nbv : 0;
+    // the two kernels of a residual, by tile plane along the split axis
+    const int Ts = dim == 3 ? Tile<3>::Z : Tile<2>::Y, Tv = dim == 3 ? 8 : kVisc2T;
+    const int ns = run->tiles[s.ax], nsv = run->ntiles_v[s.ax];
+    const int Ps = run->nb / ns, Pv = run->nbv / nsv;
+    auto visc_planes = [&](const double* Uv, double* bmv, int j0, int j1) -> cudaError_t {
+        if (!visc || j1 <= j0) return cudaSuccess;
+        ViscArgs a = visc_args(run, Uv, bmv, act);
+        a.b0 = j0 * Pv;
+        const int nblk = (j1 - j0) * Pv;
+        return dim == 2 ? launch_viscous2d(a, nblk, cs) : run->cfg.precision == FVG_PREC_MIXED ? mixed_viscous_launch(a, nblk, cs) : launch_viscous(a, nblk, cs);
+    };
+    auto stage_planes = [&](StageArgs sa, int j0, int j1) -> cudaError_t {
+        if (j1 <= j0) return cudaSuccess;
+        sa.b0 = j0 * Ps;
+        return run->stage.launch(sa, (j1 - j0) * Ps, cs);
+    };
+    auto slab_cells = [&](int k, long long* c0, long long* cn) {
+        *c0 = (long long)k * s.planes * s.pc;
+        *cn = (long long)(std::min((k + 1) * s.planes, s.N) - k * s.planes) * s.pc;
+    };
+    auto flat_blocks = [](long long n) { return (int)std::min<long long>((n + 255) / 256, 148 * 16); };
+#define CKL(call)                                                                                   \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) return fail(run, FVG_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+    // ---- the upload overlapped with the first stage
+    int* bad = reinterpret_cast<int*>(run->bm_seed);   // a 2-D mesh given rho w != 0
+    CK(cudaMemsetAsync(bad, 0, sizeof(int), cs));
+    k_begin<<<1, 1, 0, cs>>>(c, t_end, 1);
+    CKL(cudaGetLastError());
+    CK(cudaEventRecord(ev_start, cs));   // the staging buffer is free once the run's earlier work is done
+    CK(cudaStreamWaitEvent(xs, ev_start, 0));
+    run->cur = 0;
+    // the sensor refreshes its gate every sens_every steps of these calls, from the whole state
+    const bool refresh = run->sens && run->host_steps % run->sens_every == 0;
+    std::vector<int> need_v(nsv), need_s(ns);
+    for (int j = 0; j < nsv; ++j) need_v[j] = refresh ? s.n - 1 : slab_need(s, Tv, j);
+    for (int j = 0; j < ns; ++j) {
+        int p = refresh ? s.n - 1 : slab_need(s, Ts, j);
+        if (visc)   // and the viscous tile planes of its cells
+            for (int v = j * Ts / Tv; v <= (std::min((j + 1) * Ts, s.N) - 1) / Tv; ++v) p = std::max(p, need_v[v]);
+        need_s[j] = p;
+    }
+    CKL(stage_values(run, run->res_kind >= 0 ? run->res_kind : 0, act));
+    const StageArgs sa1 = stage_args(run, run->U, nullptr, run->R, kStoreR, 0, 0, visc ? run->Rv : nullptr, run->bm[0], act);
+    for (int p = 0; p < s.n; ++p) {
+        long long c0, cn;
+        slab_cells(s.ord[p], &c0, &cn);
+        CK(cudaMemcpyAsync(run->staging + 5 * c0, U_in + 5 * c0, sizeof(double) * 5 * cn, cudaMemcpyHostToDevice, xs));
+        CK(cudaEventRecord(ev_up[p], xs));
+        CK(cudaStreamWaitEvent(cs, ev_up[p], 0));
+        k_aos_to_planes<<<flat_blocks(cn), 256, 0, cs>>>(run->staging + 5 * c0, run->U + c0, pl, cn, nv, bad);
+        CKL(cudaGetLastError());
+        if (refresh && p == s.n - 1) CKL(refresh_gate(run, run->U, nullptr));
+        // the tile planes whose reads are complete now, in runs of consecutive planes
+        for (int pass = 0; pass < 2; ++pass) {
+            const std::vector<int>& need = pass ? need_s : need_v;
+            for (int j = 0; j < (int)need.size();) {
+                if (need[j] != p) {
+                    ++j;
+                    continue;
+                }
+                int k = j;
+                while (k < (int)need.size() && need[k] == p) ++k;
+                CKL(pass ? stage_planes(sa1, j, k) : visc_planes(run->U, run->bmv[0], j, k));
+                j = k;
+            }
+        }
+    }
+    k_stage1_dt<<<1, 1024, 0, cs>>>(c, run->bm[0], run->nb, run->bmv[0], nbv);
+    CKL(cudaGetLastError());
+
+    // ---- the middle stages, then the last stage overlapped with the download
+    auto download = [&](int k) -> int {
+        long long c0, cn;
+        slab_cells(k, &c0, &cn);
+        k_planes_to_aos<<<flat_blocks(cn), 256, 0, cs>>>(run->U + c0, run->staging + 5 * c0, pl, cn, nv);
+        CKL(cudaGetLastError());
+        CK(cudaEventRecord(ev_down[k], cs));
+        CK(cudaStreamWaitEvent(xs, ev_down[k], 0));
+        CK(cudaMemcpyAsync(U_out + 5 * c0, run->staging + 5 * c0, sizeof(double) * 5 * cn, cudaMemcpyDeviceToHost, xs));
+        return FVG_OK;
+    };
+    if (ts == FVG_TS_EULER) {
+        k_axpy<<<axpy_blocks(run), 256, 0, cs>>>(c, run->U, run->U, run->R, pl, run->m.ncells, nv);
+        k_end_rk<<<1, 1, 0, cs>>>(c, 1);
+        CKL(cudaGetLastError());
+        for (int k = 0; k < s.n; ++k)
+            if ((rc = download(k))) return rc;
+    } else {
+        k_axpy<<<axpy_blocks(run), 256, 0, cs>>>(c, run->Ut, run->U, run->R, pl, run->m.ncells, nv);
+        CKL(cudaGetLastError());
+        const double* Ulast = run->Ut;
+        double ca = 0.5, cb = 0.5;
+        int st = 1;
+        if (ts == FVG_TS_SSPRK3) {
+            CKL(stage_values(run, run->res_kind >= 0 ? run->res_kind : 1, act));
+            CKL(visc_planes(run->Ut, run->bmv[1], 0, nsv));
+            CKL(stage_planes(stage_args(run, run->Ut, run->U, run->R, kCombine, 0.75, 0.25, visc ? run->Rv : nullptr, run->bm[1], act), 0, ns));
+            k_stage_max<<<1, 1024, 0, cs>>>(c, act, 1, run->bm[1], run->nb, run->bmv[1], nbv);
+            CKL(cudaGetLastError());
+            Ulast = run->R;
+            ca = 1.0 / 3.0;
+            cb = 2.0 / 3.0;
+            st = 2;
+        }
+        CKL(stage_values(run, run->res_kind >= 0 ? run->res_kind : st, act));
+        const StageArgs sa = stage_args(run, Ulast, run->U, run->U, kCombine, ca, cb, visc ? run->Rv : nullptr, run->bm[st], act);
+        int jv = 0, js = 0;
+        for (int k = 0; k < s.n; ++k) {
+            // every tile plane with a cell in slabs 0 .. k, and the viscous tile planes of their cells
+            const int js_end = (std::min((k + 1) * s.planes, s.N) + Ts - 1) / Ts;
+            const int jv_end = (std::min(js_end * Ts, s.N) + Tv - 1) / Tv;
+            CKL(visc_planes(Ulast, run->bmv[st], jv, jv_end));
+            CKL(stage_planes(sa, js, js_end));
+            jv = std::max(jv, jv_end);
+            js = std::max(js, js_end);
+            if ((rc = download(k))) return rc;
+        }
+        k_stage_max<<<1, 1024, 0, cs>>>(c, act, st, run->bm[st], run->nb, run->bmv[st], nbv);
+        k_end_rk<<<1, 1, 0, cs>>>(c, ts == FVG_TS_SSPRK2 ? 2 : 3);
+        CKL(cudaGetLastError());
+    }
+#undef CKL
+    int hbad = 0;
+    CK(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, cs));
+    CK(cudaStreamSynchronize(xs));
+    Ctl h;
+    if ((rc = read_ctl(run, &h))) return rc;
+    if (hbad) return fail(run, FVG_ERR_STATE, "rho w must be zero on a 2-D mesh");
+    if (h.steps && run->sens) ++run->host_steps;
+    if (dt) *dt = h.steps ? h.dt : 0.0;
+    if (smax) *smax = h.steps ? h.s_step : 0.0;
+    return ctl_status(run, h, h.steps);
 }
 
 int fvg_part_info(const fvg_run* run, int* axis, int* first, int* count, int* depth, int* peer_lo, int* peer_hi) {
@@ -2516,6 +2751,7 @@ int fvg_set_sensor(fvg_run* run, const void* weights, float threshold, int every
     run->sens_theta = threshold;
     run->sens_every = every;
     run->sens_radius = radius;
+    run->host_steps = 0;
     return FVG_OK;
 }
 

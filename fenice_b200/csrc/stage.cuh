@@ -41,6 +41,7 @@ struct StageArgs {
     const Ctl* ctl;             // dt
     const int* gate;            // the kernel does nothing unless *gate (the control block's `active` or `seed`)
     int tiles[3];               // tiles per axis
+    int b0;                     // the tile of the launch's first CTA (a launch over a range of tiles; 0: all)
     // the learned troubled-cell sensor's tile flags (mixed-precision WENO5-Z kernels with the sensor only): one byte per
     // axis and tile (axis-major), 1 where the tile's reconstructions along the axis stay WENO5-Z, 0 where they are linear
     const unsigned char* sens_flags;
@@ -243,7 +244,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
 
     const Mesh& m = a.m;
     const int tid = threadIdx.x;
-    const int b = blockIdx.x;
+    const int b = blockIdx.x + a.b0;
     const int t0 = b % a.tiles[0], t1 = (b / a.tiles[0]) % a.tiles[1], t2 = b / (a.tiles[0] * a.tiles[1]);
     const int o3[3] = {t0 * TX, t1 * TY, t2 * TZ};
     double smax = 0.0;

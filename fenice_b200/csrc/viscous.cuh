@@ -35,6 +35,7 @@ struct ViscArgs {
     double* blockmax;
     const int* gate;   // the kernel does nothing unless *gate
     int tiles[3];
+    int b0;            // the tile of the launch's first CTA (a launch over a range of tiles; 0: all)
 };
 
 // the zero-gradient copy with the momentum rules of a wall side (BoundaryManager::viscous_ghost_3d, Boundaries.cpp:258-275)
@@ -156,7 +157,7 @@ __global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
     double* red = acc + 5 * NC;
     if (!*a.gate) return;
     const Mesh& m = a.m;
-    const int tid = threadIdx.x, b = blockIdx.x;
+    const int tid = threadIdx.x, b = blockIdx.x + a.b0;
     const int o3[3] = {(b % a.tiles[0]) * TX, ((b / a.tiles[0]) % a.tiles[1]) * TY, (b / (a.tiles[0] * a.tiles[1])) * TZ};
     const int n3[3] = {m.nx, m.ny, m.nz};
     const double h[3] = {m.dx, m.dy, m.dz};
@@ -366,7 +367,7 @@ __global__ void __launch_bounds__(NT) viscous2d_kernel(const ViscArgs a) {
     double* red = FY + 3 * S::NFY;
     if (!*a.gate) return;
     const Mesh& m = a.m;
-    const int tid = threadIdx.x, b = blockIdx.x;
+    const int tid = threadIdx.x, b = blockIdx.x + a.b0;
     const int ox = (b % a.tiles[0]) * TX, oy = (b / a.tiles[0]) * TY;
     const int nx = m.nx, ny = m.ny;
     const double dx = m.dx, dy = m.dy, mu = a.mu, kc = a.k_cond;

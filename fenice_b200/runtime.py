@@ -26,7 +26,7 @@ StepResult = namedtuple("StepResult", ["dt", "s_max"])
 
 # every entry point of include/fenice_gpu.h
 EXPORTS = ["fvg_abi_version", "fvg_create", "fvg_destroy", "fvg_last_error", "fvg_create_error", "fvg_upload_state",
-           "fvg_download_state", "fvg_residual", "fvg_step", "fvg_run_until", "fvg_get_time", "fvg_set_time", "fvg_set_stage_time",
+           "fvg_download_state", "fvg_residual", "fvg_step", "fvg_run_until", "fvg_step_host", "fvg_get_time", "fvg_set_time", "fvg_set_stage_time",
            "fvg_get_lagged_speed", "fvg_set_lagged_speed", "fvg_dt_length", "fvg_device_state", "fvg_stream",
            "fvg_synchronize", "fvg_face_flux_batch", "fvg_set_timing", "fvg_get_timing",
            "fvg_residual_noalloc",
@@ -64,6 +64,7 @@ def load_library(path=LIB_PATH):
     lib.fvg_download_state.argtypes = [c_p, dp, ctypes.c_size_t]
     lib.fvg_residual.argtypes = [c_p, ctypes.c_double, dp, ctypes.c_size_t, dp]
     lib.fvg_step.argtypes = [c_p, ctypes.c_double, dp, dp]
+    lib.fvg_step_host.argtypes = [c_p, dp, dp, ctypes.c_size_t, ctypes.c_double, dp, dp]
     lib.fvg_run_until.argtypes = [c_p, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.fvg_get_time.argtypes = [c_p, dp]
     lib.fvg_set_time.argtypes = [c_p, ctypes.c_double]
@@ -219,6 +220,21 @@ class Run:
     def step(self, t_end):
         dt, s = ctypes.c_double(), ctypes.c_double()
         self._check(self.lib.fvg_step(self.h, float(t_end), ctypes.byref(dt), ctypes.byref(s)), "step")
+        return StepResult(dt.value, s.value)
+
+    def step_host(self, U, t_end, out=None):
+        """One step of a state held in host memory (TimeScheme::step(Field& U) with the caller's U): U is uploaded, stepped
+        toward t_end and the new state written to `out` (default: U itself, in place). U and out are C-contiguous float64
+        (ncells, 5) arrays; in pinned memory (e.g. views of torch pin_memory tensors) the copies overlap the computation.
+        The result is the bits of set_state + step + state."""
+        out = U if out is None else out
+        for a, name in ((U, "U"), (out, "out")):
+            if not isinstance(a, np.ndarray) or a.shape != (self.ncells, 5) or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError(f"{name} must be a C-contiguous float64 array of shape ({self.ncells}, 5)")
+        if not out.flags.writeable:
+            raise ValueError("out must be writeable")
+        dt, s = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.fvg_step_host(self.h, _dp(U), _dp(out), self.ncells, float(t_end), ctypes.byref(dt), ctypes.byref(s)), "step_host")
         return StepResult(dt.value, s.value)
 
     def run(self, t_end, max_steps=0):

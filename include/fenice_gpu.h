@@ -150,6 +150,17 @@ int fvg_step(fvg_run* run, double t_end, double* dt, double* smax);
  * clock kept on the device; *steps gets the number taken. */
 int fvg_run_until(fvg_run* run, double t_end, int max_steps, int* steps);
 
+/* TimeScheme::step(Field& U, ...) with U in host memory (cpp/include/fv/TimeScheme.hpp:48, the seam's caller owns U):
+ * U_in (ncells x 5 doubles, reference layout) is uploaded, one step of the serial time loop taken toward t_end and the
+ * new state written to U_out (which may be U_in); dt and the step's wave speed are returned. The result is the bits of
+ * fvg_upload_state + fvg_step + fvg_download_state. For Runge-Kutta and Euler runs without an immersed body, mass-flow
+ * inlet, positivity fallback or fourth-order quadrature, the copies overlap the computation: the state crosses the host
+ * link in slabs along the slowest axis, the first stage starts on the slabs that have arrived and the last stage's slabs
+ * are read back as they are finished (pinned host buffers are needed for the overlap). Other runs take the three calls
+ * in turn. With the learned sensor, the gate is refreshed on every sens_every-th call that steps, counted from
+ * fvg_set_sensor (fvg_step refreshes it on every call). */
+int fvg_step_host(fvg_run* run, const double* U_in, double* U_out, size_t ncells, double t_end, double* dt, double* smax);
+
 /* ---- Slab decomposition (one process, or one part, per GPU; SimulationRun.cpp:1011-1446 run_mpi and
  * MPIDecomposition.cpp:114-242 split the mesh into strips the same way and exchange halos and the wave speed).
  * Part `part` of `nparts` slabs of the mesh of cfg along its slowest axis (z on a 3-D mesh, y on a 2-D one): planes
