@@ -64,11 +64,12 @@ public:
         check(fvg_step(h_, t_end, &r.dt, &r.s_max), "step", fvg_last_error(h_));
         return r;
     }
-    // the same on a host state, updated in place (upload, step, download)
+    // the same on a host state, updated in place (fvg_step_host: the bits of upload + step + download, the copies
+    // overlapped with the first and last stages where the run allows it; pin U's memory for the overlap)
     template <class Field> StepResult step(Field& U, double t_end) {
-        upload(U);
-        const StepResult r = step(t_end);
-        download(U);
+        StepResult r;
+        double* p = U.data()->data();
+        check(fvg_step_host(h_, p, p, U.size(), t_end, &r.dt, &r.s_max), "step", fvg_last_error(h_));
         return r;
     }
     int run_until(double t_end, int max_steps = 0) {
