@@ -550,11 +550,11 @@ struct fvg_run {
     double* d_loads = nullptr;
     double *d_forced = nullptr, *d_img_w = nullptr, *d_ratio = nullptr, *d_gn = nullptr, *d_span = nullptr;
     // the learned sensor (fvg_set_sensor): its weights (a copy), the logit threshold, the refresh period and dilation,
-    // the two flag buffers (the result in sens_result), the counters
+    // the network's flags of every (cell, axis), the tile flags the stage kernels read, the counters
     void* sens = nullptr;
     float sens_theta = 0.0f;
     int sens_every = 5, sens_radius = 4;
-    unsigned char* sens_flags[2] = {nullptr, nullptr};
+    unsigned char* sens_flags = nullptr;
     unsigned char* sens_tiles = nullptr;   // per axis and stage tile
     unsigned long long* sens_count = nullptr;
     // one part of a slab-decomposed mesh (fvg_create_part): the split axis (z in 3-D, y in 2-D), the part's first plane
@@ -1030,7 +1030,7 @@ cudaError_t refresh_gate(fvg_run* r, const double* Uin, const Ctl* ctl) {
     int per[3];
     for (int d = 0; d < 3; ++d) per[d] = r->cfg.bc[2 * d] == FVG_BC_PERIODIC && r->cfg.bc[2 * d + 1] == FVG_BC_PERIODIC;
     const int tile[3] = {r->dim == 3 ? Tile<3>::X : Tile<2>::X, r->dim == 3 ? Tile<3>::Y : Tile<2>::Y, r->dim == 3 ? Tile<3>::Z : 1};
-    return sensor_refresh(r->m, r->bc, r->eos, r->dim, Uin, r->sens, r->sens_theta, r->sens_radius, per, r->sens_flags[0], r->sens_flags[1], tile,
+    return sensor_refresh(r->m, r->bc, r->eos, r->dim, Uin, r->sens, r->sens_theta, r->sens_radius, per, r->sens_flags, tile,
                           r->tiles, r->sens_tiles, ctl, r->sens_every, r->sens_count, r->stream);
 }
 
@@ -2088,8 +2088,7 @@ int fvg_destroy(fvg_run* run) {
     if (run->fb_grew) cudaFree(run->fb_grew);
     if (run->sens) cudaFree(run->sens);
     if (run->sens_count) cudaFree(run->sens_count);
-    for (unsigned char* f : run->sens_flags)
-        if (f) cudaFree(f);
+    if (run->sens_flags) cudaFree(run->sens_flags);
     if (run->sens_tiles) cudaFree(run->sens_tiles);
     for (void* p : {(void*)run->d_mask, (void*)run->d_slot, (void*)run->d_forced, (void*)run->d_ghost, (void*)run->d_img_cell, (void*)run->d_img_w,
                     (void*)run->d_ratio, (void*)run->d_gn, (void*)run->d_deep, (void*)run->d_solid, (void*)run->d_loads, (void*)run->d_gvel,
@@ -2736,8 +2735,7 @@ int fvg_set_sensor(fvg_run* run, const void* weights, float threshold, int every
     if (radius < 0) radius = (int)std::ceil(run->cfg.cfl * every) + 1;
     const size_t fbytes = (size_t)run->m.plane * run->dim;
     if (!run->sens) CK(cudaMalloc(&run->sens, sizeof(SensorW)));
-    for (unsigned char*& f : run->sens_flags)
-        if (!f) CK(cudaMalloc(&f, fbytes));
+    if (!run->sens_flags) CK(cudaMalloc(&run->sens_flags, fbytes));
     if (!run->sens_tiles) CK(cudaMalloc(&run->sens_tiles, (size_t)run->nb * run->dim));
     if (!run->sens_count) {
         CK(cudaMalloc(&run->sens_count, 2 * sizeof(unsigned long long)));

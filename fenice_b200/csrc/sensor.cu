@@ -419,48 +419,18 @@ __global__ void __launch_bounds__(256) k_sensor_flags_t(Mesh m, Bc bc, Eos<doubl
     }
 }
 
-// One pass of the dilation: out = the largest flag within `radius` cells along axis d (every axis plane); the last pass
-// counts the linear (cell, axis) pairs.
-template <int DIM>
-__global__ void k_sensor_dilate(Mesh m, const unsigned char* __restrict__ in, unsigned char* __restrict__ out, int d, int radius, int periodic,
-                                const Ctl* ctl, int every, unsigned long long* counts) {
-    if (!refresh_due(ctl, every)) return;
-    const int n3[3] = {m.nx, m.ny, m.nz};
-    const long long stride = d == 0 ? 1 : (d == 1 ? (long long)m.nx : (long long)m.nx * m.ny);
-    unsigned long long lin = 0, all = 0;
-    const long long n = m.ncells * DIM;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-        const int a = (int)(e / m.ncells);
-        const long long c = e % m.ncells;
-        const int p = (int)(d == 0 ? c % m.nx : (d == 1 ? (c / m.nx) % m.ny : c / ((long long)m.nx * m.ny)));
-        const unsigned char* src = in + a * m.plane;
-        unsigned char v = 0;
-        for (int o = -radius; o <= radius && !v; ++o) {
-            int q = p + o;
-            if (q < 0 || q >= n3[d]) {
-                if (!periodic) continue;
-                q = ((q % n3[d]) + n3[d]) % n3[d];
-            }
-            v = src[c + (long long)(q - p) * stride];
-        }
-        out[a * m.plane + c] = v;
-        if (counts) {
-            lin += v ? 0 : 1;
-            all += 1;
-        }
-    }
-    if (counts) {
-        atomicAdd(counts, lin);
-        atomicAdd(counts + 1, all);
-    }
-}
+// The tile flags of the stage kernels straight from the network's flags. Tile b is linear along axis a (0) when no cell
+// whose reconstructions along a it needs (the tile extended by one cell along a) has a flagged (cell, a) pair within
+// `radius` cells per axis (the distance a wave travels until the next refresh): a max filter of that radius followed by
+// the OR over the extended tile is the OR over one box, the tile extended by radius + 1 cells along a and radius along the
+// other axes, each range wrapped across a periodic pair of sides and clipped at the others. A tile whose extension along a
+// leaves the mesh across a side that is not periodic stays WENO5-Z. One warp per (axis, tile), its lanes along x, rows of
+// the box in turn until a flagged pair is found; counts += [linear, all] tile-axes.
+__device__ __forceinline__ int wrap_index(int q, int n) { return q >= 0 && q < n ? q : ((q % n) + n) % n; }
 
-// The tile flags of the stage kernels: tile b is linear along axis a (0) when no cell whose reconstructions along a it
-// needs (the tile extended by one cell along a) is flagged; a tile whose extension leaves the mesh across a side that is
-// not periodic stays WENO5-Z. One warp per (axis, tile); counts += [linear, all] tile-axes.
 template <int DIM>
-__global__ void k_sensor_tiles(Mesh m, const unsigned char* __restrict__ flags, int TX, int TY, int TZ, int t0, int t1, int t2, int per0, int per1,
-                               int per2, unsigned char* __restrict__ out, const Ctl* ctl, int every, unsigned long long* counts) {
+__global__ void k_sensor_tilebox(Mesh m, const unsigned char* __restrict__ flags, int TX, int TY, int TZ, int t0, int t1, int t2, int per0, int per1,
+                                 int per2, int radius, unsigned char* __restrict__ out, const Ctl* ctl, int every, unsigned long long* counts) {
     if (!refresh_due(ctl, every)) return;
     const int lane = threadIdx.x & 31;
     const long long ntiles = (long long)t0 * t1 * t2, total = DIM * ntiles;
@@ -470,8 +440,7 @@ __global__ void k_sensor_tiles(Mesh m, const unsigned char* __restrict__ flags, 
         const int a = (int)(w / ntiles);
         const long long b = w % ntiles;
         const int o[3] = {(int)(b % t0) * TX, (int)((b / t0) % t1) * TY, (int)(b / ((long long)t0 * t1)) * TZ};
-        int lo[3], hi[3];   // the cell range, inclusive
-        bool edge = false;
+        int lo[3], hi[3];   // the box, inclusive (indices beyond a periodic side are wrapped when read)
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             lo[d] = o[d];
@@ -479,16 +448,26 @@ __global__ void k_sensor_tiles(Mesh m, const unsigned char* __restrict__ flags, 
         }
         lo[a] -= 1;
         hi[a] += 1;
-        if (!per[a] && (lo[a] < 0 || hi[a] > n3[a] - 1)) edge = true;
-        const int e0 = hi[0] - lo[0] + 1, e1 = hi[1] - lo[1] + 1, e2 = hi[2] - lo[2] + 1;
-        const int cnt = e0 * e1 * e2;
-        bool any = edge;
-        for (int k = lane; k < cnt && !edge; k += 32) {
-            int p3[3] = {lo[0] + k % e0, lo[1] + (k / e0) % e1, lo[2] + k / (e0 * e1)};
-            p3[a] = ((p3[a] % n3[a]) + n3[a]) % n3[a];
-            any = any || flags[a * m.plane + ((long long)p3[2] * m.ny + p3[1]) * m.nx + p3[0]] != 0;
+        bool any = !per[a] && (lo[a] < 0 || hi[a] > n3[a] - 1);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            lo[d] -= radius;
+            hi[d] += radius;
+            if (!per[d]) {
+                lo[d] = lo[d] < 0 ? 0 : lo[d];
+                hi[d] = hi[d] > n3[d] - 1 ? n3[d] - 1 : hi[d];
+            }
         }
-        any = __any_sync(0xffffffffu, any);
+        const unsigned char* src = flags + a * m.plane;
+        for (int z = lo[2]; z <= hi[2] && !any; ++z) {
+            const long long zoff = (long long)wrap_index(z, n3[2]) * m.ny;
+            for (int y = lo[1]; y <= hi[1] && !any; ++y) {
+                const unsigned char* row = src + (zoff + wrap_index(y, n3[1])) * m.nx;
+                bool f = false;
+                for (int x = lo[0] + lane; x <= hi[0]; x += 32) f = f || row[wrap_index(x, n3[0])] != 0;
+                any = __any_sync(0xffffffffu, f);
+            }
+        }
         if (lane == 0) {
             out[w] = any ? 1 : 0;
             lin += any ? 0 : 1;
@@ -509,7 +488,7 @@ int grid_for(long long rows) {
 }   // namespace
 
 cudaError_t fvg::sensor_refresh(const Mesh& m, const Bc& bc, const Eos<double>& eos, int dim, const double* U, const void* weights, float theta,
-                                int radius, const int periodic[3], unsigned char* flags0, unsigned char* flags1, const int tile[3],
+                                int radius, const int periodic[3], unsigned char* flags0, const int tile[3],
                                 const int tiles[3], unsigned char* tile_flags, const Ctl* ctl, int every, unsigned long long* counts,
                                 cudaStream_t s) {
     const SensorW* w = static_cast<const SensorW*>(weights);
@@ -520,25 +499,14 @@ cudaError_t fvg::sensor_refresh(const Mesh& m, const Bc& bc, const Eos<double>& 
         const int b0 = (m.nx + 31) / 32, b1 = (m.ny + 7) / 8;
         k_sensor_flags_t<2, 4, 32, 8, 1><<<b0 * b1, 256, 0, s>>>(m, bc, eos, U, w, theta, flags0, ctl, every, b0, b1);
     }
-    const long long n = m.ncells * dim;
-    const int db = (int)((n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16);
-    unsigned char* bufs[2] = {flags0, flags1};
-    int cur = 0;
-    for (int d = 0; d < dim; ++d) {
-        if (dim == 3)
-            k_sensor_dilate<3><<<db, 256, 0, s>>>(m, bufs[cur], bufs[cur ^ 1], d, radius, periodic[d], ctl, every, nullptr);
-        else
-            k_sensor_dilate<2><<<db, 256, 0, s>>>(m, bufs[cur], bufs[cur ^ 1], d, radius, periodic[d], ctl, every, nullptr);
-        cur ^= 1;
-    }
     const long long nt = (long long)tiles[0] * tiles[1] * tiles[2] * dim;
     const int tb = (int)((nt * 32 + 255) / 256 < 148 * 16 ? (nt * 32 + 255) / 256 : 148 * 16);
     if (dim == 3)
-        k_sensor_tiles<3><<<tb, 256, 0, s>>>(m, bufs[cur], tile[0], tile[1], tile[2], tiles[0], tiles[1], tiles[2], periodic[0], periodic[1], periodic[2],
-                                             tile_flags, ctl, every, counts);
+        k_sensor_tilebox<3><<<tb, 256, 0, s>>>(m, flags0, tile[0], tile[1], tile[2], tiles[0], tiles[1], tiles[2], periodic[0], periodic[1], periodic[2],
+                                               radius, tile_flags, ctl, every, counts);
     else
-        k_sensor_tiles<2><<<tb, 256, 0, s>>>(m, bufs[cur], tile[0], tile[1], 1, tiles[0], tiles[1], 1, periodic[0], periodic[1], 0, tile_flags, ctl,
-                                             every, counts);
+        k_sensor_tilebox<2><<<tb, 256, 0, s>>>(m, flags0, tile[0], tile[1], 1, tiles[0], tiles[1], 1, periodic[0], periodic[1], 0, radius, tile_flags,
+                                               ctl, every, counts);
     return cudaGetLastError();
 }
 

@@ -1,4 +1,5 @@
-// The sensor's refresh of a run's gate (sensor.cu): the network's flags for every (cell, axis) of the state, dilated.
+// The sensor's refresh of a run's gate (sensor.cu): the network's flags for every (cell, axis) of the state, reduced to
+// the stage kernel's tiles.
 #pragma once
 
 #include "grid.cuh"
@@ -7,12 +8,12 @@
 
 namespace fvg {
 // The network evaluated on every (cell, axis) of the state (flags0: 1 where the cell's reconstructions along the axis
-// stay WENO5-Z, logit >= theta), the troubled set grown by `radius` cells along every axis (wrapping across periodic
-// axes; flags0 / flags1 ping-pong), then reduced to the stage kernel's tiles: tile_flags[a * ntiles + b] = 0 where
-// tile b's reconstructions along axis a may all be linear. With a control block the kernels run only on the steps
+// stay WENO5-Z, logit >= theta), then, with the troubled set grown by `radius` cells along every axis (wrapping across
+// periodic axes), reduced to the stage kernel's tiles: tile_flags[a * ntiles + b] = 0 where tile b's reconstructions
+// along axis a may all be linear. With a control block the kernels run only on the steps
 // where ctl->active and ctl->steps % every == 0 (the tile flags of the last refresh stay otherwise). counts (device, may
 // be null) += [linear, all] tile-axes of each refresh.
 cudaError_t sensor_refresh(const Mesh& m, const Bc& bc, const Eos<double>& eos, int dim, const double* U, const void* weights, float theta, int radius,
-                           const int periodic[3], unsigned char* flags0, unsigned char* flags1, const int tile[3], const int tiles[3],
+                           const int periodic[3], unsigned char* flags0, const int tile[3], const int tiles[3],
                            unsigned char* tile_flags, const Ctl* ctl, int every, unsigned long long* counts, cudaStream_t s);
 }   // namespace fvg
