@@ -1030,7 +1030,7 @@ cudaError_t refresh_gate(fvg_run* r, const double* Uin, const Ctl* ctl) {
     int per[3];
     for (int d = 0; d < 3; ++d) per[d] = r->cfg.bc[2 * d] == FVG_BC_PERIODIC && r->cfg.bc[2 * d + 1] == FVG_BC_PERIODIC;
     const int tile[3] = {r->dim == 3 ? Tile<3>::X : Tile<2>::X, r->dim == 3 ? Tile<3>::Y : Tile<2>::Y, r->dim == 3 ? Tile<3>::Z : 1};
-    return sensor_refresh(r->m, r->bc, r->eos, r->dim, Uin, r->sens, r->sens_theta, r->sens_radius, per, r->sens_flags, tile,
+    return sensor_refresh(r->m, r->bc, r->eos, r->dim, Uin, r->sens, r->sens_theta, r->sens_radius, per, r->sens_flags, r->sens_flags + (size_t)r->m.plane * r->dim, tile,
                           r->tiles, r->sens_tiles, ctl, r->sens_every, r->sens_count, r->stream);
 }
 
@@ -2735,7 +2735,8 @@ int fvg_set_sensor(fvg_run* run, const void* weights, float threshold, int every
     if (radius < 0) radius = (int)std::ceil(run->cfg.cfl * every) + 1;
     const size_t fbytes = (size_t)run->m.plane * run->dim;
     if (!run->sens) CK(cudaMalloc(&run->sens, sizeof(SensorW)));
-    if (!run->sens_flags) CK(cudaMalloc(&run->sens_flags, fbytes));
+    const size_t rbytes = (size_t)run->dim * run->m.nz * run->m.ny * run->tiles[0];   // the gate's row pass (after the flags)
+    if (!run->sens_flags) CK(cudaMalloc(&run->sens_flags, fbytes + rbytes));
     if (!run->sens_tiles) CK(cudaMalloc(&run->sens_tiles, (size_t)run->nb * run->dim));
     if (!run->sens_count) {
         CK(cudaMalloc(&run->sens_count, 2 * sizeof(unsigned long long)));
@@ -2750,6 +2751,22 @@ int fvg_set_sensor(fvg_run* run, const void* weights, float threshold, int every
     run->sens_every = every;
     run->sens_radius = radius;
     run->host_steps = 0;
+    return FVG_OK;
+}
+
+int fvg_get_sensor_gate(fvg_run* run, unsigned char* cell_flags, unsigned char* tile_flags, int* tile, int* tiles) {
+    if (!run) return FVG_ERR_ARGUMENT;
+    if (!run->sens) return fail(run, FVG_ERR_CONFIG, "the run has no sensor (fvg_set_sensor)");
+    CK(cudaSetDevice(run->cfg.device));
+    CK(cudaStreamSynchronize(run->stream));
+    const int T[3] = {run->dim == 3 ? Tile<3>::X : Tile<2>::X, run->dim == 3 ? Tile<3>::Y : Tile<2>::Y, run->dim == 3 ? Tile<3>::Z : 1};
+    for (int d = 0; d < 3; ++d) {
+        if (tile) tile[d] = T[d];
+        if (tiles) tiles[d] = run->tiles[d];
+    }
+    for (int a = 0; a < run->dim && cell_flags; ++a)
+        CK(cudaMemcpy(cell_flags + a * run->m.ncells, run->sens_flags + a * run->m.plane, run->m.ncells, cudaMemcpyDeviceToHost));
+    if (tile_flags) CK(cudaMemcpy(tile_flags, run->sens_tiles, (size_t)run->nb * run->dim, cudaMemcpyDeviceToHost));
     return FVG_OK;
 }
 

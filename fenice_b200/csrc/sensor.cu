@@ -364,8 +364,11 @@ __global__ void __launch_bounds__(256) k_sensor_flags_t(Mesh m, Bc bc, Eos<doubl
                                                         float theta, unsigned char* __restrict__ flags, const Ctl* ctl, int every, int nb0, int nb1) {
     if (!refresh_due(ctl, every)) return;
     constexpr int EX = BX + 4, EY = BY + 4, EZ = DIM == 3 ? BZ + 4 : 1, BOX = EX * EY * EZ, NC = BX * BY * BZ, ROWS = NC * DIM;
+    // the planes of the primitive variables PS floats apart, PS = 7 (mod 32): the lanes that read the five quantities of
+    // one stencil position read five different banks (a plane stride that is a multiple of 32 puts them on one)
+    constexpr int PS = BOX + ((7 - BOX % 32) + 32) % 32;
     __shared__ __align__(16) unsigned char wbuf[kSensInferBytes];
-    __shared__ float P[NV * BOX];
+    __shared__ float P[NV * PS];
     __shared__ __align__(16) __nv_bfloat16 tiles[8][16 * kLd];
     const SensorW& w = *reinterpret_cast<const SensorW*>(wbuf);
     {
@@ -381,7 +384,7 @@ __global__ void __launch_bounds__(256) k_sensor_flags_t(Mesh m, Bc bc, Eos<doubl
         const int i = o0 + e % EX - 2, j = o1 + (e / EX) % EY - 2, k = DIM == 3 ? o2 + e / (EX * EY) - 2 : 0;
         const St<double, NV> wv = c2p(eos, stencil_cons<DIM, NV>(m, bc, eos, U, i, j, k));
 #pragma unroll
-        for (int q = 0; q < NV; ++q) P[q * BOX + e] = (float)wv[q];
+        for (int q = 0; q < NV; ++q) P[q * PS + e] = (float)wv[q];
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
@@ -397,7 +400,7 @@ __global__ void __launch_bounds__(256) k_sensor_flags_t(Mesh m, Bc bc, Eos<doubl
                 const int st = axis == 0 ? 1 : (axis == 1 ? EX : EX * EY);
                 float v[5];
 #pragma unroll
-                for (int k = 0; k < 5; ++k) v[k] = P[var * BOX + e + (k - 2) * st];
+                for (int k = 0; k < 5; ++k) v[k] = P[var * PS + e + (k - 2) * st];
                 sensor_quantity_features(v, f);
             }
 #pragma unroll
@@ -419,64 +422,89 @@ __global__ void __launch_bounds__(256) k_sensor_flags_t(Mesh m, Bc bc, Eos<doubl
     }
 }
 
-// The tile flags of the stage kernels straight from the network's flags. Tile b is linear along axis a (0) when no cell
-// whose reconstructions along a it needs (the tile extended by one cell along a) has a flagged (cell, a) pair within
-// `radius` cells per axis (the distance a wave travels until the next refresh): a max filter of that radius followed by
-// the OR over the extended tile is the OR over one box, the tile extended by radius + 1 cells along a and radius along the
-// other axes, each range wrapped across a periodic pair of sides and clipped at the others. A tile whose extension along a
-// leaves the mesh across a side that is not periodic stays WENO5-Z. One warp per (axis, tile), its lanes along x, rows of
-// the box in turn until a flagged pair is found; counts += [linear, all] tile-axes.
+// The tile flags of the stage kernels from the network's flags. Tile b is linear along axis a (0) when no cell whose
+// reconstructions along a it needs (the tile extended by one cell along a) has a flagged (cell, a) pair within `radius`
+// cells per axis (the distance a wave travels until the next refresh): a max filter of that radius followed by the OR over
+// the extended tile is the OR over one box, the tile extended by radius + 1 cells along a and radius along the other axes,
+// each range wrapped across a periodic pair of sides and clipped at the others. A tile whose extension along a leaves the
+// mesh across a side that is not periodic stays WENO5-Z. The box is taken in two passes: k_gate_rows ORs every row of
+// cells over each tile column's x range, k_gate_tiles ORs those bytes over the tile's y and z ranges.
 __device__ __forceinline__ int wrap_index(int q, int n) { return q >= 0 && q < n ? q : ((q % n) + n) % n; }
 
+// the box's range along axis d for a tile starting at o (inclusive; beyond a periodic side the indices wrap when read)
+__device__ __forceinline__ void gate_range(int o, int T, int n, int d, int a, int radius, bool periodic, int& lo, int& hi) {
+    lo = o;
+    hi = o + T - 1 < n - 1 ? o + T - 1 : n - 1;
+    if (d == a) {
+        lo -= 1;
+        hi += 1;
+    }
+    lo -= radius;
+    hi += radius;
+    if (!periodic) {
+        lo = lo < 0 ? 0 : lo;
+        hi = hi > n - 1 ? n - 1 : hi;
+    }
+}
+
+// rows[(a * nz + z) * ny + y][t0] = OR of flags[a] over the row (y, z) and the x range of tile column t0
 template <int DIM>
-__global__ void k_sensor_tilebox(Mesh m, const unsigned char* __restrict__ flags, int TX, int TY, int TZ, int t0, int t1, int t2, int per0, int per1,
-                                 int per2, int radius, unsigned char* __restrict__ out, const Ctl* ctl, int every, unsigned long long* counts) {
+__global__ void k_gate_rows(Mesh m, const unsigned char* __restrict__ flags, int TX, int t0n, int per0, int radius, unsigned char* __restrict__ rows,
+                            const Ctl* ctl, int every) {
     if (!refresh_due(ctl, every)) return;
-    const int lane = threadIdx.x & 31;
-    const long long ntiles = (long long)t0 * t1 * t2, total = DIM * ntiles;
-    const int n3[3] = {m.nx, m.ny, m.nz}, T[3] = {TX, TY, TZ}, per[3] = {per0, per1, per2};
+    const long long total = (long long)DIM * m.nz * m.ny * t0n;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const int t0 = (int)(e % t0n);
+        const long long ry = e / t0n;                           // (a * nz + z) * ny + y
+        const int a = (int)(ry / ((long long)m.nz * m.ny));
+        const unsigned char* row = flags + a * m.plane + (ry - (long long)a * m.nz * m.ny) * m.nx;
+        int lo, hi;
+        gate_range(t0 * TX, TX, m.nx, 0, a, radius, per0 != 0, lo, hi);
+        bool f = false;
+        for (int x = lo; x <= hi; ++x) f |= row[wrap_index(x, m.nx)] != 0;
+        rows[e] = f ? 1 : 0;
+    }
+}
+
+// out[a * ntiles + b] from the row bytes over the tile's y and z ranges, the edge rule; counts += [linear, all]
+template <int DIM>
+__global__ void k_gate_tiles(Mesh m, const unsigned char* __restrict__ rows, int TX, int TY, int TZ, int t0n, int t1n, int t2n, int per0, int per1,
+                             int per2, int radius, unsigned char* __restrict__ out, const Ctl* ctl, int every, unsigned long long* counts) {
+    if (!refresh_due(ctl, every)) return;
+    const long long ntiles = (long long)t0n * t1n * t2n, total = DIM * ntiles;
+    const int n3[3] = {m.nx, m.ny, m.nz}, per[3] = {per0, per1, per2};
     unsigned long long lin = 0, all = 0;
-    for (long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; w < total; w += ((long long)gridDim.x * blockDim.x) >> 5) {
+    for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total; w += (long long)gridDim.x * blockDim.x) {
         const int a = (int)(w / ntiles);
         const long long b = w % ntiles;
-        const int o[3] = {(int)(b % t0) * TX, (int)((b / t0) % t1) * TY, (int)(b / ((long long)t0 * t1)) * TZ};
-        int lo[3], hi[3];   // the box, inclusive (indices beyond a periodic side are wrapped when read)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            lo[d] = o[d];
-            hi[d] = o[d] + T[d] - 1 < n3[d] - 1 ? o[d] + T[d] - 1 : n3[d] - 1;
+        const int t0 = (int)(b % t0n), t1 = (int)((b / t0n) % t1n), t2 = (int)(b / ((long long)t0n * t1n));
+        const int o[3] = {t0 * TX, t1 * TY, t2 * TZ};
+        // the extension along a leaves the mesh across a side that is not periodic
+        const int T3[3] = {TX, TY, TZ};
+        const int ha = o[a] + T3[a] - 1 < n3[a] - 1 ? o[a] + T3[a] - 1 : n3[a] - 1;
+        bool any = !per[a] && (o[a] - 1 < 0 || ha + 1 > n3[a] - 1);
+        int lo1, hi1, lo2 = 0, hi2 = 0;
+        gate_range(o[1], TY, n3[1], 1, a, radius, per[1] != 0, lo1, hi1);
+        if (DIM == 3) gate_range(o[2], TZ, n3[2], 2, a, radius, per[2] != 0, lo2, hi2);
+        const unsigned char* src = rows + (long long)a * m.nz * m.ny * t0n + t0;
+        for (int z = lo2; z <= hi2 && !any; ++z) {
+            const long long zo = (long long)wrap_index(z, n3[2]) * m.ny;
+            for (int y = lo1; y <= hi1; ++y) any |= src[(zo + wrap_index(y, n3[1])) * t0n] != 0;
         }
-        lo[a] -= 1;
-        hi[a] += 1;
-        bool any = !per[a] && (lo[a] < 0 || hi[a] > n3[a] - 1);
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            lo[d] -= radius;
-            hi[d] += radius;
-            if (!per[d]) {
-                lo[d] = lo[d] < 0 ? 0 : lo[d];
-                hi[d] = hi[d] > n3[d] - 1 ? n3[d] - 1 : hi[d];
-            }
-        }
-        const unsigned char* src = flags + a * m.plane;
-        for (int z = lo[2]; z <= hi[2] && !any; ++z) {
-            const long long zoff = (long long)wrap_index(z, n3[2]) * m.ny;
-            for (int y = lo[1]; y <= hi[1] && !any; ++y) {
-                const unsigned char* row = src + (zoff + wrap_index(y, n3[1])) * m.nx;
-                bool f = false;
-                for (int x = lo[0] + lane; x <= hi[0]; x += 32) f = f || row[wrap_index(x, n3[0])] != 0;
-                any = __any_sync(0xffffffffu, f);
-            }
-        }
-        if (lane == 0) {
-            out[w] = any ? 1 : 0;
-            lin += any ? 0 : 1;
-            all += 1;
-        }
+        out[w] = any ? 1 : 0;
+        lin += any ? 0 : 1;
+        all += 1;
     }
-    if (counts && lane == 0 && all) {
-        atomicAdd(counts, lin);
-        atomicAdd(counts + 1, all);
+    if (counts) {
+#pragma unroll
+        for (int k = 16; k > 0; k >>= 1) {
+            lin += __shfl_xor_sync(0xffffffffu, lin, k);
+            all += __shfl_xor_sync(0xffffffffu, all, k);
+        }
+        if ((threadIdx.x & 31) == 0 && all) {
+            atomicAdd(counts, lin);
+            atomicAdd(counts + 1, all);
+        }
     }
 }
 
@@ -488,7 +516,7 @@ int grid_for(long long rows) {
 }   // namespace
 
 cudaError_t fvg::sensor_refresh(const Mesh& m, const Bc& bc, const Eos<double>& eos, int dim, const double* U, const void* weights, float theta,
-                                int radius, const int periodic[3], unsigned char* flags0, const int tile[3],
+                                int radius, const int periodic[3], unsigned char* flags0, unsigned char* rows, const int tile[3],
                                 const int tiles[3], unsigned char* tile_flags, const Ctl* ctl, int every, unsigned long long* counts,
                                 cudaStream_t s) {
     const SensorW* w = static_cast<const SensorW*>(weights);
@@ -499,14 +527,19 @@ cudaError_t fvg::sensor_refresh(const Mesh& m, const Bc& bc, const Eos<double>& 
         const int b0 = (m.nx + 31) / 32, b1 = (m.ny + 7) / 8;
         k_sensor_flags_t<2, 4, 32, 8, 1><<<b0 * b1, 256, 0, s>>>(m, bc, eos, U, w, theta, flags0, ctl, every, b0, b1);
     }
+    const long long nr = (long long)dim * m.nz * m.ny * tiles[0];
+    const int rb = (int)((nr + 255) / 256 < 148 * 16 ? (nr + 255) / 256 : 148 * 16);
     const long long nt = (long long)tiles[0] * tiles[1] * tiles[2] * dim;
-    const int tb = (int)((nt * 32 + 255) / 256 < 148 * 16 ? (nt * 32 + 255) / 256 : 148 * 16);
-    if (dim == 3)
-        k_sensor_tilebox<3><<<tb, 256, 0, s>>>(m, flags0, tile[0], tile[1], tile[2], tiles[0], tiles[1], tiles[2], periodic[0], periodic[1], periodic[2],
-                                               radius, tile_flags, ctl, every, counts);
-    else
-        k_sensor_tilebox<2><<<tb, 256, 0, s>>>(m, flags0, tile[0], tile[1], 1, tiles[0], tiles[1], 1, periodic[0], periodic[1], 0, radius, tile_flags,
-                                               ctl, every, counts);
+    const int tb = (int)((nt + 255) / 256 < 148 * 16 ? (nt + 255) / 256 : 148 * 16);
+    if (dim == 3) {
+        k_gate_rows<3><<<rb, 256, 0, s>>>(m, flags0, tile[0], tiles[0], periodic[0], radius, rows, ctl, every);
+        k_gate_tiles<3><<<tb, 256, 0, s>>>(m, rows, tile[0], tile[1], tile[2], tiles[0], tiles[1], tiles[2], periodic[0], periodic[1], periodic[2], radius,
+                                           tile_flags, ctl, every, counts);
+    } else {
+        k_gate_rows<2><<<rb, 256, 0, s>>>(m, flags0, tile[0], tiles[0], periodic[0], radius, rows, ctl, every);
+        k_gate_tiles<2><<<tb, 256, 0, s>>>(m, rows, tile[0], tile[1], 1, tiles[0], tiles[1], 1, periodic[0], periodic[1], 0, radius, tile_flags, ctl,
+                                           every, counts);
+    }
     return cudaGetLastError();
 }
 

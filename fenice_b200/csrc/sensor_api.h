@@ -10,10 +10,10 @@ namespace fvg {
 // The network evaluated on every (cell, axis) of the state (flags0: 1 where the cell's reconstructions along the axis
 // stay WENO5-Z, logit >= theta), then, with the troubled set grown by `radius` cells along every axis (wrapping across
 // periodic axes), reduced to the stage kernel's tiles: tile_flags[a * ntiles + b] = 0 where tile b's reconstructions
-// along axis a may all be linear. With a control block the kernels run only on the steps
+// along axis a may all be linear. rows: scratch of dim x nz x ny x tiles[0] bytes. With a control block the kernels run only on the steps
 // where ctl->active and ctl->steps % every == 0 (the tile flags of the last refresh stay otherwise). counts (device, may
 // be null) += [linear, all] tile-axes of each refresh.
 cudaError_t sensor_refresh(const Mesh& m, const Bc& bc, const Eos<double>& eos, int dim, const double* U, const void* weights, float theta, int radius,
-                           const int periodic[3], unsigned char* flags0, const int tile[3], const int tiles[3],
+                           const int periodic[3], unsigned char* flags0, unsigned char* rows, const int tile[3], const int tiles[3],
                            unsigned char* tile_flags, const Ctl* ctl, int every, unsigned long long* counts, cudaStream_t s);
 }   // namespace fvg

@@ -34,7 +34,7 @@ EXPORTS = ["fvg_abi_version", "fvg_create", "fvg_destroy", "fvg_last_error", "fv
            "fvg_batch_download", "fvg_batch_run", "fvg_batch_problem", "fvg_batch_autotune", "fvg_batch_set_schedule",
            "fvg_batch_get_schedule", "fvg_batch_stream", "fvg_batch_set_timing", "fvg_batch_get_timing",
            "fvg_sensor_sizes", "fvg_sensor_extract", "fvg_sensor_grad", "fvg_sensor_adam", "fvg_sensor_pack", "fvg_sensor_infer",
-           "fvg_set_sensor", "fvg_get_sensor_counts", "fvg_ibm_loads",
+           "fvg_set_sensor", "fvg_get_sensor_counts", "fvg_get_sensor_gate", "fvg_ibm_loads",
            "fvg_create_part", "fvg_part_info", "fvg_part_buffers", "fvg_part_begin", "fvg_part_phase", "fvg_part_status",
            "fvg_expr_eval"]
 
@@ -104,6 +104,7 @@ def load_library(path=LIB_PATH):
     lib.fvg_sensor_infer.argtypes = [c_p, c_p, ctypes.c_longlong, c_p, c_p]
     lib.fvg_set_sensor.argtypes = [c_p, c_p, ctypes.c_float, ctypes.c_int, ctypes.c_int]
     lib.fvg_get_sensor_counts.argtypes = [c_p, ll, ll, ctypes.c_int]
+    lib.fvg_get_sensor_gate.argtypes = [c_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     lib.fvg_ibm_loads.argtypes = [c_p, dp]
     ip = ctypes.POINTER(ctypes.c_int)
     dpp = ctypes.POINTER(dp)
@@ -304,6 +305,17 @@ class Run:
         refreshed every `every` steps and grown by `radius` cells (defaults: 5 steps, ceil(cfl every) + 1 cells)."""
         ptr = None if sensor is None else sensor.weights_ptr()
         self._check(self.lib.fvg_set_sensor(self.h, ptr, float(threshold), int(every), int(radius)), "set_sensor")
+
+    def sensor_gate(self):
+        """The gate of the last refresh: (cell_flags (dim, ncells) uint8: the network's flag of every (cell, axis), 1 = stays
+        WENO5-Z; tile_flags (dim, tiles z, tiles y, tiles x) uint8: what the stage kernels read; the tile's cells (x, y, z))."""
+        dim = 3 if int(self.params.get("nz", 1)) > 1 else 2
+        tile, tiles = (ctypes.c_int * 3)(), (ctypes.c_int * 3)()
+        self._check(self.lib.fvg_get_sensor_gate(self.h, None, None, tile, tiles), "sensor_gate")
+        cells = np.empty((dim, self.ncells), dtype=np.uint8)
+        tf = np.empty((dim, tiles[2], tiles[1], tiles[0]), dtype=np.uint8)
+        self._check(self.lib.fvg_get_sensor_gate(self.h, cells.ctypes.data, tf.ctypes.data, tile, tiles), "sensor_gate")
+        return cells, tf, tuple(tile)
 
     def sensor_counts(self, reset=False):
         """(cell-axis evaluations that went linear, all evaluations) since the last reset."""

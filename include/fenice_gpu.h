@@ -280,6 +280,11 @@ int fvg_sensor_pack(const float* params, void* weights, void* stream);
 int fvg_sensor_infer(const void* weights, const float* X, long long n, float* logits, void* stream);
 int fvg_set_sensor(fvg_run* run, const void* weights, float threshold, int every, int radius);
 int fvg_get_sensor_counts(fvg_run* run, long long* linear, long long* evaluated, int reset);
+/* The gate of the last refresh, for inspection (no counterpart in the reference): cell_flags (dim x ncells bytes, axis-
+ * major, cells in the reference's order; may be NULL) the network's flag of every (cell, axis), 1 = stays WENO5-Z;
+ * tile_flags (dim x the tiles' count, axis-major; may be NULL) what the stage kernels read, 1 = WENO5-Z; tile (3 ints) the
+ * stage tile's cells per axis and tiles (3 ints) the tiles per axis. */
+int fvg_get_sensor_gate(fvg_run* run, unsigned char* cell_flags, unsigned char* tile_flags, int* tile, int* tiles);
 
 /* ---- Batched independent problems (no counterpart in the reference, which runs one Simulation per process).
  *

@@ -13,6 +13,8 @@ labels and network, the check of the GPU sensor kernels (fenice_b200/csrc/sensor
 * mlp_forward / mlp_loss_grad: 32 -> 32 -> 32 -> 1 with ReLU, the product's arithmetic emulated: inputs, weights and
   hidden activations rounded to bfloat16 where the kernels feed them to the tensor cores, sums and biases in float32 (here
   float64 on the rounded operands), loss the mean class-weighted binary cross-entropy with logits.
+* gate_tiles: the stage tiles' gate from the network's flags of every (cell, axis): the troubled set grown by the travel
+  radius, then reduced to the tiles (stated below as two separate steps; the device does both in one pass).
 """
 import numpy as np
 
@@ -112,3 +114,49 @@ def mlp_loss_grad(X, y, wpos, P):
     G["W1"] = dh1b.T @ Xb
     G["b1"] = dh1.sum(axis=0)
     return loss, G
+
+
+def gate_tiles(cell_flags, tile, radius, periodic):
+    """The gate of the stage tiles from the network's flags (cell_flags: (dim, nz, ny, nx), 1 = the cell's
+    reconstructions along that axis stay WENO5-Z). (1) Every axis plane grown by `radius` cells along each mesh axis, one
+    axis after the other: a cell is flagged when a flagged cell lies within `radius` along that axis, the index wrapped
+    across a periodic pair of sides and dropped beyond the others. (2) Per axis a and tile (tile = cells per axis, the
+    last tile cut at the mesh end): 1 when a flagged cell lies in the tile extended by one cell along a (wrapped across a
+    periodic side), or when that extension leaves the mesh across a side that is not periodic. Returns
+    (dim, tiles z, tiles y, tiles x) uint8."""
+    f = np.asarray(cell_flags).astype(bool)
+    dim = f.shape[0]
+    n3 = (f.shape[3], f.shape[2], f.shape[1])
+    for d in range(dim):
+        ax = 3 - d   # mesh axis d is numpy axis 3 - d of (dim, nz, ny, nx)
+        g = np.zeros_like(f)
+        for o in range(-radius, radius + 1):
+            if periodic[d]:
+                g |= np.roll(f, -o, axis=ax)   # g[i] |= f[(i + o) mod n]
+            else:
+                src = [slice(None)] * 4
+                dst = [slice(None)] * 4
+                n = n3[d]
+                if o >= 0:
+                    src[ax], dst[ax] = slice(o, n), slice(0, max(n - o, 0))
+                else:
+                    src[ax], dst[ax] = slice(0, max(n + o, 0)), slice(-o, n)
+                g[tuple(dst)] |= f[tuple(src)]
+        f = g
+    tiles = [(n3[d] + tile[d] - 1) // tile[d] for d in range(3)]
+    out = np.zeros((dim, tiles[2], tiles[1], tiles[0]), dtype=np.uint8)
+    for a in range(dim):
+        for t2 in range(tiles[2]):
+            for t1 in range(tiles[1]):
+                for t0 in range(tiles[0]):
+                    o = (t0 * tile[0], t1 * tile[1], t2 * tile[2])
+                    lo = list(o)
+                    hi = [min(o[d] + tile[d] - 1, n3[d] - 1) for d in range(3)]
+                    lo[a] -= 1
+                    hi[a] += 1
+                    if not periodic[a] and (lo[a] < 0 or hi[a] > n3[a] - 1):
+                        out[a, t2, t1, t0] = 1
+                        continue
+                    idx = [np.arange(lo[d], hi[d] + 1) % n3[d] for d in range(3)]
+                    out[a, t2, t1, t0] = f[a][np.ix_(idx[2], idx[1], idx[0])].any()
+    return out

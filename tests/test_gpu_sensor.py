@@ -143,3 +143,54 @@ def test_gate_extremes_and_counts():
     inner = (tiles_x - 2) * tiles_y + tiles_x * (tiles_y - 2)   # x sweeps: tiles off the x sides; y sweeps: off the y sides
     print(f"gate all linear: counts {lin}/{ev} per refresh pattern, interior tile-axes {inner}")
     assert lin > 0 and lin % inner == 0 and np.abs(linear.state() - plain.state()).max() > 0
+
+
+GATE_CASES = [
+    # (name, mesh and boundaries, initial state, refresh period, dilation radius (-1: ceil(cfl every) + 1))
+    ("tgv3d_48_periodic", dict(nx=48, ny=48, nz=48, Lx=2 * np.pi, Ly=2 * np.pi, Lz=2 * np.pi, use_viscous=True, mu=6.25e-4, pr=0.71,
+                               reconstruction="weno5", riemann_solver="lowmach", time_scheme="SSP Runge-Kutta 3", cfl=0.5,
+                               bc_xmin="periodic", bc_xmax="periodic", bc_ymin="periodic", bc_ymax="periodic", bc_zmin="periodic",
+                               bc_zmax="periodic"), "tgv", 5, -1),
+    ("box3d_mixed_sides_r3", dict(nx=40, ny=36, nz=28, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", cfl=0.4, bc_xmin="periodic",
+                                  bc_xmax="periodic", bc_ymin="transmissive", bc_ymax="wall", bc_zmin="periodic", bc_zmax="periodic"), "jump", 4, 3),
+    ("quadrants2d_200x136_r6", dict(nx=200, ny=136, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", cfl=0.4, bc_xmin="transmissive",
+                                    bc_xmax="transmissive", bc_ymin="transmissive", bc_ymax="transmissive"), "quadrants", 5, 6),
+    ("periodic2d_96x80_r2", dict(nx=96, ny=80, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", cfl=0.4, bc_xmin="periodic",
+                                 bc_xmax="periodic", bc_ymin="periodic", bc_ymax="periodic"), "jump", 3, 2),
+]
+
+
+@pytest.mark.parametrize("name,params,init,every,radius", GATE_CASES, ids=[c[0] for c in GATE_CASES])
+def test_gate_matches_the_oracle(name, params, init, every, radius):
+    """The tile flags the stage kernels read, from the network's flags of the same refresh through the oracle's
+    dilation and tile reduction: identical."""
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.dirname(__file__))
+    import cases
+    from fenice_b200.sensor import Sensor
+
+    if init == "tgv":
+        import bench
+
+        U0 = bench.tgv_state(params["nx"])
+    elif init == "quadrants":
+        U0 = initial.riemann_quadrants(params["nx"], 4) if params["nx"] == params["ny"] else cases.case_field(params, 6)
+    else:
+        U0 = cases.case_field(params, 6)
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    s = Sensor.load(os.path.join(here, "fenice_b200", "sensor_weights.npz"), device=0)
+    run = Run(params, U=U0, precision=1)
+    run.set_sensor(s, float(s.meta["threshold"]), every=every, radius=radius)
+    assert run.run(1e30, max_steps=1) == 1
+    cells, tiles, tile = run.sensor_gate()
+    dim = cells.shape[0]
+    nz = int(params.get("nz", 1))
+    per = [params.get(f"bc_{a}min") == "periodic" and params.get(f"bc_{a}max") == "periodic" for a in "xyz"]
+    r = radius if radius >= 0 else int(np.ceil(params["cfl"] * every)) + 1
+    want = SO.gate_tiles(cells.reshape(dim, nz, params["ny"], params["nx"]), tile, r, per)
+    lin = int((tiles == 0).sum())
+    print(f"\n{name}: {int(cells.sum())} of {cells.size} (cell, axis) pairs flagged, {lin} of {tiles.size} tile-axes linear")
+    assert np.array_equal(tiles, want)
+    run.close()
