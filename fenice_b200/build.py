@@ -39,12 +39,33 @@ UNIT_FLAGS = {
 }
 
 
+def _deps(obj):
+    """The files an object was compiled from, from the dependency file nvcc wrote beside it (-MD); None if absent."""
+    try:
+        with open(obj + ".d") as f:
+            text = f.read().replace("\\\n", " ")
+    except OSError:
+        return None
+    return [d for d in text.split(":", 1)[1].split() if d] if ":" in text else None
+
+
+def _obj_stale(src, obj):
+    if not os.path.exists(obj):
+        return True
+    deps = _deps(obj)
+    if deps is None:
+        deps = [src] + [os.path.join(SRC, h) for h in HEADERS]
+    t = os.path.getmtime(obj)
+    return any(not os.path.exists(d) or os.path.getmtime(d) > t for d in deps + [__file__])
+
+
 def _stale():
     if not os.path.exists(LIB):
         return True
+    objdir = os.path.join(HERE, "_build")
+    objs = [os.path.join(objdir, f.replace(".cu", ".o")) for f in SOURCES]
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(SRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "fenice_gpu.h"), __file__]
-    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+    return any(_obj_stale(os.path.join(SRC, f), o) for f, o in zip(SOURCES, objs)) or any(os.path.getmtime(o) > t for o in objs if os.path.exists(o))
 
 
 def _run(cmd, verbose):
@@ -64,9 +85,11 @@ def build(force=False, verbose=False, extra=()):
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
     objs = [os.path.join(objdir, f.replace(".cu", ".o")) for f in SOURCES]
-    cmds = [[NVCC] + COMMON_FLAGS + UNIT_FLAGS[f] + list(extra) + ["-c", os.path.join(SRC, f), "-o", o] for f, o in zip(SOURCES, objs)]
+    # only the translation units whose sources or included headers changed since their object was built (all with --force)
+    cmds = [[NVCC] + COMMON_FLAGS + UNIT_FLAGS[f] + list(extra) + ["-MD", "-MF", o + ".d", "-c", os.path.join(SRC, f), "-o", o]
+            for f, o in zip(SOURCES, objs) if force or extra or _obj_stale(os.path.join(SRC, f), o)]
     # the translation units compile in parallel
-    with concurrent.futures.ThreadPoolExecutor(max_workers=len(cmds)) as pool:
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, len(cmds))) as pool:
         for fut in [pool.submit(_run, c, verbose) for c in cmds]:
             fut.result()
     _run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "--cudart", "static", "-shared", "-o", LIB] + objs, verbose)

@@ -82,6 +82,11 @@ def load_checkpoint(path, run):
         if key in a and int(a[key]) != int(n):
             raise ValueError(f"The checkpoint {path} is of a {int(a['nx'])} x {int(a['ny'])} x {int(a['nz'])} mesh, the run's is "
                              f"{run.params['nx']} x {run.params['ny']} x {run.params['nz']}")
+    # the domain's size as well, 1e-10 apart at most (the reference's test for the base mesh of an adaptive file,
+    # SimulationRestart.cpp:283-287; a uniform file of another size would resume with another spacing)
+    for key in ("Lx", "Ly", "Lz"):
+        if key in a and abs(float(a[key]) - float(run.params[key])) > 1e-10:
+            raise ValueError(f"The checkpoint {path} is of a domain with {key} = {float(a[key])!r}, the run's is {float(run.params[key])!r}")
     U = np.asarray(a["U"], dtype=np.float64)
     if U.shape[0] != run.ncells:
         raise ValueError(f"The checkpoint {path} holds {U.shape[0]} cells, the run {run.ncells}")

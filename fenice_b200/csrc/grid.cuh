@@ -204,6 +204,15 @@ __device__ __forceinline__ St<double, NV> stencil_cons(const Mesh& m, const Bc& 
         out_axis = a;
         ++nout;
     }
+    // every index onto the cells the arrays hold (a part's ghost planes included); positions beyond them belong to a
+    // tile overhanging the mesh or the part, whose results are discarded
+    const auto clamp_held = [&]() {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int lo = FULL ? -bc.ext[2 * a] : 0, hi = FULL ? n3[a] - 1 + bc.ext[2 * a + 1] : n3[a] - 1;
+            idx[a] = idx[a] < lo ? lo : (idx[a] > hi ? hi : idx[a]);
+        }
+    };
     if (nout == 1) {
         const int a = out_axis;
         const bool hi = idx[a] >= n3[a];
@@ -212,15 +221,14 @@ __device__ __forceinline__ St<double, NV> stencil_cons(const Mesh& m, const Bc& 
             int l = hi ? idx[a] - n3[a] : -1 - idx[a];
             l = l < n3[a] ? l : n3[a] - 1;
             idx[a] = hi ? n3[a] - 1 - l : l;
+            // the other axes too: beyond a part interface a position may lie past the ghost planes (a tile overhanging
+            // the part), and reading it would leave the state arrays
+            clamp_held();
             const long long c = ((long long)idx[2] * m.ny + idx[1]) * m.nx + idx[0];
             return ghost_state(e, bc, side, read_state<NV>(bc, U, m.plane, c));
         }
     }
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const int lo = FULL ? -bc.ext[2 * a] : 0, hi = FULL ? n3[a] - 1 + bc.ext[2 * a + 1] : n3[a] - 1;
-        idx[a] = idx[a] < lo ? lo : (idx[a] > hi ? hi : idx[a]);
-    }
+    clamp_held();
     const long long c = ((long long)idx[2] * m.ny + idx[1]) * m.nx + idx[0];
     return read_state<NV>(bc, U, m.plane, c);
 }

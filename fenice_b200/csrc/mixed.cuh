@@ -101,8 +101,28 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
         }
         __syncthreads();
         const int sstride = axis == 0 ? 1 : (axis == 1 ? E[0] : E[0] * E[1]);
-        bool tile_linear = false;
-        if constexpr (GATED) tile_linear = a.sens_flags[AXIS * a.tiles[0] * a.tiles[1] * a.tiles[2] + blockIdx.x + a.b0] == 0;
+        // GATED: whether this tile's reconstructions along the axis are linear, and whether each of its two seam faces
+        // along the axis (shared with the tile before and the tile after, which solve them too) may be: only when the
+        // tile across is linear as well, so both tiles compute the same flux there and the balance stays conservative.
+        // A seam face is the tile's first face and its last face inside the mesh (a partial last tile included); on a
+        // periodic axis the neighbour of an end tile is the other end tile; beyond any other side no tile solves the
+        // face twice (and the gate keeps such tiles WENO5-Z).
+        bool tile_linear = false, seam_lo = false, seam_hi = false;
+        int hi_face = 0;
+        if constexpr (GATED) {
+            const unsigned char* fl = a.sens_flags + (long long)AXIS * a.tiles[0] * a.tiles[1] * a.tiles[2];
+            const int b = blockIdx.x + a.b0;
+            tile_linear = fl[b] == 0;
+            if (tile_linear) {
+                const int nt = a.tiles[AXIS];
+                const int st = AXIS == 0 ? 1 : (AXIS == 1 ? a.tiles[0] : a.tiles[0] * a.tiles[1]);
+                const int ta = AXIS == 0 ? b % a.tiles[0] : (AXIS == 1 ? (b / a.tiles[0]) % a.tiles[1] : b / (a.tiles[0] * a.tiles[1]));
+                const bool wrap_lo = a.bc.halo[2 * AXIS] == kHaloWrap, wrap_hi = a.bc.halo[2 * AXIS + 1] == kHaloWrap;
+                seam_lo = ta > 0 ? fl[b - st] == 0 : (wrap_lo ? fl[b + (nt - 1) * st] == 0 : true);
+                seam_hi = ta < nt - 1 ? fl[b + st] == 0 : (wrap_hi ? fl[b - (nt - 1) * st] == 0 : true);
+            }
+            hi_face = n3[AXIS] - o3[AXIS] < Fd[AXIS] - 1 ? n3[AXIS] - o3[AXIS] : Fd[AXIS] - 1;
+        }
         // ---- 2. face values
         for (int it = tid; it < nF * NV; it += NT) {
             const int f = it % nF, q = it / nF;
@@ -127,7 +147,7 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
                 if (four) {
                     wl = weno3z(c1, c2, c3, weps);
                     wr = weno3z(c4, c3, c2, weps);
-                } else if (tile_linear) {
+                } else if (tile_linear && (f3[AXIS] == 0 ? seam_lo : (f3[AXIS] == hi_face ? seam_hi : true))) {
                     // linear fifth-order upwind values where the sensor passed the tile (the WENO-Z weights at their
                     // linear values 0.1, 0.6, 0.3)
                     wl = lin5(c0, c1, c2, c3, c4);

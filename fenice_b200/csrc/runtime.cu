@@ -30,6 +30,7 @@
 #include "viscous.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -2868,11 +2869,9 @@ struct NoAllocScratch {
 };
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
-struct NoAllocDevice {
-    bool ready = false;
-    NoAllocScratch* ptr = nullptr;         // the device address of g_noalloc_scratch on this device
-};
-NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+// the device address of g_noalloc_scratch on each device (null until a call on that device has looked it up); host
+// threads making their first call at once may each look it up, and each stores the same address
+std::atomic<NoAllocScratch*> g_noalloc_dev[kNoAllocMaxDevices];
 
 __global__ void k_noalloc_begin(NoAllocScratch* s) {
     s->ctl = Ctl{};
@@ -2918,19 +2917,21 @@ extern "C" int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long
                                        "(at most %d tiles of %dx%dx%d cells)", tiles, kNoAllocMaxCtas, kNoAllocMaxCtas, TX, TY, TZ);
         return noalloc_fail(FVG_ERR_CONFIG, msg);
     }
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return noalloc_fail(FVG_ERR_CUDA, "no current CUDA device");
-    NoAllocDevice& d = g_noalloc_dev[dev];
+    // the call runs on cfg->device, made current on this thread as every entry point does
+    const int dev = c.device;
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return noalloc_fail(FVG_ERR_CONFIG, "fvg_residual_noalloc: device index out of range");
+    if (cudaSetDevice(dev) != cudaSuccess) return noalloc_fail(FVG_ERR_CUDA, "cudaSetDevice failed (no such CUDA device?)");
     bool full = c.positivity_fallback || c.use_bodyforce;   // (the residual of a whole mesh: no part interface)
     for (int s = 0; s < 6; ++s) full = full || c.bc[s] == FVG_BC_NONREFLECTING;
     const StageLauncher launcher = dim == 3 ? stage_launcher<3>(c.reconstruction, c.riemann, full) : stage_launcher<2>(c.reconstruction, c.riemann, full);
-    if (!d.ready) {
+    NoAllocScratch* scratch = g_noalloc_dev[dev].load(std::memory_order_acquire);
+    if (!scratch) {
         // once per device, with that device current: the device address of the scratch array (the host-side name is not one)
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return noalloc_fail(FVG_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        d.ptr = static_cast<NoAllocScratch*>(p);
-        d.ready = true;
+        scratch = static_cast<NoAllocScratch*>(p);
+        g_noalloc_dev[dev].store(scratch, std::memory_order_release);
     }
     if (launcher.prepare() != cudaSuccess) return noalloc_fail(FVG_ERR_CUDA, "kernel set-up failed (shared-memory limit)");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -2972,21 +2973,21 @@ extern "C" int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long
     a.mode = kStoreR;
     a.U = U;
     a.out = R;
-    a.blockmax = d.ptr->blockmax;
-    a.ctl = &d.ptr->ctl;
-    a.gate = &d.ptr->ctl.always;
+    a.blockmax = scratch->blockmax;
+    a.ctl = &scratch->ctl;
+    a.gate = &scratch->ctl.always;
     a.tiles[0] = (c.nx + TX - 1) / TX;
     a.tiles[1] = (c.ny + TY - 1) / TY;
     a.tiles[2] = (c.nz + TZ - 1) / TZ;
     // the control block is written afresh by every call (gate on, dt = 0); each CTA overwrites its own maximum
-    k_noalloc_begin<<<1, 1, 0, s>>>(d.ptr);
+    k_noalloc_begin<<<1, 1, 0, s>>>(scratch);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = launcher.launch(a, (int)tiles, s);
     if (e == cudaSuccess) {
-        k_noalloc_reduce<<<1, 1024, 0, s>>>(d.ptr, (int)tiles);
+        k_noalloc_reduce<<<1, 1024, 0, s>>>(scratch, (int)tiles);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess && smax) e = cudaMemcpyAsync(smax, &d.ptr->ctl.s_stage[0], sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && smax) e = cudaMemcpyAsync(smax, &scratch->ctl.s_stage[0], sizeof(double), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return noalloc_fail(FVG_ERR_CUDA, std::string("fvg_residual_noalloc: ") + cudaGetErrorString(e));
     return FVG_OK;

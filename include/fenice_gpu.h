@@ -234,16 +234,20 @@ int fvg_face_flux_batch(fvg_run* run, const double* UL, const double* UR, const 
  * host framework that owns every device allocation (its own caching allocator or a memory pool with a fixed budget),
  * or code that runs where the caller forbids allocation. Such a caller passes its own device buffers: U and R are nvar
  * planes of `plane` doubles each (nvar = 4 on a 2-D mesh, 5 on a 3-D mesh, the layout of fvg_device_state), R receives the
- * residual (Simulation::residual) and *smax (host, may be NULL) its wave speed. The work runs on `stream` (NULL: the
- * default stream) and the call returns when it is done.
+ * residual (Simulation::residual without the MUSCL-Hancock predictor, as fvg_residual with predictor_half_dt = 0) and
+ * *smax (host, may be NULL) its wave speed. The work runs on cfg->device, which the call makes current on the calling
+ * thread (as every entry point here does), on `stream` (NULL: the default stream); the call synchronises that stream and
+ * returns when the work is done.
  *
  * The only scratch is a fixed array inside the library (about 516 KB per device, kept by every GPU that loads the library
  * until the process exits): it holds one wave-speed maximum per tile, so a mesh may have at most 65536 tiles (8x8x8 cells
- * in 3-D, 16x15 in 2-D: e.g. 320^3 or 4096 x 3840 cells); a larger mesh, a viscous run (its viscous residual would need a
- * mesh-sized scratch array) or the MUSCL-Hancock predictor is rejected with FVG_ERR_CONFIG. The first call on a device
- * finds the array's device address (with that device current), so make that first call before any stream capture. All
- * calls share the array and leave their results in it: calls that overlap on the GPU (other threads, other streams) race
- * and must be serialised by the caller. On failure, fvg_create_error() returns this thread's message. */
+ * in 3-D, 16x15 in 2-D: e.g. 320^3 or 4096 x 3840 cells). Rejected with FVG_ERR_CONFIG, besides what fvg_create rejects:
+ * a mesh of more tiles, the mixed-precision form, a viscous run (its viscous residual would need a mesh-sized scratch
+ * array), an immersed body, flux_quadrature = fourth, case-file source terms or time-dependent boundary values, a
+ * mass-flow inlet (each needs device tables or arrays of its own). The first call on a device finds the array's device
+ * address (with that device current), so make that first call before any stream capture. All calls share the array and
+ * leave their results in it: calls that overlap on the GPU (other threads, other streams) race and must be serialised by
+ * the caller. On failure, fvg_create_error() returns this thread's message. */
 int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long long plane, double* R, double* smax, void* stream);
 
 /* ---- The learned troubled-cell sensor (no counterpart in the reference, whose WENO5-Z reconstruction, weno5z and
