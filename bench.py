@@ -34,6 +34,11 @@ STAGES = 3
 BYTES_PER_CELL_STAGE = (2 + 3 + 3) / 3 * 5 * 8   # SSP-RK3, 3-D: stage 1 reads U writes R; stages 2-3 read two states, write one
 
 
+def tgv_workload(n):
+    """The configuration string of the Taylor-Green workload (the same in both arms of the benchmark)."""
+    return f"Taylor-Green vortex 3-D {n}^3, WENO5-Z + low-Mach HLLC + SSP-RK3, viscous Re 1600 Pr 0.71, CFL 0.5"
+
+
 def workload(n):
     L = 2 * math.pi
     return dict(nx=n, ny=n, nz=n, Lx=L, Ly=L, Lz=L, gamma=1.4, use_viscous=True, mu=6.25e-4, pr=0.71,
@@ -236,6 +241,75 @@ def roofline_of(tm, ms, cells, kernel, traffic):
             "algorithmic_bytes_per_launch": alg_bytes, "stage_launch_ms": round(stage_avg_ms, 4),
             "viscous_launch_ms": round(tm["viscous_ms"] / max(tm["viscous_launches"], 1), 4),
             "stage_share_of_step": round(tm["stage_ms"] / ms, 4), "viscous_share_of_step": round(tm["viscous_ms"] / ms, 4)}
+
+
+def history_run(params, U0, precision, local, steps, every, sensor=None):
+    """`steps` steps of one form with the monitor (kinetic energy, enstrophy: fvg_monitor in its fast order) at step 0
+    and every `every` steps; the steps are timed with CUDA events on the run's stream chunk by chunk (the monitor calls
+    between the chunks are outside the timed region). Returns (state, ms, history, linear share or None)."""
+    import torch
+
+    from fenice_b200 import Run
+
+    warm = Run(params, U=U0, precision=precision, device=local)
+    if sensor is not None:
+        warm.set_sensor(*sensor)
+    warm.run(1e30, max_steps=3)
+    warm.close()
+    run = Run(params, U=U0, precision=precision, device=local)
+    if sensor is not None:
+        run.set_sensor(*sensor)
+    ext = torch.cuda.ExternalStream(run.stream(), device=torch.device("cuda", local))
+    hist, ms, done = [], 0.0, 0
+
+    def sample():
+        m = run.monitor("fast")
+        hist.append({"step": done, "t": run.t, "kinetic_energy": m["kinetic_energy"], "enstrophy": m["enstrophy"]})
+
+    sample()
+    while done < steps:
+        k = min(every, steps - done)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record(ext)
+        got = run.run(1e30, max_steps=k)
+        end.record(ext)
+        run.synchronize()
+        ms += start.elapsed_time(end)
+        assert got == k, f"{got} of {k} steps ran"
+        done += k
+        sample()
+    share = None
+    if sensor is not None:
+        lin, ev = run.sensor_counts()
+        share = lin / max(ev, 1)
+    U = run.state()
+    run.close()
+    return U, ms, hist, share
+
+
+def history_block(n, local, steps, every, world):
+    """The Taylor-Green vortex run `steps` steps in the three forms: the kinetic-energy and enstrophy histories of each,
+    the throughput of each over the run, and the distance of the mixed forms from the plain FP64 form at the last step."""
+    params, U0 = workload(n), tgv_state(n)
+    out = {"steps": steps, "monitor_every": every,
+           "monitor": "volume averages of 1/2 |m|^2 / rho and 1/2 |curl u|^2 (central differences over 2h, periodic), fvg_monitor's fast order"}
+    states = {}
+    for name, prec, sens in (("plain_fp64", 0, None), ("mixed", 1, None), ("mixed_learned", 1, load_sensor(local))):
+        U, ms, hist, share = history_run(params, U0, prec, local, steps, every, sens)
+        ms = allmax(ms, world)
+        states[name] = U
+        out[name] = {"value": world * n ** 3 * STAGES * steps / (ms * 1e-3), "ms_per_step": ms / steps, "history": hist}
+        if share is not None:
+            out[name]["linear_share_of_tile_axes"] = share
+    for name in ("mixed", "mixed_learned"):
+        out[name]["vs_fp64_at_last_step"] = l1_errors(states[name], states["plain_fp64"])
+        out[name]["kinetic_energy_rel_diff_at_last_step"] = (out[name]["history"][-1]["kinetic_energy"] /
+                                                             out["plain_fp64"]["history"][-1]["kinetic_energy"] - 1.0)
+        out[name]["enstrophy_rel_diff_at_last_step"] = (out[name]["history"][-1]["enstrophy"] / out["plain_fp64"]["history"][-1]["enstrophy"] - 1.0)
+    out["l1_rho_bar"] = 1e-4
+    out["l1_rho_within_bar"] = all(out[k]["vs_fp64_at_last_step"]["rho"]["l1_rel"] <= 1e-4 for k in ("mixed", "mixed_learned"))
+    return out
 
 
 def l1_errors(U, Uref):
@@ -606,10 +680,7 @@ def gpu_arm(args, world, rank, local):
             "ms_per_step": ms_l / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 stencil / f64 state (mixed form) with bf16 sensor; plain form f64",
             "data": "synthetic (Taylor-Green initial state computed in numpy)",
-            "config": {"workload": f"Taylor-Green vortex 3-D {n}^3, WENO5-Z + low-Mach HLLC + SSP-RK3, viscous Re 1600 Pr 0.71, CFL 0.5; "
-                                   "value: the mixed-precision form gated by the learned sensor; mixed: without the sensor; "
-                                   "plain_fp64: the reference's arithmetic",
-                       "cells": cells, "stages_per_step": STAGES,
+            "config": {"workload": tgv_workload(n), "cells": cells, "stages_per_step": STAGES,
                        "parallelism": f"replicas{world}" if world > 1 else "single GPU",
                        "l2": f"inputs larger than L2 ({cells * 40 / 1e6:.0f} MB per state field), no flush"},
             "accuracy": {"vs": f"plain FP64 form after {args.warmup + args.steps} steps from the same state (the value's form)", "fields": errs,
@@ -620,6 +691,7 @@ def gpu_arm(args, world, rank, local):
                       "accuracy_l1_rho": errs_m["rho"]["l1_rel"]},
             "sensor": {"threshold": sensor[1], "tile_axes_linear": lin, "tile_axes": ev, "linear_share": lin / max(ev, 1),
                        "refresh_every_steps": 5, "speedup_vs_mixed": value / value_m},
+            "form_of_value": "the mixed-precision form gated by the learned sensor; mixed: without the sensor; plain_fp64: the reference's arithmetic",
             "roofline": rl_l, "e2e": e2e, "gpu_launches": launches, "clocks": clk_l}
     return line
 
@@ -634,13 +706,16 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-baseline", type=int, default=1, help="time the reference on the host cores (rank 0, N = 1)")
     ap.add_argument("--parts", type=int, default=2, help="slab workload at N = 1: parts of the mesh in one process")
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "quadrants", "cylinder", "slab"],
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "tgv200", "batch", "quadrants", "cylinder", "slab"],
                     help="tgv: the 3-D Taylor-Green vortex (default); batch: 512 shock tubes in one persistent launch per stage; "
                          "quadrants: a seeded four-quadrant Riemann problem (--size cells per axis, default 2048 for it)")
     ap.add_argument("--seed", type=int, default=2048, help="seed of the quadrants workload")
     ap.add_argument("--cyl-nx", type=int, default=1600, help="cylinder workload: cells along x (y: 3/2 of it)")
     ap.add_argument("--cyl-steps", type=int, default=20000, help="cylinder workload: steps of each GPU form")
     ap.add_argument("--batch", type=int, default=1, help="with --workload tgv at N = 1: add the batched workload's figures")
+    ap.add_argument("--history-steps", type=int, default=200,
+                    help="with --workload tgv: add the kinetic-energy and enstrophy histories of a run of this many steps in each form (0: none)")
+    ap.add_argument("--monitor-every", type=int, default=10, help="steps between two monitor samples of the histories")
     args = ap.parse_args()
     world, rank, local = (1, 0, 0) if args.impl == "reference" and int(os.environ.get("WORLD_SIZE", "1")) == 1 else dist_setup()
     threads = len(os.sched_getaffinity(0))
@@ -663,8 +738,7 @@ def main():
         line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": done, "warmup": warm,
                 "ms_per_step": 1e3 * wall / done, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (the reference's taylor_green_3d profile)", "impl": "reference",
-                "config": {"workload": f"Taylor-Green vortex 3-D {args.size}^3, WENO5-Z + low-Mach HLLC + SSP-RK3, viscous Re 1600 Pr 0.71, "
-                                       f"CFL 0.5", "cells": args.size ** 3, "stages_per_step": STAGES},
+                "config": {"workload": tgv_workload(args.size), "cells": args.size ** 3, "stages_per_step": STAGES},
                 "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
                 "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -747,7 +821,25 @@ def main():
 
             dist.destroy_process_group()
         return
+    if args.workload == "tgv200":
+        hb = history_block(args.size, local, args.history_steps or 200, args.monitor_every, world)
+        m = hb["mixed_learned"]
+        line = {"metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world, "steps": hb["steps"], "warmup": 3,
+                "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 stencil / f64 state with bf16 sensor (value); plain form f64", "data": "synthetic (Taylor-Green initial state computed in numpy)",
+                "config": {"workload": tgv_workload(args.size) + f", {hb['steps']} steps", "cells": args.size ** 3, "stages_per_step": STAGES,
+                           "l2": f"inputs larger than L2 ({args.size ** 3 * 40 / 1e6:.0f} MB per state field), no flush"},
+                "form_of_value": "mixed-precision form gated by the learned sensor", "history": hb, "e2e": None, "gpu_launches": None}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
     line = gpu_arm(args, world, rank, local)
+    if args.history_steps > 0:
+        line["history"] = history_block(args.size, local, args.history_steps, args.monitor_every, world)
     if world == 1 and args.batch:
         line["batch"] = batch_arm(args, world, rank, local)
         line["batch"]["workload"] = BATCH_WORKLOAD

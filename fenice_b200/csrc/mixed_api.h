@@ -13,7 +13,7 @@ struct MixedStage {
     cudaError_t (*launch)(const StageArgs&, int, cudaStream_t) = nullptr;
 };
 // the mixed stage kernel for a 2-D or 3-D mesh, a reconstruction (MUSCL, WENO3-Z, WENO5-Z) and a Riemann solver; the
-// launch geometry is the FP64 stage kernel's (3-D: 8x8x8 tiles, 192 threads; 2-D: 16x15 tiles, 256 threads)
+// tiles are the FP64 stage kernel's (3-D: 8x8x8 cells, here 384 threads; 2-D: 16x15 cells, 256 threads)
 MixedStage mixed_stage(int dim, int recon, int riemann, bool full);
 // the mixed WENO5-Z stage kernel with the learned troubled-cell sensor choosing linear or WENO5-Z reconstructions
 // (StageArgs::sens_flags)

@@ -230,6 +230,92 @@ __global__ void k_source_field(Mesh m, ExprArgs x, const Ctl* c, const int* gate
     }
 }
 
+// ---- the monitor (fvg_monitor): volume averages of rho, the kinetic energy and rho E, and the enstrophy
+// Simulation::volume_averages (cpp/src/SimulationRun.cpp:44-64) in its own order: one thread adds the cells in cell order,
+// kinetic energy 0.5 (m_x^2 + m_y^2 + m_z^2) / rho (m_z = +0 on a 2-D mesh, whose terms are exact zeros), then each sum / n
+__global__ void k_monitor_seq(const double* __restrict__ U, long long plane, long long n, int nvar, double* out) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (long long c = 0; c < n; ++c) {
+        const double r = U[c], mx = U[plane + c], my = U[2 * plane + c], e = U[3 * plane + c];
+        const double mz = nvar == 5 ? U[4 * plane + c] : 0.0;
+        s0 += r;
+        s1 += 0.5 * (mx * mx + my * my + mz * mz) / r;
+        s2 += e;
+    }
+    out[0] = s0 / (double)n;
+    out[1] = s1 / (double)n;
+    out[2] = s2 / (double)n;
+}
+
+// the velocity component q (1, 2 or 4: u, v, w) of cell (i, j, k), and its central difference along axis d: (f(+1) - f(-1))
+// / (2 h), wrapped across a periodic axis, one-sided (over h) at the two ends of any other axis
+__device__ __forceinline__ double mon_vel(const double* __restrict__ U, const Mesh& m, int q, int i, int j, int k) {
+    const long long c = ((long long)k * m.ny + j) * m.nx + i;
+    return U[q * m.plane + c] / U[c];
+}
+__device__ __forceinline__ double mon_diff(const double* __restrict__ U, const Mesh& m, const int* periodic, int q, int d, int i, int j, int k) {
+    const int n3[3] = {m.nx, m.ny, m.nz};
+    const double h = d == 0 ? m.dx : (d == 1 ? m.dy : m.dz);
+    int lo[3] = {i, j, k}, hi[3] = {i, j, k};
+    lo[d] -= 1;
+    hi[d] += 1;
+    double span = 2.0;
+    if (periodic[d]) {
+        lo[d] = (lo[d] + n3[d]) % n3[d];
+        hi[d] = hi[d] % n3[d];
+    } else {
+        if (lo[d] < 0) lo[d] = 0, span -= 1.0;
+        if (hi[d] >= n3[d]) hi[d] = n3[d] - 1, span -= 1.0;
+        if (span <= 0.0) return 0.0;
+    }
+    return (mon_vel(U, m, q, hi[0], hi[1], hi[2]) - mon_vel(U, m, q, lo[0], lo[1], lo[2])) / (span * h);
+}
+
+// per CTA: the sums of rho, the kinetic energy, rho E and 1/2 |curl u|^2 over a grid-stride share of the cells (one
+// thread's cells in order, then the CTA's threads in a fixed tree: deterministic); partial[4 * blockIdx.x + q]
+template <int NT>
+__global__ void __launch_bounds__(NT) k_monitor_cells(Mesh m, const double* __restrict__ U, int nvar, int per0, int per1, int per2, double* partial) {
+    __shared__ double red[4][NT];
+    const int periodic[3] = {per0, per1, per2};
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (long long c = blockIdx.x * (long long)NT + threadIdx.x; c < m.ncells; c += (long long)gridDim.x * NT) {
+        const int i = (int)(c % m.nx), j = (int)((c / m.nx) % m.ny), k = (int)(c / ((long long)m.nx * m.ny));
+        const double r = U[c], mx = U[m.plane + c], my = U[2 * m.plane + c], e = U[3 * m.plane + c];
+        const double mz = nvar == 5 ? U[4 * m.plane + c] : 0.0;
+        s[0] += r;
+        s[1] += 0.5 * (mx * mx + my * my + mz * mz) / r;
+        s[2] += e;
+        // vorticity (w_x, w_y, w_z) = (dw/dy - dv/dz, du/dz - dw/dx, dv/dx - du/dy); a 2-D mesh has w_z only
+        const double wz = mon_diff(U, m, periodic, 2, 0, i, j, k) - mon_diff(U, m, periodic, 1, 1, i, j, k);
+        double w2 = wz * wz;
+        if (nvar == 5) {
+            const double wx = mon_diff(U, m, periodic, 4, 1, i, j, k) - mon_diff(U, m, periodic, 2, 2, i, j, k);
+            const double wy = mon_diff(U, m, periodic, 1, 2, i, j, k) - mon_diff(U, m, periodic, 4, 0, i, j, k);
+            w2 = wx * wx + wy * wy + w2;
+        }
+        s[3] += 0.5 * w2;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) red[q][threadIdx.x] = s[q];
+    __syncthreads();
+    for (int w = NT / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) partial[4 * blockIdx.x + threadIdx.x] = red[threadIdx.x][0];
+}
+// the CTAs' partial sums in CTA order, then / n; order 1 also takes the three volume averages from them (else k_monitor_seq
+// has written them)
+__global__ void k_monitor_final(const double* partial, int nblocks, long long n, int all, double* out) {
+    if (threadIdx.x != 0) return;
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int b = 0; b < nblocks; ++b)
+        for (int q = 0; q < 4; ++q) s[q] += partial[4 * b + q];
+    for (int q = all ? 0 : 3; q < 4; ++q) out[q] = s[q] / (double)n;
+}
+
 // ---- parts of a slab-decomposed mesh
 // the largest of a stage's per-CTA speeds (and viscous bounds) into a slot the hosts all-reduce (0 when the gate is off)
 __global__ void k_part_local(const int* gate, const double* bm, int nb, const double* bmv, int nbv, double* out) {
@@ -429,7 +515,9 @@ __global__ void k_body_loads(const int* gate, const double* R, const double* U, 
 }
 
 template <int DIM> struct Tile;
-template <> struct Tile<3> { static constexpr int X = 8, Y = 8, Z = 8, NT = 192; };
+// 3-D: 256 threads per 8x8x8 tile, two CTAs per SM (at most 120 registers, 101 KB of shared memory): 16 warps per SM;
+// measured at 256^3 (WENO5-Z, low-Mach HLLC): 11.07 ms per launch against 12.60 with 192 threads, the same bits
+template <> struct Tile<3> { static constexpr int X = 8, Y = 8, Z = 8, NT = 256; };
 template <> struct Tile<2> { static constexpr int X = 16, Y = 15, Z = 1, NT = 256; };
 
 // Each kernel gets its shared-memory limit raised once, when a run is created (never during a graph capture).
@@ -471,11 +559,14 @@ template <int DIM> StageLauncher stage_launcher(int recon, int riemann, bool ful
     return full ? stage_launcher_f<DIM, true>(recon, riemann) : stage_launcher_f<DIM, false>(recon, riemann);
 }
 
+// the 3-D viscous sweep: 8x8x8 tiles, 384 threads (two CTAs per SM by shared memory, 24 warps; 3.13 ms per launch at
+// 256^3 against 4.76 with 192 threads, the same bits)
+constexpr int kViscNT = 384;
 cudaError_t prepare_viscous() {
-    return cudaFuncSetAttribute(viscous_kernel<8, 8, 8, 192>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ViscShape<8, 8, 8>::SMEM_BYTES);
+    return cudaFuncSetAttribute(viscous_kernel<8, 8, 8, kViscNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ViscShape<8, 8, 8>::SMEM_BYTES);
 }
 cudaError_t launch_viscous(const ViscArgs& a, int nblocks, cudaStream_t s) {
-    viscous_kernel<8, 8, 8, 192><<<nblocks, 192, ViscShape<8, 8, 8>::SMEM_BYTES, s>>>(a);
+    viscous_kernel<8, 8, 8, kViscNT><<<nblocks, kViscNT, ViscShape<8, 8, 8>::SMEM_BYTES, s>>>(a);
     return cudaGetLastError();
 }
 // the 2-D sweep: 16 x 16 tiles, 256 threads (the mixed form uses it too: the FP32 viscous kernel is 3-D only)
@@ -595,6 +686,8 @@ struct fvg_run {
     } body;
     double cm0[2] = {0.0, 0.0};
     double* d_bload = nullptr;
+    // fvg_monitor: per-CTA partial sums (4 per CTA) and the four results (allocated at the first call)
+    double* d_mon = nullptr;
     // a section body: its vertices where it was placed at t = 0 (the reference the poses turn about the pivot), and how far
     // a vertex lies from the pivot (ImmersedBoundary::enable_motion's reach)
     std::vector<double> ref_poly;
@@ -2093,7 +2186,7 @@ int fvg_destroy(fvg_run* run) {
     if (run->sens_tiles) cudaFree(run->sens_tiles);
     for (void* p : {(void*)run->d_mask, (void*)run->d_slot, (void*)run->d_forced, (void*)run->d_ghost, (void*)run->d_img_cell, (void*)run->d_img_w,
                     (void*)run->d_ratio, (void*)run->d_gn, (void*)run->d_deep, (void*)run->d_solid, (void*)run->d_loads, (void*)run->d_gvel,
-                    (void*)run->d_dvel, (void*)run->d_bload, (void*)run->d_span})
+                    (void*)run->d_dvel, (void*)run->d_bload, (void*)run->d_span, (void*)run->d_mon})
         if (p) cudaFree(p);
     for (cudaEvent_t e : run->ev_host) cudaEventDestroy(e);
     if (run->xfer) cudaStreamDestroy(run->xfer);
@@ -2815,6 +2908,27 @@ int fvg_ibm_loads(fvg_run* run, double* loads) {
     loads[3] = qA > 0 ? h[0] / qA : 0.0;
     loads[4] = qA > 0 ? h[1] / qA : 0.0;
     loads[5] = qA > 0 ? -h[2] / (qA * L) : 0.0;
+    return FVG_OK;
+}
+
+// the monitor's volume averages and the enstrophy of the run's current state (fvg_monitor, include/fenice_gpu.h)
+constexpr int kMonBlocks = 148 * 4, kMonNT = 256;
+int fvg_monitor(fvg_run* run, int order, double* out) {
+    if (!run || !out || (order != 0 && order != 1)) return FVG_ERR_ARGUMENT;
+    if (run->is_part) return fail(run, FVG_ERR_CONFIG, "fvg_monitor takes a whole mesh: join the parts' states for a decomposed run");
+    CK(cudaSetDevice(run->cfg.device));
+    if (!run->d_mon) CK(cudaMalloc(&run->d_mon, sizeof(double) * (4 * kMonBlocks + 4)));
+    double* res = run->d_mon + 4 * kMonBlocks;
+    const double* U = run->Ucur();
+    const fvg_config& c = run->cfg;
+    int per[3];
+    for (int d = 0; d < 3; ++d) per[d] = c.bc[2 * d] == FVG_BC_PERIODIC && c.bc[2 * d + 1] == FVG_BC_PERIODIC;
+    if (order == 0) k_monitor_seq<<<1, 1, 0, run->stream>>>(U, run->m.plane, run->m.ncells, run->nvar, res);
+    k_monitor_cells<kMonNT><<<kMonBlocks, kMonNT, 0, run->stream>>>(run->m, U, run->nvar, per[0], per[1], per[2], run->d_mon);
+    k_monitor_final<<<1, 32, 0, run->stream>>>(run->d_mon, kMonBlocks, run->m.ncells, order == 1, res);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, res, sizeof(double) * 4, cudaMemcpyDeviceToHost, run->stream));
+    CK(cudaStreamSynchronize(run->stream));
     return FVG_OK;
 }
 

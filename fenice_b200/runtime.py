@@ -34,7 +34,7 @@ EXPORTS = ["fvg_abi_version", "fvg_create", "fvg_destroy", "fvg_last_error", "fv
            "fvg_batch_download", "fvg_batch_run", "fvg_batch_problem", "fvg_batch_autotune", "fvg_batch_set_schedule",
            "fvg_batch_get_schedule", "fvg_batch_stream", "fvg_batch_set_timing", "fvg_batch_get_timing",
            "fvg_sensor_sizes", "fvg_sensor_extract", "fvg_sensor_grad", "fvg_sensor_adam", "fvg_sensor_pack", "fvg_sensor_infer",
-           "fvg_set_sensor", "fvg_get_sensor_counts", "fvg_get_sensor_gate", "fvg_ibm_loads",
+           "fvg_set_sensor", "fvg_get_sensor_counts", "fvg_get_sensor_gate", "fvg_ibm_loads", "fvg_monitor",
            "fvg_create_part", "fvg_part_info", "fvg_part_buffers", "fvg_part_begin", "fvg_part_phase", "fvg_part_status",
            "fvg_expr_eval"]
 
@@ -106,6 +106,7 @@ def load_library(path=LIB_PATH):
     lib.fvg_get_sensor_counts.argtypes = [c_p, ll, ll, ctypes.c_int]
     lib.fvg_get_sensor_gate.argtypes = [c_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     lib.fvg_ibm_loads.argtypes = [c_p, dp]
+    lib.fvg_monitor.argtypes = [c_p, ctypes.c_int, dp]
     ip = ctypes.POINTER(ctypes.c_int)
     dpp = ctypes.POINTER(dp)
     lib.fvg_create_part.argtypes = [ctypes.POINTER(P.FvgConfig), ctypes.c_int, ctypes.c_int, ctypes.POINTER(c_p)]
@@ -299,6 +300,14 @@ class Run:
         v = (ctypes.c_double * 6)()
         self._check(self.lib.fvg_ibm_loads(self.h, v), "ibm_loads")
         return dict(zip(["Fx", "Fy", "Mz", "Cd", "Cl", "Cm"], list(v)))
+
+    def monitor(self, order="reference"):
+        """{mass, kinetic_energy, total_energy, enstrophy} of the current state (fvg_monitor): the volume averages of the
+        reference's monitor file and 1/2 <|curl u|^2>. order "reference": its summation order (its bits; one device
+        thread), "fast": a fixed parallel order (within rounding of it)."""
+        v = (ctypes.c_double * 4)()
+        self._check(self.lib.fvg_monitor(self.h, 0 if order == "reference" else 1, v), "monitor")
+        return dict(zip(["mass", "kinetic_energy", "total_energy", "enstrophy"], list(v)))
 
     def set_sensor(self, sensor, threshold=0.0, every=0, radius=-1):
         """Gate the WENO5-Z reconstructions (mixed precision) with a trained ``fenice_b200.sensor.Sensor`` (None: off),

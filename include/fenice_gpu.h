@@ -224,6 +224,17 @@ int fvg_get_timing(const fvg_run* run, double* stage_ms, long long* stage_launch
  * on 1/2 rho_in u_in^2 A (A = the diameter in 2-D, pi r^2 for a sphere, diameter x Lz for a 3-D cylinder). */
 int fvg_ibm_loads(fvg_run* run, double* loads);
 
+/* The monitor of the run's current state: out[4] = {mass, kinetic_energy, total_energy, enstrophy}. The first three are
+ * the volume averages of rho, 1/2 |m|^2 / rho and rho E that the reference writes in its monitor file
+ * (Simulation::volume_averages and monitor_row, cpp/src/SimulationRun.cpp:44-64, 87-90). order 0 adds the cells in the
+ * reference's order (one device thread, cell by cell: its bits; about 5 ns per cell), order 1 in a fixed parallel
+ * order (CTA sums in a tree, then the CTAs in order: deterministic, within rounding of the reference's). The enstrophy
+ * (no counterpart in the solver; the definition of the reference's validation scripts, cases/validation/benchmarks/
+ * spectra_application.py:61-67) is 1/2 the volume average of |curl u|^2, u = m / rho, with central differences over 2h,
+ * wrapped across a periodic axis and one-sided at the ends of any other; w_z only on a 2-D mesh. A part of a decomposed
+ * mesh is refused (its ghost planes are not the current state after a step). */
+int fvg_monitor(fvg_run* run, int order, double* out);
+
 /* Face fluxes of n face pairs (UL, UR: n x 5 doubles, axis: n ints) on the device with the run's EOS and Riemann
  * solver (RiemannSolver::face_flux, cpp/src/Schemes.cpp:202-229): F (n x 5) and the wave speeds (n). */
 int fvg_face_flux_batch(fvg_run* run, const double* UL, const double* UR, const int* axis, size_t n, double* F, double* smax);

@@ -213,6 +213,41 @@ def fingerprint(F, smax):
     return h
 
 
+def enstrophy(U, shape, lengths, periodic):
+    """1/2 the volume average of |curl u|^2, u = m / rho, with central differences over 2h: the definition of the
+    reference's validation scripts (fd_enstrophy, cases/validation/benchmarks/spectra_application.py:61-67: np.roll on a
+    periodic box), one-sided over h at the two ends of an axis that is not periodic (as fvg_monitor). shape = (nx, ny, nz),
+    lengths = (Lx, Ly, Lz), periodic = three booleans; a mesh with nz = 1 has w_z only."""
+    nx, ny, nz = shape
+    rho = U[:, 0].reshape(nz, ny, nx)
+    vel = [U[:, q].reshape(nz, ny, nx) / rho for q in (1, 2, 4)]
+    hs = [lengths[0] / nx, lengths[1] / ny, lengths[2] / nz]
+
+    def d(f, axis):   # axis 0 = x, 1 = y, 2 = z (numpy axes 2, 1, 0)
+        ax, h = 2 - axis, hs[axis]
+        if periodic[axis]:
+            return (np.roll(f, -1, ax) - np.roll(f, 1, ax)) / (2 * h)
+        n = f.shape[ax]
+        if n == 1:
+            return np.zeros_like(f)
+        hi = np.take(f, np.minimum(np.arange(n) + 1, n - 1), axis=ax)
+        lo = np.take(f, np.maximum(np.arange(n) - 1, 0), axis=ax)
+        span = np.full(n, 2.0)
+        span[0] -= 1.0
+        span[-1] -= 1.0
+        sh = [1, 1, 1]
+        sh[ax] = n
+        return (hi - lo) / (span.reshape(sh) * h)
+
+    u, v, w = vel
+    wz = d(v, 0) - d(u, 1)
+    if nz == 1:
+        return 0.5 * float(np.mean(wz * wz))
+    wx = d(w, 1) - d(v, 2)
+    wy = d(u, 2) - d(w, 0)
+    return 0.5 * float(np.mean(wx * wx + wy * wy + wz * wz))
+
+
 def ref_available():
     return os.path.exists(REF_SO)
 
@@ -248,6 +283,7 @@ class Reference:
             lib.ref_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, P(ctypes.c_double), P(ctypes.c_double)]
             lib.ref_solid_mask.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
             lib.ref_ibm_loads.argtypes = [ctypes.c_void_p, P(ctypes.c_double)]
+            lib.ref_volume_averages.argtypes = [ctypes.c_void_p, P(ctypes.c_double)]
             cls._lib = lib
         return cls._lib
 
@@ -320,6 +356,12 @@ class Reference:
         if n < 0:
             return None
         return np.frombuffer(m.raw, dtype=np.int8).copy()
+
+    def volume_averages(self):
+        """The monitor's {mass, kinetic energy, total energy} of the current state (Simulation::volume_averages)."""
+        v = (ctypes.c_double * 3)()
+        self.lib().ref_volume_averages(self.h, v)
+        return list(v)
 
     def ibm_loads(self):
         """{Fx, Fy, Mz} of the immersed body from a residual of the current state (Simulation::ibm_loads)."""

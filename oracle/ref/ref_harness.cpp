@@ -231,4 +231,15 @@ int ref_ibm_loads(void* h, double* loads) {
     }
 }
 
+// The monitor's volume averages {mass, kinetic energy, total energy} of the current state (Simulation::volume_averages
+// over every cell, as the serial time loop's monitor row takes them).
+int ref_volume_averages(void* h, double* out) {
+    auto* r = static_cast<RefRun*>(h);
+    const std::array<double, 3> v = r->sim.volume_averages(r->sim.U, static_cast<long long>(r->sim.U.size()));
+    out[0] = v[0];
+    out[1] = v[1];
+    out[2] = v[2];
+    return 0;
+}
+
 }   // extern "C"

@@ -10,13 +10,14 @@ Bounds, relative to the sum over the cells of |rho|, of |rho E| and, for every m
 magnitude (a component whose total starts at 0, such as the Taylor-Green rho w, is measured against the momentum scale):
 - plain FP64: 1e-13 (each stage rounds per cell at about 1e-16 of |U|; the sum of N such errors is ~ sqrt(N) of one;
   measured 3e-15 after 50 steps);
-- mixed and gated: 1e-9. The per-cell flux differences and their balance are rounded in FP32 (6e-8 of each difference)
-  before the FP64 update. In smooth flow the differences are O(h) of the fluxes and the totals drift by ~1e-12 after 50
-  steps; across a jump a difference is O(1) of the flux, and the cells at the jumps of these boxes drift the totals by
-  ~1e-10 (measured up to 1.5e-10 after 50 steps, mixed and gated alike).
-A seam face solved differently by two tiles moves the totals by the difference of two reconstructions at every stage,
-orders of magnitude above these bounds. The totals are taken with math.fsum (exactly rounded), so the check sees the
-solver's drift only.
+- mixed and gated: the per-cell flux differences and their balance are rounded in FP32 (6e-8 of each difference) before
+  the FP64 update. In smooth flow the differences are O(h) of the fluxes: bound 2e-11 on the Taylor-Green boxes (measured
+  up to 4e-12 after 50 steps). Across a jump a difference is O(1) of the flux: bound 5e-10 on the jump boxes (measured up
+  to 1.5e-10, mixed and gated alike).
+A seam face solved differently by the two tiles that share it (a linear reconstruction on one side, WENO5-Z on the other)
+moves the totals by the difference of the two reconstructions at every stage: measured with such a kernel, 1e-10 to
+1e-9 on the Taylor-Green boxes and 1.4e-9 to 4.1e-9 on the jump boxes, beyond both bounds. The totals are taken with
+math.fsum (exactly rounded), so the check sees the solver's drift only.
 """
 import math
 import os
@@ -31,7 +32,9 @@ pytestmark = pytest.mark.gpu
 
 HERE = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 STEPS = 50
-BOUND = {"plain": 1e-13, "mixed": 1e-9, "gated": 1e-9}
+# (form, smooth flow) -> bound on the relative drift of every total
+BOUND = {("plain", True): 1e-13, ("plain", False): 1e-13, ("mixed", True): 2e-11, ("mixed", False): 5e-10, ("gated", True): 2e-11,
+         ("gated", False): 5e-10}
 
 
 def totals(U):
@@ -97,5 +100,5 @@ def test_totals_conserved(name, make, form):
         # the check needs seams between linear and WENO5-Z tiles
         assert 0 < lin < ev
     print(msg)
-    assert np.all(drift <= BOUND[form]), drift
+    assert np.all(drift <= BOUND[(form, name.startswith("tgv"))]), drift
     run.close()
