@@ -12,7 +12,8 @@ One JSON line on rank 0. `value` is timed on the device with CUDA events on the 
 `e2e` goes through the public API per step with the state copied from pinned host memory and the result read back;
 `roofline` relates the stage kernel's algorithmic bytes to its measured duration; `cpu_baseline` times the reference
 solver (compiled from its sources, oracle/_ref) on this machine's host cores on a bounded sample of the same workload.
-Under torchrun (N > 1) every rank runs its own replica of the workload (weak scaling, no exchange between ranks).
+Under torchrun (N > 1) the workload is slab-decomposed: one 256^3 part per rank of a 256 x 256 x 256 N mesh, the
+interface planes and wave speeds exchanged over NCCL (weak scaling).
 """
 import argparse
 import json
@@ -623,9 +624,78 @@ def slab_arm(args, world, rank, local):
     return out
 
 
+def dist_gpu_arm(args, world, rank, local):
+    """N > 1: the workload slab-decomposed along z, one n^3 part per GPU of an n x n x (n N) periodic mesh (weak
+    scaling; every part starts from the Taylor-Green box, so the mesh is N boxes along z), the interface planes and the
+    speeds exchanged over NCCL on each part's stream (fenice_b200.slabs.DistExchange). The three forms, each W steps
+    untimed then K steps timed with CUDA events on the part's stream, the time the slowest rank's."""
+    import torch
+
+    from fenice_b200 import slabs
+
+    n = args.size
+    params = dict(workload(n), nz=n * world, Lz=2 * math.pi * world)
+    U0 = tgv_state(n)
+    sensor = load_sensor(local)
+    out = {}
+    for name, prec, sens in (("plain_fp64", 0, None), ("mixed", 1, None), ("mixed_learned", 1, sensor)):
+        part = slabs.Part(params, world, rank, U=U0, precision=prec, device=local)
+        if sens:
+            part.set_sensor(*sens)
+        ex = slabs.DistExchange.for_part(part)
+        slabs.advance([part], ex, 1e30, args.warmup)
+        st = torch.cuda.ExternalStream(part.stream(), device=torch.device("cuda", local))
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        barrier(world)
+        with Clocks(local) as clk:
+            start.record(st)
+            steps, _ = slabs.advance([part], ex, 1e30, args.steps, check_every=args.steps)
+            end.record(st)
+            torch.cuda.synchronize()
+        barrier(world)
+        ms = allmax(start.elapsed_time(end), world)
+        out[name] = {"value": world * n ** 3 * STAGES * steps / (ms * 1e-3), "ms_per_step": ms / steps, "steps": steps, "clocks": clk.summary()}
+        if sens:
+            lin, ev = part.sensor_counts()
+            out[name]["linear_share_of_tile_axes"] = lin / max(ev, 1)
+        if sens and args.e2e_steps > 0:
+            # end to end through the public API: every step each rank's part state comes from pinned host memory and goes
+            # back there (Part.set_state / advance / Part.state: the copies not overlapped with the step)
+            host = torch.empty((n ** 3, 5), dtype=torch.float64, pin_memory=True).numpy()
+            host[:] = part.state()
+            barrier(world)
+            t0 = time.perf_counter()
+            for _ in range(args.e2e_steps):
+                part.set_state(host)
+                slabs.advance([part], ex, 1e30, 1)
+                part.state(out=host)
+            wall = allmax(time.perf_counter() - t0, world)
+            out["e2e"] = {"value": world * n ** 3 * STAGES * args.e2e_steps / wall, "unit": UNIT, "h2d_bytes_per_step": world * n ** 3 * 40,
+                          "d2h_bytes_per_step": world * n ** 3 * 40, "steps": args.e2e_steps,
+                          "timing": "host wall clock: every rank's part state in from pinned host memory, one step, out again"}
+        part.close()
+    m = out["mixed_learned"]
+    # per RK3 step: 3 stage + 3 viscous + 6 pack / unpack + 3 local maxima + dt + axpy + 2 stage speeds + end, the
+    # sensor's refresh (network + 2 gate passes) on every step (the kernels return at once off the refresh steps)
+    launches = args.steps * (3 + 3 + 6 + 3 + 1 + 1 + 2 + 1 + 3)
+    return {"metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world, "steps": m["steps"], "warmup": args.warmup,
+            "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 stencil / f64 state (mixed form) with bf16 sensor; plain form f64",
+            "data": "synthetic (Taylor-Green initial state computed in numpy)",
+            "config": {"workload": tgv_workload(n), "cells": n ** 3 * world, "stages_per_step": STAGES,
+                       "mesh": f"{n} x {n} x {n * world}, one {n}^3 part per GPU",
+                       "parallelism": f"slab decomposition along z, {world} parts, NCCL halo exchange and speed all-reduce",
+                       "l2": f"inputs larger than L2 ({n ** 3 * 40 / 1e6:.0f} MB per state field and GPU), no flush"},
+            "form_of_value": "the mixed-precision form gated by the learned sensor, decomposed (tile rows next to an interface stay WENO5-Z)",
+            "forms": out, "e2e": out.pop("e2e", None), "gpu_launches": launches, "clocks": m["clocks"]}
+
+
 def gpu_arm(args, world, rank, local):
     import torch
 
+    if world > 1:
+        return dist_gpu_arm(args, world, rank, local)
     n = args.size
     cells = n ** 3
     params = workload(n)
@@ -838,7 +908,7 @@ def main():
             dist.destroy_process_group()
         return
     line = gpu_arm(args, world, rank, local)
-    if args.history_steps > 0:
+    if args.history_steps > 0 and world == 1:
         line["history"] = history_block(args.size, local, args.history_steps, args.monitor_every, world)
     if world == 1 and args.batch:
         line["batch"] = batch_arm(args, world, rank, local)

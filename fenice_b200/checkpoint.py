@@ -9,6 +9,8 @@ Checkpoint (Simulation::checkpoint_header / save_checkpoint / load_checkpoint, c
   S               float64 scalar, the MUSCL-Hancock lagged wave speed (only when the scheme has one > 0)
   collection_time, collection_file   float64 (n,) and <U (n,): the output index of the run (empty here)
   U               float64 (ncells, 4) on a 2-D mesh (rho w left out), (ncells, 5) in 3-D, the reference's cell order
+  body_pose       float64 (10, 13, 14 or 21,): a moving immersed body's pose and state (Simulation::body_checkpoint,
+                  SimulationRestart.cpp:87-97; only for a run with a moving body, which refuses a file without it, :103)
 written to <path>_tmp.npz and renamed over the file, as the reference does. An adaptive (AMR) checkpoint (leaf_level ...)
 is refused.
 
@@ -32,9 +34,10 @@ def _write(path, arrays):
     os.replace(tmp, path)
 
 
-def checkpoint_arrays(U, t, step, params, lagged_speed=0.0, collection=()):
+def checkpoint_arrays(U, t, step, params, lagged_speed=0.0, collection=(), body_pose=None):
     """The arrays of a checkpoint (checkpoint_header + U): U of 5 columns per cell (rho w dropped on a 2-D mesh), the
-    resolved parameters of the run (nx .. Lz), the MUSCL-Hancock lagged speed (written when > 0), the output index."""
+    resolved parameters of the run (nx .. Lz), the MUSCL-Hancock lagged speed (written when > 0), the output index, the
+    moving body's body_pose (when given)."""
     nx, ny, nz = int(params["nx"]), int(params["ny"]), int(params.get("nz", 1))
     times = np.array([float(tc) for tc, _ in collection], dtype=np.float64)
     files = [str(f) for _, f in collection]
@@ -46,6 +49,8 @@ def checkpoint_arrays(U, t, step, params, lagged_speed=0.0, collection=()):
              Ly=np.array(float(params["Ly"]), dtype=np.float64), nz=np.array(nz, dtype=np.int64), Lz=np.array(float(params["Lz"]), dtype=np.float64),
              collection_time=times, collection_file=np.array(files, dtype=f"<U{max([1] + [len(f) for f in files])}"),
              U=np.ascontiguousarray(np.asarray(U, dtype=np.float64)[:, :5 if nz > 1 else 4]))
+    if body_pose is not None:
+        a["body_pose"] = np.ascontiguousarray(np.asarray(body_pose, dtype=np.float64).ravel())
     return a
 
 
@@ -55,9 +60,10 @@ def write_checkpoint(path, arrays):
 
 
 def save_checkpoint(path, run, step, collection=()):
-    """Writes the run's state, time and step (and, for MUSCL-Hancock, its lagged speed) as the reference's checkpoint."""
+    """Writes the run's state, time and step (and, for MUSCL-Hancock, its lagged speed; for a moving body, its pose) as
+    the reference's checkpoint."""
     s = run.lagged_speed if run.cfg.time_scheme == 3 else 0.0
-    _write(path, checkpoint_arrays(run.state(), run.t, step, run.params, s, collection))
+    _write(path, checkpoint_arrays(run.state(), run.t, step, run.params, s, collection, run.body_state))
 
 
 def read_checkpoint(path):
@@ -92,10 +98,15 @@ def load_checkpoint(path, run):
         raise ValueError(f"The checkpoint {path} holds {U.shape[0]} cells, the run {run.ncells}")
     full = np.zeros((run.ncells, 5))
     full[:, :U.shape[1]] = U
+    moving = run.body_state is not None
+    if moving and "body_pose" not in a:   # SimulationRestart.cpp:103
+        raise ValueError(f"The checkpoint {path} has no pose of the moving body: it is from a static run")
     run.set_state(full)
     run.t = float(a["t"])
     if run.cfg.time_scheme == 3:
         run.lagged_speed = float(a["S"]) if "S" in a else 0.0
+    if moving:
+        run.body_state = np.asarray(a["body_pose"], dtype=np.float64)
     return int(a["step"])
 
 

@@ -1123,9 +1123,12 @@ cudaError_t refresh_gate(fvg_run* r, const double* Uin, const Ctl* ctl) {
     if (!r->sens) return cudaSuccess;
     int per[3];
     for (int d = 0; d < 3; ++d) per[d] = r->cfg.bc[2 * d] == FVG_BC_PERIODIC && r->cfg.bc[2 * d + 1] == FVG_BC_PERIODIC;
+    // a part: its split axis does not wrap (beyond an interface lie the neighbour's cells, whose flags are not held here)
+    const bool interfaces = r->is_part && (r->peer[0] || r->peer[1]);
+    if (interfaces) per[r->split] = 0;
     const int tile[3] = {r->dim == 3 ? Tile<3>::X : Tile<2>::X, r->dim == 3 ? Tile<3>::Y : Tile<2>::Y, r->dim == 3 ? Tile<3>::Z : 1};
     return sensor_refresh(r->m, r->bc, r->eos, r->dim, Uin, r->sens, r->sens_theta, r->sens_radius, per, r->sens_flags, r->sens_flags + (size_t)r->m.plane * r->dim, tile,
-                          r->tiles, r->sens_tiles, ctl, r->sens_every, r->sens_count, r->stream);
+                          r->tiles, r->sens_tiles, ctl, r->sens_every, r->sens_count, r->stream, interfaces ? r->split : -1, r->peer[0], r->peer[1]);
 }
 
 int axpy_blocks(const fvg_run* r) {
@@ -1347,8 +1350,9 @@ cudaError_t part_phase(fvg_run* r, int phase, int* comm, int* nred) {
         e = part_pack(r, r->U);
         *comm = 1;
         break;
-    case 1:   // stage 1 and its speed
+    case 1:   // the sensor's refresh on its steps (the state's ghost planes now current), stage 1 and its speed
         if ((e = part_unpack(r, r->U))) break;
+        if (r->sens && (e = refresh_gate(r, r->U, c))) break;
         if ((e = residual_stage(r, r->U, nullptr, r->R, kStoreR, 0, 0, 0, act))) break;
         e = part_local(r, act, r->bm[0], r->nb, r->bmv[0], nbv, 0);
         *comm = 2;
@@ -1788,6 +1792,26 @@ void advance_body(fvg_run* r, double dt) {
     b.dt = dt;
 }
 
+// The body's geometry at a pose (ImmersedBoundary::place_geometry and build_ghosts, Physics.cpp:1204-1212 and 1310-1334):
+// the shape moved by the pose's displacement (a section also turned about its pivot by the pose's angle), its mask and
+// ghost table built on the host into tb.
+int geometry_at(fvg_run* r, const fvg_run::Pose& pose, IbmGeom& g, IbmTable& tb) {
+    g = ibm_geom(r->cfg, r->cfg.ibm_cx + pose.x, r->cfg.ibm_cy + pose.y, r->cfg.ibm_cz + pose.z);
+    if (r->cfg.ibm_shape == 2) {   // the section turned about the pivot by the pose's angle and moved by its displacement
+        const double ca = std::cos(pose.angle), sa = std::sin(pose.angle), px = r->cfg.ibm_cx, py = r->cfg.ibm_cy;
+        std::vector<double> pts(r->ref_poly.size());
+        for (size_t q = 0; q < pts.size() / 2; ++q) {
+            const double rx = r->ref_poly[2 * q] - px, ry = r->ref_poly[2 * q + 1] - py;
+            pts[2 * q] = px + pose.x + ca * rx - sa * ry;
+            pts[2 * q + 1] = py + pose.y + sa * rx + ca * ry;
+        }
+        g.set_polygon(std::move(pts));
+    }
+    const std::string msg = build_ibm_geom(g, tb);
+    if (!msg.empty()) return fail(r, FVG_ERR_CONFIG, msg);
+    return FVG_OK;
+}
+
 // The body at the start of a step at time t (place_body and ImmersedBoundary::move_to, SimulationRun.cpp:379-384 and
 // Physics.cpp:1310-1334): the geometry follows the pose in steps of a quarter cell (then the ghost table is built again
 // and the cells the body left take the wall layer's state, fill_fresh); in between only the wall velocities change.
@@ -1801,20 +1825,9 @@ int place_body(fvg_run* r, double t) {
     if (shift <= 0.25 * h) return upload_velocities(r);
     const std::vector<unsigned char> old_mask = r->tab.mask;
     r->built = pose;
-    IbmGeom g = ibm_geom(r->cfg, r->cfg.ibm_cx + pose.x, r->cfg.ibm_cy + pose.y, r->cfg.ibm_cz + pose.z);
-    if (poly) {   // the section turned about the pivot by the pose's angle and moved by its displacement
-        const double ca = std::cos(pose.angle), sa = std::sin(pose.angle), px = r->cfg.ibm_cx, py = r->cfg.ibm_cy;
-        std::vector<double> pts(r->ref_poly.size());
-        for (size_t q = 0; q < pts.size() / 2; ++q) {
-            const double rx = r->ref_poly[2 * q] - px, ry = r->ref_poly[2 * q + 1] - py;
-            pts[2 * q] = px + pose.x + ca * rx - sa * ry;
-            pts[2 * q + 1] = py + pose.y + sa * rx + ca * ry;
-        }
-        g.set_polygon(std::move(pts));
-    }
+    IbmGeom g;
     IbmTable tb;
-    const std::string msg = build_ibm_geom(g, tb);
-    if (!msg.empty()) return fail(r, FVG_ERR_CONFIG, msg);
+    if (const int rc = geometry_at(r, pose, g, tb)) return rc;
     std::vector<int> cells;   // fresh: solid before, fluid now
     for (size_t c = 0; c < tb.mask.size(); ++c)
         if (old_mask[c] && !tb.mask[c]) cells.push_back((int)c);
@@ -2156,6 +2169,24 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
     }
     *out = run;
     return FVG_OK;
+}
+
+// The body_pose entries of the reference's checkpoint (Simulation::body_checkpoint, cpp/src/SimulationRestart.cpp:87-97):
+// the pose the geometry was built at (x, y, angle), the state of a body driven by the flow (x, y, u, v, ax, ay, dt: zeros
+// for a body in prescribed motion), on a 3-D mesh then (z of the geometry, z, w, az), with a driven rotation then (angle,
+// angular velocity, its last acceleration) and on a 3-D mesh the x and y components (omega_x, omega_y, their accelerations).
+std::vector<double> body_checkpoint(const fvg_run* r) {
+    if (!r->moving) return {};
+    const fvg_run::Pose& g = r->built;
+    const fvg_run::Body& b = r->body;
+    const bool d3 = r->dim == 3;
+    std::vector<double> v = {g.x, g.y, g.angle, b.x, b.y, b.u, b.v, b.ax, b.ay, b.dt};
+    if (d3) v.insert(v.end(), {g.z, b.z, b.w, b.az});
+    if (r->cfg.ibm_inertia > 0.0) {
+        v.insert(v.end(), {b.th, b.om, b.aom});
+        if (d3) v.insert(v.end(), {b.omx, b.omy, b.aomx, b.aomy});
+    }
+    return v;
 }
 
 }   // namespace
@@ -2806,7 +2837,6 @@ int fvg_get_timing(const fvg_run* run, double* stage_ms, long long* stage_launch
 
 int fvg_set_sensor(fvg_run* run, const void* weights, float threshold, int every, int radius) {
     if (!run) return FVG_ERR_ARGUMENT;
-    if (run->is_part) return fail(run, FVG_ERR_CONFIG, "the sensor's gate is not exchanged between parts of a decomposed mesh");
     CK(cudaSetDevice(run->cfg.device));
     CK(cudaStreamSynchronize(run->stream));
     for (int g = 0; g < 2; ++g)
@@ -2909,6 +2939,89 @@ int fvg_ibm_loads(fvg_run* run, double* loads) {
     loads[4] = qA > 0 ? h[1] / qA : 0.0;
     loads[5] = qA > 0 ? -h[2] / (qA * L) : 0.0;
     return FVG_OK;
+}
+
+int fvg_get_body_state(const fvg_run* run, double* v, int* n) {
+    if (!run || !n) return FVG_ERR_ARGUMENT;
+    const std::vector<double> b = body_checkpoint(run);
+    if (v) {
+        if (*n < (int)b.size()) return fail(const_cast<fvg_run*>(run), FVG_ERR_ARGUMENT, "the body state needs " + std::to_string(b.size()) + " doubles");
+        std::copy(b.begin(), b.end(), v);
+    }
+    *n = (int)b.size();
+    return FVG_OK;
+}
+
+// Simulation::restore_body_from_checkpoint and ImmersedBoundary::restore_geometry (cpp/src/SimulationRestart.cpp:99-160,
+// cpp/src/Physics.cpp:1204-1212): the body's state, and the geometry built at the checkpoint's pose with the wall
+// velocities of that moment (a body driven by the flow: its own; a prescribed one: the configured velocities and the
+// rotation of the run's time, which set it first). The next step places the body from there.
+int fvg_set_body_state(fvg_run* run, const double* v, int n) {
+    if (!run || (!v && n)) return FVG_ERR_ARGUMENT;
+    if (!run->moving) return fail(run, FVG_ERR_CONFIG, "the run has no moving body (a static body's checkpoint has no pose)");
+    const bool d3 = run->dim == 3, rot = run->cfg.ibm_inertia > 0.0;
+    const int want = (d3 ? 14 : 10) + (rot ? (d3 ? 7 : 3) : 0);
+    if (n != want)
+        return fail(run, FVG_ERR_ARGUMENT, "a malformed body pose: " + std::to_string(n) + " entries, this run's has " + std::to_string(want) +
+                                                  " (a 2-D pose for a 3-D run, or the reverse, or a driven rotation without its angular state)");
+    CK(cudaSetDevice(run->cfg.device));
+    Ctl h;
+    if (const int rc = read_ctl(run, &h)) return rc;
+    fvg_run::Pose g;
+    g.x = v[0];
+    g.y = v[1];
+    g.angle = v[2];
+    if (d3) g.z = v[10];
+    if (run->dynamic) {
+        fvg_run::Body& b = run->body;
+        b.x = v[3];
+        b.y = v[4];
+        b.u = v[5];
+        b.v = v[6];
+        b.ax = v[7];
+        b.ay = v[8];
+        b.dt = v[9];
+        if (d3) {
+            b.z = v[11];
+            b.w = v[12];
+            b.az = v[13];
+        }
+        if (rot) {
+            const int o = n - (d3 ? 7 : 3);
+            b.th = v[o];
+            b.om = v[o + 1];
+            b.aom = v[o + 2];
+            if (d3) {
+                b.omx = v[o + 3];
+                b.omy = v[o + 4];
+                b.aomx = v[o + 5];
+                b.aomy = v[o + 6];
+            }
+        }
+        g.u = b.u;
+        g.v = b.v;
+        g.w = d3 ? b.w : 0.0;
+        g.omega = rot ? b.om : 0.0;
+        g.omega_x = rot && d3 ? b.omx : 0.0;
+        g.omega_y = rot && d3 ? b.omy : 0.0;
+    } else {
+        const fvg_run::Pose now = prescribed_pose(run->cfg, h.t);
+        g.u = run->cfg.ibm_vx;
+        g.v = run->cfg.ibm_vy;
+        g.w = run->cfg.ibm_vz;
+        g.omega = now.omega;
+        g.omega_x = now.omega_x;
+        g.omega_y = now.omega_y;
+    }
+    IbmGeom geo;
+    IbmTable tb;
+    if (const int rc = geometry_at(run, g, geo, tb)) return rc;
+    run->tab = std::move(tb);
+    run->built = g;
+    run->pose = g;
+    CK(cudaStreamSynchronize(run->stream));
+    if (const int rc = upload_ibm(run)) return rc;
+    return upload_velocities(run);
 }
 
 // the monitor's volume averages and the enstrophy of the run's current state (fvg_monitor, include/fenice_gpu.h)

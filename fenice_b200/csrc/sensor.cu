@@ -428,7 +428,9 @@ __global__ void __launch_bounds__(256) k_sensor_flags_t(Mesh m, Bc bc, Eos<doubl
 // the extended tile is the OR over one box, the tile extended by radius + 1 cells along a and radius along the other axes,
 // each range wrapped across a periodic pair of sides and clipped at the others. A tile whose extension along a leaves the
 // mesh across a side that is not periodic stays WENO5-Z. The box is taken in two passes: k_gate_rows ORs every row of
-// cells over each tile column's x range, k_gate_tiles ORs those bytes over the tile's y and z ranges.
+// cells over each tile column's x range, k_gate_tiles ORs those bytes over the tile's y and z ranges. On a part of a
+// decomposed mesh (split >= 0) a tile whose box reaches an interface of the part along the split axis (radius + 1 cells)
+// stays WENO5-Z along every axis: the neighbour's flags are not held here, and both parts then solve an interface face alike.
 __device__ __forceinline__ int wrap_index(int q, int n) { return q >= 0 && q < n ? q : ((q % n) + n) % n; }
 
 // the box's range along axis d for a tile starting at o (inclusive; beyond a periodic side the indices wrap when read)
@@ -469,7 +471,8 @@ __global__ void k_gate_rows(Mesh m, const unsigned char* __restrict__ flags, int
 // out[a * ntiles + b] from the row bytes over the tile's y and z ranges, the edge rule; counts += [linear, all]
 template <int DIM>
 __global__ void k_gate_tiles(Mesh m, const unsigned char* __restrict__ rows, int TX, int TY, int TZ, int t0n, int t1n, int t2n, int per0, int per1,
-                             int per2, int radius, unsigned char* __restrict__ out, const Ctl* ctl, int every, unsigned long long* counts) {
+                             int per2, int radius, unsigned char* __restrict__ out, const Ctl* ctl, int every, unsigned long long* counts, int split,
+                             int peer_lo, int peer_hi) {
     if (!refresh_due(ctl, every)) return;
     const long long ntiles = (long long)t0n * t1n * t2n, total = DIM * ntiles;
     const int n3[3] = {m.nx, m.ny, m.nz}, per[3] = {per0, per1, per2};
@@ -483,6 +486,10 @@ __global__ void k_gate_tiles(Mesh m, const unsigned char* __restrict__ rows, int
         const int T3[3] = {TX, TY, TZ};
         const int ha = o[a] + T3[a] - 1 < n3[a] - 1 ? o[a] + T3[a] - 1 : n3[a] - 1;
         bool any = !per[a] && (o[a] - 1 < 0 || ha + 1 > n3[a] - 1);
+        if (split >= 0) {   // the box reaches an interface of this part
+            const int hs = o[split] + T3[split] - 1 < n3[split] - 1 ? o[split] + T3[split] - 1 : n3[split] - 1;
+            any = any || (peer_lo && o[split] - (radius + 1) < 0) || (peer_hi && hs + radius + 1 > n3[split] - 1);
+        }
         int lo1, hi1, lo2 = 0, hi2 = 0;
         gate_range(o[1], TY, n3[1], 1, a, radius, per[1] != 0, lo1, hi1);
         if (DIM == 3) gate_range(o[2], TZ, n3[2], 2, a, radius, per[2] != 0, lo2, hi2);
@@ -518,7 +525,7 @@ int grid_for(long long rows) {
 cudaError_t fvg::sensor_refresh(const Mesh& m, const Bc& bc, const Eos<double>& eos, int dim, const double* U, const void* weights, float theta,
                                 int radius, const int periodic[3], unsigned char* flags0, unsigned char* rows, const int tile[3],
                                 const int tiles[3], unsigned char* tile_flags, const Ctl* ctl, int every, unsigned long long* counts,
-                                cudaStream_t s) {
+                                cudaStream_t s, int split, int peer_lo, int peer_hi) {
     const SensorW* w = static_cast<const SensorW*>(weights);
     if (dim == 3) {
         const int b0 = (m.nx + 7) / 8, b1 = (m.ny + 7) / 8, b2 = (m.nz + 3) / 4;
@@ -534,11 +541,11 @@ cudaError_t fvg::sensor_refresh(const Mesh& m, const Bc& bc, const Eos<double>& 
     if (dim == 3) {
         k_gate_rows<3><<<rb, 256, 0, s>>>(m, flags0, tile[0], tiles[0], periodic[0], radius, rows, ctl, every);
         k_gate_tiles<3><<<tb, 256, 0, s>>>(m, rows, tile[0], tile[1], tile[2], tiles[0], tiles[1], tiles[2], periodic[0], periodic[1], periodic[2], radius,
-                                           tile_flags, ctl, every, counts);
+                                           tile_flags, ctl, every, counts, split, peer_lo, peer_hi);
     } else {
         k_gate_rows<2><<<rb, 256, 0, s>>>(m, flags0, tile[0], tiles[0], periodic[0], radius, rows, ctl, every);
         k_gate_tiles<2><<<tb, 256, 0, s>>>(m, rows, tile[0], tile[1], 1, tiles[0], tiles[1], 1, periodic[0], periodic[1], 0, radius, tile_flags, ctl,
-                                           every, counts);
+                                           every, counts, split, peer_lo, peer_hi);
     }
     return cudaGetLastError();
 }

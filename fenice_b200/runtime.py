@@ -34,7 +34,7 @@ EXPORTS = ["fvg_abi_version", "fvg_create", "fvg_destroy", "fvg_last_error", "fv
            "fvg_batch_download", "fvg_batch_run", "fvg_batch_problem", "fvg_batch_autotune", "fvg_batch_set_schedule",
            "fvg_batch_get_schedule", "fvg_batch_stream", "fvg_batch_set_timing", "fvg_batch_get_timing",
            "fvg_sensor_sizes", "fvg_sensor_extract", "fvg_sensor_grad", "fvg_sensor_adam", "fvg_sensor_pack", "fvg_sensor_infer",
-           "fvg_set_sensor", "fvg_get_sensor_counts", "fvg_get_sensor_gate", "fvg_ibm_loads", "fvg_monitor",
+           "fvg_set_sensor", "fvg_get_sensor_counts", "fvg_get_sensor_gate", "fvg_ibm_loads", "fvg_monitor", "fvg_get_body_state", "fvg_set_body_state",
            "fvg_create_part", "fvg_part_info", "fvg_part_buffers", "fvg_part_begin", "fvg_part_phase", "fvg_part_status",
            "fvg_expr_eval"]
 
@@ -107,6 +107,8 @@ def load_library(path=LIB_PATH):
     lib.fvg_get_sensor_gate.argtypes = [c_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     lib.fvg_ibm_loads.argtypes = [c_p, dp]
     lib.fvg_monitor.argtypes = [c_p, ctypes.c_int, dp]
+    lib.fvg_get_body_state.argtypes = [c_p, dp, ctypes.POINTER(ctypes.c_int)]
+    lib.fvg_set_body_state.argtypes = [c_p, dp, ctypes.c_int]
     ip = ctypes.POINTER(ctypes.c_int)
     dpp = ctypes.POINTER(dp)
     lib.fvg_create_part.argtypes = [ctypes.POINTER(P.FvgConfig), ctypes.c_int, ctypes.c_int, ctypes.POINTER(c_p)]
@@ -300,6 +302,23 @@ class Run:
         v = (ctypes.c_double * 6)()
         self._check(self.lib.fvg_ibm_loads(self.h, v), "ibm_loads")
         return dict(zip(["Fx", "Fy", "Mz", "Cd", "Cl", "Cm"], list(v)))
+
+    @property
+    def body_state(self):
+        """The moving body's state in the reference's checkpoint layout (body_pose; fvg_get_body_state), or None without a
+        moving body. Assigning restores it (set the time first)."""
+        n = ctypes.c_int(0)
+        self._check(self.lib.fvg_get_body_state(self.h, None, ctypes.byref(n)), "get_body_state")
+        if n.value == 0:
+            return None
+        v = np.zeros(n.value)
+        self._check(self.lib.fvg_get_body_state(self.h, _dp(v), ctypes.byref(n)), "get_body_state")
+        return v
+
+    @body_state.setter
+    def body_state(self, v):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        self._check(self.lib.fvg_set_body_state(self.h, _dp(v), int(v.size)), "set_body_state")
 
     def monitor(self, order="reference"):
         """{mass, kinetic_energy, total_energy, enstrophy} of the current state (fvg_monitor): the volume averages of the

@@ -8,7 +8,10 @@ neighbours or all-reduce (MAX) a wave speed, on the parts' streams. Two exchange
 * ``LocalExchange``: all parts in this process (one GPU or several), by device copies between their buffers; this is how
   a decomposition is checked against the whole run on a single GPU;
 * ``DistExchange``: one part per process, torch.distributed point-to-point sends / receives and all-reduce (NCCL
-  between GPUs; gloo on CPU tensors in the host tests).
+  between GPUs, enqueued on the part's stream: no host synchronisation; gloo on CPU tensors in the host tests);
+* ``HostStagedExchange``: one part per process with the planes staged through pinned host memory and moved by a CPU
+  process group (gloo): processes that share a GPU, or GPUs without a device-to-device path, exchange this way (each
+  communication point waits on the host for the part's stream; no kernel ever waits for another process).
 
 Every part takes the same phases and the same communication in the same order. The cells beyond an interface are the
 neighbour's, and dt comes from the all-reduced speed, so a decomposed run reproduces the whole run's bits.
@@ -211,11 +214,83 @@ class DistExchange:
                 self.dist.all_reduce(self.bufs[4][:count], op=self.dist.ReduceOp.MAX, group=self.group)
 
 
-def advance(parts, exchanger, t_end, max_steps=0):
-    """Advances the parts of this process (one part per process with DistExchange, all of them with LocalExchange) toward
-    t_end, at most max_steps steps (0: no limit); returns (steps, t). Raises as fvg_run_until on divergence."""
+class HostStagedExchange:
+    """DistExchange's communication through pinned host memory and a CPU (gloo) process group: before each exchange or
+    all-reduce the part's stream is waited for, its send planes (or reduce slots) are copied to the host, moved between
+    the processes, and the received planes copied back on the part's stream. The same pairing of sends and receives as
+    DistExchange, so any number of ranks on any number of GPUs (several ranks may share one)."""
+
+    def __init__(self, part, group=None):
+        import torch
+        import torch.distributed as dist
+
+        self.dist, self.group, self.part = dist, group, part
+        self.rank, self.world = dist.get_rank(group), dist.get_world_size(group)
+        self.lo, self.hi = (self.rank - 1) % self.world, (self.rank + 1) % self.world
+        self.dev = part.tensors()
+        self.stream = torch.cuda.ExternalStream(part.stream(), device=torch.device("cuda", part.device))
+        self.host = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in self.dev]
+
+    def exchange(self):
+        import torch
+
+        send_lo, send_hi, recv_lo, recv_hi, _ = self.dev
+        h_send_lo, h_send_hi, h_recv_lo, h_recv_hi, _ = self.host
+        p = self.part
+        with torch.cuda.stream(self.stream):
+            if p.peer_lo:
+                h_send_lo.copy_(send_lo, non_blocking=True)
+            if p.peer_hi:
+                h_send_hi.copy_(send_hi, non_blocking=True)
+        self.stream.synchronize()
+        if self.world == 1:
+            if p.peer_lo:
+                h_recv_hi.copy_(h_send_lo)
+            if p.peer_hi:
+                h_recv_lo.copy_(h_send_hi)
+        else:
+            d = self.dist
+            ops = []
+            if p.peer_lo:
+                ops.append(d.P2POp(d.isend, h_send_lo, self.lo, self.group))
+            if p.peer_hi:
+                ops.append(d.P2POp(d.isend, h_send_hi, self.hi, self.group))
+            if p.peer_hi:
+                ops.append(d.P2POp(d.irecv, h_recv_hi, self.hi, self.group))
+            if p.peer_lo:
+                ops.append(d.P2POp(d.irecv, h_recv_lo, self.lo, self.group))
+            if ops:
+                for r in d.batch_isend_irecv(ops):
+                    r.wait()
+        with torch.cuda.stream(self.stream):
+            if p.peer_hi:
+                recv_hi.copy_(h_recv_hi, non_blocking=True)
+            if p.peer_lo:
+                recv_lo.copy_(h_recv_lo, non_blocking=True)
+
+    def allreduce(self, count):
+        import torch
+
+        red, h_red = self.dev[4], self.host[4]
+        with torch.cuda.stream(self.stream):
+            h_red[:count].copy_(red[:count], non_blocking=True)
+        self.stream.synchronize()
+        if self.world > 1:
+            self.dist.all_reduce(h_red[:count], op=self.dist.ReduceOp.MAX, group=self.group)
+        with torch.cuda.stream(self.stream):
+            red[:count].copy_(h_red[:count], non_blocking=True)
+
+
+def advance(parts, exchanger, t_end, max_steps=0, check_every=1):
+    """Advances the parts of this process (one part per process with DistExchange or HostStagedExchange, all of them
+    with LocalExchange) toward t_end, at most max_steps steps (0: no limit); returns (steps, t). The parts' clocks are
+    read (a host synchronisation) every `check_every` steps: steps past t_end or the step limit are gated off on the
+    device on every part alike, so enqueuing a few more only costs their empty launches. Raises as fvg_run_until on
+    divergence."""
     for p in parts:
         p.begin(t_end, max_steps)
+    if any(p.cfg.time_scheme == 3 for p in parts):   # MUSCL-Hancock swaps its state buffers on the host every step
+        check_every = 1
     while True:
         st = [p.status() for p in parts]
         active, steps, t = st[0][0], st[0][1], st[0][2]
@@ -223,17 +298,18 @@ def advance(parts, exchanger, t_end, max_steps=0):
             raise RuntimeError(f"the parts' clocks differ: {st}")
         if not active:
             return steps, t
-        phase = 0
-        while True:
-            comms = [p.phase(phase) for p in parts]
-            comm, n = comms[0]
-            if comm == COMM_DONE:
-                break
-            if comm == COMM_EXCHANGE:
-                exchanger.exchange()
-            else:
-                exchanger.allreduce(n)
-            phase += 1
+        for _ in range(max(1, int(check_every))):
+            phase = 0
+            while True:
+                comms = [p.phase(phase) for p in parts]
+                comm, n = comms[0]
+                if comm == COMM_DONE:
+                    break
+                if comm == COMM_EXCHANGE:
+                    exchanger.exchange()
+                else:
+                    exchanger.allreduce(n)
+                phase += 1
 
 
 def run_decomposed(params, U, nparts, t_end, max_steps=0, precision=0, device=0):
@@ -247,4 +323,4 @@ def run_decomposed(params, U, nparts, t_end, max_steps=0, precision=0, device=0)
             p.close()
 
 
-__all__ = ["Part", "LocalExchange", "DistExchange", "advance", "run_decomposed", "split_state", "join_states", "part_range", "split_axis", "FVG_OK"]
+__all__ = ["Part", "LocalExchange", "DistExchange", "HostStagedExchange", "advance", "run_decomposed", "split_state", "join_states", "part_range", "split_axis", "FVG_OK"]

@@ -224,6 +224,18 @@ int fvg_get_timing(const fvg_run* run, double* stage_ms, long long* stage_launch
  * on 1/2 rho_in u_in^2 A (A = the diameter in 2-D, pi r^2 for a sphere, diameter x Lz for a 3-D cylinder). */
 int fvg_ibm_loads(fvg_run* run, double* loads);
 
+/* The state of a moving immersed body in the layout of the reference's checkpoint key body_pose
+ * (Simulation::body_checkpoint / restore_body_from_checkpoint, cpp/src/SimulationRestart.cpp:87-160): the pose the geometry
+ * was built at (x, y, angle), the state of a body driven by the flow (x, y, u, v, ax, ay, dt; zeros in prescribed motion),
+ * on a 3-D mesh then (z of the geometry, z, w, az), with a driven rotation (ibm_inertia > 0) then (angle, angular velocity,
+ * angular acceleration) and on a 3-D mesh (omega_x, omega_y and their accelerations): 10, 13, 14 or 21 doubles.
+ * fvg_get_body_state: *n = the count (0 without a moving body); with v non-NULL, *n on entry is v's capacity.
+ * fvg_set_body_state: restores the body and builds its geometry at the stored pose (set the run's time first: a body in
+ * prescribed motion takes its rotation at that time); a count other than the run's is FVG_ERR_ARGUMENT, a run without a
+ * moving body FVG_ERR_CONFIG. */
+int fvg_get_body_state(const fvg_run* run, double* v, int* n);
+int fvg_set_body_state(fvg_run* run, const double* v, int n);
+
 /* The monitor of the run's current state: out[4] = {mass, kinetic_energy, total_energy, enstrophy}. The first three are
  * the volume averages of rho, 1/2 |m|^2 / rho and rho E that the reference writes in its monitor file
  * (Simulation::volume_averages and monitor_row, cpp/src/SimulationRun.cpp:44-64, 87-90). order 0 adds the cells in the

@@ -17,7 +17,8 @@ from fenice_b200 import params as P
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden")
 FENICE = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "fenice")
-NAMES = ["hancock_2d", "weno5_rk3_3d"]
+NAMES = ["hancock_2d", "weno5_rk3_3d", "free_circle_rk2_2d", "prescribed_sphere_3d", "free_sphere_3d"]
+MOVING = {"free_circle_rk2_2d": 13, "prescribed_sphere_3d": 14, "free_sphere_3d": 21}
 FINAL = np.load(os.path.join(GOLD, "ckpt_final.npz"))
 
 
@@ -40,7 +41,8 @@ def test_written_checkpoint_has_the_reference_layout(name, tmp_path):
     p = P.resolve(json.loads(str(FINAL[f"{name}/params"])))
     U5 = np.zeros((a["U"].shape[0], 5))
     U5[:, :a["U"].shape[1]] = a["U"]
-    mine = ck.checkpoint_arrays(U5, float(a["t"]), int(a["step"]), p, float(a["S"]) if "S" in a else 0.0)
+    mine = ck.checkpoint_arrays(U5, float(a["t"]), int(a["step"]), p, float(a["S"]) if "S" in a else 0.0, body_pose=a.get("body_pose"))
+    assert ("body_pose" in a) == (name in MOVING) and (name not in MOVING or a["body_pose"].shape == (MOVING[name],))
     path = str(tmp_path / "mine.npz")
     ck.write_checkpoint(path, mine)
     b = np.load(path)
@@ -71,13 +73,13 @@ def test_reference_resumes_from_a_checkpoint_written_here(name):
         out = os.path.join(tmp, "out")
         dest = os.path.join(out, str(FINAL[f"{name}/ckpt_relpath"]))
         os.makedirs(os.path.dirname(dest))
-        ck.write_checkpoint(dest, ck.checkpoint_arrays(U5, float(a["t"]), int(a["step"]), p, float(a["S"]) if "S" in a else 0.0))
-        sets = json.loads(str(FINAL[f"{name}/params"]))
-        keep = ["nx", "ny", "nz", "Lx", "Ly", "Lz", "reconstruction", "muscl_limiter", "time_scheme", "riemann_solver", "use_viscous", "mu", "cfl",
-                "boundary_order"] + [f"bc_{x}{s}" for x in "xyz" for s in ("min", "max")]
+        ck.write_checkpoint(dest, ck.checkpoint_arrays(U5, float(a["t"]), int(a["step"]), p, float(a["S"]) if "S" in a else 0.0,
+                                                       body_pose=a.get("body_pose")))
+        sets = json.loads(str(FINAL[f"{name}/sets"]))   # the case's own --set keys (its mesh, schemes, sides, body)
         cmd = [FENICE, "--case", os.path.join(tmp, "case.toml"), "--no-logo", "--threads", "2"]
-        for k in keep:
-            cmd += ["--set", f"{k}={sets[k]}"]
+        for k, v in sets.items():
+            if k not in ("t_end", "save_interval"):
+                cmd += ["--set", f"{k}={v}"]
         cmd += ["--set", "t_end=1e9", "--set", "save_interval=1000000000", "--set", "max_steps=8", "--set", f"output_root={out}",
                 "--set", "resume=true", "--set", f"dump_state={os.path.join(tmp, 'resumed.npz')}"]
         subprocess.run(cmd, capture_output=True, text=True, check=True)

@@ -1,6 +1,8 @@
 """Checkpoint interop on the GPU: a run on the device resumes from the reference's own checkpoint (step 7, with the
-MUSCL-Hancock lagged speed where the scheme has one) and reaches the reference's uninterrupted step-15 state bit for bit;
-a checkpoint written by the device run and read back resumes it exactly; the dump_state file round-trips."""
+MUSCL-Hancock lagged speed where the scheme has one, and the pose and state of a moving immersed body: a 2-D body driven by
+the flow with a driven rotation, a 3-D sphere in prescribed motion, a 3-D sphere driven by the flow) and reaches the
+reference's uninterrupted step-15 state bit for bit; a checkpoint written by the device run and read back resumes it
+exactly; the dump_state file round-trips; a moving-body run refuses a checkpoint without the body's pose."""
 import json
 import os
 
@@ -14,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 FINAL = np.load(os.path.join(GOLD, "ckpt_final.npz"))
-NAMES = ["hancock_2d", "weno5_rk3_3d"]
+NAMES = ["hancock_2d", "weno5_rk3_3d", "free_circle_rk2_2d", "prescribed_sphere_3d", "free_sphere_3d"]
 
 
 def bits_equal(a, b):
@@ -52,3 +54,15 @@ def test_device_checkpoint_round_trip(name, tmp_path):
     ck.dump_state(dump, resumed, 13)
     U, t, s = ck.read_dump(dump)
     assert bits_equal(U, resumed.state()) and t == resumed.t and s == 13
+
+
+def test_moving_body_refuses_a_checkpoint_without_its_pose(tmp_path):
+    """SimulationRestart.cpp:103: a run with a moving body does not resume from a file without body_pose."""
+    name = "free_circle_rk2_2d"
+    a = ck.read_checkpoint(os.path.join(GOLD, f"ckpt_{name}.npz"))
+    del a["body_pose"]
+    path = str(tmp_path / "static.npz")
+    ck.write_checkpoint(path, a)
+    run = Run(json.loads(str(FINAL[f"{name}/params"])))
+    with pytest.raises(ValueError, match="no pose of the moving body"):
+        ck.load_checkpoint(path, run)

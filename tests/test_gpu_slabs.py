@@ -95,3 +95,58 @@ def test_part_refuses_whole_run_entry_points():
     with pytest.raises(ValueError, match="fvg_part_phase"):
         p.residual()
     p.close()
+
+
+def test_gated_mixed_form_decomposed():
+    """The mixed form gated by the learned sensor on a decomposed mesh (2 parts of a periodic 64^3 Taylor-Green box, the
+    refresh every 5 steps after each part's interface planes arrive): the tile rows whose gate box reaches an interface
+    stay WENO5-Z along every axis, the other tiles take the flags the whole run takes from the same state, and the
+    totals stay conserved (the interface faces are solved alike by both parts)."""
+    import math
+    import os
+
+    import bench
+    from fenice_b200.sensor import Sensor
+
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    s = Sensor.load(os.path.join(here, "fenice_b200", "sensor_weights.npz"), device=0)
+    theta = float(s.meta["threshold"])
+    n, nparts, every = 64, 2, 5
+    params = bench.workload(n)
+    U0 = bench.tgv_state(n)
+    whole = Run(params, U=U0, precision=1)
+    whole.set_sensor(s, theta, every=every)
+    assert whole.run(1e30, max_steps=1) == 1
+    _, wt, tile = whole.sensor_gate()
+    parts = [slabs.Part(params, nparts, i, U=u, precision=1) for i, u in enumerate(slabs.split_state(params, U0, nparts))]
+    try:
+        for p in parts:
+            p.set_sensor(s, theta, every=every)
+        ex = slabs.LocalExchange(parts)
+        slabs.advance(parts, ex, 1e30, 1)
+        radius = int(math.ceil(0.5 * every)) + 1
+        tz = tile[2]
+        for p in parts:
+            _, pt, _ = p.sensor_gate()
+            rows = pt.shape[1]
+            for r in range(rows):
+                lo, hi = r * tz, min((r + 1) * tz, p.count) - 1
+                reaches = lo - (radius + 1) < 0 or hi + radius + 1 > p.count - 1
+                if reaches:
+                    assert np.all(pt[:, r] == 1), (p.index, r)
+                else:
+                    assert np.array_equal(pt[:, r], wt[:, (p.first + lo) // tz]), (p.index, r)
+        steps, _ = slabs.advance(parts, ex, 1e30, 20)   # (the step count and the refresh cadence start again per call)
+        assert steps == 20
+        U = slabs.join_states(params, [p.state() for p in parts])
+        lin, ev = parts[0].sensor_counts()
+        assert 0 < lin < ev
+    finally:
+        for p in parts:
+            p.close()
+        whole.close()
+    mom = math.fsum(np.sqrt(U0[:, 1] ** 2 + U0[:, 2] ** 2 + U0[:, 4] ** 2))
+    scale = np.array([math.fsum(np.abs(U0[:, 0])), mom, mom, math.fsum(np.abs(U0[:, 3])), mom])
+    drift = np.array([abs(math.fsum(U[:, q]) - math.fsum(U0[:, q])) for q in range(5)]) / scale
+    print(f"\ngated, 2 parts, 21 steps: {lin} of {ev} tile-axes linear on part 0; drift of the totals " + " ".join(f"{d:.1e}" for d in drift))
+    assert np.all(drift <= 2e-11)
