@@ -2645,6 +2645,74 @@ int fvg_step_host(fvg_run* run, const double* U_in, double* U_out, size_t ncells
         const double* Ulast = run->Ut;
         double ca = 0.5, cb = 0.5;
         int st = 1;
+        if (ts == FVG_TS_SSPRK3 && !run->tv_on && !run->src_unsteady) {
+            // stages 2 and 3 as a wavefront over the tile planes, each slab downloaded as soon as its cells are final, so
+            // the download overlaps both stages. Stage 3 on a tile plane reads stage 2's state R up to kHostHalo cells
+            // beyond it (wrapped on a periodic axis) and its viscous sweep R one cell beyond its viscous tiles; a viscous
+            // sweep of stage 3 overwrites the viscous residual Rv of its tiles only once every stage-2 tile plane over
+            // them has read it. (Without per-stage boundary values or sources: one array holds those for the stage.)
+            const StageArgs sa2 = stage_args(run, run->Ut, run->U, run->R, kCombine, 0.75, 0.25, visc ? run->Rv : nullptr, run->bm[1], act);
+            const StageArgs sa3 = stage_args(run, run->R, run->U, run->U, kCombine, 1.0 / 3.0, 2.0 / 3.0, visc ? run->Rv : nullptr, run->bm[2], act);
+            std::vector<char> done2(ns, 0), done2v(nsv, 0), done3v(nsv, 0);
+            auto plane_of = [&](int y, int T) { return (s.periodic ? ((y % s.N) + s.N) % s.N : std::min(std::max(y, 0), s.N - 1)) / T; };
+            // stage 2 on every tile plane over cells [lo, hi) not run yet (its viscous tiles first), in runs of consecutive planes
+            auto ensure2 = [&](int lo, int hi) -> int {
+                std::vector<char> want(ns, 0);
+                for (int y = lo; y < hi; ++y) want[plane_of(y, Ts)] = 1;
+                for (int j = 0; j < ns;) {
+                    if (!want[j] || done2[j]) {
+                        ++j;
+                        continue;
+                    }
+                    int k = j;
+                    while (k < ns && want[k] && !done2[k]) ++k;
+                    const int v0 = j * Ts / Tv, v1 = (std::min(k * Ts, s.N) - 1) / Tv + 1;
+                    for (int v = v0; v < v1;) {
+                        if (done2v[v]) {
+                            ++v;
+                            continue;
+                        }
+                        int w = v;
+                        while (w < v1 && !done2v[w]) done2v[w++] = 1;
+                        CKL(visc_planes(run->Ut, run->bmv[1], v, w));
+                        v = w;
+                    }
+                    CKL(stage_planes(sa2, j, k));
+                    for (int q = j; q < k; ++q) done2[q] = 1;
+                    j = k;
+                }
+                return FVG_OK;
+            };
+            int j3 = 0, kd = 0;
+            for (int k = 0; k < s.n; ++k) {
+                // stage 3 on every tile plane with a cell in slabs 0 .. k
+                const int j_end = (std::min((k + 1) * s.planes, s.N) + Ts - 1) / Ts;
+                if (j_end > j3) {
+                    const int c_lo = j3 * Ts, c_hi = std::min(j_end * Ts, s.N);
+                    if (visc) {
+                        const int v0 = c_lo / Tv, v1 = (c_hi - 1) / Tv + 1;
+                        for (int v = v0; v < v1; ++v) {
+                            if (done3v[v]) continue;
+                            if ((rc = ensure2(v * Tv - 1, std::min((v + 1) * Tv, s.N) + 1))) return rc;
+                            CKL(visc_planes(run->R, run->bmv[2], v, v + 1));
+                            done3v[v] = 1;
+                        }
+                    }
+                    if ((rc = ensure2(c_lo - kHostHalo, c_hi + kHostHalo))) return rc;
+                    CKL(stage_planes(sa3, j3, j_end));
+                    j3 = j_end;
+                }
+                // the slabs whose cells are all final now
+                for (; kd < s.n && std::min((kd + 1) * s.planes, s.N) <= std::min(j3 * Ts, s.N); ++kd)
+                    if ((rc = download(kd))) return rc;
+            }
+            for (; kd < s.n; ++kd)
+                if ((rc = download(kd))) return rc;
+            k_stage_max<<<1, 1024, 0, cs>>>(c, act, 1, run->bm[1], run->nb, run->bmv[1], nbv);
+            k_stage_max<<<1, 1024, 0, cs>>>(c, act, 2, run->bm[2], run->nb, run->bmv[2], nbv);
+            k_end_rk<<<1, 1, 0, cs>>>(c, 3);
+            CKL(cudaGetLastError());
+        } else {
         if (ts == FVG_TS_SSPRK3) {
             CKL(stage_values(run, run->res_kind >= 0 ? run->res_kind : 1, act));
             CKL(visc_planes(run->Ut, run->bmv[1], 0, nsv));
@@ -2672,6 +2740,7 @@ int fvg_step_host(fvg_run* run, const double* U_in, double* U_out, size_t ncells
         k_stage_max<<<1, 1024, 0, cs>>>(c, act, st, run->bm[st], run->nb, run->bmv[st], nbv);
         k_end_rk<<<1, 1, 0, cs>>>(c, ts == FVG_TS_SSPRK2 ? 2 : 3);
         CKL(cudaGetLastError());
+        }
     }
 #undef CKL
     int hbad = 0;
