@@ -120,13 +120,22 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(n, name):
-    """Per-launch DRAM bytes of a stage kernel from its committed ncu summary (profiles/<name>), scaled to n^3 cells, or None."""
+def ncu_profile(name):
+    """The committed ncu summary of a stage kernel (profiles/<name>: per-launch DRAM bytes at its cell count, pipe and
+    issue fractions, what limits it), or {}."""
     try:
         with open(os.path.join(ROOT, "profiles", name)) as f:
-            d = json.load(f)
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def ncu_traffic(n, name):
+    """Per-launch DRAM bytes of a stage kernel from its committed ncu summary, scaled to n^3 cells, or None."""
+    d = ncu_profile(name)
+    try:
         return d["dram_bytes_per_launch"] * (n ** 3) / d["cells"]
-    except (OSError, KeyError, ValueError):
+    except KeyError:
         return None
 
 
@@ -232,13 +241,21 @@ def timed_run(params, U0, precision, args, world, local, sensor=None):
     return run, allmax(start.elapsed_time(end), world), tm, clk.summary()
 
 
-def roofline_of(tm, ms, cells, kernel, traffic):
+def roofline_of(tm, ms, cells, kernel, traffic, profile=None):
+    """The HBM roofline of the stage kernel (algorithmic bytes per launch over its live CUDA-event duration against the
+    measured copy bandwidth) and, from its committed ncu summary, what actually limits it: the FP64 or FP32 pipe and
+    issue fractions (the stencil is compute- or latency-bound, far below the HBM roof)."""
     peak, peak_kind = measured_peak()
     stage_avg_ms = tm["stage_ms"] / max(tm["stage_launches"], 1)
     alg_bytes = cells * BYTES_PER_CELL_STAGE
     achieved = alg_bytes / (stage_avg_ms * 1e-3) / 1e9
+    prof = profile or {}
+    limits = {k: prof[k] for k in ("fp64_pipe_frac", "fp64_flop_frac", "fma_pipe_frac", "issue_frac") if k in prof}
+    if limits:
+        limits["source"] = "ncu --set full of one launch at 192^3 (profiles/)"
     return {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
             "traffic": traffic, "peak_source": f"hbm_gbs of MEASURED_PEAKS.json ({peak_kind})", "kernel": kernel,
+            "limiter": prof.get("limiter"), "pipe_fractions": limits or None,
             "algorithmic_bytes_per_launch": alg_bytes, "stage_launch_ms": round(stage_avg_ms, 4),
             "viscous_launch_ms": round(tm["viscous_ms"] / max(tm["viscous_launches"], 1), 4),
             "stage_share_of_step": round(tm["stage_ms"] / ms, 4), "viscous_share_of_step": round(tm["viscous_ms"] / ms, 4)}
@@ -737,11 +754,12 @@ def gpu_arm(args, world, rank, local):
     mixed.close()
 
     rl_l = roofline_of(tm_l, ms_l, cells, "mixed_stage_kernel<3, WENO5, LowMach, gated> (FP32 reconstruction (linear or WENO5-Z per tile) + "
-                       "Riemann + balance, FP64 RK update)", ncu_traffic(n, "mixed_stage_kernel_weno5_3d.json"))
+                       "Riemann + balance, FP64 RK update)", ncu_traffic(n, "mixed_stage_kernel_weno5_3d.json"),
+                       ncu_profile("mixed_stage_kernel_weno5_3d.json"))
     rl_m = roofline_of(tm_m, ms_m, cells, "mixed_stage_kernel<3, WENO5, LowMach> (FP32 reconstruction + Riemann + balance, FP64 RK update)",
-                       ncu_traffic(n, "mixed_stage_kernel_weno5_3d.json"))
+                       ncu_traffic(n, "mixed_stage_kernel_weno5_3d.json"), ncu_profile("mixed_stage_kernel_weno5_3d.json"))
     rl_p = roofline_of(tm_p, ms_p, cells, "stage_kernel<3, WENO5, LowMach> (FP64, the reference's arithmetic)",
-                       ncu_traffic(n, "stage_kernel_weno5_3d.json"))
+                       ncu_traffic(n, "stage_kernel_weno5_3d.json"), ncu_profile("stage_kernel_weno5_3d.json"))
     # per RK3 step: 3 viscous + 3 stage + dt + axpy + 2 stage maxima + end; one begin per run; the gated run adds the
     # sensor's refresh (network, 3 dilation passes, tile reduction) to every step (the kernels return at once off the
     # refresh steps)
