@@ -778,7 +778,7 @@ def gpu_arm(args, world, rank, local):
             "mixed": {"value": value_m, "ms_per_step": ms_m / args.steps, "roofline": rl_m, "clocks": clk_m, "speedup_vs_plain": value_m / value_p,
                       "accuracy_l1_rho": errs_m["rho"]["l1_rel"]},
             "sensor": {"threshold": sensor[1], "tile_axes_linear": lin, "tile_axes": ev, "linear_share": lin / max(ev, 1),
-                       "refresh_every_steps": 5, "speedup_vs_mixed": value / value_m},
+                       "refresh_every_steps": 10, "speedup_vs_mixed": value / value_m},
             "form_of_value": "the mixed-precision form gated by the learned sensor; mixed: without the sensor; plain_fp64: the reference's arithmetic",
             "roofline": rl_l, "e2e": e2e, "gpu_launches": launches, "clocks": clk_l}
     return line

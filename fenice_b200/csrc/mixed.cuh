@@ -74,7 +74,8 @@ template <int DIM, int RECON, int TX, int TY, int TZ> struct MixedShape {
 
 // One axis of the tile sweep of mixed_stage_kernel (compile-time extents).
 // GATED (WENO5-Z with the learned sensor): the tile's flag for this axis (one byte per tile and axis, from the sensor's
-// last refresh) makes every reconstruction of the sweep linear (0) or WENO5-Z (1); the branch is uniform over the CTA.
+// last refresh) makes the reconstructions of the sweep linear (0) or WENO5-Z (1), a branch uniform over the CTA; the seam
+// faces of a linear tile whose tile across stays WENO5-Z take WENO5-Z in a short pass of their own.
 template <int AXIS, int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT, bool GATED = false, bool FULL = true>
 __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>& ef, float sb, float weps, float* __restrict__ P,
                                            float* __restrict__ WL, float* __restrict__ WR, float* __restrict__ acc, unsigned char* __restrict__ Sf,
@@ -147,7 +148,10 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
                 if (four) {
                     wl = weno3z(c1, c2, c3, weps);
                     wr = weno3z(c4, c3, c2, weps);
-                } else if (tile_linear && (f3[AXIS] == 0 ? seam_lo : (f3[AXIS] == hi_face ? seam_hi : true))) {
+                } else if (tile_linear) {
+                    // a seam face whose tile across stays WENO5-Z is left to the seam pass below (so that this pass's
+                    // warps all take the cheap branch)
+                    if (!(f3[AXIS] == 0 ? seam_lo : (f3[AXIS] == hi_face ? seam_hi : true))) continue;
                     // linear fifth-order upwind values where the sensor passed the tile (the WENO-Z weights at their
                     // linear values 0.1, 0.6, 0.3)
                     wl = lin5(c0, c1, c2, c3, c4);
@@ -159,6 +163,39 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
             }
             WL[q * S::NF + f] = wl;
             WR[q * S::NF + f] = wr;
+        }
+        if constexpr (GATED) {
+            // the seam pass: a linear tile's seam faces whose tile across stays WENO5-Z take WENO5-Z, as that tile does
+            if (tile_linear && (!seam_lo || !seam_hi)) {
+                constexpr int PL = nF / Fd[AXIS];   // faces of one layer across the axis
+                const int layers = (!seam_lo ? 1 : 0) + (!seam_hi ? 1 : 0);
+                for (int it = tid; it < layers * PL * NV; it += NT) {
+                    const int q = it / (layers * PL), rem = it % (layers * PL), layer = rem / PL, r = rem % PL;
+                    int f3[3];
+                    f3[AXIS] = (layer == 0 && !seam_lo) ? 0 : hi_face;
+                    constexpr int A1 = AXIS == 0 ? 1 : 0, A2 = AXIS == 2 ? 1 : 2;
+                    f3[A1] = r % Fd[A1];
+                    f3[A2] = r / Fd[A1];
+                    const int f = (f3[2] * Fd[1] + f3[1]) * Fd[0] + f3[0];
+                    const int base = (f3[2] * E[1] + f3[1]) * E[0] + f3[0];
+                    const float* c = P + q * S::EXT + base;
+                    const float c0 = c[0], c1 = c[sstride], c2 = c[2 * sstride], c3 = c[3 * sstride], c4 = c[4 * sstride], c5 = c[5 * sstride];
+                    bool four = false;
+                    if (a.bc.solid)
+#pragma unroll
+                        for (int s6 = 0; s6 < 6; ++s6) four = four || Sf[base + s6 * sstride] != 0;
+                    float wl, wr;
+                    if (four) {
+                        wl = weno3z(c1, c2, c3, weps);
+                        wr = weno3z(c4, c3, c2, weps);
+                    } else {
+                        wl = weno5z(c0, c1, c2, c3, c4, weps);
+                        wr = weno5z(c5, c4, c3, c2, c1, weps);
+                    }
+                    WL[q * S::NF + f] = wl;
+                    WR[q * S::NF + f] = wr;
+                }
+            }
         }
         __syncthreads();
         // ---- 3. fluxes

@@ -2924,7 +2924,7 @@ int fvg_set_sensor(fvg_run* run, const void* weights, float threshold, int every
     }
     if (run->cfg.precision != FVG_PREC_MIXED || run->cfg.reconstruction != FVG_RECON_WENO5)
         return fail(run, FVG_ERR_CONFIG, "the sensor gates the mixed-precision WENO5-Z form");
-    if (every <= 0) every = 5;
+    if (every <= 0) every = 10;   // (10: the refresh costs a third of a stage; measured gains over the ungated step 1.04-1.10x, 0.99-1.07x with 5)
     if (radius < 0) radius = (int)std::ceil(run->cfg.cfl * every) + 1;
     const size_t fbytes = (size_t)run->m.plane * run->dim;
     if (!run->sens) CK(cudaMalloc(&run->sens, sizeof(SensorW)));

@@ -25,8 +25,9 @@ __device__ __forceinline__ unsigned hash32(unsigned long long x, unsigned seed) 
 }
 
 // Features and label statistic of every (cell, axis) of a state. mode 0: all, at index cell * DIM + axis; mode 1: the
-// troubled ones (departure > tau) and every keep_div-th other one (by a hash), appended at an atomic counter up to cap.
-// stats[0] += troubled, stats[1] += all.
+// troubled ones (statistic > tau) and every keep_div-th other one (by a hash), appended at an atomic counter up to cap.
+// stats[0] += troubled, stats[1] += all. The statistic: the largest |WENO5-Z - linear| of the cell's two face values
+// over the quantities, each relative to the quantity's physical scale at the cell (sensor_scale).
 template <int DIM, int NV>
 __global__ void k_sensor_extract(Mesh m, Bc bc, Eos<double> eos, const double* __restrict__ U, double weno_eps, int mode, int keep_div, unsigned seed,
                                  float tau, float* __restrict__ X, float* __restrict__ dep, int* count, long long cap,
@@ -48,19 +49,21 @@ __global__ void k_sensor_extract(Mesh m, Bc bc, Eos<double> eos, const double* _
         }
         float f[kSensF];
         double D = 0.0;
+        const double p_inf = eos.type == kIdeal ? 0.0 : eos.p_inf;
 #pragma unroll
         for (int sq = 0; sq < kSensQ; ++sq) {
             const int var = sensor_var<NV>(sq, axis);
+            const double scale = sensor_scale<double>(sq, w5[2][0], w5[2][3], eos.gamma, p_inf);
             float v[5];
 #pragma unroll
             for (int s = 0; s < 5; ++s) v[s] = var >= 0 ? (float)w5[s][var < 0 ? 0 : var] : 0.0f;
-            sensor_quantity_features(v, f + 5 * sq);
+            sensor_quantity_features(v, (float)scale, f + 5 * sq);
             if (var >= 0) {
                 double cv[5];
 #pragma unroll
                 for (int s = 0; s < 5; ++s) cv[s] = w5[s][var];
-                D = fmax(D, weno5z_departure(cv[0], cv[1], cv[2], cv[3], cv[4], weno_eps));
-                D = fmax(D, weno5z_departure(cv[4], cv[3], cv[2], cv[1], cv[0], weno_eps));
+                D = fmax(D, weno5z_face_gap(cv[0], cv[1], cv[2], cv[3], cv[4], weno_eps) / scale);
+                D = fmax(D, weno5z_face_gap(cv[4], cv[3], cv[2], cv[1], cv[0], weno_eps) / scale);
             }
         }
         const bool bad = D > (double)tau;
@@ -389,6 +392,7 @@ __global__ void __launch_bounds__(256) k_sensor_flags_t(Mesh m, Bc bc, Eos<doubl
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     __nv_bfloat16* Xs = tiles[warp];
+    const float gam = (float)eos.gamma, pinf = eos.type == kIdeal ? 0.0f : (float)eos.p_inf;
     for (int ch = warp; ch * 16 < ROWS; ch += 8) {
         for (int it = lane; it < 16 * kSensQ; it += 32) {
             const int row = it / kSensQ, sq = it % kSensQ, r = ch * 16 + row;
@@ -401,7 +405,7 @@ __global__ void __launch_bounds__(256) k_sensor_flags_t(Mesh m, Bc bc, Eos<doubl
                 float v[5];
 #pragma unroll
                 for (int k = 0; k < 5; ++k) v[k] = P[var * PS + e + (k - 2) * st];
-                sensor_quantity_features(v, f);
+                sensor_quantity_features(v, sensor_scale<float>(sq, P[e], P[3 * PS + e], gam, pinf), f);
             }
 #pragma unroll
             for (int k = 0; k < 5; ++k) Xs[row * kLd + 5 * sq + k] = __float2bfloat16_rn(f[k]);

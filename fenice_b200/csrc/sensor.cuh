@@ -3,16 +3,18 @@
 //
 // Inputs (per cell and axis): the 5 cells c-2 .. c+2 along the axis, 5 primitive quantities each (rho, the normal
 // velocity, the two tangential velocities (the second is 0 on a 2-D mesh), p). Per quantity: the stencil's shape (the
-// four differences v_k - v0 over the largest of them) and its amplitude (log2(1 + 1e4 M / r) / 4, M that largest
-// difference, r the root mean square of the 5 values). 25 features, padded with zeros to the 32 of two tensor-core
-// k-steps.
+// four differences v_k - v0 over the largest of them) and its amplitude (log2(1 + 1e4 M / s) / 4, M that largest
+// difference, s the quantity's physical scale at the cell: rho for the density, the sound speed for the velocities,
+// p + p_inf for the pressure). 25 features, padded with zeros to the 32 of two tensor-core k-steps.
 // Network: 32 -> 32 (ReLU) -> 32 (ReLU) -> 1 logit; weights and hidden activations in bfloat16, sums in float32
 // (mma.sync m16n8k16 bf16 with f32 accumulators, one warp per 16 cells). The cell is smooth (linear reconstruction)
 // when the logit is below a threshold chosen for a low miss rate; otherwise, and for every cell the network is not sure
 // about, WENO5-Z stays.
-// Label (what the network learns): the largest departure |omega_k - d_k| of the WENO-Z nonlinear weights from the linear
-// ones d = (0.1, 0.6, 0.3) over the quantities and the cell's two reconstructions (weno5z, cpp/src/Schemes.cpp:328-353),
-// above a label threshold.
+// Label (what the network learns): the largest gap |WENO5-Z - linear| between the cell's two WENO5-Z face values (the
+// reference's weno5z, cpp/src/Schemes.cpp:328-353) and the linear fifth-order upwind values there, over the quantities,
+// relative to the quantity's physical scale, above a label threshold: what the linear reconstruction would change at the
+// cell's faces. (WENO-Z weights that depart from the linear ones at a smooth extremum or where a velocity crosses zero
+// change the face values by a negligible amount, and such cells pass.)
 #pragma once
 
 #include <cuda_bf16.h>
@@ -49,22 +51,31 @@ struct SensorP {
 constexpr int kSensParams = sizeof(SensorP) / sizeof(float);
 
 // The five features of one quantity from its values at c-2 .. c+2: the shape of the stencil, (v_k - v0) / M for the four
-// neighbours with M = max_k |v_k - v0| (0 when the stencil is flat), and its amplitude against the quantity's size,
-// log2(1 + 1e4 M / r) / 4 with r the root mean square of the five values (WENO-Z compares the smoothness indicators with
-// an epsilon of 1e-6 r^2, so jumps of order 1e-3 r separate the two regimes). f[2] is the amplitude.
-__device__ __forceinline__ void sensor_quantity_features(const float v[5], float f[5]) {
-    float s = 0.0f, M = 0.0f;
+// neighbours with M = max_k |v_k - v0| (0 when the stencil is flat), attenuated by g = min(1, 1e4 M / s) (the shape of a
+// variation that is negligible against the quantity's physical scale s > 0, grid-scale noise of amplitude 1e-6 s for
+// instance, does not matter and must not look like a jump), and its amplitude log2(1 + 1e4 M / s) / 4. f[2] is the
+// amplitude.
+__device__ __forceinline__ void sensor_quantity_features(const float v[5], float scale, float f[5]) {
+    float M = 0.0f;
     const float v0 = v[2];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) {
-        s += v[k] * v[k];
-        M = fmaxf(M, fabsf(v[k] - v0));
-    }
-    const float r = s > 0.0f ? sqrtf(0.2f * s) : 1.0f;
-    const float iM = M > 0.0f ? 1.0f / M : 0.0f;
+    for (int k = 0; k < 5; ++k) M = fmaxf(M, fabsf(v[k] - v0));
+    const float a = 1e4f * M / scale;
+    const float g = fminf(1.0f, a);
+    const float iM = M > 0.0f ? g / M : 0.0f;
 #pragma unroll
     for (int k = 0; k < 5; ++k) f[k] = (v[k] - v0) * iM;
-    f[2] = 0.25f * __log2f(1.0f + 1e4f * M / r);
+    f[2] = 0.25f * __log2f(1.0f + a);
+}
+
+// The physical scale of sensor quantity sq (rho, u_n, u_t1, u_t2, p) at a cell of density rho and pressure p: rho, the
+// sound speed sqrt(gamma (p + p_inf) / rho), p + p_inf (rho and p + p_inf taken at least 1e-30).
+template <typename T> __device__ __forceinline__ T sensor_scale(int sq, T rho, T p, T gamma, T p_inf) {
+    const T tiny = T(1e-30);
+    const T r = rho > tiny ? rho : tiny, pp = p + p_inf > tiny ? p + p_inf : tiny;
+    if (sq == 0) return r;
+    if (sq == 4) return pp;
+    return sqrt(gamma * pp / r);
 }
 
 // Index of sensor quantity sq (rho, u_n, u_t1, u_t2, p) among the primitive variables [rho, u, v, p(, w)] for a sweep
@@ -76,20 +87,11 @@ template <int NV> __device__ __forceinline__ int sensor_var(int sq, int axis) {
     return k == 0 ? 1 : (k == 1 ? 2 : (NV == 5 ? 4 : -1));
 }
 
-// WENO-Z weights' departure from the linear ones for the value right of c2 from c0 .. c4 (double precision, the
-// reference's weno5z weights).
-__device__ __forceinline__ double weno5z_departure(double c0, double c1, double c2, double c3, double c4, double eps_rel) {
-    const double eps = eps_rel * (c0 * c0 + c1 * c1 + c2 * c2 + c3 * c3 + c4 * c4) * 0.2 + 1e-300;
-    const double s0 = c0 - 2.0 * c1 + c2, t0 = c0 - 4.0 * c1 + 3.0 * c2;
-    const double s1 = c1 - 2.0 * c2 + c3, t1 = c1 - c3;
-    const double s2 = c2 - 2.0 * c3 + c4, t2 = 3.0 * c2 - 4.0 * c3 + c4;
-    const double b0 = (13.0 / 12.0) * s0 * s0 + 0.25 * t0 * t0;
-    const double b1 = (13.0 / 12.0) * s1 * s1 + 0.25 * t1 * t1;
-    const double b2 = (13.0 / 12.0) * s2 * s2 + 0.25 * t2 * t2;
-    const double tau = fabs(b0 - b2);
-    const double a0 = 0.1 * (1.0 + tau / (b0 + eps)), a1 = 0.6 * (1.0 + tau / (b1 + eps)), a2 = 0.3 * (1.0 + tau / (b2 + eps));
-    const double is = 1.0 / (a0 + a1 + a2);
-    return fmax(fabs(a0 * is - 0.1), fmax(fabs(a1 * is - 0.6), fabs(a2 * is - 0.3)));
+// |WENO5-Z - linear| of the value right of c2 from c0 .. c4 (double precision: the reference's weno5z against the linear
+// fifth-order upwind value (2 c0 - 13 c1 + 47 c2 + 27 c3 - 3 c4) / 60).
+__device__ __forceinline__ double weno5z_face_gap(double c0, double c1, double c2, double c3, double c4, double eps_rel) {
+    const double lin = (2.0 * c0 - 13.0 * c1 + 47.0 * c2 + 27.0 * c3 - 3.0 * c4) / 60.0;
+    return fabs(weno5z(c0, c1, c2, c3, c4, eps_rel) - lin);
 }
 
 // ------------------------------------------------------------------------------------------------ tensor-core MLP

@@ -330,7 +330,7 @@ class Run:
 
     def set_sensor(self, sensor, threshold=0.0, every=0, radius=-1):
         """Gate the WENO5-Z reconstructions (mixed precision) with a trained ``fenice_b200.sensor.Sensor`` (None: off),
-        refreshed every `every` steps and grown by `radius` cells (defaults: 5 steps, ceil(cfl every) + 1 cells)."""
+        refreshed every `every` steps and grown by `radius` cells (defaults: 10 steps, ceil(cfl every) + 1 cells)."""
         ptr = None if sensor is None else sensor.weights_ptr()
         self._check(self.lib.fvg_set_sensor(self.h, ptr, float(threshold), int(every), int(radius)), "set_sensor")
 

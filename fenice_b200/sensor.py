@@ -5,7 +5,8 @@ fenice_b200/csrc/sensor.cuh. This module holds the float32 master parameters, th
 torch tensors on the GPU (torch provides the device memory and the stream; every computation is a kernel of
 libfenice_gpu.so) and drives:
 
-* ``samples(run, tau, keep_div)``: features and WENO-Z departures of a run's current state (the troubled (cell, axis)
+* ``samples(run, tau, keep_div)``: features and label statistics (the largest |WENO5-Z - linear| face-value gap of the
+  cell along the axis, relative to the quantity's physical scale) of a run's current state (the troubled (cell, axis)
   pairs and every keep_div-th other one);
 * ``train(X, y, ...)``: Adam over minibatches, forward and backward passes on the tensor cores;
 * ``logits(X)`` and ``choose_threshold``: the logit below which a cell is passed to the linear reconstruction, chosen so
@@ -19,7 +20,10 @@ import numpy as np
 from . import initial
 from .runtime import FVG_OK, Run, load_library
 
-TAU = 0.01   # label: a cell is troubled along an axis when its WENO-Z weights depart from the linear ones by more
+# label: a cell is troubled along an axis when a WENO5-Z face value of it differs from the linear one by more than TAU of
+# the quantity's physical scale (the Taylor-Green vortex at 256^3 stays below 2e-7 everywhere; shocks and contacts reach
+# 1e-2 to 1)
+TAU = 1e-5
 
 
 def _p(t):
@@ -186,9 +190,10 @@ def quadrant_training_data(sensor, seeds, n=512, t_end=0.25, snapshots=5, tau=TA
     return torch.cat(Xs), torch.cat(Ds)
 
 
-def taylor_green_training_data(sensor, n=64, steps=200, snapshots=5, tau=TAU, keep_div=8, precision=0):
+def taylor_green_training_data(sensor, n=64, steps=200, snapshots=5, tau=TAU, keep_div=8, precision=0, at=None):
     """Samples of the 3-D Taylor-Green vortex (WENO5-Z + low-Mach HLLC + SSP-RK3, viscous Re 1600) at `snapshots`
-    evenly spaced steps."""
+    evenly spaced steps, or at the steps listed in `at` (the first steps carry the grid-scale acoustic noise of the
+    initial pressure field, of negligible amplitude)."""
     import math
 
     torch = sensor.torch
@@ -198,8 +203,11 @@ def taylor_green_training_data(sensor, n=64, steps=200, snapshots=5, tau=TAU, ke
                   **{f"bc_{a}{s}": "periodic" for a in "xyz" for s in ("min", "max")})
     run = Run(params, U=initial.taylor_green_3d(n), precision=precision, device=sensor.dev.index)
     Xs, Ds = [], []
-    for k in range(snapshots):
-        run.run(1e30, max_steps=steps // snapshots)
+    marks = list(at) if at is not None else [steps // snapshots * (k + 1) for k in range(snapshots)]
+    done = 0
+    for k, mark in enumerate(marks):
+        run.run(1e30, max_steps=mark - done)
+        done = mark
         X, D, _ = sensor.samples(run, tau, keep_div, seed=77 + k, capacity=run.ncells * 3)
         Xs.append(X.clone())
         Ds.append(D.clone())

@@ -4,8 +4,9 @@
 
 Training data (labels from plain WENO5-Z runs in FP64, the reference's arithmetic): 64 seeded four-quadrant Riemann
 problems at 512^2 (WENO5-Z + HLLC + SSP-RK3, CFL 0.4, to t = 0.25, 4 snapshots), 8 seeded eight-octant problems at 64^3
-and the 3-D Taylor-Green vortex at 64^3 (Re 1600, 200 steps, 5 snapshots); of each snapshot every troubled (cell, axis)
-pair (WENO-Z weights departing from the linear ones by more than 0.01) and every 16th other one. Adam on the library's
+(every troubled (cell, axis) pair, a WENO5-Z face value more than 1e-5 of the quantity's scale from the linear one, and
+every 16th other one) and the 3-D Taylor-Green vortex at 64^3 (Re 1600, steps 3, 10, 40, 100 and 200) and 128^3 (steps
+3 and 20), every 4th pair. Adam on the library's
 tensor-core forward and backward kernels. Held-out data (4 quadrant seeds at 512^2, one octant seed, the Taylor-Green
 vortex at step 100; every (cell, axis) pair) sets the logit threshold: the largest that passes at most 0.2 % of the
 troubled pairs to the linear reconstruction. Prints the data sizes, the loss per epoch and the held-out figures.
@@ -60,6 +61,10 @@ def held_out(sensor):
     run.run(1e30, max_steps=100)
     X, D, _ = sensor.samples(run, mode=0)
     sets["Taylor-Green 64^3 step 100"] = (X.clone(), D.clone())
+    run = Run(dict(params, nx=128, ny=128, nz=128), U=initial.taylor_green_3d(128))
+    run.run(1e30, max_steps=6)
+    X, D, _ = sensor.samples(run, mode=0)
+    sets["Taylor-Green 128^3 step 6"] = (X.clone(), D.clone())
     return sets
 
 
@@ -74,7 +79,8 @@ def main():
     s = Sensor(seed=0)
     parts = [quadrant_training_data(s, seeds=range(args.seeds), n=args.n, t_end=0.25, snapshots=4, keep_div=16),
              octant_training_data(s, seeds=range(8), n=64, t_end=0.2, snapshots=4, keep_div=16),
-             taylor_green_training_data(s, n=64, steps=200, snapshots=5, keep_div=16)]
+             taylor_green_training_data(s, n=64, at=(3, 10, 40, 100, 200), keep_div=4),
+             taylor_green_training_data(s, n=128, at=(3, 20), keep_div=4)]
     X = torch.cat([p[0] for p in parts])
     D = torch.cat([p[1] for p in parts])
     del parts

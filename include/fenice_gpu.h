@@ -279,8 +279,9 @@ int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long long plane
  * A 32 -> 32 -> 32 -> 1 MLP reads a cell's 5-cell stencil along a sweep axis (25 features: rho, normal and tangential
  * velocities, p) and decides whether the cell's two reconstructions along that axis take the linear fifth-order upwind
  * values (logit below the threshold) or WENO5-Z. Weights and activations are bfloat16 on the tensor cores with float32
- * sums. The label it learns: the cell's WENO-Z nonlinear weights depart from the linear ones (0.1, 0.6, 0.3) by more
- * than a threshold tau. Training runs on the GPU through these calls, on device buffers the caller owns:
+ * sums. The label it learns: one of the cell's two WENO5-Z face values along the axis differs from the linear
+ * fifth-order upwind value there by more than tau times the quantity's physical scale at the cell (rho; the sound speed
+ * for the velocities; p + p_inf). The amplitude features are taken against the same scales. Training runs on the GPU through these calls, on device buffers the caller owns:
  *   fvg_sensor_extract  features (32 floats per sample) and the departure of every (cell, axis) of a run's state
  *                       (mode 0, at index cell * dim + axis) or of the troubled ones and every keep_div-th other one
  *                       (mode 1, appended at the device counter *count up to capacity); stats (device, may be NULL):
@@ -291,7 +292,7 @@ int fvg_residual_noalloc(const fvg_config* cfg, const double* U, long long plane
  *   fvg_sensor_pack     device weights of float32 parameters; fvg_sensor_infer: logits of n feature rows
  * Parameter layout (floats): W1[32][32] (inputs 25..31 unused), b1[32], W2[32][32], b2[32], w3[32], b3.
  * fvg_set_sensor gates a mixed-precision WENO5-Z run with device weights (copied; NULL: plain WENO5-Z again): every
- * `every` steps (<= 0: 5) a kernel evaluates the network on every (cell, axis) of the state, the troubled set is grown by
+ * `every` steps (<= 0: 10) a kernel evaluates the network on every (cell, axis) of the state, the troubled set is grown by
  * `radius` cells along every axis (< 0: ceil(cfl every) + 1, the distance a wave travels until the next refresh, plus
  * one) and reduced to the stage kernels' tiles: a tile whose cells are all untroubled along an axis takes the linear
  * reconstruction for every face of that sweep. fvg_get_sensor_counts returns the (tile, axis) pairs the refreshes

@@ -1,15 +1,18 @@
 """Test infrastructure (the oracle), not part of the product: a numpy restatement of the troubled-cell sensor's inputs,
 labels and network, the check of the GPU sensor kernels (fenice_b200/csrc/sensor.cuh).
 
+* scales(Q5): the physical scale of each quantity at the centre cell: rho, the sound speed sqrt(gamma (p + p_inf) / rho)
+  for the three velocities, p + p_inf (rho and p + p_inf at least 1e-30).
 * stencil_features(Q5): the 25 features of one (cell, axis): the 5 cells c-2 .. c+2 along the axis, 5 primitive
   quantities each (rho, normal velocity, the two tangential velocities (0 on a 2-D mesh), p). Per quantity, with
-  M = max_k |v_k - v0| and r the root mean square of the 5 values (1 when all are 0): the shape (v_k - v0) / M of the
-  four neighbours (0 when M = 0) and, in the centre slot, the amplitude log2(1 + 1e4 M / r) / 4; quantity-major, padded
-  with zeros to 32 inputs.
+  M = max_k |v_k - v0| and s its scale: the shape (v_k - v0) / M of the four neighbours (0 when M = 0) times
+  min(1, 1e4 M / s) and, in the centre slot, the amplitude log2(1 + 1e4 M / s) / 4; quantity-major, padded with zeros to
+  32 inputs.
 * departure(Q5): the label statistic: over the 5 quantities and both WENO5-Z reconstructions centred on the cell (the
-  value at its right face from c-2 .. c+2 and at its left face from c+2 .. c-2), the largest |omega_k - d_k| of the
-  WENO-Z weights (the reference's weno5z, cpp/src/Schemes.cpp:328-353) against the linear ones d = (0.1, 0.6, 0.3). A cell
-  is troubled along the axis when it exceeds the label threshold.
+  value at its right face from c-2 .. c+2 and at its left face from c+2 .. c-2), the largest gap between the WENO5-Z
+  value (the reference's weno5z, cpp/src/Schemes.cpp:328-353) and the linear fifth-order upwind value
+  (2 c0 - 13 c1 + 47 c2 + 27 c3 - 3 c4) / 60, relative to the quantity's scale. A cell is troubled along the axis when it
+  exceeds the label threshold.
 * mlp_forward / mlp_loss_grad: 32 -> 32 -> 32 -> 1 with ReLU, the product's arithmetic emulated: inputs, weights and
   hidden activations rounded to bfloat16 where the kernels feed them to the tensor cores, sums and biases in float32 (here
   float64 on the rounded operands), loss the mean class-weighted binary cross-entropy with logits.
@@ -38,17 +41,27 @@ def axis_quantities(W, axis):
     return np.stack([W[..., 0], n, t1, t2, W[..., 3]], axis=-1)
 
 
-def stencil_features(Q5):
+def scales(Q5, gamma=1.4, p_inf=0.0):
+    """(n, 5, 5) stencil quantities -> (n, 5) physical scale of each quantity at the centre cell."""
+    Q5 = np.asarray(Q5, dtype=np.float64)
+    rho = np.maximum(Q5[:, 2, 0], 1e-30)
+    pp = np.maximum(Q5[:, 2, 4] + p_inf, 1e-30)
+    c = np.sqrt(gamma * pp / rho)
+    return np.stack([rho, c, c, c, pp], axis=1)
+
+
+def stencil_features(Q5, gamma=1.4, p_inf=0.0):
     """(n, 5, 5) stencil quantities -> (n, 32) features (quantity-major: 5 entries per quantity, positions c-2 .. c+2
     with the amplitude in the centre entry; columns 25 .. 31 zero)."""
+    sc = scales(Q5, gamma, p_inf).astype(np.float32)
     Q5 = np.asarray(Q5, dtype=np.float32)
-    r = np.sqrt(np.float32(0.2) * np.sum(Q5 * Q5, axis=1))
-    r = np.where(r > 0, r, np.float32(1.0)).astype(np.float32)
     d = Q5 - Q5[:, 2:3, :]
     M = np.abs(d).max(axis=1)
-    iM = np.where(M > 0, np.float32(1.0) / np.where(M > 0, M, 1), 0).astype(np.float32)
+    a = (np.float32(1e4) * M / sc).astype(np.float32)
+    g = np.minimum(np.float32(1.0), a)
+    iM = np.where(M > 0, g / np.where(M > 0, M, 1), 0).astype(np.float32)
     f = d * iM[:, None, :]
-    f[:, 2, :] = 0.25 * np.log2(1.0 + 1e4 * M / r)
+    f[:, 2, :] = 0.25 * np.log2(1.0 + a)
     out = np.zeros((len(Q5), NK), dtype=np.float32)
     out[:, :NF] = np.transpose(f, (0, 2, 1)).reshape(len(Q5), NF)
     return out
@@ -69,14 +82,39 @@ def weno5z_weights(c, eps_rel=1e-6):
     return a / a.sum(axis=1, keepdims=True)
 
 
-def departure(Q5, eps_rel=1e-6):
-    """(n, 5, 5) -> (n,) the largest departure of the WENO-Z weights from the linear ones."""
+def weno5z_value(c, eps_rel=1e-6):
+    """The WENO5-Z value at the face right of c[:, 2] from c[:, 0..4] (float64, the operation order of the reference's
+    weno5z, cpp/src/Schemes.cpp:341-353)."""
+    c0, c1, c2, c3, c4 = (c[:, k] for k in range(5))
+    eps = eps_rel * (c0 * c0 + c1 * c1 + c2 * c2 + c3 * c3 + c4 * c4) * 0.2 + 1e-300
+    p0 = (2 * c0 - 7 * c1 + 11 * c2) / 6
+    p1 = (-c1 + 5 * c2 + 2 * c3) / 6
+    p2 = (2 * c2 + 5 * c3 - c4) / 6
+    s0, t0 = c0 - 2 * c1 + c2, c0 - 4 * c1 + 3 * c2
+    s1, t1 = c1 - 2 * c2 + c3, c1 - c3
+    s2, t2 = c2 - 2 * c3 + c4, 3 * c2 - 4 * c3 + c4
+    b0 = 13 / 12 * s0 * s0 + 0.25 * t0 * t0
+    b1 = 13 / 12 * s1 * s1 + 0.25 * t1 * t1
+    b2 = 13 / 12 * s2 * s2 + 0.25 * t2 * t2
+    tau = np.abs(b0 - b2)
+    a0, a1, a2 = 0.1 * (1 + tau / (b0 + eps)), 0.6 * (1 + tau / (b1 + eps)), 0.3 * (1 + tau / (b2 + eps))
+    return (a0 * p0 + a1 * p1 + a2 * p2) / (a0 + a1 + a2)
+
+
+def linear_value(c):
+    """The linear fifth-order upwind value at the face right of c[:, 2]."""
+    return (2 * c[:, 0] - 13 * c[:, 1] + 47 * c[:, 2] + 27 * c[:, 3] - 3 * c[:, 4]) / 60
+
+
+def departure(Q5, eps_rel=1e-6, gamma=1.4, p_inf=0.0):
+    """(n, 5, 5) -> (n,) the largest |WENO5-Z - linear| face-value gap relative to the quantity's scale."""
     Q5 = np.asarray(Q5, dtype=np.float64)
+    sc = scales(Q5, gamma, p_inf)
     out = np.zeros(len(Q5))
     for q in range(Q5.shape[2]):
         c = Q5[:, :, q]
         for cc in (c, c[:, ::-1]):
-            out = np.maximum(out, np.abs(weno5z_weights(cc, eps_rel) - D_LIN).max(axis=1))
+            out = np.maximum(out, np.abs(weno5z_value(cc, eps_rel) - linear_value(cc)) / sc[:, q])
     return out
 
 

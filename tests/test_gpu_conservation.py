@@ -97,8 +97,9 @@ def test_totals_conserved(name, make, form):
     if form == "gated":
         lin, ev = run.sensor_counts()
         msg += f"; gate {lin} of {ev} tile-axes linear"
-        # the check needs seams between linear and WENO5-Z tiles
-        assert 0 < lin < ev
+        # the jump boxes put linear and WENO5-Z tiles side by side (the seams the check is about); the Taylor-Green
+        # boxes are smooth and pass linear
+        assert (0 < lin < ev) if name.startswith("jump") else lin > 0
     print(msg)
     assert np.all(drift <= BOUND[(form, name.startswith("tgv"))]), drift
     run.close()

@@ -1,0 +1,105 @@
+"""What the trained network gains over the method without it: the mixed WENO5-Z form gated by the learned sensor
+(fenice_b200/sensor_weights.npz, its threshold, the refresh every 10 steps) against the same form without the gate, from
+the same state on the same GPU.
+
+* Taylor-Green vortex 128^3 (the benchmark configuration, reduced): the network passes the smooth flow to the linear
+  fifth-order reconstruction (at least 90 % of the tile-axes), the step, the network's refresh included, takes less time
+  than the ungated step (at most 0.97 of it), the stage kernel at most 0.90 of the ungated one, and after 13 steps the
+  state is within L1(rho) 1e-6 of the ungated run and 1e-4 of the plain FP64 run.
+* A seeded four-quadrant problem at 512^2 (C3, reduced) to t = 0.1: shocks, contacts and their neighbourhoods stay
+  WENO5-Z (the linear share below 1), and the gated run is as close to the plain FP64 run as the ungated one (L1(rho)
+  within 1.5 times its distance: the gate adds no error beyond the FP32 arithmetic's).
+Times: CUDA events on the run's stream, the better of two timed runs of 10 steps after 3 untimed ones.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from fenice_b200 import Run, initial
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+HERE = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def sensor():
+    from fenice_b200.sensor import Sensor
+
+    s = Sensor.load(os.path.join(HERE, "fenice_b200", "sensor_weights.npz"), device=0)
+    return s, float(s.meta["threshold"])
+
+
+def l1(a, b):
+    return float(np.abs(a[:, 0] - b[:, 0]).sum() / np.abs(b[:, 0]).sum())
+
+
+def timed(params, U0, gate, steps=10):
+    """(ms per step, stage kernel ms per launch, linear share, the run) of the better of two timed runs."""
+    best = None
+    for _ in range(2):
+        run = Run(params, U=U0, precision=1)
+        if gate:
+            run.set_sensor(*gate, every=10)
+        run.run(1e30, max_steps=3)
+        ext = torch.cuda.ExternalStream(run.stream())
+        run.set_timing(True)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(ext)
+        assert run.run(1e30, max_steps=steps) == steps
+        b.record(ext)
+        torch.cuda.synchronize()
+        tm = run.timing()
+        lin, ev = run.sensor_counts() if gate else (0, 1)
+        res = (a.elapsed_time(b) / steps, tm["stage_ms"] / max(tm["stage_launches"], 1), lin / max(ev, 1), run)
+        if best is None or res[0] < best[0]:
+            if best is not None:
+                best[3].close()
+            best = res
+        else:
+            run.close()
+    return best
+
+
+def test_gate_pays_on_the_taylor_green_vortex():
+    import bench
+
+    n = 128
+    params, U0 = bench.workload(n), bench.tgv_state(n)
+    g = sensor()
+    ms_m, st_m, _, mixed = timed(params, U0, None)
+    ms_g, st_g, share, gated = timed(params, U0, g)
+    plain = Run(params, U=U0, precision=0)
+    plain.run(1e30, max_steps=13)
+    d_mixed = l1(gated.state(), mixed.state())
+    d_plain = l1(gated.state(), plain.state())
+    print(f"\nTaylor-Green {n}^3: gated {ms_g:.3f} ms per step (stage {st_g:.3f} ms), ungated {ms_m:.3f} ({st_m:.3f}); "
+          f"speed-up {ms_m / ms_g:.3f}, linear share {share:.3f}; L1(rho) against the ungated run {d_mixed:.2e}, against FP64 {d_plain:.2e}")
+    for r in (mixed, gated, plain):
+        r.close()
+    assert share >= 0.9
+    assert st_g <= 0.90 * st_m
+    assert ms_g <= 0.97 * ms_m
+    assert d_mixed <= 1e-6 and d_plain <= 1e-4
+
+
+def test_gate_keeps_weno_at_discontinuities():
+    n = 512
+    params, U0 = initial.quadrant_params(n), initial.riemann_quadrants(n, 1000)
+    g = sensor()
+    plain = Run(params, U=U0, precision=0)
+    plain.run(0.1)
+    mixed = Run(params, U=U0, precision=1)
+    mixed.run(0.1)
+    gated = Run(params, U=U0, precision=1)
+    gated.set_sensor(*g, every=10)
+    gated.run(0.1)
+    lin, ev = gated.sensor_counts()
+    d_g, d_m = l1(gated.state(), plain.state()), l1(mixed.state(), plain.state())
+    print(f"\nquadrants {n}^2 to t = 0.1: {lin / ev:.3f} of the tile-axes linear; L1(rho) against FP64: gated {d_g:.2e}, ungated {d_m:.2e}")
+    for r in (plain, mixed, gated):
+        r.close()
+    assert 0.2 < lin / ev < 1.0
+    assert d_g <= 1.5 * d_m + 1e-9
