@@ -11,14 +11,35 @@ template <int DIM> struct MTile;
 template <> struct MTile<3> { static constexpr int X = 8, Y = 8, Z = 8, NT = 384; };
 template <> struct MTile<2> { static constexpr int X = 16, Y = 15, Z = 1, NT = 256; };
 
+// the kernel that stages interior tiles by TMA: 3-D WENO5-Z lean kernels, when the run passes tensor maps (StageArgs::tma)
+template <int DIM, int RECON, bool FULL> constexpr bool kHasTma = DIM == 3 && RECON == kWeno5 && !FULL;
+
+template <int RIEMANN, bool GATED> struct TmaK {
+    using T = MTile<3>;
+    using L = MixedTmaShape<T::X, T::Y, T::Z>;
+    static cudaError_t prepare() {
+        return cudaFuncSetAttribute(mixed_stage_kernel_tma<RIEMANN, T::X, T::Y, T::Z, T::NT, GATED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)L::SMEM_BYTES);
+    }
+    static cudaError_t launch(const StageArgs& a, int nblocks, cudaStream_t s) {
+        mixed_stage_kernel_tma<RIEMANN, T::X, T::Y, T::Z, T::NT, GATED><<<nblocks, T::NT, L::SMEM_BYTES, s>>>(a, *static_cast<const TmaMaps*>(a.tma));
+        return cudaGetLastError();
+    }
+};
+
 template <int DIM, int RECON, int RIEMANN, bool FULL> struct MixedK {
     using T = MTile<DIM>;
     using S = MixedShape<DIM, RECON, T::X, T::Y, T::Z>;
     static cudaError_t prepare() {
-        return cudaFuncSetAttribute(mixed_stage_kernel<DIM, RECON, RIEMANN, T::X, T::Y, T::Z, T::NT, false, FULL>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM_BYTES);
+        cudaError_t e = cudaFuncSetAttribute(mixed_stage_kernel<DIM, RECON, RIEMANN, T::X, T::Y, T::Z, T::NT, false, FULL>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM_BYTES);
+        if constexpr (kHasTma<DIM, RECON, FULL>)
+            if (e == cudaSuccess) e = TmaK<RIEMANN, false>::prepare();
+        return e;
     }
     static cudaError_t launch(const StageArgs& a, int nblocks, cudaStream_t s) {
+        if constexpr (kHasTma<DIM, RECON, FULL>)
+            if (a.tma) return TmaK<RIEMANN, false>::launch(a, nblocks, s);
         mixed_stage_kernel<DIM, RECON, RIEMANN, T::X, T::Y, T::Z, T::NT, false, FULL><<<nblocks, T::NT, S::SMEM_BYTES, s>>>(a);
         return cudaGetLastError();
     }
@@ -29,10 +50,15 @@ template <int DIM, int RIEMANN, bool FULL> struct GatedK {
     using T = MTile<DIM>;
     using S = MixedShape<DIM, kWeno5, T::X, T::Y, T::Z>;
     static cudaError_t prepare() {
-        return cudaFuncSetAttribute(mixed_stage_kernel<DIM, kWeno5, RIEMANN, T::X, T::Y, T::Z, T::NT, true, FULL>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM_BYTES);
+        cudaError_t e = cudaFuncSetAttribute(mixed_stage_kernel<DIM, kWeno5, RIEMANN, T::X, T::Y, T::Z, T::NT, true, FULL>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM_BYTES);
+        if constexpr (kHasTma<DIM, kWeno5, FULL>)
+            if (e == cudaSuccess) e = TmaK<RIEMANN, true>::prepare();
+        return e;
     }
     static cudaError_t launch(const StageArgs& a, int nblocks, cudaStream_t s) {
+        if constexpr (kHasTma<DIM, kWeno5, FULL>)
+            if (a.tma) return TmaK<RIEMANN, true>::launch(a, nblocks, s);
         mixed_stage_kernel<DIM, kWeno5, RIEMANN, T::X, T::Y, T::Z, T::NT, true, FULL><<<nblocks, T::NT, S::SMEM_BYTES, s>>>(a);
         return cudaGetLastError();
     }

@@ -27,6 +27,7 @@
 #include "sensor.cuh"
 #include "sensor_api.h"
 #include "stage.cuh"
+#include "tma.cuh"
 #include "viscous.cuh"
 
 #include <algorithm>
@@ -688,6 +689,9 @@ struct fvg_run {
     double* d_bload = nullptr;
     // fvg_monitor: per-CTA partial sums (4 per CTA) and the four results (allocated at the first call)
     double* d_mon = nullptr;
+    // TMA tensor maps of U, Ut and R for the stage kernels that stage their interior tiles by TMA (tma_on: built)
+    TmaMaps tma[3];
+    bool tma_on = false;
     // a section body: its vertices where it was placed at t = 0 (the reference the poses turn about the pivot), and how far
     // a vertex lies from the pivot (ImmersedBoundary::enable_motion's reach)
     std::vector<double> ref_poly;
@@ -895,7 +899,36 @@ StageArgs stage_args(fvg_run* r, const double* Uin, const double* U0, double* ou
     a.gate = gate;
     for (int d = 0; d < 3; ++d) a.tiles[d] = r->tiles[d];
     a.sens_flags = r->sens ? r->sens_tiles : nullptr;
+    a.tma = !r->tma_on ? nullptr : Uin == r->U ? &r->tma[0] : Uin == r->Ut ? &r->tma[1] : Uin == r->R ? &r->tma[2] : nullptr;
     return a;
+}
+
+// The TMA tensor maps of the run's state buffers U, Ut and R (tma.cuh) for the 3-D mixed WENO5-Z kernels of a whole mesh
+// without an immersed body (lean kernels); cuTensorMapEncodeTiled through the runtime's driver entry point. A mesh
+// whose row is not a multiple of 16 bytes (nx odd) keeps the index-mapping loader.
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+void build_tma_maps(fvg_run* r) {
+    r->tma_on = false;
+    const fvg_config& c = r->cfg;
+    if (r->dim != 3 || c.precision != FVG_PREC_MIXED || c.reconstruction != FVG_RECON_WENO5 || r->full || r->ibm || c.use_ibm || c.nx % 2 != 0)
+        return;
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+        return;
+    const EncodeTiled encode = reinterpret_cast<EncodeTiled>(fn);
+    const cuuint64_t dims[4] = {(cuuint64_t)r->m.nx, (cuuint64_t)r->m.ny, (cuuint64_t)r->m.nz, 5};
+    const cuuint64_t strides[3] = {(cuuint64_t)r->m.nx * 8, (cuuint64_t)r->m.nx * r->m.ny * 8, (cuuint64_t)r->m.plane * 8};
+    const cuuint32_t boxes[3][4] = {{16, 8, 8, 5}, {8, 14, 8, 5}, {8, 8, 14, 5}};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    double* bufs[3] = {r->U, r->Ut, r->R};
+    for (int b = 0; b < 3; ++b)
+        for (int a = 0; a < 3; ++a)
+            if (encode(&r->tma[b].m[a], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, bufs[b], dims, strides, boxes[a], es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                       CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                return;
+    r->tma_on = true;
 }
 
 ViscArgs visc_args(fvg_run* r, const double* Uin, double* bmv, const int* gate) {
@@ -2058,6 +2091,7 @@ int create_run(const fvg_config* cfg, int nparts, int part, bool as_part, fvg_ru
     for (double** p : {&run->U, &run->Ut, &run->R, &run->Rv})
         if (*p) cudaMemsetAsync(*p, 0, sbytes, run->stream), *p += run->goff;
     if (run->xred) cudaMemsetAsync(run->xred, 0, sizeof(double) * 2, run->stream);
+    build_tma_maps(run);
     if (c.positivity_fallback) {
         if (cudaMalloc(&run->fb_flags, run->m.ncells) != cudaSuccess || cudaMalloc(&run->fb_grew, sizeof(int)) != cudaSuccess) {
             run->err = "device allocation failed";
@@ -2297,6 +2331,7 @@ int fvg_residual(fvg_run* run, double predictor_half_dt, double* R, size_t ncell
     Ctl h;
     int rc = read_ctl(run, &h);
     if (rc) return rc;
+    if (h.status == 5) return fail(run, FVG_ERR_CUDA, "a TMA copy of a stage tile did not complete");
     if (h.status == 3) {
         char msg[256];
         std::snprintf(msg, sizeof msg, "time-dependent boundary values: not finite, or rho_in or p_out not positive, at t = %.17g", h.stage_t);

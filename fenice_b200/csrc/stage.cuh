@@ -47,6 +47,9 @@ struct StageArgs {
     const unsigned char* sens_flags;
     // positivity_fallback: the cells flagged in this stage (null: none); a face next to one takes the cells' states
     const unsigned char* fb;
+    // the TMA tensor maps of U for the three sweeps (a host address of TmaMaps, tma.cuh; null: the index-mapping loader
+    // only): the launch of a kernel that stages interior tiles by TMA passes them as a kernel parameter
+    const void* tma;
 };
 
 // positivity_fallback's flag of a stencil position (Schemes.cpp:548-557): the cell's; across a periodic seam the wrapped

@@ -35,6 +35,9 @@ SLAB_CASES = [
      69, 4, (1, 2, 3), 0),
     ("mixed_w5_rk3_visc_3d", dict(nx=20, ny=16, nz=18, reconstruction="weno5", riemann_solver="lowmach", time_scheme="SSP Runge-Kutta 3",
                                   use_viscous=True, mu=0.01, **TGV), 70, 4, (2, 3), 1),
+    # the whole run's mixed WENO5-Z kernel stages its interior tiles by TMA; the parts' kernels load every tile by index mapping
+    ("mixed_w5_rk3_visc_64_tma", dict(nx=64, ny=64, nz=64, reconstruction="weno5", riemann_solver="lowmach", time_scheme="SSP Runge-Kutta 3",
+                                      use_viscous=True, mu=0.01, **TGV), 72, 4, (1, 2), 1),
     # non-reflecting outlets: on x, whose tangential z neighbours cross the part interfaces, and at the low z end
     ("nrbc_w5_rk3_visc_3d", dict(nx=12, ny=10, nz=13, reconstruction="weno5", time_scheme="SSP Runge-Kutta 3", use_viscous=True, mu=0.01,
                                  **B("transmissive", "nonreflecting", "periodic", "periodic", z=("nonreflecting", "wall"))), 71, 3, (2, 3), 0),
