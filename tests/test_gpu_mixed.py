@@ -69,3 +69,34 @@ def test_mixed_within_l1_bar(name, params, init, t_end, steps):
     print(f"\n{name}: {n_p} steps; " + "; ".join(f"{k}: L1 {v[0]:.2e} Linf {v[1]:.2e}" for k, v in errs.items()))
     assert errs["rho"][0] <= 1e-4
     assert all(np.isfinite(v[0]) for v in errs.values())
+
+
+def perturbed(U, seed):
+    """U with every value moved by one unit in the last place of an FP32 mantissa (relative 2^-24, random sign)."""
+    rng = np.random.default_rng(seed)
+    return U * (1.0 + rng.choice([-1.0, 1.0], U.shape) * 2.0 ** -24)
+
+
+def test_reduced_quadrants_within_bar_and_the_schemes_own_sensitivity():
+    """A reduced C3 (the held-out four-quadrant problem, seed 2048, 1024^2 to t = 0.25): the mixed form within the L1 bar of
+    the FP64 form. Beside it the FP64 form itself from its input moved by FP32 rounding (2^-24 relative): its distance from the
+    unperturbed FP64 run is what an input perturbation at FP32 rounding does to this scheme on this problem. Measured on a B200:
+    mixed 3.8e-6, the perturbed FP64 run 5.3e-5; at 2048^2 (the full C3) 1.2e-3 and 2.1e-3: there the scheme's own
+    sensitivity already exceeds the bar, whatever the arithmetic."""
+    from fenice_b200 import initial
+
+    n = 1024
+    params, U0 = initial.quadrant_params(n), initial.riemann_quadrants(n, 2048)
+    runs = {}
+    for key, U, prec in (("fp64", U0, 0), ("fp64_perturbed", perturbed(U0, 99), 0), ("mixed", U0, 1)):
+        r = Run(params, U=U, precision=prec)
+        steps = r.run(0.25)
+        runs[key] = (r.state(), steps)
+        r.close()
+    ref = runs["fp64"][0]
+    d_m = rel_errors(runs["mixed"][0], ref)["rho"][0]
+    d_p = rel_errors(runs["fp64_perturbed"][0], ref)["rho"][0]
+    print(f"\nquadrants {n}^2 to t = 0.25 ({runs['fp64'][1]} steps): L1(rho) against FP64: mixed {d_m:.2e}; "
+          f"FP64 from the input moved by 2^-24: {d_p:.2e}")
+    assert d_m <= 1e-4
+    assert d_m <= 2 * d_p
