@@ -18,7 +18,7 @@ SRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfenice_gpu.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["runtime.cu", "mixed.cu", "batch.cu", "batch_mixed.cu", "sensor.cu", "expr.cu"]
+SOURCES = ["runtime.cu", "mixed.cu", "batch.cu", "batch_mixed.cu", "sensor.cu", "expr.cu", "cells.cu"]
 HEADERS = ["physics.cuh", "grid.cuh", "stage.cuh", "viscous.cuh", "hancock.cuh", "mixed.cuh", "mixed_api.h", "batch.cuh", "batch_api.h", "host_common.h", "ibm.cuh", "ibm_host.h", "sensor.cuh", "sensor_api.h", "expr.h", "expr.cuh", "fourth.cuh", "tma.cuh"]
 
 COMMON_FLAGS = [
@@ -36,6 +36,7 @@ UNIT_FLAGS = {
     "batch_mixed.cu": ["--use_fast_math"],
     "sensor.cu": ["--use_fast_math"],
     "expr.cu": ["--fmad=false", "-prec-div=true", "-prec-sqrt=true"],
+    "cells.cu": ["--fmad=false", "-prec-div=true", "-prec-sqrt=true"],
 }
 
 

@@ -36,7 +36,9 @@ EXPORTS = ["fvg_abi_version", "fvg_create", "fvg_destroy", "fvg_last_error", "fv
            "fvg_sensor_sizes", "fvg_sensor_extract", "fvg_sensor_grad", "fvg_sensor_adam", "fvg_sensor_pack", "fvg_sensor_infer",
            "fvg_set_sensor", "fvg_get_sensor_counts", "fvg_get_sensor_gate", "fvg_ibm_loads", "fvg_monitor", "fvg_get_body_state", "fvg_set_body_state",
            "fvg_create_part", "fvg_part_info", "fvg_part_buffers", "fvg_part_begin", "fvg_part_phase", "fvg_part_status",
-           "fvg_expr_eval"]
+           "fvg_expr_eval",
+           "fvg_cells_create", "fvg_cells_destroy", "fvg_cells_last_error", "fvg_cells_info", "fvg_cells_upload_state",
+           "fvg_cells_download_state", "fvg_cells_residual", "fvg_cells_step", "fvg_cells_advance", "fvg_cells_stream"]
 
 _lib = None
 ABI_VERSION = 9   # FVG_ABI_VERSION of include/fenice_gpu.h
@@ -119,6 +121,17 @@ def load_library(path=LIB_PATH):
     lib.fvg_part_status.argtypes = [c_p, ip, ip, dp, dp, dp]
     lib.fvg_expr_eval.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_char_p), dp, ctypes.c_int, dp, dp, dp, ctypes.c_double, ctypes.c_size_t, dp,
                                   ctypes.c_char_p, ctypes.c_size_t]
+    lib.fvg_cells_create.argtypes = [ctypes.POINTER(P.FvgConfig), ctypes.c_int, ip, ip, ip, ip, ctypes.POINTER(c_p)]
+    lib.fvg_cells_destroy.argtypes = [c_p]
+    lib.fvg_cells_last_error.argtypes = [c_p]
+    lib.fvg_cells_last_error.restype = ctypes.c_char_p
+    lib.fvg_cells_info.argtypes = [c_p, ll, ll]
+    lib.fvg_cells_upload_state.argtypes = [c_p, dp, ctypes.c_size_t]
+    lib.fvg_cells_download_state.argtypes = [c_p, dp, ctypes.c_size_t]
+    lib.fvg_cells_residual.argtypes = [c_p, dp, ctypes.c_size_t, dp]
+    lib.fvg_cells_step.argtypes = [c_p, ctypes.c_double, ctypes.c_double, dp]
+    lib.fvg_cells_advance.argtypes = [c_p, ctypes.c_double, ctypes.c_int, dp]
+    lib.fvg_cells_stream.argtypes = [c_p, ctypes.POINTER(c_p)]
     _lib = lib
     return lib
 

@@ -349,6 +349,37 @@ int fvg_batch_stream(fvg_batch* b, void** stream);
 int fvg_batch_set_timing(fvg_batch* b, int on);
 int fvg_batch_get_timing(const fvg_batch* b, double* stage_ms, long long* stage_launches);
 
+/* ---- The cell engine of an adaptive mesh, for meshes whose leaves are all of level 0.
+ *
+ * The reference's CellFluxEngine (cpp/include/fv/CellFlux.hpp:92-270: constructed from the run's EOS, RiemannSolver,
+ * MusclReconstruction and BoundaryManager, then build(mesh)) and CellAdvance (cpp/include/fv/CellAdvance.hpp:27-47) on a
+ * CellMesh (cpp/include/fv/CellMesh.hpp:57) given as its leaf arrays `level`, `ci`, `cj`, `ck` (CellMesh::level / ci / cj /
+ * ck; ck may be NULL on a 2-D mesh). The leaves keep the caller's order: states and residuals cross the ABI as arrays of
+ * nleaf leaves of 5 doubles in that order (CellMesh::U). cfg is the run's configuration (the base mesh nx x ny x nz, the
+ * lengths, the scheme, the boundary conditions; the periodic axes are the periodic sides). Built: every leaf of level 0
+ * (they must tile the base mesh); first order, MUSCL (every limiter), WENO3-Z, WENO5-Z; HLLC and low-Mach HLLC; the
+ * boundary types but the non-reflecting outlet and the mass-flow inlet, with boundary_order 1 or 2; Euler, SSP-RK2 and
+ * SSP-RK3 steps. Refused (FVG_ERR_CONFIG, message in fvg_create_error()): leaves above level 0, the viscous terms, an
+ * immersed body, the body force, sources and time-dependent boundary values, positivity_fallback, the fourth-order
+ * quadrature, the mixed-precision form, MUSCL-Hancock. */
+typedef struct fvg_cells fvg_cells;
+int fvg_cells_create(const fvg_config* cfg, int nleaf, const int* level, const int* ci, const int* cj, const int* ck, fvg_cells** out);
+int fvg_cells_destroy(fvg_cells* e);
+const char* fvg_cells_last_error(const fvg_cells* e);
+/* the leaves and the faces of the mesh (CellMesh::num_leaves, CellMesh::faces.size()) */
+int fvg_cells_info(const fvg_cells* e, long long* nleaf, long long* nface);
+int fvg_cells_upload_state(fvg_cells* e, const double* U, size_t nleaf);
+int fvg_cells_download_state(fvg_cells* e, double* U, size_t nleaf);
+/* R = dU/dt of the state held (CellFluxEngine::residual, cpp/src/CellFluxResidual.cpp:1088-1105); *smax (may be NULL)
+ * the largest face wave speed */
+int fvg_cells_residual(fvg_cells* e, double* R, size_t nleaf, double* smax);
+/* one step of length dt from time t of the state held (CellAdvance::step: with one level, the time scheme's
+ * advance_fixed_dt, cpp/src/TimeScheme.cpp:100-290); *smax (may be NULL) the first stage's largest face wave speed */
+int fvg_cells_step(fvg_cells* e, double dt, double t, double* smax);
+/* nsteps such steps enqueued back to back (one host synchronisation at the end) */
+int fvg_cells_advance(fvg_cells* e, double dt, int nsteps, double* smax);
+int fvg_cells_stream(fvg_cells* e, void** stream);
+
 #ifdef __cplusplus
 }
 #endif

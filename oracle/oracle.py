@@ -284,6 +284,15 @@ class Reference:
             lib.ref_solid_mask.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
             lib.ref_ibm_loads.argtypes = [ctypes.c_void_p, P(ctypes.c_double)]
             lib.ref_volume_averages.argtypes = [ctypes.c_void_p, P(ctypes.c_double)]
+            lib.ref_cells_create.argtypes = [ctypes.c_void_p, ctypes.c_int]
+            lib.ref_cells_create.restype = ctypes.c_void_p
+            lib.ref_cells_destroy.argtypes = [ctypes.c_void_p]
+            lib.ref_cells_count.argtypes = [ctypes.c_void_p, P(ctypes.c_int), P(ctypes.c_int)]
+            lib.ref_cells_leaves.argtypes = [ctypes.c_void_p] + [P(ctypes.c_int)] * 4
+            lib.ref_cells_set_state.argtypes = [ctypes.c_void_p, P(ctypes.c_double)]
+            lib.ref_cells_get_state.argtypes = [ctypes.c_void_p, P(ctypes.c_double)]
+            lib.ref_cells_residual.argtypes = [ctypes.c_void_p, P(ctypes.c_double), P(ctypes.c_double)]
+            lib.ref_cells_steps.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int, P(ctypes.c_double)]
             cls._lib = lib
         return cls._lib
 
@@ -369,3 +378,53 @@ class Reference:
         if self.lib().ref_ibm_loads(self.h, v) != 0:
             raise RuntimeError("reference ibm_loads failed: " + self.lib().ref_error().decode())
         return list(v)
+
+
+class ReferenceCells:
+    """The reference's cell engine of an adaptive mesh on a Reference run's objects (ref_cells_* of the harness): the
+    CellMesh of the run's base mesh (levels 0 .. max_level, every leaf of level 0 as built), its CellFluxEngine and a
+    CellAdvance with the run's time scheme, as the reference's level-0 tests make them. Keep the Reference alive."""
+
+    def __init__(self, ref, max_level=0):
+        lib = Reference.lib()
+        self.ref = ref
+        self.h = lib.ref_cells_create(ref.h, int(max_level))
+        if not self.h:
+            raise RuntimeError("reference cell engine failed: " + lib.ref_error().decode())
+        n, nf = ctypes.c_int(), ctypes.c_int()
+        lib.ref_cells_count(self.h, ctypes.byref(n), ctypes.byref(nf))
+        self.nleaf, self.nface = n.value, nf.value
+        arrs = [np.zeros(self.nleaf, dtype=np.int32) for _ in range(4)]
+        lib.ref_cells_leaves(self.h, *[a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)) for a in arrs])
+        self.level, self.ci, self.cj, self.ck = arrs
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            Reference.lib().ref_cells_destroy(self.h)
+            self.h = None
+
+    def set_state(self, U):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        assert U.shape == (self.nleaf, 5)
+        Reference.lib().ref_cells_set_state(self.h, _dp(U))
+
+    def state(self):
+        U = np.zeros((self.nleaf, 5))
+        Reference.lib().ref_cells_get_state(self.h, _dp(U))
+        return U
+
+    def residual(self):
+        """(R, largest face speed) of the state held (CellFluxEngine::residual)."""
+        R = np.zeros((self.nleaf, 5))
+        s = ctypes.c_double(0.0)
+        if Reference.lib().ref_cells_residual(self.h, _dp(R), ctypes.byref(s)):
+            raise RuntimeError("reference cell residual failed: " + Reference.lib().ref_error().decode())
+        return R, s.value
+
+    def steps(self, dt, n, t0=0.0):
+        """n CellAdvance::step(dt, t0 + k dt); the speed each returned."""
+        s = np.zeros(n)
+        if Reference.lib().ref_cells_steps(self.h, float(dt), float(t0), int(n), _dp(s)):
+            raise RuntimeError("reference cell steps failed: " + Reference.lib().ref_error().decode())
+        return s
+

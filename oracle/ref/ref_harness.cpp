@@ -7,10 +7,14 @@
 //   * one step is the body of the serial time loop: scheme->step, check_progress, the solid reset of the
 //     immersed body, t += dt (cpp/src/SimulationRun.cpp:441-464).
 // Nothing here changes the reference's arithmetic; it only moves arrays across the C ABI.
+#include "fv/CellAdvance.hpp"
+#include "fv/CellFlux.hpp"
+#include "fv/CellMesh.hpp"
 #include "fv/Params.hpp"
 #include "fv/Physics.hpp"
 #include "fv/Simulation.hpp"
 #include "fv/TestCases.hpp"
+#include "fv/TimeScheme.hpp"
 
 #include <chrono>
 #include <cmath>
@@ -18,6 +22,7 @@
 #include <cstring>
 #include <filesystem>
 #include <fstream>
+#include <memory>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -32,6 +37,17 @@ struct RefRun {
     fv::Simulation sim;
     fs::path dir;
     int steps = 0;
+};
+
+// The cell engine of the adaptive mesh on a run's objects, as the reference's level-0 tests build it
+// (cpp/tests/test_amr_octree_advance.cpp:17-49, cpp/tests/test_amr_mesh.cpp:484-530): the CellMesh of the run's base mesh
+// with its periodic axes, a CellFluxEngine on the run's EOS, Riemann solver, reconstruction and boundaries, and a
+// CellAdvance with a time scheme of the run's type. The run must outlive it.
+struct RefCells {
+    std::unique_ptr<fv::CellMesh> mesh;
+    std::unique_ptr<fv::CellFluxEngine> eng;
+    std::unique_ptr<fv::TimeScheme> ts;
+    std::unique_ptr<fv::CellAdvance> adv;
 };
 
 std::string trim(const std::string& s) {
@@ -240,6 +256,92 @@ int ref_volume_averages(void* h, double* out) {
     out[1] = v[1];
     out[2] = v[2];
     return 0;
+}
+
+// ---- the level-0 cell engine (see RefCells)
+
+void* ref_cells_create(void* h, int max_level) {
+    try {
+        auto* r = static_cast<RefRun*>(h);
+        const fv::Simulation& sim = r->sim;
+        const fv::Mesh& u = sim.mesh;
+        auto per = [&](int a) { return sim.boundaries.type(static_cast<fv::Face>(2 * a)) == fv::BCType::Periodic; };
+        auto* c = new RefCells();
+        if (u.nz > 1)
+            c->mesh = std::make_unique<fv::CellMesh>(fv::CellMesh::make_3d(u.Lx, u.Ly, u.Lz, u.nx, u.ny, u.nz, max_level, per(0), per(1), per(2), u.x0, u.y0, u.z0));
+        else
+            c->mesh = std::make_unique<fv::CellMesh>(u.Lx, u.Ly, u.nx, u.ny, max_level, per(0), per(1), u.x0, u.y0);
+        c->mesh->U.assign(static_cast<size_t>(c->mesh->num_leaves()), fv::State{});
+        c->eng = std::make_unique<fv::CellFluxEngine>(sim.fluid, sim.riemann, sim.muscl.get(), sim.boundaries);
+        c->eng->build(*c->mesh);
+        c->ts = fv::make_time_scheme(fv::parse_time_scheme(sim.p.time_scheme), sim.p.cfl);
+        c->adv = std::make_unique<fv::CellAdvance>(*c->mesh, *c->eng, *c->ts);
+        return c;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return nullptr;
+    }
+}
+
+void ref_cells_destroy(void* hc) { delete static_cast<RefCells*>(hc); }
+
+int ref_cells_count(void* hc, int* nleaf, int* nface) {
+    auto* c = static_cast<RefCells*>(hc);
+    *nleaf = c->mesh->num_leaves();
+    *nface = static_cast<int>(c->mesh->faces.size());
+    return 0;
+}
+
+int ref_cells_leaves(void* hc, int* level, int* ci, int* cj, int* ck) {
+    const fv::CellMesh& m = *static_cast<RefCells*>(hc)->mesh;
+    for (int l = 0; l < m.num_leaves(); ++l) {
+        level[l] = m.level[l];
+        ci[l] = m.ci[l];
+        cj[l] = m.cj[l];
+        ck[l] = m.ck[l];
+    }
+    return 0;
+}
+
+int ref_cells_set_state(void* hc, const double* U) {
+    fv::CellMesh& m = *static_cast<RefCells*>(hc)->mesh;
+    for (int l = 0; l < m.num_leaves(); ++l)
+        for (int q = 0; q < 5; ++q) m.U[l][q] = U[5 * l + q];
+    return 0;
+}
+
+int ref_cells_get_state(void* hc, double* U) {
+    const fv::CellMesh& m = *static_cast<RefCells*>(hc)->mesh;
+    for (int l = 0; l < m.num_leaves(); ++l)
+        for (int q = 0; q < 5; ++q) U[5 * l + q] = m.U[l][q];
+    return 0;
+}
+
+// CellFluxEngine::residual of the state held
+int ref_cells_residual(void* hc, double* R, double* smax) {
+    try {
+        auto* c = static_cast<RefCells*>(hc);
+        fv::Field Rf;
+        *smax = c->eng->residual(*c->mesh, c->mesh->U, Rf);
+        for (size_t l = 0; l < Rf.size(); ++l)
+            for (int q = 0; q < 5; ++q) R[5 * l + q] = Rf[l][q];
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+// CellAdvance::step(dt, t) of the state held, n times from t0 (step k at t0 + k dt); smax: the speed of each step
+int ref_cells_steps(void* hc, double dt, double t0, int n, double* smax) {
+    try {
+        auto* c = static_cast<RefCells*>(hc);
+        for (int k = 0; k < n; ++k) smax[k] = c->adv->step(dt, t0 + k * dt);
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
 }
 
 }   // extern "C"
