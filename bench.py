@@ -505,6 +505,81 @@ def quad_arm(args, world, rank, local):
     return out
 
 
+CELLS_WORKLOAD = "the cell engine of an adaptive mesh with every leaf of level 0 (leaves in Morton order), fixed dt (the first step's CFL dt): "
+
+
+def cells_arm(args, world, rank, local):
+    """The cell engine (fvg_cells_*) on the benchmark configuration as a level-0 leaf list: steps of fixed length (the first
+    step's CFL dt), timed with CUDA events on its stream; the same steps through the public API with the leaf state
+    copied from pinned host memory and back (e2e); the reference's own engine (CellFluxEngine + CellAdvance, oracle/_ref)
+    on the host cores for one step (cpu_baseline)."""
+    import torch
+
+    from fenice_b200.cells import CellEngine, base_leaves
+
+    n = args.size
+    params = workload(n)
+    lv, ci, cj, ck = base_leaves(params)
+    U = tgv_state(n)[(ck.astype(np.int64) * n + cj) * n + ci]
+    t0 = time.perf_counter()
+    eng = CellEngine(params, lv, ci, cj, ck, U=U, device=local)
+    build_s = time.perf_counter() - t0
+    _, s0 = eng.residual()
+    dx = 2 * math.pi / n
+    dt = params["cfl"] * 2.0 / (3.0 / dx) / (s0 + 1e-10)
+    ext = torch.cuda.ExternalStream(eng.stream(), device=torch.device("cuda", local))
+    eng.advance(dt, max(args.warmup, 3))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        a.record(ext)
+        eng.advance(dt, args.steps)
+        b.record(ext)
+        torch.cuda.synchronize()
+    ms = allmax(a.elapsed_time(b), world) / args.steps
+    cells = n ** 3
+    per_stage = 3 + (2 if params.get("use_viscous") else 0)   # primitive, faces, gather (+ viscous cells, viscous faces)
+    out = {"value": world * cells * STAGES / (ms * 1e-3), "ms_per_step": ms, "steps": args.steps, "dt": dt, "faces": eng.nface,
+           "gpu_launches": per_stage * STAGES * args.steps,
+           "build_s": build_s, "clocks": clk.summary(),
+           "roofline": {"bound": "hbm", "achieved": round(cells * STAGES * BYTES_PER_CELL_STAGE / (ms * 1e-3) / 1e9, 2), "peak": measured_peak()[0],
+                        "unit": "GB/s", "kernel": "the cell engine's step (primitive, face, viscous cell and face, gather kernels)"}}
+    out["roofline"]["frac"] = round(out["roofline"]["achieved"] / out["roofline"]["peak"], 4)
+    # e2e: the leaf state from pinned host memory, one step, the state back
+    hin = torch.from_numpy(U).pin_memory().numpy()
+    hout = torch.empty(U.shape, dtype=torch.float64).pin_memory().numpy()
+    eng.set_state(hin)
+    eng.step(dt)
+    eng.state(out=hout)
+    k = max(1, args.e2e_steps)
+    t0 = time.perf_counter()
+    for _ in range(k):
+        eng.set_state(hin)
+        eng.step(dt)
+        eng.state(out=hout)
+    wall = (time.perf_counter() - t0) / k
+    out["e2e"] = {"value": world * cells * STAGES / wall, "unit": UNIT, "h2d_bytes_per_step": int(U.nbytes), "d2h_bytes_per_step": int(U.nbytes),
+                  "steps": k, "timing": "host wall clock around upload + fvg_cells_step + download of the leaf state"}
+    eng.close()
+    if rank == 0 and world == 1 and args.cpu_baseline:
+        try:
+            from oracle.oracle import Reference, ReferenceCells
+
+            os.environ.setdefault("OMP_NUM_THREADS", str(len(os.sched_getaffinity(0))))
+            ref = Reference(params, initial_state=(1, 0, 0, 1, 0))
+            rc = ReferenceCells(ref, 0)
+            rc.set_state(tgv_state(n)[(rc.ck.astype(np.int64) * n + rc.cj) * n + rc.ci])
+            rc.steps(dt, 1)
+            t0 = time.perf_counter()
+            rc.steps(dt, 1)
+            wall = time.perf_counter() - t0
+            out["cpu_baseline"] = {"value": cells * STAGES / wall, "unit": UNIT, "cores": len(os.sched_getaffinity(0)), "kind": "reference",
+                                   "sample": f"1 CellAdvance step of the {n}^3 level-0 mesh after 1 untimed ({wall:.1f} s)"}
+        except Exception as e:
+            out["cpu_baseline"] = {"value": None, "unit": UNIT, "kind": "reference", "sample": f"unavailable: {e}"}
+    return out
+
+
 CYL_WORKLOAD = ("Mach 2 flow over a cylinder (diameter 1, sharp ghost-cell immersed boundary, slip wall) in an 8 x 12 box, {nx} x {ny}, "
                 "inflow rho 1.4, p 1, Mach 2, transmissive elsewhere, from the free stream, {steps} steps; plain: MUSCL (MC) + HLLC + "
                 "MUSCL-Hancock; mixed: WENO5-Z + HLLC + SSP-RK3 (FP32 stencil, FP64 state)")
@@ -794,7 +869,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-baseline", type=int, default=1, help="time the reference on the host cores (rank 0, N = 1)")
     ap.add_argument("--parts", type=int, default=2, help="slab workload at N = 1: parts of the mesh in one process")
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "tgv200", "batch", "quadrants", "cylinder", "slab"],
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "tgv200", "batch", "quadrants", "cylinder", "slab", "cells"],
                     help="tgv: the 3-D Taylor-Green vortex (default); batch: 512 shock tubes in one persistent launch per stage; "
                          "quadrants: a seeded four-quadrant Riemann problem (--size cells per axis, default 2048 for it)")
     ap.add_argument("--seed", type=int, default=2048, help="seed of the quadrants workload")
@@ -902,6 +977,23 @@ def main():
             os.environ.setdefault("OMP_NUM_THREADS", str(threads))
             rate, wall, sample = cpu_batch_rate(12.0)
             line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+    if args.workload == "cells":
+        c = cells_arm(args, world, rank, local)
+        line = {"metric": METRIC, "value": c["value"], "unit": UNIT, "n_gpus": world, "steps": c["steps"], "warmup": args.warmup,
+                "ms_per_step": c["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (Taylor-Green initial state computed in numpy)",
+                "config": {"workload": CELLS_WORKLOAD + tgv_workload(args.size), "cells": args.size ** 3, "faces": c["faces"],
+                           "stages_per_step": STAGES, "l2": f"inputs larger than L2 ({args.size ** 3 * 40 / 1e6:.0f} MB per state field), no flush"},
+                "roofline": c["roofline"], "clocks": c["clocks"], "e2e": c["e2e"], "build_s": c["build_s"], "gpu_launches": c["gpu_launches"]}
+        if "cpu_baseline" in c:
+            line["cpu_baseline"] = c["cpu_baseline"]
         if rank == 0:
             print(json.dumps(line), flush=True)
         if world > 1:

@@ -90,8 +90,11 @@ class CellEngine:
         U = self._leaf_array(U)
         self._check(self.lib.fvg_cells_upload_state(self.h, _dp(U), self.nleaf), "upload_state")
 
-    def state(self):
-        U = np.empty((self.nleaf, 5))
+    def state(self, out=None):
+        """The leaf state, into `out` if given (a C-contiguous (nleaf, 5) float64 array, e.g. in pinned memory)."""
+        U = np.empty((self.nleaf, 5)) if out is None else out
+        if U.shape != (self.nleaf, 5) or U.dtype != np.float64 or not U.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous float64 array of shape ({self.nleaf}, 5)")
         self._check(self.lib.fvg_cells_download_state(self.h, _dp(U), self.nleaf), "download_state")
         return U
 

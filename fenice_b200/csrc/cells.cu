@@ -21,6 +21,7 @@
 #include "../../include/fenice_gpu.h"
 #include "host_common.h"
 #include "stage.cuh"
+#include "viscous.cuh"
 
 #include <cuda_runtime.h>
 
@@ -40,6 +41,11 @@ struct fvg_cells {
     cudaStream_t stream = nullptr;
     double *U = nullptr, *Ut = nullptr, *W = nullptr, *R = nullptr, *F = nullptr, *staging = nullptr;
     int *code = nullptr, *meta = nullptr, *side_face = nullptr;
+    // the viscous terms (3-D): the neighbour table, the cell quantities and the viscous face fluxes
+    bool visc = false;
+    int* nbr = nullptr;
+    double *Q = nullptr, *Fv = nullptr;
+    double mu = 0.0, k_cond = 0.0, L = 0.0, inv_h2 = 0.0, h[3] = {0, 0, 0};
     unsigned long long* smax = nullptr;   // [3]: the bits of the largest face speed of each stage
     int* bad = nullptr;
     std::string err;
@@ -48,7 +54,8 @@ struct fvg_cells {
 namespace fvg {
 namespace {
 
-// what a face solves (bits 2-3 of its meta word; bits 0-1 the axis, 4-6 a boundary face's side, 7 its ghost on the right)
+// what a face solves (bits 2-3 of its meta word; bits 0-1 the axis; on a boundary face bit 8 set, 4-6 its side and 7 its
+// ghost on the right)
 constexpr int kFaceR6 = 0;    // WENO5-Z on six entries
 constexpr int kFaceR4 = 1;    // four entries (entries 1-4): MUSCL, or WENO3-Z (a WENO5-Z run's faces that hold fewer cells too)
 constexpr int kFaceFO = 2;    // first order between two leaves: their conservative states
@@ -152,9 +159,179 @@ __global__ void __launch_bounds__(kCellsNT) k_cells_faces(const CellArgs a) {
     if (threadIdx.x == 0 && bm > 0.0) atomicMax(a.smax, (unsigned long long)__double_as_longlong(bm));
 }
 
+// ---- the viscous terms on a 3-D mesh (CellFluxEngine::cell_quantities_3d / viscous_fluxes_3d / viscous_speed_3d,
+// CellFluxResidual.cpp:801-972: the expressions of NavierStokes::viscous_residual_3d, so level-0 leaves get its bits)
+
+constexpr int kQ = 13;   // cell quantities per leaf: u, v, w, T, then G[a][b] = du_a/dx_b at 4 + 3 a + b
+
+struct CellVisc {
+    ViscArgs va;   // the rules of the diffusive ghost (viscous_ghost_3d): boundary types, u_in, v_in, boundary_order 2
+    long long nleaf, lplane, nface, fplane;
+    const double* U;
+    const int* nbr;     // [6][nleaf] the leaf across each side, -1 at a physical edge
+    double* Q;          // [kQ][lplane]
+    const int* code;
+    const int* meta;
+    double* Fv;         // [4][fplane] viscous flux times the face's area: rho u, rho v, rho E, rho w
+    double h[3], length[3];
+    double mu, k_cond, L, inv_h2;
+    int bo2;
+    unsigned long long* smax;
+};
+
+__global__ void __launch_bounds__(kCellsNT) k_cells_vcells(const CellVisc v) {
+    __shared__ double red[32];
+    const long long c = blockIdx.x * (long long)kCellsNT + threadIdx.x;
+    double s = 0.0;
+    if (c < v.nleaf) {
+        const St<double, 5> Ui = leaf_state<5>(v.U, v.lplane, c);
+        const St<double, 5> W = c2p(v.va.eos, Ui);
+        const int mom[3] = {1, 2, 4};
+        const double rho = W[0];
+        double grad[3][5];
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const int lo = v.nbr[(2 * b) * v.nleaf + c], hi = v.nbr[(2 * b + 1) * v.nleaf + c];
+            const St<double, 5> nl = lo >= 0 ? leaf_state<5>(v.U, v.lplane, lo) : viscous_ghost_3d(v.va, 2 * b, Ui);
+            const St<double, 5> nh = hi >= 0 ? leaf_state<5>(v.U, v.lplane, hi) : viscous_ghost_3d(v.va, 2 * b + 1, Ui);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) grad[b][q] = (nh[q] - nl[q]) / (2.0 * v.h[b]);
+        }
+        v.Q[3 * v.lplane + c] = W[3] / rho;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const double ua = W[mom[a]];
+            v.Q[a * v.lplane + c] = ua;
+#pragma unroll
+            for (int b = 0; b < 3; ++b) v.Q[(4 + 3 * a + b) * v.lplane + c] = (grad[b][mom[a]] - ua * grad[b][0]) / rho;
+        }
+        // the leaf's viscous speed bound (ViscousBound.hpp: viscous_speed_bound of viscous_nu_eff)
+        const double nu_eff = vmax((4.0 / 3.0) * (v.mu / rho), (v.k_cond * (v.va.eos.gamma - 1.0)) / rho) + 1e-12;
+        const double vm = vmax(vmax(fabs(W[1]), fabs(W[2])), fabs(W[4]));
+        const double sv = vm + sound_speed(v.va.eos, W[3], rho) + 2.0 * v.L * v.inv_h2 * nu_eff;
+        if (sv > s) s = sv;
+    }
+    const double bm = block_max<kCellsNT>(s, red);
+    if (threadIdx.x == 0 && bm > 0.0) atomicMax(v.smax, (unsigned long long)__double_as_longlong(bm));
+}
+
+// one face normal to axis D (a template parameter, so the pairs below and every array index are constants)
+template <int D> __device__ __forceinline__ void cells_vface(const CellVisc& v, long long f, int meta) {
+    constexpr int d = D;
+    const int mom[3] = {1, 2, 4};
+    // the cross derivatives (a, b) = du_a/dx_b a face normal to axis d reads, in the uniform solver's order
+    constexpr int pa[4] = {0, 1, 2, D};
+    constexpr int pb[4] = {D == 0 ? 1 : 0, D == 1 ? 0 : 1, D == 2 ? 0 : 2, D == 2 ? 1 : 2};
+    double vL[3], vR[3], TL, TR, h;
+    double Gc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    auto G = [&](int a, int b, long long c) { return v.Q[(4 + 3 * a + b) * v.lplane + c]; };
+    if ((meta >> 8) & 1) {
+        const int side = (meta >> 4) & 7;
+        const bool ghost_left = !((meta >> 7) & 1);
+        const int c = v.code[(ghost_left ? 3 : 2) * v.fplane + f];
+        const St<double, 5> Uc = leaf_state<5>(v.U, v.lplane, c);
+        const St<double, 5> g = c2p(v.va.eos, viscous_ghost_3d(v.va, side, Uc));
+        const double gT = g[3] / g[0];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const double gv = g[mom[a]], cv = v.Q[a * v.lplane + c];
+            vL[a] = ghost_left ? gv : cv;
+            vR[a] = ghost_left ? cv : gv;
+        }
+        TL = ghost_left ? gT : v.Q[3 * v.lplane + c];
+        TR = ghost_left ? v.Q[3 * v.lplane + c] : gT;
+        h = v.h[d];
+        if (v.bo2) {
+            // the tangential difference of the face values (ghost and cell average) of the two neighbours along b; beyond a
+            // physical edge along b the neighbour is the leaf's b-ghost and its d-ghost the padded state's edge entry
+            double fval[6][3];
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                if (b == d) continue;
+#pragma unroll
+                for (int hi = 0; hi < 2; ++hi) {
+                    const int si = 2 * b + hi;
+                    const int code = v.nbr[si * v.nleaf + c];
+                    St<double, 5> in, gh;
+                    if (code >= 0) {
+                        in = leaf_state<5>(v.U, v.lplane, code);
+                        gh = viscous_ghost_3d(v.va, side, in);
+                    } else {
+                        in = viscous_ghost_3d(v.va, si, Uc);
+                        gh = d < b ? viscous_ghost_3d(v.va, side, in) : viscous_ghost_3d(v.va, si, viscous_ghost_3d(v.va, side, Uc));
+                    }
+                    const St<double, 5> Wg = c2p(v.va.eos, gh), Wi = c2p(v.va.eos, in);
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) fval[si][a] = 0.5 * (Wg[mom[a]] + Wi[mom[a]]);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) Gc[pa[k]][pb[k]] = (fval[2 * pb[k] + 1][pa[k]] - fval[2 * pb[k]][pa[k]]) / (2.0 * v.h[pb[k]]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const double x = G(pa[k], pb[k], c);
+                Gc[pa[k]][pb[k]] = 0.5 * (x + x);
+            }
+        }
+    } else {
+        const int L = v.code[2 * v.fplane + f], R = v.code[3 * v.fplane + f];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            vL[a] = v.Q[a * v.lplane + L];
+            vR[a] = v.Q[a * v.lplane + R];
+        }
+        TL = v.Q[3 * v.lplane + L];
+        TR = v.Q[3 * v.lplane + R];
+        h = 0.5 * (v.h[d] + v.h[d]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) Gc[pa[k]][pb[k]] = 0.5 * (G(pa[k], pb[k], L) + G(pa[k], pb[k], R));
+    }
+    double Gn[3], vf[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        Gn[a] = (vR[a] - vL[a]) / h;
+        vf[a] = 0.5 * (vL[a] + vR[a]);
+    }
+    const double dT = (TR - TL) / h;
+    double tau[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (a == d) {
+            double others = 0.0;
+#pragma unroll
+            for (int o = 0; o < 3; ++o)
+                if (o != d) others += Gc[o][o];
+            tau[a] = v.mu * ((4.0 / 3.0) * Gn[d] - (2.0 / 3.0) * others);
+        } else {
+            tau[a] = v.mu * (Gn[a] + Gc[d][a]);
+        }
+    }
+    const double q_d = -v.k_cond * dT;
+    const double area = v.length[d];
+    v.Fv[0 * v.fplane + f] = tau[0] * area;
+    v.Fv[1 * v.fplane + f] = tau[1] * area;
+    v.Fv[2 * v.fplane + f] = (vf[0] * tau[0] + vf[1] * tau[1] + vf[2] * tau[2] - q_d) * area;
+    v.Fv[3 * v.fplane + f] = tau[2] * area;
+}
+
+__global__ void __launch_bounds__(kCellsNT) k_cells_vfaces(const CellVisc v) {
+    const long long f = blockIdx.x * (long long)kCellsNT + threadIdx.x;
+    if (f >= v.nface) return;
+    const int meta = v.meta[f];
+    const int d = meta & 3;
+    if (d == 0)
+        cells_vface<0>(v, f, meta);
+    else if (d == 1)
+        cells_vface<1>(v, f, meta);
+    else
+        cells_vface<2>(v, f, meta);
+}
+
 struct GatherArgs {
     long long nleaf, lplane, fplane;
     const double* F;
+    const double* Fv;       // [4][fplane] viscous fluxes times the face area (null: inviscid)
     const int* side_face;   // [ns * nleaf]: the face on each side of each leaf (one at level 0)
     double length[3], inv_vol;
     int mode;
@@ -180,7 +357,16 @@ template <int DIM, int NV> __global__ void __launch_bounds__(kCellsNT) k_cells_g
         double acc = 0.0 - (G[1] - G[0]);
         acc = acc - (G[3] - G[2]);
         if constexpr (DIM == 3) acc = acc - (G[5] - G[4]);
-        const double r = acc * g.inv_vol;
+        double r = acc * g.inv_vol;
+        if (g.Fv) {   // NavierStokes::viscous_residual_3d accumulated: r += (((0 + (H1 - H0)) + (H3 - H2)) + (H5 - H4)) / volume
+            double H[NS];
+#pragma unroll
+            for (int s = 0; s < NS; ++s) H[s] = q == 0 ? 0.0 : g.Fv[(q - 1) * g.fplane + fs[s]];
+            double vac = 0.0 + (H[1] - H[0]);
+            vac = vac + (H[3] - H[2]);
+            if constexpr (DIM == 3) vac = vac + (H[5] - H[4]);
+            r += vac * g.inv_vol;
+        }
         const long long e = q * g.lplane + c;
         double o;
         if (g.mode == kStoreR)
@@ -209,6 +395,7 @@ __global__ void k_cells_out(const double* U, double* aos, long long lplane, long
 struct Tables {
     long long nface = 0;
     std::vector<int> code[6], meta, side_face;
+    std::vector<int> nbr;   // [ns][nleaf]: the leaf across each side (-1 at a physical edge)
 };
 
 std::string build_tables(const fvg_config& c, int dim, long long nleaf, const int* ci, const int* cj, const int* ck, Tables& t) {
@@ -283,7 +470,8 @@ std::string build_tables(const fvg_config& c, int dim, long long nleaf, const in
     auto boundary = [&](int l, int sd) {
         const int a = sd >> 1;
         const bool gr = (sd & 1) != 0;   // the ghost on the right: the mesh's high side
-        const int bmeta = a | kFaceBnd << 2 | sd << 4 | (gr ? 1 : 0) << 7;
+        const int bside = sd << 4 | (gr ? 1 : 0) << 7 | 1 << 8;   // every boundary face carries its side (the viscous pass reads it)
+        const int bmeta = a | kFaceBnd << 2 | bside;
         int e[6] = {0, 0, gr ? l : 0, gr ? 0 : l, 0, 0};
         if (!bo2 || !side_ok(sd)) return add(e, bmeta);
         const int n1 = nbr(l, sd ^ 1);
@@ -293,11 +481,11 @@ std::string build_tables(const fvg_config& c, int dim, long long nleaf, const in
         if (n2 >= 0) {
             const int hi[6] = {n2, n1, l, ghost_code(l, sd), ghost_code(n1, sd), ghost_code(n2, sd)};
             const int lo[6] = {ghost_code(n2, sd), ghost_code(n1, sd), ghost_code(l, sd), l, n1, n2};
-            return add(gr ? hi : lo, a | kFaceR6 << 2);
+            return add(gr ? hi : lo, a | kFaceR6 << 2 | bside);
         }
         const int hi[6] = {0, n1, l, ghost_code(l, sd), ghost_code(n1, sd), 0};
         const int lo[6] = {0, ghost_code(n1, sd), ghost_code(l, sd), l, n1, 0};
-        return add(gr ? hi : lo, a | kFaceR4 << 2);
+        return add(gr ? hi : lo, a | kFaceR4 << 2 | bside);
     };
     // faces in leaf order (a leaf makes the face on its low side of every axis, and the one on its high side at a
     // physical edge), so the faces of neighbouring leaves sit close together too
@@ -311,6 +499,9 @@ std::string build_tables(const fvg_config& c, int dim, long long nleaf, const in
         }
     }
     t.nface = (long long)t.meta.size();
+    t.nbr.resize((size_t)ns * nleaf);
+    for (int sd = 0; sd < ns; ++sd)
+        for (long long l = 0; l < nleaf; ++l) t.nbr[(size_t)sd * nleaf + l] = nbr((int)l, sd);
     for (int v : t.side_face)
         if (v < 0) return "a leaf side without a face (the leaves do not tile the base mesh)";
     return "";
@@ -376,11 +567,44 @@ int residual_pass(fvg_cells* e, const double* Uin, int slot, int mode, double ca
     a.F = e->F;
     a.smax = e->smax + slot;
     CKC(e->nvar == 5 ? launch_faces<5>(e, a) : launch_faces<4>(e, a));
+    if (e->visc) {   // the cell quantities and the leaves' speed bounds, then the viscous face fluxes
+        CellVisc v{};
+        v.va.eos = e->eos;
+        v.va.bc = e->bc;
+        v.va.u_in = e->cfg.u_in;
+        v.va.v_in = e->cfg.v_in;
+        v.va.bface2 = e->cfg.boundary_order == 2;
+        v.nleaf = n;
+        v.lplane = e->lplane;
+        v.nface = e->nface;
+        v.fplane = e->fplane;
+        v.U = Uin;
+        v.nbr = e->nbr;
+        v.Q = e->Q;
+        v.code = e->code;
+        v.meta = e->meta;
+        v.Fv = e->Fv;
+        for (int k = 0; k < 3; ++k) {
+            v.h[k] = e->h[k];
+            v.length[k] = e->length[k];
+        }
+        v.mu = e->mu;
+        v.k_cond = e->k_cond;
+        v.L = e->L;
+        v.inv_h2 = e->inv_h2;
+        v.bo2 = e->cfg.boundary_order == 2;
+        v.smax = e->smax + slot;
+        k_cells_vcells<<<(int)((n + kCellsNT - 1) / kCellsNT), kCellsNT, 0, e->stream>>>(v);
+        CKC(cudaGetLastError());
+        k_cells_vfaces<<<(int)((e->nface + kCellsNT - 1) / kCellsNT), kCellsNT, 0, e->stream>>>(v);
+        CKC(cudaGetLastError());
+    }
     GatherArgs g{};
     g.nleaf = n;
     g.lplane = e->lplane;
     g.fplane = e->fplane;
     g.F = e->F;
+    g.Fv = e->visc ? e->Fv : nullptr;
     g.side_face = e->side_face;
     for (int k = 0; k < 3; ++k) g.length[k] = e->length[k];
     g.inv_vol = e->inv_vol;
@@ -427,7 +651,7 @@ int fvg_cells_create(const fvg_config* cfg, int nleaf, const int* level, const i
     const fvg_config& c = *cfg;
     std::string why = config_error(c);
     const char* no = nullptr;
-    if (c.use_viscous) no = "the viscous terms";
+    if (c.use_viscous && c.nz <= 1) no = "the viscous terms on a 2-D mesh";
     else if (c.use_ibm) no = "an immersed body";
     else if (c.use_bodyforce) no = "the body force";
     else if (config_has_expressions(c)) no = "source terms and time-dependent boundary values";
@@ -471,6 +695,14 @@ int fvg_cells_create(const fvg_config* cfg, int nleaf, const int* level, const i
     e->bc.v_in = c.v_in;
     e->bc.p_out = c.p_out;
     const double dx = c.Lx / c.nx, dy = c.Ly / c.ny, dz = c.Lz / c.nz;   // CellMesh::dx(0) ... (CellMesh.cpp:39-67)
+    e->visc = c.use_viscous != 0;
+    e->h[0] = dx;
+    e->h[1] = dy;
+    e->h[2] = dz;
+    e->mu = c.mu;
+    e->k_cond = c.mu * c.gamma / (c.pr * (c.gamma - 1.0));                          // TransportLaw (Core.hpp:194-197)
+    e->L = 2.0 / (1.0 / dx + 1.0 / dy + 1.0 / dz);                                  // step_length_3d
+    e->inv_h2 = 1.0 / (dx * dx) + 1.0 / (dy * dy) + 1.0 / (dz * dz);                // inv_h2_3d
     if (e->dim == 3) {
         e->length[0] = dy * dz;
         e->length[1] = dx * dz;
@@ -497,6 +729,12 @@ int fvg_cells_create(const fvg_config* cfg, int nleaf, const int* level, const i
         (err = cudaMalloc(&e->side_face, sizeof(int) * e->ns * e->nleaf)) != cudaSuccess ||
         (err = cudaMalloc(&e->smax, sizeof(unsigned long long) * 3)) != cudaSuccess || (err = cudaMalloc(&e->bad, sizeof(int))) != cudaSuccess)
         return bail("cudaMalloc", err);
+    if (e->visc) {
+        if ((err = cudaMalloc(&e->nbr, sizeof(int) * t.nbr.size())) != cudaSuccess || (err = cudaMalloc(&e->Q, sizeof(double) * kQ * e->lplane)) != cudaSuccess ||
+            (err = cudaMalloc(&e->Fv, sizeof(double) * 4 * e->fplane)) != cudaSuccess)
+            return bail("cudaMalloc", err);
+        if ((err = cudaMemcpy(e->nbr, t.nbr.data(), sizeof(int) * t.nbr.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return bail("cudaMemcpy", err);
+    }
     for (int k = 0; k < 6; ++k)
         if ((err = cudaMemcpy(e->code + k * e->fplane, t.code[k].data(), sizeof(int) * e->nface, cudaMemcpyHostToDevice)) != cudaSuccess)
             return bail("cudaMemcpy", err);
@@ -513,7 +751,7 @@ int fvg_cells_destroy(fvg_cells* e) {
     cudaSetDevice(e->cfg.device);
     if (e->stream) cudaStreamSynchronize(e->stream);
     for (void* p : {(void*)e->U, (void*)e->Ut, (void*)e->W, (void*)e->R, (void*)e->F, (void*)e->staging, (void*)e->code, (void*)e->meta,
-                    (void*)e->side_face, (void*)e->smax, (void*)e->bad})
+                    (void*)e->side_face, (void*)e->smax, (void*)e->bad, (void*)e->nbr, (void*)e->Q, (void*)e->Fv})
         if (p) cudaFree(p);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;

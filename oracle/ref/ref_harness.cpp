@@ -273,6 +273,11 @@ void* ref_cells_create(void* h, int max_level) {
             c->mesh = std::make_unique<fv::CellMesh>(u.Lx, u.Ly, u.nx, u.ny, max_level, per(0), per(1), u.x0, u.y0);
         c->mesh->U.assign(static_cast<size_t>(c->mesh->num_leaves()), fv::State{});
         c->eng = std::make_unique<fv::CellFluxEngine>(sim.fluid, sim.riemann, sim.muscl.get(), sim.boundaries);
+        if (sim.ns) {   // the viscous terms, as the reference's viscous level-0 tests set them (test_amr_octree_physics.cpp:16-20)
+            fv::CellPhysics ph;
+            ph.ns = sim.ns.get();
+            c->eng->set_physics(ph);
+        }
         c->eng->build(*c->mesh);
         c->ts = fv::make_time_scheme(fv::parse_time_scheme(sim.p.time_scheme), sim.p.cfl);
         c->adv = std::make_unique<fv::CellAdvance>(*c->mesh, *c->eng, *c->ts);

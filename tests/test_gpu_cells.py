@@ -1,7 +1,7 @@
 """The cell engine of an adaptive mesh on the GPU (fvg_cells_*, fenice_b200.cells) against the reference's own engine
 (CellFluxEngine + CellAdvance compiled from its sources, oracle/_ref) on level-0 meshes, bit for bit: the matrices of the
 reference's level-0 tests (cpp/tests/test_amr_octree_advance.cpp:70-108 in 3-D, cpp/tests/test_amr_mesh.cpp:440-531 in
-2-D) -- boundary sets with walls, no-slip and moving walls, inlets, outlets, transmissive and periodic sides; first order,
+2-D, cpp/tests/test_amr_octree_physics.cpp:54-92 for the 3-D viscous terms) -- boundary sets with walls, no-slip and moving walls, inlets, outlets, transmissive and periodic sides; first order,
 MUSCL, WENO3-Z and WENO5-Z with boundary_order 1 and 2; Euler, SSP-RK2 and SSP-RK3 -- each advanced 4 steps of
 dt = 2e-3 from a seeded smooth state on the reference rig's mesh (9 x 7 x 5 cells of 1.7 x 1.1 x 0.9), the CellMesh built
 with max_level 0 and 2 (every leaf of level 0 either way). The residual is compared too, and with the uniform path's
@@ -126,3 +126,37 @@ def test_leaf_order_is_free():
     Ua = np.empty_like(U)
     Ua[(ck.astype(np.int64) * 7 + cj) * 9 + ci] = a.state()
     assert bits_equal(Ua, b.state())
+
+
+VSETS = [("moving_wall", "no_slip", "wall", "moving_wall", "no_slip", "moving_wall"), ("no_slip", "moving_wall", "moving_wall", "wall", "moving_wall", "wall"),
+         ("wall", "transmissive", "no_slip", "moving_wall", "periodic", "periodic"), ("periodic", "periodic", "moving_wall", "no_slip", "wall", "moving_wall"),
+         ("outlet", "vel_inlet", "periodic", "periodic", "no_slip", "moving_wall"), ("periodic",) * 6]
+VRECON = [("none", 1), ("muscl", 1), ("muscl", 2), ("weno3", 2), ("weno5", 2)]
+
+
+@pytest.mark.parametrize("bc", VSETS, ids=["/".join(b) for b in VSETS])
+@pytest.mark.parametrize("recon,order", VRECON, ids=[f"{r}_bo{o}" for r, o in VRECON])
+def test_viscous_level0_octree_matches_the_reference(bc, recon, order):
+    """The 3-D viscous terms (every wall rule, moving walls on every axis, boundary_order 1 and 2, mu small and large so the
+    viscous speed bound wins in some cases): residual and speed bit for bit against the reference's engine and the uniform
+    path, then 4 SSP-RK3 steps against CellAdvance."""
+    for mu in (0.02, 0.6):
+        params = params_of(RIG3, bc, recon, order, SCHEMES[2], use_viscous=True, mu=mu, pr=0.72)
+        ref = Reference(params, initial_state=(1, 0, 0, 1, 0))
+        rc = ReferenceCells(ref, 0)
+        Urows, Ul = leaf_state(params, 60, rc)
+        rc.set_state(Ul)
+        eng = CellEngine(params, rc.level, rc.ci, rc.cj, rc.ck, U=Ul)
+        R, s = eng.residual()
+        R_ref, s_ref = rc.residual()
+        assert bits_equal(R, R_ref) and s == s_ref, (mu, np.abs(R - R_ref).max(), s, s_ref)
+        run = Run(params, U=Urows)
+        Ru, su = run.residual(Urows)
+        nx, ny = params["nx"], params["ny"]
+        assert bits_equal(R, Ru[(rc.ck.astype(np.int64) * ny + rc.cj) * nx + rc.ci]) and s == su
+        run.close()
+        s_refs = rc.steps(2e-3, 4)
+        for k in range(4):
+            assert eng.step(2e-3, k * 2e-3) == s_refs[k]
+        assert bits_equal(eng.state(), rc.state())
+        eng.close()
