@@ -19,7 +19,7 @@ LIB = os.path.join(HERE, "libfenice_gpu.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 SOURCES = ["runtime.cu", "mixed.cu", "batch.cu", "batch_mixed.cu", "sensor.cu", "expr.cu", "cells.cu"]
-HEADERS = ["physics.cuh", "grid.cuh", "stage.cuh", "viscous.cuh", "hancock.cuh", "mixed.cuh", "mixed_api.h", "batch.cuh", "batch_api.h", "host_common.h", "ibm.cuh", "ibm_host.h", "sensor.cuh", "sensor_api.h", "expr.h", "expr.cuh", "fourth.cuh", "tma.cuh"]
+HEADERS = ["physics.cuh", "grid.cuh", "stage.cuh", "viscous.cuh", "hancock.cuh", "mixed.cuh", "mixed_api.h", "batch.cuh", "batch_api.h", "host_common.h", "ibm.cuh", "ibm_host.h", "sensor.cuh", "sensor_api.h", "expr.h", "expr.cuh", "fourth.cuh", "tma.cuh", "tc.cuh"]
 
 COMMON_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

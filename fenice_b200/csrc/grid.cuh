@@ -34,7 +34,8 @@ struct Ctl {
     int always;         // 1: the gate of calls outside the time loop
     int steps, max_steps;
     int status;         // 0 ok; 1 the solution diverged (non-finite speed or dt, or t no longer advances); 3 a
-                        // time-dependent boundary value was not finite, or rho_in or p_out not positive, at a stage time
+                        // time-dependent boundary value was not finite, or rho_in or p_out not positive, at a stage time;
+                        // 5 a TMA copy of a stage tile, 6 a tensor-core step of the sensor did not complete (a bounded wait gave up)
 };
 
 struct Mesh {

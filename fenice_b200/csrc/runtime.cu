@@ -2332,6 +2332,7 @@ int fvg_residual(fvg_run* run, double predictor_half_dt, double* R, size_t ncell
     int rc = read_ctl(run, &h);
     if (rc) return rc;
     if (h.status == 5) return fail(run, FVG_ERR_CUDA, "a TMA copy of a stage tile did not complete");
+    if (h.status == 6) return fail(run, FVG_ERR_CUDA, "a tensor-core step of the sensor did not complete");
     if (h.status == 3) {
         char msg[256];
         std::snprintf(msg, sizeof msg, "time-dependent boundary values: not finite, or rho_in or p_out not positive, at t = %.17g", h.stage_t);
@@ -2350,6 +2351,9 @@ int fvg_residual(fvg_run* run, double predictor_half_dt, double* R, size_t ncell
 
 // The control block's verdict after `done` steps: a time-dependent boundary value out of range, or a diverged step.
 static int ctl_status(fvg_run* run, const Ctl& h, int done) {
+    // a bounded wait of a kernel that gave up (the run's state is not to be trusted after it)
+    if (h.status == 5) return fail(run, FVG_ERR_CUDA, "a TMA copy of a stage tile did not complete");
+    if (h.status == 6) return fail(run, FVG_ERR_CUDA, "a tensor-core step of the sensor did not complete");
     if (h.status == 3) {
         char msg[256];
         std::snprintf(msg, sizeof msg, "time-dependent boundary values: not finite, or rho_in or p_out not positive, at t = %.17g (step %d)", h.stage_t,

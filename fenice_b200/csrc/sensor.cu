@@ -6,6 +6,8 @@
 #include "host_common.h"
 #include "sensor.cuh"
 #include "sensor_api.h"
+#include "tc.cuh"
+#include "tma.cuh"
 
 #include <cuda_runtime.h>
 
@@ -325,34 +327,142 @@ __global__ void k_sensor_adam(float* P, float* m, float* v, float* grad, int ste
     pack_weights(*reinterpret_cast<const SensorP*>(P), out);
 }
 
-// Logits of n feature rows.
-__global__ void __launch_bounds__(256) k_sensor_infer(const SensorW* __restrict__ wg, const float* __restrict__ X, long long n, float* __restrict__ logits) {
-    __shared__ SensorW w;
-    __shared__ __align__(16) __nv_bfloat16 tiles[8][16 * kLd];
-    {
-        const int* src = reinterpret_cast<const int*>(wg);
-        int* dst = reinterpret_cast<int*>(&w);
-        for (int i = threadIdx.x; i < (int)(sizeof(SensorW) / 4); i += blockDim.x) dst[i] = src[i];
+// ------------------------------------------------------------------------------------------------ the network on tcgen05
+// A CTA of 256 threads evaluates the network 128 rows at a time on the fifth-generation tensor cores: the feature tile X
+// (128 x 32 bf16) and the weights in shared memory in the MMA's canonical layout (tc.cuh), the layer's 128 x 32 f32
+// accumulator in 32 TMEM columns; thread 0 issues the two k-steps of a layer and commits them to a shared-memory barrier;
+// warps 0-3 read the accumulator rows back (warp w its rows 32 w .. 32 w + 31), add the bias, apply ReLU, round to bf16
+// and write the hidden tile for the next layer (or, after the second layer, take the dot product with w3 in registers).
+struct __align__(128) SensTc {
+    __nv_bfloat16 X[128 * kSensK];   // canonical
+    __nv_bfloat16 H[128 * kSensH];   // canonical: the first layer's activations
+    __nv_bfloat16 W1[kSensH * kSensK];
+    __nv_bfloat16 W2[kSensH * kSensH];
+    float b1[kSensH], b2[kSensH], w3[kSensH];
+    float b3;
+    unsigned long long bar;
+    uint32_t tmem;
+    int fail;
+};
+constexpr int kTcPolls = 1 << 22;   // polls of the barrier before a wait gives up (a completion takes well under a microsecond)
+
+// the weights into s (all threads), the zero padding of X's columns kSensF .. 31, the barrier and 32 TMEM columns
+// (warp 0); ends with a block barrier
+__device__ __forceinline__ void sens_tc_setup(SensTc& s, const SensorW* __restrict__ wg) {
+    for (int i = threadIdx.x; i < kSensH * kSensK; i += blockDim.x) {
+        s.W1[tc::cl_index(i >> 5, i & 31)] = wg->W1[i];
+        s.W2[tc::cl_index(i >> 5, i & 31)] = wg->W2[i];
+    }
+    for (int i = threadIdx.x; i < kSensH; i += blockDim.x) {
+        s.b1[i] = wg->b1[i];
+        s.b2[i] = wg->b2[i];
+        s.w3[i] = wg->w3[i];
+    }
+    for (int i = threadIdx.x; i < 128 * (kSensK - kSensF); i += blockDim.x) s.X[tc::cl_index(i / (kSensK - kSensF), kSensF + i % (kSensK - kSensF))] = __float2bfloat16_rn(0.0f);
+    if (threadIdx.x == 0) {
+        s.b3 = wg->b3;
+        s.fail = 0;
+        tma::mbar_init(&s.bar, 1);
+        tma::fence_mbar_init();
+    }
+    if ((threadIdx.x >> 5) == 0) tc::tmem_alloc(&s.tmem, 32);
+    tma::fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+}
+
+__device__ __forceinline__ void sens_tc_release(SensTc& s) {
+    tc::fence_before_sync();
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(s.tmem, 32);
+    }
+}
+
+// wait for the barrier's next completion (bounded); false if it did not come
+__device__ __forceinline__ bool sens_tc_wait(SensTc& s, unsigned& phase) {
+    int polls = 0;
+    while (!tma::mbar_try_wait(&s.bar, phase & 1))
+        if (++polls >= kTcPolls) return false;
+    ++phase;
+    return true;
+}
+
+// The logit of tile row 32 w + lane in thread lane of warp w < 4 (the other warps get 0), from the feature tile s.X that
+// every thread has finished writing (each writer fenced the async proxy) before a block barrier. Contains one block
+// barrier; phase is the count of the barrier's completions so far (the same in every thread of warps 0-3).
+__device__ __forceinline__ float sens_tc_tile(SensTc& s, unsigned& phase) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    tc::fence_after_sync();
+    constexpr uint32_t ID = tc::idesc_bf16<128, kSensH>();
+    const uint32_t trow = s.tmem + ((uint32_t)(32 * warp) << 16);
+    if (threadIdx.x == 0) {
+        tc::mma_bf16(s.tmem, tc::smem_desc(s.X, 0), tc::smem_desc(s.W1, 0), ID, false);
+        tc::mma_bf16(s.tmem, tc::smem_desc(s.X, 1), tc::smem_desc(s.W1, 1), ID, true);
+        tc::commit(&s.bar);
+    }
+    if (warp < 4) {
+        if (!sens_tc_wait(s, phase)) s.fail = 1;
+        tc::fence_after_sync();
+        float d[32];
+        tc::ld32(trow, d);
+        const int r = 32 * warp + lane;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            uint32_t pk[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int j = 8 * c + 2 * k;
+                pk[k] = pack_bf16(fmaxf(d[j] + s.b1[j], 0.0f), fmaxf(d[j + 1] + s.b1[j + 1], 0.0f));
+            }
+            *reinterpret_cast<uint4*>(&s.H[tc::cl_index(r, 8 * c)]) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        }
+        tma::fence_proxy_async();
+        tc::fence_before_sync();
     }
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    __nv_bfloat16* Xs = tiles[warp];
-    const long long chunks = (n + 15) / 16;
-    for (long long ch = (long long)blockIdx.x * 8 + warp; ch < chunks; ch += (long long)gridDim.x * 8) {
-        const long long r0 = ch * 16;
-        for (int idx = lane; idx < 16 * kSensK; idx += 32) {
-            const int r = idx / kSensK, col = idx % kSensK;
-            Xs[r * kLd + col] = __float2bfloat16_rn(r0 + r < n ? X[(r0 + r) * kSensK + col] : 0.0f);
-        }
-        __syncwarp();
-        float lo, hi;
-        sensor_logits(w, Xs, kLd, lo, hi);
-        if (t == 0) {
-            if (r0 + g < n) logits[r0 + g] = lo;
-            if (r0 + g + 8 < n) logits[r0 + g + 8] = hi;
-        }
-        __syncwarp();
+    tc::fence_after_sync();
+    if (threadIdx.x == 0) {
+        tc::mma_bf16(s.tmem, tc::smem_desc(s.H, 0), tc::smem_desc(s.W2, 0), ID, false);
+        tc::mma_bf16(s.tmem, tc::smem_desc(s.H, 1), tc::smem_desc(s.W2, 1), ID, true);
+        tc::commit(&s.bar);
     }
+    float z = 0.0f;
+    if (warp < 4) {
+        if (!sens_tc_wait(s, phase)) s.fail = 1;
+        tc::fence_after_sync();
+        float d[32];
+        tc::ld32(trow, d);
+#pragma unroll
+        for (int j = 0; j < kSensH; ++j) z += round_bf16(fmaxf(d[j] + s.b2[j], 0.0f)) * s.w3[j];
+        z += s.b3;
+        tc::fence_before_sync();
+    }
+    return z;
+}
+
+// Logits of n feature rows, 128 rows per tile on the tensor cores (a NaN logit: the tensor-core step did not complete).
+__global__ void __launch_bounds__(256) k_sensor_infer(const SensorW* __restrict__ wg, const float* __restrict__ X, long long n, float* __restrict__ logits) {
+    __shared__ SensTc st;
+    sens_tc_setup(st, wg);
+    unsigned phase = 0;
+    const long long ntile = (n + 127) / 128;
+    for (long long tt = blockIdx.x; tt < ntile; tt += gridDim.x) {
+        const long long r0 = tt * 128;
+        for (int idx = threadIdx.x; idx < 128 * kSensF; idx += blockDim.x) {
+            const int r = idx / kSensF, col = idx % kSensF;
+            st.X[tc::cl_index(r, col)] = __float2bfloat16_rn(r0 + r < n ? X[(r0 + r) * kSensK + col] : 0.0f);
+        }
+        tma::fence_proxy_async();
+        __syncthreads();
+        const float z = sens_tc_tile(st, phase);
+        __syncthreads();
+        const int r = threadIdx.x;
+        if (r < 128 && r0 + r < n) logits[r0 + r] = st.fail ? __int_as_float(0x7fc00000) : z;
+    }
+    sens_tc_release(st);
 }
 
 // ------------------------------------------------------------------------------------------------ the gate
@@ -364,23 +474,16 @@ __device__ __forceinline__ bool refresh_due(const Ctl* ctl, int every) { return 
 // quantity), logits on the tensor cores.
 template <int DIM, int NV, int BX, int BY, int BZ>
 __global__ void __launch_bounds__(256) k_sensor_flags_t(Mesh m, Bc bc, Eos<double> eos, const double* __restrict__ U, const SensorW* __restrict__ wg,
-                                                        float theta, unsigned char* __restrict__ flags, const Ctl* ctl, int every, int nb0, int nb1) {
+                                                        float theta, unsigned char* __restrict__ flags, const Ctl* ctl, int every, int nb0, int nb1,
+                                                        int* err) {
     if (!refresh_due(ctl, every)) return;
     constexpr int EX = BX + 4, EY = BY + 4, EZ = DIM == 3 ? BZ + 4 : 1, BOX = EX * EY * EZ, NC = BX * BY * BZ, ROWS = NC * DIM;
     // the planes of the primitive variables PS floats apart, PS = 7 (mod 32): the lanes that read the five quantities of
     // one stencil position read five different banks (a plane stride that is a multiple of 32 puts them on one)
     constexpr int PS = BOX + ((7 - BOX % 32) + 32) % 32;
-    __shared__ __align__(16) unsigned char wbuf[kSensInferBytes];
     __shared__ float P[NV * PS];
-    __shared__ __align__(16) __nv_bfloat16 tiles[8][16 * kLd];
-    const SensorW& w = *reinterpret_cast<const SensorW*>(wbuf);
-    {
-        const int* src = reinterpret_cast<const int*>(wg);
-        int* dst = reinterpret_cast<int*>(wbuf);
-        for (int i = threadIdx.x; i < kSensInferBytes / 4; i += blockDim.x) dst[i] = src[i];
-        for (int i = threadIdx.x; i < 8 * 16; i += blockDim.x)
-            for (int k = kSensF; k < kSensK; ++k) tiles[i / 16][(i % 16) * kLd + k] = __float2bfloat16_rn(0.0f);
-    }
+    __shared__ SensTc st;
+    sens_tc_setup(st, wg);
     const int b = blockIdx.x;
     const int o0 = (b % nb0) * BX, o1 = ((b / nb0) % nb1) * BY, o2 = DIM == 3 ? (b / (nb0 * nb1)) * BZ : 0;
     for (int e = threadIdx.x; e < BOX; e += blockDim.x) {
@@ -390,40 +493,45 @@ __global__ void __launch_bounds__(256) k_sensor_flags_t(Mesh m, Bc bc, Eos<doubl
         for (int q = 0; q < NV; ++q) P[q * PS + e] = (float)wv[q];
     }
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    __nv_bfloat16* Xs = tiles[warp];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const float gam = (float)eos.gamma, pinf = eos.type == kIdeal ? 0.0f : (float)eos.p_inf;
-    for (int ch = warp; ch * 16 < ROWS; ch += 8) {
+    unsigned phase = 0;
+    for (int t0 = 0; t0 < ROWS; t0 += 128) {
+        // features of the tile's rows: warp w takes rows 16 w .. 16 w + 15, one lane per (row, quantity)
         for (int it = lane; it < 16 * kSensQ; it += 32) {
-            const int row = it / kSensQ, sq = it % kSensQ, r = ch * 16 + row;
-            const int c = r / DIM, axis = r % DIM;
-            const int var = sensor_var<NV>(sq, axis);
+            const int row = 16 * warp + it / kSensQ, sq = it % kSensQ, r = t0 + row;
             float f[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-            if (var >= 0) {
-                const int e = ((DIM == 3 ? c / (BX * BY) + 2 : 0) * EY + (c / BX) % BY + 2) * EX + c % BX + 2;
-                const int st = axis == 0 ? 1 : (axis == 1 ? EX : EX * EY);
-                float v[5];
+            if (r < ROWS) {
+                const int c = r / DIM, axis = r % DIM;
+                const int var = sensor_var<NV>(sq, axis);
+                if (var >= 0) {
+                    const int e = ((DIM == 3 ? c / (BX * BY) + 2 : 0) * EY + (c / BX) % BY + 2) * EX + c % BX + 2;
+                    const int st_ = axis == 0 ? 1 : (axis == 1 ? EX : EX * EY);
+                    float v[5];
 #pragma unroll
-                for (int k = 0; k < 5; ++k) v[k] = P[var * PS + e + (k - 2) * st];
-                sensor_quantity_features(v, sensor_scale<float>(sq, P[e], P[3 * PS + e], gam, pinf), f);
+                    for (int k = 0; k < 5; ++k) v[k] = P[var * PS + e + (k - 2) * st_];
+                    sensor_quantity_features(v, sensor_scale<float>(sq, P[e], P[3 * PS + e], gam, pinf), f);
+                }
             }
 #pragma unroll
-            for (int k = 0; k < 5; ++k) Xs[row * kLd + 5 * sq + k] = __float2bfloat16_rn(f[k]);
+            for (int k = 0; k < 5; ++k) st.X[tc::cl_index(row, 5 * sq + k)] = __float2bfloat16_rn(f[k]);
         }
-        __syncwarp();
-        float lo, hi;
-        sensor_logits(w, Xs, kLd, lo, hi);
-        if (t == 0) {
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int r = ch * 16 + g + 8 * h, c = r / DIM, axis = r % DIM;
+        tma::fence_proxy_async();
+        __syncthreads();
+        const float z = sens_tc_tile(st, phase);
+        __syncthreads();
+        if (warp < 4) {
+            const int r = t0 + 32 * warp + lane;
+            if (r < ROWS) {
+                const int c = r / DIM, axis = r % DIM;
                 const int i = o0 + c % BX, j = o1 + (c / BX) % BY, k = DIM == 3 ? o2 + c / (BX * BY) : 0;
-                if (i >= m.nx || j >= m.ny || k >= m.nz) continue;
-                flags[axis * m.plane + ((long long)k * m.ny + j) * m.nx + i] = (h ? hi : lo) < theta ? 0 : 1;
+                // a tensor-core step that did not complete leaves the row WENO5-Z
+                if (i < m.nx && j < m.ny && k < m.nz) flags[axis * m.plane + ((long long)k * m.ny + j) * m.nx + i] = (!st.fail && z < theta) ? 0 : 1;
             }
         }
-        __syncwarp();
     }
+    if (st.fail && threadIdx.x == 0 && err) atomicExch(err, 6);
+    sens_tc_release(st);
 }
 
 // The tile flags of the stage kernels from the network's flags. Tile b is linear along axis a (0) when no cell whose
@@ -531,12 +639,14 @@ cudaError_t fvg::sensor_refresh(const Mesh& m, const Bc& bc, const Eos<double>& 
                                 const int tiles[3], unsigned char* tile_flags, const Ctl* ctl, int every, unsigned long long* counts,
                                 cudaStream_t s, int split, int peer_lo, int peer_hi) {
     const SensorW* w = static_cast<const SensorW*>(weights);
+    // a tensor-core step of the network that did not complete: status 6 in the run's control block
+    int* err = ctl ? const_cast<int*>(&ctl->status) : nullptr;
     if (dim == 3) {
         const int b0 = (m.nx + 7) / 8, b1 = (m.ny + 7) / 8, b2 = (m.nz + 3) / 4;
-        k_sensor_flags_t<3, 5, 8, 8, 4><<<b0 * b1 * b2, 256, 0, s>>>(m, bc, eos, U, w, theta, flags0, ctl, every, b0, b1);
+        k_sensor_flags_t<3, 5, 8, 8, 4><<<b0 * b1 * b2, 256, 0, s>>>(m, bc, eos, U, w, theta, flags0, ctl, every, b0, b1, err);
     } else {
         const int b0 = (m.nx + 31) / 32, b1 = (m.ny + 7) / 8;
-        k_sensor_flags_t<2, 4, 32, 8, 1><<<b0 * b1, 256, 0, s>>>(m, bc, eos, U, w, theta, flags0, ctl, every, b0, b1);
+        k_sensor_flags_t<2, 4, 32, 8, 1><<<b0 * b1, 256, 0, s>>>(m, bc, eos, U, w, theta, flags0, ctl, every, b0, b1, err);
     }
     const long long nr = (long long)dim * m.nz * m.ny * tiles[0];
     const int rb = (int)((nr + 255) / 256 < 148 * 16 ? (nr + 255) / 256 : 148 * 16);
