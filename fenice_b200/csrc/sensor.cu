@@ -96,203 +96,6 @@ __global__ void k_sensor_extract(Mesh m, Bc bc, Eos<double> eos, const double* _
 }
 
 // ------------------------------------------------------------------------------------------------ training
-constexpr int kLd = 40;   // row stride (bf16) of the per-warp 16 x 32 tiles in shared memory (rows on distinct banks)
-
-// A 16 x 16 row-major A fragment whose element (m, k) is T[k][m0 + m] of a tile T (rows = k): the transpose of a tile.
-__device__ __forceinline__ void load_at_frag(const __nv_bfloat16* T, int m0, uint32_t (&a)[4]) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    a[0] = pack_bf16_raw(T[(2 * t) * kLd + m0 + g], T[(2 * t + 1) * kLd + m0 + g]);
-    a[1] = pack_bf16_raw(T[(2 * t) * kLd + m0 + g + 8], T[(2 * t + 1) * kLd + m0 + g + 8]);
-    a[2] = pack_bf16_raw(T[(2 * t + 8) * kLd + m0 + g], T[(2 * t + 9) * kLd + m0 + g]);
-    a[3] = pack_bf16_raw(T[(2 * t + 8) * kLd + m0 + g + 8], T[(2 * t + 9) * kLd + m0 + g + 8]);
-}
-// A 16 x 8 col B fragment whose element (k, n) is T[k][n0 + n].
-__device__ __forceinline__ void load_b_frag(const __nv_bfloat16* T, int n0, uint32_t (&b)[2]) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    b[0] = pack_bf16_raw(T[(2 * t) * kLd + n0 + g], T[(2 * t + 1) * kLd + n0 + g]);
-    b[1] = pack_bf16_raw(T[(2 * t + 8) * kLd + n0 + g], T[(2 * t + 9) * kLd + n0 + g]);
-}
-// acc[mt][nt] += L^T R over the 16 rows of two tiles: (32 x 16) x (16 x 32) on the tensor cores.
-__device__ __forceinline__ void outer_acc(const __nv_bfloat16* L, const __nv_bfloat16* R, float (&acc)[2][4][4]) {
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt) {
-        uint32_t a[4];
-        load_at_frag(L, 16 * mt, a);
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-            uint32_t b[2];
-            load_b_frag(R, 8 * nt, b);
-            mma16816(acc[mt][nt], a, b);
-        }
-    }
-}
-// store a C-layout 16 x 32 tile (rows g, g + 8 of the four n-tiles) to shared memory as bf16
-__device__ __forceinline__ void store_c_tile(__nv_bfloat16* T, const float (&v)[4][4]) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int nt = 0; nt < 4; ++nt) {
-        *reinterpret_cast<uint32_t*>(T + g * kLd + 8 * nt + 2 * t) = pack_bf16(v[nt][0], v[nt][1]);
-        *reinterpret_cast<uint32_t*>(T + (g + 8) * kLd + 8 * nt + 2 * t) = pack_bf16(v[nt][2], v[nt][3]);
-    }
-}
-__device__ __forceinline__ float group_sum(float v) {   // over the 8 groups (lanes with the same t)
-    v += __shfl_xor_sync(0xffffffffu, v, 4);
-    v += __shfl_xor_sync(0xffffffffu, v, 8);
-    v += __shfl_xor_sync(0xffffffffu, v, 16);
-    return v;
-}
-
-// Gradients of the mean class-weighted binary cross-entropy (weight wpos on troubled samples) over n samples, added
-// to grad (a SensorP of float32) and the loss sum to *loss. Each warp takes 16 samples at a time: forward on the
-// tensor cores, the backward products (hidden gradients x weights, and the weight gradients as sums over the samples
-// of outer products) on the tensor cores too, bfloat16 operands and float32 sums.
-__global__ void __launch_bounds__(256) k_sensor_grad(const SensorW* __restrict__ wg, const float* __restrict__ X, const float* __restrict__ y, long long n,
-                                                     float wpos, float inv_n, float* __restrict__ grad, float* __restrict__ loss) {
-    __shared__ SensorW w;
-    __shared__ float gs[kSensParams];
-    __shared__ __align__(16) __nv_bfloat16 tiles[8][3][16 * kLd];
-    {
-        const int* src = reinterpret_cast<const int*>(wg);
-        int* dst = reinterpret_cast<int*>(&w);
-        for (int i = threadIdx.x; i < (int)(sizeof(SensorW) / 4); i += blockDim.x) dst[i] = src[i];
-        for (int i = threadIdx.x; i < kSensParams; i += blockDim.x) gs[i] = 0.0f;
-    }
-    __syncthreads();
-    SensorP& G = *reinterpret_cast<SensorP*>(gs);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    __nv_bfloat16* Xs = tiles[warp][0];
-    __nv_bfloat16* H1s = tiles[warp][1];
-    __nv_bfloat16* D2s = tiles[warp][2];
-    float gW1[2][4][4] = {}, gW2[2][4][4] = {};
-    float gb1[4][2] = {}, gb2[4][2] = {}, gw3[4][2] = {};
-    float gb3 = 0.0f, lsum = 0.0f;
-    const long long chunks = (n + 15) / 16;
-    for (long long ch = (long long)blockIdx.x * 8 + warp; ch < chunks; ch += (long long)gridDim.x * 8) {
-        const long long r0 = ch * 16;
-        for (int idx = lane; idx < 16 * kSensK; idx += 32) {
-            const int r = idx / kSensK, col = idx % kSensK;
-            Xs[r * kLd + col] = __float2bfloat16_rn(r0 + r < n ? X[(r0 + r) * kSensK + col] : 0.0f);
-        }
-        __syncwarp();
-        // ---- forward
-        uint32_t a[2][4];
-        float h1[4][4], h2[4][4];
-        load_a_frags(Xs, kLd, a);
-        dense32(a, w.W1, h1);
-        relu_to_a(h1, w.b1, a);
-        store_c_tile(H1s, h1);
-        dense32(a, w.W2, h2);
-        relu_to_a(h2, w.b2, a);
-        float zl = 0.0f, zh = 0.0f;
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-            const float w0 = w.w3[8 * nt + 2 * t], w1 = w.w3[8 * nt + 2 * t + 1];
-            zl += h2[nt][0] * w0 + h2[nt][1] * w1;
-            zh += h2[nt][2] * w0 + h2[nt][3] * w1;
-        }
-        zl += __shfl_xor_sync(0xffffffffu, zl, 1);
-        zl += __shfl_xor_sync(0xffffffffu, zl, 2);
-        zh += __shfl_xor_sync(0xffffffffu, zh, 1);
-        zh += __shfl_xor_sync(0xffffffffu, zh, 2);
-        zl += w.b3;
-        zh += w.b3;
-        // ---- loss and the logit gradients of rows g and g + 8
-        float dzl = 0.0f, dzh = 0.0f;
-        {
-            const long long rl = r0 + g, rh = r0 + g + 8;
-            const float yl = rl < n ? y[rl] : 0.0f, yh = rh < n ? y[rh] : 0.0f;
-            const float wl = rl < n ? (yl > 0.5f ? wpos : 1.0f) : 0.0f, wh = rh < n ? (yh > 0.5f ? wpos : 1.0f) : 0.0f;
-            const float spl = fmaxf(zl, 0.0f) + log1pf(__expf(-fabsf(zl))), sph = fmaxf(zh, 0.0f) + log1pf(__expf(-fabsf(zh)));
-            dzl = wl * (1.0f / (1.0f + __expf(-zl)) - yl) * inv_n;
-            dzh = wh * (1.0f / (1.0f + __expf(-zh)) - yh) * inv_n;
-            if (t == 0) {
-                lsum += wl * (spl - yl * zl) + wh * (sph - yh * zh);
-                gb3 += dzl + dzh;
-            }
-        }
-        // ---- backward: dh2 = dz w3 (z2 > 0), dh1 = (dh2 W2) (z1 > 0)
-        float d2[4][4];
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-#pragma unroll
-            for (int jj = 0; jj < 2; ++jj) {
-                const float w3v = w.w3[8 * nt + 2 * t + jj];
-                gw3[nt][jj] += dzl * h2[nt][jj] + dzh * h2[nt][jj + 2];
-                d2[nt][jj] = h2[nt][jj] > 0.0f ? dzl * w3v : 0.0f;
-                d2[nt][jj + 2] = h2[nt][jj + 2] > 0.0f ? dzh * w3v : 0.0f;
-                gb2[nt][jj] += d2[nt][jj] + d2[nt][jj + 2];
-            }
-        }
-        store_c_tile(D2s, d2);
-        uint32_t ad[2][4];
-#pragma unroll
-        for (int s2 = 0; s2 < 2; ++s2) {
-            ad[s2][0] = pack_bf16(d2[2 * s2][0], d2[2 * s2][1]);
-            ad[s2][1] = pack_bf16(d2[2 * s2][2], d2[2 * s2][3]);
-            ad[s2][2] = pack_bf16(d2[2 * s2 + 1][0], d2[2 * s2 + 1][1]);
-            ad[s2][3] = pack_bf16(d2[2 * s2 + 1][2], d2[2 * s2 + 1][3]);
-        }
-        float d1[4][4];
-        dense32(ad, w.W2T, d1);
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) d1[nt][q] = h1[nt][q] > 0.0f ? d1[nt][q] : 0.0f;
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-            gb1[nt][0] += d1[nt][0] + d1[nt][2];
-            gb1[nt][1] += d1[nt][1] + d1[nt][3];
-        }
-        __syncwarp();
-        // ---- weight gradients: dW2 += dh2^T h1, then dW1 += dh1^T x (dh1 takes the slot of h1)
-        outer_acc(D2s, H1s, gW2);
-        __syncwarp();
-        store_c_tile(H1s, d1);
-        __syncwarp();
-        outer_acc(H1s, Xs, gW1);
-        __syncwarp();
-    }
-    // ---- the warp's sums into the block's, then the block's into grad
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-            const int o = 16 * mt + g, i = 8 * nt + 2 * t;
-            atomicAdd(&G.W1[o * kSensK + i], gW1[mt][nt][0]);
-            atomicAdd(&G.W1[o * kSensK + i + 1], gW1[mt][nt][1]);
-            atomicAdd(&G.W1[(o + 8) * kSensK + i], gW1[mt][nt][2]);
-            atomicAdd(&G.W1[(o + 8) * kSensK + i + 1], gW1[mt][nt][3]);
-            atomicAdd(&G.W2[o * kSensH + i], gW2[mt][nt][0]);
-            atomicAdd(&G.W2[o * kSensH + i + 1], gW2[mt][nt][1]);
-            atomicAdd(&G.W2[(o + 8) * kSensH + i], gW2[mt][nt][2]);
-            atomicAdd(&G.W2[(o + 8) * kSensH + i + 1], gW2[mt][nt][3]);
-        }
-#pragma unroll
-    for (int nt = 0; nt < 4; ++nt)
-#pragma unroll
-        for (int jj = 0; jj < 2; ++jj) {
-            const float v1 = group_sum(gb1[nt][jj]), v2 = group_sum(gb2[nt][jj]), v3 = group_sum(gw3[nt][jj]);
-            if (g == 0) {
-                atomicAdd(&G.b1[8 * nt + 2 * t + jj], v1);
-                atomicAdd(&G.b2[8 * nt + 2 * t + jj], v2);
-                atomicAdd(&G.w3[8 * nt + 2 * t + jj], v3);
-            }
-        }
-    gb3 = group_sum(gb3);
-    lsum = group_sum(lsum);
-    gb3 += __shfl_xor_sync(0xffffffffu, gb3, 1);
-    gb3 += __shfl_xor_sync(0xffffffffu, gb3, 2);
-    lsum += __shfl_xor_sync(0xffffffffu, lsum, 1);
-    lsum += __shfl_xor_sync(0xffffffffu, lsum, 2);
-    if (lane == 0) {
-        atomicAdd(&G.b3, gb3);
-        atomicAdd(loss, lsum);
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < kSensParams; i += blockDim.x)
-        if (gs[i] != 0.0f) atomicAdd(&grad[i], gs[i]);
-}
-
 // The device weights (bfloat16 copies, the transposed second layer) of float32 master parameters.
 __device__ void pack_weights(const SensorP& P, SensorW* out) {
     for (int i = threadIdx.x; i < kSensH * kSensK; i += blockDim.x) out->W1[i] = __float2bfloat16_rn((i % kSensK) < kSensF ? P.W1[i] : 0.0f);
@@ -328,26 +131,32 @@ __global__ void k_sensor_adam(float* P, float* m, float* v, float* grad, int ste
 }
 
 // ------------------------------------------------------------------------------------------------ the network on tcgen05
-// A CTA of 256 threads evaluates the network 128 rows at a time on the fifth-generation tensor cores: the feature tile X
-// (128 x 32 bf16) and the weights in shared memory in the MMA's canonical layout (tc.cuh), the layer's 128 x 32 f32
-// accumulator in 32 TMEM columns; thread 0 issues the two k-steps of a layer and commits them to a shared-memory barrier;
-// warps 0-3 read the accumulator rows back (warp w its rows 32 w .. 32 w + 31), add the bias, apply ReLU, round to bf16
-// and write the hidden tile for the next layer (or, after the second layer, take the dot product with w3 in registers).
+// A CTA of 256 threads evaluates the network 128 rows at a time on the fifth-generation tensor cores, as two independent
+// warpgroups (warps 0-3 and 4-7) that take alternate tiles: each has its own feature tile X (128 x 32 bf16) and hidden
+// tile H in shared memory in the MMA's canonical layout (tc.cuh), its own 32 TMEM columns for the layer's 128 x 32 f32
+// accumulator, its own completion barrier and a named barrier for its 128 threads. The first thread of the group issues
+// the two k-steps of a layer and commits them; the group's warps read the accumulator rows back (warp w its TMEM lane
+// quarter w % 4: rows 32 (w % 4) .. + 31), add the bias, apply ReLU, round to bf16 and write H for the second layer, or,
+// after the second layer, take the dot product with w3 in registers. The two groups' tiles interleave on the tensor core.
 struct __align__(128) SensTc {
-    __nv_bfloat16 X[128 * kSensK];   // canonical
-    __nv_bfloat16 H[128 * kSensH];   // canonical: the first layer's activations
+    __nv_bfloat16 X[2][128 * kSensK];   // canonical, one per warpgroup
+    __nv_bfloat16 H[2][128 * kSensH];   // canonical: the first layer's activations
     __nv_bfloat16 W1[kSensH * kSensK];
     __nv_bfloat16 W2[kSensH * kSensH];
     float b1[kSensH], b2[kSensH], w3[kSensH];
     float b3;
-    unsigned long long bar;
+    unsigned long long bar[2];
     uint32_t tmem;
     int fail;
 };
-constexpr int kTcPolls = 1 << 22;   // polls of the barrier before a wait gives up (a completion takes well under a microsecond)
+constexpr int kTcPolls = 1 << 22;   // polls of a barrier before a wait gives up (a completion takes well under a microsecond)
 
-// the weights into s (all threads), the zero padding of X's columns kSensF .. 31, the barrier and 32 TMEM columns
-// (warp 0); ends with a block barrier
+__device__ __forceinline__ void wg_sync(int g) {   // the 128 threads of warpgroup g
+    asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory");
+}
+
+// the weights into s (all threads), the zero padding of both X tiles' columns kSensF .. 31, the barriers and 64 TMEM
+// columns (warp 0); ends with a block barrier
 __device__ __forceinline__ void sens_tc_setup(SensTc& s, const SensorW* __restrict__ wg) {
     for (int i = threadIdx.x; i < kSensH * kSensK; i += blockDim.x) {
         s.W1[tc::cl_index(i >> 5, i & 31)] = wg->W1[i];
@@ -358,14 +167,16 @@ __device__ __forceinline__ void sens_tc_setup(SensTc& s, const SensorW* __restri
         s.b2[i] = wg->b2[i];
         s.w3[i] = wg->w3[i];
     }
-    for (int i = threadIdx.x; i < 128 * (kSensK - kSensF); i += blockDim.x) s.X[tc::cl_index(i / (kSensK - kSensF), kSensF + i % (kSensK - kSensF))] = __float2bfloat16_rn(0.0f);
+    constexpr int PAD = kSensK - kSensF;
+    for (int i = threadIdx.x; i < 2 * 128 * PAD; i += blockDim.x) s.X[i / (128 * PAD)][tc::cl_index((i / PAD) % 128, kSensF + i % PAD)] = __float2bfloat16_rn(0.0f);
     if (threadIdx.x == 0) {
         s.b3 = wg->b3;
         s.fail = 0;
-        tma::mbar_init(&s.bar, 1);
+        tma::mbar_init(&s.bar[0], 1);
+        tma::mbar_init(&s.bar[1], 1);
         tma::fence_mbar_init();
     }
-    if ((threadIdx.x >> 5) == 0) tc::tmem_alloc(&s.tmem, 32);
+    if ((threadIdx.x >> 5) == 0) tc::tmem_alloc(&s.tmem, 64);
     tma::fence_proxy_async();
     tc::fence_before_sync();
     __syncthreads();
@@ -377,90 +188,295 @@ __device__ __forceinline__ void sens_tc_release(SensTc& s) {
     __syncthreads();
     if ((threadIdx.x >> 5) == 0) {
         tc::fence_after_sync();
-        tc::tmem_dealloc(s.tmem, 32);
+        tc::tmem_dealloc(s.tmem, 64);
     }
 }
 
-// wait for the barrier's next completion (bounded); false if it did not come
-__device__ __forceinline__ bool sens_tc_wait(SensTc& s, unsigned& phase) {
+// the next completion of warpgroup g's barrier (bounded; a wait that gives up sets s.fail)
+__device__ __forceinline__ void sens_tc_wait(SensTc& s, int g, unsigned& phase) {
+    int polls = 0;
+    while (!tma::mbar_try_wait(&s.bar[g], phase & 1))
+        if (++polls >= kTcPolls) {
+            s.fail = 1;
+            break;
+        }
+    ++phase;
+    tc::fence_after_sync();
+}
+
+// The logit of row 32 (warp % 4) + lane of warpgroup g's feature tile s.X[g], which the group's threads have written (each
+// fenced the async proxy after its writes); called by the 128 threads of the group, which it synchronises twice. phase
+// counts the completions of the group's barrier so far.
+__device__ __forceinline__ float sens_tc_tile(SensTc& s, int g, unsigned& phase) {
+    const int q = (threadIdx.x >> 5) & 3, lane = threadIdx.x & 31;
+    const bool issuer = (threadIdx.x & 127) == 0;
+    constexpr uint32_t ID = tc::idesc_bf16<128, kSensH>();
+    const uint32_t tcol = s.tmem + 32u * g, trow = tcol + ((uint32_t)(32 * q) << 16);
+    tc::fence_before_sync();
+    wg_sync(g);
+    tc::fence_after_sync();
+    if (issuer) {
+        tc::mma_bf16(tcol, tc::smem_desc(s.X[g], 0), tc::smem_desc(s.W1, 0), ID, false);
+        tc::mma_bf16(tcol, tc::smem_desc(s.X[g], 1), tc::smem_desc(s.W1, 1), ID, true);
+        tc::commit(&s.bar[g]);
+    }
+    sens_tc_wait(s, g, phase);
+    float d[32];
+    tc::ld32(trow, d);
+    const int r = 32 * q + lane;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        uint32_t pk[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int j = 8 * c + 2 * k;
+            pk[k] = pack_bf16(fmaxf(d[j] + s.b1[j], 0.0f), fmaxf(d[j + 1] + s.b1[j + 1], 0.0f));
+        }
+        *reinterpret_cast<uint4*>(&s.H[g][tc::cl_index(r, 8 * c)]) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    }
+    tma::fence_proxy_async();
+    tc::fence_before_sync();
+    wg_sync(g);
+    tc::fence_after_sync();
+    if (issuer) {
+        tc::mma_bf16(tcol, tc::smem_desc(s.H[g], 0), tc::smem_desc(s.W2, 0), ID, false);
+        tc::mma_bf16(tcol, tc::smem_desc(s.H[g], 1), tc::smem_desc(s.W2, 1), ID, true);
+        tc::commit(&s.bar[g]);
+    }
+    sens_tc_wait(s, g, phase);
+    tc::ld32(trow, d);
+    float z = 0.0f;
+#pragma unroll
+    for (int j = 0; j < kSensH; ++j) z += round_bf16(fmaxf(d[j] + s.b2[j], 0.0f)) * s.w3[j];
+    return z + s.b3;
+}
+
+// ---- training on tcgen05
+// Gradients of the mean class-weighted binary cross-entropy (weight wpos on troubled samples) over n samples, added to
+// grad (a SensorP of float32) and the loss sum to *loss. A CTA of 256 threads takes 128 samples at a time; every product is
+// a tcgen05.mma with bf16 operands in shared memory and f32 accumulators in TMEM:
+//   forward   z1 = x W1^T, z2 = h1 W2^T                                      (M = 128 samples, N = 32, K = 32)
+//   backward  dh1 = dh2 W2 (masked by z1 > 0)                                (M = 128, N = 32, K = 32)
+//   weights   G += A^T B over the samples, accumulated in TMEM over all the CTA's tiles (M = 128, N = 96, K = 128 per tile)
+//             with A = [dh2 | dh1 | dz | 0] (128 columns) and B = [h1 | x | h2] (96 columns; x's padding input 31 set to 1):
+//             G[0:32, 0:32] = dW2, G[0:32, 63] = db2, G[32:64, 32:64] = dW1 (column 63: db1), G[64, 64:96] = dw3, G[64, 63] = db3.
+// A and B are stored as samples x columns in the canonical layout (core matrices of 8 samples x 8 columns, 128 bytes, the
+// column groups of an 8-sample group adjacent): read with the samples as K they are MN-major operands, with the samples as
+// M K-major ones. Back-propagated values enter the products rounded to bf16 (dh2, dh1, dz).
+constexpr int kGA = 128, kGB = 96;   // columns of the A and B tiles
+struct __align__(1024) GradTc {
+    __nv_bfloat16 A[128 * kGA];   // 16 column groups per 8-sample group (2048 bytes)
+    __nv_bfloat16 B[128 * kGB];   // 12 column groups per 8-sample group (1536 bytes)
+    __nv_bfloat16 W1[kSensH * kSensK], W2[kSensH * kSensH], W2T[kSensH * kSensH];   // canonical, K-major
+    float b1[kSensH], b2[kSensH], w3[kSensH];
+    float b3, loss;
+    unsigned long long bar;
+    uint32_t tmem;
+    int fail;
+};
+constexpr int kGradSmem = (int)sizeof(GradTc);
+
+// element offset of (sample r, column c) of a canonical tile with `groups` column groups
+__device__ __forceinline__ int gt_index(int r, int c, int groups) { return ((r >> 3) * groups + (c >> 3)) * 64 + (r & 7) * 8 + (c & 7); }
+
+// the next completion of the barrier, waited for by warps 0-3 (bounded: a wait that gives up sets s.fail)
+__device__ __forceinline__ void grad_wait(GradTc& s, unsigned& phase) {
     int polls = 0;
     while (!tma::mbar_try_wait(&s.bar, phase & 1))
-        if (++polls >= kTcPolls) return false;
+        if (++polls >= kTcPolls) {
+            s.fail = 1;
+            break;
+        }
     ++phase;
-    return true;
+    tc::fence_after_sync();
 }
 
-// The logit of tile row 32 w + lane in thread lane of warp w < 4 (the other warps get 0), from the feature tile s.X that
-// every thread has finished writing (each writer fenced the async proxy) before a block barrier. Contains one block
-// barrier; phase is the count of the barrier's completions so far (the same in every thread of warps 0-3).
-__device__ __forceinline__ float sens_tc_tile(SensTc& s, unsigned& phase) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    tc::fence_after_sync();
-    constexpr uint32_t ID = tc::idesc_bf16<128, kSensH>();
-    const uint32_t trow = s.tmem + ((uint32_t)(32 * warp) << 16);
-    if (threadIdx.x == 0) {
-        tc::mma_bf16(s.tmem, tc::smem_desc(s.X, 0), tc::smem_desc(s.W1, 0), ID, false);
-        tc::mma_bf16(s.tmem, tc::smem_desc(s.X, 1), tc::smem_desc(s.W1, 1), ID, true);
-        tc::commit(&s.bar);
-    }
-    if (warp < 4) {
-        if (!sens_tc_wait(s, phase)) s.fail = 1;
-        tc::fence_after_sync();
-        float d[32];
-        tc::ld32(trow, d);
-        const int r = 32 * warp + lane;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            uint32_t pk[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int j = 8 * c + 2 * k;
-                pk[k] = pack_bf16(fmaxf(d[j] + s.b1[j], 0.0f), fmaxf(d[j + 1] + s.b1[j + 1], 0.0f));
-            }
-            *reinterpret_cast<uint4*>(&s.H[tc::cl_index(r, 8 * c)]) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-        }
-        tma::fence_proxy_async();
-        tc::fence_before_sync();
-    }
+// every thread's shared-memory writes visible to the next MMA, every TMEM read done before it
+__device__ __forceinline__ void grad_sync() {
+    tma::fence_proxy_async();
+    tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    if (threadIdx.x == 0) {
-        tc::mma_bf16(s.tmem, tc::smem_desc(s.H, 0), tc::smem_desc(s.W2, 0), ID, false);
-        tc::mma_bf16(s.tmem, tc::smem_desc(s.H, 1), tc::smem_desc(s.W2, 1), ID, true);
-        tc::commit(&s.bar);
-    }
-    float z = 0.0f;
-    if (warp < 4) {
-        if (!sens_tc_wait(s, phase)) s.fail = 1;
-        tc::fence_after_sync();
-        float d[32];
-        tc::ld32(trow, d);
-#pragma unroll
-        for (int j = 0; j < kSensH; ++j) z += round_bf16(fmaxf(d[j] + s.b2[j], 0.0f)) * s.w3[j];
-        z += s.b3;
-        tc::fence_before_sync();
-    }
-    return z;
 }
 
-// Logits of n feature rows, 128 rows per tile on the tensor cores (a NaN logit: the tensor-core step did not complete).
+__global__ void __launch_bounds__(256) k_sensor_grad(const SensorW* __restrict__ wg, const float* __restrict__ X, const float* __restrict__ y, long long n,
+                                                     float wpos, float inv_n, float* __restrict__ grad, float* __restrict__ loss) {
+    extern __shared__ __align__(1024) unsigned char gsm[];
+    GradTc& s = *reinterpret_cast<GradTc*>(gsm);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = threadIdx.x; i < kSensH * kSensK; i += blockDim.x) {
+        s.W1[tc::cl_index(i >> 5, i & 31)] = wg->W1[i];
+        s.W2[tc::cl_index(i >> 5, i & 31)] = wg->W2[i];
+        s.W2T[tc::cl_index(i >> 5, i & 31)] = wg->W2T[i];
+    }
+    for (int i = threadIdx.x; i < kSensH; i += blockDim.x) {
+        s.b1[i] = wg->b1[i];
+        s.b2[i] = wg->b2[i];
+        s.w3[i] = wg->w3[i];
+    }
+    for (int i = threadIdx.x; i < 128 * kGA; i += blockDim.x) s.A[i] = __float2bfloat16_rn(0.0f);   // columns 65 .. 127 stay 0
+    if (threadIdx.x == 0) {
+        s.b3 = wg->b3;
+        s.loss = 0.0f;
+        s.fail = 0;
+        tma::mbar_init(&s.bar, 1);
+        tma::fence_mbar_init();
+    }
+    if (warp == 0) tc::tmem_alloc(&s.tmem, 128);   // columns 0-95: G; 96-127: the layers' accumulator
+    grad_sync();
+    const uint32_t tG = s.tmem, tZ = s.tmem + 96, lane_off = (uint32_t)(32 * (warp & 3)) << 16;
+    constexpr uint32_t ID32 = tc::idesc_bf16<128, 32>(), IDG = tc::idesc_bf16<128, kGB, true>();
+    // tZ = A W^T of a 128 x 32 block of a tile read K-major (samples as M: 8-sample groups `sbo` bytes apart, column groups
+    // 128), committed to the barrier
+    auto layer = [&](const void* abase, uint32_t aoff, uint32_t sbo, const __nv_bfloat16* W) {
+        if (threadIdx.x == 0) {
+            tc::mma_bf16(tZ, tc::smem_desc_at(abase, aoff, 128, sbo), tc::smem_desc(W, 0), ID32, false);
+            tc::mma_bf16(tZ, tc::smem_desc_at(abase, aoff + 256, 128, sbo), tc::smem_desc(W, 1), ID32, true);
+            tc::commit(&s.bar);
+        }
+    };
+    unsigned phase = 0;
+    float lsum = 0.0f;
+    const long long ntile = (n + 127) / 128;
+    int done = 0;
+    for (long long tt = blockIdx.x; tt < ntile; tt += gridDim.x, ++done) {
+        const long long r0 = tt * 128;
+        // x into B's columns 32 .. 63 (input 31 = 1 on a sample: the bias column of the products)
+        for (int idx = threadIdx.x; idx < 128 * kSensK; idx += blockDim.x) {
+            const int r = idx / kSensK, c = idx % kSensK;
+            const bool in = r0 + r < n;
+            const float v = !in ? 0.0f : (c < kSensF ? X[(r0 + r) * kSensK + c] : (c == kSensK - 1 ? 1.0f : 0.0f));
+            s.B[gt_index(r, 32 + c, 12)] = __float2bfloat16_rn(v);
+        }
+        grad_sync();
+        layer(s.B, 4 * 128, 1536, s.W1);   // z1 = x W1^T
+        uint32_t mask1 = 0;
+        if (warp < 4) {
+            grad_wait(s, phase);
+            float d[32];
+            tc::ld32(tZ + lane_off, d);
+            const int r = 32 * warp + lane;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const float z = d[j] + s.b1[j];
+                mask1 |= (z > 0.0f ? 1u : 0u) << j;
+                s.B[gt_index(r, j, 12)] = __float2bfloat16_rn(fmaxf(z, 0.0f));
+            }
+        }
+        grad_sync();
+        layer(s.B, 0, 1536, s.W2);   // z2 = h1 W2^T
+        if (warp < 4) {
+            grad_wait(s, phase);
+            float d[32];
+            tc::ld32(tZ + lane_off, d);
+            const int r = 32 * warp + lane;
+            const long long gr = r0 + r;
+            float h2[32], zsum = 0.0f;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                h2[j] = round_bf16(fmaxf(d[j] + s.b2[j], 0.0f));
+                zsum += h2[j] * s.w3[j];
+            }
+            const float z = zsum + s.b3;
+            float dz = 0.0f;
+            if (gr < n) {
+                const float yv = y[gr], wv = yv > 0.5f ? wpos : 1.0f;
+                lsum += wv * (fmaxf(z, 0.0f) + log1pf(__expf(-fabsf(z))) - yv * z);
+                dz = wv * (1.0f / (1.0f + __expf(-z)) - yv) * inv_n;
+            }
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                s.A[gt_index(r, j, 16)] = __float2bfloat16_rn(d[j] + s.b2[j] > 0.0f ? dz * s.w3[j] : 0.0f);
+                s.B[gt_index(r, 64 + j, 12)] = __float2bfloat16_rn(h2[j]);
+            }
+            s.A[gt_index(r, 64, 16)] = __float2bfloat16_rn(dz);
+        }
+        grad_sync();
+        layer(s.A, 0, 2048, s.W2T);   // dh2 W2 (W2T: [in][out], read K-major)
+        if (warp < 4) {
+            grad_wait(s, phase);
+            float d[32];
+            tc::ld32(tZ + lane_off, d);
+            const int r = 32 * warp + lane;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) s.A[gt_index(r, 32 + j, 16)] = __float2bfloat16_rn((mask1 >> j) & 1u ? d[j] : 0.0f);
+        }
+        grad_sync();
+        // G += A^T B over the tile's 128 samples: 8 k-steps of 16 samples (two 8-sample groups each)
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                tc::mma_bf16(tG, tc::smem_desc_at(s.A, 4096u * k, 2048, 128), tc::smem_desc_at(s.B, 3072u * k, 1536, 128), IDG, done > 0 || k > 0);
+            tc::commit(&s.bar);
+        }
+        if (warp < 4) grad_wait(s, phase);   // the tiles are rewritten next: the products must have read them
+        grad_sync();
+    }
+    // ---- the CTA's sums into grad (warps 0-3: TMEM lane m = 32 warp + lane holds row m of G)
+    if (warp < 4 && done > 0 && !s.fail) {
+        SensorP& G = *reinterpret_cast<SensorP*>(grad);
+        const int m = 32 * warp + lane;
+        float g0[32], g1[32], g2[32];
+        tc::ld32(tG + lane_off, g0);
+        tc::ld32(tG + lane_off + 32, g1);
+        tc::ld32(tG + lane_off + 64, g2);
+        if (m < 32) {
+#pragma unroll
+            for (int i = 0; i < 32; ++i) atomicAdd(&G.W2[m * kSensH + i], g0[i]);
+            atomicAdd(&G.b2[m], g1[31]);
+        } else if (m < 64) {
+#pragma unroll
+            for (int i = 0; i < kSensF; ++i) atomicAdd(&G.W1[(m - 32) * kSensK + i], g1[i]);
+            atomicAdd(&G.b1[m - 32], g1[31]);
+        } else if (m == 64) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) atomicAdd(&G.w3[j], g2[j]);
+            atomicAdd(&G.b3, g1[31]);
+        }
+    }
+    // the loss: lanes, then warps, then the CTA (NaN when a wait gave up)
+#pragma unroll
+    for (int k = 16; k > 0; k >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, k);
+    if (lane == 0 && warp < 4) atomicAdd(&s.loss, lsum);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(loss, s.fail ? __int_as_float(0x7fc00000) : s.loss);
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(s.tmem, 128);
+    }
+}
+
+// Logits of n feature rows, 128 rows per tile on the tensor cores (a NaN logit: a tensor-core step did not complete):
+// warpgroup g of CTA b takes tiles 2 b + g, 2 b + g + 2 gridDim.x, ...
 __global__ void __launch_bounds__(256) k_sensor_infer(const SensorW* __restrict__ wg, const float* __restrict__ X, long long n, float* __restrict__ logits) {
     __shared__ SensTc st;
     sens_tc_setup(st, wg);
+    const int g = threadIdx.x >> 7, t = threadIdx.x & 127;
     unsigned phase = 0;
     const long long ntile = (n + 127) / 128;
-    for (long long tt = blockIdx.x; tt < ntile; tt += gridDim.x) {
+    for (long long tt = 2LL * blockIdx.x + g; tt < ntile; tt += 2LL * gridDim.x) {
         const long long r0 = tt * 128;
-        for (int idx = threadIdx.x; idx < 128 * kSensF; idx += blockDim.x) {
-            const int r = idx / kSensF, col = idx % kSensF;
-            st.X[tc::cl_index(r, col)] = __float2bfloat16_rn(r0 + r < n ? X[(r0 + r) * kSensK + col] : 0.0f);
+        // row r, column group c: two float4 loads, one 16-byte store of 8 bf16 into the canonical tile
+        for (int idx = t; idx < 128 * 4; idx += 128) {
+            const int r = idx >> 2, c = idx & 3;
+            uint32_t pk[4] = {0u, 0u, 0u, 0u};
+            if (r0 + r < n && 8 * c < kSensF) {
+                const float4 a = *reinterpret_cast<const float4*>(X + (r0 + r) * kSensK + 8 * c);
+                const float4 b = *reinterpret_cast<const float4*>(X + (r0 + r) * kSensK + 8 * c + 4);
+                const float v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int j = 8 * c + 2 * k;
+                    pk[k] = pack_bf16(j < kSensF ? v[2 * k] : 0.0f, j + 1 < kSensF ? v[2 * k + 1] : 0.0f);
+                }
+            }
+            *reinterpret_cast<uint4*>(&st.X[g][tc::cl_index(r, 8 * c)]) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
         }
         tma::fence_proxy_async();
-        __syncthreads();
-        const float z = sens_tc_tile(st, phase);
-        __syncthreads();
-        const int r = threadIdx.x;
-        if (r < 128 && r0 + r < n) logits[r0 + r] = st.fail ? __int_as_float(0x7fc00000) : z;
+        const float z = sens_tc_tile(st, g, phase);
+        const int r = 32 * ((threadIdx.x >> 5) & 3) + (threadIdx.x & 31);
+        if (r0 + r < n) logits[r0 + r] = st.fail ? __int_as_float(0x7fc00000) : z;
     }
     sens_tc_release(st);
 }
@@ -481,8 +497,9 @@ __global__ void __launch_bounds__(256) k_sensor_flags_t(Mesh m, Bc bc, Eos<doubl
     // the planes of the primitive variables PS floats apart, PS = 7 (mod 32): the lanes that read the five quantities of
     // one stencil position read five different banks (a plane stride that is a multiple of 32 puts them on one)
     constexpr int PS = BOX + ((7 - BOX % 32) + 32) % 32;
-    __shared__ float P[NV * PS];
-    __shared__ SensTc st;
+    extern __shared__ __align__(1024) unsigned char fsm[];   // SensTc, then the primitive planes P (flags_smem bytes)
+    SensTc& st = *reinterpret_cast<SensTc*>(fsm);
+    float* P = reinterpret_cast<float*>(fsm + sizeof(SensTc));
     sens_tc_setup(st, wg);
     const int b = blockIdx.x;
     const int o0 = (b % nb0) * BX, o1 = ((b / nb0) % nb1) * BY, o2 = DIM == 3 ? (b / (nb0 * nb1)) * BZ : 0;
@@ -493,13 +510,14 @@ __global__ void __launch_bounds__(256) k_sensor_flags_t(Mesh m, Bc bc, Eos<doubl
         for (int q = 0; q < NV; ++q) P[q * PS + e] = (float)wv[q];
     }
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = threadIdx.x >> 7, q = (threadIdx.x >> 5) & 3, lane = threadIdx.x & 31;
     const float gam = (float)eos.gamma, pinf = eos.type == kIdeal ? 0.0f : (float)eos.p_inf;
     unsigned phase = 0;
-    for (int t0 = 0; t0 < ROWS; t0 += 128) {
-        // features of the tile's rows: warp w takes rows 16 w .. 16 w + 15, one lane per (row, quantity)
-        for (int it = lane; it < 16 * kSensQ; it += 32) {
-            const int row = 16 * warp + it / kSensQ, sq = it % kSensQ, r = t0 + row;
+    // warpgroup g takes the 128-row tiles 2 k + g of the block's ROWS (cell, axis) rows
+    for (int t0 = 128 * g; t0 < ROWS; t0 += 256) {
+        // features of the tile's rows: warp q of the group rows 32 q .. 32 q + 31, one lane per (row, quantity)
+        for (int it = lane; it < 32 * kSensQ; it += 32) {
+            const int row = 32 * q + it / kSensQ, sq = it % kSensQ, r = t0 + row;
             float f[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
             if (r < ROWS) {
                 const int c = r / DIM, axis = r % DIM;
@@ -514,20 +532,16 @@ __global__ void __launch_bounds__(256) k_sensor_flags_t(Mesh m, Bc bc, Eos<doubl
                 }
             }
 #pragma unroll
-            for (int k = 0; k < 5; ++k) st.X[tc::cl_index(row, 5 * sq + k)] = __float2bfloat16_rn(f[k]);
+            for (int k = 0; k < 5; ++k) st.X[g][tc::cl_index(row, 5 * sq + k)] = __float2bfloat16_rn(f[k]);
         }
         tma::fence_proxy_async();
-        __syncthreads();
-        const float z = sens_tc_tile(st, phase);
-        __syncthreads();
-        if (warp < 4) {
-            const int r = t0 + 32 * warp + lane;
-            if (r < ROWS) {
-                const int c = r / DIM, axis = r % DIM;
-                const int i = o0 + c % BX, j = o1 + (c / BX) % BY, k = DIM == 3 ? o2 + c / (BX * BY) : 0;
-                // a tensor-core step that did not complete leaves the row WENO5-Z
-                if (i < m.nx && j < m.ny && k < m.nz) flags[axis * m.plane + ((long long)k * m.ny + j) * m.nx + i] = (!st.fail && z < theta) ? 0 : 1;
-            }
+        const float z = sens_tc_tile(st, g, phase);
+        const int r = t0 + 32 * q + lane;
+        if (r < ROWS) {
+            const int c = r / DIM, axis = r % DIM;
+            const int i = o0 + c % BX, j = o1 + (c / BX) % BY, k = DIM == 3 ? o2 + c / (BX * BY) : 0;
+            // a tensor-core step that did not complete leaves the row WENO5-Z
+            if (i < m.nx && j < m.ny && k < m.nz) flags[axis * m.plane + ((long long)k * m.ny + j) * m.nx + i] = (!st.fail && z < theta) ? 0 : 1;
         }
     }
     if (st.fail && threadIdx.x == 0 && err) atomicExch(err, 6);
@@ -632,6 +646,23 @@ int grid_for(long long rows) {
     return (int)(b < 1 ? 1 : (b > 148 * 4 ? 148 * 4 : b));
 }
 
+// the dynamic shared memory of k_sensor_flags_t<DIM, NV, BX, BY, BZ>: the network's tiles, then NV primitive planes of the
+// block and its 2-cell halo (plane stride 7 mod 32)
+template <int DIM, int NV, int BX, int BY, int BZ> constexpr int flags_smem() {
+    constexpr int BOX = (BX + 4) * (BY + 4) * (DIM == 3 ? BZ + 4 : 1);
+    return (int)sizeof(SensTc) + 4 * NV * (BOX + ((7 - BOX % 32) + 32) % 32);
+}
+
+template <int DIM, int NV, int BX, int BY, int BZ>
+cudaError_t launch_flags(int blocks, cudaStream_t s, const Mesh& m, const Bc& bc, const Eos<double>& eos, const double* U, const SensorW* w, float theta,
+                         unsigned char* flags0, const Ctl* ctl, int every, int b0, int b1, int* err) {
+    constexpr int SM = flags_smem<DIM, NV, BX, BY, BZ>();
+    static const cudaError_t attr = cudaFuncSetAttribute(k_sensor_flags_t<DIM, NV, BX, BY, BZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
+    if (attr != cudaSuccess) return attr;
+    k_sensor_flags_t<DIM, NV, BX, BY, BZ><<<blocks, 256, SM, s>>>(m, bc, eos, U, w, theta, flags0, ctl, every, b0, b1, err);
+    return cudaGetLastError();
+}
+
 }   // namespace
 
 cudaError_t fvg::sensor_refresh(const Mesh& m, const Bc& bc, const Eos<double>& eos, int dim, const double* U, const void* weights, float theta,
@@ -643,10 +674,12 @@ cudaError_t fvg::sensor_refresh(const Mesh& m, const Bc& bc, const Eos<double>& 
     int* err = ctl ? const_cast<int*>(&ctl->status) : nullptr;
     if (dim == 3) {
         const int b0 = (m.nx + 7) / 8, b1 = (m.ny + 7) / 8, b2 = (m.nz + 3) / 4;
-        k_sensor_flags_t<3, 5, 8, 8, 4><<<b0 * b1 * b2, 256, 0, s>>>(m, bc, eos, U, w, theta, flags0, ctl, every, b0, b1, err);
+        const cudaError_t e = launch_flags<3, 5, 8, 8, 4>(b0 * b1 * b2, s, m, bc, eos, U, w, theta, flags0, ctl, every, b0, b1, err);
+        if (e != cudaSuccess) return e;
     } else {
         const int b0 = (m.nx + 31) / 32, b1 = (m.ny + 7) / 8;
-        k_sensor_flags_t<2, 4, 32, 8, 1><<<b0 * b1, 256, 0, s>>>(m, bc, eos, U, w, theta, flags0, ctl, every, b0, b1, err);
+        const cudaError_t e = launch_flags<2, 4, 32, 8, 1>(b0 * b1, s, m, bc, eos, U, w, theta, flags0, ctl, every, b0, b1, err);
+        if (e != cudaSuccess) return e;
     }
     const long long nr = (long long)dim * m.nz * m.ny * tiles[0];
     const int rb = (int)((nr + 255) / 256 < 148 * 16 ? (nr + 255) / 256 : 148 * 16);
@@ -707,7 +740,9 @@ int fvg_sensor_extract(fvg_run* run, int mode, int keep_div, unsigned seed, floa
 int fvg_sensor_grad(const void* weights, const float* X, const float* y, long long n, float wpos, float* grad, float* loss, void* stream) {
     if (!weights || !X || !y || !grad || !loss || n < 1) return serr(FVG_ERR_ARGUMENT, "null argument or no samples");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    k_sensor_grad<<<grid_for(n), 256, 0, s>>>(static_cast<const SensorW*>(weights), X, y, n, wpos, 1.0f / (float)n, grad, loss);
+    static const cudaError_t attr = cudaFuncSetAttribute(k_sensor_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, kGradSmem);
+    SK(attr);
+    k_sensor_grad<<<grid_for(n), 256, kGradSmem, s>>>(static_cast<const SensorW*>(weights), X, y, n, wpos, 1.0f / (float)n, grad, loss);
     SK(cudaGetLastError());
     return FVG_OK;
 }

@@ -6,8 +6,8 @@
 // four differences v_k - v0 over the largest of them) and its amplitude (log2(1 + 1e4 M / s) / 4, M that largest
 // difference, s the quantity's physical scale at the cell: rho for the density, the sound speed for the velocities,
 // p + p_inf for the pressure). 25 features, padded with zeros to the 32 of two tensor-core k-steps.
-// Network: 32 -> 32 (ReLU) -> 32 (ReLU) -> 1 logit; weights and hidden activations in bfloat16, sums in float32
-// (mma.sync m16n8k16 bf16 with f32 accumulators, one warp per 16 cells). The cell is smooth (linear reconstruction)
+// Network: 32 -> 32 (ReLU) -> 32 (ReLU) -> 1 logit; weights and hidden activations in bfloat16, sums in float32 (the
+// dense layers as tcgen05 MMAs of 128 rows with f32 accumulators in tensor memory: sensor.cu, tc.cuh). The cell is smooth (linear reconstruction)
 // when the logit is below a threshold chosen for a low miss rate; otherwise, and for every cell the network is not sure
 // about, WENO5-Z stays.
 // Label (what the network learns): the largest gap |WENO5-Z - linear| between the cell's two WENO5-Z face values (the
@@ -94,96 +94,11 @@ __device__ __forceinline__ double weno5z_face_gap(double c0, double c1, double c
     return fabs(weno5z(c0, c1, c2, c3, c4, eps_rel) - lin);
 }
 
-// ------------------------------------------------------------------------------------------------ tensor-core MLP
+// ------------------------------------------------------------------------------------------------ bf16 helpers
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
     return *reinterpret_cast<uint32_t*>(&v);
 }
-__device__ __forceinline__ uint32_t pack_bf16_raw(__nv_bfloat16 lo, __nv_bfloat16 hi) {
-    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
-}
 __device__ __forceinline__ float round_bf16(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
-
-// D += A B with A 16x16 (row), B 16x8 (col), bf16 operands, f32 accumulators (PTX mma.sync.m16n8k16).
-__device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
-    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-// The A fragments (two k-steps) of 16 rows x 32 bf16 stored row-major with a row stride of `ld` elements.
-__device__ __forceinline__ void load_a_frags(const __nv_bfloat16* X, int ld, uint32_t (&a)[2][4]) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int s = 0; s < 2; ++s) {
-        const int k = 16 * s + 2 * t;
-        a[s][0] = *reinterpret_cast<const uint32_t*>(X + g * ld + k);
-        a[s][1] = *reinterpret_cast<const uint32_t*>(X + (g + 8) * ld + k);
-        a[s][2] = *reinterpret_cast<const uint32_t*>(X + g * ld + k + 8);
-        a[s][3] = *reinterpret_cast<const uint32_t*>(X + (g + 8) * ld + k + 8);
-    }
-}
-
-// One dense layer on the tensor cores: acc[nt] (n-tile nt = outputs 8 nt .. 8 nt + 7) = A W^T, W [32 out][32 in] bf16.
-__device__ __forceinline__ void dense32(const uint32_t (&a)[2][4], const __nv_bfloat16* W, float (&acc)[4][4]) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int nt = 0; nt < 4; ++nt) {
-        acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.0f;
-#pragma unroll
-        for (int s = 0; s < 2; ++s) {
-            const uint32_t* wp = reinterpret_cast<const uint32_t*>(W + (8 * nt + g) * 32 + 16 * s + 2 * t);
-            const uint32_t b[2] = {wp[0], wp[4]};   // k = 16 s + 2 t (+1) and + 8
-            mma16816(acc[nt], a[s], b);
-        }
-    }
-}
-
-// Bias, ReLU and bfloat16 rounding of a layer's accumulators, repacked as the next layer's A fragments (the C fragment
-// of n-tiles 2s, 2s+1 is the A fragment of k-step s); acc keeps the rounded activations.
-__device__ __forceinline__ void relu_to_a(float (&acc)[4][4], const float* bias, uint32_t (&a)[2][4]) {
-    const int t = (threadIdx.x & 31) & 3;
-#pragma unroll
-    for (int nt = 0; nt < 4; ++nt) {
-        const float b0 = bias[8 * nt + 2 * t], b1v = bias[8 * nt + 2 * t + 1];
-        acc[nt][0] = round_bf16(fmaxf(acc[nt][0] + b0, 0.0f));
-        acc[nt][1] = round_bf16(fmaxf(acc[nt][1] + b1v, 0.0f));
-        acc[nt][2] = round_bf16(fmaxf(acc[nt][2] + b0, 0.0f));
-        acc[nt][3] = round_bf16(fmaxf(acc[nt][3] + b1v, 0.0f));
-    }
-#pragma unroll
-    for (int s = 0; s < 2; ++s) {
-        a[s][0] = pack_bf16(acc[2 * s][0], acc[2 * s][1]);
-        a[s][1] = pack_bf16(acc[2 * s][2], acc[2 * s][3]);
-        a[s][2] = pack_bf16(acc[2 * s + 1][0], acc[2 * s + 1][1]);
-        a[s][3] = pack_bf16(acc[2 * s + 1][2], acc[2 * s + 1][3]);
-    }
-}
-
-// Logits of the 16 rows of a warp's feature tile X (bf16, 16 x 32, row stride ld): lo = row g, hi = row g + 8 (g = lane / 4),
-// the same in the four lanes of a group.
-__device__ __forceinline__ void sensor_logits(const SensorW& w, const __nv_bfloat16* X, int ld, float& lo, float& hi) {
-    uint32_t a[2][4];
-    float acc[4][4];
-    load_a_frags(X, ld, a);
-    dense32(a, w.W1, acc);
-    relu_to_a(acc, w.b1, a);
-    dense32(a, w.W2, acc);
-    relu_to_a(acc, w.b2, a);
-    const int t = (threadIdx.x & 31) & 3;
-    float s0 = 0.0f, s1 = 0.0f;
-#pragma unroll
-    for (int nt = 0; nt < 4; ++nt) {
-        const float w0 = w.w3[8 * nt + 2 * t], w1 = w.w3[8 * nt + 2 * t + 1];
-        s0 += acc[nt][0] * w0 + acc[nt][1] * w1;
-        s1 += acc[nt][2] * w0 + acc[nt][3] * w1;
-    }
-    s0 += __shfl_xor_sync(0xffffffffu, s0, 1);
-    s0 += __shfl_xor_sync(0xffffffffu, s0, 2);
-    s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
-    s1 += __shfl_xor_sync(0xffffffffu, s1, 2);
-    lo = s0 + w.b3;
-    hi = s1 + w.b3;
-}
 
 }   // namespace fvg

@@ -27,9 +27,18 @@ __device__ __forceinline__ uint64_t smem_desc(const void* base, int s) {
     return addr | (uint64_t(128 >> 4) << 16) | (uint64_t(512 >> 4) << 32) | (1ull << 46);
 }
 
-// instruction descriptor of kind::f16: f32 accumulator, bf16 A and B, both K-major, N columns, M rows
-template <int M, int N> __host__ __device__ constexpr uint32_t idesc_bf16() {
-    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+// a matrix descriptor with explicit byte offsets: start `base` + `off`, leading byte offset `lbo` (between the core
+// matrices adjacent along K for a K-major operand, along K too for an MN-major one), stride byte offset `sbo` (between
+// the core matrices adjacent along M or N); no swizzle
+__device__ __forceinline__ uint64_t smem_desc_at(const void* base, uint32_t off, uint32_t lbo, uint32_t sbo) {
+    const uint64_t addr = (uint64_t)((su32(base) + off) >> 4) & 0x3FFFull;
+    return addr | (uint64_t((lbo >> 4) & 0x3FFF) << 16) | (uint64_t((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// instruction descriptor of kind::f16: f32 accumulator, bf16 A and B, N columns, M rows; A and B K-major (MN_MAJOR
+// false) or both MN-major
+template <int M, int N, bool MN_MAJOR = false> __host__ __device__ constexpr uint32_t idesc_bf16() {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (MN_MAJOR ? (1u << 15) | (1u << 16) : 0u) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
 }
 
 // TMEM allocation of `cols` columns (a power of two >= 32) by one whole warp; the address lands in *slot (shared memory)
