@@ -44,7 +44,7 @@ struct fvg_cells {
     // the viscous terms (3-D): the neighbour table, the cell quantities and the viscous face fluxes
     bool visc = false;
     int* nbr = nullptr;
-    double *Q = nullptr, *Fv = nullptr;
+    double *Q = nullptr, *Fv = nullptr;   // Q: 13 planes in 3-D, 7 in 2-D
     double mu = 0.0, k_cond = 0.0, L = 0.0, inv_h2 = 0.0, h[3] = {0, 0, 0};
     unsigned long long* smax = nullptr;   // [3]: the bits of the largest face speed of each stage
     int* bad = nullptr;
@@ -328,10 +328,150 @@ __global__ void __launch_bounds__(kCellsNT) k_cells_vfaces(const CellVisc v) {
         cells_vface<2>(v, f, meta);
 }
 
+// ---- the viscous terms on a 2-D mesh (CellFluxEngine::cell_quantities / viscous_fluxes / viscous_speed for a quadtree,
+// CellFluxResidual.cpp:592-800): u, v, T and the four velocity derivatives per leaf, the x and y face fluxes. The diffusive
+// ghost of a 2-D side (BoundaryManager::viscous_ghost) is the 3-D rule with w = 0 (the same momentum rules on rho u and
+// rho v, and match_kinetic_energy with a zero w term).
+constexpr int kQ2 = 7;   // cell quantities per leaf on a 2-D mesh: u, v, T, du/dx, du/dy, dv/dx, dv/dy
+
+__device__ __forceinline__ St<double, 4> vghost2(const ViscArgs& va, int side, const St<double, 4>& c) {
+    St<double, 5> c5;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) c5[q] = c[q];
+    c5[4] = 0.0;
+    const St<double, 5> g5 = viscous_ghost_3d(va, side, c5);
+    St<double, 4> g;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) g[q] = g5[q];
+    return g;
+}
+
+__global__ void __launch_bounds__(kCellsNT) k_cells_vcells2(const CellVisc v) {
+    __shared__ double red[32];
+    const long long c = blockIdx.x * (long long)kCellsNT + threadIdx.x;
+    double s = 0.0;
+    if (c < v.nleaf) {
+        const St<double, 4> Ui = leaf_state<4>(v.U, v.lplane, c);
+        const St<double, 4> W = c2p(v.va.eos, Ui);
+        St<double, 4> nb[4];   // left, right, bottom, top (the diffusive ghost at a physical edge)
+#pragma unroll
+        for (int sd = 0; sd < 4; ++sd) {
+            const int code = v.nbr[sd * v.nleaf + c];
+            nb[sd] = code >= 0 ? leaf_state<4>(v.U, v.lplane, code) : vghost2(v.va, sd, Ui);
+        }
+        double gx[3], gy[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            gx[q] = (nb[1][q] - nb[0][q]) / (2.0 * v.h[0]);
+            gy[q] = (nb[3][q] - nb[2][q]) / (2.0 * v.h[1]);
+        }
+        const double rho = W[0], u = W[1], vv = W[2];
+        v.Q[0 * v.lplane + c] = u;
+        v.Q[1 * v.lplane + c] = vv;
+        v.Q[2 * v.lplane + c] = W[3] / rho;
+        v.Q[3 * v.lplane + c] = (gx[1] - u * gx[0]) / rho;
+        v.Q[4 * v.lplane + c] = (gy[1] - u * gy[0]) / rho;
+        v.Q[5 * v.lplane + c] = (gx[2] - vv * gx[0]) / rho;
+        v.Q[6 * v.lplane + c] = (gy[2] - vv * gy[0]) / rho;
+        const double nu_eff = vmax((4.0 / 3.0) * (v.mu / rho), (v.k_cond * (v.va.eos.gamma - 1.0)) / rho) + 1e-12;
+        const double sv = vmax(fabs(W[1]), fabs(W[2])) + sound_speed(v.va.eos, W[3], rho) + 2.0 * v.L * v.inv_h2 * nu_eff;
+        if (sv > s) s = sv;
+    }
+    const double bm = block_max<kCellsNT>(s, red);
+    if (threadIdx.x == 0 && bm > 0.0) atomicMax(v.smax, (unsigned long long)__double_as_longlong(bm));
+}
+
+__global__ void __launch_bounds__(kCellsNT) k_cells_vfaces2(const CellVisc v) {
+    const long long f = blockIdx.x * (long long)kCellsNT + threadIdx.x;
+    if (f >= v.nface) return;
+    const int meta = v.meta[f];
+    const int ax = meta & 3;
+    auto Q = [&](int k, long long c) { return v.Q[k * v.lplane + c]; };
+    double uL, vL, TL, uR, vR, TR, h, ca, cb;   // ca, cb: the cross derivatives of u and v along the other axis
+    if ((meta >> 8) & 1) {
+        const int side = (meta >> 4) & 7;
+        const bool ghost_left = !((meta >> 7) & 1);
+        const int c = v.code[(ghost_left ? 3 : 2) * v.fplane + f];
+        const St<double, 4> Uc = leaf_state<4>(v.U, v.lplane, c);
+        const St<double, 4> g = c2p(v.va.eos, vghost2(v.va, side, Uc));
+        const double gu = g[1], gv = g[2], gT = g[3] / g[0];
+        uL = ghost_left ? gu : Q(0, c);
+        vL = ghost_left ? gv : Q(1, c);
+        TL = ghost_left ? gT : Q(2, c);
+        uR = ghost_left ? Q(0, c) : gu;
+        vR = ghost_left ? Q(1, c) : gv;
+        TR = ghost_left ? Q(2, c) : gT;
+        h = v.h[ax];
+        if (v.bo2) {
+            // the tangential difference of the face values (ghost and cell average) of the two neighbours along the wall; the
+            // neighbour across a physical edge of the tangential side is the leaf's ghost on that side, its ghost the corner entry
+            const int tl = ax == 0 ? 2 : 0;
+            double fu[2], fv[2];
+#pragma unroll
+            for (int hi = 0; hi < 2; ++hi) {
+                const int si = tl + hi;
+                const int code = v.nbr[si * v.nleaf + c];
+                St<double, 4> in, gh;
+                if (code >= 0) {
+                    in = leaf_state<4>(v.U, v.lplane, code);
+                    gh = vghost2(v.va, side, in);
+                } else {
+                    in = vghost2(v.va, si, Uc);
+                    gh = ax == 0 ? vghost2(v.va, side, in) : vghost2(v.va, si, vghost2(v.va, side, Uc));
+                }
+                const St<double, 4> Wg = c2p(v.va.eos, gh), Wi = c2p(v.va.eos, in);
+                fu[hi] = 0.5 * (Wg[1] + Wi[1]);
+                fv[hi] = 0.5 * (Wg[2] + Wi[2]);
+            }
+            const double h2 = 2.0 * (ax == 0 ? v.h[1] : v.h[0]);
+            ca = (fu[1] - fu[0]) / h2;
+            cb = (fv[1] - fv[0]) / h2;
+        } else {
+            const double a = ax == 0 ? Q(4, c) : Q(3, c), b = ax == 0 ? Q(6, c) : Q(5, c);
+            ca = 0.5 * (a + a);
+            cb = 0.5 * (b + b);
+        }
+    } else {
+        const int L = v.code[2 * v.fplane + f], R = v.code[3 * v.fplane + f];
+        uL = Q(0, L);
+        vL = Q(1, L);
+        TL = Q(2, L);
+        uR = Q(0, R);
+        vR = Q(1, R);
+        TR = Q(2, R);
+        h = 0.5 * (v.h[ax] + v.h[ax]);
+        ca = ax == 0 ? 0.5 * (Q(4, L) + Q(4, R)) : 0.5 * (Q(3, L) + Q(3, R));
+        cb = ax == 0 ? 0.5 * (Q(6, L) + Q(6, R)) : 0.5 * (Q(5, L) + Q(5, R));
+    }
+    const double u_f = 0.5 * (uL + uR), v_f = 0.5 * (vL + vR);
+    const double du_n = (uR - uL) / h, dv_n = (vR - vL) / h, dT_n = (TR - TL) / h;
+    const double len = v.length[ax];
+    double F1, F2, F3;
+    if (ax == 0) {
+        const double tau_xx = v.mu * ((4.0 / 3.0) * du_n - (2.0 / 3.0) * cb);
+        const double tau_xy = v.mu * (ca + dv_n);
+        const double q_x = -v.k_cond * dT_n;
+        F1 = tau_xx * len;
+        F2 = tau_xy * len;
+        F3 = (u_f * tau_xx + v_f * tau_xy - q_x) * len;
+    } else {
+        const double tau_yy = v.mu * ((4.0 / 3.0) * dv_n - (2.0 / 3.0) * ca);
+        const double tau_yx = v.mu * (du_n + cb);
+        const double q_y = -v.k_cond * dT_n;
+        F1 = tau_yx * len;
+        F2 = tau_yy * len;
+        F3 = (u_f * tau_yx + v_f * tau_yy - q_y) * len;
+    }
+    v.Fv[0 * v.fplane + f] = F1;
+    v.Fv[1 * v.fplane + f] = F2;
+    v.Fv[2 * v.fplane + f] = F3;
+}
+
 struct GatherArgs {
     long long nleaf, lplane, fplane;
     const double* F;
     const double* Fv;       // [4][fplane] viscous fluxes times the face area (null: inviscid)
+    Bc bc;                  // the body force (bc.grav, when bc.grav_on)
     const int* side_face;   // [ns * nleaf]: the face on each side of each leaf (one at level 0)
     double length[3], inv_vol;
     int mode;
@@ -349,6 +489,7 @@ template <int DIM, int NV> __global__ void __launch_bounds__(kCellsNT) k_cells_g
     int fs[NS];
 #pragma unroll
     for (int s = 0; s < NS; ++s) fs[s] = g.side_face[NS * c + s];
+    St<double, NV> r;
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
         double G[NS];
@@ -357,24 +498,29 @@ template <int DIM, int NV> __global__ void __launch_bounds__(kCellsNT) k_cells_g
         double acc = 0.0 - (G[1] - G[0]);
         acc = acc - (G[3] - G[2]);
         if constexpr (DIM == 3) acc = acc - (G[5] - G[4]);
-        double r = acc * g.inv_vol;
-        if (g.Fv) {   // NavierStokes::viscous_residual_3d accumulated: r += (((0 + (H1 - H0)) + (H3 - H2)) + (H5 - H4)) / volume
+        r[q] = acc * g.inv_vol;
+        if (g.Fv) {   // the viscous terms accumulated: r += (((0 + (H1 - H0)) + (H3 - H2)) + (H5 - H4)) / volume
             double H[NS];
 #pragma unroll
             for (int s = 0; s < NS; ++s) H[s] = q == 0 ? 0.0 : g.Fv[(q - 1) * g.fplane + fs[s]];
             double vac = 0.0 + (H[1] - H[0]);
             vac = vac + (H[3] - H[2]);
             if constexpr (DIM == 3) vac = vac + (H[5] - H[4]);
-            r += vac * g.inv_vol;
+            r[q] += vac * g.inv_vol;
         }
+    }
+    // the body force after the viscous terms (CellFluxEngine::gather, CellFluxResidual.cpp:1015-1024)
+    if (g.bc.grav_on) add_body_force<NV>(g.bc, leaf_state<NV>(g.U, g.lplane, c), r);
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
         const long long e = q * g.lplane + c;
         double o;
         if (g.mode == kStoreR)
-            o = r;
+            o = r[q];
         else if (g.mode == kAxpy)
-            o = g.U[e] + g.dt * r;
+            o = g.U[e] + g.dt * r[q];
         else
-            o = g.ca * g.U0[e] + g.cb * (g.U[e] + g.dt * r);
+            o = g.ca * g.U0[e] + g.cb * (g.U[e] + g.dt * r[q]);
         g.out[e] = o;
     }
 }
@@ -594,9 +740,16 @@ int residual_pass(fvg_cells* e, const double* Uin, int slot, int mode, double ca
         v.inv_h2 = e->inv_h2;
         v.bo2 = e->cfg.boundary_order == 2;
         v.smax = e->smax + slot;
-        k_cells_vcells<<<(int)((n + kCellsNT - 1) / kCellsNT), kCellsNT, 0, e->stream>>>(v);
-        CKC(cudaGetLastError());
-        k_cells_vfaces<<<(int)((e->nface + kCellsNT - 1) / kCellsNT), kCellsNT, 0, e->stream>>>(v);
+        const int bl = (int)((n + kCellsNT - 1) / kCellsNT), bf = (int)((e->nface + kCellsNT - 1) / kCellsNT);
+        if (e->dim == 3) {
+            k_cells_vcells<<<bl, kCellsNT, 0, e->stream>>>(v);
+            CKC(cudaGetLastError());
+            k_cells_vfaces<<<bf, kCellsNT, 0, e->stream>>>(v);
+        } else {
+            k_cells_vcells2<<<bl, kCellsNT, 0, e->stream>>>(v);
+            CKC(cudaGetLastError());
+            k_cells_vfaces2<<<bf, kCellsNT, 0, e->stream>>>(v);
+        }
         CKC(cudaGetLastError());
     }
     GatherArgs g{};
@@ -605,6 +758,7 @@ int residual_pass(fvg_cells* e, const double* Uin, int slot, int mode, double ca
     g.fplane = e->fplane;
     g.F = e->F;
     g.Fv = e->visc ? e->Fv : nullptr;
+    g.bc = e->bc;
     g.side_face = e->side_face;
     for (int k = 0; k < 3; ++k) g.length[k] = e->length[k];
     g.inv_vol = e->inv_vol;
@@ -651,9 +805,7 @@ int fvg_cells_create(const fvg_config* cfg, int nleaf, const int* level, const i
     const fvg_config& c = *cfg;
     std::string why = config_error(c);
     const char* no = nullptr;
-    if (c.use_viscous && c.nz <= 1) no = "the viscous terms on a 2-D mesh";
-    else if (c.use_ibm) no = "an immersed body";
-    else if (c.use_bodyforce) no = "the body force";
+    if (c.use_ibm) no = "an immersed body";
     else if (config_has_expressions(c)) no = "source terms and time-dependent boundary values";
     else if (c.positivity_fallback) no = "positivity_fallback";
     else if (c.flux_quadrature == 1) no = "flux_quadrature = fourth";
@@ -701,8 +853,17 @@ int fvg_cells_create(const fvg_config* cfg, int nleaf, const int* level, const i
     e->h[2] = dz;
     e->mu = c.mu;
     e->k_cond = c.mu * c.gamma / (c.pr * (c.gamma - 1.0));                          // TransportLaw (Core.hpp:194-197)
-    e->L = 2.0 / (1.0 / dx + 1.0 / dy + 1.0 / dz);                                  // step_length_3d
-    e->inv_h2 = 1.0 / (dx * dx) + 1.0 / (dy * dy) + 1.0 / (dz * dz);                // inv_h2_3d
+    if (e->dim == 3) {
+        e->L = 2.0 / (1.0 / dx + 1.0 / dy + 1.0 / dz);                              // step_length_3d
+        e->inv_h2 = 1.0 / (dx * dx) + 1.0 / (dy * dy) + 1.0 / (dz * dz);            // inv_h2_3d
+    } else {
+        e->L = vmin(dx, dy);                                                         // step_length_2d
+        e->inv_h2 = 1.0 / (dx * dx) + 1.0 / (dy * dy);                              // inv_h2_2d
+    }
+    e->bc.grav_on = c.use_bodyforce ? 1 : 0;   // ConstantBodyForce (gz only on a 3-D mesh)
+    e->bc.grav[0] = c.use_bodyforce ? c.gx : 0.0;
+    e->bc.grav[1] = c.use_bodyforce ? c.gy : 0.0;
+    e->bc.grav[2] = c.use_bodyforce && e->dim == 3 ? c.gz : 0.0;
     if (e->dim == 3) {
         e->length[0] = dy * dz;
         e->length[1] = dx * dz;
@@ -730,7 +891,7 @@ int fvg_cells_create(const fvg_config* cfg, int nleaf, const int* level, const i
         (err = cudaMalloc(&e->smax, sizeof(unsigned long long) * 3)) != cudaSuccess || (err = cudaMalloc(&e->bad, sizeof(int))) != cudaSuccess)
         return bail("cudaMalloc", err);
     if (e->visc) {
-        if ((err = cudaMalloc(&e->nbr, sizeof(int) * t.nbr.size())) != cudaSuccess || (err = cudaMalloc(&e->Q, sizeof(double) * kQ * e->lplane)) != cudaSuccess ||
+        if ((err = cudaMalloc(&e->nbr, sizeof(int) * t.nbr.size())) != cudaSuccess || (err = cudaMalloc(&e->Q, sizeof(double) * (e->dim == 3 ? kQ : kQ2) * e->lplane)) != cudaSuccess ||
             (err = cudaMalloc(&e->Fv, sizeof(double) * 4 * e->fplane)) != cudaSuccess)
             return bail("cudaMalloc", err);
         if ((err = cudaMemcpy(e->nbr, t.nbr.data(), sizeof(int) * t.nbr.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return bail("cudaMemcpy", err);

@@ -2432,7 +2432,8 @@ static int run_steps(fvg_run* run, double t_end, int max_steps, int use_graph, i
         const int cur0 = run->cur;
         int chunk = 4, before = 0;
         while (true) {
-            for (int k = 0; k < chunk; ++k) {
+            const int n = max_steps > 0 ? std::max(1, std::min(chunk, max_steps - before)) : chunk;
+            for (int k = 0; k < n; ++k) {
                 run->t_stage.step_start.push_back(run->t_stage.used);
                 run->t_visc.step_start.push_back(run->t_visc.used);
                 cudaError_t e = enqueue_step(run);
@@ -2468,11 +2469,16 @@ static int run_steps(fvg_run* run, double t_end, int max_steps, int use_graph, i
             CK(cudaGraphInstantiate(&graph, g, 0));
             cudaGraphDestroy(g);
         }
-        int chunk = 4;
+        // graphs in growing chunks between two reads of the clock, never more than a step limit still needs (the steps
+        // past it would only be gated off on the device, but their launches cost time)
+        const int per_graph = run->sens ? run->sens_every : 2;
+        int chunk = 4, ran = 0;
         while (true) {
-            for (int k = 0; k < chunk; ++k) CK(cudaGraphLaunch(graph, run->stream));
+            const int n = max_steps > 0 ? std::max(1, std::min(chunk, (max_steps - ran + per_graph - 1) / per_graph)) : chunk;
+            for (int k = 0; k < n; ++k) CK(cudaGraphLaunch(graph, run->stream));
             if ((rc = read_ctl(run, &h))) return rc;
             if (!h.active) break;
+            ran = h.steps;
             if (chunk < 64) chunk *= 2;
         }
         done = h.steps;

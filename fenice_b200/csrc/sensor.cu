@@ -132,15 +132,16 @@ __global__ void k_sensor_adam(float* P, float* m, float* v, float* grad, int ste
 
 // ------------------------------------------------------------------------------------------------ the network on tcgen05
 // A CTA of 256 threads evaluates the network 128 rows at a time on the fifth-generation tensor cores, as two independent
-// warpgroups (warps 0-3 and 4-7) that take alternate tiles: each has its own feature tile X (128 x 32 bf16) and hidden
-// tile H in shared memory in the MMA's canonical layout (tc.cuh), its own 32 TMEM columns for the layer's 128 x 32 f32
+// warpgroups (warps 0-3 and 4-7) that take alternate tiles: each has its own tile X (128 x 32 bf16: the features, then the
+// first layer's activations, which overwrite them once the first layer has read them) in shared memory in the MMA's
+// canonical layout (tc.cuh), its own 32 TMEM columns for the layer's 128 x 32 f32
 // accumulator, its own completion barrier and a named barrier for its 128 threads. The first thread of the group issues
 // the two k-steps of a layer and commits them; the group's warps read the accumulator rows back (warp w its TMEM lane
-// quarter w % 4: rows 32 (w % 4) .. + 31), add the bias, apply ReLU, round to bf16 and write H for the second layer, or,
+// quarter w % 4: rows 32 (w % 4) .. + 31), add the bias, apply ReLU, round to bf16 and write X for the second layer, or,
 // after the second layer, take the dot product with w3 in registers. The two groups' tiles interleave on the tensor core.
 struct __align__(128) SensTc {
-    __nv_bfloat16 X[2][128 * kSensK];   // canonical, one per warpgroup
-    __nv_bfloat16 H[2][128 * kSensH];   // canonical: the first layer's activations
+    // canonical, one per warpgroup: the features, then (once the first layer has read them) the first layer's activations
+    __nv_bfloat16 X[2][128 * kSensK];
     __nv_bfloat16 W1[kSensH * kSensK];
     __nv_bfloat16 W2[kSensH * kSensH];
     float b1[kSensH], b2[kSensH], w3[kSensH];
@@ -155,8 +156,7 @@ __device__ __forceinline__ void wg_sync(int g) {   // the 128 threads of warpgro
     asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory");
 }
 
-// the weights into s (all threads), the zero padding of both X tiles' columns kSensF .. 31, the barriers and 64 TMEM
-// columns (warp 0); ends with a block barrier
+// the weights into s (all threads), the barriers and 64 TMEM columns (warp 0); ends with a block barrier
 __device__ __forceinline__ void sens_tc_setup(SensTc& s, const SensorW* __restrict__ wg) {
     for (int i = threadIdx.x; i < kSensH * kSensK; i += blockDim.x) {
         s.W1[tc::cl_index(i >> 5, i & 31)] = wg->W1[i];
@@ -167,8 +167,6 @@ __device__ __forceinline__ void sens_tc_setup(SensTc& s, const SensorW* __restri
         s.b2[i] = wg->b2[i];
         s.w3[i] = wg->w3[i];
     }
-    constexpr int PAD = kSensK - kSensF;
-    for (int i = threadIdx.x; i < 2 * 128 * PAD; i += blockDim.x) s.X[i / (128 * PAD)][tc::cl_index((i / PAD) % 128, kSensF + i % PAD)] = __float2bfloat16_rn(0.0f);
     if (threadIdx.x == 0) {
         s.b3 = wg->b3;
         s.fail = 0;
@@ -232,15 +230,15 @@ __device__ __forceinline__ float sens_tc_tile(SensTc& s, int g, unsigned& phase)
             const int j = 8 * c + 2 * k;
             pk[k] = pack_bf16(fmaxf(d[j] + s.b1[j], 0.0f), fmaxf(d[j + 1] + s.b1[j + 1], 0.0f));
         }
-        *reinterpret_cast<uint4*>(&s.H[g][tc::cl_index(r, 8 * c)]) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        *reinterpret_cast<uint4*>(&s.X[g][tc::cl_index(r, 8 * c)]) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
     }
     tma::fence_proxy_async();
     tc::fence_before_sync();
     wg_sync(g);
     tc::fence_after_sync();
     if (issuer) {
-        tc::mma_bf16(tcol, tc::smem_desc(s.H[g], 0), tc::smem_desc(s.W2, 0), ID, false);
-        tc::mma_bf16(tcol, tc::smem_desc(s.H[g], 1), tc::smem_desc(s.W2, 1), ID, true);
+        tc::mma_bf16(tcol, tc::smem_desc(s.X[g], 0), tc::smem_desc(s.W2, 0), ID, false);
+        tc::mma_bf16(tcol, tc::smem_desc(s.X[g], 1), tc::smem_desc(s.W2, 1), ID, true);
         tc::commit(&s.bar[g]);
     }
     sens_tc_wait(s, g, phase);
@@ -534,6 +532,8 @@ __global__ void __launch_bounds__(256) k_sensor_flags_t(Mesh m, Bc bc, Eos<doubl
 #pragma unroll
             for (int k = 0; k < 5; ++k) st.X[g][tc::cl_index(row, 5 * sq + k)] = __float2bfloat16_rn(f[k]);
         }
+        // the padding inputs (the previous tile's hidden values sit there)
+        for (int k = kSensF; k < kSensK; ++k) st.X[g][tc::cl_index(threadIdx.x & 127, k)] = __float2bfloat16_rn(0.0f);
         tma::fence_proxy_async();
         const float z = sens_tc_tile(st, g, phase);
         const int r = t0 + 32 * q + lane;

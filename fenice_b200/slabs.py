@@ -115,40 +115,61 @@ class Part(Run):
 
 
 class LocalExchange:
-    """The communication of all parts of a decomposition held by this process: device copies between their buffers, each
-    communication point bracketed by synchronisations of the parts' streams (ordering on the host)."""
+    """The communication of all parts of a decomposition held by this process, ordered on the parts' CUDA streams with
+    events (no host synchronisation): a part's receive buffers are filled by copies on its own stream once the sending
+    part's stream has packed them, and a sender's later work (its next pack) waits for those copies; the all-reduce runs
+    on the first part's stream once every part has written its values and every part waits for its result."""
 
     def __init__(self, parts):
-        self.parts = list(parts)
-
-    def _sync(self):
         import torch
 
-        for p in self.parts:
-            p.synchronize()
-        torch.cuda.synchronize()
+        self.parts = list(parts)
+        self.streams = [torch.cuda.ExternalStream(p.stream(), device=torch.device("cuda", p.device)) for p in self.parts]
+        self.ready = [torch.cuda.Event() for _ in self.parts]
+        self.copied = [torch.cuda.Event() for _ in self.parts]
+        self.reduced = torch.cuda.Event()
+
+    def _record_ready(self):
+        for s, ev in zip(self.streams, self.ready):
+            ev.record(s)
 
     def exchange(self):
         import torch
 
-        self._sync()
+        self._record_ready()
         n = len(self.parts)
         for i, p in enumerate(self.parts):
-            send_lo, send_hi = p.tensors()[0], p.tensors()[1]
-            if p.peer_lo:   # to the low neighbour's recv_hi
-                self.parts[(i - 1) % n].tensors()[3].copy_(send_lo)
-            if p.peer_hi:   # to the high neighbour's recv_lo
-                self.parts[(i + 1) % n].tensors()[2].copy_(send_hi)
-        torch.cuda.synchronize()
+            s = self.streams[i]
+            with torch.cuda.stream(s):
+                if p.peer_lo:   # the low neighbour's send_hi -> my recv_lo
+                    j = (i - 1) % n
+                    s.wait_event(self.ready[j])
+                    p.tensors()[2].copy_(self.parts[j].tensors()[1])
+                if p.peer_hi:   # the high neighbour's send_lo -> my recv_hi
+                    j = (i + 1) % n
+                    s.wait_event(self.ready[j])
+                    p.tensors()[3].copy_(self.parts[j].tensors()[0])
+            self.copied[i].record(s)
+        for i, p in enumerate(self.parts):   # the sender's send buffers are free again once its receivers have copied them
+            if p.peer_lo:
+                self.streams[i].wait_event(self.copied[(i - 1) % n])
+            if p.peer_hi:
+                self.streams[i].wait_event(self.copied[(i + 1) % n])
 
     def allreduce(self, count):
         import torch
 
-        self._sync()
-        red = torch.stack([p.tensors()[4][:count] for p in self.parts]).amax(dim=0)
-        for p in self.parts:
-            p.tensors()[4][:count].copy_(red)
-        torch.cuda.synchronize()
+        self._record_ready()
+        s0 = self.streams[0]
+        with torch.cuda.stream(s0):
+            for ev in self.ready:
+                s0.wait_event(ev)
+            red = torch.stack([p.tensors()[4][:count] for p in self.parts]).amax(dim=0)
+            for p in self.parts:
+                p.tensors()[4][:count].copy_(red)
+        self.reduced.record(s0)
+        for s in self.streams:
+            s.wait_event(self.reduced)
 
 
 class DistExchange:

@@ -359,9 +359,9 @@ int fvg_batch_get_timing(const fvg_batch* b, double* stage_ms, long long* stage_
  * lengths, the scheme, the boundary conditions; the periodic axes are the periodic sides). Built: every leaf of level 0
  * (they must tile the base mesh); first order, MUSCL (every limiter), WENO3-Z, WENO5-Z; HLLC and low-Mach HLLC; the
  * boundary types but the non-reflecting outlet and the mass-flow inlet, with boundary_order 1 or 2; Euler, SSP-RK2 and
- * SSP-RK3 steps. Refused (FVG_ERR_CONFIG, message in fvg_create_error()): leaves above level 0, the viscous terms, an
- * immersed body, the body force, sources and time-dependent boundary values, positivity_fallback, the fourth-order
- * quadrature, the mixed-precision form, MUSCL-Hancock. */
+ * SSP-RK3 steps; the viscous terms (2-D and 3-D) and the body force. Refused (FVG_ERR_CONFIG, message in
+ * fvg_create_error()): leaves above level 0, an immersed body, sources and time-dependent boundary values,
+ * positivity_fallback, the fourth-order quadrature, the mixed-precision form, MUSCL-Hancock. */
 typedef struct fvg_cells fvg_cells;
 int fvg_cells_create(const fvg_config* cfg, int nleaf, const int* level, const int* ci, const int* cj, const int* ck, fvg_cells** out);
 int fvg_cells_destroy(fvg_cells* e);

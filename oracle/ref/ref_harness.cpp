@@ -273,9 +273,11 @@ void* ref_cells_create(void* h, int max_level) {
             c->mesh = std::make_unique<fv::CellMesh>(u.Lx, u.Ly, u.nx, u.ny, max_level, per(0), per(1), u.x0, u.y0);
         c->mesh->U.assign(static_cast<size_t>(c->mesh->num_leaves()), fv::State{});
         c->eng = std::make_unique<fv::CellFluxEngine>(sim.fluid, sim.riemann, sim.muscl.get(), sim.boundaries);
-        if (sim.ns) {   // the viscous terms, as the reference's viscous level-0 tests set them (test_amr_octree_physics.cpp:16-20)
+        if (sim.ns || sim.body_force) {   // the viscous terms and the body force, as the reference's tests set them (physics_of,
+                                          // cpp/tests/test_amr_common.hpp:424-438)
             fv::CellPhysics ph;
             ph.ns = sim.ns.get();
+            ph.body = sim.body_force.get();
             c->eng->set_physics(ph);
         }
         c->eng->build(*c->mesh);

@@ -39,7 +39,6 @@ def test_refusals():
     out = ci.copy()
     out[0] = 9
     refused(P3, lv, out, cj, ck, "outside the base mesh")
-    refused(dict(P2, use_viscous=True, mu=0.01), *base_leaves(P2), "viscous terms on a 2-D mesh")
     for extra, what in ((dict(time_scheme="MUSCL-Hancock", reconstruction="muscl"), "MUSCL-Hancock"),
                         (dict(bc_xmax="non_reflecting"), "non-reflecting"), (dict(positivity_fallback=True), "positivity_fallback")):
         refused(dict(P3, **extra), lv, ci, cj, ck, what)

@@ -160,3 +160,29 @@ def test_viscous_level0_octree_matches_the_reference(bc, recon, order):
             assert eng.step(2e-3, k * 2e-3) == s_refs[k]
         assert bits_equal(eng.state(), rc.state())
         eng.close()
+
+
+VSETS2 = [("moving_wall", "no_slip", "wall", "moving_wall"), ("periodic", "periodic", "moving_wall", "no_slip"), ("wall", "outlet", "periodic", "periodic"),
+          ("no_slip", "vel_inlet", "moving_wall", "transmissive")]
+
+
+@pytest.mark.parametrize("bc", VSETS2, ids=["/".join(b) for b in VSETS2])
+@pytest.mark.parametrize("recon,order", VRECON, ids=[f"{r}_bo{o}" for r, o in VRECON])
+def test_viscous_level0_quadtree_matches_the_reference(bc, recon, order):
+    """The 2-D viscous terms (cell_quantities / viscous_fluxes of a quadtree): residual and speed bit for bit against the
+    reference's engine, then 4 SSP-RK3 steps against CellAdvance; mu small and large."""
+    for mu in (0.02, 0.6):
+        params = params_of(RIG, bc, recon, order, SCHEMES[2], use_viscous=True, mu=mu, pr=0.72)
+        compare(params, seed=70, max_levels=(0,))
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("recon,order", [("muscl", 2), ("weno5", 2), ("none", 1)])
+def test_body_force_level0_matches_the_reference(dim, recon, order):
+    """The body force (ConstantBodyForce on every axis, after the viscous terms in 3-D), bit for bit."""
+    rig = RIG3 if dim == 3 else RIG
+    bc = SETS3[0] if dim == 3 else SETS2[0]
+    extra = dict(use_bodyforce=True, gx=0.3, gy=-0.7, gz=0.2)
+    if dim == 3:
+        extra.update(use_viscous=True, mu=0.05, pr=0.72)
+    compare(params_of(rig, bc, recon, order, SCHEMES[2], **extra), seed=80, max_levels=(0,))
