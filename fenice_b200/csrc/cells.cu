@@ -20,6 +20,7 @@
 // leaves only the residual has the bits of the uniform solver's, as the reference's own tests check for its engine.
 #include "../../include/fenice_gpu.h"
 #include "host_common.h"
+#include "hancock.cuh"
 #include "stage.cuh"
 #include "viscous.cuh"
 
@@ -46,6 +47,7 @@ struct fvg_cells {
     int* nbr = nullptr;
     double *Q = nullptr, *Fv = nullptr;   // Q: 13 planes in 3-D, 7 in 2-D
     double mu = 0.0, k_cond = 0.0, L = 0.0, inv_h2 = 0.0, h[3] = {0, 0, 0};
+    double *PL = nullptr, *PR = nullptr;  // MUSCL-Hancock: the face states of the faces' two sides
     unsigned long long* smax = nullptr;   // [3]: the bits of the largest face speed of each stage
     int* bad = nullptr;
     std::string err;
@@ -76,7 +78,13 @@ struct CellArgs {
     const int* meta;           // [fplane]
     double* F;                 // [NV][fplane] face fluxes (per unit measure)
     unsigned long long* smax;  // the bits of the largest face speed
+    double *PL, *PR;           // MUSCL-Hancock: [NV][fplane] the face states of the face's left / right side
 };
+
+// what the face kernel does with a face's two states: solve the Riemann problem (a residual), keep them for the
+// MUSCL-Hancock predictor (CellFluxEngine::fluxes with collect_), or solve it on the predicted states PL / PR
+// (CellFluxEngine::predicted_fluxes, CellFluxResidual.cpp:358-392)
+constexpr int kFacesFlux = 0, kFacesCollect = 1, kFacesPredicted = 2;
 
 template <int NV> __device__ __forceinline__ St<double, NV> leaf_state(const double* __restrict__ U, long long lplane, long long c) {
     St<double, NV> s;
@@ -102,7 +110,7 @@ template <int NV> __device__ __forceinline__ double entry(const CellArgs& a, int
     return c2p(a.eos, Ug)[q];
 }
 
-template <int NV, int RECON, int RIEMANN>
+template <int NV, int RECON, int RIEMANN, int MODE = kFacesFlux>
 __global__ void __launch_bounds__(kCellsNT) k_cells_faces(const CellArgs a) {
     __shared__ double red[32];
     const long long f = blockIdx.x * (long long)kCellsNT + threadIdx.x;
@@ -111,7 +119,10 @@ __global__ void __launch_bounds__(kCellsNT) k_cells_faces(const CellArgs a) {
         const int meta = a.meta[f];
         const int axis = meta & 3, kind = (meta >> 2) & 3;
         St<double, NV> UL, UR, F;
-        if (kind == kFaceBnd) {
+        if (MODE == kFacesPredicted) {
+            UL = leaf_state<NV>(a.PL, a.fplane, f);
+            UR = leaf_state<NV>(a.PR, a.fplane, f);
+        } else if (kind == kFaceBnd) {
             const int side = (meta >> 4) & 7;
             const bool ghost_right = (meta >> 7) & 1;
             const St<double, NV> Ui = leaf_state<NV>(a.U, a.lplane, a.code[(ghost_right ? 2 : 3) * a.fplane + f]);
@@ -149,14 +160,97 @@ __global__ void __launch_bounds__(kCellsNT) k_cells_faces(const CellArgs a) {
             UL = p2c(a.eos, wl);
             UR = p2c(a.eos, wr);
         }
-        const double sf = face_flux<RIEMANN>(a.eos, a.shock_blend, UL, UR, axis, F);
-        if (sf > s) s = sf;
+        if constexpr (MODE == kFacesCollect) {
 #pragma unroll
-        for (int q = 0; q < NV; ++q) a.F[q * a.fplane + f] = F[q];
+            for (int q = 0; q < NV; ++q) {
+                a.PL[q * a.fplane + f] = UL[q];
+                a.PR[q * a.fplane + f] = UR[q];
+            }
+        } else {
+            const double sf = face_flux<RIEMANN>(a.eos, a.shock_blend, UL, UR, axis, F);
+            if (sf > s) s = sf;
+#pragma unroll
+            for (int q = 0; q < NV; ++q) a.F[q * a.fplane + f] = F[q];
+        }
     }
-    const double bm = block_max<kCellsNT>(s, red);
-    // a non-negative double orders like its bits (a NaN speed never enters: the comparisons above drop it)
-    if (threadIdx.x == 0 && bm > 0.0) atomicMax(a.smax, (unsigned long long)__double_as_longlong(bm));
+    if constexpr (MODE != kFacesCollect) {
+        const double bm = block_max<kCellsNT>(s, red);
+        // a non-negative double orders like its bits (a NaN speed never enters: the comparisons above drop it)
+        if (threadIdx.x == 0 && bm > 0.0) atomicMax(a.smax, (unsigned long long)__double_as_longlong(bm));
+    }
+}
+
+// MUSCL-Hancock's predictor of every leaf (CellFluxEngine::predict_cells, CellFluxResidual.cpp:424-470, with
+// MusclReconstruction::hancock_cell_2d / 3d, cpp/src/Schemes.cpp:2153-2198): the leaf's limited states on its sides (its
+// faces' PR on a low side, PL on a high side) advanced by half_dt times the difference of their own Euler fluxes (the body
+// force, with half_dt, joins the difference), each kept where the advanced state is not admissible, and put back on the
+// faces; beside a reflecting wall the ghost side of the face is the wall's mirror of the predicted state.
+struct PredArgs {
+    Eos<double> eos;
+    Bc bc;
+    long long nleaf, lplane, fplane;
+    const double* U;   // the state at the start of the step (the body force of the predictor)
+    const int* side_face;
+    const int* meta;
+    double *PL, *PR;
+    double hx, hy, hz, half_dt;
+};
+
+template <int DIM, int NV> __global__ void __launch_bounds__(kCellsNT) k_cells_predict(const PredArgs p) {
+    const long long c = blockIdx.x * (long long)kCellsNT + threadIdx.x;
+    if (c >= p.nleaf) return;
+    constexpr int NS = 2 * DIM;
+    int fs[NS];
+    St<double, NV> st[NS];
+#pragma unroll
+    for (int sd = 0; sd < NS; ++sd) {
+        fs[sd] = p.side_face[NS * c + sd];
+        st[sd] = leaf_state<NV>((sd & 1) ? p.PL : p.PR, p.fplane, fs[sd]);   // the high side of a leaf is the left of its face
+    }
+    St<double, NV> fl[NS];
+#pragma unroll
+    for (int sd = 0; sd < NS; ++sd) {
+        if constexpr (NV == 5)
+            fl[sd] = euler_flux3(p.eos, st[sd], sd >> 1);
+        else
+            fl[sd] = euler_flux2(p.eos, st[sd], sd >> 1);
+    }
+    St<double, NV> d;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        d[q] = p.hx * (fl[1][q] - fl[0][q]) + p.hy * (fl[3][q] - fl[2][q]);
+        if constexpr (DIM == 3) d[q] = d[q] + p.hz * (fl[5][q] - fl[4][q]);
+    }
+    if (p.bc.grav_on) {
+        const St<double, NV> src = body_source<NV>(p.bc, p.U, p.lplane, c);
+#pragma unroll
+        for (int q = 0; q < NV; ++q) d[q] = d[q] - p.half_dt * src[q];
+    }
+#pragma unroll
+    for (int sd = 0; sd < NS; ++sd) {
+        St<double, NV> nst;
+#pragma unroll
+        for (int q = 0; q < NV; ++q) nst[q] = st[sd][q] - d[q];
+        bool ok;
+        if constexpr (NV == 5)
+            ok = admissible3(p.eos, nst);
+        else
+            ok = admissible(p.eos, nst);
+        if (ok) st[sd] = nst;
+        double* mine = (sd & 1) ? p.PL : p.PR;
+#pragma unroll
+        for (int q = 0; q < NV; ++q) mine[q * p.fplane + fs[sd]] = st[sd][q];
+        const int meta = p.meta[fs[sd]];
+        if ((meta >> 8) & 1) {
+            const int side = (meta >> 4) & 7, type = p.bc.type[side];
+            if (type == kBcWall || type == kBcNoSlip || type == kBcMovingWall) {
+                const St<double, NV> g = ghost_state(p.eos, p.bc, side, st[sd]);
+                double* other = (sd & 1) ? p.PR : p.PL;
+#pragma unroll
+                for (int q = 0; q < NV; ++q) other[q * p.fplane + fs[sd]] = g[q];
+            }
+        }
+    }
 }
 
 // ---- the viscous terms on a 3-D mesh (CellFluxEngine::cell_quantities_3d / viscous_fluxes_3d / viscous_speed_3d,
@@ -472,6 +566,7 @@ struct GatherArgs {
     const double* F;
     const double* Fv;       // [4][fplane] viscous fluxes times the face area (null: inviscid)
     Bc bc;                  // the body force (bc.grav, when bc.grav_on)
+    int hancock;            // MUSCL-Hancock: the predictor's source (the body force from zero) is added as a whole
     const int* side_face;   // [ns * nleaf]: the face on each side of each leaf (one at level 0)
     double length[3], inv_vol;
     int mode;
@@ -509,8 +604,17 @@ template <int DIM, int NV> __global__ void __launch_bounds__(kCellsNT) k_cells_g
             r[q] += vac * g.inv_vol;
         }
     }
-    // the body force after the viscous terms (CellFluxEngine::gather, CellFluxResidual.cpp:1015-1024)
-    if (g.bc.grav_on) add_body_force<NV>(g.bc, leaf_state<NV>(g.U, g.lplane, c), r);
+    // the body force after the viscous terms (CellFluxEngine::gather, CellFluxResidual.cpp:1015-1024); with MUSCL-Hancock
+    // the predictor's source, the body force summed from zero, joins as r + src (:1011-1014)
+    if (g.bc.grav_on) {
+        if (g.hancock) {
+            const St<double, NV> src = body_source<NV>(g.bc, g.U, g.lplane, c);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) r[q] = r[q] + src[q];
+        } else {
+            add_body_force<NV>(g.bc, leaf_state<NV>(g.U, g.lplane, c), r);
+        }
+    }
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
         const long long e = q * g.lplane + c;
@@ -666,14 +770,14 @@ int fail(fvg_cells* e, int code, const std::string& msg) {
 
 int flat_blocks(long long n) { return (int)std::min<long long>((n + 255) / 256, 148 * 16); }
 
-template <int NV> cudaError_t launch_faces(const fvg_cells* e, const CellArgs& a) {
+template <int NV, int MODE = kFacesFlux> cudaError_t launch_faces(const fvg_cells* e, const CellArgs& a) {
     const int blocks = (int)((a.nface + kCellsNT - 1) / kCellsNT);
     const int recon = e->cfg.reconstruction, lm = e->cfg.riemann == FVG_RIEMANN_LOWMACH;
 #define FACES(R)                                                                                            \
     if (lm)                                                                                                 \
-        k_cells_faces<NV, R, kLowMach><<<blocks, kCellsNT, 0, e->stream>>>(a);                              \
+        k_cells_faces<NV, R, kLowMach, MODE><<<blocks, kCellsNT, 0, e->stream>>>(a);                        \
     else                                                                                                    \
-        k_cells_faces<NV, R, kHLLC><<<blocks, kCellsNT, 0, e->stream>>>(a);
+        k_cells_faces<NV, R, kHLLC, MODE><<<blocks, kCellsNT, 0, e->stream>>>(a);
     switch (recon) {
     case FVG_RECON_NONE: FACES(kFirstOrder) break;
     case FVG_RECON_MUSCL: FACES(kMuscl) break;
@@ -684,8 +788,11 @@ template <int NV> cudaError_t launch_faces(const fvg_cells* e, const CellArgs& a
     return cudaGetLastError();
 }
 
-// one residual of Uin (its largest face speed into smax[slot]), gathered into out with the stage update `mode`
-int residual_pass(fvg_cells* e, const double* Uin, int slot, int mode, double ca, double cb, double dt, const double* U0, double* out) {
+// one residual of Uin (its largest face speed into smax[slot]), gathered into out with the stage update `mode`; with
+// half_dt > 0 the residual of MUSCL-Hancock (the face states predicted by half_dt first, CellAdvance::advance with
+// CellFluxEngine::predict_level and compute_level_fluxes(predicted), cpp/src/CellAdvance.cpp)
+int residual_pass(fvg_cells* e, const double* Uin, int slot, int mode, double ca, double cb, double dt, const double* U0, double* out,
+                  double half_dt = 0.0) {
     const long long n = e->nleaf;
     CKC(cudaMemsetAsync(e->smax + slot, 0, sizeof(unsigned long long), e->stream));
     if (e->cfg.reconstruction != FVG_RECON_NONE) {
@@ -712,7 +819,35 @@ int residual_pass(fvg_cells* e, const double* Uin, int slot, int mode, double ca
     a.meta = e->meta;
     a.F = e->F;
     a.smax = e->smax + slot;
-    CKC(e->nvar == 5 ? launch_faces<5>(e, a) : launch_faces<4>(e, a));
+    a.PL = e->PL;
+    a.PR = e->PR;
+    if (half_dt > 0.0) {   // the limited face states, the prediction of every leaf, the Riemann problems on the predicted states
+        CKC((e->nvar == 5 ? launch_faces<5, kFacesCollect>(e, a) : launch_faces<4, kFacesCollect>(e, a)));
+        PredArgs pa{};
+        pa.eos = e->eos;
+        pa.bc = e->bc;
+        pa.nleaf = n;
+        pa.lplane = e->lplane;
+        pa.fplane = e->fplane;
+        pa.U = Uin;
+        pa.side_face = e->side_face;
+        pa.meta = e->meta;
+        pa.PL = e->PL;
+        pa.PR = e->PR;
+        pa.hx = half_dt / e->h[0];   // hx = half_dt / dx, as the uniform solver's predictor
+        pa.hy = half_dt / e->h[1];
+        pa.hz = e->dim == 3 ? half_dt / e->h[2] : 0.0;
+        pa.half_dt = half_dt;
+        const int bl = (int)((n + kCellsNT - 1) / kCellsNT);
+        if (e->dim == 3)
+            k_cells_predict<3, 5><<<bl, kCellsNT, 0, e->stream>>>(pa);
+        else
+            k_cells_predict<2, 4><<<bl, kCellsNT, 0, e->stream>>>(pa);
+        CKC(cudaGetLastError());
+        CKC((e->nvar == 5 ? launch_faces<5, kFacesPredicted>(e, a) : launch_faces<4, kFacesPredicted>(e, a)));
+    } else {
+        CKC(e->nvar == 5 ? launch_faces<5>(e, a) : launch_faces<4>(e, a));
+    }
     if (e->visc) {   // the cell quantities and the leaves' speed bounds, then the viscous face fluxes
         CellVisc v{};
         v.va.eos = e->eos;
@@ -759,6 +894,7 @@ int residual_pass(fvg_cells* e, const double* Uin, int slot, int mode, double ca
     g.F = e->F;
     g.Fv = e->visc ? e->Fv : nullptr;
     g.bc = e->bc;
+    g.hancock = half_dt > 0.0;
     g.side_face = e->side_face;
     for (int k = 0; k < 3; ++k) g.length[k] = e->length[k];
     g.inv_vol = e->inv_vol;
@@ -810,7 +946,6 @@ int fvg_cells_create(const fvg_config* cfg, int nleaf, const int* level, const i
     else if (c.positivity_fallback) no = "positivity_fallback";
     else if (c.flux_quadrature == 1) no = "flux_quadrature = fourth";
     else if (c.precision != FVG_PREC_FP64) no = "the mixed-precision form";
-    else if (c.time_scheme == FVG_TS_HANCOCK) no = "MUSCL-Hancock";
     for (int s = 0; s < 6 && !no; ++s)
         if (c.bc[s] == FVG_BC_NONREFLECTING || c.bc[s] == FVG_BC_MASSFLOWINLET) no = "non-reflecting outlets and mass-flow inlets";
     if (why.empty() && no) why = std::string("the cell engine on the device does not take ") + no + " yet";
@@ -890,6 +1025,9 @@ int fvg_cells_create(const fvg_config* cfg, int nleaf, const int* level, const i
         (err = cudaMalloc(&e->side_face, sizeof(int) * e->ns * e->nleaf)) != cudaSuccess ||
         (err = cudaMalloc(&e->smax, sizeof(unsigned long long) * 3)) != cudaSuccess || (err = cudaMalloc(&e->bad, sizeof(int))) != cudaSuccess)
         return bail("cudaMalloc", err);
+    if (c.time_scheme == FVG_TS_HANCOCK &&
+        ((err = cudaMalloc(&e->PL, fb)) != cudaSuccess || (err = cudaMalloc(&e->PR, fb)) != cudaSuccess))
+        return bail("cudaMalloc", err);
     if (e->visc) {
         if ((err = cudaMalloc(&e->nbr, sizeof(int) * t.nbr.size())) != cudaSuccess || (err = cudaMalloc(&e->Q, sizeof(double) * (e->dim == 3 ? kQ : kQ2) * e->lplane)) != cudaSuccess ||
             (err = cudaMalloc(&e->Fv, sizeof(double) * 4 * e->fplane)) != cudaSuccess)
@@ -912,7 +1050,7 @@ int fvg_cells_destroy(fvg_cells* e) {
     cudaSetDevice(e->cfg.device);
     if (e->stream) cudaStreamSynchronize(e->stream);
     for (void* p : {(void*)e->U, (void*)e->Ut, (void*)e->W, (void*)e->R, (void*)e->F, (void*)e->staging, (void*)e->code, (void*)e->meta,
-                    (void*)e->side_face, (void*)e->smax, (void*)e->bad, (void*)e->nbr, (void*)e->Q, (void*)e->Fv})
+                    (void*)e->side_face, (void*)e->smax, (void*)e->bad, (void*)e->nbr, (void*)e->Q, (void*)e->Fv, (void*)e->PL, (void*)e->PR})
         if (p) cudaFree(p);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
@@ -981,6 +1119,7 @@ static int cells_enqueue_step(fvg_cells* e, double dt) {
     const int ts = e->cfg.time_scheme;
     int rc;
     if (ts == FVG_TS_EULER) return residual_pass(e, e->U, 0, kAxpy, 0.0, 0.0, dt, nullptr, e->U);
+    if (ts == FVG_TS_HANCOCK) return residual_pass(e, e->U, 0, kAxpy, 0.0, 0.0, dt, nullptr, e->U, 0.5 * dt);
     if ((rc = residual_pass(e, e->U, 0, kAxpy, 0.0, 0.0, dt, nullptr, e->Ut))) return rc;   // U1 = U + dt R(U)
     if (ts == FVG_TS_SSPRK2) return residual_pass(e, e->Ut, 1, kCombine, 0.5, 0.5, dt, e->U, e->U);
     if ((rc = residual_pass(e, e->Ut, 1, kCombine, 0.75, 0.25, dt, e->U, e->Ut))) return rc;

@@ -359,9 +359,9 @@ int fvg_batch_get_timing(const fvg_batch* b, double* stage_ms, long long* stage_
  * lengths, the scheme, the boundary conditions; the periodic axes are the periodic sides). Built: every leaf of level 0
  * (they must tile the base mesh); first order, MUSCL (every limiter), WENO3-Z, WENO5-Z; HLLC and low-Mach HLLC; the
  * boundary types but the non-reflecting outlet and the mass-flow inlet, with boundary_order 1 or 2; Euler, SSP-RK2 and
- * SSP-RK3 steps; the viscous terms (2-D and 3-D) and the body force. Refused (FVG_ERR_CONFIG, message in
+ * SSP-RK3 and MUSCL-Hancock steps; the viscous terms (2-D and 3-D) and the body force. Refused (FVG_ERR_CONFIG, message in
  * fvg_create_error()): leaves above level 0, an immersed body, sources and time-dependent boundary values,
- * positivity_fallback, the fourth-order quadrature, the mixed-precision form, MUSCL-Hancock. */
+ * positivity_fallback, the fourth-order quadrature, the mixed-precision form. */
 typedef struct fvg_cells fvg_cells;
 int fvg_cells_create(const fvg_config* cfg, int nleaf, const int* level, const int* ci, const int* cj, const int* ck, fvg_cells** out);
 int fvg_cells_destroy(fvg_cells* e);
@@ -374,7 +374,8 @@ int fvg_cells_download_state(fvg_cells* e, double* U, size_t nleaf);
  * the largest face wave speed */
 int fvg_cells_residual(fvg_cells* e, double* R, size_t nleaf, double* smax);
 /* one step of length dt from time t of the state held (CellAdvance::step: with one level, the time scheme's
- * advance_fixed_dt, cpp/src/TimeScheme.cpp:100-290); *smax (may be NULL) the first stage's largest face wave speed */
+ * advance_fixed_dt, cpp/src/TimeScheme.cpp:100-290; MUSCL-Hancock: the leaves' limited side states predicted by dt / 2,
+ * then one residual on them); *smax (may be NULL) the first stage's largest face wave speed */
 int fvg_cells_step(fvg_cells* e, double dt, double t, double* smax);
 /* nsteps such steps enqueued back to back (one host synchronisation at the end) */
 int fvg_cells_advance(fvg_cells* e, double dt, int nsteps, double* smax);

@@ -39,6 +39,6 @@ def test_refusals():
     out = ci.copy()
     out[0] = 9
     refused(P3, lv, out, cj, ck, "outside the base mesh")
-    for extra, what in ((dict(time_scheme="MUSCL-Hancock", reconstruction="muscl"), "MUSCL-Hancock"),
-                        (dict(bc_xmax="non_reflecting"), "non-reflecting"), (dict(positivity_fallback=True), "positivity_fallback")):
+    for extra, what in ((dict(bc_xmax="non_reflecting"), "non-reflecting"), (dict(positivity_fallback=True), "positivity_fallback"),
+                        (dict(flux_quadrature="fourth"), "fourth")):
         refused(dict(P3, **extra), lv, ci, cj, ck, what)

@@ -32,7 +32,8 @@ def bits_equal(a, b):
 
 
 def params_of(rig, bc, recon, order, scheme, **extra):
-    p = dict(rig, reconstruction=recon, boundary_order=order, time_scheme=scheme, muscl_limiter="Van Leer", **extra)
+    p = dict(rig, reconstruction=recon, boundary_order=order, time_scheme=scheme, muscl_limiter="Van Leer")
+    p.update(extra)
     names = ("bc_xmin", "bc_xmax", "bc_ymin", "bc_ymax", "bc_zmin", "bc_zmax")
     p.update(dict(zip(names, bc)))
     if len(bc) == 4:
@@ -186,3 +187,25 @@ def test_body_force_level0_matches_the_reference(dim, recon, order):
     if dim == 3:
         extra.update(use_viscous=True, mu=0.05, pr=0.72)
     compare(params_of(rig, bc, recon, order, SCHEMES[2], **extra), seed=80, max_levels=(0,))
+
+
+@pytest.mark.parametrize("visc", [False, True], ids=["inviscid", "viscous"])
+@pytest.mark.parametrize("order", [1, 2])
+@pytest.mark.parametrize("bc", SETS3, ids=["/".join(b) for b in SETS3])
+def test_hancock_level0_octree_matches_the_reference(bc, order, visc):
+    """MUSCL-Hancock on a level-0 octree (cpp/tests/test_amr_octree_advance.cpp:110-152): the leaves' limited side states
+    predicted by half a step, the Riemann problems on them, bit for bit against CellAdvance for 4 steps."""
+    extra = dict(use_viscous=True, mu=0.02, pr=0.72) if visc else {}
+    compare(params_of(RIG3, bc, "muscl", order, "MUSCL-Hancock", **extra), seed=90)
+
+
+@pytest.mark.parametrize("bc", SETS2, ids=["/".join(b) for b in SETS2])
+def test_hancock_level0_quadtree_matches_the_reference(bc):
+    for order in (1, 2):
+        compare(params_of(RIG, bc, "muscl", order, "MUSCL-Hancock", muscl_limiter="MC"), seed=91)
+        compare(params_of(dict(RIG, nx=96, ny=64), bc, "muscl", order, "MUSCL-Hancock"), seed=92, max_levels=(0,))
+
+
+def test_hancock_body_force_level0_matches_the_reference():
+    for rig, bc in ((RIG3, SETS3[1]), (RIG, SETS2[0])):
+        compare(params_of(rig, bc, "muscl", 2, "MUSCL-Hancock", use_bodyforce=True, gx=0.3, gy=-0.7, gz=0.2), seed=93, max_levels=(0,))
