@@ -176,6 +176,15 @@ __global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
         return u;
     };
 
+    // whether a side of the tile lies on a side of the mesh that is neither periodic nor a part interface (without one,
+    // every box position is a cell the arrays hold, after the periodic wrap, and no face of the tile has a wall rule),
+    // and whether the tile lies wholly inside the mesh
+    bool walls = false;
+#pragma unroll
+    for (int x = 0; x < 3; ++x)
+        walls = walls || (o3[x] == 0 && !a.through[2 * x]) || (o3[x] + (x == 0 ? TX : (x == 1 ? TY : TZ)) >= n3[x] && !a.through[2 * x + 1]);
+    const bool full = o3[0] + TX <= n3[0] && o3[1] + TY <= n3[1] && o3[2] + TZ <= n3[2];
+
     // ---- 0. the padded conservative state of the tile and one cell around it. A position beyond a periodic side is the
     // wrapped cell (so the box holds the neighbours the reference reads for that cell); the rest is the reference's
     // padded array (padded_cons). The eight corners are never read.
@@ -187,7 +196,7 @@ __global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
         // a tile that overhangs the mesh: positions past the ghost layer are clamped onto it (their results are not used)
 #pragma unroll
         for (int x = 0; x < 3; ++x) g[x] = box_clamp(a, x, g[x], n3[x]);
-        const St<double, 5> u = padded_cons(a, g[0], g[1], g[2]);
+        const St<double, 5> u = walls ? padded_cons(a, g[0], g[1], g[2]) : cell_at(a, g[0], g[1], g[2]);
 #pragma unroll
         for (int q = 0; q < 5; ++q) B[q * NB + e] = u[q];
     }
@@ -225,11 +234,12 @@ __global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
             const int g3[3] = {o3[0] + f3[0], o3[1] + f3[1], o3[2] + f3[2]};
             const int t = g3[d];
             bool inside = true;
+            if (!full)
 #pragma unroll
-            for (int x = 0; x < 3; ++x) inside = inside && (x == d ? g3[x] <= n3[x] : g3[x] < n3[x]);
+                for (int x = 0; x < 3; ++x) inside = inside && (x == d ? g3[x] <= n3[x] : g3[x] < n3[x]);
             double out[4] = {0.0, 0.0, 0.0, 0.0};
             if (inside) {
-                const bool lo = t == 0, hi = t == n3[d];
+                const bool lo = walls && t == 0, hi = walls && t == n3[d];
                 const int eL = (f3[2] * E[1] + f3[1]) * E[0] + f3[0];   // extended position of the cell t-1 (or the ghost)
                 const int eR = eL + estride;
                 int lc[3] = {f3[0], f3[1], f3[2]};
