@@ -65,6 +65,7 @@ __device__ __forceinline__ void batch_item_args(const BatchArgs& b, const BatchP
     sa.U0 = b.U0 ? b.U0 + pr.off : nullptr;
     sa.out = b.out + pr.off;
     sa.Rv = nullptr;
+    sa.Rvf = nullptr;
     sa.blockmax = nullptr;
     sa.ctl = nullptr;
     sa.gate = nullptr;

@@ -291,6 +291,13 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
         }
 }
 
+// r plus the viscous residual of variable q at `cell`: the FP64 residual of Rv, or the 3-D FP32 balance sum of Rvf times
+// 1 / volume (an uncontracted product: the value the FP64 array held when the viscous kernel stored that product)
+__device__ __forceinline__ double add_viscous(const StageArgs& a, double r, int q, long long cell) {
+    if (a.Rvf) return q == 0 ? r + 0.0 : r + __dmul_rn((double)a.Rvf[(q - 1) * a.m.plane + cell], a.m.inv_cell);
+    return a.Rv ? r + a.Rv[q * a.m.plane + cell] : r;
+}
+
 // The mixed-precision stage kernel: the tile sweep of stage_kernel (same phases, same launch geometry) with FP32 stencil
 // arithmetic; see the file comment for what stays FP64.
 // FULL = false: a run without part interfaces or non-reflecting sides (their code compiled out of the hot loop)
@@ -325,7 +332,7 @@ __global__ void __launch_bounds__(NT) mixed_stage_kernel(const StageArgs a) {
 #pragma unroll
         for (int q = 0; q < NV; ++q) {
             double r = (double)acc[q * NC + c] * m.inv_cell;
-            if (a.Rv) r = r + a.Rv[q * m.plane + cell];
+            r = add_viscous(a, r, q, cell);
             const long long e = q * m.plane + cell;
             double o;
             if (a.mode == kStoreR)
@@ -529,9 +536,8 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
         const int g3[3] = {o3[0] + c3[0], o3[1] + c3[1], o3[2] + c3[2]};
         if (g3[0] >= m.nx || g3[1] >= m.ny || g3[2] >= m.nz) continue;
         const long long cell = ((long long)g3[2] * m.ny + g3[1]) * m.nx + g3[0];
-        a.Rv[cell] = 0.0;
 #pragma unroll
-        for (int q = 1; q < 5; ++q) a.Rv[q * m.plane + cell] = (double)acc[(q - 1) * NC + c] * m.inv_cell;
+        for (int q = 1; q < 5; ++q) a.Rvf[(q - 1) * m.plane + cell] = acc[(q - 1) * NC + c];
         const int p = bidx(c3[0], c3[1], c3[2]);
         const float rho = vmax(B[p], Num<float>::eos_eps);
         const float T = B[4 * NB + p];
@@ -598,7 +604,7 @@ __global__ void __launch_bounds__(NT) mixed_stage_kernel_tma(const StageArgs a, 
 #pragma unroll
         for (int q = 0; q < NV; ++q) {
             double r = (double)acc[q * NC + c] * m.inv_cell;
-            if (a.Rv) r = r + a.Rv[q * m.plane + cell];
+            r = add_viscous(a, r, q, cell);
             const long long e = q * m.plane + cell;
             double o;
             if (a.mode == kStoreR)

@@ -893,7 +893,10 @@ StageArgs stage_args(fvg_run* r, const double* Uin, const double* U0, double* ou
     a.U = Uin;
     a.U0 = U0;
     a.out = out;
-    a.Rv = Rv;
+    // the 3-D mixed viscous kernel keeps its FP32 balance sums in the Rv array (4 float planes in the room of 5 doubles)
+    const bool f32v = Rv && r->cfg.precision == FVG_PREC_MIXED && r->dim == 3;
+    a.Rv = f32v ? nullptr : Rv;
+    a.Rvf = f32v ? reinterpret_cast<const float*>(Rv) : nullptr;
     a.blockmax = bm;
     a.ctl = r->ctl;
     a.gate = gate;
@@ -953,6 +956,7 @@ ViscArgs visc_args(fvg_run* r, const double* Uin, double* bmv, const int* gate) 
     }
     a.U = Uin;
     a.Rv = r->Rv;
+    a.Rvf = r->cfg.precision == FVG_PREC_MIXED && r->dim == 3 ? reinterpret_cast<float*>(r->Rv) : nullptr;
     a.blockmax = bmv;
     a.gate = gate;
     for (int d = 0; d < 3; ++d) a.tiles[d] = r->ntiles_v[d];

@@ -37,6 +37,9 @@ struct StageArgs {
     const double* U0;           // COMBINE: the state at the start of the step (read at the cell only)
     double* out;                // R or the updated state (never aliases U; may alias U0)
     const double* Rv;           // viscous residual to add (null: none)
+    // the 3-D mixed form's viscous balance sums instead (FP32, the planes rho u .. rho w after the density's, whose
+    // viscous term is 0): the viscous residual is each sum widened to FP64 times 1 / volume (null: none)
+    const float* Rvf;
     double* blockmax;           // per-CTA largest wave speed
     const Ctl* ctl;             // dt
     const int* gate;            // the kernel does nothing unless *gate (the control block's `active` or `seed`)

@@ -32,6 +32,7 @@ struct ViscArgs {
     int nvar;          // state planes: 4 on a 2-D mesh (rho w is +0 there), 5 in 3-D
     const double* U;
     double* Rv;
+    float* Rvf;        // the 3-D mixed form: the FP32 viscous balance sums of the planes 1 .. 4 (StageArgs::Rvf)
     double* blockmax;
     const int* gate;   // the kernel does nothing unless *gate
     int tiles[3];
