@@ -42,8 +42,8 @@ __device__ __forceinline__ void thin_y_mixed(const StageArgs& a, const Eos<float
         if (s_t > smax) smax = s_t;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const float d = (Ft[q] - Fb[q]) * A;
-            acc[q * TX + c] = acc[q * TX + c] - d;
+            const float d = __fmul_rn(Ft[q] - Fb[q], A);   // (rounded explicitly, as mixed_axis's balance)
+            acc[q * TX + c] = __fsub_rn(acc[q * TX + c], d);
         }
     }
     __syncthreads();
@@ -85,19 +85,10 @@ __global__ void __launch_bounds__(NT) batch_mixed_kernel(const BatchArgs b) {
             const int i = o3[0] + c % TX, j = o3[1] + c / TX;
             if (i >= m.nx || j >= m.ny) continue;
             const long long cell = (long long)j * m.nx + i;
+            CellIn<NV> in;
+            cell_load(sa, cell, in);
 #pragma unroll
-            for (int q = 0; q < NV; ++q) {
-                const double r = (double)acc[q * NC + c] * m.inv_cell;
-                const long long e = q * m.plane + cell;
-                double o;
-                if (sa.mode == kStoreR)
-                    o = r;
-                else if (sa.mode == kAxpy)
-                    o = sa.U[e] + dt * r;
-                else
-                    o = sa.ca * sa.U0[e] + sa.cb * (sa.U[e] + dt * r);
-                sa.out[e] = o;
-            }
+            for (int q = 0; q < NV; ++q) sa.out[q * m.plane + cell] = cell_out(sa, in, q, acc[q * NC + c], dt);
         }
         const double bm = block_max<NT>((double)smax, red);
         if (tid == 0) batch_stage_max(&b.ctl[it.prob], b.stage, bm);

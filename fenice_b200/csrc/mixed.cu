@@ -11,18 +11,18 @@ template <int DIM> struct MTile;
 template <> struct MTile<3> { static constexpr int X = 8, Y = 8, Z = 8, NT = 384; };
 template <> struct MTile<2> { static constexpr int X = 16, Y = 15, Z = 1, NT = 256; };
 
-// the kernel that stages interior tiles by TMA: 3-D WENO5-Z lean kernels, when the run passes tensor maps (StageArgs::tma)
+// the cross-box kernel whose tiles inside the mesh come in by TMA: the 3-D WENO5-Z lean kernels, when the run passes
+// tensor maps (StageArgs::tma); 8x8x8 tiles of 384 threads
 template <int DIM, int RECON, bool FULL> constexpr bool kHasTma = DIM == 3 && RECON == kWeno5 && !FULL;
 
 template <int RIEMANN, bool GATED> struct TmaK {
-    using T = MTile<3>;
-    using L = MixedTmaShape<T::X, T::Y, T::Z>;
+    static constexpr int NT = MTile<3>::NT;
+    static_assert(MTile<3>::X == 8 && MTile<3>::Y == 8 && MTile<3>::Z == 8, "the cross-box kernel's tile");
     static cudaError_t prepare() {
-        return cudaFuncSetAttribute(mixed_stage_kernel_tma<RIEMANN, T::X, T::Y, T::Z, T::NT, GATED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)L::SMEM_BYTES);
+        return cudaFuncSetAttribute(mixed_stage_kernel_tma<RIEMANN, NT, GATED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CrossShape::SMEM_BYTES);
     }
     static cudaError_t launch(const StageArgs& a, int nblocks, cudaStream_t s) {
-        mixed_stage_kernel_tma<RIEMANN, T::X, T::Y, T::Z, T::NT, GATED><<<nblocks, T::NT, L::SMEM_BYTES, s>>>(a, *static_cast<const TmaMaps*>(a.tma));
+        mixed_stage_kernel_tma<RIEMANN, NT, GATED><<<nblocks, NT, CrossShape::SMEM_BYTES, s>>>(a, *static_cast<const TmaMaps*>(a.tma));
         return cudaGetLastError();
     }
 };

@@ -53,8 +53,10 @@ __device__ __forceinline__ float face_flux_prim(const Eos<float>& e, float shock
 }
 
 // the fifth-order upwind value right of c2 from c0 .. c4: 0.1 p0 + 0.6 p1 + 0.3 p2 of the three candidate stencils
+// (explicitly rounded FMAs, as the single-precision weno5z: the same bits in every kernel)
 __device__ __forceinline__ float lin5(float c0, float c1, float c2, float c3, float c4) {
-    return (2.0f * c0 - 13.0f * c1 + 47.0f * c2 + 27.0f * c3 - 3.0f * c4) * (1.0f / 60.0f);
+    const float s = __fmaf_rn(-3.0f, c4, __fmaf_rn(27.0f, c3, __fmaf_rn(47.0f, c2, __fmaf_rn(-13.0f, c1, __fmul_rn(2.0f, c0)))));
+    return __fmul_rn(s, 1.0f / 60.0f);
 }
 
 template <int DIM, int RECON, int TX, int TY, int TZ> struct MixedShape {
@@ -282,20 +284,44 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
             const int fl = (c3[2] * Fd[1] + c3[1]) * Fd[0] + c3[0];
             const int fr = fl + (axis == 0 ? 1 : (axis == 1 ? Fd[0] : Fd[0] * Fd[1]));
 #pragma unroll
-            for (int q = 0; q < NV; ++q) {
-                const float d = (WL[q * S::NF + fr] - WL[q * S::NF + fl]) * A;
-                acc[q * NC + c] = axis == 0 ? -d : acc[q * NC + c] - d;
+            for (int q = 0; q < NV; ++q) {   // (rounded products and differences, never contracted: every kernel of
+                                               // the mixed form sums a cell's balance to the same bits)
+                const float d = __fmul_rn(WL[q * S::NF + fr] - WL[q * S::NF + fl], A);
+                acc[q * NC + c] = axis == 0 ? -d : __fsub_rn(acc[q * NC + c], d);
             }
         }
         __syncthreads();
         }
 }
 
-// r plus the viscous residual of variable q at `cell`: the FP64 residual of Rv, or the 3-D FP32 balance sum of Rvf times
-// 1 / volume (an uncontracted product: the value the FP64 array held when the viscous kernel stored that product)
-__device__ __forceinline__ double add_viscous(const StageArgs& a, double r, int q, long long cell) {
-    if (a.Rvf) return q == 0 ? r + 0.0 : r + __dmul_rn((double)a.Rvf[(q - 1) * a.m.plane + cell], a.m.inv_cell);
-    return a.Rv ? r + a.Rv[q * a.m.plane + cell] : r;
+// The epilogue of the mixed form. A cell's global operands (U, U0, the viscous residual) are loaded first, all variables
+// at once, so that their latency overlaps; then every FP64 product and sum is rounded by an explicit intrinsic (nothing
+// left for a compiler pass to contract one way in one kernel and another way in the next: each kernel that updates a
+// cell gives it the same bits).
+template <int NV> struct CellIn {
+    double u[NV], u0[NV], rv[NV];
+};
+template <int NV> __device__ __forceinline__ void cell_load(const StageArgs& a, long long cell, CellIn<NV>& in) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        const long long e = q * a.m.plane + cell;
+        in.u[q] = a.mode != kStoreR ? a.U[e] : 0.0;
+        in.u0[q] = a.mode == kCombine ? a.U0[e] : 0.0;
+        in.rv[q] = a.Rvf ? (q == 0 ? 0.0 : (double)a.Rvf[(q - 1) * a.m.plane + cell]) : (a.Rv ? a.Rv[e] : 0.0);
+    }
+}
+// variable q's output from the tile's FP32 balance sum: the residual sum / volume plus the viscous residual (Rv, or the
+// 3-D FP32 viscous balance sum of Rvf / volume; the density's viscous term is +0), then R, U + dt R, or ca U0 + cb (U + dt R)
+template <int NV> __device__ __forceinline__ double cell_out(const StageArgs& a, const CellIn<NV>& in, int q, float sum, double dt) {
+    double r = __dmul_rn((double)sum, a.m.inv_cell);
+    if (a.Rvf)
+        r = q == 0 ? __dadd_rn(r, 0.0) : __dadd_rn(r, __dmul_rn(in.rv[q], a.m.inv_cell));
+    else if (a.Rv)
+        r = __dadd_rn(r, in.rv[q]);
+    if (a.mode == kStoreR) return r;
+    const double u = __dadd_rn(in.u[q], __dmul_rn(dt, r));
+    if (a.mode == kAxpy) return u;
+    return __dadd_rn(__dmul_rn(a.ca, in.u0[q]), __dmul_rn(a.cb, u));
 }
 
 // The mixed-precision stage kernel: the tile sweep of stage_kernel (same phases, same launch geometry) with FP32 stencil
@@ -329,20 +355,10 @@ __global__ void __launch_bounds__(NT) mixed_stage_kernel(const StageArgs a) {
         const int g3[3] = {o3[0] + c3[0], o3[1] + c3[1], o3[2] + c3[2]};
         if (g3[0] >= m.nx || g3[1] >= m.ny || g3[2] >= m.nz) continue;
         const long long cell = ((long long)g3[2] * m.ny + g3[1]) * m.nx + g3[0];
+        CellIn<NV> in;
+        cell_load(a, cell, in);
 #pragma unroll
-        for (int q = 0; q < NV; ++q) {
-            double r = (double)acc[q * NC + c] * m.inv_cell;
-            r = add_viscous(a, r, q, cell);
-            const long long e = q * m.plane + cell;
-            double o;
-            if (a.mode == kStoreR)
-                o = r;
-            else if (a.mode == kAxpy)
-                o = a.U[e] + dt * r;
-            else
-                o = a.ca * a.U0[e] + a.cb * (a.U[e] + dt * r);
-            a.out[e] = o;
-        }
+        for (int q = 0; q < NV; ++q) a.out[q * m.plane + cell] = cell_out(a, in, q, acc[q * NC + c], dt);
     }
     const double bm = block_max<NT>((double)smax, red);
     if (tid == 0) a.blockmax[b] = bm;
@@ -551,12 +567,9 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
     if (tid == 0) a.blockmax[b] = bm;
 }
 
-// The mixed WENO5-Z stage kernel of a 3-D mesh without part interfaces, non-reflecting sides or an immersed body, with
-// the boxes of its interior tiles staged by TMA (tma.cuh; the boundary tiles keep the index-mapping loader): the same
-// arithmetic and bits as mixed_stage_kernel. Shared memory: red [32 doubles] | the barrier | P | acc | Sf | (128-byte
-// aligned) WL, WR, sized for the largest box (16 x 8 x 8 x 5 doubles, 40 KB), which the copy fills while the face-value
-// arrays are idle: 70 KB, three CTAs of 384 threads per SM as the kernel without TMA. Measured at 256^3 (Taylor-Green):
-// 2.61 ms per launch against 2.92 ms.
+// The per-axis sweep's shared memory with TMA boxes (mixed_axis with TMA): red [32 doubles] | the barrier | P | acc | Sf |
+// (128-byte aligned) WL, WR, sized for the largest box (16 x 8 x 8 x 5 doubles, 40 KB), which the copy fills while the
+// face-value arrays are idle.
 template <int TX, int TY, int TZ> struct MixedTmaShape {
     using S = MixedShape<3, kWeno5, TX, TY, TZ>;
     static constexpr int P_OFF = 272, ACC_OFF = P_OFF + 4 * S::NV * S::EXT, SF_OFF = ACC_OFF + 4 * S::NV * S::NC;
@@ -566,19 +579,295 @@ template <int TX, int TY, int TZ> struct MixedTmaShape {
     static constexpr size_t SMEM_BYTES = STG_OFF + STG_BYTES;
 };
 
-template <int RIEMANN, int TX, int TY, int TZ, int NT, bool GATED>
-__global__ void __launch_bounds__(NT) mixed_stage_kernel_tma(const StageArgs a, const __grid_constant__ TmaMaps maps) {
-    using S = MixedShape<3, kWeno5, TX, TY, TZ>;
-    using L = MixedTmaShape<TX, TY, TZ>;
+// The mixed WENO5-Z stage kernel of a 3-D mesh without part interfaces, non-reflecting sides or an immersed body, whose
+// boxes come in by TMA (tma.cuh; no copy multicasts), in two forms chosen per tile (a branch uniform over the CTA):
+// - the per-axis sweep of mixed_stage_kernel (mixed_axis with TMA: a 16 x 8 x 8, 8 x 14 x 8 or 8 x 8 x 14 box per axis),
+//   for every tile of the ungated kernel and for the gated tiles that keep WENO5-Z along some axis or beside a seam;
+// - the cross (gated tiles linear along all three axes and at all six seams): one image of the tile and its three halos
+//   (the 8x8x8 tile and 3 cells beyond each of its six faces, 1664 cells) converted once, from a 16 x 8 x 8 box (the tile
+//   and its x halos) and four 3-deep halo boxes; then every face of the three axes in one pass, one thread per face and
+//   all five variables (the linear face values straight into the Riemann solver, no face-value arrays); then the
+//   balance ((0 - x) - y) - z of each cell from the three flux arrays in the epilogue.
+// Both forms give the bits of mixed_stage_kernel (the explicitly rounded lin5 / weno5z, balance and update), so a face
+// between tiles of the two forms gets one flux. A tile whose boxes would leave the mesh (wrapped or ghost cells) takes the
+// index-mapping loader for those parts. Measured at 256^3 (Taylor-Green, every tile-axis linear, with the viscous sums
+// and U0): 1.98 ms per launch for the cross against 2.12 ms for the per-axis sweep; with WENO5-Z along every axis the
+// per-axis sweep is the faster (2.74 against 3.01 ms: its (face, variable) items spread the WENO5-Z work finer).
+// Shared memory: the larger of the two layouts (72.9 KB), three CTAs of 384 threads per SM (at most 56 registers).
+struct CrossShape {
+    static constexpr int NV = 5, NCORE = 512, NHALO = 192, NPC = NCORE + 6 * NHALO;   // cells of the cross
+    static constexpr int NFA = 576, NFACE = 3 * NFA, NINNER = 448;                    // faces per axis; t = 1 .. 7
+    static constexpr int BAR_OFF = 256, P_OFF = 272;
+    static constexpr int STG_OFF = (P_OFF + 4 * NV * NPC + 127) / 128 * 128;
+    static constexpr int XBOX = 16 * 8 * 8, HBOX = 8 * 3 * 8;   // cells of the x box and of one halo box
+    static constexpr int STG_BYTES = XBOX * NV * 8;
+    static constexpr size_t CROSS_BYTES = STG_OFF + STG_BYTES;
+    static constexpr size_t SMEM_BYTES = CROSS_BYTES > MixedTmaShape<8, 8, 8>::SMEM_BYTES ? CROSS_BYTES : MixedTmaShape<8, 8, 8>::SMEM_BYTES;
+    static_assert(4 * HBOX * NV * 8 <= STG_BYTES && 3 * NV * NFA * 4 <= STG_BYTES, "the staging area holds the halo boxes and the fluxes");
+};
+
+// the cross's slot of the cell at s along axis A (s in [-3, 11)) and (u, v) along the other two axes in increasing
+// order: the tile's 512 cells (x fastest), then the six halos (axis-major, low side first), each 3 deep x 64 cells
+template <int A> __device__ __forceinline__ int cross_slot(int s, int u, int v) {
+    if (s < 0) return 512 + (2 * A) * 192 + (s + 3) + 3 * (u + 8 * v);
+    if (s >= 8) return 512 + (2 * A + 1) * 192 + (s - 8) + 3 * (u + 8 * v);
+    return A == 0 ? s + 8 * u + 64 * v : (A == 1 ? u + 8 * s + 64 * v : u + 8 * v + 64 * s);
+}
+// the tile-local cell of slot e (the inverse of cross_slot)
+__device__ __forceinline__ void cross_cell(int e, int l3[3]) {
+    if (e < 512) {
+        l3[0] = e & 7;
+        l3[1] = (e >> 3) & 7;
+        l3[2] = e >> 6;
+        return;
+    }
+    const int k = (e - 512) / 192, r = (e - 512) % 192, A = k >> 1;
+    const int l = r % 3, uv = r / 3, u = uv & 7, v = uv >> 3;
+    const int s = (k & 1) ? 8 + l : l - 3;
+    l3[0] = A == 0 ? s : u;
+    l3[1] = A == 0 ? u : (A == 1 ? s : v);
+    l3[2] = A == 2 ? s : v;
+}
+
+// One face of axis A in the cross (linear face values): item r of the axis (the 448 faces inside the tile, t = 1 .. 7,
+// then the two seam layers t = 0 and 8); its flux goes to Fs at the face's index in mixed_axis's numbering.
+template <int A, int RIEMANN>
+__device__ __forceinline__ void cross_face(const StageArgs& a, const Eos<float>& ef, float sb, const float* __restrict__ P, float* __restrict__ Fs,
+                                           int r, const int o3[3], float& smax) {
+    constexpr int NV = 5, NPC = CrossShape::NPC;
+    int t, u, v;
+    if (r < CrossShape::NINNER) {
+        if (A == 0) {
+            t = 1 + r % 7;
+            u = (r / 7) & 7;
+            v = r / 56;
+        } else {
+            u = r & 7;
+            t = 1 + (r >> 3) % 7;
+            v = (r >> 3) / 7;
+        }
+    } else {
+        const int q = r - CrossShape::NINNER;
+        u = q & 7;
+        v = (q >> 3) & 7;
+        t = (q >> 6) * 8;
+    }
+    const int f = A == 0 ? t + 9 * (u + 8 * v) : (A == 1 ? u + 8 * (t + 9 * v) : u + 8 * (v + 8 * t));
+    int sl[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) sl[k] = cross_slot<A>(t - 3 + k, u, v);
+    St<float, NV> wl, wr;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        const float* c = P + q * NPC;
+        const float c0 = c[sl[0]], c1 = c[sl[1]], c2 = c[sl[2]], c3 = c[sl[3]], c4 = c[sl[4]], c5 = c[sl[5]];
+        wl[q] = lin5(c0, c1, c2, c3, c4);
+        wr[q] = lin5(c5, c4, c3, c2, c1);
+    }
+    const Mesh& m = a.m;
+    const int n3[3] = {m.nx, m.ny, m.nz};
+    const int g3[3] = {o3[0] + (A == 0 ? t : u), o3[1] + (A == 0 ? u : (A == 1 ? t : v)), o3[2] + (A == 2 ? t : v)};
+    bool inside = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) inside = inside && (d == A ? g3[d] <= n3[d] : g3[d] < n3[d]);
+    St<float, NV> F;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) F[q] = 0.0f;
+    if (inside) {
+        const int tg = g3[A];
+        const bool lo_face = tg == 0 && a.bc.halo[2 * A] == kHaloNone;
+        const bool hi_face = tg == n3[A] && a.bc.halo[2 * A + 1] == kHaloNone;
+        if (lo_face || hi_face) {   // a side without a halo: the first-order side states, as mixed_axis
+            int c3[3] = {g3[0], g3[1], g3[2]};
+            if (hi_face) c3[A] = n3[A] - 1;
+            St<double, NV> UL, UR;
+            side_states<NV, false>(m, a.bc, a.eos, a.U, lo_face ? 2 * A : 2 * A + 1, c3[0], c3[1], c3[2], UL, UR);
+            const St<double, NV> dl = c2p(a.eos, UL), dr = c2p(a.eos, UR);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) {
+                wl[q] = (float)dl[q];
+                wr[q] = (float)dr[q];
+            }
+        }
+        const float sp = face_flux_prim<RIEMANN>(ef, sb, wl, wr, A, F);
+        if (sp > smax) smax = sp;
+    }
+#pragma unroll
+    for (int q = 0; q < NV; ++q) Fs[(A * NV + q) * CrossShape::NFA + f] = F[q];
+}
+
+// The cross form of a tile (see mixed_stage_kernel_tma): maps m[0] (the 16 x 8 x 8 box), m[3] and m[4] (the y and z halo
+// boxes); `phase` counts the barrier's completed copies.
+template <int RIEMANN, int NT>
+__device__ __forceinline__ void cross_tile(const StageArgs& a, const TmaMaps& maps, unsigned char* smem_b, const int o3[3], unsigned& phase, float& smax) {
+    using L = CrossShape;
+    constexpr int NV = 5, NPC = L::NPC;
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_b + L::BAR_OFF);
+    float* P = reinterpret_cast<float*>(smem_b + L::P_OFF);
+    double* stg = reinterpret_cast<double*>(smem_b + L::STG_OFF);
+    float* Fs = reinterpret_cast<float*>(smem_b + L::STG_OFF);
+    const Mesh& m = a.m;
+    const int n3[3] = {m.nx, m.ny, m.nz};
+    const Eos<float> ef{a.eos.type, (float)a.eos.gamma, (float)a.eos.p_inf};
+    const float sb = (float)a.shock_blend;
+    const int tid = threadIdx.x;
+    const bool aligned = (tma::su32(stg) & 127u) == 0;
+    // every thread waits for the barrier's current phase, at most 2^22 polls; a copy that never completes stops the run
+    // (status 5) instead of hanging the GPU
+    auto wait = [&]() -> bool {
+        bool done = false;
+        for (int it = 0; it < (1 << 22) && !done; ++it) done = tma::mbar_try_wait(bar, phase & 1u);
+        ++phase;
+        if (!done && tid == 0) atomicExch(const_cast<int*>(&a.ctl->status), 5);
+        return done;
+    };
+    // slots e0 .. e1 of the cross by index mapping (wrapped and ghost cells), the primitive state recovered in FP64
+    auto load_slots = [&](int e0, int e1) {
+        for (int e = e0 + tid; e < e1; e += NT) {
+            int l3[3];
+            cross_cell(e, l3);
+            const St<double, NV> w = c2p(a.eos, stencil_cons<3, NV, false>(m, a.bc, a.eos, a.U, o3[0] + l3[0], o3[1] + l3[1], o3[2] + l3[2]));
+#pragma unroll
+            for (int q = 0; q < NV; ++q) P[q * NPC + e] = (float)w[q];
+        }
+    };
+    // the epilogue's operands that no box brings in (the tile's rows of U0 and of the viscous sums) head for L2 now
+    if (a.mode == kCombine || a.Rvf) {
+        for (int k = tid; k < 9 * 64; k += NT) {
+            const int q = k >> 6, y = o3[1] + (k & 7), z = o3[2] + ((k >> 3) & 7);
+            if (y >= n3[1] || z >= n3[2]) continue;
+            const long long row = ((long long)z * n3[1] + y) * n3[0] + o3[0];
+            if (q < 5 && a.mode == kCombine) tma::prefetch_l2(a.U0 + q * m.plane + row);
+            if (q >= 5 && a.Rvf) tma::prefetch_l2(a.Rvf + (q - 5) * m.plane + row);
+        }
+    }
+    // ---- 1. the tile and its x halos (slots 0 .. 895): one 16 x 8 x 8 box from x = o - 4
+    if (aligned && o3[0] >= 4 && o3[0] + 12 <= n3[0] && o3[1] + 8 <= n3[1] && o3[2] + 8 <= n3[2]) {
+        if (tid == 0) {
+            tma::fence_proxy_async();
+            tma::mbar_expect_tx(bar, (unsigned)(L::XBOX * NV * 8));
+            tma::load_4d(stg, &maps.m[0], o3[0] - 4, o3[1], o3[2], 0, bar);
+        }
+        const bool done = wait();
+        for (int e = tid; e < 14 * 64; e += NT) {
+            const int xl = e % 14 - 3, y = (e / 14) & 7, z = e / 112;
+            const int si = (z * 8 + y) * 16 + xl + 4;
+            St<double, NV> uc;
+#pragma unroll
+            for (int q = 0; q < NV; ++q) uc[q] = done ? stg[q * L::XBOX + si] : 1.0;
+            const St<double, NV> w = c2p(a.eos, uc);
+            const int p = cross_slot<0>(xl, y, z);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) P[q * NPC + p] = (float)w[q];
+        }
+    } else {
+        load_slots(0, 896);
+    }
+    __syncthreads();
+    // ---- 2. the y and z halos (slots 896 .. 1663): four 3-deep boxes on one barrier phase
+    if (aligned && o3[1] >= 3 && o3[1] + 11 <= n3[1] && o3[2] >= 3 && o3[2] + 11 <= n3[2] && o3[0] + 8 <= n3[0]) {
+        if (tid == 0) {
+            tma::fence_proxy_async();
+            tma::mbar_expect_tx(bar, (unsigned)(4 * L::HBOX * NV * 8));
+            tma::load_4d(stg, &maps.m[3], o3[0], o3[1] - 3, o3[2], 0, bar);
+            tma::load_4d(stg + 1 * L::HBOX * NV, &maps.m[3], o3[0], o3[1] + 8, o3[2], 0, bar);
+            tma::load_4d(stg + 2 * L::HBOX * NV, &maps.m[4], o3[0], o3[1], o3[2] - 3, 0, bar);
+            tma::load_4d(stg + 3 * L::HBOX * NV, &maps.m[4], o3[0], o3[1], o3[2] + 8, 0, bar);
+        }
+        const bool done = wait();
+        for (int e = tid; e < 4 * L::HBOX; e += NT) {
+            const int k = e / L::HBOX, r = e % L::HBOX;
+            const double* box = stg + k * L::HBOX * NV;
+            int si, p;
+            if (k < 2) {   // 8 x 3 x 8 boxes below and above the tile along y
+                const int x = r & 7, yb = (r >> 3) % 3, z = r / 24;
+                si = (z * 3 + yb) * 8 + x;
+                p = cross_slot<1>(k == 0 ? yb - 3 : 8 + yb, x, z);
+            } else {       // 8 x 8 x 3 boxes along z
+                const int x = r & 7, y = (r >> 3) & 7, zb = r >> 6;
+                si = (zb * 8 + y) * 8 + x;
+                p = cross_slot<2>(k == 2 ? zb - 3 : 8 + zb, x, y);
+            }
+            St<double, NV> uc;
+#pragma unroll
+            for (int q = 0; q < NV; ++q) uc[q] = done ? box[q * L::HBOX + si] : 1.0;
+            const St<double, NV> w = c2p(a.eos, uc);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) P[q * NPC + p] = (float)w[q];
+        }
+    } else {
+        load_slots(896, NPC);
+    }
+    __syncthreads();
+    // ---- 3. every face of the three axes (the faces inside the tile first, 448 per axis, then the seam layers)
+    for (int it = tid; it < L::NFACE; it += NT) {
+        int A, r;
+        if (it < 3 * L::NINNER) {
+            A = it / L::NINNER;
+            r = it - A * L::NINNER;
+        } else {
+            const int q = it - 3 * L::NINNER;
+            A = q >> 7;
+            r = L::NINNER + (q & 127);
+        }
+        if (A == 0)
+            cross_face<0, RIEMANN>(a, ef, sb, P, Fs, r, o3, smax);
+        else if (A == 1)
+            cross_face<1, RIEMANN>(a, ef, sb, P, Fs, r, o3, smax);
+        else
+            cross_face<2, RIEMANN>(a, ef, sb, P, Fs, r, o3, smax);
+    }
+    __syncthreads();
+    // ---- 4. the balance ((0 - x) - y) - z, the residual widened to FP64 and the FP64 stage update
+    const float Ax = (float)m.area[0], Ay = (float)m.area[1], Az = (float)m.area[2];
+    const double dt = a.ctl->dt;
+    for (int c = tid; c < 512; c += NT) {
+        const int c3[3] = {c & 7, (c >> 3) & 7, c >> 6};
+        const int g3[3] = {o3[0] + c3[0], o3[1] + c3[1], o3[2] + c3[2]};
+        if (g3[0] >= m.nx || g3[1] >= m.ny || g3[2] >= m.nz) continue;
+        const long long cell = ((long long)g3[2] * m.ny + g3[1]) * m.nx + g3[0];
+        const int fx = (c3[2] * 8 + c3[1]) * 9 + c3[0], fy = (c3[2] * 9 + c3[1]) * 8 + c3[0], fz = c;
+        CellIn<NV> in;
+        cell_load(a, cell, in);
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            const float* X = Fs + (0 * NV + q) * L::NFA;
+            const float* Y = Fs + (1 * NV + q) * L::NFA;
+            const float* Z = Fs + (2 * NV + q) * L::NFA;
+            float acc = -__fmul_rn(X[fx + 1] - X[fx], Ax);
+            acc = __fsub_rn(acc, __fmul_rn(Y[fy + 8] - Y[fy], Ay));
+            acc = __fsub_rn(acc, __fmul_rn(Z[fz + 64] - Z[fz], Az));
+            a.out[q * m.plane + cell] = cell_out(a, in, q, acc, dt);
+        }
+    }
+}
+
+// whether a gated tile is linear along all three axes and at all six seams (the seam rule of mixed_axis)
+__device__ __forceinline__ bool tile_all_linear(const StageArgs& a, int b, const int o3[3]) {
+    const long long nt3 = (long long)a.tiles[0] * a.tiles[1] * a.tiles[2];
+    bool lin = true;
+#pragma unroll
+    for (int A = 0; A < 3; ++A) {
+        const unsigned char* fl = a.sens_flags + A * nt3;
+        const int nt = a.tiles[A];
+        const int st = A == 0 ? 1 : (A == 1 ? a.tiles[0] : a.tiles[0] * a.tiles[1]);
+        const int ta = A == 0 ? b % a.tiles[0] : (A == 1 ? (b / a.tiles[0]) % a.tiles[1] : b / (a.tiles[0] * a.tiles[1]));
+        const bool wrap_lo = a.bc.halo[2 * A] == kHaloWrap, wrap_hi = a.bc.halo[2 * A + 1] == kHaloWrap;
+        lin = lin && fl[b] == 0;
+        lin = lin && (ta > 0 ? fl[b - st] == 0 : (wrap_lo ? fl[b + (nt - 1) * st] == 0 : true));
+        lin = lin && (ta < nt - 1 ? fl[b + st] == 0 : (wrap_hi ? fl[b - (nt - 1) * st] == 0 : true));
+    }
+    return lin;
+}
+
+template <int RIEMANN, int NT, bool GATED>
+__global__ void __launch_bounds__(NT, 3) mixed_stage_kernel_tma(const StageArgs a, const __grid_constant__ TmaMaps maps) {
+    using S = MixedShape<3, kWeno5, 8, 8, 8>;
+    using LO = MixedTmaShape<8, 8, 8>;
     constexpr int NV = S::NV, NC = S::NC;
     extern __shared__ __align__(128) unsigned char smem_b[];
     double* red = reinterpret_cast<double*>(smem_b);
-    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_b + 256);
-    float* P = reinterpret_cast<float*>(smem_b + L::P_OFF);
-    float* acc = reinterpret_cast<float*>(smem_b + L::ACC_OFF);
-    unsigned char* Sf = smem_b + L::SF_OFF;
-    float* WL = reinterpret_cast<float*>(smem_b + L::STG_OFF);
-    float* WR = WL + NV * S::NF;
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_b + CrossShape::BAR_OFF);
     if (!*a.gate) return;
     if (threadIdx.x == 0) {
         tma::mbar_init(bar, 1);
@@ -586,34 +875,35 @@ __global__ void __launch_bounds__(NT) mixed_stage_kernel_tma(const StageArgs a, 
     }
     __syncthreads();
     const Mesh& m = a.m;
-    const Eos<float> ef{a.eos.type, (float)a.eos.gamma, (float)a.eos.p_inf};
-    const float sb = (float)a.shock_blend, weps = (float)a.weno_eps;
     const int tid = threadIdx.x, b = blockIdx.x + a.b0;
-    const int o3[3] = {(b % a.tiles[0]) * TX, ((b / a.tiles[0]) % a.tiles[1]) * TY, (b / (a.tiles[0] * a.tiles[1])) * TZ};
+    const int o3[3] = {(b % a.tiles[0]) * 8, ((b / a.tiles[0]) % a.tiles[1]) * 8, (b / (a.tiles[0] * a.tiles[1])) * 8};
     float smax = 0.0f;
     unsigned phase = 0;
-    mixed_axis<0, 3, kWeno5, RIEMANN, TX, TY, TZ, NT, GATED, false, true>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax, maps.m, bar, &phase);
-    mixed_axis<1, 3, kWeno5, RIEMANN, TX, TY, TZ, NT, GATED, false, true>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax, maps.m, bar, &phase);
-    mixed_axis<2, 3, kWeno5, RIEMANN, TX, TY, TZ, NT, GATED, false, true>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax, maps.m, bar, &phase);
-    const double dt = a.ctl->dt;
-    for (int c = tid; c < NC; c += NT) {
-        const int c3[3] = {c % TX, (c / TX) % TY, c / (TX * TY)};
-        const int g3[3] = {o3[0] + c3[0], o3[1] + c3[1], o3[2] + c3[2]};
-        if (g3[0] >= m.nx || g3[1] >= m.ny || g3[2] >= m.nz) continue;
-        const long long cell = ((long long)g3[2] * m.ny + g3[1]) * m.nx + g3[0];
+    bool cross = false;
+    if constexpr (GATED) cross = tile_all_linear(a, b, o3);
+    if (cross) {
+        cross_tile<RIEMANN, NT>(a, maps, smem_b, o3, phase, smax);
+    } else {
+        float* P = reinterpret_cast<float*>(smem_b + LO::P_OFF);
+        float* acc = reinterpret_cast<float*>(smem_b + LO::ACC_OFF);
+        unsigned char* Sf = smem_b + LO::SF_OFF;
+        float* WL = reinterpret_cast<float*>(smem_b + LO::STG_OFF);
+        float* WR = WL + NV * S::NF;
+        const Eos<float> ef{a.eos.type, (float)a.eos.gamma, (float)a.eos.p_inf};
+        const float sb = (float)a.shock_blend, weps = (float)a.weno_eps;
+        mixed_axis<0, 3, kWeno5, RIEMANN, 8, 8, 8, NT, GATED, false, true>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax, maps.m, bar, &phase);
+        mixed_axis<1, 3, kWeno5, RIEMANN, 8, 8, 8, NT, GATED, false, true>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax, maps.m, bar, &phase);
+        mixed_axis<2, 3, kWeno5, RIEMANN, 8, 8, 8, NT, GATED, false, true>(a, ef, sb, weps, P, WL, WR, acc, Sf, o3, smax, maps.m, bar, &phase);
+        const double dt = a.ctl->dt;
+        for (int c = tid; c < NC; c += NT) {
+            const int c3[3] = {c % 8, (c / 8) % 8, c / 64};
+            const int g3[3] = {o3[0] + c3[0], o3[1] + c3[1], o3[2] + c3[2]};
+            if (g3[0] >= m.nx || g3[1] >= m.ny || g3[2] >= m.nz) continue;
+            const long long cell = ((long long)g3[2] * m.ny + g3[1]) * m.nx + g3[0];
+            CellIn<NV> in;
+            cell_load(a, cell, in);
 #pragma unroll
-        for (int q = 0; q < NV; ++q) {
-            double r = (double)acc[q * NC + c] * m.inv_cell;
-            r = add_viscous(a, r, q, cell);
-            const long long e = q * m.plane + cell;
-            double o;
-            if (a.mode == kStoreR)
-                o = r;
-            else if (a.mode == kAxpy)
-                o = a.U[e] + dt * r;
-            else
-                o = a.ca * a.U0[e] + a.cb * (a.U[e] + dt * r);
-            a.out[e] = o;
+            for (int q = 0; q < NV; ++q) a.out[q * m.plane + cell] = cell_out(a, in, q, acc[q * NC + c], dt);
         }
     }
     const double bm = block_max<NT>((double)smax, red);

@@ -164,6 +164,33 @@ template <typename T> __device__ __forceinline__ T weno5z(T c0, T c1, T c2, T c3
     const T a0 = T(0.1) * (T(1) + tau / (b0 + eps)), a1 = T(0.6) * (T(1) + tau / (b1 + eps)), a2 = T(0.3) * (T(1) + tau / (b2 + eps));
     return (a0 * p0 + a1 * p1 + a2 * p2) / (a0 + a1 + a2);
 }
+// The single-precision WENO5-Z of the mixed form: the same weights, with every product and sum rounded by an explicit
+// intrinsic (FMAs placed by hand) and the candidates' common 1/6 folded into the last division, so that no compiler pass
+// contracts it one way in one kernel and another way in the next: every kernel that solves a face gets the same bits.
+__device__ __forceinline__ float weno5z(float c0, float c1, float c2, float c3, float c4, float eps_rel) {
+    float ss = __fmul_rn(c0, c0);
+    ss = __fmaf_rn(c1, c1, ss);
+    ss = __fmaf_rn(c2, c2, ss);
+    ss = __fmaf_rn(c3, c3, ss);
+    ss = __fmaf_rn(c4, c4, ss);
+    const float eps = __fmaf_rn(__fmul_rn(eps_rel, ss), 0.2f, Num<float>::weno_floor);
+    const float p0 = __fmaf_rn(11.0f, c2, __fmaf_rn(-7.0f, c1, __fmul_rn(2.0f, c0)));   // 6 x the three candidates
+    const float p1 = __fmaf_rn(2.0f, c3, __fmaf_rn(5.0f, c2, -c1));
+    const float p2 = __fmaf_rn(5.0f, c3, __fmaf_rn(2.0f, c2, -c4));
+    const float s0 = __fadd_rn(__fmaf_rn(-2.0f, c1, c0), c2), t0 = __fmaf_rn(3.0f, c2, __fmaf_rn(-4.0f, c1, c0));
+    const float s1 = __fadd_rn(__fmaf_rn(-2.0f, c2, c1), c3), t1 = __fsub_rn(c1, c3);
+    const float s2 = __fadd_rn(__fmaf_rn(-2.0f, c3, c2), c4), t2 = __fadd_rn(__fmaf_rn(-4.0f, c3, __fmul_rn(3.0f, c2)), c4);
+    constexpr float k = 13.0f / 12.0f;
+    const float b0 = __fmaf_rn(__fmul_rn(k, s0), s0, __fmul_rn(__fmul_rn(0.25f, t0), t0));
+    const float b1 = __fmaf_rn(__fmul_rn(k, s1), s1, __fmul_rn(__fmul_rn(0.25f, t1), t1));
+    const float b2 = __fmaf_rn(__fmul_rn(k, s2), s2, __fmul_rn(__fmul_rn(0.25f, t2), t2));
+    const float tau = fabsf(__fsub_rn(b0, b2));
+    const float a0 = __fmul_rn(0.1f, __fadd_rn(1.0f, tau / __fadd_rn(b0, eps)));
+    const float a1 = __fmul_rn(0.6f, __fadd_rn(1.0f, tau / __fadd_rn(b1, eps)));
+    const float a2 = __fmul_rn(0.3f, __fadd_rn(1.0f, tau / __fadd_rn(b2, eps)));
+    const float num = __fmaf_rn(a2, p2, __fmaf_rn(a1, p1, __fmul_rn(a0, p0)));
+    return num / __fmul_rn(6.0f, __fadd_rn(__fadd_rn(a0, a1), a2));
+}
 
 // ------------------------------------------------------------------ HLLC (Toro) with Einfeldt bounds (Schemes.cpp:116-200)
 template <typename T> __device__ __forceinline__ T safe_denom(T x) { return copysign(vmax(fabs(x), Num<T>::denom_eps), x); }

@@ -923,11 +923,11 @@ void build_tma_maps(fvg_run* r) {
     const EncodeTiled encode = reinterpret_cast<EncodeTiled>(fn);
     const cuuint64_t dims[4] = {(cuuint64_t)r->m.nx, (cuuint64_t)r->m.ny, (cuuint64_t)r->m.nz, 5};
     const cuuint64_t strides[3] = {(cuuint64_t)r->m.nx * 8, (cuuint64_t)r->m.nx * r->m.ny * 8, (cuuint64_t)r->m.plane * 8};
-    const cuuint32_t boxes[3][4] = {{16, 8, 8, 5}, {8, 14, 8, 5}, {8, 8, 14, 5}};
+    const cuuint32_t boxes[5][4] = {{16, 8, 8, 5}, {8, 14, 8, 5}, {8, 8, 14, 5}, {8, 3, 8, 5}, {8, 8, 3, 5}};   // (TmaMaps)
     const cuuint32_t es[4] = {1, 1, 1, 1};
     double* bufs[3] = {r->U, r->Ut, r->R};
     for (int b = 0; b < 3; ++b)
-        for (int a = 0; a < 3; ++a)
+        for (int a = 0; a < 5; ++a)
             if (encode(&r->tma[b].m[a], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, bufs[b], dims, strides, boxes[a], es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
                 return;

@@ -2,19 +2,21 @@
 // bulk tensor copy and of the shared-memory barrier that completes it.
 //
 // A state of nvar FP64 planes is a 4-D tensor (x, y, z, plane): dims (nx, ny, nz, nvar), byte strides (8 nx, 8 nx ny,
-// 8 plane). A stage sweep along axis a reads the 8x8x8 tile extended by 3 cells along a: on the x sweep the box is 16 x 8 x 8
-// starting at x = o - 4 (the start of a TMA box must lie on 16 bytes, an even cell index for 8-byte values), on the y and
-// z sweeps 8 x 14 x 8 and 8 x 8 x 14. Only tiles whose box lies inside the mesh use it (wrapped, ghost and forced cells
-// need the index-mapping loader), and no copy here ever multicasts.
+// 8 plane). The mixed stage kernel reads the 8x8x8 tile with 3 cells beyond its faces: a 16 x 8 x 8 box starting at
+// x = o - 4 (the tile and its x halos; the start of a TMA box must lie on 16 bytes, an even cell index for 8-byte
+// values), and either 8 x 14 x 8 / 8 x 8 x 14 boxes (the per-axis sweep) or 8 x 3 x 8 / 8 x 8 x 3 boxes (the halos of the
+// cross). Only boxes inside the mesh are copied (wrapped, ghost and forced cells need the index-mapping loader), and no
+// copy here ever multicasts.
 #pragma once
 
 #include <cuda.h>
 
 namespace fvg {
 
-// the maps of one state buffer for the x, y and z sweeps (passed to the kernel as a __grid_constant__ parameter)
+// the maps of one state buffer (passed to the kernel as a __grid_constant__ parameter): the 16 x 8 x 8 box, the per-axis
+// sweep's 8 x 14 x 8 and 8 x 8 x 14 boxes, the cross's 8 x 3 x 8 and 8 x 8 x 3 halo boxes
 struct TmaMaps {
-    CUtensorMap m[3];
+    CUtensorMap m[5];
 };
 
 namespace tma {
@@ -45,6 +47,8 @@ __device__ __forceinline__ void load_4d(void* dst, const CUtensorMap* map, int x
         "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(q), "r"(su32(bar))
         : "memory");
 }
+// the cache line of a global address towards L2 (a hint: no completion, no fault on an address the kernel owns)
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 }   // namespace tma
 
 }   // namespace fvg

@@ -102,4 +102,7 @@ def test_gate_keeps_weno_at_discontinuities():
     for r in (plain, mixed, gated):
         r.close()
     assert 0.2 < lin / ev < 1.0
-    assert d_g <= 1.5 * d_m + 1e-9
+    # a shock or contact reconstructed linearly would leave oscillations of the order of its jump along the tiles it
+    # crosses (an L1 distance of 1e-4 .. 1e-3 at this size); rounding moves the gated and the ungated run alike, by
+    # 1e-7 .. 3e-7 from the FP64 run: the gated run stays within 1e-6 of the ungated run's distance
+    assert d_g <= d_m + 1e-6
