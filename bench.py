@@ -65,7 +65,9 @@ def tgv_state(n, gamma=1.4):
 
 
 class Clocks:
-    """nvidia-smi samples of the SM clock and throttle reasons while the timed region runs."""
+    """nvidia-smi samples of the SM clock and throttle reasons while the timed region runs: the sampler is running (its
+    first line has arrived) before the region starts, samples every 50 ms, and only the lines that arrive inside the
+    region are kept."""
 
     FIELDS = ["clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
               "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
@@ -73,24 +75,40 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.lines = []
+        self.first = 0
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line)
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + ",".join(self.FIELDS), "--format=csv,noheader,nounits",
-                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                                          "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return self
+        self.reader = threading.Thread(target=self._read, daemon=True)
+        self.reader.start()
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 10 and self.proc.poll() is None:
+            time.sleep(0.005)
+        self.first = len(self.lines)
         return self
 
     def __exit__(self, *exc):
         self.out = ""
         if self.proc:
+            end = len(self.lines)
             self.proc.terminate()
             try:
-                self.out, _ = self.proc.communicate(timeout=5)
+                self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-                self.out, _ = self.proc.communicate()
+                self.proc.wait()
+            self.reader.join(timeout=5)
+            self.out = "".join(self.lines[self.first:end])
 
     def summary(self):
         sm, smax, reasons = [], 0.0, set()
@@ -828,10 +846,10 @@ def gpu_arm(args, world, rank, local):
                "timing": "host wall clock around fvg_step_host: pinned host state in, one step, pinned host state out"}
     mixed.close()
 
-    rl_l = roofline_of(tm_l, ms_l, cells, "mixed_stage_kernel<3, WENO5, LowMach, gated> (FP32 reconstruction (linear or WENO5-Z per tile) + "
-                       "Riemann + balance, FP64 RK update)", ncu_traffic(n, "mixed_stage_kernel_weno5_3d.json"),
-                       ncu_profile("mixed_stage_kernel_weno5_3d.json"))
-    rl_m = roofline_of(tm_m, ms_m, cells, "mixed_stage_kernel<3, WENO5, LowMach> (FP32 reconstruction + Riemann + balance, FP64 RK update)",
+    rl_l = roofline_of(tm_l, ms_l, cells, "mixed_stage_kernel_tma<LowMach, gated> (FP32 reconstruction, linear or WENO5-Z per tile-axis, + "
+                       "Riemann + balance, FP64 RK update; the cross form on tiles linear along every axis)",
+                       ncu_traffic(n, "mixed_stage_kernel_tma_gated_3d.json"), ncu_profile("mixed_stage_kernel_tma_gated_3d.json"))
+    rl_m = roofline_of(tm_m, ms_m, cells, "mixed_stage_kernel_tma<LowMach> (the per-axis sweep: FP32 WENO5-Z + Riemann + balance, FP64 RK update)",
                        ncu_traffic(n, "mixed_stage_kernel_weno5_3d.json"), ncu_profile("mixed_stage_kernel_weno5_3d.json"))
     rl_p = roofline_of(tm_p, ms_p, cells, "stage_kernel<3, WENO5, LowMach> (FP64, the reference's arithmetic)",
                        ncu_traffic(n, "stage_kernel_weno5_3d.json"), ncu_profile("stage_kernel_weno5_3d.json"))
