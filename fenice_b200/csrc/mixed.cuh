@@ -591,11 +591,13 @@ template <int TX, int TY, int TZ> struct MixedTmaShape {
 // Both forms give the bits of mixed_stage_kernel (the explicitly rounded lin5 / weno5z, balance and update), so a face
 // between tiles of the two forms gets one flux. A tile whose boxes would leave the mesh (wrapped or ghost cells) takes the
 // index-mapping loader for those parts. Measured at 256^3 (Taylor-Green, every tile-axis linear, with the viscous sums
-// and U0): 1.98 ms per launch for the cross against 2.12 ms for the per-axis sweep; with WENO5-Z along every axis the
+// and U0): 1.72 ms per launch for the cross against 2.12 ms for the per-axis sweep; with WENO5-Z along every axis the
 // per-axis sweep is the faster (2.74 against 3.01 ms: its (face, variable) items spread the WENO5-Z work finer).
-// Shared memory: the larger of the two layouts (72.9 KB), three CTAs of 384 threads per SM (at most 56 registers).
+// Shared memory: the larger of the two layouts (74.1 KB), three CTAs of 384 threads per SM (at most 56 registers).
 struct CrossShape {
-    static constexpr int NV = 5, NCORE = 512, NHALO = 192, NPC = NCORE + 6 * NHALO;   // cells of the cross
+    // slots of the cross: the tile's 512 cells in rows of 9 (576 slots: x + 9 y + 72 z, so that a warp reading one x
+    // column of 32 rows touches 32 banks), then the six 3-deep halos of 192 cells
+    static constexpr int NV = 5, NCORE = 576, NHALO = 192, NPC = NCORE + 6 * NHALO;
     static constexpr int NFA = 576, NFACE = 3 * NFA, NINNER = 448;                    // faces per axis; t = 1 .. 7
     static constexpr int BAR_OFF = 256, P_OFF = 272;
     static constexpr int STG_OFF = (P_OFF + 4 * NV * NPC + 127) / 128 * 128;
@@ -607,19 +609,20 @@ struct CrossShape {
 };
 
 // the cross's slot of the cell at s along axis A (s in [-3, 11)) and (u, v) along the other two axes in increasing
-// order: the tile's 512 cells (x fastest), then the six halos (axis-major, low side first), each 3 deep x 64 cells
+// order: the tile's cells (x + 9 y + 72 z), then the six halos (axis-major, low side first), each 3 deep x 64 cells
 template <int A> __device__ __forceinline__ int cross_slot(int s, int u, int v) {
-    if (s < 0) return 512 + (2 * A) * 192 + (s + 3) + 3 * (u + 8 * v);
-    if (s >= 8) return 512 + (2 * A + 1) * 192 + (s - 8) + 3 * (u + 8 * v);
-    return A == 0 ? s + 8 * u + 64 * v : (A == 1 ? u + 8 * s + 64 * v : u + 8 * v + 64 * s);
+    if (s < 0) return 576 + (2 * A) * 192 + (s + 3) + 3 * (u + 8 * v);
+    if (s >= 8) return 576 + (2 * A + 1) * 192 + (s - 8) + 3 * (u + 8 * v);
+    return A == 0 ? s + 9 * u + 72 * v : (A == 1 ? u + 9 * s + 72 * v : u + 9 * v + 72 * s);
 }
-// the tile-local cell of slot e (the inverse of cross_slot)
-__device__ __forceinline__ void cross_cell(int e, int l3[3]) {
+// cell e of the cross (the tile's 512 cells, x fastest, then the six halos of cross_slot's order): its tile-local
+// coordinates and its slot
+__device__ __forceinline__ int cross_cell(int e, int l3[3]) {
     if (e < 512) {
         l3[0] = e & 7;
         l3[1] = (e >> 3) & 7;
         l3[2] = e >> 6;
-        return;
+        return l3[0] + 9 * l3[1] + 72 * l3[2];
     }
     const int k = (e - 512) / 192, r = (e - 512) % 192, A = k >> 1;
     const int l = r % 3, uv = r / 3, u = uv & 7, v = uv >> 3;
@@ -627,6 +630,7 @@ __device__ __forceinline__ void cross_cell(int e, int l3[3]) {
     l3[0] = A == 0 ? s : u;
     l3[1] = A == 0 ? u : (A == 1 ? s : v);
     l3[2] = A == 2 ? s : v;
+    return e + 64;
 }
 
 // One face of axis A in the cross (linear face values): item r of the axis (the 448 faces inside the tile, t = 1 .. 7,
@@ -636,15 +640,19 @@ __device__ __forceinline__ void cross_face(const StageArgs& a, const Eos<float>&
                                            int r, const int o3[3], float& smax) {
     constexpr int NV = 5, NPC = CrossShape::NPC;
     int t, u, v;
-    if (r < CrossShape::NINNER) {
+    if (r < CrossShape::NINNER) {   // (the lanes of a warp run along the cross's rows: no two on one bank)
         if (A == 0) {
             t = 1 + r % 7;
             u = (r / 7) & 7;
             v = r / 56;
-        } else {
+        } else if (A == 1) {
             u = r & 7;
             t = 1 + (r >> 3) % 7;
             v = (r >> 3) / 7;
+        } else {
+            u = r & 7;
+            v = (r >> 3) & 7;
+            t = 1 + (r >> 6);
         }
     } else {
         const int q = r - CrossShape::NINNER;
@@ -721,14 +729,14 @@ __device__ __forceinline__ void cross_tile(const StageArgs& a, const TmaMaps& ma
         if (!done && tid == 0) atomicExch(const_cast<int*>(&a.ctl->status), 5);
         return done;
     };
-    // slots e0 .. e1 of the cross by index mapping (wrapped and ghost cells), the primitive state recovered in FP64
+    // cells e0 .. e1 of the cross by index mapping (wrapped and ghost cells), the primitive state recovered in FP64
     auto load_slots = [&](int e0, int e1) {
         for (int e = e0 + tid; e < e1; e += NT) {
             int l3[3];
-            cross_cell(e, l3);
+            const int p = cross_cell(e, l3);
             const St<double, NV> w = c2p(a.eos, stencil_cons<3, NV, false>(m, a.bc, a.eos, a.U, o3[0] + l3[0], o3[1] + l3[1], o3[2] + l3[2]));
 #pragma unroll
-            for (int q = 0; q < NV; ++q) P[q * NPC + e] = (float)w[q];
+            for (int q = 0; q < NV; ++q) P[q * NPC + p] = (float)w[q];
         }
     };
     // the epilogue's operands that no box brings in (the tile's rows of U0 and of the viscous sums) head for L2 now
@@ -741,7 +749,7 @@ __device__ __forceinline__ void cross_tile(const StageArgs& a, const TmaMaps& ma
             if (q >= 5 && a.Rvf) tma::prefetch_l2(a.Rvf + (q - 5) * m.plane + row);
         }
     }
-    // ---- 1. the tile and its x halos (slots 0 .. 895): one 16 x 8 x 8 box from x = o - 4
+    // ---- 1. the tile and its x halos (cells 0 .. 895): one 16 x 8 x 8 box from x = o - 4
     if (aligned && o3[0] >= 4 && o3[0] + 12 <= n3[0] && o3[1] + 8 <= n3[1] && o3[2] + 8 <= n3[2]) {
         if (tid == 0) {
             tma::fence_proxy_async();
@@ -764,7 +772,7 @@ __device__ __forceinline__ void cross_tile(const StageArgs& a, const TmaMaps& ma
         load_slots(0, 896);
     }
     __syncthreads();
-    // ---- 2. the y and z halos (slots 896 .. 1663): four 3-deep boxes on one barrier phase
+    // ---- 2. the y and z halos (cells 896 .. 1663): four 3-deep boxes on one barrier phase
     if (aligned && o3[1] >= 3 && o3[1] + 11 <= n3[1] && o3[2] >= 3 && o3[2] + 11 <= n3[2] && o3[0] + 8 <= n3[0]) {
         if (tid == 0) {
             tma::fence_proxy_async();
@@ -796,7 +804,7 @@ __device__ __forceinline__ void cross_tile(const StageArgs& a, const TmaMaps& ma
             for (int q = 0; q < NV; ++q) P[q * NPC + p] = (float)w[q];
         }
     } else {
-        load_slots(896, NPC);
+        load_slots(896, 1664);
     }
     __syncthreads();
     // ---- 3. every face of the three axes (the faces inside the tile first, 448 per axis, then the seam layers)
