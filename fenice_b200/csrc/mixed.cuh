@@ -530,6 +530,12 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
             for (int x = 0; x < 4; ++x) Fv[x * S::NF + f] = out[x];
         }
         __syncthreads();
+    };
+    // the balance of one axis into acc: each thread its own cells (the same ones in every call and in the epilogue), so it
+    // shares a phase with the next axis's gradients (disjoint arrays) and needs no barrier before the epilogue
+    auto balance = [&](auto axis_c) {
+        constexpr int d = decltype(axis_c)::value;
+        constexpr int Fd[3] = {TX + (d == 0), TY + (d == 1), TZ + (d == 2)};
         for (int c = tid; c < NC; c += NT) {
             const int c3[3] = {c % TX, (c / TX) % TY, c / (TX * TY)};
             const int fl = (c3[2] * Fd[1] + c3[1]) * Fd[0] + c3[0];
@@ -540,11 +546,13 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
                 acc[q * NC + c] = d == 0 ? dif : acc[q * NC + c] + dif;
             }
         }
-        __syncthreads();
     };
     sweep(std::integral_constant<int, 0>{});
+    balance(std::integral_constant<int, 0>{});
     sweep(std::integral_constant<int, 1>{});
+    balance(std::integral_constant<int, 1>{});
     sweep(std::integral_constant<int, 2>{});
+    balance(std::integral_constant<int, 2>{});
     double smax = 0.0;
     const float gm1 = (float)(a.eos.gamma - 1.0);
     for (int c = tid; c < NC; c += NT) {

@@ -318,7 +318,8 @@ __global__ void __launch_bounds__(NT) viscous_kernel(const ViscArgs a) {
                 acc[q * NC + c] = d == 0 ? 0.0 + dif : acc[q * NC + c] + dif;
             }
         }
-        __syncthreads();
+        // (no barrier: each thread balances its own cells, the same ones in every sweep and in the epilogue, and the
+        // next sweep's gradients touch neither Fv nor acc; its faces come after its own barrier)
     };
     sweep(std::integral_constant<int, 0>{});
     sweep(std::integral_constant<int, 1>{});
