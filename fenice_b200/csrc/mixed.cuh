@@ -366,33 +366,38 @@ __global__ void __launch_bounds__(NT) mixed_stage_kernel(const StageArgs a) {
 
 template <int TX, int TY, int TZ> struct MixedViscShape {
     static constexpr int NC = TX * TY * TZ;
-    // red [32 doubles], floats: B [5][NB] box (rho, u, v, w, T), G [4][NE], F [4][NF], acc [4][NC] (the momentum and
-    // energy balances; the mass balance is 0): 4 CTAs of the 8x8x8 tile fit on an SM
+    // red [32 doubles], then float4 arrays: V [NB] box (u, v, w, T), G [NE] (the sweep's four gradient entries), F [NF]
+    // (the four face fluxes: rho u, rho v, rho E, rho w; the mass flux is 0), acc [NC] (the four balances); then R [NB]
+    // floats (the box's rho): 4 CTAs of the 8x8x8 tile fit on an SM
     static constexpr int BX = TX + 2, BY = TY + 2, BZ = TZ + 2, NB = BX * BY * BZ;
     static constexpr int cmax(int x, int y) { return x > y ? x : y; }
     static constexpr int NE = cmax(cmax((TX + 2) * TY * TZ, TX * (TY + 2) * TZ), TX * TY * (TZ + 2));
     static constexpr int NF = cmax(cmax((TX + 1) * TY * TZ, TX * (TY + 1) * TZ), TX * TY * (TZ + 1));
-    static constexpr int SMEM_FLOATS = 64 + 5 * NB + 4 * NE + 4 * NF + 4 * NC;
-    static constexpr size_t SMEM_BYTES = sizeof(float) * SMEM_FLOATS;
+    static constexpr size_t SMEM_BYTES = 256 + 16 * (NB + NE + NF + NC) + 4 * NB;
 };
+// component a (0 u, 1 v, 2 w, 3 T) of a box position's float4
+__device__ __forceinline__ float f4c(float4 v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : (a == 2 ? v.z : v.w)); }
 // The mixed-precision viscous kernel: viscous_kernel's phases in FP32; the padded state is read in FP64 and each box
 // position's velocity and T = p / rho come from an FP64 pressure recovery. The velocity gradients
 // G[a][b] = (d(rho u_a)/dx_b - u_a d(rho)/dx_b) / rho take the box's rho and u_a: (rho+ (u_a+ - u_a) - rho- (u_a- - u_a))
 // / (2 h_b rho), the same difference in exact arithmetic. A tile none of whose sides is a wall, inlet or outlet (only
 // periodic sides and part interfaces around it) reads its box without the ghost rules and solves its faces without the
-// wall tests; a tile wholly inside the mesh skips the test for faces beyond it. Measured at 256^3 (Taylor-Green): 0.89 ms
-// per launch against 1.14 ms for the previous form (rho u_a in the box, 1 / rho, the general path for every tile), the
-// same distance from the FP64 viscous residual (1.24e-3 of its largest value, both).
+// wall tests; a tile wholly inside the mesh skips the test for faces beyond it. The four values a position, a face or a
+// cell carries sit together in one float4 (one shared-memory access each); each axis's balance shares a phase with the
+// next axis's gradients (six barriers per tile). Measured at 256^3 (Taylor-Green): 0.89 ms per launch against 1.14 ms for
+// the first form (rho u_a in the box, 1 / rho, the general path for every tile), the same distance from the FP64 viscous
+// residual (1.24e-3 of its largest value, both).
 template <int TX, int TY, int TZ, int NT>
 __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
     using S = MixedViscShape<TX, TY, TZ>;
     constexpr int NC = S::NC, BX = S::BX, BY = S::BY, NB = S::NB;
     extern __shared__ double smem_d[];
     double* red = smem_d;
-    float* B = reinterpret_cast<float*>(smem_d + 32);   // [5][NB]: rho, u, v, w, T
-    float* G = B + 5 * NB;
-    float* Fv = G + 4 * S::NE;
-    float* acc = Fv + 4 * S::NF;
+    float4* V = reinterpret_cast<float4*>(smem_d + 32);   // [NB]: u, v, w, T
+    float4* G = V + NB;
+    float4* Fv = G + S::NE;
+    float4* acc = Fv + S::NF;
+    float* R = reinterpret_cast<float*>(acc + NC);         // [NB]: rho
     if (!*a.gate) return;
     const Mesh& m = a.m;
     const int tid = threadIdx.x, b = blockIdx.x + a.b0;
@@ -418,11 +423,8 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
         const St<double, 5> u = walls ? padded_cons(a, g[0], g[1], g[2]) : cell_at(a, g[0], g[1], g[2]);
         double inv;
         const St<double, 5> w = c2p(a.eos, u, inv);
-        B[0 * NB + e] = (float)u[0];
-        B[1 * NB + e] = (float)w[1];
-        B[2 * NB + e] = (float)w[2];
-        B[3 * NB + e] = (float)w[4];
-        B[4 * NB + e] = (float)(w[3] * inv);
+        R[e] = (float)u[0];
+        V[e] = make_float4((float)w[1], (float)w[2], (float)w[4], (float)(w[3] * inv));
     }
     __syncthreads();
     auto sweep = [&](auto axis_c) {
@@ -437,20 +439,22 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
             int l[3] = {e % E[0], (e / E[0]) % E[1], e / (E[0] * E[1])};
             l[d] -= 1;
             const int p = bidx(l[0], l[1], l[2]);
-            const float rc = B[p];
+            const float rc = R[p];
             const float inv_rho = 1.0f / vmax(rc, Num<float>::eos_eps);
-            const float rp0 = B[p + off0], rm0 = B[p - off0], rp1 = B[p + off1], rm1 = B[p - off1];
+            const float rp0 = R[p + off0], rm0 = R[p - off0], rp1 = R[p + off1], rm1 = R[p - off1];
+            const float4 vc = V[p], vp0 = V[p + off0], vm0 = V[p - off0], vp1 = V[p + off1], vm1 = V[p - off1];
             const float i20 = 0.5f / h[b0], i21 = 0.5f / h[b1];
+            float gs[4];
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
                 const int ga = GA[d][s];
                 const bool first = GB[d][s] == b0;
-                const int off = first ? off0 : off1;
-                const float uc = B[(1 + ga) * NB + p];
-                const float up = B[(1 + ga) * NB + p + off], um = B[(1 + ga) * NB + p - off];
+                const float uc = f4c(vc, ga);
+                const float up = first ? f4c(vp0, ga) : f4c(vp1, ga), um = first ? f4c(vm0, ga) : f4c(vm1, ga);
                 const float rp = first ? rp0 : rp1, rm = first ? rm0 : rm1;
-                G[s * S::NE + e] = (rp * (up - uc) - rm * (um - uc)) * (first ? i20 : i21) * inv_rho;
+                gs[s] = (rp * (up - uc) - rm * (um - uc)) * (first ? i20 : i21) * inv_rho;
             }
+            G[e] = make_float4(gs[0], gs[1], gs[2], gs[3]);
         }
         __syncthreads();
         const float area = (float)m.area[d];
@@ -486,27 +490,31 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
             }
             if (inside) {
                 float Gc[4];
+                if (phys) {
 #pragma unroll
-                for (int s = 0; s < 4; ++s) {
-                    if (phys) {
+                    for (int s = 0; s < 4; ++s) {
                         const int ga = GA[d][s], gb = GB[d][s];
                         const int pg = lo ? pL : pR, pc = lo ? pR : pL;
                         const int off = gb == 0 ? 1 : (gb == 1 ? BX : BX * BY);
-                        const float fp = 0.5f * (B[(1 + ga) * NB + pg + off] + B[(1 + ga) * NB + pc + off]);
-                        const float fm = 0.5f * (B[(1 + ga) * NB + pg - off] + B[(1 + ga) * NB + pc - off]);
+                        const float fp = 0.5f * (f4c(V[pg + off], ga) + f4c(V[pc + off], ga));
+                        const float fm = 0.5f * (f4c(V[pg - off], ga) + f4c(V[pc - off], ga));
                         Gc[s] = (fp - fm) * (0.5f / h[gb]);
-                    } else {
-                        Gc[s] = 0.5f * (G[s * S::NE + xL] + G[s * S::NE + xR]);
                     }
+                } else {
+                    const float4 gl = G[xL], gr = G[xR];
+                    Gc[0] = 0.5f * (gl.x + gr.x);
+                    Gc[1] = 0.5f * (gl.y + gr.y);
+                    Gc[2] = 0.5f * (gl.z + gr.z);
+                    Gc[3] = 0.5f * (gl.w + gr.w);
                 }
+                const float4 vl = V[pL], vr = V[pR];
                 float Gn[3], vf[3];
 #pragma unroll
                 for (int x = 0; x < 3; ++x) {
-                    const float vl = B[(1 + x) * NB + pL], vr = B[(1 + x) * NB + pR];
-                    Gn[x] = (vr - vl) * inv_h;
-                    vf[x] = 0.5f * (vl + vr);
+                    Gn[x] = (f4c(vr, x) - f4c(vl, x)) * inv_h;
+                    vf[x] = 0.5f * (f4c(vl, x) + f4c(vr, x));
                 }
-                const float dT = (B[4 * NB + pR] - B[4 * NB + pL]) * inv_h;
+                const float dT = (vr.w - vl.w) * inv_h;
                 float tau[3];
                 if (d == 0) {
                     tau[0] = mu * ((4.0f / 3.0f) * Gn[0] - (2.0f / 3.0f) * (Gc[1] + Gc[2]));
@@ -526,8 +534,7 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
                 out[2] = (vf[0] * tau[0] + vf[1] * tau[1] + vf[2] * tau[2] + kc * dT) * area;
                 out[3] = tau[2] * area;
             }
-#pragma unroll
-            for (int x = 0; x < 4; ++x) Fv[x * S::NF + f] = out[x];
+            Fv[f] = make_float4(out[0], out[1], out[2], out[3]);
         }
         __syncthreads();
     };
@@ -540,10 +547,13 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
             const int c3[3] = {c % TX, (c / TX) % TY, c / (TX * TY)};
             const int fl = (c3[2] * Fd[1] + c3[1]) * Fd[0] + c3[0];
             const int fr = fl + (d == 0 ? 1 : (d == 1 ? Fd[0] : Fd[0] * Fd[1]));
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const float dif = Fv[q * S::NF + fr] - Fv[q * S::NF + fl];
-                acc[q * NC + c] = d == 0 ? dif : acc[q * NC + c] + dif;
+            const float4 l = Fv[fl], r = Fv[fr];
+            const float4 dif = make_float4(r.x - l.x, r.y - l.y, r.z - l.z, r.w - l.w);
+            if (d == 0) {
+                acc[c] = dif;
+            } else {
+                const float4 s = acc[c];
+                acc[c] = make_float4(s.x + dif.x, s.y + dif.y, s.z + dif.z, s.w + dif.w);
             }
         }
     };
@@ -560,13 +570,17 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
         const int g3[3] = {o3[0] + c3[0], o3[1] + c3[1], o3[2] + c3[2]};
         if (g3[0] >= m.nx || g3[1] >= m.ny || g3[2] >= m.nz) continue;
         const long long cell = ((long long)g3[2] * m.ny + g3[1]) * m.nx + g3[0];
-#pragma unroll
-        for (int q = 1; q < 5; ++q) a.Rvf[(q - 1) * m.plane + cell] = acc[(q - 1) * NC + c];
+        const float4 s4 = acc[c];
+        a.Rvf[cell] = s4.x;
+        a.Rvf[m.plane + cell] = s4.y;
+        a.Rvf[2 * m.plane + cell] = s4.z;
+        a.Rvf[3 * m.plane + cell] = s4.w;
         const int p = bidx(c3[0], c3[1], c3[2]);
-        const float rho = vmax(B[p], Num<float>::eos_eps);
-        const float T = B[4 * NB + p];
+        const float rho = vmax(R[p], Num<float>::eos_eps);
+        const float4 v = V[p];
+        const float T = v.w;
         const float nu_eff = vmax((4.0f / 3.0f) * (mu / rho), (kc * gm1) / rho) + 1e-12f;
-        const float vm = vmax(vmax(fabsf(B[NB + p]), fabsf(B[2 * NB + p])), fabsf(B[3 * NB + p]));
+        const float vm = vmax(vmax(fabsf(v.x), fabsf(v.y)), fabsf(v.z));
         const float cs = sqrtf((float)a.eos.gamma * (T + (float)a.eos.p_inf / rho));
         const double s = (double)(vm + cs + 2.0f * (float)a.L * (float)a.inv_h2 * nu_eff);
         if (s > smax) smax = s;
