@@ -1,5 +1,6 @@
 // The mixed-precision kernels' translation unit (see mixed.cuh). Built with --use_fast_math: FP32 division and square
-// root are the fast approximations and multiplies and adds contract into FMAs; FP64 arithmetic keeps IEEE rounding.
+// root are the fast approximations and multiplies and adds may contract into FMAs, except where mixed.cuh rounds each
+// operation explicitly (the face values, the balance, the FP64 update); FP64 division and square root stay IEEE.
 #include "mixed.cuh"
 #include "mixed_api.h"
 

@@ -5,7 +5,9 @@
 // pressure recovery p = (gamma - 1)(E - 1/2 rho |u|^2) of every cell (cons_to_prim in double when a cell is loaded, so a
 // low-Mach cell, where E and the kinetic energy nearly cancel, loses nothing). What runs in FP32 (compiled with fast
 // single-precision division and square root, and contraction into FMAs): the WENO-Z / MUSCL reconstruction of the
-// primitives, the Riemann solver, the flux balance, the viscous stresses and heat flux.
+// primitives, the Riemann solver, the flux balance, the viscous stresses and heat flux. The linear and WENO5-Z face values,
+// the balance and the FP64 update round every operation explicitly instead, so that every kernel that solves a face or
+// updates a cell (the per-axis sweep, the cross form, the batched kernels) gives it the same bits.
 //
 // One algorithmic difference from the plain form: the Riemann solver takes the reconstructed primitive states directly
 // (their density and pressure floored as cons_to_prim floors them) instead of converting them to conservative form and
