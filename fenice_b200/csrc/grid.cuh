@@ -359,6 +359,9 @@ __device__ __forceinline__ double warp_max(double v) {
     return v;
 }
 
+// the cache line of a global address towards L2 (a hint: no completion, no fault on an address the kernel owns)
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 template <int NT> __device__ __forceinline__ double block_max(double v, double* red) {
     v = warp_max(v);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

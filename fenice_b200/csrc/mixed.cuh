@@ -738,8 +738,8 @@ template <int NT> __device__ __forceinline__ void prefetch_epilogue(const StageA
         const int q = k >> 6, y = o3[1] + (k & 7), z = o3[2] + ((k >> 3) & 7);
         if (y >= m.ny || z >= m.nz) continue;
         const long long row = ((long long)z * m.ny + y) * m.nx + o3[0];
-        if (q < 5 && a.mode == kCombine) tma::prefetch_l2(a.U0 + q * m.plane + row);
-        if (q >= 5 && a.Rvf) tma::prefetch_l2(a.Rvf + (q - 5) * m.plane + row);
+        if (q < 5 && a.mode == kCombine) prefetch_l2(a.U0 + q * m.plane + row);
+        if (q >= 5 && a.Rvf) prefetch_l2(a.Rvf + (q - 5) * m.plane + row);
     }
 }
 

@@ -235,6 +235,23 @@ __device__ __forceinline__ void stage_axis(const StageArgs& a, double* __restric
 
 // FULL = false: a run without part interfaces, non-reflecting sides, the positivity fallback or the body force (their
 // code compiled out of the hot loop: a branch never taken still costs the others registers and instruction fetch).
+// The epilogue's operands that no sweep reads (the tile's rows of U0 and of the viscous residual) head for L2 at the
+// start of the tile, so that the epilogue's loads find them there; the arithmetic is untouched.
+template <int NV, int TX, int TY, int TZ, int NT> __device__ __forceinline__ void prefetch_tile_rows(const StageArgs& a, const int o3[3]) {
+    const bool u0 = a.mode == kCombine, rv = a.Rv != nullptr;
+    if (!u0 && !rv) return;
+    const Mesh& m = a.m;
+    constexpr int R = TY * TZ;   // rows of TX cells
+    for (int k = threadIdx.x; k < 2 * NV * R; k += NT) {
+        const int which = k / (NV * R), q = (k / R) % NV, r = k % R;
+        const int y = o3[1] + r % TY, z = o3[2] + r / TY;
+        if (y >= m.ny || z >= m.nz) continue;
+        const long long row = ((long long)z * m.ny + y) * m.nx + o3[0];
+        if (which == 0 && u0) prefetch_l2(a.U0 + q * m.plane + row);
+        if (which == 1 && rv) prefetch_l2(a.Rv + q * m.plane + row);
+    }
+}
+
 template <int DIM, int RECON, int RIEMANN, int TX, int TY, int TZ, int NT, bool FULL = true>
 __global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
     using S = StageShape<DIM, RECON, TX, TY, TZ>;
@@ -254,6 +271,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
     const int t0 = b % a.tiles[0], t1 = (b / a.tiles[0]) % a.tiles[1], t2 = b / (a.tiles[0] * a.tiles[1]);
     const int o3[3] = {t0 * TX, t1 * TY, t2 * TZ};
     double smax = 0.0;
+    prefetch_tile_rows<NV, TX, TY, TZ, NT>(a, o3);
 
     stage_axis<0, DIM, RECON, RIEMANN, TX, TY, TZ, NT, FULL>(a, P, WL, WR, acc, Sf, o3, smax);
     stage_axis<1, DIM, RECON, RIEMANN, TX, TY, TZ, NT, FULL>(a, P, WL, WR, acc, Sf, o3, smax);

@@ -47,8 +47,6 @@ __device__ __forceinline__ void load_4d(void* dst, const CUtensorMap* map, int x
         "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(q), "r"(su32(bar))
         : "memory");
 }
-// the cache line of a global address towards L2 (a hint: no completion, no fault on an address the kernel owns)
-__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 }   // namespace tma
 
 }   // namespace fvg
