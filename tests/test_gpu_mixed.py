@@ -1,6 +1,6 @@
 """The mixed-precision form (FP32 stencil, flux and viscous arithmetic; FP64 state accumulation and pressure recovery)
-against the plain FP64 form, which the other tests pin bit for bit to the reference. The bar is the north-star one: L1
-density error <= 1e-4 relative to the FP64 result; every field's relative L1 and Linf distances are printed per case."""
+against the plain FP64 form, which the other tests pin bit for bit to the reference. The bar the mixed form is held to:
+L1 density error <= 1e-4 relative to the FP64 result; every field's relative L1 and Linf distances are printed per case."""
 import math
 
 import numpy as np
