@@ -42,8 +42,7 @@ __device__ __forceinline__ void thin_y_mixed(const StageArgs& a, const Eos<float
         if (s_t > smax) smax = s_t;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const float d = __fmul_rn(Ft[q] - Fb[q], A);   // (rounded explicitly, as mixed_axis's balance)
-            acc[q * TX + c] = __fsub_rn(acc[q * TX + c], d);
+            acc[q * TX + c] = __fmaf_rn(-(Ft[q] - Fb[q]), A, acc[q * TX + c]);   // (an explicit FMA, as mixed_axis's balance)
         }
     }
     __syncthreads();

@@ -286,10 +286,10 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
             const int fl = (c3[2] * Fd[1] + c3[1]) * Fd[0] + c3[0];
             const int fr = fl + (axis == 0 ? 1 : (axis == 1 ? Fd[0] : Fd[0] * Fd[1]));
 #pragma unroll
-            for (int q = 0; q < NV; ++q) {   // (rounded products and differences, never contracted: every kernel of
-                                               // the mixed form sums a cell's balance to the same bits)
-                const float d = __fmul_rn(WL[q * S::NF + fr] - WL[q * S::NF + fl], A);
-                acc[q * NC + c] = axis == 0 ? -d : __fsub_rn(acc[q * NC + c], d);
+            for (int q = 0; q < NV; ++q) {   // (explicit FMAs, never left to the compiler: every kernel of the mixed
+                                               // form sums a cell's balance to the same bits)
+                const float df = WL[q * S::NF + fr] - WL[q * S::NF + fl];
+                acc[q * NC + c] = axis == 0 ? -__fmul_rn(df, A) : __fmaf_rn(-df, A, acc[q * NC + c]);
             }
         }
         __syncthreads();
@@ -297,9 +297,9 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
 }
 
 // The epilogue of the mixed form. A cell's global operands (U, U0, the viscous residual) are loaded first, all variables
-// at once, so that their latency overlaps; then every FP64 product and sum is rounded by an explicit intrinsic (nothing
-// left for a compiler pass to contract one way in one kernel and another way in the next: each kernel that updates a
-// cell gives it the same bits).
+// at once, so that their latency overlaps; then every FP64 operation is an explicit intrinsic, FMAs placed by hand
+// (nothing left for a compiler pass to contract one way in one kernel and another way in the next: each kernel that
+// updates a cell gives it the same bits).
 template <int NV> struct CellIn {
     double u[NV], u0[NV], rv[NV];
 };
@@ -317,13 +317,13 @@ template <int NV> __device__ __forceinline__ void cell_load(const StageArgs& a, 
 template <int NV> __device__ __forceinline__ double cell_out(const StageArgs& a, const CellIn<NV>& in, int q, float sum, double dt) {
     double r = __dmul_rn((double)sum, a.m.inv_cell);
     if (a.Rvf)
-        r = q == 0 ? __dadd_rn(r, 0.0) : __dadd_rn(r, __dmul_rn(in.rv[q], a.m.inv_cell));
+        r = q == 0 ? __dadd_rn(r, 0.0) : __fma_rn(in.rv[q], a.m.inv_cell, r);
     else if (a.Rv)
         r = __dadd_rn(r, in.rv[q]);
     if (a.mode == kStoreR) return r;
-    const double u = __dadd_rn(in.u[q], __dmul_rn(dt, r));
+    const double u = __fma_rn(dt, r, in.u[q]);
     if (a.mode == kAxpy) return u;
-    return __dadd_rn(__dmul_rn(a.ca, in.u0[q]), __dmul_rn(a.cb, u));
+    return __fma_rn(a.ca, in.u0[q], __dmul_rn(a.cb, u));
 }
 
 // The mixed-precision stage kernel: the tile sweep of stage_kernel (same phases, same launch geometry) with FP32 stencil
@@ -873,8 +873,8 @@ __device__ __forceinline__ void cross_tile(const StageArgs& a, const TmaMaps& ma
             const float* Y = Fs + (1 * NV + q) * L::NFA;
             const float* Z = Fs + (2 * NV + q) * L::NFA;
             float acc = -__fmul_rn(X[fx + 1] - X[fx], Ax);
-            acc = __fsub_rn(acc, __fmul_rn(Y[fy + 8] - Y[fy], Ay));
-            acc = __fsub_rn(acc, __fmul_rn(Z[fz + 64] - Z[fz], Az));
+            acc = __fmaf_rn(-(Y[fy + 8] - Y[fy]), Ay, acc);
+            acc = __fmaf_rn(-(Z[fz + 64] - Z[fz]), Az, acc);
             a.out[q * m.plane + cell] = cell_out(a, in, q, acc, dt);
         }
     }
