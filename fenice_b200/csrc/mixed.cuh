@@ -705,22 +705,10 @@ __device__ __forceinline__ void cross_face(const StageArgs& a, const Eos<float>&
     St<float, NV> F;
 #pragma unroll
     for (int q = 0; q < NV; ++q) F[q] = 0.0f;
+    // (no face of a tile in the cross form lies on a side without a halo: the gate keeps every tile whose extension along
+    // an axis leaves the mesh across a side that is not periodic WENO5-Z along that axis, so such a tile never takes the
+    // cross form; mixed_axis's first-order side states are not needed here)
     if (inside) {
-        const int tg = g3[A];
-        const bool lo_face = tg == 0 && a.bc.halo[2 * A] == kHaloNone;
-        const bool hi_face = tg == n3[A] && a.bc.halo[2 * A + 1] == kHaloNone;
-        if (lo_face || hi_face) {   // a side without a halo: the first-order side states, as mixed_axis
-            int c3[3] = {g3[0], g3[1], g3[2]};
-            if (hi_face) c3[A] = n3[A] - 1;
-            St<double, NV> UL, UR;
-            side_states<NV, false>(m, a.bc, a.eos, a.U, lo_face ? 2 * A : 2 * A + 1, c3[0], c3[1], c3[2], UL, UR);
-            const St<double, NV> dl = c2p(a.eos, UL), dr = c2p(a.eos, UR);
-#pragma unroll
-            for (int q = 0; q < NV; ++q) {
-                wl[q] = (float)dl[q];
-                wr[q] = (float)dr[q];
-            }
-        }
         const float sp = face_flux_prim<RIEMANN>(ef, sb, wl, wr, A, F);
         if (sp > smax) smax = sp;
     }
