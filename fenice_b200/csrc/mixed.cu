@@ -94,14 +94,24 @@ MixedStage mixed_stage_gated(int dim, int riemann, bool full) {
     return full ? pick_gated<2, true>(riemann) : pick_gated<2, false>(riemann);
 }
 
-// the FP32 viscous sweep: 384 threads per 8x8x8 tile (1.15 ms per launch at 256^3 against 1.28 with 192 threads)
+// the FP32 viscous sweep: 384 threads per 8x8x8 tile (1.15 ms per launch at 256^3 against 1.28 with 192 threads); the
+// instantiation without the ghost rules and wall tests when every side of the launch is periodic or a part interface
 constexpr int kMixedViscNT = 384;
 cudaError_t mixed_viscous_prepare() {
-    return cudaFuncSetAttribute(mixed_viscous_kernel<8, 8, 8, kMixedViscNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)MixedViscShape<8, 8, 8>::SMEM_BYTES);
+    cudaError_t e = cudaFuncSetAttribute(mixed_viscous_kernel<8, 8, 8, kMixedViscNT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)MixedViscShape<8, 8, 8>::SMEM_BYTES);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(mixed_viscous_kernel<8, 8, 8, kMixedViscNT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)MixedViscShape<8, 8, 8>::SMEM_BYTES);
+    return e;
 }
 cudaError_t mixed_viscous_launch(const ViscArgs& a, int nblocks, cudaStream_t s) {
-    mixed_viscous_kernel<8, 8, 8, kMixedViscNT><<<nblocks, kMixedViscNT, MixedViscShape<8, 8, 8>::SMEM_BYTES, s>>>(a);
+    bool walls = false;
+    for (int side = 0; side < 6; ++side) walls = walls || !a.through[side];
+    if (walls)
+        mixed_viscous_kernel<8, 8, 8, kMixedViscNT, true><<<nblocks, kMixedViscNT, MixedViscShape<8, 8, 8>::SMEM_BYTES, s>>>(a);
+    else
+        mixed_viscous_kernel<8, 8, 8, kMixedViscNT, false><<<nblocks, kMixedViscNT, MixedViscShape<8, 8, 8>::SMEM_BYTES, s>>>(a);
     return cudaGetLastError();
 }
 

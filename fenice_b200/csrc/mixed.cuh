@@ -136,7 +136,7 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
             l3[axis] -= H;
             const St<double, NV> w = c2p(a.eos, stencil_cons<DIM, NV, FULL>(m, a.bc, a.eos, a.U, o3[0] + l3[0], o3[1] + l3[1], o3[2] + l3[2]));
             if constexpr (RECON == kWeno5)
-                if (a.bc.solid) Sf[e] = stencil_solid<DIM>(m, a.bc, o3[0] + l3[0], o3[1] + l3[1], o3[2] + l3[2]);
+                if (!TMA && a.bc.solid) Sf[e] = stencil_solid<DIM>(m, a.bc, o3[0] + l3[0], o3[1] + l3[1], o3[2] + l3[2]);
 #pragma unroll
             for (int q = 0; q < NV; ++q) P[q * S::EXT + e] = (float)w[q];
         }
@@ -182,7 +182,7 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
                 const float c0 = c[0], c1 = c[sstride], c2 = c[2 * sstride], c3 = c[3 * sstride], c4 = c[4 * sstride], c5 = c[5 * sstride];
                 const int base = (f3[2] * E[1] + f3[1]) * E[0] + f3[0];
                 bool four = false;
-                if (a.bc.solid)
+                if (!TMA && a.bc.solid)   // (the TMA kernel never runs with an immersed body)
 #pragma unroll
                     for (int s6 = 0; s6 < 6; ++s6) four = four || Sf[base + s6 * sstride] != 0;
                 if (four) {
@@ -221,7 +221,7 @@ __device__ __forceinline__ void mixed_axis(const StageArgs& a, const Eos<float>&
                     const float* c = P + q * S::EXT + base;
                     const float c0 = c[0], c1 = c[sstride], c2 = c[2 * sstride], c3 = c[3 * sstride], c4 = c[4 * sstride], c5 = c[5 * sstride];
                     bool four = false;
-                    if (a.bc.solid)
+                    if (!TMA && a.bc.solid)   // (the TMA kernel never runs with an immersed body)
 #pragma unroll
                         for (int s6 = 0; s6 < 6; ++s6) four = four || Sf[base + s6 * sstride] != 0;
                     float wl, wr;
@@ -389,8 +389,10 @@ __device__ __forceinline__ float f4c(float4 v, int a) { return a == 0 ? v.x : (a
 // next axis's gradients (six barriers per tile). Measured at 256^3 (Taylor-Green): 0.89 ms per launch against 1.14 ms for
 // the first form (rho u_a in the box, 1 / rho, the general path for every tile), the same distance from the FP64 viscous
 // residual (1.24e-3 of its largest value, both).
-template <int TX, int TY, int TZ, int NT>
-__global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
+// WALLS = false: a launch whose every side is periodic or a part interface (no wall, inlet or outlet anywhere): the ghost
+// rules and the wall tests are compiled out.
+template <int TX, int TY, int TZ, int NT, bool WALLS = true>
+__global__ void __launch_bounds__(NT, 4) mixed_viscous_kernel(const ViscArgs a) {
     using S = MixedViscShape<TX, TY, TZ>;
     constexpr int NC = S::NC, BX = S::BX, BY = S::BY, NB = S::NB;
     extern __shared__ double smem_d[];
@@ -412,8 +414,10 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
     auto bidx = [&](int i, int j, int k) { return ((k + 1) * BY + (j + 1)) * BX + (i + 1); };
     // whether a side of the tile lies on a side of the mesh that is neither periodic nor a part interface
     bool walls = false;
+    if constexpr (WALLS) {
 #pragma unroll
-    for (int x = 0; x < 3; ++x) walls = walls || (o3[x] == 0 && !a.through[2 * x]) || (o3[x] + (x == 0 ? TX : (x == 1 ? TY : TZ)) >= n3[x] && !a.through[2 * x + 1]);
+        for (int x = 0; x < 3; ++x) walls = walls || (o3[x] == 0 && !a.through[2 * x]) || (o3[x] + (x == 0 ? TX : (x == 1 ? TY : TZ)) >= n3[x] && !a.through[2 * x + 1]);
+    }
     const bool full = o3[0] + TX <= n3[0] && o3[1] + TY <= n3[1] && o3[2] + TZ <= n3[2];   // no cell of the tile beyond the mesh
     for (int e = tid; e < NB; e += NT) {
         int g[3] = {o3[0] + e % BX - 1, o3[1] + (e / BX) % BY - 1, o3[2] + e / (BX * BY) - 1};
@@ -422,7 +426,11 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
             if (a.periodic[x] && (g[x] < 0 || g[x] >= n3[x])) g[x] = ((g[x] % n3[x]) + n3[x]) % n3[x];
 #pragma unroll
         for (int x = 0; x < 3; ++x) g[x] = box_clamp(a, x, g[x], n3[x]);
-        const St<double, 5> u = walls ? padded_cons(a, g[0], g[1], g[2]) : cell_at(a, g[0], g[1], g[2]);
+        St<double, 5> u;
+        if constexpr (WALLS)
+            u = walls ? padded_cons(a, g[0], g[1], g[2]) : cell_at(a, g[0], g[1], g[2]);
+        else
+            u = cell_at(a, g[0], g[1], g[2]);
         double inv;
         const St<double, 5> w = c2p(a.eos, u, inv);
         R[e] = (float)u[0];
@@ -474,7 +482,7 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
             bool inside = true;
             int xL = eL, xR = eR;
             bool phys = false, lo = false;
-            if (walls) {
+            if (WALLS && walls) {
                 const int g3[3] = {o3[0] + f3[0], o3[1] + f3[1], o3[2] + f3[2]};
 #pragma unroll
                 for (int x = 0; x < 3; ++x) inside = inside && (x == d ? g3[x] <= n3[x] : g3[x] < n3[x]);
@@ -492,7 +500,7 @@ __global__ void __launch_bounds__(NT) mixed_viscous_kernel(const ViscArgs a) {
             }
             if (inside) {
                 float Gc[4];
-                if (phys) {
+                if (WALLS && phys) {
 #pragma unroll
                     for (int s = 0; s < 4; ++s) {
                         const int ga = GA[d][s], gb = GB[d][s];
