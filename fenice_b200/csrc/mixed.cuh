@@ -386,11 +386,10 @@ __device__ __forceinline__ float f4c(float4 v, int a) { return a == 0 ? v.x : (a
 // periodic sides and part interfaces around it) reads its box without the ghost rules and solves its faces without the
 // wall tests; a tile wholly inside the mesh skips the test for faces beyond it. The four values a position, a face or a
 // cell carries sit together in one float4 (one shared-memory access each); each axis's balance shares a phase with the
-// next axis's gradients (six barriers per tile). Measured at 256^3 (Taylor-Green): 0.89 ms per launch against 1.14 ms for
+// next axis's gradients (six barriers per tile); WALLS = false drops the ghost rules and wall tests from launches whose
+// every side is periodic or a part interface. Measured at 256^3 (Taylor-Green): 0.77 ms per launch against 1.14 ms for
 // the first form (rho u_a in the box, 1 / rho, the general path for every tile), the same distance from the FP64 viscous
 // residual (1.24e-3 of its largest value, both).
-// WALLS = false: a launch whose every side is periodic or a part interface (no wall, inlet or outlet anywhere): the ghost
-// rules and the wall tests are compiled out.
 template <int TX, int TY, int TZ, int NT, bool WALLS = true>
 __global__ void __launch_bounds__(NT, 4) mixed_viscous_kernel(const ViscArgs a) {
     using S = MixedViscShape<TX, TY, TZ>;
@@ -623,8 +622,9 @@ template <int TX, int TY, int TZ> struct MixedTmaShape {
 // Both forms give the bits of mixed_stage_kernel (the explicitly rounded lin5 / weno5z, balance and update), so a face
 // between tiles of the two forms gets one flux. A tile whose boxes would leave the mesh (wrapped or ghost cells) takes the
 // index-mapping loader for those parts. Measured at 256^3 (Taylor-Green, every tile-axis linear, with the viscous sums
-// and U0): 1.72 ms per launch for the cross against 2.12 ms for the per-axis sweep; with WENO5-Z along every axis the
-// per-axis sweep is the faster (2.74 against 3.01 ms: its (face, variable) items spread the WENO5-Z work finer).
+// and U0): 1.60 ms per launch for the cross against 2.11 ms for the per-axis sweep; with WENO5-Z along every axis the
+// per-axis sweep is the faster (2.74 against 3.01 ms for a cross that solved WENO5-Z faces too: the per-axis sweep's
+// (face, variable) items spread the WENO5-Z work finer).
 // Shared memory: the larger of the two layouts (74.1 KB), three CTAs of 384 threads per SM (at most 56 registers).
 struct CrossShape {
     // slots of the cross: the tile's 512 cells in rows of 9 (576 slots: x + 9 y + 72 z, so that a warp reading one x
